@@ -1,0 +1,184 @@
+/*
+ * ragdoll_cuda.h -- C ABI of the B200 (sm_100a) macroblock analysis / reconstruction engine.
+ *
+ * The engine performs the data-parallel half of ragdoll's Balanced H.264 encoder on the GPU:
+ * per-macroblock P_Skip probe, diamond + quarter-pel motion search, intra 16x16 / 4x4 analysis,
+ * 4x4 / 8x8 transform, quantisation, decimation, dequantisation, reconstruction, the in-loop
+ * deblocking filter and SSIM / MS-SSIM of the reconstruction. Entropy coding (CAVLC / CABAC),
+ * slice headers and NAL packing stay on the host, driven by the per-macroblock records below.
+ *
+ * Reference boundary replaced (oddurs/ragdoll):
+ *   H264Encoder::new / with_profile / with_rate_control   crates/ragdoll-codec/src/h264.rs:3032-3135
+ *   H264Encoder::encode_frame                              crates/ragdoll-codec/src/h264.rs:3153
+ *   MB raster loop of encode_frame_body                    crates/ragdoll-codec/src/h264/enc.rs:2382-2434
+ *   EncState::deblock + extend_borders                     crates/ragdoll-codec/src/h264/enc.rs:3776, :165
+ *   ssim_plane_u8 / ms_ssim_plane_u8                       crates/ragdoll-pix/src/metrics.rs:55, :154
+ *   GopRingEncoder::encode_wave (GOP batching)             crates/ragdoll-pipeline/src/lib.rs:543
+ *
+ * Conventions: every entry point returns 0 on success or a negative RG_ERR_* code, and
+ * rg_last_error() describes the most recent failure of the calling thread. A context is used by
+ * one host thread at a time. Pointers are plain host pointers unless a name says "device".
+ */
+#ifndef RAGDOLL_CUDA_H
+#define RAGDOLL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------------------------- */
+#define RG_OK 0
+#define RG_ERR_INVALID (-1)     /* bad argument or dimension (RagdollError::InvalidArgument)  */
+#define RG_ERR_OOM (-2)         /* device allocation failed                                    */
+#define RG_ERR_CUDA (-3)        /* CUDA runtime error                                          */
+#define RG_ERR_TIMEOUT (-4)     /* a device wait gave up (bounded spin)                         */
+#define RG_ERR_UNSUPPORTED (-5) /* configuration outside the GPU form (RagdollError::Unsupported)*/
+#define RG_ERR_STATE (-6)       /* call out of order (e.g. P frame before any IDR)              */
+
+/* ---- configuration ----------------------------------------------------------------------- */
+/* Profile ids follow H264Profile (crates/ragdoll-codec/src/h264.rs:30). */
+#define RG_PROFILE_BASELINE 0
+#define RG_PROFILE_MAIN 1
+#define RG_PROFILE_HIGH 2
+
+/* Frame kinds (PicKind, crates/ragdoll-codec/src/h264/enc.rs:447). */
+#define RG_FRAME_IDR 0
+#define RG_FRAME_P 1
+
+typedef struct rg_config {
+    int32_t width;       /* display width in luma samples (1..8192)                          */
+    int32_t height;      /* display height (1..8192)                                          */
+    int32_t profile;     /* RG_PROFILE_*; Main/High enable CABAC-side decisions, High the 8x8 */
+    int32_t qp;          /* fixed QP 1..51 (RateControlMode::FixedQp)                          */
+    int32_t num_streams; /* independent streams / GOPs analysed together (>= 1)                */
+    int32_t device;      /* CUDA device ordinal                                                */
+} rg_config;
+
+/* ---- per-macroblock decision record ------------------------------------------------------ */
+#define RG_MB_P_SKIP 0
+#define RG_MB_P_L0_16X16 1
+#define RG_MB_I16X16 2
+#define RG_MB_I4X4 3
+
+/*
+ * One macroblock's decisions and levels, everything the entropy coder reads
+ * (code_inter / code_i16 / code_i4 / code_skip, enc.rs:2874-3772). Levels are stored in coding
+ * (zig-zag) order so the host coder scans nothing.
+ */
+typedef struct rg_mb_out {
+    uint8_t mb_type;       /* RG_MB_*                                                          */
+    uint8_t i16_mode;      /* Intra16x16PredMode (0 V, 1 H, 2 DC, 3 plane)                      */
+    uint8_t chroma_mode;   /* intra_chroma_pred_mode (0 DC, 1 H, 2 V, 3 plane)                  */
+    uint8_t cbp;           /* coded_block_pattern: luma bits 0-3 | chroma (0..2) << 4           */
+    uint8_t transform_8x8; /* transform_size_8x8_flag of an inter MB                            */
+    uint8_t qp;            /* QP_Y of the macroblock                                            */
+    int8_t qp_delta;       /* mb_qp_delta (0 under fixed QP)                                    */
+    uint8_t reserved0;
+    int16_t mv[2];         /* motion vector, quarter samples (P_Skip: the skip vector)          */
+    int16_t mvd[2];        /* mv - mvp                                                          */
+    uint8_t i4_modes[16];  /* Intra4x4PredMode per 4x4 block, decoding order                     */
+    uint16_t nz_mask;      /* bit b: luma 4x4 block b (decoding order) holds levels            */
+    uint16_t reserved1;
+    int16_t luma[256];     /* 16 blocks x 16 zig-zag levels, or (8x8) 4 blocks x 64 zig-zag     */
+    int16_t luma_dc[16];   /* Intra16x16 DC levels, zig-zag                                     */
+    int16_t chroma_dc[2][4];
+    int16_t chroma_ac[2][4][16]; /* zig-zag; slot 0 (the DC position) is unused              */
+} rg_mb_out;
+
+/* SSIM / MS-SSIM of a reconstruction against its source (QualityReport subset,
+ * crates/ragdoll-pix/src/metrics.rs:13). */
+typedef struct rg_quality {
+    double ssim_y, ssim_u, ssim_v, ssim_avg, ms_ssim;
+    double psnr_y, psnr_u, psnr_v;
+} rg_quality;
+
+typedef struct rg_ctx rg_ctx;
+
+/* Last error message of the calling thread ("" when none). */
+const char* rg_last_error(void);
+
+/* Version string of the library build. */
+const char* rg_version(void);
+
+/*
+ * Creates a context: device buffers for cfg->num_streams streams of one size, each holding its
+ * reference picture and motion state (replaces H264Encoder::new + with_profile +
+ * with_rate_control(FixedQp), h264.rs:3032-3135). Returns NULL on failure (see rg_last_error).
+ */
+rg_ctx* rg_create(const rg_config* cfg);
+
+/* Frees every device and host resource of the context. NULL is allowed. */
+void rg_destroy(rg_ctx* ctx);
+
+/* Coded (macroblock-aligned) size in macroblocks. */
+int rg_mb_dims(const rg_ctx* ctx, int32_t* mb_w, int32_t* mb_h);
+
+/*
+ * Analyses, reconstructs and deblocks one frame of one stream from host planes (replaces
+ * encode_frame_body's macroblock loop, deblock and border extension, enc.rs:2382-2503).
+ * kind: RG_FRAME_IDR or RG_FRAME_P (a P frame needs an earlier frame of the stream).
+ * out: mb_w * mb_h records in raster order (may be NULL to skip the copy).
+ */
+int rg_analyse_frame(rg_ctx* ctx, int32_t stream, const uint8_t* y, const uint8_t* u,
+                     const uint8_t* v, size_t stride_y, size_t stride_uv, int32_t kind,
+                     rg_mb_out* out);
+
+/*
+ * Batched form of rg_analyse_frame: the next frame of every stream, all analysed in one
+ * macroblock wavefront (one launch per anti-diagonal step, streams side by side). planes holds
+ * 3 * num_streams host pointers (y, u, v per stream); kinds one RG_FRAME_* per stream; out
+ * num_streams * mb_w * mb_h records (stream-major) or NULL.
+ */
+int rg_analyse_batch(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y,
+                     size_t stride_uv, const int32_t* kinds, rg_mb_out* out);
+
+/*
+ * Same as rg_analyse_batch with the source planes already resident on the device:
+ * dev_planes holds 3 * num_streams device pointers with the given strides. Records stay on the
+ * device (rg_copy_records fetches them). Asynchronous on the context's stream; rg_sync waits.
+ */
+int rg_analyse_batch_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t stride_y,
+                            size_t stride_uv, const int32_t* kinds);
+
+/* Waits for queued device work of the context. */
+int rg_sync(rg_ctx* ctx);
+
+/* Copies the records of the last analysed frame of every stream to host memory. */
+int rg_copy_records(rg_ctx* ctx, rg_mb_out* out);
+
+/*
+ * Copies the deblocked reconstruction (display size) of the last frame of `stream` into host
+ * planes (VideoFrame layout: luma width x height, chroma ceil(w/2) x ceil(h/2)).
+ */
+int rg_get_recon(rg_ctx* ctx, int32_t stream, uint8_t* y, uint8_t* u, uint8_t* v,
+                 size_t stride_y, size_t stride_uv);
+
+/*
+ * Copies the reconstruction before deblocking (coded size, luma mb_w*16 x mb_h*16) of the last
+ * frame of `stream`; used by the parity tests of the deblocking filter.
+ */
+int rg_get_recon_unfiltered(rg_ctx* ctx, int32_t stream, uint8_t* y, uint8_t* u, uint8_t* v);
+
+/*
+ * SSIM of Y/U/V, their (4Y+U+V)/6 average, 5-scale luma MS-SSIM and PSNR of the last
+ * reconstruction of `stream` against the given source planes (evaluate_frame_quality,
+ * crates/ragdoll-pix/src/metrics.rs:328), computed on the device.
+ */
+int rg_quality_frame(rg_ctx* ctx, int32_t stream, const uint8_t* y, const uint8_t* u,
+                     const uint8_t* v, size_t stride_y, size_t stride_uv, rg_quality* q);
+
+/*
+ * Stand-alone plane metrics on host planes (ssim_plane_u8 / ms_ssim_plane_u8,
+ * crates/ragdoll-pix/src/metrics.rs:55, :154), computed on device `device`.
+ */
+int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8_t* b,
+                  size_t stride_b, int32_t width, int32_t height, double* ssim, double* ms_ssim);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RAGDOLL_CUDA_H */

@@ -1,0 +1,121 @@
+"""Seeded synthetic video sources.
+
+Two generators:
+
+* :func:`synth_video_frame` restates ragdoll's procedural test picture (SMPTE-style luma step
+  bars over a moving diagonal gradient, blocky moving chroma), the source of the reference's
+  pinned corpus clips (crates/ragdoll-pipeline/src/lib.rs:2919-2952).
+* :func:`grating_clip` produces the seeded benchmark clips: a sum of four sinusoidal gratings
+  plus blurred uniform noise, shifted per frame by a quarter-sample global motion, with
+  independently moving textured rectangles; chroma is the field decimated 2x plus 128.
+
+Frames are ``(y, u, v)`` tuples of C-contiguous ``uint8`` numpy arrays (``VideoFrame``
+Yuv420p layout: chroma planes ``ceil(w/2) x ceil(h/2)``).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def synth_video_frame(width: int, height: int, frame_idx: int):
+    """Procedural frame ``frame_idx`` (crates/ragdoll-pipeline/src/lib.rs:2919)."""
+    shift = frame_idx * 4
+    y = np.empty((height, width), np.uint8)
+    xs = np.arange(width)
+    bars = (16 + ((xs * 8) // max(width, 1)) * 28).astype(np.uint8)
+    top = height // 3
+    y[:top, :] = bars[None, :]
+    yy = np.arange(top, height)[:, None]
+    g = ((xs[None, :] + yy + shift) >> 2) & 0xFF
+    y[top:, :] = (16 + (g * 219) // 255).astype(np.uint8)
+    cw, ch = (width + 1) // 2, (height + 1) // 2
+    cx = np.arange(cw)
+    cy = np.arange(ch)
+    u_row = (96 + (((cx + shift // 2) // 16) & 0x3F)).astype(np.uint8)
+    v_col = (160 - (((cy + shift // 2) // 16) & 0x3F)).astype(np.uint8)
+    u = np.ascontiguousarray(np.broadcast_to(u_row[None, :], (ch, cw)))
+    v = np.ascontiguousarray(np.broadcast_to(v_col[:, None], (ch, cw)))
+    return y, u, v
+
+
+def _blur_1d(a: np.ndarray, sigma: float, axis: int) -> np.ndarray:
+    r = int(np.ceil(3 * sigma))
+    k = np.exp(-0.5 * (np.arange(-r, r + 1) / sigma) ** 2)
+    k /= k.sum()
+    pad = [(0, 0)] * a.ndim
+    pad[axis] = (r, r)
+    ap = np.pad(a, pad, mode="reflect")
+    out = np.zeros_like(a)
+    for i, w in enumerate(k):
+        sl = [slice(None)] * a.ndim
+        sl[axis] = slice(i, i + a.shape[axis])
+        out += w * ap[tuple(sl)]
+    return out
+
+
+def grating_clip(width: int, height: int, frames: int, seed: int, motion: float = 8.0,
+                 rects: int = 6):
+    """Seeded grating clip: a list of ``frames`` Yuv420p frames.
+
+    Luma is the sum of 4 sinusoidal gratings (periods 8-64 px, random orientation and phase)
+    plus Gaussian-blurred (sigma 1.5) uniform noise of amplitude +-20, clamped to [16, 235].
+    Each frame moves the whole field by a global shift drawn uniformly in +-``motion`` px at
+    quarter-sample precision (the gratings are evaluated at the shifted coordinates and the
+    noise field is resampled bilinearly), and ``rects`` textured rectangles of 64-256 px move
+    independently. Chroma is the field decimated 2x (2x2 mean) plus an offset of 128.
+    """
+    rng = np.random.default_rng(seed)
+    periods = rng.uniform(8, 64, 4)
+    angles = rng.uniform(0, np.pi, 4)
+    phases = rng.uniform(0, 2 * np.pi, 4)
+    amps = rng.uniform(12, 28, 4)
+    pad = int(np.ceil(motion * frames)) + 8
+    nh, nw = height + 2 * pad, width + 2 * pad
+    noise = rng.uniform(-20, 20, (nh, nw)).astype(np.float32)
+    noise = _blur_1d(_blur_1d(noise, 1.5, 0), 1.5, 1)
+    rect_state = []
+    for _ in range(rects):
+        rw, rh = rng.integers(64, 257, 2)
+        rx, ry = rng.uniform(0, max(1, width - rw)), rng.uniform(0, max(1, height - rh))
+        vx, vy = rng.uniform(-motion, motion, 2)
+        tex_p = rng.uniform(6, 24)
+        tex_a = rng.uniform(0, np.pi)
+        base = rng.uniform(40, 215)
+        rect_state.append([rw, rh, rx, ry, vx, vy, tex_p, tex_a, base])
+    ys, xs = np.mgrid[0:height, 0:width].astype(np.float32)
+    out = []
+    gx = gy = 0.0
+    for f in range(frames):
+        if f:
+            gx += np.round(rng.uniform(-motion, motion) * 4) / 4
+            gy += np.round(rng.uniform(-motion, motion) * 4) / 4
+        X, Y = xs + gx, ys + gy
+        field = np.full((height, width), 126.0, np.float32)
+        for p, a, ph, am in zip(periods, angles, phases, amps):
+            field += am * np.sin(2 * np.pi * (X * np.cos(a) + Y * np.sin(a)) / p + ph)
+        # bilinear resample of the static noise field at the shifted grid
+        nx, ny = X + pad, Y + pad
+        x0, y0 = np.floor(nx).astype(np.int64), np.floor(ny).astype(np.int64)
+        fx, fy = nx - x0, ny - y0
+        x0 = np.clip(x0, 0, nw - 2)
+        y0 = np.clip(y0, 0, nh - 2)
+        n = (noise[y0, x0] * (1 - fx) * (1 - fy) + noise[y0, x0 + 1] * fx * (1 - fy)
+             + noise[y0 + 1, x0] * (1 - fx) * fy + noise[y0 + 1, x0 + 1] * fx * fy)
+        field += n
+        for r in rect_state:
+            rw, rh, rx, ry, vx, vy, tp, ta, base = r
+            x0r, y0r = int(round(rx + vx * f)), int(round(ry + vy * f))
+            xa, xb = max(0, x0r), min(width, x0r + int(rw))
+            ya, yb = max(0, y0r), min(height, y0r + int(rh))
+            if xa < xb and ya < yb:
+                lx, ly = xs[ya:yb, xa:xb] - x0r, ys[ya:yb, xa:xb] - y0r
+                field[ya:yb, xa:xb] = base + 30 * np.sin(
+                    2 * np.pi * (lx * np.cos(ta) + ly * np.sin(ta)) / tp)
+        y = np.clip(np.rint(field), 16, 235).astype(np.uint8)
+        cw, ch = (width + 1) // 2, (height + 1) // 2
+        fp = np.pad(field, ((0, 2 * ch - height), (0, 2 * cw - width)), mode="edge")
+        c = fp.reshape(ch, 2, cw, 2).mean(axis=(1, 3)) - 126.0
+        u = np.clip(np.rint(c * 0.5 + 128), 16, 240).astype(np.uint8)
+        v = np.clip(np.rint(-c * 0.4 + 128), 16, 240).astype(np.uint8)
+        out.append((np.ascontiguousarray(y), np.ascontiguousarray(u), np.ascontiguousarray(v)))
+    return out
