@@ -163,6 +163,23 @@ int rg_get_recon(rg_ctx* ctx, int32_t stream, uint8_t* y, uint8_t* u, uint8_t* v
 int rg_get_recon_unfiltered(rg_ctx* ctx, int32_t stream, uint8_t* y, uint8_t* u, uint8_t* v);
 
 /*
+ * Deblocked reconstruction of the last frame of `stream` at coded size (luma mb_w*16 x
+ * mb_h*16, chroma half that, tightly packed): the reference picture the next P frame predicts
+ * from, as EncState::refp holds it after deblock (enc.rs:2470-2490).
+ */
+int rg_get_recon_coded(rg_ctx* ctx, int32_t stream, uint8_t* y, uint8_t* u, uint8_t* v);
+
+/*
+ * Keeps a device copy of every reconstruction before deblocking so that
+ * rg_get_recon_unfiltered can return it (a test hook of this library; costs one extra store per
+ * macroblock while enabled).
+ */
+int rg_keep_unfiltered(rg_ctx* ctx, int32_t enable);
+
+/* The context's CUDA stream (cudaStream_t) for callers that time or order work around it. */
+void* rg_cuda_stream(rg_ctx* ctx);
+
+/*
  * SSIM of Y/U/V, their (4Y+U+V)/6 average, 5-scale luma MS-SSIM and PSNR of the last
  * reconstruction of `stream` against the given source planes (evaluate_frame_quality,
  * crates/ragdoll-pix/src/metrics.rs:328), computed on the device.

@@ -1,0 +1,76 @@
+// Internal layout shared by the engine kernels (engine_kernels.cu) and the C-ABI (rg_api.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ragdoll_cuda.h"
+
+namespace rg {
+
+// Padding of the reconstructed planes. Motion compensation of a vector within the Balanced
+// search bounds (MV_MARGIN = 28 samples past the edge, enc.rs:61) plus the 6-tap reach stays
+// within 48 luma / 16 chroma samples; 64 / 32 keep every row 64-byte aligned.
+constexpr int kPadY = 64;
+constexpr int kPadC = 32;
+constexpr int kMaxStreams = 1024;
+
+// Per-macroblock state read by later macroblocks of the same picture (motion prediction,
+// intra mode prediction) and by the deblocking filter; 16 bytes, one per macroblock.
+struct __align__(16) MbInfo {
+  int16_t mv[2];      // quarter-sample vector (0 for intra)
+  int8_t ref;         // 0 inter / skip, -1 intra
+  uint8_t flags;      // bit 0 intra, bit 1 skip, bit 2 transform 8x8 with levels
+  uint8_t cbp_luma;   // coded_block_pattern luma bits
+  uint8_t qp;         // QP_Y
+  uint16_t nz16;      // 4x4 luma blocks holding levels (decoding-order bit)
+  uint16_t i4_bottom;  // Intra4x4PredMode of the bottom row, 4 bits per x = 0..3 (2 if not I4x4)
+  uint16_t i4_right;   // of the right column, 4 bits per y = 0..3
+  uint16_t pad_;
+};
+static_assert(sizeof(MbInfo) == 16, "MbInfo layout");
+
+constexpr uint8_t kFlagIntra = 1, kFlagSkip = 2, kFlagT8 = 4;
+
+// Device view of one stream for one picture.
+struct StreamDev {
+  const uint8_t* src_y;   // source planes (display size, any stride)
+  const uint8_t* src_u;
+  const uint8_t* src_v;
+  uint8_t* cur_y;         // reconstruction being built: pointer to sample (0, 0) of the padded plane
+  uint8_t* cur_u;
+  uint8_t* cur_v;
+  const uint8_t* ref_y;   // previous (deblocked, border-extended) reconstruction
+  const uint8_t* ref_u;
+  const uint8_t* ref_v;
+  MbInfo* info;           // this picture's macroblock state
+  const MbInfo* prev_info;  // previous picture's (co-located candidate vectors)
+  rg_mb_out* rec;         // decision records (raster order)
+  uint8_t* unf_y;         // optional copy of the reconstruction before deblocking (coded size)
+  uint8_t* unf_u;
+  uint8_t* unf_v;
+  int32_t kind;           // RG_FRAME_IDR or RG_FRAME_P
+  int32_t pad_;
+};
+
+// Frame-constant parameters of one wavefront (all streams share the size and QP).
+struct FrameParams {
+  int32_t width, height;      // display size
+  int32_t mb_w, mb_h;
+  int32_t src_stride_y, src_stride_uv;
+  int32_t stride_y, stride_c; // padded reconstruction strides
+  int32_t qp, qpc;
+  int32_t t8x8;               // High profile: 8x8 transform decision (needs CABAC too)
+  int32_t deblock;            // disable_deblocking_filter_idc == 0
+  // SkipBounds (enc.rs:2104) of qp
+  uint32_t sb_luma, sb_luma_ssd, sb_chroma, sb_chroma_ssd, sb_probe;
+  int32_t n_streams;
+};
+
+// Host launchers (engine_kernels.cu).
+void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st);
+void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st);
+int wavefront_steps(const FrameParams& fp);
+void upload_tables();
+
+}  // namespace rg

@@ -1,0 +1,1875 @@
+// B200 (sm_100a) macroblock engine: one warp analyses, reconstructs or deblocks one macroblock.
+//
+// A picture is processed as a 2:1 wavefront over anti-diagonals d = mb_x + 2 mb_y: every
+// macroblock of diagonal d depends only on macroblocks of smaller diagonals (left, top, top-left
+// and top-right neighbours: unfiltered reconstruction for intra edges, motion for the median
+// predictor), so one launch per diagonal reproduces the reference's raster-order decisions
+// exactly. Deblocking of diagonal d runs in the launch of analysis diagonal d + 3: by then every
+// macroblock that reads its unfiltered pixels (right, below, below-left, below-right neighbours)
+// has been analysed, and the two touch disjoint samples. Streams (independent GOPs) sit side by
+// side in blockIdx.y.
+//
+// Arithmetic follows ragdoll's Balanced encoder (crates/ragdoll-codec/src/h264/enc.rs) and the
+// scalar kernels it calls (crates/ragdoll-simd/src/*.rs); citations are given per function.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "engine.h"
+#include "h264_consts.h"
+
+namespace rg {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr uint32_t UMAX = 0xffffffffu;
+
+__constant__ uint16_t c_lambda[52];
+__constant__ uint8_t c_dec4[16];
+__constant__ uint8_t c_dec8[64];
+__constant__ uint8_t c_scan4[16];
+__constant__ uint8_t c_scan8[64];
+__constant__ uint16_t c_mf4[6][3];
+__constant__ uint8_t c_dq4[6][3];
+__constant__ uint16_t c_mf8[6][6];
+__constant__ uint8_t c_dq8[6][6];
+__constant__ uint8_t c_cqp[52];
+__constant__ uint8_t c_alpha[52];
+__constant__ uint8_t c_beta[52];
+__constant__ uint8_t c_tc0[52][3];
+
+// ---------------------------------------------------------------------------------------------
+// Shared memory of one macroblock warp.
+struct __align__(16) Smem {
+  uint8_t src_y[256];
+  uint8_t src_u[64];
+  uint8_t src_v[64];
+  uint8_t pred_y[256];
+  uint8_t pred_u[64];
+  uint8_t pred_v[64];
+  uint8_t tmp_y[256];       // plane prediction / I4x4 reconstruction
+  uint8_t cand_u[64];       // chroma intra candidates
+  uint8_t cand_v[64];
+  uint8_t win[23 * 24];     // integer samples of a half-sample window (rows -2.., cols -2..)
+  uint8_t hph[18 * 20];     // b samples (horizontal half)
+  uint8_t hpv[18 * 20];     // h samples (vertical half)
+  uint8_t hpj[18 * 20];     // j samples (centre)
+  int16_t hr[23 * 18];      // unrounded horizontal 6-tap sums
+  int16_t coef[256];        // luma 4x4 levels: block b (decoding order) at [16 b], raster
+  int16_t coef8[256];       // luma 8x8 levels: block b at [64 b], raster
+  int32_t t8[256];          // 8x8 transform intermediates
+  int16_t ccoef[128];       // chroma levels: block (plane * 4 + b) at [16 *], raster
+  int16_t cdcraw[8];
+  int16_t cdc[8];
+  int16_t ldc[16];          // I16x16 DC levels, raster
+  int16_t ldcr[16];         // I16x16 DC reconstruction, raster
+  uint8_t top[24];          // luma row above the macroblock (x0 .. x0 + 23)
+  uint8_t left[16];
+  uint8_t ctop[2][8];
+  uint8_t cleft[2][8];
+  uint8_t i4m[16];          // Intra4x4PredMode of this macroblock (decoding order)
+  uint8_t i4pred[16];
+  int16_t i4d[16];
+  int32_t i4t[16];
+  int32_t red[32];
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ uint32_t wsum(uint32_t v) { return __reduce_add_sync(FULL, v); }
+__device__ __forceinline__ uint32_t wmin(uint32_t v) { return __reduce_min_sync(FULL, v); }
+__device__ __forceinline__ uint32_t wor(uint32_t v) { return __reduce_or_sync(FULL, v); }
+__device__ __forceinline__ int clip255(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+__device__ __forceinline__ int16_t clamp_i16(int v) { return (int16_t)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v)); }
+
+// Column and row of 4x4 block b in decoding order (enc.rs:522 blk_xy).
+__device__ __forceinline__ int blk_x(int b) { return (b & 1) + ((b >> 1) & 2); }
+__device__ __forceinline__ int blk_y(int b) { return ((b >> 1) & 1) + ((b >> 2) & 2); }
+// Position class of raster coefficient i in a 4x4 / 8x8 block (h264.rs:1204, :1343).
+__device__ __forceinline__ int pos4(int i) {
+  int r = i >> 2, c = i & 3;
+  if (((r | c) & 1) == 0) return 0;
+  return ((r & c) & 1) ? 1 : 2;
+}
+__device__ __forceinline__ int pos8(int i) {
+  int r = (i >> 3) & 3, c = i & 3;
+  if (r == 0 && c == 0) return 0;
+  if ((r & 1) && (c & 1)) return 1;
+  if (r == 2 && c == 2) return 2;
+  if ((r == 0 && (c & 1)) || ((r & 1) && c == 0)) return 3;
+  if ((r == 0 && c == 2) || (r == 2 && c == 0)) return 4;
+  return 5;
+}
+__device__ __forceinline__ int chroma_qp(int qp) { return c_cqp[qp < 0 ? 0 : (qp > 51 ? 51 : qp)]; }
+// Bits of se(v) (enc.rs:546).
+__device__ __forceinline__ uint32_t se_bits(int d) {
+  uint32_t v = (uint32_t)(d < 0 ? -d : d) * 2u - (d > 0 ? 1u : 0u);
+  return 2u * (32u - (uint32_t)__clz(v + 1u)) - 1u;
+}
+__device__ __forceinline__ uint32_t mvd_cost(int d, uint32_t lambda) {
+  uint32_t c = lambda * se_bits(d);
+  return (d >= -4096 && d <= 4096) ? (c & 0xFFFFu) : c;
+}
+
+// 8 unaligned bytes from global memory (two 32-bit words).
+__device__ __forceinline__ uint2 load8(const uint8_t* p) {
+  uintptr_t a = (uintptr_t)p;
+  const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
+  uint32_t sh = (uint32_t)(a & 3) * 8u;
+  uint32_t w0 = b[0], w1 = b[1], w2 = b[2];
+  return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
+}
+__device__ __forceinline__ uint2 ldg8(const uint8_t* p) {
+  uintptr_t a = (uintptr_t)p;
+  const unsigned int* b = (const unsigned int*)(a & ~(uintptr_t)3);
+  uint32_t sh = (uint32_t)(a & 3) * 8u;
+  uint32_t w0 = __ldg(b), w1 = __ldg(b + 1), w2 = __ldg(b + 2);
+  return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
+}
+__device__ __forceinline__ uint32_t vsad8(uint2 a, uint2 b) { return __vsadu4(a.x, b.x) + __vsadu4(a.y, b.y); }
+
+// ---------------------------------------------------------------------------------------------
+// Per-lane transforms (crates/ragdoll-simd/src/fixed.rs:104,192,322; h264_idct.rs:225)
+__device__ __forceinline__ void fdct4(const int* d, int* o) {
+  int t[16];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    int s03 = d[r * 4] + d[r * 4 + 3], s12 = d[r * 4 + 1] + d[r * 4 + 2];
+    int d03 = d[r * 4] - d[r * 4 + 3], d12 = d[r * 4 + 1] - d[r * 4 + 2];
+    t[r * 4] = s03 + s12; t[r * 4 + 1] = 2 * d03 + d12; t[r * 4 + 2] = s03 - s12; t[r * 4 + 3] = d03 - 2 * d12;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    int s03 = t[c] + t[c + 12], s12 = t[c + 4] + t[c + 8], d03 = t[c] - t[c + 12], d12 = t[c + 4] - t[c + 8];
+    o[c] = (int16_t)(s03 + s12); o[c + 4] = (int16_t)(2 * d03 + d12);
+    o[c + 8] = (int16_t)(s03 - s12); o[c + 12] = (int16_t)(d03 - 2 * d12);
+  }
+}
+__device__ __forceinline__ void idct4(const int* c, int* o) {
+  int t[16];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    int e0 = c[r * 4] + c[r * 4 + 2], e1 = c[r * 4] - c[r * 4 + 2];
+    int e2 = (c[r * 4 + 1] >> 1) - c[r * 4 + 3], e3 = c[r * 4 + 1] + (c[r * 4 + 3] >> 1);
+    t[r * 4] = e0 + e3; t[r * 4 + 1] = e1 + e2; t[r * 4 + 2] = e1 - e2; t[r * 4 + 3] = e0 - e3;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int e0 = t[k] + t[k + 8], e1 = t[k] - t[k + 8];
+    int e2 = (t[k + 4] >> 1) - t[k + 12], e3 = t[k + 4] + (t[k + 12] >> 1);
+    o[k] = (int16_t)((e0 + e3 + 32) >> 6); o[k + 4] = (int16_t)((e1 + e2 + 32) >> 6);
+    o[k + 8] = (int16_t)((e1 - e2 + 32) >> 6); o[k + 12] = (int16_t)((e0 - e3 + 32) >> 6);
+  }
+}
+// One row / column of the 8x8 forward transform (fixed.rs:392).
+__device__ __forceinline__ void fdct8_1d(const int* a, int* o) {
+  int a0 = a[0] + a[7], a1 = a[1] + a[6], a2 = a[2] + a[5], a3 = a[3] + a[4];
+  int a4 = a[0] - a[7], a5 = a[1] - a[6], a6 = a[2] - a[5], a7 = a[3] - a[4];
+  int b0 = a0 + a3, b1 = a1 + a2, b2 = a0 - a3, b3 = a1 - a2;
+  int b4 = a5 + a6 + ((a4 >> 1) + a4), b5 = a4 - a7 - ((a6 >> 1) + a6);
+  int b6 = a4 + a7 - ((a5 >> 1) + a5), b7 = a5 - a6 + ((a7 >> 1) + a7);
+  o[0] = b0 + b1; o[1] = b4 + (b7 >> 2); o[2] = b2 + (b3 >> 1); o[3] = b5 + (b6 >> 2);
+  o[4] = b0 - b1; o[5] = b6 - (b5 >> 2); o[6] = (b2 >> 1) - b3; o[7] = (b4 >> 2) - b7;
+}
+// The 1-D inverse 8x8 transform in wrapping 32-bit arithmetic (h264_idct.rs:225).
+__device__ __forceinline__ void idct8_1d(const int* d, int* o) {
+  unsigned a0 = (unsigned)d[0] + (unsigned)d[4];
+  unsigned a1 = (unsigned)d[5] - (unsigned)d[3] - (unsigned)d[7] - (unsigned)(d[7] >> 1);
+  unsigned a2 = (unsigned)d[0] - (unsigned)d[4];
+  unsigned a3 = (unsigned)d[1] + (unsigned)d[7] - (unsigned)d[3] - (unsigned)(d[3] >> 1);
+  unsigned a4 = (unsigned)(d[2] >> 1) - (unsigned)d[6];
+  unsigned a5 = (unsigned)d[7] - (unsigned)d[1] + (unsigned)d[5] + (unsigned)(d[5] >> 1);
+  unsigned a6 = (unsigned)d[2] + (unsigned)(d[6] >> 1);
+  unsigned a7 = (unsigned)d[3] + (unsigned)d[5] + (unsigned)d[1] + (unsigned)(d[1] >> 1);
+  unsigned b0 = a0 + a6, b1 = a1 + (unsigned)((int)a7 >> 2), b2 = a2 + a4, b3 = a3 + (unsigned)((int)a5 >> 2);
+  unsigned b4 = a2 - a4, b5 = (unsigned)((int)a3 >> 2) - a5, b6 = a0 - a6, b7 = a7 - (unsigned)((int)a1 >> 2);
+  o[0] = (int)(b0 + b7); o[1] = (int)(b2 + b5); o[2] = (int)(b4 + b3); o[3] = (int)(b6 + b1);
+  o[4] = (int)(b6 - b1); o[5] = (int)(b4 - b3); o[6] = (int)(b2 - b5); o[7] = (int)(b0 - b7);
+}
+// Decimation score of n zig-zag levels (enc.rs:559 decimate_score).
+__device__ __forceinline__ uint32_t decimate_score(const int16_t* s, int n, const uint8_t* table) {
+  int idx = n;
+  while (idx > 0 && s[idx - 1] == 0) idx--;
+  uint32_t score = 0;
+  while (idx > 0) {
+    idx--;
+    int v = s[idx];
+    if (v > 1 || v < -1) return 9;
+    int run = 0;
+    while (idx > 0 && s[idx - 1] == 0) { idx--; run++; }
+    score += table[run];
+  }
+  return score;
+}
+// SATD of a 4x4 block (metrics.rs:705, halved).
+__device__ __forceinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
+  int t[4][4];
+#pragma unroll
+  for (int y = 0; y < 4; y++) {
+    int d0 = a[y * sa] - b[y * sb], d1 = a[y * sa + 1] - b[y * sb + 1];
+    int d2 = a[y * sa + 2] - b[y * sb + 2], d3 = a[y * sa + 3] - b[y * sb + 3];
+    int s03 = d0 + d3, s12 = d1 + d2, d03 = d0 - d3, d12 = d1 - d2;
+    t[y][0] = s03 + s12; t[y][1] = d03 + d12; t[y][2] = s03 - s12; t[y][3] = d03 - d12;
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    int s03 = t[0][x] + t[3][x], s12 = t[1][x] + t[2][x], d03 = t[0][x] - t[3][x], d12 = t[1][x] - t[2][x];
+    s += abs(s03 + s12) + abs(d03 + d12) + abs(s03 - s12) + abs(d03 - d12);
+  }
+  return s;  // caller halves the sum of the blocks
+}
+
+// ---------------------------------------------------------------------------------------------
+// Half-sample window (h264_enc.rs:747 hpel_window, :803 hpel_window_centre): integer origin
+// (ox, oy); plane coordinate (r, c) is the sample at (ox + c, oy + r).
+__device__ void stage_window(const uint8_t* ref, int stride, int ox, int oy, Smem& sm) {
+  int lane = lane_id();
+  for (int q = lane; q < 23 * 6; q += 32) {
+    int k = q / 6, w = q % 6;
+    const uint8_t* p = ref + (long)(oy - 2 + k) * stride + (ox - 2) + 4 * w;
+    uintptr_t a = (uintptr_t)p;
+    const unsigned int* b = (const unsigned int*)(a & ~(uintptr_t)3);
+    uint32_t sh = (uint32_t)(a & 3) * 8u;
+    uint32_t v = __funnelshift_r(__ldg(b), __ldg(b + 1), sh);
+    *(uint32_t*)&sm.win[k * 24 + 4 * w] = v;
+  }
+  __syncwarp();
+}
+// need: bit 0 b plane (h), bit 1 h plane (v), bit 2 j plane (c)
+__device__ void build_hpel(Smem& sm, int need) {
+  int lane = lane_id();
+  if (need & 5) {
+    for (int i = lane; i < 23 * 18; i += 32) {
+      int k = i / 18, c = i - k * 18;
+      const uint8_t* w = &sm.win[k * 24 + c];
+      sm.hr[i] = (int16_t)(w[0] - 5 * w[1] + 20 * w[2] + 20 * w[3] - 5 * w[4] + w[5]);
+    }
+  }
+  __syncwarp();
+  for (int i = lane; i < 18 * 18; i += 32) {
+    int r = i / 18, c = i - r * 18;
+    if (need & 1) sm.hph[r * 20 + c] = (uint8_t)clip255((sm.hr[(r + 2) * 18 + c] + 16) >> 5);
+    if (need & 2) {
+      const uint8_t* w = &sm.win[r * 24 + c + 2];
+      int v = w[0] - 5 * w[24] + 20 * w[48] + 20 * w[72] - 5 * w[96] + w[120];
+      sm.hpv[r * 20 + c] = (uint8_t)clip255((v + 16) >> 5);
+    }
+    if (need & 4) {
+      const int16_t* t = &sm.hr[r * 18 + c];
+      int j = t[0] - 5 * t[18] + 20 * t[36] + 20 * t[54] - 5 * t[72] + t[90];
+      sm.hpj[r * 20 + c] = (uint8_t)clip255((j + 512) >> 10);
+    }
+  }
+  __syncwarp();
+}
+// Planes a vector with fractional part (fx, fy) reads (window_src, enc.rs:1395).
+__device__ __forceinline__ int planes_needed(int fx, int fy) {
+  if ((fx | fy) == 0) return 0;
+  if (fy == 0) return 1;
+  if (fx == 0) return 2;
+  if (fx == 2 && fy == 2) return 4;
+  if (fx == 2) return 5;
+  if (fy == 2) return 6;
+  return 3;
+}
+// Quarter-sample prediction sample (i, j) of the 16x16 block whose integer position is
+// (wx, wy) in window coordinates (ITU-T H.264 8.4.2.2.1 as h264_luma_mc_scalar, h264_mc.rs:148).
+__device__ __forceinline__ int qpel_sample(const Smem& sm, int wx, int wy, int fx, int fy, int i, int j) {
+  int r = wy + i, c = wx + j;
+#define G_(dr, dc) ((int)sm.win[(r + (dr) + 2) * 24 + c + (dc) + 2])
+#define B_(dr, dc) ((int)sm.hph[(r + (dr)) * 20 + c + (dc)])
+#define V_(dr, dc) ((int)sm.hpv[(r + (dr)) * 20 + c + (dc)])
+#define J_(dr, dc) ((int)sm.hpj[(r + (dr)) * 20 + c + (dc)])
+#define AV(a, b) (((a) + (b) + 1) >> 1)
+  switch (fx | (fy << 2)) {
+    case 0: return G_(0, 0);
+    case 1: return AV(G_(0, 0), B_(0, 0));
+    case 2: return B_(0, 0);
+    case 3: return AV(B_(0, 0), G_(0, 1));
+    case 4: return AV(G_(0, 0), V_(0, 0));
+    case 5: return AV(B_(0, 0), V_(0, 0));
+    case 6: return AV(B_(0, 0), J_(0, 0));
+    case 7: return AV(B_(0, 0), V_(0, 1));
+    case 8: return V_(0, 0);
+    case 9: return AV(V_(0, 0), J_(0, 0));
+    case 10: return J_(0, 0);
+    case 11: return AV(J_(0, 0), V_(0, 1));
+    case 12: return AV(V_(0, 0), G_(1, 0));
+    case 13: return AV(V_(0, 0), B_(1, 0));
+    case 14: return AV(J_(0, 0), B_(1, 0));
+    default: return AV(V_(0, 1), B_(1, 0));
+  }
+#undef G_
+#undef B_
+#undef V_
+#undef J_
+#undef AV
+}
+// 8 prediction samples of this lane (row lane/2, columns 8 (lane&1) ..) packed in two words.
+__device__ __forceinline__ uint2 qpel8(const Smem& sm, int wx, int wy, int fx, int fy) {
+  int lane = lane_id(), i = lane >> 1, j0 = (lane & 1) * 8;
+  uint32_t w[2] = {0, 0};
+#pragma unroll
+  for (int k = 0; k < 8; k++) w[k >> 2] |= (uint32_t)qpel_sample(sm, wx, wy, fx, fy, i, j0 + k) << (8 * (k & 3));
+  return make_uint2(w[0], w[1]);
+}
+__device__ __forceinline__ uint2 src8(const Smem& sm) {
+  int lane = lane_id();
+  return *(const uint2*)&sm.src_y[(lane >> 1) * 16 + (lane & 1) * 8];
+}
+// Prediction of the 16x16 block displaced by mv into pred_y (enc.rs:1058 mc_luma).
+__device__ void mc_luma16(const uint8_t* ref, int stride, int x0, int y0, int mvx, int mvy, Smem& sm) {
+  int ix = x0 + (mvx >> 2), iy = y0 + (mvy >> 2), fx = mvx & 3, fy = mvy & 3;
+  int lane = lane_id();
+  if ((fx | fy) == 0) {
+    uint2 v = ldg8(ref + (long)(iy + (lane >> 1)) * stride + ix + (lane & 1) * 8);
+    *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
+    __syncwarp();
+    return;
+  }
+  stage_window(ref, stride, ix, iy, sm);
+  build_hpel(sm, planes_needed(fx, fy));
+  uint2 v = qpel8(sm, 0, 0, fx, fy);
+  *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
+  __syncwarp();
+}
+// Chroma prediction of both planes (h264_enc.rs:1279 chroma_mc_8x8_x2_scalar; enc.rs:1082).
+__device__ void mc_chroma8(const uint8_t* ru, const uint8_t* rv, int stride, int mbx, int mby, int mvx, int mvy, Smem& sm) {
+  int lane = lane_id();
+  int cx = mbx * 8 + (mvx >> 3), cy = mby * 8 + (mvy >> 3), fx = mvx & 7, fy = mvy & 7;
+  int wa = (8 - fx) * (8 - fy), wb = fx * (8 - fy), wc = (8 - fx) * fy, wd = fx * fy;
+  int plane = lane >> 4, idx = (lane & 15) * 4, r = idx >> 3, c0 = idx & 7;
+  const uint8_t* src = (plane ? rv : ru) + (long)(cy + r) * stride + cx + c0;
+  uint8_t* out = (plane ? sm.pred_v : sm.pred_u) + r * 8 + c0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int a = __ldg(src + k), b = __ldg(src + k + 1), cc = __ldg(src + stride + k), d = __ldg(src + stride + k + 1);
+    out[k] = (uint8_t)((wa * a + wb * b + wc * cc + wd * d + 32) >> 6);
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Quantisation helpers (enc.rs:1703-1779, h264_enc.rs:408)
+__device__ __forceinline__ void quant4_params(int qp, bool intra, uint32_t& shift, uint32_t& bias) {
+  shift = 15 + qp / 6;
+  bias = (1u << shift) / (intra ? 3u : 6u);
+}
+__device__ __forceinline__ int quant_level(int c, uint32_t mf, uint32_t bias, uint32_t shift) {
+  uint32_t a = (uint32_t)(c < 0 ? -c : c);
+  uint64_t l = ((uint64_t)a * mf + bias) >> shift;
+  if (l > 32767) l = 32767;
+  return c < 0 ? -(int)l : (int)l;
+}
+
+// Luma 4x4 residual of pred_y, quantised (inter) and decimated into sm.coef
+// (enc.rs:1810 quant_luma_4x4_inter). Returns cbp; lanes 0..15 own block lane.
+__device__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_out) {
+  int lane = lane_id();
+  int qp = fp.qp;
+  uint32_t shift, bias;
+  quant4_params(qp, false, shift, bias);
+  int my_nz = 0, my_big = 0;
+  uint32_t my_score = 0;
+  if (lane < 16) {
+    int bx = blk_x(lane), by = blk_y(lane);
+    int d[16], c[16];
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        int o = (by * 4 + y) * 16 + bx * 4 + x;
+        d[y * 4 + x] = (int)sm.src_y[o] - (int)sm.pred_y[o];
+      }
+    fdct4(d, c);
+    int16_t zz[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      int l = quant_level(c[i], c_mf4[qp % 6][pos4(i)], bias, shift);
+      sm.coef[lane * 16 + i] = (int16_t)l;
+      if (l) my_nz = 1;
+      if (l > 1 || l < -1) my_big = 1;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) zz[i] = sm.coef[lane * 16 + c_scan4[i]];
+    my_score = decimate_score(zz, 16, c_dec4);
+  }
+  // per-8x8 aggregates (lanes 4g..4g+3)
+  int g_nz = my_nz | __shfl_xor_sync(FULL, my_nz, 1);
+  g_nz |= __shfl_xor_sync(FULL, g_nz, 2);
+  int g_big = my_big | __shfl_xor_sync(FULL, my_big, 1);
+  g_big |= __shfl_xor_sync(FULL, g_big, 2);
+  uint32_t g_sc = my_score + __shfl_xor_sync(FULL, my_score, 1);
+  g_sc += __shfl_xor_sync(FULL, g_sc, 2);
+  int cbp = 0;
+  uint32_t total = 0;
+  int keep[4];
+#pragma unroll
+  for (int g = 0; g < 4; g++) {
+    int nz = __shfl_sync(FULL, g_nz, 4 * g), big = __shfl_sync(FULL, g_big, 4 * g);
+    uint32_t sc = __shfl_sync(FULL, g_sc, 4 * g);
+    keep[g] = 0;
+    if (!nz) continue;
+    if (big) { cbp |= 1 << g; total += 9; keep[g] = 1; continue; }
+    if (sc >= 4) { cbp |= 1 << g; keep[g] = 1; }
+    total += sc;
+  }
+  if (total < 6 && cbp) cbp = 0;
+  if (lane < 16 && !((cbp >> (lane >> 2)) & 1)) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) sm.coef[lane * 16 + i] = 0;
+  }
+  (void)keep;
+  __syncwarp();
+  if (nz_lane_out) *nz_lane_out = (lane < 16 && ((cbp >> (lane >> 2)) & 1)) ? (uint32_t)my_nz : 0u;
+  return cbp;
+}
+
+// Luma 8x8 residual of pred_y, quantised (inter) and decimated into sm.coef8
+// (enc.rs:2041 quant_luma_8x8_inter). Lanes 8b..8b+7 own block b. Returns cbp; *nnz8 = count.
+__device__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint32_t* nnz8) {
+  int lane = lane_id();
+  int b = lane >> 3, q = lane & 7;
+  int bx = (b & 1) * 8, by = (b >> 1) * 8;
+  int qp = fp.qp;
+  uint32_t shift = 16 + qp / 6, bias = (1u << shift) / 6u;
+  {  // row pass: row q of block b
+    int a[8], o[8];
+#pragma unroll
+    for (int x = 0; x < 8; x++) {
+      int off = (by + q) * 16 + bx + x;
+      a[x] = (int)sm.src_y[off] - (int)sm.pred_y[off];
+    }
+    fdct8_1d(a, o);
+#pragma unroll
+    for (int x = 0; x < 8; x++) sm.t8[b * 64 + q * 8 + x] = o[x];
+  }
+  __syncwarp();
+  int my_nz = 0, my_big = 0;
+  {  // column pass: column q
+    int a[8], o[8];
+#pragma unroll
+    for (int y = 0; y < 8; y++) a[y] = sm.t8[b * 64 + y * 8 + q];
+    fdct8_1d(a, o);
+#pragma unroll
+    for (int y = 0; y < 8; y++) {
+      int i = y * 8 + q;
+      int l = quant_level((int16_t)o[y], c_mf8[qp % 6][pos8(i)], bias, shift);
+      sm.coef8[b * 64 + i] = (int16_t)l;
+      if (l) my_nz = 1;
+      if (l > 1 || l < -1) my_big = 1;
+    }
+  }
+  __syncwarp();
+  int bnz = my_nz, bbig = my_big;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) { bnz |= __shfl_xor_sync(FULL, bnz, o); bbig |= __shfl_xor_sync(FULL, bbig, o); }
+  uint32_t score = 0;
+  if (q == 0) {
+    if (!bnz) score = 0;
+    else if (bbig) score = 9;
+    else {
+      int16_t zz[64];
+      for (int i = 0; i < 64; i++) zz[i] = sm.coef8[b * 64 + c_scan8[i]];
+      score = decimate_score(zz, 64, c_dec8);
+    }
+  }
+  int cbp = 0;
+  uint32_t total = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint32_t s = __shfl_sync(FULL, score, 8 * k);
+    total += s;
+    if (s >= 4) cbp |= 1 << k;
+  }
+  if (total < 6 && cbp) cbp = 0;
+  uint32_t cnt = 0;
+  if (!((cbp >> b) & 1)) {
+#pragma unroll
+    for (int y = 0; y < 8; y++) sm.coef8[b * 64 + y * 8 + q] = 0;
+  } else {
+#pragma unroll
+    for (int y = 0; y < 8; y++) cnt += sm.coef8[b * 64 + y * 8 + q] != 0;
+  }
+  __syncwarp();
+  *nnz8 = wsum(cnt);
+  return cbp;
+}
+
+// Chroma residual of pred_u/pred_v (enc.rs:1899 quant_chroma): lanes 0..7 own block
+// (plane = lane / 4, b = lane % 4). Levels into sm.ccoef (raster), DC levels into sm.cdc.
+// Outputs per plane: AC present and AC decimation score. Lanes 0..31 all return the values.
+__device__ void chroma_quant(int qpc, bool intra, Smem& sm, uint32_t ac_any[2], uint32_t ac_score[2]) {
+  int lane = lane_id();
+  uint32_t shift, bias;
+  quant4_params(qpc, intra, shift, bias);
+  uint32_t my_ac = 0, my_score = 0;
+  if (lane < 8) {
+    int p = lane >> 2, b = lane & 3;
+    const uint8_t* s = p ? sm.src_v : sm.src_u;
+    const uint8_t* pr = p ? sm.pred_v : sm.pred_u;
+    int o = (b >> 1) * 32 + (b & 1) * 4;
+    int d[16], c[16];
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) d[y * 4 + x] = (int)s[o + y * 8 + x] - (int)pr[o + y * 8 + x];
+    fdct4(d, c);
+    sm.cdcraw[lane] = (int16_t)c[0];
+    int16_t zz[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) sm.ccoef[lane * 16 + i] = (int16_t)quant_level(c[i], c_mf4[qpc % 6][pos4(i)], bias, shift);
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      zz[i] = sm.ccoef[lane * 16 + c_scan4[i]];
+      if (i && zz[i]) my_ac = 1;
+    }
+    my_score = decimate_score(zz + 1, 15, c_dec4);
+  }
+  __syncwarp();
+  // 2x2 DC transform + quantisation (enc.rs:1938 quant_chroma_dc; f = 2^qbits / 3 always)
+  if (lane == 0 || lane == 4) {
+    int d0 = sm.cdcraw[lane], d1 = sm.cdcraw[lane + 1], d2 = sm.cdcraw[lane + 2], d3 = sm.cdcraw[lane + 3];
+    int had[4] = {d0 + d1 + d2 + d3, d0 - d1 + d2 - d3, d0 + d1 - d2 - d3, d0 - d1 - d2 + d3};
+    int qbits = 16 + qpc / 6, mf = c_mf4[qpc % 6][0], f = (1 << qbits) / 3;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      int a = had[i] < 0 ? -had[i] : had[i];
+      int l = (a * mf + f) >> qbits;
+      sm.cdc[lane + i] = (int16_t)(had[i] < 0 ? -l : l);
+    }
+  }
+  uint32_t pa = my_ac | __shfl_xor_sync(FULL, my_ac, 1);
+  pa |= __shfl_xor_sync(FULL, pa, 2);
+  uint32_t ps = my_score + __shfl_xor_sync(FULL, my_score, 1);
+  ps += __shfl_xor_sync(FULL, ps, 2);
+  ac_any[0] = __shfl_sync(FULL, pa, 0);
+  ac_any[1] = __shfl_sync(FULL, pa, 4);
+  ac_score[0] = __shfl_sync(FULL, ps, 0);
+  ac_score[1] = __shfl_sync(FULL, ps, 4);
+  __syncwarp();
+}
+__device__ __forceinline__ bool chroma_dc_any(const Smem& sm) {
+  bool a = false;
+#pragma unroll
+  for (int i = 0; i < 8; i++) a |= sm.cdc[i] != 0;
+  return a;
+}
+
+// Adds the dequantised chroma residual to pred_u / pred_v (enc.rs:1992 recon_chroma).
+__device__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
+  int lane = lane_id();
+  if (cbpc == 0) return;
+  if (lane < 8) {
+    int p = lane >> 2, b = lane & 3;
+    // dequantize_idct_chroma_dc2x2 (h264.rs:1674)
+    int qmul = (c_dq4[qpc % 6][0] * 16) << (qpc / 6 + 2);
+    int a = sm.cdc[p * 4], bb = sm.cdc[p * 4 + 1], c = sm.cdc[p * 4 + 2], d = sm.cdc[p * 4 + 3];
+    int e = a - bb, apb = a + bb, cmd = c - d, cpd = c + d;
+    int dcr[4] = {((apb + cpd) * qmul) >> 7, ((e + cmd) * qmul) >> 7, ((apb - cpd) * qmul) >> 7, ((e - cmd) * qmul) >> 7};
+    int blk[16], res[16];
+    int scale_shift = qpc / 6;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      int v = 0;
+      if (cbpc >= 2) v = clamp_i16((int)sm.ccoef[lane * 16 + i] * ((int)c_dq4[qpc % 6][pos4(i)] << scale_shift));
+      blk[i] = v;
+    }
+    blk[0] = (int16_t)dcr[b];
+    idct4(blk, res);
+    uint8_t* pr = (p ? sm.pred_v : sm.pred_u) + (b >> 1) * 32 + (b & 1) * 4;
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) pr[y * 8 + x] = (uint8_t)clip255(pr[y * 8 + x] + res[y * 4 + x]);
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Intra prediction (h264.rs:1715 predict_intra_16x16_scalar, :1967 chroma; enc.rs:1561,1586)
+__device__ __forceinline__ int pred16_sample(int mode, const Smem& sm, bool ht, bool hl, int tl, int dc,
+                                             int pa, int pb, int pc, int x, int y) {
+  switch (mode) {
+    case 0: return ht ? sm.top[x] : 128;
+    case 1: return hl ? sm.left[y] : 128;
+    case 2: return dc;
+    default: return clip255((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5);
+  }
+}
+__device__ void plane16_params(const Smem& sm, bool ht, bool hl, int tl, int& pa, int& pb, int& pc) {
+  int H = 0, V = 0;
+  for (int q = 0; q < 8; q++) {
+    int t8 = ht ? sm.top[8 + q] : 128, l8 = hl ? sm.left[8 + q] : 128;
+    int pt = q == 7 ? tl : (ht ? sm.top[6 - q] : 128), pl = q == 7 ? tl : (hl ? sm.left[6 - q] : 128);
+    H += (q + 1) * (t8 - pt);
+    V += (q + 1) * (l8 - pl);
+  }
+  int t15 = ht ? sm.top[15] : 128, l15 = hl ? sm.left[15] : 128;
+  pa = 16 * (t15 + l15);
+  pb = (5 * H + 32) >> 6;
+  pc = (5 * V + 32) >> 6;
+}
+__device__ __forceinline__ int dc16(const Smem& sm, bool ht, bool hl) {
+  uint32_t st = 0, sl = 0;
+  for (int q = 0; q < 16; q++) { st += ht ? sm.top[q] : 0; sl += hl ? sm.left[q] : 0; }
+  if (ht && hl) return (int)((st + sl + 16) >> 5);
+  if (ht) return (int)((st + 8) >> 4);
+  if (hl) return (int)((sl + 8) >> 4);
+  return 128;
+}
+__device__ void pred16_into(int mode, Smem& sm, uint8_t* dst, bool ht, bool hl, int tl) {
+  int lane = lane_id();
+  int dc = mode == 2 ? dc16(sm, ht, hl) : 0;
+  int pa = 0, pb = 0, pc = 0;
+  if (mode == 3) plane16_params(sm, ht, hl, tl, pa, pb, pc);
+  int y = lane >> 1, x0 = (lane & 1) * 8;
+#pragma unroll
+  for (int k = 0; k < 8; k++) dst[y * 16 + x0 + k] = (uint8_t)pred16_sample(mode, sm, ht, hl, tl, dc, pa, pb, pc, x0 + k, y);
+  __syncwarp();
+}
+// Intra 16x16 analysis (enc.rs:1637 analyse_i16_edges): SATD per mode; returns best mode.
+__device__ int analyse_i16(Smem& sm, bool ht, bool hl, int tl, uint32_t* best_cost) {
+  int lane = lane_id();
+  int dc = dc16(sm, ht, hl);
+  uint32_t sv = 0, sh = 0, sd = 0;
+  if (lane < 16) {
+    int bx = lane & 3, by = lane >> 2;
+    // hadamard4x4_16x4_scalar of the source block, out[4 v + h]
+    int rows[4][4];
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const uint8_t* s = &sm.src_y[(by * 4 + y) * 16 + bx * 4];
+      int s01 = s[0] + s[1], d01 = s[0] - s[1], s23 = s[2] + s[3], d23 = s[2] - s[3];
+      rows[y][0] = s01 + s23; rows[y][1] = s01 - s23; rows[y][2] = d01 + d23; rows[y][3] = d01 - d23;
+    }
+    int tv[4], th[4];
+    {
+      const uint8_t* t = &sm.top[bx * 4];
+      int e0 = ht ? t[0] : 0, e1 = ht ? t[1] : 0, e2 = ht ? t[2] : 0, e3 = ht ? t[3] : 0;
+      int s01 = e0 + e1, d01 = e0 - e1, s23 = e2 + e3, d23 = e2 - e3;
+      tv[0] = 4 * (s01 + s23); tv[1] = 4 * (s01 - s23); tv[2] = 4 * (d01 + d23); tv[3] = 4 * (d01 - d23);
+      const uint8_t* l = &sm.left[by * 4];
+      e0 = hl ? l[0] : 0; e1 = hl ? l[1] : 0; e2 = hl ? l[2] : 0; e3 = hl ? l[3] : 0;
+      s01 = e0 + e1; d01 = e0 - e1; s23 = e2 + e3; d23 = e2 - e3;
+      th[0] = 4 * (s01 + s23); th[1] = 4 * (s01 - s23); th[2] = 4 * (d01 + d23); th[3] = 4 * (d01 - d23);
+    }
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      int c0 = rows[0][h], c1 = rows[1][h], c2 = rows[2][h], c3 = rows[3][h];
+      int s01 = c0 + c1, d01 = c0 - c1, s23 = c2 + c3, d23 = c2 - c3;
+      int col[4] = {s01 + s23, s01 - s23, d01 + d23, d01 - d23};
+#pragma unroll
+      for (int v = 0; v < 4; v++) {
+        int c = col[v], k = 4 * v + h;
+        int pv = v == 0 ? tv[h] : 0, ph = h == 0 ? th[v] : 0, pd = k == 0 ? 16 * dc : 0;
+        sv += abs(c - pv); sh += abs(c - ph); sd += abs(c - pd);
+      }
+    }
+  }
+  sv = wsum(sv) >> 1; sh = wsum(sh) >> 1; sd = wsum(sd) >> 1;
+  uint32_t best = sd;
+  int mode = 2;
+  if (ht && sv < best) { best = sv; mode = 0; }
+  if (hl && sh < best) { best = sh; mode = 1; }
+  if (ht && hl) {
+    pred16_into(3, sm, sm.tmp_y, ht, hl, tl);
+    uint32_t s = 0;
+    if (lane < 16) {
+      int bx = lane & 3, by = lane >> 2;
+      s = satd4(&sm.src_y[by * 64 + bx * 4], 16, &sm.tmp_y[by * 64 + bx * 4], 16);
+    }
+    s = wsum(s) >> 1;
+    if (s < best) { best = s; mode = 3; }
+  }
+  *best_cost = best;
+  return mode;
+}
+// Chroma intra prediction sample of mode for plane p at (x, y).
+__device__ __forceinline__ int predc_sample(int mode, const Smem& sm, int p, bool ht, bool hl, int tl, int x, int y,
+                                            const int* dcv, int pa, int pb, int pc) {
+  switch (mode) {
+    case 0: return dcv[(y >> 2) * 2 + (x >> 2)];
+    case 1: return hl ? sm.cleft[p][y] : 128;
+    case 2: return ht ? sm.ctop[p][x] : 128;
+    default: return clip255((pa + pb * (x - 3) + pc * (y - 3) + 16) >> 5);
+  }
+}
+__device__ void chroma_pred_params(const Smem& sm, int p, bool ht, bool hl, int tl, int* dcv, int& pa, int& pb, int& pc) {
+  const uint8_t* t = sm.ctop[p];
+  const uint8_t* l = sm.cleft[p];
+  int st0 = ht ? t[0] + t[1] + t[2] + t[3] : 0, st1 = ht ? t[4] + t[5] + t[6] + t[7] : 0;
+  int sl0 = hl ? l[0] + l[1] + l[2] + l[3] : 0, sl1 = hl ? l[4] + l[5] + l[6] + l[7] : 0;
+  if (ht && hl) {
+    dcv[0] = (st0 + sl0 + 4) >> 3; dcv[1] = (st1 + 2) >> 2; dcv[2] = (sl1 + 2) >> 2; dcv[3] = (st1 + sl1 + 4) >> 3;
+  } else if (ht) {
+    dcv[0] = dcv[2] = (st0 + 2) >> 2; dcv[1] = dcv[3] = (st1 + 2) >> 2;
+  } else if (hl) {
+    dcv[0] = dcv[1] = (sl0 + 2) >> 2; dcv[2] = dcv[3] = (sl1 + 2) >> 2;
+  } else {
+    dcv[0] = dcv[1] = dcv[2] = dcv[3] = 128;
+  }
+  int H = 0, V = 0;
+  for (int q = 0; q < 4; q++) {
+    int t4 = ht ? t[4 + q] : 128, l4 = hl ? l[4 + q] : 128;
+    int pt = q == 3 ? tl : (ht ? t[2 - q] : 128), pl = q == 3 ? tl : (hl ? l[2 - q] : 128);
+    H += (q + 1) * (t4 - pt);
+    V += (q + 1) * (l4 - pl);
+  }
+  pa = 16 * ((ht ? t[7] : 128) + (hl ? l[7] : 128));
+  pb = (17 * H + 16) >> 5;
+  pc = (17 * V + 16) >> 5;
+}
+// Intra chroma mode by SAD (enc.rs:1526 analyse_chroma_intra); best prediction into pred_u/v.
+__device__ int analyse_chroma(Smem& sm, bool ht, bool hl, const int* ctl) {
+  int lane = lane_id();
+  int plane = lane >> 4, idx = (lane & 15) * 4, y = idx >> 3, x0 = idx & 7;
+  int dcv[4], pa, pb, pc;
+  chroma_pred_params(sm, plane, ht, hl, ctl[plane], dcv, pa, pb, pc);
+  const uint8_t* s = (plane ? sm.src_v : sm.src_u) + y * 8 + x0;
+  uint32_t best = UMAX;
+  int bm = 0;
+  for (int mode = 0; mode < 4; mode++) {
+    bool ok = mode == 1 ? hl : (mode == 2 ? ht : (mode == 3 ? (ht && hl) : true));
+    if (!ok) continue;
+    uint32_t sad = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) sad += abs((int)s[k] - predc_sample(mode, sm, plane, ht, hl, ctl[plane], x0 + k, y, dcv, pa, pb, pc));
+    uint32_t cost = wsum(sad) + (mode == 0 ? 0u : 8u);
+    if (cost < best) { best = cost; bm = mode; }
+  }
+  uint8_t* out = (plane ? sm.pred_v : sm.pred_u) + y * 8 + x0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) out[k] = (uint8_t)predc_sample(bm, sm, plane, ht, hl, ctl[plane], x0 + k, y, dcv, pa, pb, pc);
+  __syncwarp();
+  return bm;
+}
+
+// Intra 4x4 prediction of mode m (h264_dsp.rs:799 predict_intra_4x4_u8_scalar) into out[16].
+__device__ void pred4x4(int mode, const uint8_t* t, const uint8_t* l, bool ht, bool hl, int m, uint8_t* o) {
+  int A = t[0], B = t[1], C = t[2], D = t[3], E = t[4], F = t[5], G = t[6], H = t[7];
+  int I = l[0], J = l[1], K = l[2], L = l[3];
+#define A2(x, y) (uint8_t)(((x) + (y) + 1) >> 1)
+#define A3(x, y, z) (uint8_t)(((x) + 2 * (y) + (z) + 2) >> 2)
+  switch (mode) {
+    case 0: for (int i = 0; i < 16; i++) o[i] = t[i & 3]; break;
+    case 1: for (int i = 0; i < 16; i++) o[i] = l[i >> 2]; break;
+    case 2: {
+      int dc;
+      if (ht && hl) dc = (A + B + C + D + I + J + K + L + 4) >> 3;
+      else if (ht) dc = (A + B + C + D + 2) >> 2;
+      else if (hl) dc = (I + J + K + L + 2) >> 2;
+      else dc = 128;
+      for (int i = 0; i < 16; i++) o[i] = (uint8_t)dc;
+      break;
+    }
+    case 3: {
+      uint8_t p[7] = {A3(A, B, C), A3(B, C, D), A3(C, D, E), A3(D, E, F), A3(E, F, G), A3(F, G, H), A3(G, H, H)};
+      for (int y = 0; y < 4; y++) for (int x = 0; x < 4; x++) o[y * 4 + x] = p[x + y];
+      break;
+    }
+    case 4: {
+      uint8_t lm = A3(K, J, I), kj = A3(L, K, J), ji = A3(J, I, m), im = A3(I, m, A), ma = A3(m, A, B), ab = A3(A, B, C), bc = A3(B, C, D);
+      uint8_t r[16] = {im, ma, ab, bc, ji, im, ma, ab, lm, ji, im, ma, kj, lm, ji, im};
+      for (int i = 0; i < 16; i++) o[i] = r[i];
+      break;
+    }
+    case 5: {
+      uint8_t r0[4] = {A2(m, A), A2(A, B), A2(B, C), A2(C, D)};
+      uint8_t r1[4] = {A3(I, m, A), A3(m, A, B), A3(A, B, C), A3(B, C, D)};
+      uint8_t r[16] = {r0[0], r0[1], r0[2], r0[3], r1[0], r1[1], r1[2], r1[3],
+                       A3(J, I, m), r0[0], r0[1], r0[2], A3(K, J, I), r1[0], r1[1], r1[2]};
+      for (int i = 0; i < 16; i++) o[i] = r[i];
+      break;
+    }
+    case 6: {
+      uint8_t r0[4] = {A2(m, I), A3(I, m, A), A3(m, A, B), A3(A, B, C)};
+      uint8_t r1[4] = {A2(I, J), A3(m, I, J), r0[0], r0[1]};
+      uint8_t r2[4] = {A2(J, K), A3(I, J, K), r1[0], r1[1]};
+      uint8_t r3[4] = {A2(K, L), A3(J, K, L), r2[0], r2[1]};
+      for (int i = 0; i < 4; i++) { o[i] = r0[i]; o[4 + i] = r1[i]; o[8 + i] = r2[i]; o[12 + i] = r3[i]; }
+      break;
+    }
+    case 7: {
+      uint8_t r0[4] = {A2(A, B), A2(B, C), A2(C, D), A2(D, E)};
+      uint8_t r1[4] = {A3(A, B, C), A3(B, C, D), A3(C, D, E), A3(D, E, F)};
+      uint8_t r[16] = {r0[0], r0[1], r0[2], r0[3], r1[0], r1[1], r1[2], r1[3],
+                       r0[1], r0[2], r0[3], A2(E, F), r1[1], r1[2], r1[3], A3(E, F, G)};
+      for (int i = 0; i < 16; i++) o[i] = r[i];
+      break;
+    }
+    default: {
+      uint8_t p0 = A2(I, J), p1 = A3(I, J, K), p2 = A2(J, K), p3 = A3(J, K, L), p4 = A2(K, L), p5 = A3(K, L, L), p6 = (uint8_t)L;
+      uint8_t r[16] = {p0, p1, p2, p3, p2, p3, p4, p5, p4, p5, p6, p6, p6, p6, p6, p6};
+      for (int i = 0; i < 16; i++) o[i] = r[i];
+      break;
+    }
+  }
+#undef A2
+#undef A3
+}
+
+// ---------------------------------------------------------------------------------------------
+struct Ctx {
+  const FrameParams* fp;
+  const StreamDev* sd;
+  int mbx, mby, mb;
+};
+
+// Loads the source macroblock, replicating the last row / column past the picture edges
+// (enc.rs:400 MbSrc::load, h264.rs:3660 extract_mb_planes).
+__device__ void load_source(const Ctx& c, Smem& sm) {
+  const FrameParams& fp = *c.fp;
+  int lane = lane_id();
+  int W = fp.width, H = fp.height, cw = (W + 1) >> 1, ch = (H + 1) >> 1;
+  int y = min(c.mby * 16 + (lane >> 1), H - 1);
+  const uint8_t* row = c.sd->src_y + (long)y * fp.src_stride_y;
+  int x0 = c.mbx * 16 + (lane & 1) * 8;
+#pragma unroll
+  for (int k = 0; k < 8; k++) sm.src_y[(lane >> 1) * 16 + (lane & 1) * 8 + k] = __ldg(row + min(x0 + k, W - 1));
+  int plane = lane >> 4, idx = (lane & 15) * 4, r = idx >> 3, c0 = idx & 7;
+  int cy = min(c.mby * 8 + r, ch - 1);
+  const uint8_t* crow = (plane ? c.sd->src_v : c.sd->src_u) + (long)cy * fp.src_stride_uv;
+  uint8_t* dst = (plane ? sm.src_v : sm.src_u) + r * 8 + c0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) dst[k] = __ldg(crow + min(c.mbx * 8 + c0 + k, cw - 1));
+  __syncwarp();
+}
+// Intra edges from the unfiltered reconstruction of this picture (enc.rs:1459-1521).
+__device__ void load_edges(const Ctx& c, Smem& sm, bool want_topright, int& tl, int* ctl) {
+  const FrameParams& fp = *c.fp;
+  int lane = lane_id();
+  const uint8_t* Y = c.sd->cur_y;
+  int x0 = c.mbx * 16, y0 = c.mby * 16;
+  bool ht = c.mby > 0, hl = c.mbx > 0;
+  if (ht && lane < 24) {
+    bool ok = lane < 16 || (want_topright && c.mbx + 1 < fp.mb_w);
+    sm.top[lane] = ok ? Y[(long)(y0 - 1) * fp.stride_y + x0 + lane] : 0;
+  }
+  if (hl && lane < 16) sm.left[lane] = Y[(long)(y0 + lane) * fp.stride_y + x0 - 1];
+  int cx0 = c.mbx * 8, cy0 = c.mby * 8;
+  if (lane < 16) {
+    int p = lane >> 3, k = lane & 7;
+    const uint8_t* P = p ? c.sd->cur_v : c.sd->cur_u;
+    if (ht) sm.ctop[p][k] = P[(long)(cy0 - 1) * fp.stride_c + cx0 + k];
+    if (hl) sm.cleft[p][k] = P[(long)(cy0 + k) * fp.stride_c + cx0 - 1];
+  }
+  tl = (ht && hl) ? Y[(long)(y0 - 1) * fp.stride_y + x0 - 1] : 128;
+  ctl[0] = (ht && hl) ? c.sd->cur_u[(long)(cy0 - 1) * fp.stride_c + cx0 - 1] : 128;
+  ctl[1] = (ht && hl) ? c.sd->cur_v[(long)(cy0 - 1) * fp.stride_c + cx0 - 1] : 128;
+  __syncwarp();
+}
+
+// Stores the reconstruction of pred_y/u/v (or tmp_y for luma) into the current picture.
+__device__ void store_recon(const Ctx& c, const uint8_t* ly, Smem& sm) {
+  const FrameParams& fp = *c.fp;
+  int lane = lane_id();
+  int y = lane >> 1, x = (lane & 1) * 8;
+  uint2 v = *(const uint2*)&ly[y * 16 + x];
+  *(uint2*)(c.sd->cur_y + (long)(c.mby * 16 + y) * fp.stride_y + c.mbx * 16 + x) = v;
+  if (c.sd->unf_y) {
+    int cw = fp.mb_w * 16;
+    *(uint2*)(c.sd->unf_y + (long)(c.mby * 16 + y) * cw + c.mbx * 16 + x) = v;
+  }
+  if (lane < 16) {
+    int p = lane >> 3, r = lane & 7;
+    uint2 cv = *(const uint2*)&(p ? sm.pred_v : sm.pred_u)[r * 8];
+    uint8_t* P = p ? c.sd->cur_v : c.sd->cur_u;
+    *(uint2*)(P + (long)(c.mby * 8 + r) * fp.stride_c + c.mbx * 8) = cv;
+    uint8_t* U = p ? c.sd->unf_v : c.sd->unf_u;
+    if (U) *(uint2*)(U + (long)(c.mby * 8 + r) * (fp.mb_w * 8) + c.mbx * 8) = cv;
+  }
+}
+
+// Writes the chroma part of the record (chroma levels in zig-zag) and clears the rest.
+__device__ void record_chroma(rg_mb_out* rec, Smem& sm, int cbpc) {
+  int lane = lane_id();
+  if (lane < 8) {
+    int p = lane >> 2, b = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 16; i++) rec->chroma_ac[p][b][i] = (i && cbpc >= 2) ? sm.ccoef[lane * 16 + c_scan4[i]] : 0;
+    if (b == 0)
+      for (int i = 0; i < 4; i++) rec->chroma_dc[p][i] = cbpc >= 1 ? sm.cdc[p * 4 + i] : 0;
+  }
+}
+__device__ void record_header(rg_mb_out* rec, int type, int i16_mode, int cmode, int cbp, int t8, int qp, int mvx, int mvy,
+                              int mvdx, int mvdy, uint16_t nz) {
+  rec->mb_type = (uint8_t)type;
+  rec->i16_mode = (uint8_t)i16_mode;
+  rec->chroma_mode = (uint8_t)cmode;
+  rec->cbp = (uint8_t)cbp;
+  rec->transform_8x8 = (uint8_t)t8;
+  rec->qp = (uint8_t)qp;
+  rec->qp_delta = 0;
+  rec->reserved0 = 0;
+  rec->mv[0] = (int16_t)mvx;
+  rec->mv[1] = (int16_t)mvy;
+  rec->mvd[0] = (int16_t)mvdx;
+  rec->mvd[1] = (int16_t)mvdy;
+  rec->nz_mask = nz;
+  rec->reserved1 = 0;
+}
+__device__ void write_info(const Ctx& c, int flags, int cbpl, int mvx, int mvy, int ref, uint16_t nz, const uint8_t* i4m) {
+  MbInfo inf;
+  inf.mv[0] = (int16_t)mvx;
+  inf.mv[1] = (int16_t)mvy;
+  inf.ref = (int8_t)ref;
+  inf.flags = (uint8_t)flags;
+  inf.cbp_luma = (uint8_t)cbpl;
+  inf.qp = (uint8_t)c.fp->qp;
+  inf.nz16 = nz;
+  inf.i4_bottom = 0;
+  inf.i4_right = 0;
+  for (int k = 0; k < 4; k++) {
+    // bottom row blocks (x = k, y = 3) and right column blocks (x = 3, y = k), decoding order
+    int bb = ((3 >> 1) << 3) | ((k >> 1) << 2) | ((3 & 1) << 1) | (k & 1);
+    int br = ((k >> 1) << 3) | ((3 >> 1) << 2) | ((k & 1) << 1) | (3 & 1);
+    inf.i4_bottom |= (uint16_t)((i4m ? i4m[bb] : 2) << (4 * k));
+    inf.i4_right |= (uint16_t)((i4m ? i4m[br] : 2) << (4 * k));
+  }
+  inf.pad_ = 0;
+  c.sd->info[c.mb] = inf;
+}
+
+// I16x16 coding and reconstruction (enc.rs:3587 code_i16) with prediction mode `mode`.
+__device__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
+  const FrameParams& fp = *c.fp;
+  int lane = lane_id();
+  int qp = fp.qp, qpc = fp.qpc;
+  pred16_into(mode, sm, sm.pred_y, ht, hl, tl);
+  int cmode = analyse_chroma(sm, ht, hl, ctl);
+  uint32_t shift, bias;
+  quant4_params(qp, true, shift, bias);
+  uint32_t my_ac = 0, my_nz = 0;
+  int lv[16];
+  if (lane < 16) {
+    int bx = blk_x(lane), by = blk_y(lane);
+    int d[16], cc[16];
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        int o = (by * 4 + y) * 16 + bx * 4 + x;
+        d[y * 4 + x] = (int)sm.src_y[o] - (int)sm.pred_y[o];
+      }
+    fdct4(d, cc);
+    sm.ldc[by * 4 + bx] = (int16_t)cc[0];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      lv[i] = quant_level(cc[i], c_mf4[qp % 6][pos4(i)], bias, shift);
+      if (lv[i]) my_nz = 1;
+    }
+  }
+  // a group with any level drops its DC slots; AC presence counts only slots 1..15
+  uint32_t gnz = my_nz | __shfl_xor_sync(FULL, my_nz, 1);
+  gnz |= __shfl_xor_sync(FULL, gnz, 2);
+  if (lane < 16) {
+    if (gnz) lv[0] = 0;
+    else {
+#pragma unroll
+      for (int i = 0; i < 16; i++) lv[i] = 0;
+    }
+#pragma unroll
+    for (int i = 1; i < 16; i++) if (lv[i]) my_ac = 1;
+#pragma unroll
+    for (int i = 0; i < 16; i++) sm.coef[lane * 16 + i] = (int16_t)lv[i];
+  }
+  __syncwarp();
+  int cbpl = wor(my_ac) ? 15 : 0;
+  // luma DC: Hadamard (>> 1) + quantisation (enc.rs:1960), then inverse (h264.rs:1645)
+  if (lane == 0) {
+    int t[16], had[16];
+    for (int r = 0; r < 4; r++) {
+      int b0 = sm.ldc[r * 4], b1 = sm.ldc[r * 4 + 1], b2 = sm.ldc[r * 4 + 2], b3 = sm.ldc[r * 4 + 3];
+      int s03 = b0 + b3, s12 = b1 + b2, d03 = b0 - b3, d12 = b1 - b2;
+      t[r * 4] = s03 + s12; t[r * 4 + 1] = d03 + d12; t[r * 4 + 2] = s03 - s12; t[r * 4 + 3] = d03 - d12;
+    }
+    for (int k = 0; k < 4; k++) {
+      int s03 = t[k] + t[k + 12], s12 = t[k + 4] + t[k + 8], d03 = t[k] - t[k + 12], d12 = t[k + 4] - t[k + 8];
+      had[k] = (int16_t)((s03 + s12) >> 1); had[k + 4] = (int16_t)((d03 + d12) >> 1);
+      had[k + 8] = (int16_t)((s03 - s12) >> 1); had[k + 12] = (int16_t)((d03 - d12) >> 1);
+    }
+    int qbits = 16 + qp / 6, mf = c_mf4[qp % 6][0], f = (1 << qbits) / 3;
+    int lvl[16];
+    for (int i = 0; i < 16; i++) {
+      int a = had[i] < 0 ? -had[i] : had[i];
+      int l = (a * mf + f) >> qbits;
+      lvl[i] = had[i] < 0 ? -l : l;
+      sm.ldc[i] = (int16_t)lvl[i];
+    }
+    int qmul = (c_dq4[qp % 6][0] * 16) << (qp / 6 + 2);
+    int tt[16];
+    for (int i = 0; i < 4; i++) {
+      int z0 = lvl[4 * i] + lvl[4 * i + 1], z1 = lvl[4 * i] - lvl[4 * i + 1];
+      int z2 = lvl[4 * i + 2] - lvl[4 * i + 3], z3 = lvl[4 * i + 2] + lvl[4 * i + 3];
+      tt[4 * i] = z0 + z3; tt[4 * i + 1] = z0 - z3; tt[4 * i + 2] = z1 - z2; tt[4 * i + 3] = z1 + z2;
+    }
+    for (int i = 0; i < 4; i++) {
+      int z0 = tt[i] + tt[8 + i], z1 = tt[i] - tt[8 + i], z2 = tt[4 + i] - tt[12 + i], z3 = tt[4 + i] + tt[12 + i];
+      sm.ldcr[i] = (int16_t)(((z0 + z3) * qmul + 128) >> 8);
+      sm.ldcr[4 + i] = (int16_t)(((z1 + z2) * qmul + 128) >> 8);
+      sm.ldcr[8 + i] = (int16_t)(((z1 - z2) * qmul + 128) >> 8);
+      sm.ldcr[12 + i] = (int16_t)(((z0 - z3) * qmul + 128) >> 8);
+    }
+  }
+  uint32_t ac_any[2], ac_sc[2];
+  chroma_quant(qpc, true, sm, ac_any, ac_sc);
+  int cbpc = (ac_any[0] | ac_any[1]) ? 2 : (chroma_dc_any(sm) ? 1 : 0);
+  __syncwarp();
+  // record
+  rg_mb_out* rec = c.sd->rec + c.mb;
+  uint16_t nzm = 0;
+  if (lane < 16) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) rec->luma[lane * 16 + i] = sm.coef[lane * 16 + c_scan4[i]];
+    rec->luma_dc[lane] = sm.ldc[c_scan4[lane]];
+    rec->i4_modes[lane] = 2;
+  }
+  nzm = (uint16_t)__ballot_sync(FULL, lane < 16 && cbpl && my_ac);
+  record_chroma(rec, sm, cbpc);
+  if (lane == 0) record_header(rec, RG_MB_I16X16, mode, cmode, cbpl | (cbpc << 4), 0, qp, 0, 0, 0, 0, nzm);
+  // reconstruction
+  if (lane < 16) {
+    int bx = blk_x(lane), by = blk_y(lane);
+    int blk[16], res[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      int v = sm.coef[lane * 16 + i];
+      blk[i] = cbpl ? clamp_i16(v * ((int)c_dq4[qp % 6][pos4(i)] << (qp / 6))) : v;
+    }
+    blk[0] = sm.ldcr[by * 4 + bx];
+    idct4(blk, res);
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        int o = (by * 4 + y) * 16 + bx * 4 + x;
+        sm.pred_y[o] = (uint8_t)clip255(sm.pred_y[o] + res[y * 4 + x]);
+      }
+  }
+  __syncwarp();
+  chroma_recon(qpc, cbpc, sm);
+  store_recon(c, sm.pred_y, sm);
+  if (lane == 0) write_info(c, kFlagIntra, cbpl, 0, 0, -1, nzm, nullptr);
+}
+
+// I4x4 analysis (enc.rs:3336 analyse_i4): sixteen blocks in decoding order, each choosing among
+// the nine modes by SATD + lambda * mode bits, reconstructed into tmp_y before the next.
+// Returns false when the running cost reaches the budget. Levels go to sm.coef.
+__device__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out) {
+  const FrameParams& fp = *c.fp;
+  int lane = lane_id();
+  int qp = fp.qp;
+  uint32_t lambda = c_lambda[qp];
+  uint32_t shift, bias;
+  quant4_params(qp, true, shift, bias);
+  uint32_t total = lambda * 24;
+  int cbpl = 0;
+  const MbInfo* info = c.sd->info;
+  uint8_t lmodes[4], tmodes[4];
+  for (int k = 0; k < 4; k++) {
+    lmodes[k] = hl_mb ? (info[c.mb - 1].i4_right >> (4 * k)) & 15 : 2;
+    tmodes[k] = ht_mb ? (info[c.mb - fp.mb_w].i4_bottom >> (4 * k)) & 15 : 2;
+  }
+  for (int b = 0; b < 16; b++) {
+    int bx = blk_x(b), by = blk_y(b), px = bx * 4, py = by * 4;
+    bool ht = by > 0 || ht_mb, hl = bx > 0 || hl_mb;
+    uint8_t top[8], left[4];
+    int tl = 128;
+    if (ht) {
+      for (int k = 0; k < 4; k++) top[k] = by > 0 ? sm.tmp_y[(py - 1) * 16 + px + k] : sm.top[px + k];
+      bool tr = !(b == 3 || b == 7 || b == 11 || b == 13 || b == 15) && (b != 5 || c.mbx + 1 < fp.mb_w);
+      for (int k = 0; k < 4; k++) top[4 + k] = tr ? (by > 0 ? sm.tmp_y[(py - 1) * 16 + px + 4 + k] : sm.top[px + 4 + k]) : top[3];
+    } else {
+      for (int k = 0; k < 8; k++) top[k] = 128;
+    }
+    if (hl) {
+      for (int k = 0; k < 4; k++) left[k] = bx > 0 ? sm.tmp_y[(py + k) * 16 + px - 1] : sm.left[py + k];
+    } else {
+      for (int k = 0; k < 4; k++) left[k] = 128;
+    }
+    if (ht && hl) {
+      if (by > 0 && bx > 0) tl = sm.tmp_y[(py - 1) * 16 + px - 1];
+      else if (by > 0) tl = sm.left[py - 1];
+      else if (bx > 0) tl = sm.top[px - 1];
+      else tl = tl_mb;
+    }
+    // predicted mode (h264.rs:3283)
+    int gx = c.mbx * 4 + bx, gy = c.mby * 4 + by;
+    int pm;
+    if (gx == 0 || gy == 0) pm = 2;
+    else {
+      int ml = bx > 0 ? sm.i4m[(((by >> 1) << 3) | (((bx - 1) >> 1) << 2) | ((by & 1) << 1) | ((bx - 1) & 1))] : lmodes[by];
+      int mt = by > 0 ? sm.i4m[((((by - 1) >> 1) << 3) | ((bx >> 1) << 2) | (((by - 1) & 1) << 1) | (bx & 1))] : tmodes[bx];
+      pm = min(ml, mt);
+    }
+    // lanes 0..8: one mode each
+    uint32_t key = UMAX;
+    uint8_t pr[16];
+    if (lane < 9) {
+      int m = lane;
+      bool av = (m == 0 || m == 3 || m == 7) ? ht : ((m == 1 || m == 8) ? hl : (m == 2 ? true : (ht && hl)));
+      if (av) {
+        pred4x4(m, top, left, ht, hl, tl, pr);
+        uint32_t s = satd4(&sm.src_y[py * 16 + px], 16, pr, 4) >> 1;
+        uint32_t cost = s + lambda * (m == pm ? 1u : 4u);
+        key = (cost << 4) | (uint32_t)m;
+      }
+    }
+    key = wmin(key);
+    int bm = (int)(key & 15);
+    total += key >> 4;
+    if (total >= budget) return false;
+    if (lane == bm) {
+      for (int k = 0; k < 16; k++) sm.i4pred[k] = pr[k];
+    }
+    if (lane == 0) sm.i4m[b] = (uint8_t)bm;
+    __syncwarp();
+    // residual transform (matrix form of the core transform) and quantisation: lane k -> coeff k
+    int lvl = 0, dq = 0;
+    if (lane < 16) {
+      int u = lane >> 2, v = lane & 3;
+      const int Cf[4][4] = {{1, 1, 1, 1}, {2, 1, -1, -2}, {1, -1, -1, 1}, {1, -2, 2, -1}};
+      int acc = 0;
+#pragma unroll
+      for (int y = 0; y < 4; y++)
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+          acc += Cf[u][y] * Cf[v][x] * ((int)sm.src_y[(py + y) * 16 + px + x] - (int)sm.i4pred[y * 4 + x]);
+      acc = (int16_t)acc;
+      uint32_t a = (uint32_t)(acc < 0 ? -acc : acc);
+      int l = (int)((a * c_mf4[qp % 6][pos4(lane)] + bias) >> shift);
+      lvl = acc < 0 ? -l : l;
+      dq = clamp_i16(lvl * ((int)c_dq4[qp % 6][pos4(lane)] << (qp / 6)));
+      sm.coef[b * 16 + lane] = (int16_t)lvl;
+      sm.i4d[lane] = (int16_t)dq;
+    }
+    bool nz = __ballot_sync(FULL, lane < 16 && lvl != 0) != 0;
+    __syncwarp();
+    if (nz) cbpl |= 1 << (b >> 2);
+    // inverse transform (rows then columns, fixed.rs:192) and reconstruction
+    if (lane < 4) {
+      int r = lane;
+      int c0 = sm.i4d[r * 4], c1 = sm.i4d[r * 4 + 1], c2 = sm.i4d[r * 4 + 2], c3 = sm.i4d[r * 4 + 3];
+      int e0 = c0 + c2, e1 = c0 - c2, e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1);
+      sm.i4t[r * 4] = e0 + e3; sm.i4t[r * 4 + 1] = e1 + e2; sm.i4t[r * 4 + 2] = e1 - e2; sm.i4t[r * 4 + 3] = e0 - e3;
+    }
+    __syncwarp();
+    if (lane < 4) {
+      int k = lane;
+      int t0 = sm.i4t[k], t4 = sm.i4t[k + 4], t8 = sm.i4t[k + 8], t12 = sm.i4t[k + 12];
+      int e0 = t0 + t8, e1 = t0 - t8, e2 = (t4 >> 1) - t12, e3 = t4 + (t12 >> 1);
+      int res[4] = {(int16_t)((e0 + e3 + 32) >> 6), (int16_t)((e1 + e2 + 32) >> 6), (int16_t)((e1 - e2 + 32) >> 6),
+                    (int16_t)((e0 - e3 + 32) >> 6)};
+      for (int y = 0; y < 4; y++) {
+        int p = sm.i4pred[y * 4 + k];
+        sm.tmp_y[(py + y) * 16 + px + k] = (uint8_t)(nz ? clip255(p + res[y]) : p);
+      }
+    }
+    __syncwarp();
+  }
+  *cbpl_out = cbpl;
+  return true;
+}
+
+__device__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
+  const FrameParams& fp = *c.fp;
+  int lane = lane_id();
+  int qpc = fp.qpc;
+  int cmode = analyse_chroma(sm, ht, hl, ctl);
+  uint32_t ac_any[2], ac_sc[2];
+  chroma_quant(qpc, true, sm, ac_any, ac_sc);
+  int cbpc = (ac_any[0] | ac_any[1]) ? 2 : (chroma_dc_any(sm) ? 1 : 0);
+  rg_mb_out* rec = c.sd->rec + c.mb;
+  uint32_t bnz = 0;
+  if (lane < 16) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      int16_t v = sm.coef[lane * 16 + c_scan4[i]];
+      rec->luma[lane * 16 + i] = v;
+      bnz |= v != 0;
+    }
+    rec->luma_dc[lane] = 0;
+    rec->i4_modes[lane] = sm.i4m[lane];
+  }
+  uint16_t nzm = (uint16_t)__ballot_sync(FULL, lane < 16 && bnz);
+  record_chroma(rec, sm, cbpc);
+  if (lane == 0) record_header(rec, RG_MB_I4X4, 0, cmode, cbpl | (cbpc << 4), 0, fp.qp, 0, 0, 0, 0, nzm);
+  chroma_recon(qpc, cbpc, sm);
+  store_recon(c, sm.tmp_y, sm);
+  if (lane == 0) write_info(c, kFlagIntra, cbpl, 0, 0, -1, nzm, sm.i4m);
+}
+
+// One macroblock of an I slice (enc.rs:3311 code_intra).
+__device__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
+  const FrameParams& fp = *c.fp;
+  int tl, ctl[2];
+  load_edges(c, sm, true, tl, ctl);
+  bool ht = c.mby > 0, hl = c.mbx > 0;
+  uint32_t lambda = c_lambda[fp.qp];
+  uint32_t i16c;
+  int i16m = analyse_i16(sm, ht, hl, tl, &i16c);
+  if (i16c > 40 * lambda) {
+    int cbpl;
+    if (analyse_i4(c, sm, i16c + lambda * 4, ht, hl, tl, &cbpl)) {
+      code_i4(c, sm, cbpl, ht, hl, ctl);
+      return;
+    }
+  }
+  code_i16(c, sm, i16m, ht, hl, tl, ctl);
+}
+
+// Codes P_Skip with vector mv; prediction already in pred_y / pred_u / pred_v.
+__device__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy) {
+  int lane = lane_id();
+  rg_mb_out* rec = c.sd->rec + c.mb;
+  if (lane < 16) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) rec->luma[lane * 16 + i] = 0;
+    rec->luma_dc[lane] = 0;
+    rec->i4_modes[lane] = 2;
+  }
+  if (lane < 8) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) rec->chroma_ac[lane >> 2][lane & 3][i] = 0;
+    rec->chroma_dc[lane >> 2][lane & 3] = 0;
+  }
+  if (lane == 0) {
+    record_header(rec, RG_MB_P_SKIP, 0, 0, 0, 0, c.fp->qp, mvx, mvy, 0, 0, 0);
+    write_info(c, kFlagSkip, 0, mvx, mvy, 0, 0, nullptr);
+  }
+  store_recon(c, sm.pred_y, sm);
+}
+
+// Probe of the skip residual (enc.rs:2163 probe_skip_luma): no level above 1 and a total
+// decimation score below 6.
+__device__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
+  int lane = lane_id();
+  uint32_t shift, bias;
+  quant4_params(fp.qp, false, shift, bias);
+  uint32_t big = 0, score = 0;
+  if (lane < 16) {
+    int bx = blk_x(lane), by = blk_y(lane);
+    int d[16], cc[16];
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        int o = (by * 4 + y) * 16 + bx * 4 + x;
+        d[y * 4 + x] = (int)sm.src_y[o] - (int)sm.pred_y[o];
+      }
+    fdct4(d, cc);
+    int16_t lv[16], zz[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      int l = quant_level(cc[i], c_mf4[fp.qp % 6][pos4(i)], bias, shift);
+      lv[i] = (int16_t)l;
+      if (l > 1 || l < -1) big = 1;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) zz[i] = lv[c_scan4[i]];
+    score = decimate_score(zz, 16, c_dec4);
+  }
+  big = wor(big);
+  score = wsum(score);
+  return !big && score < 6;
+}
+
+// One macroblock of a P slice (enc.rs:3011 code_p_mb).
+__device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
+  const FrameParams& fp = *c.fp;
+  const StreamDev& sd = *c.sd;
+  int lane = lane_id();
+  int mbx = c.mbx, mby = c.mby, mb_w = fp.mb_w;
+  int x0 = mbx * 16, y0 = mby * 16;
+  int qp = fp.qp;
+  uint32_t lambda = c_lambda[qp];
+  int cw = fp.mb_w * 16, chh = fp.mb_h * 16;
+  // MvBounds (enc.rs:1105)
+  int bmin0 = -4 * (x0 + 28), bmin1 = max(-4 * (y0 + 28), -2048);
+  int bmax0 = 4 * (cw - 16 - x0 + 28), bmax1 = min(4 * (chh - 16 - y0 + 28), 2044);
+  // neighbours (this picture)
+  const MbInfo* info = sd.info;
+  int lref = -2, tref = -2, dref = -2;
+  int a0 = 0, a1 = 0, b0 = 0, b1 = 0, c0 = 0, c1 = 0;
+  if (mbx > 0) { MbInfo n = info[c.mb - 1]; lref = n.ref; a0 = n.mv[0]; a1 = n.mv[1]; }
+  if (mby > 0) { MbInfo n = info[c.mb - mb_w]; tref = n.ref; b0 = n.mv[0]; b1 = n.mv[1]; }
+  if (mby > 0 && mbx + 1 < mb_w) { MbInfo n = info[c.mb - mb_w + 1]; dref = n.ref; c0 = n.mv[0]; c1 = n.mv[1]; }
+  else if (mby > 0 && mbx > 0) { MbInfo n = info[c.mb - mb_w - 1]; dref = n.ref; c0 = n.mv[0]; c1 = n.mv[1]; }
+  // pred_motion_partition (h264.rs:3577), 16x16, ref 0
+  int mvp0, mvp1;
+  {
+    auto med = [](int x, int y, int z) { return min(max(x, y), max(min(x, y), z)); };
+    int m = (lref == 0) + (tref == 0) + (dref == 0);
+    if (m > 1) { mvp0 = med(a0, b0, c0); mvp1 = med(a1, b1, c1); }
+    else if (m == 1) {
+      if (lref == 0) { mvp0 = a0; mvp1 = a1; }
+      else if (tref == 0) { mvp0 = b0; mvp1 = b1; }
+      else { mvp0 = c0; mvp1 = c1; }
+    } else if (tref == -2 && dref == -2 && lref != -2) { mvp0 = a0; mvp1 = a1; }
+    else { mvp0 = med(a0, b0, c0); mvp1 = med(a1, b1, c1); }
+  }
+  int ps0 = mvp0, ps1 = mvp1;
+  if (mbx == 0 || mby == 0 || (lref == 0 && a0 == 0 && a1 == 0) || (tref == 0 && b0 == 0 && b1 == 0)) { ps0 = 0; ps1 = 0; }
+  load_source(c, sm);
+  int qpc = fp.qpc;
+
+  // 1. skip probe (enc.rs:2906 try_p_skip)
+  if (ps0 >= bmin0 && ps0 <= bmax0 && ps1 >= bmin1 && ps1 <= bmax1) {
+    mc_luma16(sd.ref_y, fp.stride_y, x0, y0, ps0, ps1, sm);
+    uint2 s = src8(sm), p = *(const uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8];
+    uint32_t sad = wsum(vsad8(s, p));
+    if (sad < fp.sb_probe) {
+      bool lz = sad <= fp.sb_luma;
+      if (!lz) {
+        uint32_t ssd = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          int d0 = (int)((s.x >> (8 * k)) & 255) - (int)((p.x >> (8 * k)) & 255);
+          int d1 = (int)((s.y >> (8 * k)) & 255) - (int)((p.y >> (8 * k)) & 255);
+          ssd += d0 * d0 + d1 * d1;
+        }
+        lz = wsum(ssd) <= fp.sb_luma_ssd;
+      }
+      if (!lz) lz = probe_skip_luma(fp, sm);
+      if (lz) {
+        mc_chroma8(sd.ref_u, sd.ref_v, fp.stride_c, mbx, mby, ps0, ps1, sm);
+        // per plane SAD / SSD bounds (lanes 0..15 U, 16..31 V, 4 samples each)
+        int plane = lane >> 4, idx = (lane & 15) * 4;
+        const uint8_t* ss = (plane ? sm.src_v : sm.src_u) + idx;
+        const uint8_t* pp = (plane ? sm.pred_v : sm.pred_u) + idx;
+        uint32_t sadp = 0, ssdp = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) { int d = (int)ss[k] - (int)pp[k]; sadp += abs(d); ssdp += d * d; }
+        uint32_t sad_u = wsum(plane == 0 ? sadp : 0), sad_v = wsum(plane == 1 ? sadp : 0);
+        uint32_t ssd_u = wsum(plane == 0 ? ssdp : 0), ssd_v = wsum(plane == 1 ? ssdp : 0);
+        bool zu = sad_u <= fp.sb_chroma || ssd_u <= fp.sb_chroma_ssd;
+        bool zv = sad_v <= fp.sb_chroma || ssd_v <= fp.sb_chroma_ssd;
+        bool cz = zu && zv;
+        if (!cz) {
+          uint32_t ac_any[2], ac_sc[2];
+          chroma_quant(qpc, false, sm, ac_any, ac_sc);
+          cz = !chroma_dc_any(sm) && ac_sc[0] < 7 && ac_sc[1] < 7;
+        }
+        if (cz) {
+          code_skip(c, sm, ps0, ps1);
+          return;
+        }
+      }
+    }
+  }
+
+  // 2. motion search (enc.rs:3084-3117)
+  const uint8_t* ref = sd.ref_y;
+  int stride = fp.stride_y;
+  int cand[5][2];
+  int n = 0;
+  cand[n][0] = mvp0; cand[n][1] = mvp1; n++;
+  cand[n][0] = 0; cand[n][1] = 0; n++;
+  if (mbx > 0) { cand[n][0] = a0; cand[n][1] = a1; n++; }
+  if (mby > 0) { cand[n][0] = b0; cand[n][1] = b1; n++; }
+  {
+    MbInfo pv = sd.prev_info[c.mb];
+    cand[n][0] = pv.mv[0]; cand[n][1] = pv.mv[1]; n++;
+  }
+  int imin0 = (bmin0 + 3) >> 2, imin1 = (bmin1 + 3) >> 2, imax0 = bmax0 >> 2, imax1 = bmax1 >> 2;
+  uint2 sv = src8(sm);
+  const uint8_t* base = ref + (long)(y0 + (lane >> 1)) * stride + x0 + (lane & 1) * 8;
+  int best0 = 0, best1 = 0;
+  uint32_t best_cost = UMAX;
+  int seen[5][2];
+  for (int k = 0; k < n; k++) {
+    int mx = min(max((cand[k][0] + 2) >> 2, imin0), imax0);
+    int my = min(max((cand[k][1] + 2) >> 2, imin1), imax1);
+    bool dup = false;
+    for (int j = 0; j < k; j++) dup |= (seen[j][0] == mx && seen[j][1] == my);
+    seen[k][0] = dup ? 0x7fffffff : mx;
+    seen[k][1] = dup ? 0x7fffffff : my;
+    if (dup) continue;
+    uint32_t s = wsum(vsad8(sv, ldg8(base + (long)my * stride + mx)));
+    uint32_t cost = s + mvd_cost(mx * 4 - mvp0, lambda) + mvd_cost(my * 4 - mvp1, lambda);
+    if (cost < best_cost) { best_cost = cost; best0 = mx; best1 = my; }
+  }
+  // diamond (enc.rs:1207-1272)
+  for (int it = 0; it < 16; it++) {
+    int pts[4][2] = {{best0, best1 - 1}, {best0 - 1, best1}, {best0 + 1, best1}, {best0, best1 + 1}};
+    int moved = -1;
+    uint32_t costs[4];
+    const uint8_t* cp = base + (long)best1 * stride + best0;
+    bool in[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) in[k] = pts[k][0] >= imin0 && pts[k][0] <= imax0 && pts[k][1] >= imin1 && pts[k][1] <= imax1;
+    uint32_t s0 = in[0] ? vsad8(sv, ldg8(cp - stride)) : 0;
+    uint32_t s1 = in[1] ? vsad8(sv, ldg8(cp - 1)) : 0;
+    uint32_t s2 = in[2] ? vsad8(sv, ldg8(cp + 1)) : 0;
+    uint32_t s3 = in[3] ? vsad8(sv, ldg8(cp + stride)) : 0;
+    s0 = wsum(s0); s1 = wsum(s1); s2 = wsum(s2); s3 = wsum(s3);
+    uint32_t sads[4] = {s0, s1, s2, s3};
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      costs[k] = in[k] ? sads[k] + mvd_cost(pts[k][0] * 4 - mvp0, lambda) + mvd_cost(pts[k][1] * 4 - mvp1, lambda) : UMAX;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (in[k] && costs[k] < best_cost) { best_cost = costs[k]; moved = k; }
+    if (moved < 0) break;
+    best0 = pts[moved][0]; best1 = pts[moved][1];
+  }
+  int mv0, mv1;
+  {
+    int fm0 = best0 * 4, fm1 = best1 * 4;
+    uint32_t full_mvc = mvd_cost(fm0 - mvp0, lambda) + mvd_cost(fm1 - mvp1, lambda);
+    if (best_cost - full_mvc <= fp.sb_luma) {
+      mv0 = fm0; mv1 = fm1;
+      uint2 v = ldg8(base + (long)best1 * stride + best0);
+      *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
+      __syncwarp();
+    } else {
+      // sub-pel refinement over a half-sample window around the full-pel best (enc.rs:1283)
+      int bxp = x0 + best0, byp = y0 + best1;
+      stage_window(ref, stride, bxp - 1, byp - 1, sm);
+      build_hpel(sm, 7);
+      int q0 = fm0, q1 = fm1;
+      uint32_t bc = best_cost;
+      for (int si = 0; si < 2; si++) {
+        int st = si == 0 ? 2 : 1, iters = si == 0 ? 1 : 2;
+        for (int it = 0; it < iters; it++) {
+          int f0 = q0, f1 = q1;
+          int dd[4][2] = {{0, -st}, {-st, 0}, {st, 0}, {0, st}};
+          uint32_t cc[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            int cx = f0 + dd[k][0], cy = f1 + dd[k][1];
+            bool ok = abs(cx - fm0) <= 3 && abs(cy - fm1) <= 3 && cx >= bmin0 && cx <= bmax0 && cy >= bmin1 && cy <= bmax1;
+            uint32_t s = 0;
+            if (ok) {
+              int wx = (cx >> 2) - best0 + 1, wy = (cy >> 2) - best1 + 1;
+              s = vsad8(sv, qpel8(sm, wx, wy, cx & 3, cy & 3));
+            }
+            s = wsum(s);
+            cc[k] = ok ? s + mvd_cost(cx - mvp0, lambda) + mvd_cost(cy - mvp1, lambda) : UMAX;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (cc[k] < bc) { bc = cc[k]; q0 = f0 + dd[k][0]; q1 = f1 + dd[k][1]; }
+          if (q0 == f0 && q1 == f1) break;
+        }
+      }
+      mv0 = q0; mv1 = q1;
+      uint2 v = qpel8(sm, (q0 >> 2) - best0 + 1, (q1 >> 2) - best1 + 1, q0 & 3, q1 & 3);
+      *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
+      __syncwarp();
+    }
+  }
+
+  // 3. intra 16x16 when the inter prediction is poor (enc.rs:3121-3156)
+  uint32_t inter_satd = 0;
+  if (lane < 16) {
+    int bx = lane & 3, by = lane >> 2;
+    inter_satd = satd4(&sm.src_y[by * 64 + bx * 4], 16, &sm.pred_y[by * 64 + bx * 4], 16);
+  }
+  inter_satd = wsum(inter_satd) >> 1;
+  uint32_t inter_cost = inter_satd + lambda * (se_bits(mv0 - mvp0) + se_bits(mv1 - mvp1) + 1);
+  if (inter_satd > 24 * lambda) {
+    int tl, ctl[2];
+    load_edges(c, sm, false, tl, ctl);
+    bool ht = mby > 0, hl = mbx > 0;
+    uint32_t i16c;
+    int i16m = analyse_i16(sm, ht, hl, tl, &i16c);
+    if (i16c + lambda * 8 < inter_cost) {
+      code_i16(c, sm, i16m, ht, hl, tl, ctl);
+      return;
+    }
+  }
+
+  // 4. P_L0_16x16 residual (enc.rs:3158-3190)
+  mc_chroma8(sd.ref_u, sd.ref_v, fp.stride_c, mbx, mby, mv0, mv1, sm);
+  uint32_t nz_lane;
+  int cbp4 = luma4x4_inter(fp, sm, &nz_lane);
+  int cbpl = cbp4;
+  bool use8 = false;
+  if (fp.t8x8 && cbp4) {
+    uint32_t nnz4 = 0;
+    if (lane < 16)
+      for (int i = 0; i < 16; i++) nnz4 += sm.coef[lane * 16 + i] != 0;
+    nnz4 = wsum(nnz4);
+    uint32_t nnz8;
+    int cbp8 = luma8x8_inter(fp, sm, &nnz8);
+    if (nnz8 <= nnz4) { use8 = true; cbpl = cbp8; }
+  }
+  uint32_t ac_any[2], ac_sc[2];
+  chroma_quant(qpc, false, sm, ac_any, ac_sc);
+  // drop a plane's AC levels when nearly empty (enc.rs:2095)
+  bool drop_u = ac_any[0] && ac_sc[0] < 7, drop_v = ac_any[1] && ac_sc[1] < 7;
+  if (lane < 8) {
+    bool d = (lane >> 2) ? drop_v : drop_u;
+    if (d)
+#pragma unroll
+      for (int i = 0; i < 16; i++) sm.ccoef[lane * 16 + i] = 0;
+  }
+  __syncwarp();
+  bool acu = ac_any[0] && !drop_u, acv = ac_any[1] && !drop_v;
+  int cbpc = (acu || acv) ? 2 : (chroma_dc_any(sm) ? 1 : 0);
+  if (cbpl == 0 && cbpc == 0 && mv0 == ps0 && mv1 == ps1) {
+    code_skip(c, sm, mv0, mv1);
+    return;
+  }
+  // code_inter (enc.rs:3196)
+  rg_mb_out* rec = c.sd->rec + c.mb;
+  bool t8flag = use8 && cbpl != 0;
+  uint16_t nzm;
+  if (use8) {
+    int b = lane >> 3, q = lane & 7;
+#pragma unroll
+    for (int k = 0; k < 8; k++) rec->luma[b * 64 + q * 8 + k] = sm.coef8[b * 64 + c_scan8[q * 8 + k]];
+    nzm = 0;
+    for (int k = 0; k < 4; k++) if ((cbpl >> k) & 1) nzm |= (uint16_t)(0xF << (4 * k));
+  } else {
+    uint32_t bnz = 0;
+    if (lane < 16) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        int16_t v = sm.coef[lane * 16 + c_scan4[i]];
+        rec->luma[lane * 16 + i] = v;
+        bnz |= v != 0;
+      }
+    }
+    nzm = (uint16_t)__ballot_sync(FULL, lane < 16 && bnz);
+  }
+  if (lane < 16) { rec->luma_dc[lane] = 0; rec->i4_modes[lane] = 2; }
+  record_chroma(rec, sm, cbpc);
+  if (lane == 0) {
+    record_header(rec, RG_MB_P_L0_16X16, 0, 0, cbpl | (cbpc << 4), t8flag, qp, mv0, mv1, mv0 - mvp0, mv1 - mvp1, nzm);
+    write_info(c, t8flag ? kFlagT8 : 0, cbpl, mv0, mv1, 0, nzm, nullptr);
+  }
+  // reconstruction
+  if (use8) {
+    int b = lane >> 3, q = lane & 7;
+    bool coded = (cbpl >> b) & 1;
+    if (coded) {  // dequantize_block8x8 (h264.rs:1403) then rows of the inverse transform
+      int qdiv = qp / 6, rem = qp % 6;
+      int d[8], o[8];
+#pragma unroll
+      for (int x = 0; x < 8; x++) {
+        int i = q * 8 + x, v = c_dq8[rem][pos8(i)], l = sm.coef8[b * 64 + i];
+        int dv = qdiv >= 2 ? l * (v << (qdiv - 2)) : ((l * v + (1 << (1 - qdiv))) >> (2 - qdiv));
+        d[x] = clamp_i16(dv);
+      }
+      idct8_1d(d, o);
+#pragma unroll
+      for (int x = 0; x < 8; x++) sm.t8[b * 64 + q * 8 + x] = o[x];
+    }
+    __syncwarp();
+    if (coded) {
+      int d[8], o[8];
+#pragma unroll
+      for (int y = 0; y < 8; y++) d[y] = sm.t8[b * 64 + y * 8 + q];
+      idct8_1d(d, o);
+      int bx = (b & 1) * 8, by = (b >> 1) * 8;
+#pragma unroll
+      for (int y = 0; y < 8; y++) {
+        int off = (by + y) * 16 + bx + q;
+        int v = (int)((unsigned)o[y] + 32u) >> 6;
+        sm.pred_y[off] = (uint8_t)clip255((int)((unsigned)sm.pred_y[off] + (unsigned)v));
+      }
+    }
+  } else if (lane < 16 && ((cbpl >> (lane >> 2)) & 1)) {
+    int bx = blk_x(lane), by = blk_y(lane);
+    int blk[16], res[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) blk[i] = clamp_i16((int)sm.coef[lane * 16 + i] * ((int)c_dq4[qp % 6][pos4(i)] << (qp / 6)));
+    idct4(blk, res);
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        int o = (by * 4 + y) * 16 + bx * 4 + x;
+        sm.pred_y[o] = (uint8_t)clip255(sm.pred_y[o] + res[y * 4 + x]);
+      }
+  }
+  __syncwarp();
+  chroma_recon(qpc, cbpc, sm);
+  store_recon(c, sm.pred_y, sm);
+  (void)nz_lane;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Deblocking of one macroblock (enc.rs:3776 deblock, h264_deblock.rs:71,187): vertical edges
+// then horizontal ones, on a shared-memory tile with 4 samples of the left / top neighbours.
+struct EdgeParams {
+  int alpha, beta, tc0[4];
+  bool strong, on;
+};
+__device__ __forceinline__ EdgeParams edge_params(int qp, const int* bs) {
+  EdgeParams e;
+  int ia = qp < 0 ? 0 : (qp > 51 ? 51 : qp);
+  e.alpha = c_alpha[ia];
+  e.beta = c_beta[ia];
+  e.on = e.alpha != 0 && e.beta != 0;
+  for (int k = 0; k < 4; k++) {
+    int b = bs[k] > 4 ? 4 : bs[k];
+    e.tc0[k] = b == 0 ? -1 : (b == 4 ? 0 : c_tc0[ia][b - 1]);
+  }
+  e.strong = bs[0] == 4;
+  return e;
+}
+__device__ __forceinline__ void luma_line(uint8_t* o, int xs, const EdgeParams& e, int tc0) {
+  if (!e.strong && tc0 < 0) return;
+  int p0 = o[-xs], q0 = o[0], p1 = o[-2 * xs], q1 = o[xs];
+  if (abs(p0 - q0) >= e.alpha || abs(p1 - p0) >= e.beta || abs(q1 - q0) >= e.beta) return;
+  int p2 = o[-3 * xs], q2 = o[2 * xs];
+  bool ap = abs(p2 - p0) < e.beta, aq = abs(q2 - q0) < e.beta;
+  if (!e.strong) {
+    int tc = tc0 + ap + aq;
+    int d = min(max((((q0 - p0) << 2) + (p1 - q1) + 4) >> 3, -tc), tc);
+    o[-xs] = (uint8_t)clip255(p0 + d);
+    o[0] = (uint8_t)clip255(q0 - d);
+    if (ap) o[-2 * xs] = (uint8_t)(p1 + min(max((p2 + ((p0 + q0 + 1) >> 1) - (p1 << 1)) >> 1, -tc0), tc0));
+    if (aq) o[xs] = (uint8_t)(q1 + min(max((q2 + ((p0 + q0 + 1) >> 1) - (q1 << 1)) >> 1, -tc0), tc0));
+  } else {
+    int p3 = o[-4 * xs], q3 = o[3 * xs];
+    bool small = abs(p0 - q0) < ((e.alpha >> 2) + 2);
+    if (ap && small) {
+      o[-xs] = (uint8_t)((p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3);
+      o[-2 * xs] = (uint8_t)((p2 + p1 + p0 + q0 + 2) >> 2);
+      o[-3 * xs] = (uint8_t)((2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3);
+    } else {
+      o[-xs] = (uint8_t)((2 * p1 + p0 + q1 + 2) >> 2);
+    }
+    if (aq && small) {
+      o[0] = (uint8_t)((p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3);
+      o[xs] = (uint8_t)((p0 + q0 + q1 + q2 + 2) >> 2);
+      o[2 * xs] = (uint8_t)((2 * q3 + 3 * q2 + q1 + q0 + p0 + 4) >> 3);
+    } else {
+      o[0] = (uint8_t)((2 * q1 + q0 + p1 + 2) >> 2);
+    }
+  }
+}
+__device__ __forceinline__ void chroma_line(uint8_t* o, int xs, const EdgeParams& e, int tc0) {
+  if (!e.strong && tc0 < 0) return;
+  int p1 = o[-2 * xs], p0 = o[-xs], q0 = o[0], q1 = o[xs];
+  if (abs(p0 - q0) >= e.alpha || abs(p1 - p0) >= e.beta || abs(q1 - q0) >= e.beta) return;
+  if (e.strong) {
+    o[-xs] = (uint8_t)((2 * p1 + p0 + q1 + 2) >> 2);
+    o[0] = (uint8_t)((2 * q1 + q0 + p1 + 2) >> 2);
+  } else {
+    int tc = tc0 + 1;
+    int d = min(max((((q0 - p0) << 2) + (p1 - q1) + 4) >> 3, -tc), tc);
+    o[-xs] = (uint8_t)clip255(p0 + d);
+    o[0] = (uint8_t)clip255(q0 - d);
+  }
+}
+__device__ __forceinline__ int nz_at(uint16_t nz, int bx, int by) {
+  int b = ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1);
+  return (nz >> b) & 1;
+}
+// Boundary strengths of edge e in direction dir (0 vertical); returns false to skip the edge.
+__device__ bool edge_bs(const MbInfo& q, const MbInfo* p, int dir, int e, int* bs) {
+  bool qi = q.flags & kFlagIntra;
+  bool pi = p ? (p->flags & kFlagIntra) : qi;
+  if (qi || pi) {
+    for (int k = 0; k < 4; k++) bs[k] = e == 0 ? 4 : 3;
+    return true;
+  }
+  int coded[4];
+  for (int k = 0; k < 4; k++) {
+    if (dir == 0) coded[k] = nz_at(q.nz16, e, k) | (e == 0 ? nz_at(p->nz16, 3, k) : nz_at(q.nz16, e - 1, k));
+    else coded[k] = nz_at(q.nz16, k, e) | (e == 0 ? nz_at(p->nz16, k, 3) : nz_at(q.nz16, k, e - 1));
+  }
+  bool motion = false;
+  if (e == 0) motion = q.ref != p->ref || abs(q.mv[0] - p->mv[0]) >= 4 || abs(q.mv[1] - p->mv[1]) >= 4;
+  if (!coded[0] && !coded[1] && !coded[2] && !coded[3] && !motion) return false;
+  for (int k = 0; k < 4; k++) bs[k] = coded[k] ? 2 : (motion ? 1 : 0);
+  return true;
+}
+
+__device__ void deblock_mb(const FrameParams& fp, const StreamDev& sd, int mbx, int mby, Smem& sm) {
+  int lane = lane_id();
+  int m = mby * fp.mb_w + mbx;
+  MbInfo q = sd.info[m];
+  MbInfo lf, tp;
+  bool hasl = mbx > 0, hast = mby > 0;
+  if (hasl) lf = sd.info[m - 1];
+  if (hast) tp = sd.info[m - fp.mb_w];
+  auto quiet = [](const MbInfo& i) { return !(i.flags & kFlagIntra) && i.cbp_luma == 0; };
+  if (quiet(q) && (!hasl || (quiet(lf) && lf.mv[0] == q.mv[0] && lf.mv[1] == q.mv[1])) &&
+      (!hast || (quiet(tp) && tp.mv[0] == q.mv[0] && tp.mv[1] == q.mv[1])))
+    return;
+  // tiles: luma 20x20 at (x0-4, y0-4) stride 20 in win; chroma 12x12 each in hph / hpv
+  uint8_t* ty = sm.win;
+  uint8_t* tc[2] = {sm.hph, sm.hpv};
+  const int x0 = mbx * 16, y0 = mby * 16, cx0 = mbx * 8, cy0 = mby * 8;
+  for (int w = lane; w < 100; w += 32) {  // 20 rows x 5 words
+    int r = w / 5, k = w % 5;
+    if ((r < 4 && !hast) || (k == 0 && !hasl)) continue;
+    *(uint32_t*)&ty[r * 20 + 4 * k] = *(const uint32_t*)(sd.cur_y + (long)(y0 - 4 + r) * fp.stride_y + x0 - 4 + 4 * k);
+  }
+  for (int w = lane; w < 72; w += 32) {  // 2 planes x 12 rows x 3 words
+    int p = w / 36, rem = w % 36, r = rem / 3, k = rem % 3;
+    if ((r < 4 && !hast) || (k == 0 && !hasl)) continue;
+    const uint8_t* P = p ? sd.cur_v : sd.cur_u;
+    *(uint32_t*)&tc[p][r * 12 + 4 * k] = *(const uint32_t*)(P + (long)(cy0 - 4 + r) * fp.stride_c + cx0 - 4 + 4 * k);
+  }
+  __syncwarp();
+  bool intra = q.flags & kFlagIntra;
+  bool internal = intra || q.cbp_luma != 0;
+  bool skip_odd = q.flags & kFlagT8;
+  int qpq = q.qp, qpcq = chroma_qp(qpq);
+  for (int dir = 0; dir < 2; dir++) {
+    for (int e = 0; e < 4; e++) {
+      const MbInfo* pm;
+      if (e == 0) {
+        if (dir == 0 ? !hasl : !hast) continue;
+        pm = dir == 0 ? &lf : &tp;
+      } else {
+        if (!internal || ((e & 1) && skip_odd)) continue;
+        pm = nullptr;
+      }
+      int bs[4];
+      if (!edge_bs(q, pm ? pm : &q, dir, e, bs)) continue;
+      int qpl, qpc;
+      if (!pm) { qpl = qpq; qpc = qpcq; }
+      else { qpl = (qpq + pm->qp + 1) >> 1; qpc = (qpcq + chroma_qp(pm->qp) + 1) >> 1; }
+      EdgeParams el = edge_params(qpl, bs);
+      if (lane < 16 && el.on) {
+        if (dir == 0) luma_line(&ty[(4 + lane) * 20 + 4 + e * 4], 1, el, el.tc0[lane >> 2]);
+        else luma_line(&ty[(4 + e * 4) * 20 + 4 + lane], 20, el, el.tc0[lane >> 2]);
+      }
+      if (!(e & 1) && lane >= 16) {
+        EdgeParams ec = edge_params(qpc, bs);
+        if (ec.on) {
+          int j = lane - 16, p = j >> 3, k = j & 7;
+          if (dir == 0) chroma_line(&tc[p][(4 + k) * 12 + 4 + e * 2], 1, ec, ec.tc0[k >> 1]);
+          else chroma_line(&tc[p][(4 + e * 2) * 12 + 4 + k], 12, ec, ec.tc0[k >> 1]);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // write back the samples this macroblock filters (rows 0..15 x cols -4..15, rows -4..-1 x cols 0..15)
+  for (int w = lane; w < 100; w += 32) {
+    int r = w / 5, k = w % 5;
+    if (r < 4 && k == 0) continue;
+    if ((r < 4 && !hast) || (k == 0 && !hasl)) continue;
+    *(uint32_t*)(sd.cur_y + (long)(y0 - 4 + r) * fp.stride_y + x0 - 4 + 4 * k) = *(const uint32_t*)&ty[r * 20 + 4 * k];
+  }
+  for (int w = lane; w < 72; w += 32) {
+    int p = w / 36, rem = w % 36, r = rem / 3, k = rem % 3;
+    if (r < 4 && k == 0) continue;
+    if ((r < 4 && !hast) || (k == 0 && !hasl)) continue;
+    uint8_t* P = p ? sd.cur_v : sd.cur_u;
+    *(uint32_t*)(P + (long)(cy0 - 4 + r) * fp.stride_c + cx0 - 4 + 4 * k) = *(const uint32_t*)&tc[p][r * 12 + 4 * k];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int diag_first(const FrameParams& fp, int d) {
+  int a = d - fp.mb_w + 1;
+  return a > 0 ? (a + 1) >> 1 : 0;
+}
+__device__ __forceinline__ int diag_len(const FrameParams& fp, int d) {
+  if (d < 0) return 0;
+  int lo = diag_first(fp, d), hi = min(fp.mb_h - 1, d >> 1);
+  return hi >= lo ? hi - lo + 1 : 0;
+}
+
+__global__ void __launch_bounds__(32) wavefront_step_kernel(FrameParams fp, const StreamDev* __restrict__ streams, int step) {
+  __shared__ Smem sm;
+  const StreamDev& sd = streams[blockIdx.y];
+  int na = diag_len(fp, step);
+  int nd = fp.deblock ? diag_len(fp, step - 3) : 0;
+  int k = blockIdx.x;
+  if (k < na) {
+    int mby = diag_first(fp, step) + k, mbx = step - 2 * mby;
+    Ctx c{&fp, &sd, mbx, mby, mby * fp.mb_w + mbx};
+    if (sd.kind == RG_FRAME_IDR) {
+      load_source(c, sm);
+      analyse_intra_mb(c, sm);
+    } else {
+      analyse_p_mb(c, sm);
+    }
+  } else if (k - na < nd) {
+    int d = step - 3;
+    int mby = diag_first(fp, d) + (k - na), mbx = d - 2 * mby;
+    deblock_mb(fp, sd, mbx, mby, sm);
+  }
+}
+
+// Border extension (enc.rs:165 extend_borders): every padding sample takes the value of the
+// nearest picture sample. One thread per 16-byte chunk of a padded row.
+__global__ void extend_borders_kernel(FrameParams fp, const StreamDev* __restrict__ streams) {
+  const StreamDev& sd = streams[blockIdx.z / 3];
+  int plane = blockIdx.z % 3;
+  int w = plane ? fp.mb_w * 8 : fp.mb_w * 16, h = plane ? fp.mb_h * 8 : fp.mb_h * 16;
+  int pad = plane ? kPadC : kPadY, stride = plane ? fp.stride_c : fp.stride_y;
+  uint8_t* P = plane == 0 ? sd.cur_y : (plane == 1 ? sd.cur_u : sd.cur_v);
+  int chunks = stride / 16;
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int rows = h + 2 * pad;
+  if (idx >= rows * chunks) return;
+  int ry = idx / chunks, cx = (idx % chunks) * 16;  // padded coordinates
+  int y = ry - pad;
+  int xs = cx - pad;
+  bool row_inside = y >= 0 && y < h;
+  if (row_inside && xs >= 0 && xs + 16 <= w) return;  // all interior
+  int sy = min(max(y, 0), h - 1);
+  const uint8_t* srow = P + (long)sy * stride;
+  uint8_t* drow = P + (long)y * stride;
+  for (int k = 0; k < 16; k++) {
+    int x = xs + k;
+    if (row_inside && x >= 0 && x < w) continue;
+    drow[x] = srow[min(max(x, 0), w - 1)];
+  }
+}
+
+}  // namespace
+
+void upload_tables() {
+  using namespace tables;
+  cudaMemcpyToSymbol(c_lambda, kLambda, sizeof(kLambda));
+  cudaMemcpyToSymbol(c_dec4, kDecimate4, sizeof(kDecimate4));
+  uint8_t d8[64] = {0};
+  for (int i = 0; i < 24; i++) d8[i] = kDecimate8[i];
+  cudaMemcpyToSymbol(c_dec8, d8, sizeof(d8));
+  cudaMemcpyToSymbol(c_scan4, kScan4, sizeof(kScan4));
+  cudaMemcpyToSymbol(c_scan8, kScan8, sizeof(kScan8));
+  cudaMemcpyToSymbol(c_mf4, kMf4, sizeof(kMf4));
+  cudaMemcpyToSymbol(c_dq4, kDq4, sizeof(kDq4));
+  cudaMemcpyToSymbol(c_mf8, kMf8, sizeof(kMf8));
+  cudaMemcpyToSymbol(c_dq8, kDq8, sizeof(kDq8));
+  cudaMemcpyToSymbol(c_cqp, kChromaQp, sizeof(kChromaQp));
+  cudaMemcpyToSymbol(c_alpha, kAlpha, sizeof(kAlpha));
+  cudaMemcpyToSymbol(c_beta, kBeta, sizeof(kBeta));
+  cudaMemcpyToSymbol(c_tc0, kTc0, sizeof(kTc0));
+}
+
+int wavefront_steps(const FrameParams& fp) {
+  int diags = (fp.mb_w - 1) + 2 * (fp.mb_h - 1) + 1;
+  return diags + (fp.deblock ? 3 : 0);
+}
+
+static int max_diag_len(const FrameParams& fp) {
+  int best = 0;
+  int diags = (fp.mb_w - 1) + 2 * (fp.mb_h - 1) + 1;
+  for (int d = 0; d < diags; d++) {
+    int a = d - fp.mb_w + 1;
+    int lo = a > 0 ? (a + 1) >> 1 : 0, hi = fp.mb_h - 1 < (d >> 1) ? fp.mb_h - 1 : (d >> 1);
+    if (hi - lo + 1 > best) best = hi - lo + 1;
+  }
+  return best;
+}
+
+void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st) {
+  dim3 grid(2 * max_diag_len(fp), fp.n_streams);
+  wavefront_step_kernel<<<grid, 32, 0, st>>>(fp, d_streams, step);
+}
+
+void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st) {
+  int rows = fp.mb_h * 16 + 2 * kPadY;
+  int chunks = fp.stride_y / 16;
+  int threads = 256;
+  dim3 grid((rows * chunks + threads - 1) / threads, 1, 3 * fp.n_streams);
+  extend_borders_kernel<<<grid, threads, 0, st>>>(fp, d_streams);
+}
+
+}  // namespace rg

@@ -1,0 +1,611 @@
+// C ABI of the engine (include/ragdoll_cuda.h): contexts, batched wavefront launches, host <->
+// device copies, reconstruction and quality read-back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "h264_consts.h"
+#include "ssim_kernels.h"
+
+using namespace rg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(expr)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess) return fail(RG_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+
+struct Quant4Host {
+  uint32_t mf[16], bias, shift;
+};
+int pos4h(int i) {
+  int r = i >> 2, c = i & 3;
+  if (((r | c) & 1) == 0) return 0;
+  return ((r & c) & 1) ? 1 : 2;
+}
+Quant4Host quant4h(int qp, bool intra) {
+  Quant4Host q;
+  q.shift = 15 + qp / 6;
+  for (int i = 0; i < 16; i++) q.mf[i] = tables::kMf4[qp % 6][pos4h(i)];
+  q.bias = (1u << q.shift) / (intra ? 3u : 6u);
+  return q;
+}
+
+// SkipBounds::new (enc.rs:2135) for the inter quantiser at qp / qpc.
+void skip_bounds(int qp, int qpc, FrameParams& fp) {
+  Quant4Host q = quant4h(qp, false), qc = quant4h(qpc, false);
+  auto zsad = [](const Quant4Host& qq) {
+    static const uint32_t W[4] = {1, 2, 1, 2};
+    uint32_t room = (1u << qq.shift) - qq.bias - 1, mn = 0xffffffffu;
+    for (int i = 0; i < 16; i++) mn = std::min(mn, room / (qq.mf[i] * W[i >> 2] * W[i & 3]));
+    return mn;
+  };
+  auto zssd = [](const Quant4Host& qq) {
+    static const uint32_t N[4] = {4, 10, 4, 10};
+    uint32_t room = (1u << qq.shift) - qq.bias - 1, mn = 0xffffffffu;
+    for (int i = 0; i < 16; i++) {
+      uint32_t lim = room / qq.mf[i];
+      mn = std::min(mn, lim * lim / (N[i >> 2] * N[i & 3]));
+    }
+    return mn;
+  };
+  uint32_t dsh = 16 + qpc / 6;
+  uint32_t droom = (1u << dsh) - (1u << dsh) / 3 - 1;
+  uint32_t dc = droom / tables::kMf4[qpc % 6][0];
+  fp.sb_luma = zsad(q);
+  fp.sb_luma_ssd = zssd(q);
+  fp.sb_chroma = std::min(zsad(qc), dc);
+  fp.sb_chroma_ssd = std::min(zssd(qc), dc * dc / 64);
+  fp.sb_probe = 16 * (((1u << q.shift) - q.bias) / q.mf[0] + 1);
+}
+
+}  // namespace
+
+struct rg_ctx {
+  rg_config cfg{};
+  FrameParams fp{};
+  int S = 0, n_mb = 0;
+  int rows_y = 0, rows_c = 0;      // padded rows
+  size_t pic_y = 0, pic_c = 0;     // bytes of one padded plane
+  cudaStream_t stream = nullptr;
+  uint8_t* pics = nullptr;         // [S][2][Y U V]
+  MbInfo* infos = nullptr;         // [S][2][n_mb]
+  rg_mb_out* recs = nullptr;       // [S][n_mb]
+  uint8_t* srcs = nullptr;         // [S][Y U V] compact display-size staging
+  uint8_t* unf = nullptr;          // [S][Y U V] coded-size copies before deblocking
+  bool keep_unfiltered = false;
+  StreamDev* d_streams[2] = {nullptr, nullptr};
+  StreamDev* h_streams[2] = {nullptr, nullptr};  // pinned
+  cudaEvent_t slot_done[2] = {nullptr, nullptr};
+  int slot = 0;
+  std::vector<int> frames;         // frames analysed per stream
+  // metrics scratch
+  float* m_rows = nullptr;
+  double* m_out = nullptr;
+  unsigned long long* m_sse = nullptr;
+  uint8_t* m_pyr = nullptr;
+  SsimJob* m_jobs = nullptr;
+  DecimateJob* m_djobs = nullptr;
+  uint8_t* m_src = nullptr;
+
+  uint8_t* pic_plane(int s, int parity, int plane) const {
+    size_t per_pic = pic_y + 2 * pic_c;
+    uint8_t* base = pics + ((size_t)s * 2 + parity) * per_pic;
+    if (plane == 0) return base + (size_t)kPadY * fp.stride_y + kPadY;
+    return base + pic_y + (plane - 1) * pic_c + (size_t)kPadC * fp.stride_c + kPadC;
+  }
+  size_t src_bytes() const {
+    int cw = (cfg.width + 1) / 2, ch = (cfg.height + 1) / 2;
+    return (size_t)cfg.width * cfg.height + 2 * (size_t)cw * ch;
+  }
+  size_t unf_bytes() const { return (size_t)fp.mb_w * fp.mb_h * 384; }
+};
+
+extern "C" {
+
+const char* rg_last_error(void) { return g_last_error.c_str(); }
+
+const char* rg_version(void) { return "ragdoll_b200 0.1 (sm_100a)"; }
+
+rg_ctx* rg_create(const rg_config* cfg) {
+  if (!cfg) { fail(RG_ERR_INVALID, "rg_create: null config"); return nullptr; }
+  if (cfg->width < 1 || cfg->height < 1 || cfg->width > 8192 || cfg->height > 8192) {
+    fail(RG_ERR_INVALID, "rg_create: size %dx%d outside 1..8192", cfg->width, cfg->height);
+    return nullptr;
+  }
+  if (cfg->qp < 1 || cfg->qp > 51) {
+    fail(RG_ERR_UNSUPPORTED, "rg_create: qp %d outside 1..51 (QP 0 codes I_PCM)", cfg->qp);
+    return nullptr;
+  }
+  if (cfg->profile < RG_PROFILE_BASELINE || cfg->profile > RG_PROFILE_HIGH) {
+    fail(RG_ERR_INVALID, "rg_create: profile %d", cfg->profile);
+    return nullptr;
+  }
+  if (cfg->num_streams < 1 || cfg->num_streams > kMaxStreams) {
+    fail(RG_ERR_INVALID, "rg_create: num_streams %d outside 1..%d", cfg->num_streams, kMaxStreams);
+    return nullptr;
+  }
+  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+    fail(RG_ERR_CUDA, "rg_create: cudaSetDevice(%d) failed", cfg->device);
+    return nullptr;
+  }
+  auto* c = new rg_ctx();
+  c->cfg = *cfg;
+  c->S = cfg->num_streams;
+  FrameParams& fp = c->fp;
+  fp.width = cfg->width;
+  fp.height = cfg->height;
+  fp.mb_w = (cfg->width + 15) / 16;
+  fp.mb_h = (cfg->height + 15) / 16;
+  fp.stride_y = ((fp.mb_w * 16 + 2 * kPadY) + 63) & ~63;
+  fp.stride_c = ((fp.mb_w * 8 + 2 * kPadC) + 63) & ~63;
+  fp.src_stride_y = cfg->width;
+  fp.src_stride_uv = (cfg->width + 1) / 2;
+  fp.qp = cfg->qp;
+  fp.qpc = tables::kChromaQp[cfg->qp];
+  fp.t8x8 = cfg->profile == RG_PROFILE_HIGH;
+  fp.deblock = 1;
+  fp.n_streams = c->S;
+  skip_bounds(fp.qp, fp.qpc, fp);
+  c->n_mb = fp.mb_w * fp.mb_h;
+  c->rows_y = fp.mb_h * 16 + 2 * kPadY;
+  c->rows_c = fp.mb_h * 8 + 2 * kPadC;
+  c->pic_y = (size_t)fp.stride_y * c->rows_y;
+  c->pic_c = (size_t)fp.stride_c * c->rows_c;
+  c->frames.assign(c->S, 0);
+  bool ok = true;
+  auto alloc = [&](void** p, size_t n) {
+    if (!ok) return;
+    if (cudaMalloc(p, n) != cudaSuccess) { ok = false; return; }
+    cudaMemset(*p, 0, n);
+  };
+  alloc((void**)&c->pics, (c->pic_y + 2 * c->pic_c) * 2 * c->S);
+  alloc((void**)&c->infos, sizeof(MbInfo) * c->n_mb * 2 * c->S);
+  alloc((void**)&c->recs, sizeof(rg_mb_out) * c->n_mb * c->S);
+  alloc((void**)&c->srcs, c->src_bytes() * c->S);
+  alloc((void**)&c->d_streams[0], sizeof(StreamDev) * c->S);
+  alloc((void**)&c->d_streams[1], sizeof(StreamDev) * c->S);
+  if (!ok) {
+    fail(RG_ERR_OOM, "rg_create: device allocation failed");
+    rg_destroy(c);
+    return nullptr;
+  }
+  if (cudaMallocHost((void**)&c->h_streams[0], sizeof(StreamDev) * c->S) != cudaSuccess ||
+      cudaMallocHost((void**)&c->h_streams[1], sizeof(StreamDev) * c->S) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->slot_done[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->slot_done[1], cudaEventDisableTiming) != cudaSuccess) {
+    fail(RG_ERR_CUDA, "rg_create: stream / pinned buffer setup failed");
+    rg_destroy(c);
+    return nullptr;
+  }
+  upload_tables();
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    fail(RG_ERR_CUDA, "rg_create: %s", cudaGetErrorString(cudaGetLastError()));
+    rg_destroy(c);
+    return nullptr;
+  }
+  return c;
+}
+
+void rg_destroy(rg_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->pics);
+  cudaFree(c->infos);
+  cudaFree(c->recs);
+  cudaFree(c->srcs);
+  cudaFree(c->unf);
+  cudaFree(c->d_streams[0]);
+  cudaFree(c->d_streams[1]);
+  cudaFree(c->m_rows);
+  cudaFree(c->m_out);
+  cudaFree(c->m_sse);
+  cudaFree(c->m_pyr);
+  cudaFree(c->m_jobs);
+  cudaFree(c->m_djobs);
+  cudaFree(c->m_src);
+  if (c->h_streams[0]) cudaFreeHost(c->h_streams[0]);
+  if (c->h_streams[1]) cudaFreeHost(c->h_streams[1]);
+  for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int rg_mb_dims(const rg_ctx* c, int32_t* mb_w, int32_t* mb_h) {
+  if (!c || !mb_w || !mb_h) return fail(RG_ERR_INVALID, "rg_mb_dims: null argument");
+  *mb_w = c->fp.mb_w;
+  *mb_h = c->fp.mb_h;
+  return RG_OK;
+}
+
+// Test hook: keep a copy of every reconstruction before deblocking (rg_get_recon_unfiltered).
+int rg_keep_unfiltered(rg_ctx* c, int32_t enable) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_keep_unfiltered: null context");
+  if (enable && !c->unf) {
+    if (cudaMalloc((void**)&c->unf, c->unf_bytes() * c->S) != cudaSuccess)
+      return fail(RG_ERR_OOM, "rg_keep_unfiltered: allocation failed");
+  }
+  c->keep_unfiltered = enable != 0;
+  return RG_OK;
+}
+
+void* rg_cuda_stream(rg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
+                            const int32_t* kinds) {
+  if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_batch_device: null argument");
+  if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
+    return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stride too small");
+  for (int s = 0; s < c->S; s++) {
+    if (kinds[s] != RG_FRAME_IDR && kinds[s] != RG_FRAME_P)
+      return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stream %d kind %d", s, kinds[s]);
+    if (kinds[s] == RG_FRAME_P && c->frames[s] == 0)
+      return fail(RG_ERR_STATE, "rg_analyse_batch_device: stream %d P frame without a reference", s);
+    if (!dev_planes[3 * s] || !dev_planes[3 * s + 1] || !dev_planes[3 * s + 2])
+      return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stream %d null plane", s);
+  }
+  int slot = c->slot;
+  c->slot ^= 1;
+  CK(cudaEventSynchronize(c->slot_done[slot]));  // the pinned descriptor slot is free again
+  StreamDev* h = c->h_streams[slot];
+  size_t unf = c->unf_bytes();
+  for (int s = 0; s < c->S; s++) {
+    int par = c->frames[s] & 1;
+    StreamDev& d = h[s];
+    d.src_y = dev_planes[3 * s];
+    d.src_u = dev_planes[3 * s + 1];
+    d.src_v = dev_planes[3 * s + 2];
+    d.cur_y = c->pic_plane(s, par, 0);
+    d.cur_u = c->pic_plane(s, par, 1);
+    d.cur_v = c->pic_plane(s, par, 2);
+    d.ref_y = c->pic_plane(s, par ^ 1, 0);
+    d.ref_u = c->pic_plane(s, par ^ 1, 1);
+    d.ref_v = c->pic_plane(s, par ^ 1, 2);
+    d.info = c->infos + ((size_t)s * 2 + par) * c->n_mb;
+    d.prev_info = c->infos + ((size_t)s * 2 + (par ^ 1)) * c->n_mb;
+    d.rec = c->recs + (size_t)s * c->n_mb;
+    if (c->keep_unfiltered) {
+      uint8_t* u = c->unf + unf * s;
+      d.unf_y = u;
+      d.unf_u = u + (size_t)c->fp.mb_w * c->fp.mb_h * 256;
+      d.unf_v = d.unf_u + (size_t)c->fp.mb_w * c->fp.mb_h * 64;
+    } else {
+      d.unf_y = d.unf_u = d.unf_v = nullptr;
+    }
+    d.kind = kinds[s];
+    d.pad_ = 0;
+  }
+  FrameParams fp = c->fp;
+  fp.src_stride_y = (int)stride_y;
+  fp.src_stride_uv = (int)stride_uv;
+  CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * c->S, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(c->slot_done[slot], c->stream));
+  int steps = wavefront_steps(fp);
+  for (int t = 0; t < steps; t++) launch_wavefront_step(fp, c->d_streams[slot], t, c->stream);
+  launch_extend_borders(fp, c->d_streams[slot], c->stream);
+  CK(cudaGetLastError());
+  for (int s = 0; s < c->S; s++) c->frames[s]++;
+  return RG_OK;
+}
+
+int rg_sync(rg_ctx* c) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_sync: null context");
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
+}
+
+int rg_copy_records(rg_ctx* c, rg_mb_out* out) {
+  if (!c || !out) return fail(RG_ERR_INVALID, "rg_copy_records: null argument");
+  CK(cudaMemcpyAsync(out, c->recs, sizeof(rg_mb_out) * c->n_mb * c->S, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
+}
+
+static int upload_planes(rg_ctx* c, int s, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t sy, size_t suv) {
+  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  uint8_t* d = c->srcs + c->src_bytes() * s;
+  CK(cudaMemcpy2DAsync(d, w, y, sy, w, h, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpy2DAsync(d + (size_t)w * h, cw, u, suv, cw, ch, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpy2DAsync(d + (size_t)w * h + (size_t)cw * ch, cw, v, suv, cw, ch, cudaMemcpyHostToDevice, c->stream));
+  return RG_OK;
+}
+
+int rg_analyse_batch(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
+                     rg_mb_out* out) {
+  if (!c || !planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_batch: null argument");
+  int w = c->cfg.width, cw = (w + 1) / 2;
+  if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "rg_analyse_batch: stride too small");
+  std::vector<const uint8_t*> dev(3 * c->S);
+  for (int s = 0; s < c->S; s++) {
+    if (!planes[3 * s] || !planes[3 * s + 1] || !planes[3 * s + 2])
+      return fail(RG_ERR_INVALID, "rg_analyse_batch: stream %d null plane", s);
+    int r = upload_planes(c, s, planes[3 * s], planes[3 * s + 1], planes[3 * s + 2], stride_y, stride_uv);
+    if (r) return r;
+    uint8_t* d = c->srcs + c->src_bytes() * s;
+    dev[3 * s] = d;
+    dev[3 * s + 1] = d + (size_t)w * c->cfg.height;
+    dev[3 * s + 2] = d + (size_t)w * c->cfg.height + (size_t)cw * ((c->cfg.height + 1) / 2);
+  }
+  int r = rg_analyse_batch_device(c, dev.data(), w, cw, kinds);
+  if (r) return r;
+  if (out) return rg_copy_records(c, out);
+  return rg_sync(c);
+}
+
+int rg_analyse_frame(rg_ctx* c, int32_t stream, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t stride_y,
+                     size_t stride_uv, int32_t kind, rg_mb_out* out) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_analyse_frame: null context");
+  if (c->S != 1) return fail(RG_ERR_INVALID, "rg_analyse_frame: context has %d streams; use rg_analyse_batch", c->S);
+  if (stream != 0) return fail(RG_ERR_INVALID, "rg_analyse_frame: stream %d", stream);
+  const uint8_t* planes[3] = {y, u, v};
+  return rg_analyse_batch(c, planes, stride_y, stride_uv, &kind, out);
+}
+
+int rg_get_recon(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v, size_t sy, size_t suv) {
+  if (!c || !y || !u || !v) return fail(RG_ERR_INVALID, "rg_get_recon: null argument");
+  if (s < 0 || s >= c->S) return fail(RG_ERR_INVALID, "rg_get_recon: stream %d", s);
+  if (c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_get_recon: stream %d has no frame", s);
+  int par = (c->frames[s] - 1) & 1;
+  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  CK(cudaMemcpy2DAsync(y, sy, c->pic_plane(s, par, 0), c->fp.stride_y, w, h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpy2DAsync(u, suv, c->pic_plane(s, par, 1), c->fp.stride_c, cw, ch, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpy2DAsync(v, suv, c->pic_plane(s, par, 2), c->fp.stride_c, cw, ch, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
+}
+
+// Coded-size reconstruction after deblocking (for parity tests against the oracle).
+int rg_get_recon_coded(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v) {
+  if (!c || !y || !u || !v) return fail(RG_ERR_INVALID, "rg_get_recon_coded: null argument");
+  if (s < 0 || s >= c->S || c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_get_recon_coded: stream %d", s);
+  int par = (c->frames[s] - 1) & 1;
+  int w = c->fp.mb_w * 16, h = c->fp.mb_h * 16;
+  CK(cudaMemcpy2DAsync(y, w, c->pic_plane(s, par, 0), c->fp.stride_y, w, h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpy2DAsync(u, w / 2, c->pic_plane(s, par, 1), c->fp.stride_c, w / 2, h / 2, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpy2DAsync(v, w / 2, c->pic_plane(s, par, 2), c->fp.stride_c, w / 2, h / 2, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
+}
+
+int rg_get_recon_unfiltered(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v) {
+  if (!c || !y || !u || !v) return fail(RG_ERR_INVALID, "rg_get_recon_unfiltered: null argument");
+  if (!c->unf || !c->keep_unfiltered) return fail(RG_ERR_STATE, "rg_get_recon_unfiltered: enable rg_keep_unfiltered first");
+  if (s < 0 || s >= c->S || c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_get_recon_unfiltered: stream %d", s);
+  size_t ny = (size_t)c->fp.mb_w * c->fp.mb_h * 256, nc = ny / 4;
+  uint8_t* b = c->unf + c->unf_bytes() * s;
+  CK(cudaMemcpyAsync(y, b, ny, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(u, b + ny, nc, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(v, b + ny + nc, nc, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Metrics: SSIM of Y/U/V, 5-scale MS-SSIM of Y and PSNR (evaluate_frame_quality,
+// crates/ragdoll-pix/src/metrics.rs:328).
+namespace {
+
+const double kMsWeights[5] = {0.0448, 0.2856, 0.3001, 0.2363, 0.1333};
+
+struct PlanePair {
+  const uint8_t* a;
+  long sa;
+  const uint8_t* b;
+  long sb;
+  int w, h;
+};
+
+// Evaluates SSIM of each pair, MS-SSIM of pairs with want_ms, SSE of all, on stream st.
+int device_metrics(const std::vector<PlanePair>& pairs, const std::vector<bool>& want_ms, cudaStream_t st,
+                   std::vector<double>& ssim, std::vector<double>& ms, std::vector<unsigned long long>& sse) {
+  int n = (int)pairs.size();
+  // pyramid levels of the MS-SSIM pairs
+  std::vector<SsimJob> jobs;
+  std::vector<DecimateJob> djobs_per_level[4];
+  std::vector<int> level_count(n, 1);
+  size_t rows_total = 0, pyr_total = 0;
+  for (int i = 0; i < n; i++) {
+    rows_total += pairs[i].h / 4 + 1;
+    if (want_ms[i]) {
+      int w = pairs[i].w, h = pairs[i].h;
+      for (int l = 1; l < 5; l++) {
+        w >>= 1; h >>= 1;
+        if (w < 8 || h < 8) break;
+        pyr_total += 2 * (size_t)w * h;
+        rows_total += h / 4 + 1;
+        level_count[i]++;
+      }
+    }
+  }
+  float* rows = nullptr;
+  double* outs = nullptr;
+  unsigned long long* sses = nullptr;
+  uint8_t* pyr = nullptr;
+  SsimJob* d_jobs = nullptr;
+  DecimateJob* d_djobs = nullptr;
+  int total_jobs = 0;
+  for (int i = 0; i < n; i++) total_jobs += want_ms[i] ? level_count[i] : 1;
+  auto cleanup = [&]() {
+    cudaFree(rows); cudaFree(outs); cudaFree(sses); cudaFree(pyr); cudaFree(d_jobs); cudaFree(d_djobs);
+  };
+  if (cudaMalloc(&rows, rows_total * sizeof(float) + 16) != cudaSuccess ||
+      cudaMalloc(&outs, total_jobs * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&sses, n * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&pyr, pyr_total + 16) != cudaSuccess || cudaMalloc(&d_jobs, total_jobs * sizeof(SsimJob)) != cudaSuccess ||
+      cudaMalloc(&d_djobs, (4 * n + 1) * sizeof(DecimateJob)) != cudaSuccess) {
+    cleanup();
+    return fail(RG_ERR_OOM, "metrics: device allocation failed");
+  }
+  cudaMemsetAsync(sses, 0, n * sizeof(unsigned long long), st);
+  size_t rofs = 0, pofs = 0;
+  int maxw = 0, maxh = 0;
+  std::vector<int> job_of(n * 5, -1);
+  for (int i = 0; i < n; i++) {
+    const PlanePair& p = pairs[i];
+    SsimJob j{p.a, p.b, p.sa, p.sb, p.w, p.h, rows + rofs, outs + jobs.size(), sses + i};
+    rofs += p.h / 4 + 1;
+    job_of[i * 5] = (int)jobs.size();
+    jobs.push_back(j);
+    maxw = std::max(maxw, p.w);
+    maxh = std::max(maxh, p.h);
+    if (want_ms[i]) {
+      const uint8_t* sa = p.a;
+      const uint8_t* sb = p.b;
+      long ssa = p.sa, ssb = p.sb;
+      int w = p.w, h = p.h;
+      for (int l = 1; l < level_count[i]; l++) {
+        int nw = w >> 1, nh = h >> 1;
+        uint8_t* da = pyr + pofs;
+        uint8_t* db = da + (size_t)nw * nh;
+        pofs += 2 * (size_t)nw * nh;
+        djobs_per_level[l - 1].push_back(DecimateJob{sa, sb, ssa, ssb, w, h, da, db});
+        SsimJob jl{da, db, nw, nw, nw, nh, rows + rofs, outs + jobs.size(), nullptr};
+        rofs += nh / 4 + 1;
+        job_of[i * 5 + l] = (int)jobs.size();
+        jobs.push_back(jl);
+        sa = da; sb = db; ssa = nw; ssb = nw; w = nw; h = nh;
+      }
+    }
+  }
+  // decimation levels in order, then every SSIM job in one launch
+  std::vector<DecimateJob> all_d;
+  std::vector<int> dofs;
+  for (int l = 0; l < 4; l++) {
+    dofs.push_back((int)all_d.size());
+    all_d.insert(all_d.end(), djobs_per_level[l].begin(), djobs_per_level[l].end());
+  }
+  if (!all_d.empty()) CK(cudaMemcpyAsync(d_djobs, all_d.data(), all_d.size() * sizeof(DecimateJob), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(SsimJob), cudaMemcpyHostToDevice, st));
+  for (int l = 0; l < 4; l++) {
+    int cnt = (int)djobs_per_level[l].size();
+    if (!cnt) continue;
+    int maxpix = 0;
+    for (auto& d : djobs_per_level[l]) maxpix = std::max(maxpix, (d.src_w >> 1) * (d.src_h >> 1));
+    launch_decimate(d_djobs + dofs[l], cnt, maxpix, st);
+  }
+  launch_ssim(d_jobs, (int)jobs.size(), maxw, maxh, st);
+  launch_sse(d_jobs, n, st);
+  std::vector<double> res(jobs.size());
+  sse.assign(n, 0);
+  CK(cudaMemcpyAsync(res.data(), outs, jobs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(sse.data(), sses, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  cudaError_t e = cudaStreamSynchronize(st);
+  cleanup();
+  if (e != cudaSuccess) return fail(RG_ERR_CUDA, "metrics: %s", cudaGetErrorString(e));
+  ssim.assign(n, 0.0);
+  ms.assign(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    ssim[i] = res[job_of[i * 5]];
+    if (!want_ms[i]) continue;
+    // ms_ssim_plane_u8 (crates/ragdoll-pix/src/metrics.rs:154)
+    double s0 = std::min(1.0, std::max(0.0, ssim[i]));
+    if (std::fabs(1.0 - s0) < 1e-12 || (pairs[i].w >> 1) < 8 || (pairs[i].h >> 1) < 8) { ms[i] = s0; continue; }
+    double scores[5] = {s0, s0, s0, s0, s0};
+    int active = level_count[i];
+    for (int l = 1; l < active; l++) scores[l] = std::min(1.0, std::max(0.0, res[job_of[i * 5 + l]]));
+    double wsum = 0.0;
+    for (int l = 0; l < active; l++) wsum += kMsWeights[l];
+    double prod = 1.0;
+    for (int l = 0; l < active; l++) prod *= std::pow(std::max(scores[l], 1e-9), kMsWeights[l] / wsum);
+    ms[i] = std::min(1.0, std::max(0.0, prod));
+  }
+  return RG_OK;
+}
+
+double psnr_of(unsigned long long sse, long n) {
+  if (sse == 0) return INFINITY;
+  double mse = (double)sse / (double)n;
+  return 10.0 * std::log10((255.0 * 255.0) / mse);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rg_quality_frame(rg_ctx* c, int32_t s, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t sy, size_t suv,
+                     rg_quality* q) {
+  if (!c || !y || !u || !v || !q) return fail(RG_ERR_INVALID, "rg_quality_frame: null argument");
+  if (s < 0 || s >= c->S || c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_quality_frame: stream %d", s);
+  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  if (!c->m_src && cudaMalloc((void**)&c->m_src, c->src_bytes()) != cudaSuccess)
+    return fail(RG_ERR_OOM, "rg_quality_frame: allocation failed");
+  CK(cudaMemcpy2DAsync(c->m_src, w, y, sy, w, h, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpy2DAsync(c->m_src + (size_t)w * h, cw, u, suv, cw, ch, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpy2DAsync(c->m_src + (size_t)w * h + (size_t)cw * ch, cw, v, suv, cw, ch, cudaMemcpyHostToDevice, c->stream));
+  int par = (c->frames[s] - 1) & 1;
+  std::vector<PlanePair> pairs = {
+      {c->m_src, w, c->pic_plane(s, par, 0), c->fp.stride_y, w, h},
+      {c->m_src + (size_t)w * h, cw, c->pic_plane(s, par, 1), c->fp.stride_c, cw, ch},
+      {c->m_src + (size_t)w * h + (size_t)cw * ch, cw, c->pic_plane(s, par, 2), c->fp.stride_c, cw, ch}};
+  std::vector<double> ss, ms;
+  std::vector<unsigned long long> sse;
+  int r = device_metrics(pairs, {true, false, false}, c->stream, ss, ms, sse);
+  if (r) return r;
+  q->ssim_y = ss[0];
+  q->ssim_u = ss[1];
+  q->ssim_v = ss[2];
+  q->ssim_avg = (4.0 * ss[0] + ss[1] + ss[2]) / 6.0;
+  q->ms_ssim = ms[0];
+  q->psnr_y = psnr_of(sse[0], (long)w * h);
+  q->psnr_u = psnr_of(sse[1], (long)cw * ch);
+  q->psnr_v = psnr_of(sse[2], (long)cw * ch);
+  return RG_OK;
+}
+
+int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8_t* b, size_t stride_b, int32_t width,
+                  int32_t height, double* ssim, double* ms_ssim) {
+  if (!a || !b || width < 1 || height < 1) return fail(RG_ERR_INVALID, "rg_ssim_plane: bad argument");
+  if (width < 8 || height < 8) return fail(RG_ERR_INVALID, "rg_ssim_plane: plane smaller than one 8x8 window");
+  CK(cudaSetDevice(device));
+  size_t n = (size_t)width * height;
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, 2 * n) != cudaSuccess) return fail(RG_ERR_OOM, "rg_ssim_plane: allocation failed");
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(d);
+    return fail(RG_ERR_CUDA, "rg_ssim_plane: stream creation failed");
+  }
+  int r = RG_OK;
+  if (cudaMemcpy2DAsync(d, width, a, stride_a, width, height, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpy2DAsync(d + n, width, b, stride_b, width, height, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    r = fail(RG_ERR_CUDA, "rg_ssim_plane: copy failed");
+  } else {
+    std::vector<double> ss, ms;
+    std::vector<unsigned long long> sse;
+    r = device_metrics({{d, width, d + n, width, width, height}}, {ms_ssim != nullptr}, st, ss, ms, sse);
+    if (!r) {
+      if (ssim) *ssim = ss[0];
+      if (ms_ssim) *ms_ssim = ms[0];
+    }
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaFree(d);
+  return r;
+}
+
+}  // extern "C"

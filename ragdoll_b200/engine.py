@@ -1,0 +1,217 @@
+"""ctypes binding of the sm_100a engine library (include/ragdoll_cuda.h).
+
+:class:`Engine` wraps one ``rg_ctx``: a fixed picture size, profile and QP, and ``num_streams``
+independent streams (GOPs) analysed side by side in one macroblock wavefront. Every call goes
+through the C ABI; there is no CPU fallback -- loading fails loudly when the library or a CUDA
+device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libragdoll_cuda.so"
+
+RG_PROFILE_BASELINE, RG_PROFILE_MAIN, RG_PROFILE_HIGH = 0, 1, 2
+RG_FRAME_IDR, RG_FRAME_P = 0, 1
+PROFILES = {"baseline": RG_PROFILE_BASELINE, "main": RG_PROFILE_MAIN, "high": RG_PROFILE_HIGH}
+
+ERRORS = {-1: "RG_ERR_INVALID", -2: "RG_ERR_OOM", -3: "RG_ERR_CUDA", -4: "RG_ERR_TIMEOUT",
+          -5: "RG_ERR_UNSUPPORTED", -6: "RG_ERR_STATE"}
+
+# rg_mb_out (include/ragdoll_cuda.h)
+RECORD_DTYPE = np.dtype([
+    ("mb_type", "u1"), ("i16_mode", "u1"), ("chroma_mode", "u1"), ("cbp", "u1"),
+    ("transform_8x8", "u1"), ("qp", "u1"), ("qp_delta", "i1"), ("reserved0", "u1"),
+    ("mv", "<i2", (2,)), ("mvd", "<i2", (2,)), ("i4_modes", "u1", (16,)),
+    ("nz_mask", "<u2"), ("reserved1", "<u2"), ("luma", "<i2", (256,)), ("luma_dc", "<i2", (16,)),
+    ("chroma_dc", "<i2", (2, 4)), ("chroma_ac", "<i2", (2, 4, 16)),
+])
+assert RECORD_DTYPE.itemsize == 852
+
+# Every symbol include/ragdoll_cuda.h declares.
+EXPORTS = [
+    "rg_last_error", "rg_version", "rg_create", "rg_destroy", "rg_mb_dims", "rg_analyse_frame",
+    "rg_analyse_batch", "rg_analyse_batch_device", "rg_sync", "rg_copy_records", "rg_get_recon",
+    "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
+    "rg_quality_frame", "rg_ssim_plane",
+]
+
+
+class RgError(RuntimeError):
+    """A negative RG_ERR_* return (RagdollError on the reference side)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class RgConfig(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("profile", ctypes.c_int32),
+                ("qp", ctypes.c_int32), ("num_streams", ctypes.c_int32), ("device", ctypes.c_int32)]
+
+
+class RgQuality(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("ssim_y", "ssim_u", "ssim_v", "ssim_avg", "ms_ssim", "psnr_y", "psnr_u", "psnr_v")]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libragdoll_cuda.so (built in-tree by ragdoll_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        from . import build as _b
+        _b.build()
+    L = ctypes.CDLL(str(LIB_PATH))
+    P = ctypes.c_void_p
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    L.rg_last_error.restype = ctypes.c_char_p
+    L.rg_version.restype = ctypes.c_char_p
+    L.rg_create.restype = P
+    L.rg_create.argtypes = [ctypes.POINTER(RgConfig)]
+    L.rg_destroy.argtypes = [P]
+    L.rg_mb_dims.argtypes = [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.rg_analyse_frame.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t,
+                                   ctypes.c_int32, P]
+    L.rg_analyse_batch.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, P]
+    L.rg_analyse_batch_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P]
+    L.rg_sync.argtypes = [P]
+    L.rg_copy_records.argtypes = [P, P]
+    L.rg_get_recon.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t]
+    L.rg_get_recon_coded.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p]
+    L.rg_get_recon_unfiltered.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p]
+    L.rg_keep_unfiltered.argtypes = [P, ctypes.c_int32]
+    L.rg_cuda_stream.restype = P
+    L.rg_cuda_stream.argtypes = [P]
+    L.rg_quality_frame.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t,
+                                   ctypes.POINTER(RgQuality)]
+    L.rg_ssim_plane.argtypes = [ctypes.c_int32, u8p, ctypes.c_size_t, u8p, ctypes.c_size_t,
+                                ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(ctypes.c_double)]
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RgError(rc, lib().rg_last_error().decode())
+
+
+def _u8(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+
+
+class Engine:
+    """One ``rg_ctx``: ``num_streams`` streams of one size, profile and fixed QP."""
+
+    def __init__(self, width: int, height: int, qp: int, profile: int = RG_PROFILE_BASELINE,
+                 num_streams: int = 1, device: int = 0):
+        self.width, self.height, self.qp, self.profile = width, height, qp, profile
+        self.num_streams = num_streams
+        cfg = RgConfig(width, height, profile, qp, num_streams, device)
+        h = lib().rg_create(ctypes.byref(cfg))
+        if not h:
+            raise RgError(-1, lib().rg_last_error().decode())
+        self.h = h
+        mw, mh = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().rg_mb_dims(h, ctypes.byref(mw), ctypes.byref(mh)))
+        self.mb_w, self.mb_h = mw.value, mh.value
+        self.n_mb = self.mb_w * self.mb_h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().rg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def keep_unfiltered(self, enable: bool = True) -> None:
+        _check(lib().rg_keep_unfiltered(self.h, 1 if enable else 0))
+
+    @property
+    def cuda_stream(self) -> int:
+        return lib().rg_cuda_stream(self.h) or 0
+
+    def analyse(self, frames, kinds) -> np.ndarray:
+        """Analyses the next frame of every stream from host planes; returns the records
+        ``[num_streams, mb_h * mb_w]``."""
+        assert len(frames) == self.num_streams and len(kinds) == self.num_streams
+        planes = (ctypes.c_void_p * (3 * self.num_streams))()
+        keep = []
+        sy = suv = None
+        for s, (y, u, v) in enumerate(frames):
+            y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (y, u, v))
+            keep += [y, u, v]
+            if sy is None:
+                sy, suv = y.strides[0], u.strides[0]
+            assert y.strides[0] == sy and u.strides[0] == suv == v.strides[0]
+            planes[3 * s], planes[3 * s + 1], planes[3 * s + 2] = y.ctypes.data, u.ctypes.data, v.ctypes.data
+        k = (ctypes.c_int32 * self.num_streams)(*kinds)
+        out = np.zeros((self.num_streams, self.n_mb), RECORD_DTYPE)
+        _check(lib().rg_analyse_batch(self.h, planes, sy, suv, k, out.ctypes.data))
+        return out
+
+    def analyse_device(self, dev_planes, stride_y: int, stride_uv: int, kinds) -> None:
+        """Queues the next frame of every stream from device planes (3 pointers per stream)."""
+        planes = (ctypes.c_void_p * (3 * self.num_streams))(*dev_planes)
+        k = (ctypes.c_int32 * self.num_streams)(*kinds)
+        _check(lib().rg_analyse_batch_device(self.h, planes, stride_y, stride_uv, k))
+
+    def sync(self) -> None:
+        _check(lib().rg_sync(self.h))
+
+    def records(self) -> np.ndarray:
+        out = np.zeros((self.num_streams, self.n_mb), RECORD_DTYPE)
+        _check(lib().rg_copy_records(self.h, out.ctypes.data))
+        return out
+
+    def recon(self, stream: int = 0):
+        w, h = self.width, self.height
+        cw, ch = (w + 1) // 2, (h + 1) // 2
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((ch, cw), np.uint8)
+        v = np.zeros((ch, cw), np.uint8)
+        _check(lib().rg_get_recon(self.h, stream, _u8(y), _u8(u), _u8(v), w, cw))
+        return y, u, v
+
+    def recon_coded(self, stream: int = 0):
+        cw, ch = self.mb_w * 16, self.mb_h * 16
+        y = np.zeros((ch, cw), np.uint8)
+        u = np.zeros((ch // 2, cw // 2), np.uint8)
+        v = np.zeros((ch // 2, cw // 2), np.uint8)
+        _check(lib().rg_get_recon_coded(self.h, stream, _u8(y), _u8(u), _u8(v)))
+        return y, u, v
+
+    def recon_unfiltered(self, stream: int = 0):
+        cw, ch = self.mb_w * 16, self.mb_h * 16
+        y = np.zeros((ch, cw), np.uint8)
+        u = np.zeros((ch // 2, cw // 2), np.uint8)
+        v = np.zeros((ch // 2, cw // 2), np.uint8)
+        _check(lib().rg_get_recon_unfiltered(self.h, stream, _u8(y), _u8(u), _u8(v)))
+        return y, u, v
+
+    def quality(self, frame, stream: int = 0) -> dict:
+        y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in frame)
+        q = RgQuality()
+        _check(lib().rg_quality_frame(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],
+                                      ctypes.byref(q)))
+        return {n: getattr(q, n) for n, _ in RgQuality._fields_}
+
+
+def ssim_plane(a: np.ndarray, b: np.ndarray, device: int = 0):
+    """(SSIM, MS-SSIM) of two 8-bit planes on the GPU (ssim_plane_u8 / ms_ssim_plane_u8)."""
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.uint8)
+    s, m = ctypes.c_double(), ctypes.c_double()
+    _check(lib().rg_ssim_plane(device, _u8(a), a.strides[0], _u8(b), b.strides[0], a.shape[1], a.shape[0],
+                               ctypes.byref(s), ctypes.byref(m)))
+    return s.value, m.value
