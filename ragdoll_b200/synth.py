@@ -62,57 +62,59 @@ def grating_clip(width: int, height: int, frames: int, seed: int, motion: float 
     Each frame moves the whole field by a global shift drawn uniformly in +-``motion`` px at
     quarter-sample precision (the gratings are evaluated at the shifted coordinates and the
     noise field is resampled bilinearly), and ``rects`` textured rectangles of 64-256 px move
-    independently. Chroma is the field decimated 2x (2x2 mean) plus an offset of 128.
+    independently. Chroma is the field decimated 2x (2x2 mean) around an offset of 128.
     """
     rng = np.random.default_rng(seed)
     periods = rng.uniform(8, 64, 4)
     angles = rng.uniform(0, np.pi, 4)
     phases = rng.uniform(0, 2 * np.pi, 4)
     amps = rng.uniform(12, 28, 4)
-    pad = int(np.ceil(motion * frames)) + 8
-    nh, nw = height + 2 * pad, width + 2 * pad
+    steps = np.round(rng.uniform(-motion, motion, (frames, 2)) * 4) / 4
+    steps[0] = 0
+    pos = np.cumsum(steps, axis=0)
+    ox = int(np.ceil(max(0.0, -pos[:, 0].min()))) + 2
+    oy = int(np.ceil(max(0.0, -pos[:, 1].min()))) + 2
+    nw = width + ox + int(np.ceil(max(0.0, pos[:, 0].max()))) + 3
+    nh = height + oy + int(np.ceil(max(0.0, pos[:, 1].max()))) + 3
     noise = rng.uniform(-20, 20, (nh, nw)).astype(np.float32)
     noise = _blur_1d(_blur_1d(noise, 1.5, 0), 1.5, 1)
     rect_state = []
     for _ in range(rects):
-        rw, rh = rng.integers(64, 257, 2)
+        rw, rh = (int(v) for v in rng.integers(64, 257, 2))
         rx, ry = rng.uniform(0, max(1, width - rw)), rng.uniform(0, max(1, height - rh))
         vx, vy = rng.uniform(-motion, motion, 2)
-        tex_p = rng.uniform(6, 24)
-        tex_a = rng.uniform(0, np.pi)
-        base = rng.uniform(40, 215)
-        rect_state.append([rw, rh, rx, ry, vx, vy, tex_p, tex_a, base])
+        rect_state.append((rw, rh, rx, ry, vx, vy, rng.uniform(6, 24), rng.uniform(0, np.pi),
+                           rng.uniform(40, 215)))
     ys, xs = np.mgrid[0:height, 0:width].astype(np.float32)
+    base = []
+    for p, a, ph in zip(periods, angles, phases):
+        b = (2 * np.pi * (xs * np.cos(a) + ys * np.sin(a)) / p + ph).astype(np.float32)
+        base.append((np.sin(b), np.cos(b)))
+    cw, ch = (width + 1) // 2, (height + 1) // 2
     out = []
-    gx = gy = 0.0
     for f in range(frames):
-        if f:
-            gx += np.round(rng.uniform(-motion, motion) * 4) / 4
-            gy += np.round(rng.uniform(-motion, motion) * 4) / 4
-        X, Y = xs + gx, ys + gy
+        gx, gy = pos[f]
         field = np.full((height, width), 126.0, np.float32)
-        for p, a, ph, am in zip(periods, angles, phases, amps):
-            field += am * np.sin(2 * np.pi * (X * np.cos(a) + Y * np.sin(a)) / p + ph)
-        # bilinear resample of the static noise field at the shifted grid
-        nx, ny = X + pad, Y + pad
-        x0, y0 = np.floor(nx).astype(np.int64), np.floor(ny).astype(np.int64)
-        fx, fy = nx - x0, ny - y0
-        x0 = np.clip(x0, 0, nw - 2)
-        y0 = np.clip(y0, 0, nh - 2)
-        n = (noise[y0, x0] * (1 - fx) * (1 - fy) + noise[y0, x0 + 1] * fx * (1 - fy)
-             + noise[y0 + 1, x0] * (1 - fx) * fy + noise[y0 + 1, x0 + 1] * fx * fy)
-        field += n
-        for r in rect_state:
-            rw, rh, rx, ry, vx, vy, tp, ta, base = r
+        for (sb, cb), p, a, am in zip(base, periods, angles, amps):
+            s = 2 * np.pi * (gx * np.cos(a) + gy * np.sin(a)) / p
+            field += np.float32(am * np.cos(s)) * sb + np.float32(am * np.sin(s)) * cb
+        # the static noise field sampled at the shifted grid: one global bilinear offset
+        x0, y0 = int(np.floor(gx)) + ox, int(np.floor(gy)) + oy
+        fx, fy = np.float32(gx - np.floor(gx)), np.float32(gy - np.floor(gy))
+        n00 = noise[y0:y0 + height, x0:x0 + width]
+        n01 = noise[y0:y0 + height, x0 + 1:x0 + 1 + width]
+        n10 = noise[y0 + 1:y0 + 1 + height, x0:x0 + width]
+        n11 = noise[y0 + 1:y0 + 1 + height, x0 + 1:x0 + 1 + width]
+        field += (1 - fx) * (1 - fy) * n00 + fx * (1 - fy) * n01 + (1 - fx) * fy * n10 + fx * fy * n11
+        for rw, rh, rx, ry, vx, vy, tp, ta, bse in rect_state:
             x0r, y0r = int(round(rx + vx * f)), int(round(ry + vy * f))
-            xa, xb = max(0, x0r), min(width, x0r + int(rw))
-            ya, yb = max(0, y0r), min(height, y0r + int(rh))
+            xa, xb = max(0, x0r), min(width, x0r + rw)
+            ya, yb = max(0, y0r), min(height, y0r + rh)
             if xa < xb and ya < yb:
                 lx, ly = xs[ya:yb, xa:xb] - x0r, ys[ya:yb, xa:xb] - y0r
-                field[ya:yb, xa:xb] = base + 30 * np.sin(
+                field[ya:yb, xa:xb] = bse + 30 * np.sin(
                     2 * np.pi * (lx * np.cos(ta) + ly * np.sin(ta)) / tp)
         y = np.clip(np.rint(field), 16, 235).astype(np.uint8)
-        cw, ch = (width + 1) // 2, (height + 1) // 2
         fp = np.pad(field, ((0, 2 * ch - height), (0, 2 * cw - width)), mode="edge")
         c = fp.reshape(ch, 2, cw, 2).mean(axis=(1, 3)) - 126.0
         u = np.clip(np.rint(c * 0.5 + 128), 16, 240).astype(np.uint8)
