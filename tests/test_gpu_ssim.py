@@ -1,0 +1,51 @@
+"""SSIM / MS-SSIM / PSNR on the GPU against the oracle (GPU tests).
+
+Tolerance: 1e-6 absolute for SSIM and MS-SSIM (the reference's per-row f32 order is reproduced,
+so the plane SSIM agrees to the last bit in practice; MS-SSIM's final pow runs in f64 on the
+host), 1e-9 for PSNR (integer SSE).
+"""
+import numpy as np
+import pytest
+
+import oracle_lib
+from ragdoll_b200.synth import grating_clip, synth_video_frame
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+@pytest.mark.parametrize("w,h", [(1920, 1080), (333, 197), (64, 36), (9, 9), (15, 33)])
+def test_ssim_plane_matches_oracle(w, h):
+    from ragdoll_b200.engine import ssim_plane
+    rng = np.random.default_rng(w * 31 + h)
+    a = rng.integers(0, 256, (h, w), dtype=np.uint8)
+    b = np.clip(a.astype(int) + rng.integers(-12, 13, (h, w)), 0, 255).astype(np.uint8)
+    s, m = ssim_plane(a, b)
+    assert abs(s - oracle_lib.ssim_plane(a, b)) <= TOL
+    assert abs(m - oracle_lib.ms_ssim_plane(a, b)) <= TOL
+
+
+def test_ssim_identical_planes_is_one():
+    from ragdoll_b200.engine import ssim_plane
+    a = synth_video_frame(160, 90, 3)[0]
+    s, m = ssim_plane(a, a)
+    assert s == pytest.approx(1.0, abs=1e-7) and m == pytest.approx(1.0, abs=1e-7)
+
+
+def test_quality_of_reconstruction_matches_oracle():
+    """rg_quality_frame on the engine's reconstruction equals the oracle's metrics of the
+    oracle's (identical) reconstruction: Y/U/V SSIM, the 4:1:1 average, MS-SSIM, PSNR."""
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_HIGH, Engine
+    w, h, qp = 352, 288, 30
+    frames = grating_clip(w, h, 3, seed=5, motion=5.0, rects=2)
+    eng = Engine(w, h, qp, profile=RG_PROFILE_HIGH)
+    for i, fr in enumerate(frames):
+        eng.analyse([fr], [RG_FRAME_IDR if i == 0 else RG_FRAME_P])
+        q = eng.quality(fr)
+        ry, ru, rv = eng.recon()
+        assert abs(q["ssim_y"] - oracle_lib.ssim_plane(fr[0], ry)) <= TOL
+        assert abs(q["ssim_u"] - oracle_lib.ssim_plane(fr[1], ru)) <= TOL
+        assert abs(q["ssim_v"] - oracle_lib.ssim_plane(fr[2], rv)) <= TOL
+        assert abs(q["ms_ssim"] - oracle_lib.ms_ssim_plane(fr[0], ry)) <= TOL
+        assert abs(q["ssim_avg"] - (4 * q["ssim_y"] + q["ssim_u"] + q["ssim_v"]) / 6) <= 1e-12
+        assert q["psnr_y"] == pytest.approx(oracle_lib.psnr_plane(fr[0], ry), abs=1e-9)
