@@ -194,6 +194,29 @@ int rg_quality_frame(rg_ctx* ctx, int32_t stream, const uint8_t* y, const uint8_
 int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8_t* b,
                   size_t stride_b, int32_t width, int32_t height, double* ssim, double* ms_ssim);
 
+/*
+ * Allocation-free SSIM / MS-SSIM of two planes already on the device. No counterpart in the
+ * reference: it exists for callers that may not call cudaMalloc / cudaFree when they measure --
+ * a frame loop whose device memory is all reserved by another allocator (a framework's caching
+ * pool), or a latency-critical loop where an allocation would synchronise the device and stall
+ * its other streams. Results equal rg_ssim_plane's (same arithmetic order).
+ *
+ * dev_a / dev_b: device planes (8-bit, given strides); dev_out: caller-owned device memory for two
+ * doubles, written as {SSIM, MS-SSIM}; cuda_stream: the cudaStream_t to run on (NULL = legacy
+ * default stream). Asynchronous: the results are ready when the stream reaches them.
+ *
+ * The working memory is one fixed __device__ array of the library (about 1.4 MB per GPU that
+ * loads it, held until the process exits), so planes are limited to width and height in 8..4096
+ * and at most 1920 x 1088 samples; larger ones get RG_ERR_INVALID (use rg_ssim_plane). Every call
+ * on a device shares that array: calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller. The first call on each device looks the array up
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture begins.
+ */
+int rg_ssim_plane_device_noalloc(const uint8_t* dev_a, size_t stride_a, const uint8_t* dev_b,
+                                 size_t stride_b, int32_t width, int32_t height, double* dev_out,
+                                 void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libragdoll_cuda.so"
 BUILD = PKG / "_build"
 
-SOURCES = ["engine_kernels.cu", "ssim_kernels.cu", "rg_api.cu"]
+SOURCES = ["engine_kernels.cu", "ssim_kernels.cu", "rg_api.cu", "ssim_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "-Xcompiler", "-march=x86-64-v3", "--expt-relaxed-constexpr"]
@@ -46,7 +46,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     for src in SOURCES:
         obj = BUILD / (Path(src).stem + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_v else []
-        if src == "ssim_kernels.cu":
+        if src in ("ssim_kernels.cu", "ssim_noalloc.cu"):
             extra += ["-fmad=false"]
         cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:

@@ -82,6 +82,11 @@ void skip_bounds(int qp, int qpc, FrameParams& fp) {
 
 }  // namespace
 
+namespace rg {
+// Records msg as the calling thread's rg_last_error() (used by entry points in other files).
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace rg
+
 struct rg_ctx {
   rg_config cfg{};
   FrameParams fp{};

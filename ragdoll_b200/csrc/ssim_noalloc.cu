@@ -25,9 +25,12 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
-#include <string>
 
 #include "../../include/ragdoll_cuda.h"
+
+namespace rg {
+void set_last_error(const char* msg);
+}
 
 namespace {
 
@@ -155,14 +158,13 @@ __global__ void na_finish_kernel(NaPack p) {
   p.out[1] = fmin(1.0, fmax(0.0, prod));
 }
 
-thread_local std::string na_error;
 int na_fail(int code, const char* fmt, ...) {
   char buf[384];
   va_list ap;
   va_start(ap, fmt);
   vsnprintf(buf, sizeof buf, fmt, ap);
   va_end(ap);
-  na_error = buf;
+  rg::set_last_error(buf);
   return code;
 }
 
@@ -189,8 +191,6 @@ int na_setup(int dev, uint8_t** out) {
 }
 
 }  // namespace
-
-extern "C" const char* rg_noalloc_last_error(void) { return na_error.c_str(); }
 
 extern "C" int rg_ssim_plane_device_noalloc(const uint8_t* dev_a, size_t stride_a, const uint8_t* dev_b,
                                             size_t stride_b, int32_t width, int32_t height, double* dev_out,

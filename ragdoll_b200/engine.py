@@ -37,7 +37,7 @@ EXPORTS = [
     "rg_last_error", "rg_version", "rg_create", "rg_destroy", "rg_mb_dims", "rg_analyse_frame",
     "rg_analyse_batch", "rg_analyse_batch_device", "rg_sync", "rg_copy_records", "rg_get_recon",
     "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
-    "rg_quality_frame", "rg_ssim_plane",
+    "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc",
 ]
 
 
@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
     L.rg_ssim_plane.argtypes = [ctypes.c_int32, u8p, ctypes.c_size_t, u8p, ctypes.c_size_t,
                                 ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(ctypes.c_double)]
+    L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
+                                               ctypes.c_int32, P, P]
     _lib = L
     return L
 
@@ -215,3 +217,11 @@ def ssim_plane(a: np.ndarray, b: np.ndarray, device: int = 0):
     _check(lib().rg_ssim_plane(device, _u8(a), a.strides[0], _u8(b), b.strides[0], a.shape[1], a.shape[0],
                                ctypes.byref(s), ctypes.byref(m)))
     return s.value, m.value
+
+
+def ssim_plane_device_noalloc(dev_a: int, stride_a: int, dev_b: int, stride_b: int, width: int, height: int,
+                              dev_out: int, stream: int = 0) -> None:
+    """Queues SSIM / MS-SSIM of two device planes into ``dev_out`` (two device doubles) on
+    ``stream`` without any device allocation (rg_ssim_plane_device_noalloc)."""
+    _check(lib().rg_ssim_plane_device_noalloc(dev_a, stride_a, dev_b, stride_b, width, height, dev_out,
+                                               stream or None))
