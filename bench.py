@@ -183,22 +183,36 @@ def run_engine(args, rank, world, local):
         p = base + i * fbytes
         return [p, p + W * H, p + W * H + cw * ch]
 
-    eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local)
+    eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
+    if args.skew is not None:
+        eng.set_pipeline_tuning(skew=args.skew)
     stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
     torch.cuda.synchronize()
-
-    def device_step():
-        for i in range(GOP):
-            ptrs = []
-            for g in range(gops):
-                ptrs += planes(g * GOP + i)
-            eng.analyse_device(ptrs, W, cw, [RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops)
-
+    gop_ptrs, gop_kinds = [], []
+    for i in range(GOP):
+        for g in range(gops):
+            gop_ptrs += planes(g * GOP + i)
+            gop_kinds.append(RG_FRAME_IDR if i == 0 else RG_FRAME_P)
     frames_host = [[clip[g * GOP + i] for g in range(gops)] for i in range(GOP)]
+    kinds_host = [[RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops for i in range(GOP)]
 
-    def host_step():
-        for i in range(GOP):
-            eng.analyse(frames_host[i], [RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops)
+    if args.mode == "pipelined":
+        def device_step():
+            eng.analyse_gops_device(gop_ptrs, W, cw, gop_kinds, GOP)
+
+        def host_step():
+            eng.analyse_gops(frames_host, kinds_host)
+    else:
+        def device_step():
+            for i in range(GOP):
+                ptrs = []
+                for g in range(gops):
+                    ptrs += planes(g * GOP + i)
+                eng.analyse_device(ptrs, W, cw, [RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops)
+
+        def host_step():
+            for i in range(GOP):
+                eng.analyse(frames_host[i], [RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops)
 
     def barrier():
         if dist is not None:
@@ -225,6 +239,7 @@ def run_engine(args, rank, world, local):
         device_step()
     ev1.record(stream)
     ev1.synchronize()
+    eng.sync()
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
@@ -240,32 +255,16 @@ def run_engine(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps)
 
-    # per-launch duration of the wavefront kernel: events around every launch of one batch
-    from ragdoll_b200.engine import lib
-    steps_per_frame = None
-    launch_ms = None
-    if True:
-        import ctypes
-        evs = []
-        ptrs = []
-        for g in range(gops):
-            ptrs += planes(g * GOP + 1)
-        # time one P batch (same content as the timed P frames) launch by launch
-        mb_w, mb_h = eng.mb_w, eng.mb_h
-        steps_per_frame = (mb_w - 1) + 2 * (mb_h - 1) + 1 + 3
-        e_start = torch.cuda.Event(enable_timing=True)
-        e_end = torch.cuda.Event(enable_timing=True)
-        # a fresh IDR then one P batch, timing the P batch as a whole
-        idr_ptrs = []
-        for g in range(gops):
-            idr_ptrs += planes(g * GOP)
-        eng.analyse_device(idr_ptrs, W, cw, [RG_FRAME_IDR] * gops)
-        e_start.record(stream)
-        eng.analyse_device(ptrs, W, cw, [RG_FRAME_P] * gops)
-        e_end.record(stream)
-        e_end.synchronize()
-        batch_ms = e_start.elapsed_time(e_end)
-        launch_ms = batch_ms / (steps_per_frame + 1)
+    # per-launch duration of the dominant kernel
+    steps_per_frame = (eng.mb_w - 1) + 2 * (eng.mb_h - 1) + 1 + 3
+    if args.mode == "pipelined":
+        kernel_name, launches_per_step = "pipeline_kernel", 1
+        launch_ms = dev_ms
+        bytes_per_launch = BYTES_PER_FRAME * FRAMES
+    else:
+        kernel_name, launches_per_step = "wavefront_step_kernel", GOP * (steps_per_frame + 1)
+        launch_ms = dev_ms / launches_per_step
+        bytes_per_launch = BYTES_PER_FRAME * gops / (steps_per_frame + 1)
 
     frames_total = FRAMES * world
     value = frames_total / (dev_ms / 1000)
@@ -276,9 +275,8 @@ def run_engine(args, rank, world, local):
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    bytes_per_launch = BYTES_PER_FRAME * gops / (steps_per_frame + 1)
     achieved = bytes_per_launch / (launch_ms / 1000) / 1e9
-    launches = args.steps * GOP * (steps_per_frame + 1)
+    launches = args.steps * launches_per_step
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -294,6 +292,7 @@ def run_engine(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": round(dev_ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings, BASELINE config 2 shape)",
             "config": {"workload": "1080p High QP26 Balanced, 120 frames = 8 GOPs x 15 (IDR + 14 P) side by side",
+                       "mode": args.mode,
                        "width": W, "height": H, "frames_per_gpu": FRAMES, "gop": GOP, "qp": QP, "profile": "high",
                        "motion_px": MOTION, "rects": RECTS, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (373 MB source clip per GPU)"},
@@ -301,7 +300,7 @@ def run_engine(args, rank, world, local):
                     "d2h_bytes_per_step": GOP * gops * eng.n_mb * 852},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "traffic": None,
-                         "kernel": "wavefront_step_kernel", "launch_ms": round(launch_ms, 5),
+                         "kernel": kernel_name, "launch_ms": round(launch_ms, 5),
                          "bytes_per_launch": round(bytes_per_launch)},
             "cpu_baseline": cpu,
             "clocks": clk,
@@ -313,6 +312,75 @@ def run_engine(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_profile_case(args, local):
+    """Small case for ncu: one IDR batch and one P batch of the 8-GOP 1080p workload (16 frames),
+    with the device time of each batch -- per anti-diagonal launches, or (pipelined) the first
+    three pictures (IDR, P, P) of the 8 GOPs in one persistent launch."""
+    import torch
+
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_HIGH, Engine
+
+    torch.cuda.set_device(local)
+    gops = FRAMES // GOP
+    clip = make_clip(2000, GOP + 1)
+    # GOP g reads frames (g, g+1) of one short clip: distinct content per GOP, 16 frames in total
+    cw, ch = (W + 1) // 2, (H + 1) // 2
+    fbytes = W * H + 2 * cw * ch
+    host = np.empty((len(clip), fbytes), np.uint8)
+    for i, (y, u, v) in enumerate(clip):
+        host[i] = np.concatenate([y.reshape(-1), u.reshape(-1), v.reshape(-1)])
+    dev = torch.from_numpy(host).to(f"cuda:{local}")
+    base = dev.data_ptr()
+    if args.profile_case == "pipelined":
+        nf = 3
+        eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=nf)
+        if args.skew is not None:
+            eng.set_pipeline_tuning(skew=args.skew)
+        stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+        ptrs, kinds = [], []
+        for f in range(nf):
+            for g in range(gops):
+                p = base + (g + f) * fbytes
+                ptrs += [p, p + W * H, p + W * H + cw * ch]
+                kinds.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.analyse_gops_device(ptrs, W, cw, kinds, nf)
+            e1.record(stream)
+            e1.synchronize()
+            eng.sync()
+            times.append(e0.elapsed_time(e1))
+        print(json.dumps({"profile_case": "1080p High QP26, 8 streams x 3 pictures (IDR, P, P), one pipelined launch",
+                          "launch_ms": [round(t, 3) for t in times]}), flush=True)
+        eng.close()
+        return
+    eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local)
+    stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    times = []
+    for f in range(2):
+        ptrs = []
+        for g in range(gops):
+            p = base + (g + f) * fbytes
+            ptrs += [p, p + W * H, p + W * H + cw * ch]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.analyse_device(ptrs, W, cw, [RG_FRAME_IDR if f == 0 else RG_FRAME_P] * gops)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    recs = eng.records()
+    kinds = np.bincount(recs["mb_type"].reshape(-1), minlength=4).tolist()
+    print(json.dumps({"profile_case": "1080p High QP26, 8 streams, IDR batch then P batch",
+                      "idr_batch_ms": round(times[0], 3), "p_batch_ms": round(times[1], 3),
+                      "launches_per_batch": eng.mb_w - 1 + 2 * (eng.mb_h - 1) + 1 + 3 + 1,
+                      "p_mb_types[skip,p16,i16,i4]": kinds}), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,8 +388,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],
+                    help="one persistent launch for all 15 pictures of the 8 GOPs, or one launch per anti-diagonal")
+    ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
+                    choices=["wavefront", "pipelined"],
+                    help="a small slice of the workload (the ncu capture case)")
+    ap.add_argument("--skew", type=int, default=None,
+                    help="pipelined mode: row-times between the starts of consecutive pictures")
     args = ap.parse_args()
     rank, world, local = dist_env()
+    if args.profile_case:
+        run_profile_case(args, local)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

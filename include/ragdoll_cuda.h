@@ -55,6 +55,7 @@ typedef struct rg_config {
     int32_t qp;          /* fixed QP 1..51 (RateControlMode::FixedQp)                          */
     int32_t num_streams; /* independent streams / GOPs analysed together (>= 1)                */
     int32_t device;      /* CUDA device ordinal                                                */
+    int32_t max_frames;  /* pictures per stream in one rg_analyse_gops call (0 or 1: one)       */
 } rg_config;
 
 /* ---- per-macroblock decision record ------------------------------------------------------ */
@@ -142,6 +143,36 @@ int rg_analyse_batch(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y,
  */
 int rg_analyse_batch_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t stride_y,
                             size_t stride_uv, const int32_t* kinds);
+
+/*
+ * Pipelined form: `frames` consecutive pictures of every stream (frames <= cfg.max_frames) in
+ * one persistent launch (the frame loop of GopRingEncoder::encode_wave's workers,
+ * crates/ragdoll-pipeline/src/lib.rs:580-597, for all GOPs at once). Picture f+1 of a stream
+ * starts as soon as the region of picture f its motion search can reach is final, so the
+ * pictures of a GOP overlap. dev_planes: frames * num_streams * 3 device pointers, picture-major
+ * ([f][s][y,u,v]); kinds: frames * num_streams RG_FRAME_* values ([f][s]). Records of picture f,
+ * stream s land at record index (f * num_streams + s) * mb_w * mb_h (rg_copy_records_gops).
+ * Asynchronous; rg_sync reports RG_ERR_TIMEOUT if a device wait gave up.
+ */
+int rg_analyse_gops_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t stride_y,
+                           size_t stride_uv, const int32_t* kinds, int32_t frames);
+
+/* Host-buffer form of rg_analyse_gops_device; out receives frames * num_streams * mb_w * mb_h
+ * records (or NULL). */
+int rg_analyse_gops(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                    const int32_t* kinds, int32_t frames, rg_mb_out* out);
+
+/* Copies the records of the last `frames` pictures of an rg_analyse_gops* call. */
+int rg_copy_records_gops(rg_ctx* ctx, int32_t frames, rg_mb_out* out);
+
+/*
+ * Tuning / test hook of the pipelined mode: skew = row-times between consecutive pictures of a
+ * stream in the work order (1..10; larger is safer for long motion, smaller overlaps more
+ * pictures), grid = resident warps (0 = all that fit), timeout_ms = limit of one device wait
+ * (0 = 2000). A wait that runs out makes the launch stop and rg_sync re-run the call on the
+ * per-diagonal path, which has no waits.
+ */
+int rg_set_pipeline_tuning(rg_ctx* ctx, int32_t skew, int32_t grid, int32_t timeout_ms);
 
 /* Waits for queued device work of the context. */
 int rg_sync(rg_ctx* ctx);

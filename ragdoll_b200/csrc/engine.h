@@ -71,6 +71,13 @@ struct FrameParams {
 void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st);
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st);
 int wavefront_steps(const FrameParams& fp);
+// Pipelined mode: d_streams holds frames x n_streams descriptors (picture-major); counters is
+// pipeline_counter_ints() zeroed ints; counters[1] is non-zero after a failed wait.
+int pipeline_grid(int device);
+size_t pipeline_counter_ints(const FrameParams& fp, int frames);
+int pipeline_ticket_table(const FrameParams& fp, int frames, int skew, int* table);
+void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int* d_table,
+                     int n_times, int skew, int grid, unsigned long long timeout_ns, cudaStream_t st);
 void upload_tables();
 
 }  // namespace rg

@@ -76,6 +76,13 @@ struct __align__(16) Smem {
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ MbInfo ld_info(const MbInfo* p) {
+  int4 v;
+  asm volatile("ld.global.v4.s32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  MbInfo m;
+  *(int4*)&m = v;
+  return m;
+}
 __device__ __forceinline__ uint32_t wsum(uint32_t v) { return __reduce_add_sync(FULL, v); }
 __device__ __forceinline__ uint32_t wmin(uint32_t v) { return __reduce_min_sync(FULL, v); }
 __device__ __forceinline__ uint32_t wor(uint32_t v) { return __reduce_or_sync(FULL, v); }
@@ -111,19 +118,26 @@ __device__ __forceinline__ uint32_t mvd_cost(int d, uint32_t lambda) {
   return (d >= -4096 && d <= 4096) ? (c & 0xFFFFu) : c;
 }
 
-// 8 unaligned bytes from global memory (two 32-bit words).
-__device__ __forceinline__ uint2 load8(const uint8_t* p) {
-  uintptr_t a = (uintptr_t)p;
-  const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
-  uint32_t sh = (uint32_t)(a & 3) * 8u;
-  uint32_t w0 = b[0], w1 = b[1], w2 = b[2];
-  return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
+// Reconstructed pictures and macroblock state are produced by other warps of the same launch in
+// the pipelined mode. They are read with plain weak loads (never the non-coherent path), and only
+// after an ld.acquire that observed the producer's release: the memory model then guarantees the
+// loads see the produced values, L1 included.
+__device__ __forceinline__ uint32_t ldw32(const void* p) {
+  uint32_t v;
+  asm volatile("ld.global.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
 }
+__device__ __forceinline__ uint8_t ldcg_u8(const uint8_t* p) {
+  uint16_t v;
+  asm volatile("ld.global.u8 %0, [%1];" : "=h"(v) : "l"(p));
+  return (uint8_t)v;
+}
+__device__ __forceinline__ uint32_t ldcg_u32(const uint8_t* p) { return ldw32(p); }
 __device__ __forceinline__ uint2 ldg8(const uint8_t* p) {
   uintptr_t a = (uintptr_t)p;
-  const unsigned int* b = (const unsigned int*)(a & ~(uintptr_t)3);
+  const uint8_t* b = (const uint8_t*)(a & ~(uintptr_t)3);
   uint32_t sh = (uint32_t)(a & 3) * 8u;
-  uint32_t w0 = __ldg(b), w1 = __ldg(b + 1), w2 = __ldg(b + 2);
+  uint32_t w0 = ldw32(b), w1 = ldw32(b + 4), w2 = ldw32(b + 8);
   return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
 }
 __device__ __forceinline__ uint32_t vsad8(uint2 a, uint2 b) { return __vsadu4(a.x, b.x) + __vsadu4(a.y, b.y); }
@@ -223,7 +237,7 @@ __device__ __forceinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_
 // ---------------------------------------------------------------------------------------------
 // Half-sample window (h264_enc.rs:747 hpel_window, :803 hpel_window_centre): integer origin
 // (ox, oy); plane coordinate (r, c) is the sample at (ox + c, oy + r).
-__device__ void stage_window(const uint8_t* ref, int stride, int ox, int oy, Smem& sm) {
+__device__ __noinline__ void stage_window(const uint8_t* ref, int stride, int ox, int oy, Smem& sm) {
   int lane = lane_id();
   for (int q = lane; q < 23 * 6; q += 32) {
     int k = q / 6, w = q % 6;
@@ -231,13 +245,13 @@ __device__ void stage_window(const uint8_t* ref, int stride, int ox, int oy, Sme
     uintptr_t a = (uintptr_t)p;
     const unsigned int* b = (const unsigned int*)(a & ~(uintptr_t)3);
     uint32_t sh = (uint32_t)(a & 3) * 8u;
-    uint32_t v = __funnelshift_r(__ldg(b), __ldg(b + 1), sh);
+    uint32_t v = __funnelshift_r(ldw32(b), ldw32(b + 1), sh);
     *(uint32_t*)&sm.win[k * 24 + 4 * w] = v;
   }
   __syncwarp();
 }
 // need: bit 0 b plane (h), bit 1 h plane (v), bit 2 j plane (c)
-__device__ void build_hpel(Smem& sm, int need) {
+__device__ __noinline__ void build_hpel(Smem& sm, int need) {
   int lane = lane_id();
   if (need & 5) {
     for (int i = lane; i < 23 * 18; i += 32) {
@@ -273,53 +287,60 @@ __device__ __forceinline__ int planes_needed(int fx, int fy) {
   if (fy == 2) return 6;
   return 3;
 }
-// Quarter-sample prediction sample (i, j) of the 16x16 block whose integer position is
-// (wx, wy) in window coordinates (ITU-T H.264 8.4.2.2.1 as h264_luma_mc_scalar, h264_mc.rs:148).
-__device__ __forceinline__ int qpel_sample(const Smem& sm, int wx, int wy, int fx, int fy, int i, int j) {
-  int r = wy + i, c = wx + j;
-#define G_(dr, dc) ((int)sm.win[(r + (dr) + 2) * 24 + c + (dc) + 2])
-#define B_(dr, dc) ((int)sm.hph[(r + (dr)) * 20 + c + (dc)])
-#define V_(dr, dc) ((int)sm.hpv[(r + (dr)) * 20 + c + (dc)])
-#define J_(dr, dc) ((int)sm.hpj[(r + (dr)) * 20 + c + (dc)])
-#define AV(a, b) (((a) + (b) + 1) >> 1)
+// Quarter-sample prediction of the 16x16 block whose integer position is (wx, wy) in window
+// coordinates: one window plane, or the rounded average of two (window_src, enc.rs:1395; equal
+// to h264_luma_mc_scalar, h264_mc.rs:148, by enc.rs:4030). Returns the two source rows' bases.
+struct QSrc {
+  const uint8_t* a;
+  const uint8_t* b;
+  int sa, sb, avg;
+};
+__device__ __noinline__ QSrc qpel_src(const Smem& sm, int wx, int wy, int fx, int fy) {
+  const uint8_t* G = &sm.win[(wy + 2) * 24 + wx + 2];
+  const uint8_t* B = &sm.hph[wy * 20 + wx];
+  const uint8_t* V = &sm.hpv[wy * 20 + wx];
+  const uint8_t* J = &sm.hpj[wy * 20 + wx];
   switch (fx | (fy << 2)) {
-    case 0: return G_(0, 0);
-    case 1: return AV(G_(0, 0), B_(0, 0));
-    case 2: return B_(0, 0);
-    case 3: return AV(B_(0, 0), G_(0, 1));
-    case 4: return AV(G_(0, 0), V_(0, 0));
-    case 5: return AV(B_(0, 0), V_(0, 0));
-    case 6: return AV(B_(0, 0), J_(0, 0));
-    case 7: return AV(B_(0, 0), V_(0, 1));
-    case 8: return V_(0, 0);
-    case 9: return AV(V_(0, 0), J_(0, 0));
-    case 10: return J_(0, 0);
-    case 11: return AV(J_(0, 0), V_(0, 1));
-    case 12: return AV(V_(0, 0), G_(1, 0));
-    case 13: return AV(V_(0, 0), B_(1, 0));
-    case 14: return AV(J_(0, 0), B_(1, 0));
-    default: return AV(V_(0, 1), B_(1, 0));
+    case 0: return {G, G, 24, 24, 0};
+    case 1: return {G, B, 24, 20, 1};
+    case 2: return {B, B, 20, 20, 0};
+    case 3: return {B, G + 1, 20, 24, 1};
+    case 4: return {G, V, 24, 20, 1};
+    case 5: return {B, V, 20, 20, 1};
+    case 6: return {B, J, 20, 20, 1};
+    case 7: return {B, V + 1, 20, 20, 1};
+    case 8: return {V, V, 20, 20, 0};
+    case 9: return {V, J, 20, 20, 1};
+    case 10: return {J, J, 20, 20, 0};
+    case 11: return {J, V + 1, 20, 20, 1};
+    case 12: return {V, G + 24, 20, 24, 1};
+    case 13: return {V, B + 20, 20, 20, 1};
+    case 14: return {J, B + 20, 20, 20, 1};
+    default: return {V + 1, B + 20, 20, 20, 1};
   }
-#undef G_
-#undef B_
-#undef V_
-#undef J_
-#undef AV
 }
-// 8 prediction samples of this lane (row lane/2, columns 8 (lane&1) ..) packed in two words.
-__device__ __forceinline__ uint2 qpel8(const Smem& sm, int wx, int wy, int fx, int fy) {
+// 8 bytes of shared memory at any alignment (rows of the window planes are 4-byte aligned).
+__device__ __forceinline__ uint2 lds8(const uint8_t* p) {
+  uintptr_t a = (uintptr_t)p;
+  const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
+  uint32_t sh = (uint32_t)(a & 3) * 8u;
+  uint32_t w0 = b[0], w1 = b[1], w2 = b[2];
+  return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
+}
+// This lane's 8 prediction samples (row lane/2, columns 8 (lane&1) ..) packed in two words.
+__device__ __forceinline__ uint2 qpel8(const QSrc& q) {
   int lane = lane_id(), i = lane >> 1, j0 = (lane & 1) * 8;
-  uint32_t w[2] = {0, 0};
-#pragma unroll
-  for (int k = 0; k < 8; k++) w[k >> 2] |= (uint32_t)qpel_sample(sm, wx, wy, fx, fy, i, j0 + k) << (8 * (k & 3));
-  return make_uint2(w[0], w[1]);
+  uint2 a = lds8(q.a + i * q.sa + j0);
+  if (!q.avg) return a;
+  uint2 b = lds8(q.b + i * q.sb + j0);
+  return make_uint2(__vavgu4(a.x, b.x), __vavgu4(a.y, b.y));
 }
 __device__ __forceinline__ uint2 src8(const Smem& sm) {
   int lane = lane_id();
   return *(const uint2*)&sm.src_y[(lane >> 1) * 16 + (lane & 1) * 8];
 }
 // Prediction of the 16x16 block displaced by mv into pred_y (enc.rs:1058 mc_luma).
-__device__ void mc_luma16(const uint8_t* ref, int stride, int x0, int y0, int mvx, int mvy, Smem& sm) {
+__device__ __noinline__ void mc_luma16(const uint8_t* ref, int stride, int x0, int y0, int mvx, int mvy, Smem& sm) {
   int ix = x0 + (mvx >> 2), iy = y0 + (mvy >> 2), fx = mvx & 3, fy = mvy & 3;
   int lane = lane_id();
   if ((fx | fy) == 0) {
@@ -330,12 +351,12 @@ __device__ void mc_luma16(const uint8_t* ref, int stride, int x0, int y0, int mv
   }
   stage_window(ref, stride, ix, iy, sm);
   build_hpel(sm, planes_needed(fx, fy));
-  uint2 v = qpel8(sm, 0, 0, fx, fy);
+  uint2 v = qpel8(qpel_src(sm, 0, 0, fx, fy));
   *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
   __syncwarp();
 }
 // Chroma prediction of both planes (h264_enc.rs:1279 chroma_mc_8x8_x2_scalar; enc.rs:1082).
-__device__ void mc_chroma8(const uint8_t* ru, const uint8_t* rv, int stride, int mbx, int mby, int mvx, int mvy, Smem& sm) {
+__device__ __noinline__ void mc_chroma8(const uint8_t* ru, const uint8_t* rv, int stride, int mbx, int mby, int mvx, int mvy, Smem& sm) {
   int lane = lane_id();
   int cx = mbx * 8 + (mvx >> 3), cy = mby * 8 + (mvy >> 3), fx = mvx & 7, fy = mvy & 7;
   int wa = (8 - fx) * (8 - fy), wb = fx * (8 - fy), wc = (8 - fx) * fy, wd = fx * fy;
@@ -344,7 +365,7 @@ __device__ void mc_chroma8(const uint8_t* ru, const uint8_t* rv, int stride, int
   uint8_t* out = (plane ? sm.pred_v : sm.pred_u) + r * 8 + c0;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    int a = __ldg(src + k), b = __ldg(src + k + 1), cc = __ldg(src + stride + k), d = __ldg(src + stride + k + 1);
+    int a = ldcg_u8(src + k), b = ldcg_u8(src + k + 1), cc = ldcg_u8(src + stride + k), d = ldcg_u8(src + stride + k + 1);
     out[k] = (uint8_t)((wa * a + wb * b + wc * cc + wd * d + 32) >> 6);
   }
   __syncwarp();
@@ -365,7 +386,7 @@ __device__ __forceinline__ int quant_level(int c, uint32_t mf, uint32_t bias, ui
 
 // Luma 4x4 residual of pred_y, quantised (inter) and decimated into sm.coef
 // (enc.rs:1810 quant_luma_4x4_inter). Returns cbp; lanes 0..15 own block lane.
-__device__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_out) {
+__device__ __noinline__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_out) {
   int lane = lane_id();
   int qp = fp.qp;
   uint32_t shift, bias;
@@ -404,15 +425,13 @@ __device__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_
   g_sc += __shfl_xor_sync(FULL, g_sc, 2);
   int cbp = 0;
   uint32_t total = 0;
-  int keep[4];
 #pragma unroll
   for (int g = 0; g < 4; g++) {
     int nz = __shfl_sync(FULL, g_nz, 4 * g), big = __shfl_sync(FULL, g_big, 4 * g);
     uint32_t sc = __shfl_sync(FULL, g_sc, 4 * g);
-    keep[g] = 0;
     if (!nz) continue;
-    if (big) { cbp |= 1 << g; total += 9; keep[g] = 1; continue; }
-    if (sc >= 4) { cbp |= 1 << g; keep[g] = 1; }
+    if (big) { cbp |= 1 << g; total += 9; continue; }
+    if (sc >= 4) cbp |= 1 << g;
     total += sc;
   }
   if (total < 6 && cbp) cbp = 0;
@@ -420,7 +439,6 @@ __device__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_
 #pragma unroll
     for (int i = 0; i < 16; i++) sm.coef[lane * 16 + i] = 0;
   }
-  (void)keep;
   __syncwarp();
   if (nz_lane_out) *nz_lane_out = (lane < 16 && ((cbp >> (lane >> 2)) & 1)) ? (uint32_t)my_nz : 0u;
   return cbp;
@@ -428,7 +446,7 @@ __device__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_
 
 // Luma 8x8 residual of pred_y, quantised (inter) and decimated into sm.coef8
 // (enc.rs:2041 quant_luma_8x8_inter). Lanes 8b..8b+7 own block b. Returns cbp; *nnz8 = count.
-__device__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint32_t* nnz8) {
+__device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint32_t* nnz8) {
   int lane = lane_id();
   int b = lane >> 3, q = lane & 7;
   int bx = (b & 1) * 8, by = (b >> 1) * 8;
@@ -500,7 +518,7 @@ __device__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint32_t* nnz8) {
 // Chroma residual of pred_u/pred_v (enc.rs:1899 quant_chroma): lanes 0..7 own block
 // (plane = lane / 4, b = lane % 4). Levels into sm.ccoef (raster), DC levels into sm.cdc.
 // Outputs per plane: AC present and AC decimation score. Lanes 0..31 all return the values.
-__device__ void chroma_quant(int qpc, bool intra, Smem& sm, uint32_t ac_any[2], uint32_t ac_score[2]) {
+__device__ __noinline__ void chroma_quant(int qpc, bool intra, Smem& sm, uint32_t ac_any[2], uint32_t ac_score[2]) {
   int lane = lane_id();
   uint32_t shift, bias;
   quant4_params(qpc, intra, shift, bias);
@@ -558,7 +576,7 @@ __device__ __forceinline__ bool chroma_dc_any(const Smem& sm) {
 }
 
 // Adds the dequantised chroma residual to pred_u / pred_v (enc.rs:1992 recon_chroma).
-__device__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
+__device__ __noinline__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
   int lane = lane_id();
   if (cbpc == 0) return;
   if (lane < 8) {
@@ -619,7 +637,7 @@ __device__ __forceinline__ int dc16(const Smem& sm, bool ht, bool hl) {
   if (hl) return (int)((sl + 8) >> 4);
   return 128;
 }
-__device__ void pred16_into(int mode, Smem& sm, uint8_t* dst, bool ht, bool hl, int tl) {
+__device__ __noinline__ void pred16_into(int mode, Smem& sm, uint8_t* dst, bool ht, bool hl, int tl) {
   int lane = lane_id();
   int dc = mode == 2 ? dc16(sm, ht, hl) : 0;
   int pa = 0, pb = 0, pc = 0;
@@ -630,7 +648,7 @@ __device__ void pred16_into(int mode, Smem& sm, uint8_t* dst, bool ht, bool hl, 
   __syncwarp();
 }
 // Intra 16x16 analysis (enc.rs:1637 analyse_i16_edges): SATD per mode; returns best mode.
-__device__ int analyse_i16(Smem& sm, bool ht, bool hl, int tl, uint32_t* best_cost) {
+__device__ __noinline__ int analyse_i16(Smem& sm, bool ht, bool hl, int tl, uint32_t* best_cost) {
   int lane = lane_id();
   int dc = dc16(sm, ht, hl);
   uint32_t sv = 0, sh = 0, sd = 0;
@@ -722,7 +740,7 @@ __device__ void chroma_pred_params(const Smem& sm, int p, bool ht, bool hl, int 
   pc = (17 * V + 16) >> 5;
 }
 // Intra chroma mode by SAD (enc.rs:1526 analyse_chroma_intra); best prediction into pred_u/v.
-__device__ int analyse_chroma(Smem& sm, bool ht, bool hl, const int* ctl) {
+__device__ __noinline__ int analyse_chroma(Smem& sm, bool ht, bool hl, const int* ctl) {
   int lane = lane_id();
   int plane = lane >> 4, idx = (lane & 15) * 4, y = idx >> 3, x0 = idx & 7;
   int dcv[4], pa, pb, pc;
@@ -747,7 +765,7 @@ __device__ int analyse_chroma(Smem& sm, bool ht, bool hl, const int* ctl) {
 }
 
 // Intra 4x4 prediction of mode m (h264_dsp.rs:799 predict_intra_4x4_u8_scalar) into out[16].
-__device__ void pred4x4(int mode, const uint8_t* t, const uint8_t* l, bool ht, bool hl, int m, uint8_t* o) {
+__device__ __noinline__ void pred4x4(int mode, const uint8_t* t, const uint8_t* l, bool ht, bool hl, int m, uint8_t* o) {
   int A = t[0], B = t[1], C = t[2], D = t[3], E = t[4], F = t[5], G = t[6], H = t[7];
   int I = l[0], J = l[1], K = l[2], L = l[3];
 #define A2(x, y) (uint8_t)(((x) + (y) + 1) >> 1)
@@ -819,7 +837,7 @@ struct Ctx {
 
 // Loads the source macroblock, replicating the last row / column past the picture edges
 // (enc.rs:400 MbSrc::load, h264.rs:3660 extract_mb_planes).
-__device__ void load_source(const Ctx& c, Smem& sm) {
+__device__ __noinline__ void load_source(const Ctx& c, Smem& sm) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int W = fp.width, H = fp.height, cw = (W + 1) >> 1, ch = (H + 1) >> 1;
@@ -837,7 +855,7 @@ __device__ void load_source(const Ctx& c, Smem& sm) {
   __syncwarp();
 }
 // Intra edges from the unfiltered reconstruction of this picture (enc.rs:1459-1521).
-__device__ void load_edges(const Ctx& c, Smem& sm, bool want_topright, int& tl, int* ctl) {
+__device__ __noinline__ void load_edges(const Ctx& c, Smem& sm, bool want_topright, int& tl, int* ctl) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   const uint8_t* Y = c.sd->cur_y;
@@ -845,24 +863,24 @@ __device__ void load_edges(const Ctx& c, Smem& sm, bool want_topright, int& tl, 
   bool ht = c.mby > 0, hl = c.mbx > 0;
   if (ht && lane < 24) {
     bool ok = lane < 16 || (want_topright && c.mbx + 1 < fp.mb_w);
-    sm.top[lane] = ok ? Y[(long)(y0 - 1) * fp.stride_y + x0 + lane] : 0;
+    sm.top[lane] = ok ? ldcg_u8(Y + (long)(y0 - 1) * fp.stride_y + x0 + lane) : 0;
   }
-  if (hl && lane < 16) sm.left[lane] = Y[(long)(y0 + lane) * fp.stride_y + x0 - 1];
+  if (hl && lane < 16) sm.left[lane] = ldcg_u8(Y + (long)(y0 + lane) * fp.stride_y + x0 - 1);
   int cx0 = c.mbx * 8, cy0 = c.mby * 8;
   if (lane < 16) {
     int p = lane >> 3, k = lane & 7;
     const uint8_t* P = p ? c.sd->cur_v : c.sd->cur_u;
-    if (ht) sm.ctop[p][k] = P[(long)(cy0 - 1) * fp.stride_c + cx0 + k];
-    if (hl) sm.cleft[p][k] = P[(long)(cy0 + k) * fp.stride_c + cx0 - 1];
+    if (ht) sm.ctop[p][k] = ldcg_u8(P + (long)(cy0 - 1) * fp.stride_c + cx0 + k);
+    if (hl) sm.cleft[p][k] = ldcg_u8(P + (long)(cy0 + k) * fp.stride_c + cx0 - 1);
   }
-  tl = (ht && hl) ? Y[(long)(y0 - 1) * fp.stride_y + x0 - 1] : 128;
-  ctl[0] = (ht && hl) ? c.sd->cur_u[(long)(cy0 - 1) * fp.stride_c + cx0 - 1] : 128;
-  ctl[1] = (ht && hl) ? c.sd->cur_v[(long)(cy0 - 1) * fp.stride_c + cx0 - 1] : 128;
+  tl = (ht && hl) ? ldcg_u8(Y + (long)(y0 - 1) * fp.stride_y + x0 - 1) : 128;
+  ctl[0] = (ht && hl) ? ldcg_u8(c.sd->cur_u + (long)(cy0 - 1) * fp.stride_c + cx0 - 1) : 128;
+  ctl[1] = (ht && hl) ? ldcg_u8(c.sd->cur_v + (long)(cy0 - 1) * fp.stride_c + cx0 - 1) : 128;
   __syncwarp();
 }
 
 // Stores the reconstruction of pred_y/u/v (or tmp_y for luma) into the current picture.
-__device__ void store_recon(const Ctx& c, const uint8_t* ly, Smem& sm) {
+__device__ __noinline__ void store_recon(const Ctx& c, const uint8_t* ly, Smem& sm) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int y = lane >> 1, x = (lane & 1) * 8;
@@ -883,7 +901,7 @@ __device__ void store_recon(const Ctx& c, const uint8_t* ly, Smem& sm) {
 }
 
 // Writes the chroma part of the record (chroma levels in zig-zag) and clears the rest.
-__device__ void record_chroma(rg_mb_out* rec, Smem& sm, int cbpc) {
+__device__ __noinline__ void record_chroma(rg_mb_out* rec, Smem& sm, int cbpc) {
   int lane = lane_id();
   if (lane < 8) {
     int p = lane >> 2, b = lane & 3;
@@ -893,7 +911,7 @@ __device__ void record_chroma(rg_mb_out* rec, Smem& sm, int cbpc) {
       for (int i = 0; i < 4; i++) rec->chroma_dc[p][i] = cbpc >= 1 ? sm.cdc[p * 4 + i] : 0;
   }
 }
-__device__ void record_header(rg_mb_out* rec, int type, int i16_mode, int cmode, int cbp, int t8, int qp, int mvx, int mvy,
+__device__ __noinline__ void record_header(rg_mb_out* rec, int type, int i16_mode, int cmode, int cbp, int t8, int qp, int mvx, int mvy,
                               int mvdx, int mvdy, uint16_t nz) {
   rec->mb_type = (uint8_t)type;
   rec->i16_mode = (uint8_t)i16_mode;
@@ -910,7 +928,7 @@ __device__ void record_header(rg_mb_out* rec, int type, int i16_mode, int cmode,
   rec->nz_mask = nz;
   rec->reserved1 = 0;
 }
-__device__ void write_info(const Ctx& c, int flags, int cbpl, int mvx, int mvy, int ref, uint16_t nz, const uint8_t* i4m) {
+__device__ __noinline__ void write_info(const Ctx& c, int flags, int cbpl, int mvx, int mvy, int ref, uint16_t nz, const uint8_t* i4m) {
   MbInfo inf;
   inf.mv[0] = (int16_t)mvx;
   inf.mv[1] = (int16_t)mvy;
@@ -933,7 +951,7 @@ __device__ void write_info(const Ctx& c, int flags, int cbpl, int mvx, int mvy, 
 }
 
 // I16x16 coding and reconstruction (enc.rs:3587 code_i16) with prediction mode `mode`.
-__device__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
+__device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int qp = fp.qp, qpc = fp.qpc;
@@ -1057,7 +1075,7 @@ __device__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int
 // I4x4 analysis (enc.rs:3336 analyse_i4): sixteen blocks in decoding order, each choosing among
 // the nine modes by SATD + lambda * mode bits, reconstructed into tmp_y before the next.
 // Returns false when the running cost reaches the budget. Levels go to sm.coef.
-__device__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out) {
+__device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int qp = fp.qp;
@@ -1069,8 +1087,8 @@ __device__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, 
   const MbInfo* info = c.sd->info;
   uint8_t lmodes[4], tmodes[4];
   for (int k = 0; k < 4; k++) {
-    lmodes[k] = hl_mb ? (info[c.mb - 1].i4_right >> (4 * k)) & 15 : 2;
-    tmodes[k] = ht_mb ? (info[c.mb - fp.mb_w].i4_bottom >> (4 * k)) & 15 : 2;
+    lmodes[k] = hl_mb ? (ld_info(&info[c.mb - 1]).i4_right >> (4 * k)) & 15 : 2;
+    tmodes[k] = ht_mb ? (ld_info(&info[c.mb - fp.mb_w]).i4_bottom >> (4 * k)) & 15 : 2;
   }
   for (int b = 0; b < 16; b++) {
     int bx = blk_x(b), by = blk_y(b), px = bx * 4, py = by * 4;
@@ -1173,7 +1191,7 @@ __device__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, 
   return true;
 }
 
-__device__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
+__device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int qpc = fp.qpc;
@@ -1202,7 +1220,7 @@ __device__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, cons
 }
 
 // One macroblock of an I slice (enc.rs:3311 code_intra).
-__device__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
+__device__ __noinline__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
   const FrameParams& fp = *c.fp;
   int tl, ctl[2];
   load_edges(c, sm, true, tl, ctl);
@@ -1221,7 +1239,7 @@ __device__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
 }
 
 // Codes P_Skip with vector mv; prediction already in pred_y / pred_u / pred_v.
-__device__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy) {
+__device__ __noinline__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy) {
   int lane = lane_id();
   rg_mb_out* rec = c.sd->rec + c.mb;
   if (lane < 16) {
@@ -1244,7 +1262,7 @@ __device__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy) {
 
 // Probe of the skip residual (enc.rs:2163 probe_skip_luma): no level above 1 and a total
 // decimation score below 6.
-__device__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
+__device__ __noinline__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
   int lane = lane_id();
   uint32_t shift, bias;
   quant4_params(fp.qp, false, shift, bias);
@@ -1276,8 +1294,55 @@ __device__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
   return !big && score < 6;
 }
 
-// One macroblock of a P slice (enc.rs:3011 code_p_mb).
-__device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
+// ---------------------------------------------------------------------------------------------
+// Pipelined mode synchronisation: monotonic progress counters, published with release stores
+// after a fence by every lane, polled with acquire loads by every lane. Every wait has a time
+// limit; when it runs out the kernel records RG_ERR_TIMEOUT and all warps leave.
+struct PipeWait {
+  const int* ana_prev;   // analysis progress per macroblock row of the reference frame
+  const int* db_prev;    // deblocking progress per row of the reference frame (padding included)
+  int* error;
+  unsigned long long timeout_ns;
+};
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits until *p >= need (all lanes). Returns false on timeout or when another warp failed.
+__device__ __noinline__ bool wait_geq(const int* p, int need, int* error, unsigned long long timeout_ns) {
+  if (__all_sync(FULL, ld_acquire(p) >= need)) return true;
+  unsigned long long t0 = global_ns();
+  while (true) {
+    if (__all_sync(FULL, ld_acquire(p) >= need)) return true;
+    int e = __shfl_sync(FULL, lane_id() == 0 ? ld_acquire(error) : 0, 0);
+    if (e) return false;
+    unsigned long long dt = __shfl_sync(FULL, global_ns() - t0, 0);
+    if (dt > timeout_ns) {
+      if (lane_id() == 0) atomicCAS(error, 0, 1);
+      return false;
+    }
+    __nanosleep(200);
+  }
+}
+// Makes this warp's global writes visible, then publishes v.
+__device__ __forceinline__ void publish(int* p, int v) {
+  __threadfence();
+  __syncwarp();
+  if (lane_id() == 0) st_release(p, v);
+}
+
+// One macroblock of a P slice (enc.rs:3011 code_p_mb). In the pipelined mode (pw != null) it
+// first waits for the reference frame to be final over every sample its search can read.
+__device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, const PipeWait* pw) {
   const FrameParams& fp = *c.fp;
   const StreamDev& sd = *c.sd;
   int lane = lane_id();
@@ -1293,10 +1358,10 @@ __device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
   const MbInfo* info = sd.info;
   int lref = -2, tref = -2, dref = -2;
   int a0 = 0, a1 = 0, b0 = 0, b1 = 0, c0 = 0, c1 = 0;
-  if (mbx > 0) { MbInfo n = info[c.mb - 1]; lref = n.ref; a0 = n.mv[0]; a1 = n.mv[1]; }
-  if (mby > 0) { MbInfo n = info[c.mb - mb_w]; tref = n.ref; b0 = n.mv[0]; b1 = n.mv[1]; }
-  if (mby > 0 && mbx + 1 < mb_w) { MbInfo n = info[c.mb - mb_w + 1]; dref = n.ref; c0 = n.mv[0]; c1 = n.mv[1]; }
-  else if (mby > 0 && mbx > 0) { MbInfo n = info[c.mb - mb_w - 1]; dref = n.ref; c0 = n.mv[0]; c1 = n.mv[1]; }
+  if (mbx > 0) { MbInfo n = ld_info(&info[c.mb - 1]); lref = n.ref; a0 = n.mv[0]; a1 = n.mv[1]; }
+  if (mby > 0) { MbInfo n = ld_info(&info[c.mb - mb_w]); tref = n.ref; b0 = n.mv[0]; b1 = n.mv[1]; }
+  if (mby > 0 && mbx + 1 < mb_w) { MbInfo n = ld_info(&info[c.mb - mb_w + 1]); dref = n.ref; c0 = n.mv[0]; c1 = n.mv[1]; }
+  else if (mby > 0 && mbx > 0) { MbInfo n = ld_info(&info[c.mb - mb_w - 1]); dref = n.ref; c0 = n.mv[0]; c1 = n.mv[1]; }
   // pred_motion_partition (h264.rs:3577), 16x16, ref 0
   int mvp0, mvp1;
   {
@@ -1314,6 +1379,27 @@ __device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
   if (mbx == 0 || mby == 0 || (lref == 0 && a0 == 0 && a1 == 0) || (tref == 0 && b0 == 0 && b1 == 0)) { ps0 = 0; ps1 = 0; }
   load_source(c, sm);
   int qpc = fp.qpc;
+  // co-located vector of the previous picture: a search candidate (enc.rs:3094)
+  if (pw && !wait_geq(pw->ana_prev + mby, mbx + 1, pw->error, pw->timeout_ns)) return;
+  MbInfo prevmb = ld_info(&sd.prev_info[c.mb]);
+  if (pw) {
+    // The right- and bottom-most reference sample this macroblock can read: the full-pel
+    // candidates, a diamond of at most 16 steps around the best, the half-sample window
+    // (-3..+20) and 8-byte loads. Everything above and to the left of it (padding included) is
+    // final once the macroblock holding it is.
+    int cx[5] = {mvp0, 0, a0, b0, prevmb.mv[0]}, cy[5] = {mvp1, 0, a1, b1, prevmb.mv[1]};
+    int hi0 = -(1 << 20), hi1 = -(1 << 20);
+    int imn0 = (bmin0 + 3) >> 2, imn1 = (bmin1 + 3) >> 2, imx0 = bmax0 >> 2, imx1 = bmax1 >> 2;
+    for (int k = 0; k < 5; k++) {
+      hi0 = max(hi0, min(max((cx[k] + 2) >> 2, imn0), imx0));
+      hi1 = max(hi1, min(max((cy[k] + 2) >> 2, imn1), imx1));
+    }
+    int xb = (x0 + hi0 + 44) >> 4, rb = (y0 + hi1 + 40) >> 4;
+    int rr = min(max(rb, 0), fp.mb_h - 1), xx = min(max(xb, 0), fp.mb_w - 1);
+    bool ok = rr < fp.mb_h - 1 ? wait_geq(pw->db_prev + rr + 1, xx + 1, pw->error, pw->timeout_ns)
+                               : wait_geq(pw->db_prev + rr, min(xx + 2, fp.mb_w), pw->error, pw->timeout_ns);
+    if (!ok) return;
+  }
 
   // 1. skip probe (enc.rs:2906 try_p_skip)
   if (ps0 >= bmin0 && ps0 <= bmax0 && ps1 >= bmin1 && ps1 <= bmax1) {
@@ -1369,10 +1455,7 @@ __device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
   cand[n][0] = 0; cand[n][1] = 0; n++;
   if (mbx > 0) { cand[n][0] = a0; cand[n][1] = a1; n++; }
   if (mby > 0) { cand[n][0] = b0; cand[n][1] = b1; n++; }
-  {
-    MbInfo pv = sd.prev_info[c.mb];
-    cand[n][0] = pv.mv[0]; cand[n][1] = pv.mv[1]; n++;
-  }
+  cand[n][0] = prevmb.mv[0]; cand[n][1] = prevmb.mv[1]; n++;
   int imin0 = (bmin0 + 3) >> 2, imin1 = (bmin1 + 3) >> 2, imax0 = bmax0 >> 2, imax1 = bmax1 >> 2;
   uint2 sv = src8(sm);
   const uint8_t* base = ref + (long)(y0 + (lane >> 1)) * stride + x0 + (lane & 1) * 8;
@@ -1444,7 +1527,7 @@ __device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
             uint32_t s = 0;
             if (ok) {
               int wx = (cx >> 2) - best0 + 1, wy = (cy >> 2) - best1 + 1;
-              s = vsad8(sv, qpel8(sm, wx, wy, cx & 3, cy & 3));
+              s = vsad8(sv, qpel8(qpel_src(sm, wx, wy, cx & 3, cy & 3)));
             }
             s = wsum(s);
             cc[k] = ok ? s + mvd_cost(cx - mvp0, lambda) + mvd_cost(cy - mvp1, lambda) : UMAX;
@@ -1456,7 +1539,7 @@ __device__ void analyse_p_mb(const Ctx& c, Smem& sm) {
         }
       }
       mv0 = q0; mv1 = q1;
-      uint2 v = qpel8(sm, (q0 >> 2) - best0 + 1, (q1 >> 2) - best1 + 1, q0 & 3, q1 & 3);
+      uint2 v = qpel8(qpel_src(sm, (q0 >> 2) - best0 + 1, (q1 >> 2) - best1 + 1, q0 & 3, q1 & 3));
       *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
       __syncwarp();
     }
@@ -1683,14 +1766,14 @@ __device__ bool edge_bs(const MbInfo& q, const MbInfo* p, int dir, int e, int* b
   return true;
 }
 
-__device__ void deblock_mb(const FrameParams& fp, const StreamDev& sd, int mbx, int mby, Smem& sm) {
+__device__ __noinline__ void deblock_mb(const FrameParams& fp, const StreamDev& sd, int mbx, int mby, Smem& sm) {
   int lane = lane_id();
   int m = mby * fp.mb_w + mbx;
-  MbInfo q = sd.info[m];
+  MbInfo q = ld_info(&sd.info[m]);
   MbInfo lf, tp;
   bool hasl = mbx > 0, hast = mby > 0;
-  if (hasl) lf = sd.info[m - 1];
-  if (hast) tp = sd.info[m - fp.mb_w];
+  if (hasl) lf = ld_info(&sd.info[m - 1]);
+  if (hast) tp = ld_info(&sd.info[m - fp.mb_w]);
   auto quiet = [](const MbInfo& i) { return !(i.flags & kFlagIntra) && i.cbp_luma == 0; };
   if (quiet(q) && (!hasl || (quiet(lf) && lf.mv[0] == q.mv[0] && lf.mv[1] == q.mv[1])) &&
       (!hast || (quiet(tp) && tp.mv[0] == q.mv[0] && tp.mv[1] == q.mv[1])))
@@ -1702,13 +1785,13 @@ __device__ void deblock_mb(const FrameParams& fp, const StreamDev& sd, int mbx, 
   for (int w = lane; w < 100; w += 32) {  // 20 rows x 5 words
     int r = w / 5, k = w % 5;
     if ((r < 4 && !hast) || (k == 0 && !hasl)) continue;
-    *(uint32_t*)&ty[r * 20 + 4 * k] = *(const uint32_t*)(sd.cur_y + (long)(y0 - 4 + r) * fp.stride_y + x0 - 4 + 4 * k);
+    *(uint32_t*)&ty[r * 20 + 4 * k] = ldcg_u32(sd.cur_y + (long)(y0 - 4 + r) * fp.stride_y + x0 - 4 + 4 * k);
   }
   for (int w = lane; w < 72; w += 32) {  // 2 planes x 12 rows x 3 words
     int p = w / 36, rem = w % 36, r = rem / 3, k = rem % 3;
     if ((r < 4 && !hast) || (k == 0 && !hasl)) continue;
     const uint8_t* P = p ? sd.cur_v : sd.cur_u;
-    *(uint32_t*)&tc[p][r * 12 + 4 * k] = *(const uint32_t*)(P + (long)(cy0 - 4 + r) * fp.stride_c + cx0 - 4 + 4 * k);
+    *(uint32_t*)&tc[p][r * 12 + 4 * k] = ldcg_u32(P + (long)(cy0 - 4 + r) * fp.stride_c + cx0 - 4 + 4 * k);
   }
   __syncwarp();
   bool intra = q.flags & kFlagIntra;
@@ -1786,12 +1869,152 @@ __global__ void __launch_bounds__(32) wavefront_step_kernel(FrameParams fp, cons
       load_source(c, sm);
       analyse_intra_mb(c, sm);
     } else {
-      analyse_p_mb(c, sm);
+      analyse_p_mb(c, sm, nullptr);
     }
   } else if (k - na < nd) {
     int d = step - 3;
     int mby = diag_first(fp, d) + (k - na), mbx = d - 2 * mby;
     deblock_mb(fp, sd, mbx, mby, sm);
+  }
+}
+
+// Border extension (enc.rs:165 extend_borders) of the padding that takes its values from
+// macroblock (a, b), once that macroblock is final: the left / right padding of its rows when it
+// is the first / last of its row, and the padding above / below its columns when it is in the
+// first / last row -- corners included, which come from the corner macroblocks. Applied to every
+// macroblock of the picture this writes every padding sample exactly once, so a picture's
+// padding is complete wherever the macroblocks it copies are final. One warp, 4-byte stores.
+__device__ __noinline__ void extend_mb(const FrameParams& fp, const StreamDev& sd, int a, int b) {
+  int lane = lane_id();
+  bool left = a == 0, right = a == fp.mb_w - 1, top = b == 0, bottom = b == fp.mb_h - 1;
+  if (!(left || right || top || bottom)) return;
+  for (int plane = 0; plane < 3; plane++) {
+    uint8_t* P = plane == 0 ? sd.cur_y : (plane == 1 ? sd.cur_u : sd.cur_v);
+    int bw = plane ? 8 : 16;
+    int w = fp.mb_w * bw, h = fp.mb_h * bw;
+    int pad = plane ? kPadC : kPadY, stride = plane ? fp.stride_c : fp.stride_y;
+    int lw = pad / 4;
+    // columns owned by this macroblock, in 4-byte words relative to the padded row start
+    int c_lo = left ? 0 : (pad + a * bw) / 4;
+    int c_hi = right ? stride / 4 : (pad + (a + 1) * bw) / 4;
+    // rows owned: its own rows, plus the padding above / below the picture
+    int r_lo = top ? -pad : b * bw, r_hi = bottom ? h + pad : (b + 1) * bw;
+    int ncol = c_hi - c_lo, n = (r_hi - r_lo) * ncol;
+    for (int i = lane; i < n; i += 32) {
+      int yy = r_lo + i / ncol, cw = c_lo + i % ncol;
+      int xw = cw * 4 - pad;  // first picture column of this word
+      bool in_rows = yy >= 0 && yy < h;
+      if (in_rows && cw >= lw && cw < lw + w / 4) continue;  // picture sample: no copy
+      int sy = min(max(yy, 0), h - 1);
+      const uint8_t* srow = P + (long)sy * stride;
+      uint32_t v;
+      if (xw < 0) v = ldcg_u8(srow) * 0x01010101u;
+      else if (xw >= w) v = ldcg_u8(srow + w - 1) * 0x01010101u;
+      else v = ldcg_u32(srow + xw);
+      *(uint32_t*)(P + (long)yy * stride + xw) = v;
+    }
+  }
+}
+
+// Persistent pipelined mode: F pictures of every stream in one launch. Work is cut into row
+// tasks handed out in ticket order -- per picture, analysis of row y for every stream, then
+// deblocking of row y-1 -- and every wait is for a task of a smaller ticket (the row above,
+// the row below's analysis two macroblocks ahead, the reference picture's final region), so
+// any number of resident warps makes progress. Picture f+1 starts as soon as the part of
+// picture f its search can reach is deblocked and border-extended.
+struct PipeParams {
+  int* ticket;
+  int* error;
+  int* ana;    // [F][S][mb_h] analysed macroblocks per row
+  int* db;     // [F][S][mb_h] deblocked macroblocks per row; a macroblock's deblocking also
+               // extends the padding of the macroblocks it makes final
+  const int* t_off;  // first ticket of each row-time T (T = tau + skew * f), n_times + 1 entries
+  int n_times;
+  int skew;    // row-times between the starts of consecutive pictures of a stream
+  int frames;
+  int n_tickets;
+  unsigned long long timeout_ns;
+};
+
+__global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
+  __shared__ Smem sm;
+  const int lane = lane_id();
+  const int S = fp.n_streams, H = fp.mb_h, Wm = fp.mb_w;
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(pp.ticket, 1);
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= pp.n_tickets) break;
+    if (__shfl_sync(FULL, lane == 0 ? ld_acquire(pp.error) : 0, 0)) break;
+    // Ticket -> (row-time T, picture f, role, row, stream). At picture-local row-time tau a
+    // picture has the analysis of row tau (tau < H) then the deblocking of row tau - 1 (tau >= 1);
+    // pictures of one T in increasing order, streams innermost.
+    int lo = 0, hi = pp.n_times;  // largest T with t_off[T] <= t
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (pp.t_off[mid] <= t) lo = mid; else hi = mid;
+    }
+    int T = lo, rem = t - pp.t_off[T];
+    // pictures open at T: tau = T - skew * f in [0, H], oldest (largest tau) first
+    int f = T - H > 0 ? (T - H + pp.skew - 1) / pp.skew : 0;
+    int tau = 0, na = 0, nd = 0;
+    for (;; f++) {
+      tau = T - pp.skew * f;
+      na = tau < H ? 1 : 0;
+      nd = tau >= 1 ? 1 : 0;
+      int cnt = S * (na + nd);
+      if (rem < cnt) break;
+      rem -= cnt;
+    }
+    bool ana = rem < S * na;
+    int s = ana ? rem : rem - S * na;
+    int y = ana ? tau : tau - 1;
+    const StreamDev& sd = sds[f * S + s];
+    int* ana_rows = pp.ana + (f * S + s) * H;
+    int* db_rows = pp.db + (f * S + s) * H;
+    bool failed = false;
+    if (ana) {
+      PipeWait pw;
+      bool has_prev = f > 0 && sd.kind == RG_FRAME_P;
+      if (has_prev) {
+        pw.ana_prev = pp.ana + ((f - 1) * S + s) * H;
+        pw.db_prev = pp.db + ((f - 1) * S + s) * H;
+      }
+      pw.error = pp.error;
+      pw.timeout_ns = pp.timeout_ns;
+      for (int x = 0; x < Wm && !failed; x++) {
+        if (y > 0 && !wait_geq(ana_rows + y - 1, min(x + 2, Wm), pp.error, pp.timeout_ns)) { failed = true; break; }
+        Ctx c{&fp, &sd, x, y, y * Wm + x};
+        if (sd.kind == RG_FRAME_IDR) {
+          load_source(c, sm);
+          analyse_intra_mb(c, sm);
+        } else {
+          analyse_p_mb(c, sm, has_prev ? &pw : nullptr);
+          if (__shfl_sync(FULL, lane == 0 ? ld_acquire(pp.error) : 0, 0)) { failed = true; break; }
+        }
+        publish(ana_rows + y, x + 1);
+      }
+    } else {
+      for (int x = 0; x < Wm; x++) {
+        if (!wait_geq(ana_rows + y, min(x + 2, Wm), pp.error, pp.timeout_ns) ||
+            (y + 1 < H && !wait_geq(ana_rows + y + 1, min(x + 1, Wm), pp.error, pp.timeout_ns)) ||
+            (y > 0 && !wait_geq(db_rows + y - 1, min(x + 2, Wm), pp.error, pp.timeout_ns))) {
+          failed = true;
+          break;
+        }
+        deblock_mb(fp, sd, x, y, sm);
+        // Macroblock (x, y - 1) is final now: (x + 1, y - 1) was deblocked before this one. In
+        // the last row, so is (x - 1, y), and the last macroblock is final after its own pass.
+        __syncwarp();
+        if (y >= 1) extend_mb(fp, sd, x, y - 1);
+        if (y == H - 1) {
+          if (x >= 1) extend_mb(fp, sd, x - 1, y);
+          if (x == Wm - 1) extend_mb(fp, sd, x, y);
+        }
+        publish(db_rows + y, x + 1);
+      }
+    }
+    if (failed) break;
   }
 }
 
@@ -1862,6 +2085,53 @@ static int max_diag_len(const FrameParams& fp) {
 void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st) {
   dim3 grid(2 * max_diag_len(fp), fp.n_streams);
   wavefront_step_kernel<<<grid, 32, 0, st>>>(fp, d_streams, step);
+}
+
+int pipeline_grid(int device) {
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel, 32, 0);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return per_sm * sms;
+}
+
+// Ticket table of the skewed order: t_off[T] = first ticket of row-time T (host-built, n_times + 1
+// ints written to `table`). Returns the number of row-times.
+int pipeline_ticket_table(const FrameParams& fp, int frames, int skew, int* table) {
+  int S = fp.n_streams, H = fp.mb_h;
+  int n_times = H + 1 + skew * (frames - 1);
+  int acc = 0;
+  for (int T = 0; T < n_times; T++) {
+    table[T] = acc;
+    for (int f = 0; f < frames; f++) {
+      int tau = T - skew * f;
+      if (tau < 0 || tau > H) continue;
+      acc += S * ((tau < H ? 1 : 0) + (tau >= 1 ? 1 : 0));
+    }
+  }
+  table[n_times] = acc;
+  return n_times;
+}
+
+void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int* d_table,
+                     int n_times, int skew, int grid, unsigned long long timeout_ns, cudaStream_t st) {
+  int S = fp.n_streams, H = fp.mb_h;
+  PipeParams pp;
+  pp.ticket = counters;
+  pp.error = counters + 1;
+  pp.ana = counters + 4;
+  pp.db = pp.ana + frames * S * H;
+  pp.t_off = d_table;
+  pp.n_times = n_times;
+  pp.skew = skew;
+  pp.frames = frames;
+  pp.n_tickets = frames * 2 * H * S;
+  pp.timeout_ns = timeout_ns;
+  int g = grid < pp.n_tickets ? grid : pp.n_tickets;
+  pipeline_kernel<<<g, 32, 0, st>>>(fp, d_streams, pp);
+}
+
+size_t pipeline_counter_ints(const FrameParams& fp, int frames) {
+  return 4 + 2 * (size_t)frames * fp.n_streams * fp.mb_h;
 }
 
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st) {

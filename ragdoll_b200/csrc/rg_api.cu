@@ -100,10 +100,25 @@ struct rg_ctx {
   uint8_t* srcs = nullptr;         // [S][Y U V] compact display-size staging
   uint8_t* unf = nullptr;          // [S][Y U V] coded-size copies before deblocking
   bool keep_unfiltered = false;
-  StreamDev* d_streams[2] = {nullptr, nullptr};
+  StreamDev* d_streams[2] = {nullptr, nullptr};  // [max_frames][S] descriptors each
   StreamDev* h_streams[2] = {nullptr, nullptr};  // pinned
   cudaEvent_t slot_done[2] = {nullptr, nullptr};
   int slot = 0;
+  int max_frames = 1, nslots = 2;  // pictures per pipelined call; picture ring per stream
+  int* counters = nullptr;         // pipelined-mode progress counters
+  size_t n_counters = 0;
+  int* h_err = nullptr;            // pinned copy of the device error word
+  int grid = 0;
+  int skew = 10;                   // row-times between pictures of a stream in the pipelined order
+  unsigned long long timeout_ns = 2000000000ull;  // limit of one device wait
+  int* d_table = nullptr;          // ticket table of the pipelined order
+  int* h_table = nullptr;          // pinned
+  // the pending pipelined call, kept to re-run it on the per-diagonal path after a failed wait
+  std::vector<const uint8_t*> pend_planes;
+  std::vector<int32_t> pend_kinds;
+  std::vector<int> pend_start;
+  int pend_frames = 0;
+  size_t pend_sy = 0, pend_suv = 0;
   std::vector<int> frames;         // frames analysed per stream
   // metrics scratch
   float* m_rows = nullptr;
@@ -114,9 +129,9 @@ struct rg_ctx {
   DecimateJob* m_djobs = nullptr;
   uint8_t* m_src = nullptr;
 
-  uint8_t* pic_plane(int s, int parity, int plane) const {
+  uint8_t* pic_plane(int s, int slot_, int plane) const {
     size_t per_pic = pic_y + 2 * pic_c;
-    uint8_t* base = pics + ((size_t)s * 2 + parity) * per_pic;
+    uint8_t* base = pics + ((size_t)s * nslots + slot_) * per_pic;
     if (plane == 0) return base + (size_t)kPadY * fp.stride_y + kPadY;
     return base + pic_y + (plane - 1) * pic_c + (size_t)kPadC * fp.stride_c + kPadC;
   }
@@ -179,25 +194,37 @@ rg_ctx* rg_create(const rg_config* cfg) {
   c->pic_y = (size_t)fp.stride_y * c->rows_y;
   c->pic_c = (size_t)fp.stride_c * c->rows_c;
   c->frames.assign(c->S, 0);
+  c->max_frames = cfg->max_frames > 1 ? cfg->max_frames : 1;
+  if (c->max_frames > 64) {
+    fail(RG_ERR_INVALID, "rg_create: max_frames %d outside 0..64", cfg->max_frames);
+    delete c;
+    return nullptr;
+  }
+  c->nslots = c->max_frames + 1;
+  c->n_counters = pipeline_counter_ints(fp, c->max_frames);
   bool ok = true;
   auto alloc = [&](void** p, size_t n) {
     if (!ok) return;
     if (cudaMalloc(p, n) != cudaSuccess) { ok = false; return; }
     cudaMemset(*p, 0, n);
   };
-  alloc((void**)&c->pics, (c->pic_y + 2 * c->pic_c) * 2 * c->S);
-  alloc((void**)&c->infos, sizeof(MbInfo) * c->n_mb * 2 * c->S);
-  alloc((void**)&c->recs, sizeof(rg_mb_out) * c->n_mb * c->S);
-  alloc((void**)&c->srcs, c->src_bytes() * c->S);
-  alloc((void**)&c->d_streams[0], sizeof(StreamDev) * c->S);
-  alloc((void**)&c->d_streams[1], sizeof(StreamDev) * c->S);
+  alloc((void**)&c->pics, (c->pic_y + 2 * c->pic_c) * c->nslots * c->S);
+  alloc((void**)&c->infos, sizeof(MbInfo) * c->n_mb * c->nslots * c->S);
+  alloc((void**)&c->recs, sizeof(rg_mb_out) * c->n_mb * c->S * c->max_frames);
+  alloc((void**)&c->srcs, c->src_bytes() * c->S * c->max_frames);
+  alloc((void**)&c->d_streams[0], sizeof(StreamDev) * c->S * c->max_frames);
+  alloc((void**)&c->d_streams[1], sizeof(StreamDev) * c->S * c->max_frames);
+  alloc((void**)&c->counters, sizeof(int) * c->n_counters);
+  alloc((void**)&c->d_table, sizeof(int) * (fp.mb_h + 4 + (size_t)c->skew * c->max_frames));
   if (!ok) {
     fail(RG_ERR_OOM, "rg_create: device allocation failed");
     rg_destroy(c);
     return nullptr;
   }
-  if (cudaMallocHost((void**)&c->h_streams[0], sizeof(StreamDev) * c->S) != cudaSuccess ||
-      cudaMallocHost((void**)&c->h_streams[1], sizeof(StreamDev) * c->S) != cudaSuccess ||
+  if (cudaMallocHost((void**)&c->h_streams[0], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
+      cudaMallocHost((void**)&c->h_streams[1], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
+      cudaMallocHost((void**)&c->h_err, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void**)&c->h_table, sizeof(int) * (fp.mb_h + 4 + (size_t)c->skew * c->max_frames)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->slot_done[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->slot_done[1], cudaEventDisableTiming) != cudaSuccess) {
@@ -205,6 +232,8 @@ rg_ctx* rg_create(const rg_config* cfg) {
     rg_destroy(c);
     return nullptr;
   }
+  *c->h_err = 0;
+  c->grid = pipeline_grid(cfg->device);
   upload_tables();
   if (cudaDeviceSynchronize() != cudaSuccess) {
     fail(RG_ERR_CUDA, "rg_create: %s", cudaGetErrorString(cudaGetLastError()));
@@ -231,6 +260,10 @@ void rg_destroy(rg_ctx* c) {
   cudaFree(c->m_jobs);
   cudaFree(c->m_djobs);
   cudaFree(c->m_src);
+  cudaFree(c->counters);
+  cudaFree(c->d_table);
+  if (c->h_err) cudaFreeHost(c->h_err);
+  if (c->h_table) cudaFreeHost(c->h_table);
   if (c->h_streams[0]) cudaFreeHost(c->h_streams[0]);
   if (c->h_streams[1]) cudaFreeHost(c->h_streams[1]);
   for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
@@ -258,8 +291,18 @@ int rg_keep_unfiltered(rg_ctx* c, int32_t enable) {
 
 void* rg_cuda_stream(rg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
+static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
+                             const int32_t* kinds, rg_mb_out* rec_base);
+
 int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                             const int32_t* kinds) {
+  return enqueue_wavefront(c, dev_planes, stride_y, stride_uv, kinds, nullptr);
+}
+
+// One picture of every stream, one launch per anti-diagonal step; records at rec_base
+// (default: the first picture's records).
+static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
+                             const int32_t* kinds, rg_mb_out* rec_base) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_batch_device: null argument");
   if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
     return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stride too small");
@@ -277,7 +320,7 @@ int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t 
   StreamDev* h = c->h_streams[slot];
   size_t unf = c->unf_bytes();
   for (int s = 0; s < c->S; s++) {
-    int par = c->frames[s] & 1;
+    int par = c->frames[s] % c->nslots, prv = (c->frames[s] + c->nslots - 1) % c->nslots;
     StreamDev& d = h[s];
     d.src_y = dev_planes[3 * s];
     d.src_u = dev_planes[3 * s + 1];
@@ -285,12 +328,12 @@ int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t 
     d.cur_y = c->pic_plane(s, par, 0);
     d.cur_u = c->pic_plane(s, par, 1);
     d.cur_v = c->pic_plane(s, par, 2);
-    d.ref_y = c->pic_plane(s, par ^ 1, 0);
-    d.ref_u = c->pic_plane(s, par ^ 1, 1);
-    d.ref_v = c->pic_plane(s, par ^ 1, 2);
-    d.info = c->infos + ((size_t)s * 2 + par) * c->n_mb;
-    d.prev_info = c->infos + ((size_t)s * 2 + (par ^ 1)) * c->n_mb;
-    d.rec = c->recs + (size_t)s * c->n_mb;
+    d.ref_y = c->pic_plane(s, prv, 0);
+    d.ref_u = c->pic_plane(s, prv, 1);
+    d.ref_v = c->pic_plane(s, prv, 2);
+    d.info = c->infos + ((size_t)s * c->nslots + par) * c->n_mb;
+    d.prev_info = c->infos + ((size_t)s * c->nslots + prv) * c->n_mb;
+    d.rec = (rec_base ? rec_base : c->recs) + (size_t)s * c->n_mb;
     if (c->keep_unfiltered) {
       uint8_t* u = c->unf + unf * s;
       d.unf_y = u;
@@ -315,14 +358,153 @@ int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t 
   return RG_OK;
 }
 
+int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
+                           const int32_t* kinds, int32_t frames) {
+  if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null argument");
+  if (frames < 1 || frames > c->max_frames)
+    return fail(RG_ERR_INVALID, "rg_analyse_gops_device: frames %d outside 1..%d (rg_config.max_frames)", frames,
+                c->max_frames);
+  if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
+    return fail(RG_ERR_INVALID, "rg_analyse_gops_device: stride too small");
+  int S = c->S;
+  for (int f = 0; f < frames; f++)
+    for (int s = 0; s < S; s++) {
+      int k = kinds[f * S + s];
+      if (k != RG_FRAME_IDR && k != RG_FRAME_P)
+        return fail(RG_ERR_INVALID, "rg_analyse_gops_device: picture %d stream %d kind %d", f, s, k);
+      if (k == RG_FRAME_P && f == 0 && c->frames[s] == 0)
+        return fail(RG_ERR_STATE, "rg_analyse_gops_device: stream %d starts with a P picture without a reference", s);
+      for (int p = 0; p < 3; p++)
+        if (!dev_planes[(f * S + s) * 3 + p])
+          return fail(RG_ERR_INVALID, "rg_analyse_gops_device: picture %d stream %d null plane", f, s);
+    }
+  int slot = c->slot;
+  c->slot ^= 1;
+  CK(cudaEventSynchronize(c->slot_done[slot]));
+  StreamDev* h = c->h_streams[slot];
+  for (int f = 0; f < frames; f++)
+    for (int s = 0; s < S; s++) {
+      int g = c->frames[s] + f;
+      int cur = g % c->nslots, prv = (g + c->nslots - 1) % c->nslots;
+      StreamDev& d = h[f * S + s];
+      d.src_y = dev_planes[(f * S + s) * 3];
+      d.src_u = dev_planes[(f * S + s) * 3 + 1];
+      d.src_v = dev_planes[(f * S + s) * 3 + 2];
+      d.cur_y = c->pic_plane(s, cur, 0);
+      d.cur_u = c->pic_plane(s, cur, 1);
+      d.cur_v = c->pic_plane(s, cur, 2);
+      d.ref_y = c->pic_plane(s, prv, 0);
+      d.ref_u = c->pic_plane(s, prv, 1);
+      d.ref_v = c->pic_plane(s, prv, 2);
+      d.info = c->infos + ((size_t)s * c->nslots + cur) * c->n_mb;
+      d.prev_info = c->infos + ((size_t)s * c->nslots + prv) * c->n_mb;
+      d.rec = c->recs + ((size_t)f * S + s) * c->n_mb;
+      d.unf_y = d.unf_u = d.unf_v = nullptr;
+      d.kind = kinds[f * S + s];
+      d.pad_ = 0;
+    }
+  FrameParams fp = c->fp;
+  fp.src_stride_y = (int)stride_y;
+  fp.src_stride_uv = (int)stride_uv;
+  CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * S * frames, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(c->slot_done[slot], c->stream));
+  CK(cudaMemsetAsync(c->counters, 0, sizeof(int) * pipeline_counter_ints(c->fp, frames), c->stream));
+  CK(cudaStreamSynchronize(c->stream));  // the pinned ticket table is rewritten below
+  int n_times = pipeline_ticket_table(fp, frames, c->skew, c->h_table);
+  CK(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(int) * (n_times + 1), cudaMemcpyHostToDevice, c->stream));
+  // a generous bound on any single wait: a whole picture of the batch takes far less
+  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_table, n_times, c->skew, c->grid, c->timeout_ns,
+                  c->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->h_err, c->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  c->pend_planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
+  c->pend_kinds.assign(kinds, kinds + (size_t)frames * S);
+  c->pend_start = c->frames;
+  c->pend_frames = frames;
+  c->pend_sy = stride_y;
+  c->pend_suv = stride_uv;
+  for (int s = 0; s < S; s++) c->frames[s] += frames;
+  return RG_OK;
+}
+
+int rg_copy_records_gops(rg_ctx* c, int32_t frames, rg_mb_out* out) {
+  if (!c || !out) return fail(RG_ERR_INVALID, "rg_copy_records_gops: null argument");
+  if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "rg_copy_records_gops: frames %d", frames);
+  int r = rg_sync(c);  // completes (or re-runs) the pending call first
+  if (r) return r;
+  CK(cudaMemcpyAsync(out, c->recs, sizeof(rg_mb_out) * c->n_mb * c->S * frames, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
+}
+
+int rg_set_pipeline_tuning(rg_ctx* c, int32_t skew, int32_t grid, int32_t timeout_ms) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: null context");
+  if (skew < 0 || skew > 10) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: skew %d outside 0..10", skew);
+  if (grid < 0 || timeout_ms < 0) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: negative argument");
+  CK(cudaStreamSynchronize(c->stream));
+  c->skew = skew > 0 ? skew : 1;
+  if (skew == 0) c->skew = 1;
+  if (grid > 0) c->grid = grid;
+  else c->grid = pipeline_grid(c->cfg.device);
+  c->timeout_ns = timeout_ms > 0 ? (unsigned long long)timeout_ms * 1000000ull : 2000000000ull;
+  return RG_OK;
+}
+
+int rg_analyse_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
+                    int32_t frames, rg_mb_out* out) {
+  if (!c || !planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops: null argument");
+  if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "rg_analyse_gops: frames %d", frames);
+  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "rg_analyse_gops: stride too small");
+  int S = c->S;
+  std::vector<const uint8_t*> dev(3 * (size_t)S * frames);
+  for (int f = 0; f < frames; f++)
+    for (int s = 0; s < S; s++) {
+      const uint8_t* const* pl = planes + (f * S + s) * 3;
+      if (!pl[0] || !pl[1] || !pl[2]) return fail(RG_ERR_INVALID, "rg_analyse_gops: picture %d stream %d null plane", f, s);
+      uint8_t* d = c->srcs + c->src_bytes() * ((size_t)f * S + s);
+      CK(cudaMemcpy2DAsync(d, w, pl[0], stride_y, w, h, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpy2DAsync(d + (size_t)w * h, cw, pl[1], stride_uv, cw, ch, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpy2DAsync(d + (size_t)w * h + (size_t)cw * ch, cw, pl[2], stride_uv, cw, ch, cudaMemcpyHostToDevice,
+                           c->stream));
+      dev[(f * S + s) * 3] = d;
+      dev[(f * S + s) * 3 + 1] = d + (size_t)w * h;
+      dev[(f * S + s) * 3 + 2] = d + (size_t)w * h + (size_t)cw * ch;
+    }
+  int r = rg_analyse_gops_device(c, dev.data(), w, cw, kinds, frames);
+  if (r) return r;
+  if (out) return rg_copy_records_gops(c, frames, out);
+  return rg_sync(c);
+}
+
 int rg_sync(rg_ctx* c) {
   if (!c) return fail(RG_ERR_INVALID, "rg_sync: null context");
   CK(cudaStreamSynchronize(c->stream));
+  if (*c->h_err) {
+    // A wait of the pipelined launch gave up (a search reaching further than the picture skew
+    // allows, or a fault of another warp). Every picture of the call wrote its own ring slot and
+    // the reference it started from is untouched, so the call is re-run, picture by picture, on
+    // the per-diagonal path, which has no waits. Results are identical.
+    *c->h_err = 0;
+    if (c->pend_frames == 0) return fail(RG_ERR_TIMEOUT, "rg_sync: a device wait gave up");
+    int S = c->S, F = c->pend_frames;
+    c->frames = c->pend_start;
+    c->pend_frames = 0;
+    for (int f = 0; f < F; f++) {
+      int r = enqueue_wavefront(c, c->pend_planes.data() + (size_t)f * S * 3, c->pend_sy, c->pend_suv,
+                                c->pend_kinds.data() + (size_t)f * S, c->recs + (size_t)f * S * c->n_mb);
+      if (r) return r;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->pend_frames = 0;
   return RG_OK;
 }
 
 int rg_copy_records(rg_ctx* c, rg_mb_out* out) {
   if (!c || !out) return fail(RG_ERR_INVALID, "rg_copy_records: null argument");
+  int r0 = rg_sync(c);
+  if (r0) return r0;
   CK(cudaMemcpyAsync(out, c->recs, sizeof(rg_mb_out) * c->n_mb * c->S, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return RG_OK;
@@ -372,7 +554,7 @@ int rg_get_recon(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v, size_
   if (!c || !y || !u || !v) return fail(RG_ERR_INVALID, "rg_get_recon: null argument");
   if (s < 0 || s >= c->S) return fail(RG_ERR_INVALID, "rg_get_recon: stream %d", s);
   if (c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_get_recon: stream %d has no frame", s);
-  int par = (c->frames[s] - 1) & 1;
+  int par = (c->frames[s] - 1) % c->nslots;
   int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
   CK(cudaMemcpy2DAsync(y, sy, c->pic_plane(s, par, 0), c->fp.stride_y, w, h, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpy2DAsync(u, suv, c->pic_plane(s, par, 1), c->fp.stride_c, cw, ch, cudaMemcpyDeviceToHost, c->stream));
@@ -385,7 +567,7 @@ int rg_get_recon(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v, size_
 int rg_get_recon_coded(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v) {
   if (!c || !y || !u || !v) return fail(RG_ERR_INVALID, "rg_get_recon_coded: null argument");
   if (s < 0 || s >= c->S || c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_get_recon_coded: stream %d", s);
-  int par = (c->frames[s] - 1) & 1;
+  int par = (c->frames[s] - 1) % c->nslots;
   int w = c->fp.mb_w * 16, h = c->fp.mb_h * 16;
   CK(cudaMemcpy2DAsync(y, w, c->pic_plane(s, par, 0), c->fp.stride_y, w, h, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpy2DAsync(u, w / 2, c->pic_plane(s, par, 1), c->fp.stride_c, w / 2, h / 2, cudaMemcpyDeviceToHost, c->stream));
@@ -561,7 +743,7 @@ int rg_quality_frame(rg_ctx* c, int32_t s, const uint8_t* y, const uint8_t* u, c
   CK(cudaMemcpy2DAsync(c->m_src, w, y, sy, w, h, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpy2DAsync(c->m_src + (size_t)w * h, cw, u, suv, cw, ch, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpy2DAsync(c->m_src + (size_t)w * h + (size_t)cw * ch, cw, v, suv, cw, ch, cudaMemcpyHostToDevice, c->stream));
-  int par = (c->frames[s] - 1) & 1;
+  int par = (c->frames[s] - 1) % c->nslots;
   std::vector<PlanePair> pairs = {
       {c->m_src, w, c->pic_plane(s, par, 0), c->fp.stride_y, w, h},
       {c->m_src + (size_t)w * h, cw, c->pic_plane(s, par, 1), c->fp.stride_c, cw, ch},

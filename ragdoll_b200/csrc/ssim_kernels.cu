@@ -49,7 +49,6 @@ __global__ void ssim_rows_kernel(const SsimJob* __restrict__ jobs) {
     int s1 = 0, s2 = 0, ss = 0, s12 = 0;
 #pragma unroll
     for (int dy = 0; dy < 4; dy++) {
-      uint32_t a = 0, b = 0;
       const uint8_t* pa = j.a + (long)(y + dy) * j.stride_a + x;
       const uint8_t* pb = j.b + (long)(y + dy) * j.stride_b + x;
 #pragma unroll
@@ -57,7 +56,6 @@ __global__ void ssim_rows_kernel(const SsimJob* __restrict__ jobs) {
         int va = pa[k], vb = pb[k];
         s1 += va; s2 += vb; ss += va * va + vb * vb; s12 += va * vb;
       }
-      (void)a; (void)b;
     }
     int* o = sums + (size_t)i * 4;
     o[0] = s1; o[1] = s2; o[2] = ss; o[3] = s12;

@@ -37,7 +37,8 @@ EXPORTS = [
     "rg_last_error", "rg_version", "rg_create", "rg_destroy", "rg_mb_dims", "rg_analyse_frame",
     "rg_analyse_batch", "rg_analyse_batch_device", "rg_sync", "rg_copy_records", "rg_get_recon",
     "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
-    "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc",
+    "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc", "rg_analyse_gops",
+    "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning",
 ]
 
 
@@ -51,7 +52,8 @@ class RgError(RuntimeError):
 
 class RgConfig(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("profile", ctypes.c_int32),
-                ("qp", ctypes.c_int32), ("num_streams", ctypes.c_int32), ("device", ctypes.c_int32)]
+                ("qp", ctypes.c_int32), ("num_streams", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("max_frames", ctypes.c_int32)]
 
 
 class RgQuality(ctypes.Structure):
@@ -96,6 +98,10 @@ def lib() -> ctypes.CDLL:
     L.rg_ssim_plane.argtypes = [ctypes.c_int32, u8p, ctypes.c_size_t, u8p, ctypes.c_size_t,
                                 ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(ctypes.c_double)]
+    L.rg_analyse_gops.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
+    L.rg_analyse_gops_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32]
+    L.rg_copy_records_gops.argtypes = [P, ctypes.c_int32, P]
+    L.rg_set_pipeline_tuning.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
     _lib = L
@@ -115,10 +121,11 @@ class Engine:
     """One ``rg_ctx``: ``num_streams`` streams of one size, profile and fixed QP."""
 
     def __init__(self, width: int, height: int, qp: int, profile: int = RG_PROFILE_BASELINE,
-                 num_streams: int = 1, device: int = 0):
+                 num_streams: int = 1, device: int = 0, max_frames: int = 1):
         self.width, self.height, self.qp, self.profile = width, height, qp, profile
         self.num_streams = num_streams
-        cfg = RgConfig(width, height, profile, qp, num_streams, device)
+        self.max_frames = max(1, max_frames)
+        cfg = RgConfig(width, height, profile, qp, num_streams, device, max_frames)
         h = lib().rg_create(ctypes.byref(cfg))
         if not h:
             raise RgError(-1, lib().rg_last_error().decode())
@@ -167,6 +174,41 @@ class Engine:
         planes = (ctypes.c_void_p * (3 * self.num_streams))(*dev_planes)
         k = (ctypes.c_int32 * self.num_streams)(*kinds)
         _check(lib().rg_analyse_batch_device(self.h, planes, stride_y, stride_uv, k))
+
+    def analyse_gops(self, frames, kinds) -> np.ndarray:
+        """Pipelined form: ``frames[f][s]`` is picture f of stream s (host planes), ``kinds[f][s]``
+        its kind; all pictures in one persistent launch. Returns records ``[F, S, n_mb]``."""
+        F, S = len(frames), self.num_streams
+        planes = (ctypes.c_void_p * (3 * S * F))()
+        keep = []
+        sy = suv = None
+        for f in range(F):
+            assert len(frames[f]) == S
+            for s, (y, u, v) in enumerate(frames[f]):
+                y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (y, u, v))
+                keep += [y, u, v]
+                if sy is None:
+                    sy, suv = y.strides[0], u.strides[0]
+                i = (f * S + s) * 3
+                planes[i], planes[i + 1], planes[i + 2] = y.ctypes.data, u.ctypes.data, v.ctypes.data
+        k = (ctypes.c_int32 * (S * F))(*[kinds[f][s] for f in range(F) for s in range(S)])
+        out = np.zeros((F, S, self.n_mb), RECORD_DTYPE)
+        _check(lib().rg_analyse_gops(self.h, planes, sy, suv, k, F, out.ctypes.data))
+        return out
+
+    def analyse_gops_device(self, dev_planes, stride_y: int, stride_uv: int, kinds, frames: int) -> None:
+        """Queues ``frames`` pictures of every stream from device planes ([f][s][y,u,v])."""
+        planes = (ctypes.c_void_p * len(dev_planes))(*dev_planes)
+        k = (ctypes.c_int32 * len(kinds))(*kinds)
+        _check(lib().rg_analyse_gops_device(self.h, planes, stride_y, stride_uv, k, frames))
+
+    def set_pipeline_tuning(self, skew: int = 10, grid: int = 0, timeout_ms: int = 0) -> None:
+        _check(lib().rg_set_pipeline_tuning(self.h, skew, grid, timeout_ms))
+
+    def records_gops(self, frames: int) -> np.ndarray:
+        out = np.zeros((frames, self.num_streams, self.n_mb), RECORD_DTYPE)
+        _check(lib().rg_copy_records_gops(self.h, frames, out.ctypes.data))
+        return out
 
     def sync(self) -> None:
         _check(lib().rg_sync(self.h))

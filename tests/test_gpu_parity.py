@@ -59,3 +59,56 @@ def test_batched_streams_match_single():
             rs = solo[s].analyse([clips[s][f]], [kind])[0]
             assert rb[s].tobytes() == rs.tobytes()
             assert all(np.array_equal(a, b) for a, b in zip(batch.recon(s), solo[s].recon()))
+
+
+@pytest.mark.parametrize("w,h,qp,profile,streams,frames", [
+    (176, 144, 26, 2, 3, 5),
+    (250, 138, 30, 0, 2, 4),
+    (64, 32, 22, 1, 4, 6),
+])
+def test_pipelined_gops_match_oracle(w, h, qp, profile, streams, frames):
+    """One persistent launch for all pictures of several GOPs (pictures of a GOP overlapping)
+    gives the oracle's records and deblocked reconstruction for every picture."""
+    from oracle_lib import OracleEncoder
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
+    from gpu_parity_util import first_record_mismatch, first_pixel_mismatch
+
+    clips = [grating_clip(w, h, frames, seed=100 + 7 * s + w, motion=6.0, rects=2) for s in range(streams)]
+    eng = Engine(w, h, qp, profile=profile, num_streams=streams, max_frames=frames)
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * streams for f in range(frames)]
+    recs = eng.analyse_gops([[clips[s][f] for s in range(streams)] for f in range(frames)], kinds)
+    for s in range(streams):
+        orc = OracleEncoder(w, h, qp, profile=profile, keyint=frames + 1)
+        for f in range(frames):
+            _, ref = orc.encode(clips[s][f])
+            m = first_record_mismatch(ref, recs[f, s], orc.mb_w)
+            assert m is None, f"stream {s} picture {f}: {m}"
+        # the last picture's reference (deblocked, coded size) stays on the device
+        for p, (a, b) in enumerate(zip(orc.recon(True), eng.recon_coded(s))):
+            assert first_pixel_mismatch(a, b) is None, f"stream {s} plane {p}"
+    # a second call continues the streams with P pictures from the kept references
+    more = [grating_clip(w, h, 2, seed=900 + s, motion=3.0, rects=1) for s in range(streams)]
+    eng.analyse_gops([[more[s][f] for s in range(streams)] for f in range(2)], [[RG_FRAME_P] * streams] * 2)
+
+
+def test_pipelined_wait_timeout_falls_back_to_exact_path():
+    """Failure detection without a GPU fault: one resident warp and no skew make a picture's
+    first row wait for rows of the previous picture that no warp will ever take (a flag nothing
+    sets). The wait gives up after 300 ms, the launch stops with an error status the host reads,
+    and the call is re-run on the per-diagonal path: results stay exact, the context usable."""
+    from oracle_lib import OracleEncoder
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
+    from gpu_parity_util import first_record_mismatch
+
+    w, h, qp, frames = 96, 96, 28, 3
+    clip = grating_clip(w, h, frames, seed=77, motion=4.0, rects=1)
+    eng = Engine(w, h, qp, profile=2, num_streams=1, max_frames=frames)
+    eng.set_pipeline_tuning(skew=1, grid=1, timeout_ms=300)
+    recs = eng.analyse_gops([[clip[f]] for f in range(frames)], [[RG_FRAME_IDR]] + [[RG_FRAME_P]] * (frames - 1))
+    orc = OracleEncoder(w, h, qp, profile=2, keyint=frames + 1)
+    for f in range(frames):
+        _, ref = orc.encode(clip[f])
+        assert first_record_mismatch(ref, recs[f, 0], orc.mb_w) is None
+    eng.set_pipeline_tuning()
+    more = grating_clip(w, h, 2, seed=78, motion=4.0, rects=1)
+    eng.analyse_gops([[more[0]], [more[1]]], [[RG_FRAME_P], [RG_FRAME_P]])
