@@ -184,8 +184,7 @@ def run_engine(args, rank, world, local):
         return [p, p + W * H, p + W * H + cw * ch]
 
     eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
-    if args.skew is not None:
-        eng.set_pipeline_tuning(skew=args.skew)
+    eng.set_pipeline_tuning(lag=args.lag, seg=args.seg)
     stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
     torch.cuda.synchronize()
     gop_ptrs, gop_kinds = [], []
@@ -334,8 +333,7 @@ def run_profile_case(args, local):
     if args.profile_case == "pipelined":
         nf = 3
         eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=nf)
-        if args.skew is not None:
-            eng.set_pipeline_tuning(skew=args.skew)
+        eng.set_pipeline_tuning(lag=args.lag, seg=args.seg)
         stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
         ptrs, kinds = [], []
         for f in range(nf):
@@ -393,8 +391,10 @@ def main():
     ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
                     choices=["wavefront", "pipelined"],
                     help="a small slice of the workload (the ncu capture case)")
-    ap.add_argument("--skew", type=int, default=None,
-                    help="pipelined mode: row-times between the starts of consecutive pictures")
+    ap.add_argument("--lag", type=int, default=0,
+                    help="pipelined mode: macroblock-times between consecutive pictures in the work order (0 = default)")
+    ap.add_argument("--seg", type=int, default=0,
+                    help="pipelined mode: macroblocks per work segment (0 = default)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.profile_case:

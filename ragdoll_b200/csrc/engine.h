@@ -75,9 +75,12 @@ int wavefront_steps(const FrameParams& fp);
 // pipeline_counter_ints() zeroed ints; counters[1] is non-zero after a failed wait.
 int pipeline_grid(int device);
 size_t pipeline_counter_ints(const FrameParams& fp, int frames);
-int pipeline_ticket_table(const FrameParams& fp, int frames, int skew, int* table);
-void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int* d_table,
-                     int n_times, int skew, int grid, unsigned long long timeout_ns, cudaStream_t st);
+// Work list: every analysis / deblocking segment of `seg` macroblocks, in expected-ready order
+// with `lag` macroblock-times between consecutive pictures of a stream.
+size_t pipeline_task_count(const FrameParams& fp, int frames, int seg);
+size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, int2* tasks);
+void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
+                     size_t n_tasks, int seg, int grid, unsigned long long timeout_ns, cudaStream_t st);
 void upload_tables();
 
 }  // namespace rg

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "engine.h"
 #include "h264_consts.h"
@@ -69,9 +70,8 @@ struct __align__(16) Smem {
   uint8_t ctop[2][8];
   uint8_t cleft[2][8];
   uint8_t i4m[16];          // Intra4x4PredMode of this macroblock (decoding order)
-  uint8_t i4pred[16];
-  int16_t i4d[16];
-  int32_t i4t[16];
+  uint8_t i4q[16];          // edge samples of the current 4x4 block (i4_edge_index)
+  uint8_t i4all[9 * 16];    // its nine predictions, mode-major, raster
   int32_t red[32];
 };
 
@@ -765,67 +765,55 @@ __device__ __noinline__ int analyse_chroma(Smem& sm, bool ht, bool hl, const int
 }
 
 // Intra 4x4 prediction of mode m (h264_dsp.rs:799 predict_intra_4x4_u8_scalar) into out[16].
-__device__ __noinline__ void pred4x4(int mode, const uint8_t* t, const uint8_t* l, bool ht, bool hl, int m, uint8_t* o) {
-  int A = t[0], B = t[1], C = t[2], D = t[3], E = t[4], F = t[5], G = t[6], H = t[7];
-  int I = l[0], J = l[1], K = l[2], L = l[3];
-#define A2(x, y) (uint8_t)(((x) + (y) + 1) >> 1)
-#define A3(x, y, z) (uint8_t)(((x) + 2 * (y) + (z) + 2) >> 2)
-  switch (mode) {
-    case 0: for (int i = 0; i < 16; i++) o[i] = t[i & 3]; break;
-    case 1: for (int i = 0; i < 16; i++) o[i] = l[i >> 2]; break;
-    case 2: {
-      int dc;
-      if (ht && hl) dc = (A + B + C + D + I + J + K + L + 4) >> 3;
-      else if (ht) dc = (A + B + C + D + 2) >> 2;
-      else if (hl) dc = (I + J + K + L + 2) >> 2;
-      else dc = 128;
-      for (int i = 0; i < 16; i++) o[i] = (uint8_t)dc;
-      break;
-    }
-    case 3: {
-      uint8_t p[7] = {A3(A, B, C), A3(B, C, D), A3(C, D, E), A3(D, E, F), A3(E, F, G), A3(F, G, H), A3(G, H, H)};
-      for (int y = 0; y < 4; y++) for (int x = 0; x < 4; x++) o[y * 4 + x] = p[x + y];
-      break;
-    }
-    case 4: {
-      uint8_t lm = A3(K, J, I), kj = A3(L, K, J), ji = A3(J, I, m), im = A3(I, m, A), ma = A3(m, A, B), ab = A3(A, B, C), bc = A3(B, C, D);
-      uint8_t r[16] = {im, ma, ab, bc, ji, im, ma, ab, lm, ji, im, ma, kj, lm, ji, im};
-      for (int i = 0; i < 16; i++) o[i] = r[i];
-      break;
-    }
+// Intra 4x4 prediction (h264.rs:3223 predict_4x4, the nine modes of H.264 8.3.1.2) in closed
+// form. The block's edge samples are gathered into Q[16]:
+//   Q[0] = Q[1] = l3, Q[2] = l2, Q[3] = l1, Q[4] = l0, Q[5] = top-left, Q[6..13] = t0..t7,
+//   Q[14] = t7, Q[15] = the DC value,
+// so that every predicted sample of every mode is Q[i], avg2(Q[i], Q[i+1]) or avg3(Q[i], Q[i+1],
+// Q[i+2]) with i a function of (mode, x, y) -- e.g. diagonal down-right is avg3 at 4 + x - y,
+// horizontal-up at z = x + 2y is avg2 at 3 - z/2 (z even), avg3 at 2 - z/2 (z odd) and l3 past z = 5.
+// Returns kind (0 copy, 1 avg2, 2 avg3) << 8 | i.
+__device__ __forceinline__ int i4_tap(int m, int x, int y) {
+  switch (m) {
+    case 0: return 6 + x;
+    case 1: return 4 - y;
+    case 2: return 15;
+    case 3: return 0x200 | (6 + x + y);
+    case 4: return 0x200 | (4 + x - y);
     case 5: {
-      uint8_t r0[4] = {A2(m, A), A2(A, B), A2(B, C), A2(C, D)};
-      uint8_t r1[4] = {A3(I, m, A), A3(m, A, B), A3(A, B, C), A3(B, C, D)};
-      uint8_t r[16] = {r0[0], r0[1], r0[2], r0[3], r1[0], r1[1], r1[2], r1[3],
-                       A3(J, I, m), r0[0], r0[1], r0[2], A3(K, J, I), r1[0], r1[1], r1[2]};
-      for (int i = 0; i < 16; i++) o[i] = r[i];
-      break;
+      int z = 2 * x - y;
+      return z < 0 ? 0x200 | (5 + z) : ((z & 1) ? 0x200 | (4 + x - (y >> 1)) : 0x100 | (5 + x - (y >> 1)));
     }
     case 6: {
-      uint8_t r0[4] = {A2(m, I), A3(I, m, A), A3(m, A, B), A3(A, B, C)};
-      uint8_t r1[4] = {A2(I, J), A3(m, I, J), r0[0], r0[1]};
-      uint8_t r2[4] = {A2(J, K), A3(I, J, K), r1[0], r1[1]};
-      uint8_t r3[4] = {A2(K, L), A3(J, K, L), r2[0], r2[1]};
-      for (int i = 0; i < 4; i++) { o[i] = r0[i]; o[4 + i] = r1[i]; o[8 + i] = r2[i]; o[12 + i] = r3[i]; }
-      break;
+      int z = 2 * y - x;
+      return z < 0 ? 0x200 | (3 - z) : ((z & 1) ? 0x200 | (3 - (z >> 1)) : 0x100 | (4 - (z >> 1)));
     }
-    case 7: {
-      uint8_t r0[4] = {A2(A, B), A2(B, C), A2(C, D), A2(D, E)};
-      uint8_t r1[4] = {A3(A, B, C), A3(B, C, D), A3(C, D, E), A3(D, E, F)};
-      uint8_t r[16] = {r0[0], r0[1], r0[2], r0[3], r1[0], r1[1], r1[2], r1[3],
-                       r0[1], r0[2], r0[3], A2(E, F), r1[1], r1[2], r1[3], A3(E, F, G)};
-      for (int i = 0; i < 16; i++) o[i] = r[i];
-      break;
-    }
+    case 7: return ((y & 1) ? 0x200 : 0x100) | (6 + x + (y >> 1));
     default: {
-      uint8_t p0 = A2(I, J), p1 = A3(I, J, K), p2 = A2(J, K), p3 = A3(J, K, L), p4 = A2(K, L), p5 = A3(K, L, L), p6 = (uint8_t)L;
-      uint8_t r[16] = {p0, p1, p2, p3, p2, p3, p4, p5, p4, p5, p6, p6, p6, p6, p6, p6};
-      for (int i = 0; i < 16; i++) o[i] = r[i];
-      break;
+      int z = x + 2 * y;
+      return z > 5 ? 1 : ((z & 1) ? 0x200 | (2 - (z >> 1)) : 0x100 | (3 - (z >> 1)));
     }
   }
-#undef A2
-#undef A3
+}
+// One pass of the 4x4 forward core transform along the axis whose lanes are `step` apart in a
+// 16-lane group (i = position along it): [1 1 1 1; 2 1 -1 -2; 1 -1 -1 1; 1 -2 2 -1].
+__device__ __forceinline__ int fwd4_pass(int v, int step, int i) {
+  int b = __shfl_xor_sync(FULL, v, 3 * step);
+  int s = v + b, dd = v - b;
+  int ps = __shfl_xor_sync(FULL, s, step), pd = __shfl_xor_sync(FULL, dd, step);
+  return i == 0 ? s + ps : (i == 1 ? 2 * pd + dd : (i == 2 ? ps - s : 2 * pd - dd));
+}
+// One pass of the inverse core transform (fixed.rs:192): e0 = c0 + c2, e1 = c0 - c2,
+// e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1); out = e0 + e3, e1 + e2, e1 - e2, e0 - e3.
+__device__ __forceinline__ int inv4_pass(int v, int step, int i) {
+  int b = __shfl_xor_sync(FULL, v, 2 * step);
+  int ea, eb;
+  if (i == 0) { ea = v + b; eb = v - b; }
+  else if (i == 2) { ea = b + v; eb = b - v; }
+  else if (i == 1) { ea = (v >> 1) - b; eb = v + (b >> 1); }
+  else { ea = (b >> 1) - v; eb = b + (v >> 1); }
+  int pa = __shfl_xor_sync(FULL, ea, step), pb = __shfl_xor_sync(FULL, eb, step);
+  return i == 0 ? ea + pb : (i == 1 ? pb + ea : (i == 2 ? eb - pa : pa - eb));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1073,64 +1061,75 @@ __device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht,
 }
 
 // I4x4 analysis (enc.rs:3336 analyse_i4): sixteen blocks in decoding order, each choosing among
-// the nine modes by SATD + lambda * mode bits, reconstructed into tmp_y before the next.
-// Returns false when the running cost reaches the budget. Levels go to sm.coef.
+// the available modes by SATD + lambda * (1 if the predicted mode else 4), then quantising and
+// reconstructing before the next block. Per block the warp gathers the edge samples (lane k ->
+// Q[k]), builds all nine predictions (lane -> pixel, the two half-warps taking even / odd modes),
+// costs the modes (lane -> mode), and transforms the chosen residual with shuffles (lane ->
+// coefficient). Gives up (false) as soon as the running cost reaches `budget`.
 __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
+  int p = lane & 15, xl = p & 3, yl = p >> 2;
   int qp = fp.qp;
   uint32_t lambda = c_lambda[qp];
   uint32_t shift, bias;
   quant4_params(qp, true, shift, bias);
+  uint32_t mf = c_mf4[qp % 6][pos4(p)];
+  int dqs = (int)c_dq4[qp % 6][pos4(p)] << (qp / 6);
   uint32_t total = lambda * 24;
   int cbpl = 0;
   const MbInfo* info = c.sd->info;
-  uint8_t lmodes[4], tmodes[4];
-  for (int k = 0; k < 4; k++) {
-    lmodes[k] = hl_mb ? (ld_info(&info[c.mb - 1]).i4_right >> (4 * k)) & 15 : 2;
-    tmodes[k] = ht_mb ? (ld_info(&info[c.mb - fp.mb_w]).i4_bottom >> (4 * k)) & 15 : 2;
-  }
+  uint32_t lmodes = hl_mb ? ld_info(&info[c.mb - 1]).i4_right : 0x2222u;
+  uint32_t tmodes = ht_mb ? ld_info(&info[c.mb - fp.mb_w]).i4_bottom : 0x2222u;
   for (int b = 0; b < 16; b++) {
     int bx = blk_x(b), by = blk_y(b), px = bx * 4, py = by * 4;
     bool ht = by > 0 || ht_mb, hl = bx > 0 || hl_mb;
-    uint8_t top[8], left[4];
-    int tl = 128;
-    if (ht) {
-      for (int k = 0; k < 4; k++) top[k] = by > 0 ? sm.tmp_y[(py - 1) * 16 + px + k] : sm.top[px + k];
-      bool tr = !(b == 3 || b == 7 || b == 11 || b == 13 || b == 15) && (b != 5 || c.mbx + 1 < fp.mb_w);
-      for (int k = 0; k < 4; k++) top[4 + k] = tr ? (by > 0 ? sm.tmp_y[(py - 1) * 16 + px + 4 + k] : sm.top[px + 4 + k]) : top[3];
-    } else {
-      for (int k = 0; k < 8; k++) top[k] = 128;
+    bool tr = !(b == 3 || b == 7 || b == 11 || b == 13 || b == 15) && (b != 5 || c.mbx + 1 < fp.mb_w);
+    // edge samples (unavailable ones 128; top-right replicated from t3 when unavailable)
+    int q = 128;
+    if (p <= 4) {
+      int j = p <= 1 ? 3 : 4 - p;
+      if (hl) q = bx > 0 ? sm.tmp_y[(py + j) * 16 + px - 1] : sm.left[py + j];
+    } else if (p == 5) {
+      if (ht && hl)
+        q = (by > 0 && bx > 0) ? sm.tmp_y[(py - 1) * 16 + px - 1]
+                               : (by > 0 ? sm.left[py - 1] : (bx > 0 ? sm.top[px - 1] : tl_mb));
+    } else if (p <= 14) {
+      int i = min(p - 6, 7);
+      if (i >= 4 && !tr) i = 3;
+      if (ht) q = by > 0 ? sm.tmp_y[(py - 1) * 16 + px + i] : sm.top[px + i];
     }
-    if (hl) {
-      for (int k = 0; k < 4; k++) left[k] = bx > 0 ? sm.tmp_y[(py + k) * 16 + px - 1] : sm.left[py + k];
-    } else {
-      for (int k = 0; k < 4; k++) left[k] = 128;
-    }
-    if (ht && hl) {
-      if (by > 0 && bx > 0) tl = sm.tmp_y[(py - 1) * 16 + px - 1];
-      else if (by > 0) tl = sm.left[py - 1];
-      else if (bx > 0) tl = sm.top[px - 1];
-      else tl = tl_mb;
-    }
+    uint32_t sums = wsum(lane < 16 ? ((p >= 6 && p <= 9) ? (uint32_t)q : 0u) + ((p >= 1 && p <= 4) ? (uint32_t)q << 16 : 0u) : 0u);
+    int st = (int)(sums & 0xffff), sl = (int)(sums >> 16);
+    int dc = ht && hl ? (st + sl + 4) >> 3 : (ht ? (st + 2) >> 2 : (hl ? (sl + 2) >> 2 : 128));
+    if (lane < 16) sm.i4q[p] = (uint8_t)(p == 15 ? dc : q);
     // predicted mode (h264.rs:3283)
     int gx = c.mbx * 4 + bx, gy = c.mby * 4 + by;
     int pm;
     if (gx == 0 || gy == 0) pm = 2;
     else {
-      int ml = bx > 0 ? sm.i4m[(((by >> 1) << 3) | (((bx - 1) >> 1) << 2) | ((by & 1) << 1) | ((bx - 1) & 1))] : lmodes[by];
-      int mt = by > 0 ? sm.i4m[((((by - 1) >> 1) << 3) | ((bx >> 1) << 2) | (((by - 1) & 1) << 1) | (bx & 1))] : tmodes[bx];
+      int ml = bx > 0 ? sm.i4m[(((by >> 1) << 3) | (((bx - 1) >> 1) << 2) | ((by & 1) << 1) | ((bx - 1) & 1))]
+                      : (int)((lmodes >> (4 * by)) & 15);
+      int mt = by > 0 ? sm.i4m[((((by - 1) >> 1) << 3) | ((bx >> 1) << 2) | (((by - 1) & 1) << 1) | (bx & 1))]
+                      : (int)((tmodes >> (4 * bx)) & 15);
       pm = min(ml, mt);
     }
+    __syncwarp();
+    // nine predictions: half-warp h builds modes h, h + 2, ...
+    for (int m = lane >> 4; m < 9; m += 2) {
+      int tap = i4_tap(m, xl, yl), i = tap & 0xff;
+      int a0 = sm.i4q[i], a1 = sm.i4q[min(i + 1, 15)], a2 = sm.i4q[min(i + 2, 15)];
+      int v = (tap >> 8) == 0 ? a0 : ((tap >> 8) == 1 ? (a0 + a1 + 1) >> 1 : (a0 + 2 * a1 + a2 + 2) >> 2);
+      sm.i4all[m * 16 + p] = (uint8_t)v;
+    }
+    __syncwarp();
     // lanes 0..8: one mode each
     uint32_t key = UMAX;
-    uint8_t pr[16];
     if (lane < 9) {
       int m = lane;
       bool av = (m == 0 || m == 3 || m == 7) ? ht : ((m == 1 || m == 8) ? hl : (m == 2 ? true : (ht && hl)));
       if (av) {
-        pred4x4(m, top, left, ht, hl, tl, pr);
-        uint32_t s = satd4(&sm.src_y[py * 16 + px], 16, pr, 4) >> 1;
+        uint32_t s = satd4(&sm.src_y[py * 16 + px], 16, &sm.i4all[m * 16], 4) >> 1;
         uint32_t cost = s + lambda * (m == pm ? 1u : 4u);
         key = (cost << 4) | (uint32_t)m;
       }
@@ -1139,52 +1138,25 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
     int bm = (int)(key & 15);
     total += key >> 4;
     if (total >= budget) return false;
-    if (lane == bm) {
-      for (int k = 0; k < 16; k++) sm.i4pred[k] = pr[k];
-    }
     if (lane == 0) sm.i4m[b] = (uint8_t)bm;
-    __syncwarp();
-    // residual transform (matrix form of the core transform) and quantisation: lane k -> coeff k
-    int lvl = 0, dq = 0;
-    if (lane < 16) {
-      int u = lane >> 2, v = lane & 3;
-      const int Cf[4][4] = {{1, 1, 1, 1}, {2, 1, -1, -2}, {1, -1, -1, 1}, {1, -2, 2, -1}};
-      int acc = 0;
-#pragma unroll
-      for (int y = 0; y < 4; y++)
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-          acc += Cf[u][y] * Cf[v][x] * ((int)sm.src_y[(py + y) * 16 + px + x] - (int)sm.i4pred[y * 4 + x]);
-      acc = (int16_t)acc;
-      uint32_t a = (uint32_t)(acc < 0 ? -acc : acc);
-      int l = (int)((a * c_mf4[qp % 6][pos4(lane)] + bias) >> shift);
-      lvl = acc < 0 ? -l : l;
-      dq = clamp_i16(lvl * ((int)c_dq4[qp % 6][pos4(lane)] << (qp / 6)));
-      sm.coef[b * 16 + lane] = (int16_t)lvl;
-      sm.i4d[lane] = (int16_t)dq;
-    }
+    // residual transform and quantisation, lane p -> coefficient p (raster)
+    int pred = sm.i4all[bm * 16 + p];
+    int acc = fwd4_pass(fwd4_pass((int)sm.src_y[(py + yl) * 16 + px + xl] - pred, 1, xl), 4, yl);
+    acc = (int16_t)acc;
+    uint32_t aa = (uint32_t)(acc < 0 ? -acc : acc);
+    int l = (int)((aa * mf + bias) >> shift);
+    int lvl = acc < 0 ? -l : l;
+    if (lane < 16) sm.coef[b * 16 + p] = (int16_t)lvl;
     bool nz = __ballot_sync(FULL, lane < 16 && lvl != 0) != 0;
-    __syncwarp();
     if (nz) cbpl |= 1 << (b >> 2);
-    // inverse transform (rows then columns, fixed.rs:192) and reconstruction
-    if (lane < 4) {
-      int r = lane;
-      int c0 = sm.i4d[r * 4], c1 = sm.i4d[r * 4 + 1], c2 = sm.i4d[r * 4 + 2], c3 = sm.i4d[r * 4 + 3];
-      int e0 = c0 + c2, e1 = c0 - c2, e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1);
-      sm.i4t[r * 4] = e0 + e3; sm.i4t[r * 4 + 1] = e1 + e2; sm.i4t[r * 4 + 2] = e1 - e2; sm.i4t[r * 4 + 3] = e0 - e3;
+    // inverse transform (rows then columns) and reconstruction
+    int rec = pred;
+    if (nz) {
+      int dq = clamp_i16(lvl * dqs);
+      int r = (int16_t)((inv4_pass(inv4_pass(dq, 1, xl), 4, yl) + 32) >> 6);
+      rec = clip255(pred + r);
     }
-    __syncwarp();
-    if (lane < 4) {
-      int k = lane;
-      int t0 = sm.i4t[k], t4 = sm.i4t[k + 4], t8 = sm.i4t[k + 8], t12 = sm.i4t[k + 12];
-      int e0 = t0 + t8, e1 = t0 - t8, e2 = (t4 >> 1) - t12, e3 = t4 + (t12 >> 1);
-      int res[4] = {(int16_t)((e0 + e3 + 32) >> 6), (int16_t)((e1 + e2 + 32) >> 6), (int16_t)((e1 - e2 + 32) >> 6),
-                    (int16_t)((e0 - e3 + 32) >> 6)};
-      for (int y = 0; y < 4; y++) {
-        int p = sm.i4pred[y * 4 + k];
-        sm.tmp_y[(py + y) * 16 + px + k] = (uint8_t)(nz ? clip255(p + res[y]) : p);
-      }
-    }
+    if (lane < 16) sm.tmp_y[(py + yl) * 16 + px + xl] = (uint8_t)rec;
     __syncwarp();
   }
   *cbpl_out = cbpl;
@@ -1295,18 +1267,17 @@ __device__ __noinline__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Pipelined mode synchronisation: monotonic progress counters, published with release stores
-// after a fence by every lane, polled with acquire loads by every lane. Every wait has a time
-// limit; when it runs out the kernel records RG_ERR_TIMEOUT and all warps leave.
-struct PipeWait {
-  const int* ana_prev;   // analysis progress per macroblock row of the reference frame
-  const int* db_prev;    // deblocking progress per row of the reference frame (padding included)
-  int* error;
-  unsigned long long timeout_ns;
-};
+// Pipelined mode synchronisation: monotonic progress counters, published with a release store
+// after a fence, awaited with an acquire load. Every wait has a time limit; when it runs out
+// the kernel records RG_ERR_TIMEOUT and all warps leave.
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
   asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_release(int* p, int v) {
@@ -1317,21 +1288,42 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Waits until *p >= need (all lanes). Returns false on timeout or when another warp failed.
-__device__ __noinline__ bool wait_geq(const int* p, int need, int* error, unsigned long long timeout_ns) {
-  if (__all_sync(FULL, ld_acquire(p) >= need)) return true;
+// Waits until *p >= need. The first check and the final one are acquire loads by every lane;
+// in between lane 0 polls with relaxed loads (which leave the SM's L1 alone) and sleeps 32 ns
+// doubling to 512 ns. Returns the acquired value, or -1 on timeout (recorded in *error) or
+// when another warp failed.
+__device__ __noinline__ int wait_geq(const int* p, int need, int* error, unsigned long long timeout_ns) {
+  int v = ld_acquire(p);
+  if (__all_sync(FULL, v >= need)) return v;
   unsigned long long t0 = global_ns();
+  unsigned int sleep = 32;
   while (true) {
-    if (__all_sync(FULL, ld_acquire(p) >= need)) return true;
-    int e = __shfl_sync(FULL, lane_id() == 0 ? ld_acquire(error) : 0, 0);
-    if (e) return false;
+    int r = 0;
+    if (lane_id() == 0) r = ld_relaxed(p) >= need ? 1 : (ld_relaxed(error) ? 2 : 0);
+    r = __shfl_sync(FULL, r, 0);
+    if (r == 1) {
+      v = ld_acquire(p);
+      if (__all_sync(FULL, v >= need)) return v;
+    }
+    if (r == 2) return -1;
     unsigned long long dt = __shfl_sync(FULL, global_ns() - t0, 0);
     if (dt > timeout_ns) {
       if (lane_id() == 0) atomicCAS(error, 0, 1);
-      return false;
+      return -1;
     }
-    __nanosleep(200);
+    __nanosleep(sleep);
+    sleep = min(sleep * 2, 512u);
   }
+}
+// wait_geq with the last acquired value of the counter kept in `seen`: no load when it already
+// covers `need` (the acquire that returned it orders every later load of this warp).
+__device__ __forceinline__ bool wait_seen(const int* p, int need, int& seen, int* error,
+                                          unsigned long long timeout_ns) {
+  if (seen >= need) return true;
+  int v = wait_geq(p, need, error, timeout_ns);
+  if (v < 0) return false;
+  seen = v;
+  return true;
 }
 // Makes this warp's global writes visible, then publishes v.
 __device__ __forceinline__ void publish(int* p, int v) {
@@ -1339,10 +1331,21 @@ __device__ __forceinline__ void publish(int* p, int v) {
   __syncwarp();
   if (lane_id() == 0) st_release(p, v);
 }
+// What a P macroblock of the pipelined mode waits for in its reference picture.
+struct PipeWait {
+  const int* ana_prev;   // analysis progress per macroblock row of the reference picture
+  const int* db_prev;    // deblocking progress per row of the reference picture (padding included)
+  int* error;
+  unsigned long long timeout_ns;
+  int seen_ana;          // last acquired ana_prev[row of this segment]
+  int db_row, seen_db;   // last acquired db_prev[db_row]
+  bool failed;
+};
 
 // One macroblock of a P slice (enc.rs:3011 code_p_mb). In the pipelined mode (pw != null) it
-// first waits for the reference frame to be final over every sample its search can read.
-__device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, const PipeWait* pw) {
+// first waits for the reference frame to be final over every sample its search can read; when
+// a wait gives up it returns with pw->failed set and writes nothing.
+__device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) {
   const FrameParams& fp = *c.fp;
   const StreamDev& sd = *c.sd;
   int lane = lane_id();
@@ -1380,7 +1383,10 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, const PipeWait
   load_source(c, sm);
   int qpc = fp.qpc;
   // co-located vector of the previous picture: a search candidate (enc.rs:3094)
-  if (pw && !wait_geq(pw->ana_prev + mby, mbx + 1, pw->error, pw->timeout_ns)) return;
+  if (pw && !wait_seen(pw->ana_prev + mby, mbx + 1, pw->seen_ana, pw->error, pw->timeout_ns)) {
+    pw->failed = true;
+    return;
+  }
   MbInfo prevmb = ld_info(&sd.prev_info[c.mb]);
   if (pw) {
     // The right- and bottom-most reference sample this macroblock can read: the full-pel
@@ -1396,9 +1402,17 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, const PipeWait
     }
     int xb = (x0 + hi0 + 44) >> 4, rb = (y0 + hi1 + 40) >> 4;
     int rr = min(max(rb, 0), fp.mb_h - 1), xx = min(max(xb, 0), fp.mb_w - 1);
-    bool ok = rr < fp.mb_h - 1 ? wait_geq(pw->db_prev + rr + 1, xx + 1, pw->error, pw->timeout_ns)
-                               : wait_geq(pw->db_prev + rr, min(xx + 2, fp.mb_w), pw->error, pw->timeout_ns);
-    if (!ok) return;
+    // rows above the last are final where the row below is deblocked; the last row where its
+    // right neighbour is
+    int row = rr < fp.mb_h - 1 ? rr + 1 : rr, need = rr < fp.mb_h - 1 ? xx + 1 : min(xx + 2, fp.mb_w);
+    if (row != pw->db_row) {
+      pw->db_row = row;
+      pw->seen_db = 0;
+    }
+    if (!wait_seen(pw->db_prev + row, need, pw->seen_db, pw->error, pw->timeout_ns)) {
+      pw->failed = true;
+      return;
+    }
   }
 
   // 1. skip probe (enc.rs:2906 try_p_skip)
@@ -1916,23 +1930,22 @@ __device__ __noinline__ void extend_mb(const FrameParams& fp, const StreamDev& s
   }
 }
 
-// Persistent pipelined mode: F pictures of every stream in one launch. Work is cut into row
-// tasks handed out in ticket order -- per picture, analysis of row y for every stream, then
-// deblocking of row y-1 -- and every wait is for a task of a smaller ticket (the row above,
-// the row below's analysis two macroblocks ahead, the reference picture's final region), so
-// any number of resident warps makes progress. Picture f+1 starts as soon as the part of
-// picture f its search can reach is deblocked and border-extended.
+// Persistent pipelined mode: F pictures of every stream in one launch. The work is cut into
+// segments of `seg` consecutive macroblocks of one row -- analysis segments and deblocking
+// segments -- listed by the host in the order they are expected to become ready (pipeline_task_
+// list) and handed out by an atomic ticket. A warp only holds one short segment, so the resident
+// warps cover the work that is about to be ready rather than whole rows far from it, and every
+// wait is normally for a segment of a smaller ticket. Picture f+1 of a stream starts as soon as
+// the part of picture f its search can reach is deblocked and border-extended.
 struct PipeParams {
   int* ticket;
   int* error;
   int* ana;    // [F][S][mb_h] analysed macroblocks per row
   int* db;     // [F][S][mb_h] deblocked macroblocks per row; a macroblock's deblocking also
                // extends the padding of the macroblocks it makes final
-  const int* t_off;  // first ticket of each row-time T (T = tau + skew * f), n_times + 1 entries
-  int n_times;
-  int skew;    // row-times between the starts of consecutive pictures of a stream
-  int frames;
-  int n_tickets;
+  const int2* tasks;  // {picture * S + stream, row << 16 | first macroblock << 1 | deblock}
+  int n_tasks;
+  int seg;
   unsigned long long timeout_ns;
 };
 
@@ -1944,61 +1957,54 @@ __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const 
     int t = 0;
     if (lane == 0) t = atomicAdd(pp.ticket, 1);
     t = __shfl_sync(FULL, t, 0);
-    if (t >= pp.n_tickets) break;
-    if (__shfl_sync(FULL, lane == 0 ? ld_acquire(pp.error) : 0, 0)) break;
-    // Ticket -> (row-time T, picture f, role, row, stream). At picture-local row-time tau a
-    // picture has the analysis of row tau (tau < H) then the deblocking of row tau - 1 (tau >= 1);
-    // pictures of one T in increasing order, streams innermost.
-    int lo = 0, hi = pp.n_times;  // largest T with t_off[T] <= t
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (pp.t_off[mid] <= t) lo = mid; else hi = mid;
-    }
-    int T = lo, rem = t - pp.t_off[T];
-    // pictures open at T: tau = T - skew * f in [0, H], oldest (largest tau) first
-    int f = T - H > 0 ? (T - H + pp.skew - 1) / pp.skew : 0;
-    int tau = 0, na = 0, nd = 0;
-    for (;; f++) {
-      tau = T - pp.skew * f;
-      na = tau < H ? 1 : 0;
-      nd = tau >= 1 ? 1 : 0;
-      int cnt = S * (na + nd);
-      if (rem < cnt) break;
-      rem -= cnt;
-    }
-    bool ana = rem < S * na;
-    int s = ana ? rem : rem - S * na;
-    int y = ana ? tau : tau - 1;
-    const StreamDev& sd = sds[f * S + s];
-    int* ana_rows = pp.ana + (f * S + s) * H;
-    int* db_rows = pp.db + (f * S + s) * H;
+    if (t >= pp.n_tasks) break;
+    if (__shfl_sync(FULL, lane == 0 ? ld_relaxed(pp.error) : 0, 0)) break;
+    int2 task = __ldg(pp.tasks + t);
+    int ps = task.x, f = ps / S;
+    int y = task.y >> 16, x0 = (task.y >> 1) & 0x7fff, x1 = min(x0 + pp.seg, Wm);
+    bool ana = (task.y & 1) == 0;
+    const StreamDev& sd = sds[ps];
+    int* ana_rows = pp.ana + ps * H;
+    int* db_rows = pp.db + ps * H;
     bool failed = false;
     if (ana) {
       PipeWait pw;
       bool has_prev = f > 0 && sd.kind == RG_FRAME_P;
       if (has_prev) {
-        pw.ana_prev = pp.ana + ((f - 1) * S + s) * H;
-        pw.db_prev = pp.db + ((f - 1) * S + s) * H;
+        pw.ana_prev = pp.ana + (ps - S) * H;
+        pw.db_prev = pp.db + (ps - S) * H;
       }
       pw.error = pp.error;
       pw.timeout_ns = pp.timeout_ns;
-      for (int x = 0; x < Wm && !failed; x++) {
-        if (y > 0 && !wait_geq(ana_rows + y - 1, min(x + 2, Wm), pp.error, pp.timeout_ns)) { failed = true; break; }
+      pw.seen_ana = 0;
+      pw.db_row = -1;
+      pw.seen_db = 0;
+      pw.failed = false;
+      int seen_own = 0, seen_up = 0;
+      // the previous segment of this row, then per macroblock the row above two ahead
+      if (x0 > 0 && !wait_seen(ana_rows + y, x0, seen_own, pp.error, pp.timeout_ns)) failed = true;
+      for (int x = x0; x < x1 && !failed; x++) {
+        if (y > 0 && !wait_seen(ana_rows + y - 1, min(x + 2, Wm), seen_up, pp.error, pp.timeout_ns)) {
+          failed = true;
+          break;
+        }
         Ctx c{&fp, &sd, x, y, y * Wm + x};
         if (sd.kind == RG_FRAME_IDR) {
           load_source(c, sm);
           analyse_intra_mb(c, sm);
         } else {
           analyse_p_mb(c, sm, has_prev ? &pw : nullptr);
-          if (__shfl_sync(FULL, lane == 0 ? ld_acquire(pp.error) : 0, 0)) { failed = true; break; }
+          if (pw.failed) { failed = true; break; }
         }
         publish(ana_rows + y, x + 1);
       }
     } else {
-      for (int x = 0; x < Wm; x++) {
-        if (!wait_geq(ana_rows + y, min(x + 2, Wm), pp.error, pp.timeout_ns) ||
-            (y + 1 < H && !wait_geq(ana_rows + y + 1, min(x + 1, Wm), pp.error, pp.timeout_ns)) ||
-            (y > 0 && !wait_geq(db_rows + y - 1, min(x + 2, Wm), pp.error, pp.timeout_ns))) {
+      int seen_own = 0, seen_a0 = 0, seen_a1 = 0, seen_up = 0;
+      if (x0 > 0 && !wait_seen(db_rows + y, x0, seen_own, pp.error, pp.timeout_ns)) failed = true;
+      for (int x = x0; x < x1 && !failed; x++) {
+        if (!wait_seen(ana_rows + y, min(x + 2, Wm), seen_a0, pp.error, pp.timeout_ns) ||
+            (y + 1 < H && !wait_seen(ana_rows + y + 1, min(x + 1, Wm), seen_a1, pp.error, pp.timeout_ns)) ||
+            (y > 0 && !wait_seen(db_rows + y - 1, min(x + 2, Wm), seen_up, pp.error, pp.timeout_ns))) {
           failed = true;
           break;
         }
@@ -2094,39 +2100,63 @@ int pipeline_grid(int device) {
   return per_sm * sms;
 }
 
-// Ticket table of the skewed order: t_off[T] = first ticket of row-time T (host-built, n_times + 1
-// ints written to `table`). Returns the number of row-times.
-int pipeline_ticket_table(const FrameParams& fp, int frames, int skew, int* table) {
-  int S = fp.n_streams, H = fp.mb_h;
-  int n_times = H + 1 + skew * (frames - 1);
-  int acc = 0;
-  for (int T = 0; T < n_times; T++) {
-    table[T] = acc;
-    for (int f = 0; f < frames; f++) {
-      int tau = T - skew * f;
-      if (tau < 0 || tau > H) continue;
-      acc += S * ((tau < H ? 1 : 0) + (tau >= 1 ? 1 : 0));
-    }
-  }
-  table[n_times] = acc;
-  return n_times;
+// Work list of the pipelined mode, written to `tasks` (pipeline_task_count entries): every
+// analysis and deblocking segment of every picture and stream, ordered by a key of the
+// macroblock-time it can start -- a = max(seg, 2) per row, 1 per column, lag per picture:
+//   analysis of row y from column x0:    a * y + x0 + lag * f
+//   deblocking of row y from column x0:  a * (y + 1) + x0 + 1 + lag * f
+// and, at equal keys, by picture, role (analysis first), stream and row. Every macroblock of a
+// segment depends only on segments of a smaller key or of an equal key earlier in that order
+// (the row above two macroblocks ahead lies in a segment of key <= a * (y - 1) + x0 + seg; the
+// deblocking of (x, y) needs the analysis of (x + 1, y) and (x, y + 1) and the deblocking of
+// (x + 1, y - 1)), so warps taking tickets in order never wait for an untaken segment of the same
+// picture. The wait for the reference picture depends on the motion vectors: a search whose
+// window reaches r macroblocks beyond the co-located ones (r = 0 for zero motion) waits for a
+// smaller key when lag >= a * (4 + r) + seg + r + 3. lag <= 0 takes r = 6 (about 96 samples).
+size_t pipeline_task_count(const FrameParams& fp, int frames, int seg) {
+  size_t segs = (size_t)(fp.mb_w + seg - 1) / seg;
+  return 2 * (size_t)frames * fp.n_streams * fp.mb_h * segs;
 }
 
-void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int* d_table,
-                     int n_times, int skew, int grid, unsigned long long timeout_ns, cudaStream_t st) {
+size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, int2* tasks) {
+  int S = fp.n_streams, H = fp.mb_h, W = fp.mb_w;
+  int segs = (W + seg - 1) / seg, a = seg > 2 ? seg : 2;
+  if (lag <= 0) lag = a * 10 + seg + 9;
+  auto key = [&](int f, int role, int y, int k) {
+    return (size_t)a * (y + role) + (size_t)k * seg + role + (size_t)lag * f;
+  };
+  size_t n_keys = key(frames - 1, 1, H - 1, segs - 1) + 1;
+  std::vector<size_t> start(n_keys + 1, 0);
+  for (int f = 0; f < frames; f++)
+    for (int role = 0; role < 2; role++)
+      for (int y = 0; y < H; y++)
+        for (int k = 0; k < segs; k++) start[key(f, role, y, k) + 1] += S;
+  for (size_t i = 0; i < n_keys; i++) start[i + 1] += start[i];
+  // placed in (picture, role, stream, row, segment) order within a key: a stable counting sort
+  for (int f = 0; f < frames; f++)
+    for (int role = 0; role < 2; role++)
+      for (int s = 0; s < S; s++)
+        for (int y = 0; y < H; y++)
+          for (int k = 0; k < segs; k++) {
+            size_t at = start[key(f, role, y, k)]++;
+            tasks[at] = make_int2(f * S + s, (y << 16) | ((k * seg) << 1) | role);
+          }
+  return pipeline_task_count(fp, frames, seg);
+}
+
+void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
+                     size_t n_tasks, int seg, int grid, unsigned long long timeout_ns, cudaStream_t st) {
   int S = fp.n_streams, H = fp.mb_h;
   PipeParams pp;
   pp.ticket = counters;
   pp.error = counters + 1;
   pp.ana = counters + 4;
   pp.db = pp.ana + frames * S * H;
-  pp.t_off = d_table;
-  pp.n_times = n_times;
-  pp.skew = skew;
-  pp.frames = frames;
-  pp.n_tickets = frames * 2 * H * S;
+  pp.tasks = d_tasks;
+  pp.n_tasks = (int)n_tasks;
+  pp.seg = seg;
   pp.timeout_ns = timeout_ns;
-  int g = grid < pp.n_tickets ? grid : pp.n_tickets;
+  int g = grid < pp.n_tasks ? grid : pp.n_tasks;
   pipeline_kernel<<<g, 32, 0, st>>>(fp, d_streams, pp);
 }
 

@@ -20,6 +20,9 @@ namespace {
 
 thread_local std::string g_last_error;
 
+constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the segment length
+constexpr int kDefaultSeg = 8;   // macroblocks per work segment
+
 int fail(int code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -109,10 +112,13 @@ struct rg_ctx {
   size_t n_counters = 0;
   int* h_err = nullptr;            // pinned copy of the device error word
   int grid = 0;
-  int skew = 10;                   // row-times between pictures of a stream in the pipelined order
+  int lag = kDefaultLag;           // macroblock-times between pictures of a stream in the work order
+  int seg = kDefaultSeg;           // macroblocks per work segment
   unsigned long long timeout_ns = 2000000000ull;  // limit of one device wait
-  int* d_table = nullptr;          // ticket table of the pipelined order
-  int* h_table = nullptr;          // pinned
+  int2* d_tasks = nullptr;         // work list of the pipelined mode
+  size_t tasks_cap = 0, n_tasks = 0;
+  int tasks_frames = -1, tasks_lag = -1, tasks_seg = -1;  // what d_tasks holds
+  std::vector<int2> h_tasks;
   // the pending pipelined call, kept to re-run it on the per-diagonal path after a failed wait
   std::vector<const uint8_t*> pend_planes;
   std::vector<int32_t> pend_kinds;
@@ -215,7 +221,8 @@ rg_ctx* rg_create(const rg_config* cfg) {
   alloc((void**)&c->d_streams[0], sizeof(StreamDev) * c->S * c->max_frames);
   alloc((void**)&c->d_streams[1], sizeof(StreamDev) * c->S * c->max_frames);
   alloc((void**)&c->counters, sizeof(int) * c->n_counters);
-  alloc((void**)&c->d_table, sizeof(int) * (fp.mb_h + 4 + (size_t)c->skew * c->max_frames));
+  c->tasks_cap = pipeline_task_count(fp, c->max_frames, c->seg);
+  alloc((void**)&c->d_tasks, sizeof(int2) * c->tasks_cap);
   if (!ok) {
     fail(RG_ERR_OOM, "rg_create: device allocation failed");
     rg_destroy(c);
@@ -224,7 +231,6 @@ rg_ctx* rg_create(const rg_config* cfg) {
   if (cudaMallocHost((void**)&c->h_streams[0], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
       cudaMallocHost((void**)&c->h_streams[1], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
       cudaMallocHost((void**)&c->h_err, sizeof(int)) != cudaSuccess ||
-      cudaMallocHost((void**)&c->h_table, sizeof(int) * (fp.mb_h + 4 + (size_t)c->skew * c->max_frames)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->slot_done[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->slot_done[1], cudaEventDisableTiming) != cudaSuccess) {
@@ -261,9 +267,8 @@ void rg_destroy(rg_ctx* c) {
   cudaFree(c->m_djobs);
   cudaFree(c->m_src);
   cudaFree(c->counters);
-  cudaFree(c->d_table);
+  cudaFree(c->d_tasks);
   if (c->h_err) cudaFreeHost(c->h_err);
-  if (c->h_table) cudaFreeHost(c->h_table);
   if (c->h_streams[0]) cudaFreeHost(c->h_streams[0]);
   if (c->h_streams[1]) cudaFreeHost(c->h_streams[1]);
   for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
@@ -409,11 +414,17 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
   CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * S * frames, cudaMemcpyHostToDevice, c->stream));
   CK(cudaEventRecord(c->slot_done[slot], c->stream));
   CK(cudaMemsetAsync(c->counters, 0, sizeof(int) * pipeline_counter_ints(c->fp, frames), c->stream));
-  CK(cudaStreamSynchronize(c->stream));  // the pinned ticket table is rewritten below
-  int n_times = pipeline_ticket_table(fp, frames, c->skew, c->h_table);
-  CK(cudaMemcpyAsync(c->d_table, c->h_table, sizeof(int) * (n_times + 1), cudaMemcpyHostToDevice, c->stream));
-  // a generous bound on any single wait: a whole picture of the batch takes far less
-  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_table, n_times, c->skew, c->grid, c->timeout_ns,
+  if (frames != c->tasks_frames || c->lag != c->tasks_lag || c->seg != c->tasks_seg) {
+    // rebuilt only when the call's shape or the tuning changes; the copy is stream-ordered
+    // after any launch still reading the old list
+    c->h_tasks.resize(pipeline_task_count(fp, frames, c->seg));
+    c->n_tasks = pipeline_task_list(fp, frames, c->lag, c->seg, c->h_tasks.data());
+    CK(cudaMemcpyAsync(c->d_tasks, c->h_tasks.data(), sizeof(int2) * c->n_tasks, cudaMemcpyHostToDevice, c->stream));
+    c->tasks_frames = frames;
+    c->tasks_lag = c->lag;
+    c->tasks_seg = c->seg;
+  }
+  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->seg, c->grid, c->timeout_ns,
                   c->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_err, c->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -437,13 +448,26 @@ int rg_copy_records_gops(rg_ctx* c, int32_t frames, rg_mb_out* out) {
   return RG_OK;
 }
 
-int rg_set_pipeline_tuning(rg_ctx* c, int32_t skew, int32_t grid, int32_t timeout_ms) {
+int rg_set_pipeline_tuning(rg_ctx* c, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms) {
   if (!c) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: null context");
-  if (skew < 0 || skew > 10) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: skew %d outside 0..10", skew);
+  if (lag < 0 || lag > 4096) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: lag %d outside 0..4096", lag);
+  if (seg < 0 || seg > c->fp.mb_w) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: seg %d outside 0..%d", seg, c->fp.mb_w);
   if (grid < 0 || timeout_ms < 0) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: negative argument");
   CK(cudaStreamSynchronize(c->stream));
-  c->skew = skew > 0 ? skew : 1;
-  if (skew == 0) c->skew = 1;
+  int new_seg = seg > 0 ? seg : kDefaultSeg;
+  if (new_seg > c->fp.mb_w) new_seg = c->fp.mb_w;
+  size_t need = pipeline_task_count(c->fp, c->max_frames, new_seg);
+  if (need > c->tasks_cap) {
+    int2* p = nullptr;
+    if (cudaMalloc((void**)&p, sizeof(int2) * need) != cudaSuccess)
+      return fail(RG_ERR_OOM, "rg_set_pipeline_tuning: work list of %zu segments", need);
+    cudaFree(c->d_tasks);
+    c->d_tasks = p;
+    c->tasks_cap = need;
+  }
+  c->lag = lag > 0 ? lag : kDefaultLag;
+  c->seg = new_seg;
+  c->tasks_frames = -1;
   if (grid > 0) c->grid = grid;
   else c->grid = pipeline_grid(c->cfg.device);
   c->timeout_ns = timeout_ms > 0 ? (unsigned long long)timeout_ms * 1000000ull : 2000000000ull;
@@ -481,7 +505,7 @@ int rg_sync(rg_ctx* c) {
   if (!c) return fail(RG_ERR_INVALID, "rg_sync: null context");
   CK(cudaStreamSynchronize(c->stream));
   if (*c->h_err) {
-    // A wait of the pipelined launch gave up (a search reaching further than the picture skew
+    // A wait of the pipelined launch gave up (a search reaching further than the picture lag
     // allows, or a fault of another warp). Every picture of the call wrote its own ring slot and
     // the reference it started from is untouched, so the call is re-run, picture by picture, on
     // the per-diagonal path, which has no waits. Results are identical.

@@ -92,10 +92,11 @@ def test_pipelined_gops_match_oracle(w, h, qp, profile, streams, frames):
 
 
 def test_pipelined_wait_timeout_falls_back_to_exact_path():
-    """Failure detection without a GPU fault: one resident warp and no skew make a picture's
-    first row wait for rows of the previous picture that no warp will ever take (a flag nothing
-    sets). The wait gives up after 300 ms, the launch stops with an error status the host reads,
-    and the call is re-run on the per-diagonal path: results stay exact, the context usable."""
+    """Failure detection without a GPU fault: one resident warp and a lag of one macroblock-time
+    make a picture's first segment wait for deblocking of the previous picture that no warp will
+    ever take (a flag nothing sets). The wait gives up after 300 ms, the launch stops with an
+    error status the host reads, and the call is re-run on the per-diagonal path: results stay
+    exact, the context usable."""
     from oracle_lib import OracleEncoder
     from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
     from gpu_parity_util import first_record_mismatch
@@ -103,7 +104,7 @@ def test_pipelined_wait_timeout_falls_back_to_exact_path():
     w, h, qp, frames = 96, 96, 28, 3
     clip = grating_clip(w, h, frames, seed=77, motion=4.0, rects=1)
     eng = Engine(w, h, qp, profile=2, num_streams=1, max_frames=frames)
-    eng.set_pipeline_tuning(skew=1, grid=1, timeout_ms=300)
+    eng.set_pipeline_tuning(lag=1, grid=1, timeout_ms=300)
     recs = eng.analyse_gops([[clip[f]] for f in range(frames)], [[RG_FRAME_IDR]] + [[RG_FRAME_P]] * (frames - 1))
     orc = OracleEncoder(w, h, qp, profile=2, keyint=frames + 1)
     for f in range(frames):
