@@ -184,7 +184,7 @@ def run_engine(args, rank, world, local):
         return [p, p + W * H, p + W * H + cw * ch]
 
     eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
-    eng.set_pipeline_tuning(lag=args.lag, seg=args.seg)
+    eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms)
     stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
     torch.cuda.synchronize()
     gop_ptrs, gop_kinds = [], []
@@ -314,7 +314,7 @@ def run_engine(args, rank, world, local):
 def run_profile_case(args, local):
     """Small case for ncu: one IDR batch and one P batch of the 8-GOP 1080p workload (16 frames),
     with the device time of each batch -- per anti-diagonal launches, or (pipelined) the first
-    three pictures (IDR, P, P) of the 8 GOPs in one persistent launch."""
+    --profile-frames pictures (IDR, P, ...) of the 8 GOPs in one persistent launch."""
     import torch
 
     from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_HIGH, Engine
@@ -331,9 +331,9 @@ def run_profile_case(args, local):
     dev = torch.from_numpy(host).to(f"cuda:{local}")
     base = dev.data_ptr()
     if args.profile_case == "pipelined":
-        nf = 3
+        nf = args.profile_frames
         eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=nf)
-        eng.set_pipeline_tuning(lag=args.lag, seg=args.seg)
+        eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms)
         stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
         ptrs, kinds = [], []
         for f in range(nf):
@@ -351,7 +351,7 @@ def run_profile_case(args, local):
             e1.synchronize()
             eng.sync()
             times.append(e0.elapsed_time(e1))
-        print(json.dumps({"profile_case": "1080p High QP26, 8 streams x 3 pictures (IDR, P, P), one pipelined launch",
+        print(json.dumps({"profile_case": f"1080p High QP26, 8 streams x {nf} pictures (IDR, then P), one pipelined launch",
                           "launch_ms": [round(t, 3) for t in times]}), flush=True)
         eng.close()
         return
@@ -391,6 +391,12 @@ def main():
     ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
                     choices=["wavefront", "pipelined"],
                     help="a small slice of the workload (the ncu capture case)")
+    ap.add_argument("--profile-frames", type=int, default=3, choices=range(1, 9),
+                    help="pictures per stream of the pipelined profile case")
+    ap.add_argument("--grid", type=int, default=0,
+                    help="pipelined mode: resident warps (0 = default)")
+    ap.add_argument("--deblock-sms", type=int, default=0,
+                    help="pipelined mode: SMs taking deblocking segments first (0 = default, -1 = one mixed queue)")
     ap.add_argument("--lag", type=int, default=0,
                     help="pipelined mode: macroblock-times between consecutive pictures in the work order (0 = default)")
     ap.add_argument("--seg", type=int, default=0,

@@ -167,15 +167,18 @@ int rg_copy_records_gops(rg_ctx* ctx, int32_t frames, rg_mb_out* out);
 
 /*
  * Tuning / test hook of the pipelined mode: lag = macroblock-times between consecutive pictures
- * of a stream in the work order (1..4096; 0 = 10 * max(seg, 2) + seg + 9, which orders every
- * wait of a search reaching up to 6 macroblock rows beyond zero motion after the work it waits
+ * of a stream in the work order (1..4096; 0 = 8 * max(seg, 2) + seg + 7, which orders every
+ * wait of a search reaching up to 4 macroblock rows beyond zero motion after the work it waits
  * for; larger is safer for long motion, smaller favours newer pictures), seg = macroblocks per
- * work segment (1..mb_w, 0 = 8), grid = resident warps (0 = all that fit), timeout_ms = limit of
- * one device wait (0 = 2000). A wait that runs out makes the launch stop and rg_sync re-run the
- * call on the per-diagonal path, which has no waits. No counterpart in the reference (its GOP
- * threads have no device schedule).
+ * work segment (1..mb_w, 0 = 2), grid = resident warps (0 = six per SM, fewer if they do not
+ * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take
+ * deblocking segments first from a queue of their own (0 = one SM in nine, -1 = one mixed queue
+ * for all warps). A wait that runs out makes the launch stop and rg_sync re-run the call on the
+ * per-diagonal path, which has no waits. No counterpart in the reference (its GOP threads have
+ * no device schedule).
  */
-int rg_set_pipeline_tuning(rg_ctx* ctx, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms);
+int rg_set_pipeline_tuning(rg_ctx* ctx, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms,
+                           int32_t deblock_sms);
 
 /* Waits for queued device work of the context. */
 int rg_sync(rg_ctx* ctx);

@@ -74,13 +74,16 @@ int wavefront_steps(const FrameParams& fp);
 // Pipelined mode: d_streams holds frames x n_streams descriptors (picture-major); counters is
 // pipeline_counter_ints() zeroed ints; counters[1] is non-zero after a failed wait.
 int pipeline_grid(int device);
+int pipeline_sms(int device);
 size_t pipeline_counter_ints(const FrameParams& fp, int frames);
 // Work list: every analysis / deblocking segment of `seg` macroblocks, in expected-ready order
 // with `lag` macroblock-times between consecutive pictures of a stream.
 size_t pipeline_task_count(const FrameParams& fp, int frames, int seg);
-size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, int2* tasks);
+// split: analysis segments first, then deblocking segments, as two queues (*n_ana analysis).
+size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, int2* tasks, size_t* n_ana);
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
-                     size_t n_tasks, int seg, int grid, unsigned long long timeout_ns, cudaStream_t st);
+                     size_t n_tasks, size_t n_ana, int deblock_sms, int sms, int seg, int grid,
+                     unsigned long long timeout_ns, cudaStream_t st);
 void upload_tables();
 
 }  // namespace rg

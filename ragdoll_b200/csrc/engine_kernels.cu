@@ -77,8 +77,7 @@ struct __align__(16) Smem {
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ MbInfo ld_info(const MbInfo* p) {
-  int4 v;
-  asm volatile("ld.global.v4.s32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  int4 v = *(const int4*)p;
   MbInfo m;
   *(int4*)&m = v;
   return m;
@@ -119,25 +118,18 @@ __device__ __forceinline__ uint32_t mvd_cost(int d, uint32_t lambda) {
 }
 
 // Reconstructed pictures and macroblock state are produced by other warps of the same launch in
-// the pipelined mode. They are read with plain weak loads (never the non-coherent path), and only
-// after an ld.acquire that observed the producer's release: the memory model then guarantees the
-// loads see the produced values, L1 included.
-__device__ __forceinline__ uint32_t ldw32(const void* p) {
-  uint32_t v;
-  asm volatile("ld.global.b32 %0, [%1];" : "=r"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ uint8_t ldcg_u8(const uint8_t* p) {
-  uint16_t v;
-  asm volatile("ld.global.u8 %0, [%1];" : "=h"(v) : "l"(p));
-  return (uint8_t)v;
-}
+// the pipelined mode. They are read with plain (weak, coherent-path) loads -- never the
+// non-coherent read-only path -- and only after an ld.acquire that observed the producer's
+// release, which the memory model makes sufficient for the loads to see the produced values.
+// Plain loads also let the compiler issue independent loads back to back.
+__device__ __forceinline__ uint32_t ldw32(const void* p) { return *(const uint32_t*)p; }
+__device__ __forceinline__ uint8_t ldcg_u8(const uint8_t* p) { return *p; }
 __device__ __forceinline__ uint32_t ldcg_u32(const uint8_t* p) { return ldw32(p); }
 __device__ __forceinline__ uint2 ldg8(const uint8_t* p) {
   uintptr_t a = (uintptr_t)p;
-  const uint8_t* b = (const uint8_t*)(a & ~(uintptr_t)3);
+  const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
   uint32_t sh = (uint32_t)(a & 3) * 8u;
-  uint32_t w0 = ldw32(b), w1 = ldw32(b + 4), w2 = ldw32(b + 8);
+  uint32_t w0 = b[0], w1 = b[1], w2 = b[2];
   return make_uint2(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh));
 }
 __device__ __forceinline__ uint32_t vsad8(uint2 a, uint2 b) { return __vsadu4(a.x, b.x) + __vsadu4(a.y, b.y); }
@@ -239,14 +231,25 @@ __device__ __forceinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_
 // (ox, oy); plane coordinate (r, c) is the sample at (ox + c, oy + r).
 __device__ __noinline__ void stage_window(const uint8_t* ref, int stride, int ox, int oy, Smem& sm) {
   int lane = lane_id();
-  for (int q = lane; q < 23 * 6; q += 32) {
-    int k = q / 6, w = q % 6;
-    const uint8_t* p = ref + (long)(oy - 2 + k) * stride + (ox - 2) + 4 * w;
-    uintptr_t a = (uintptr_t)p;
-    const unsigned int* b = (const unsigned int*)(a & ~(uintptr_t)3);
-    uint32_t sh = (uint32_t)(a & 3) * 8u;
-    uint32_t v = __funnelshift_r(ldw32(b), ldw32(b + 1), sh);
-    *(uint32_t*)&sm.win[k * 24 + 4 * w] = v;
+  // 23 rows x 6 words: five words per lane, all loads issued before the first use
+  uint32_t lo[5], hi[5], sh[5];
+#pragma unroll
+  for (int r = 0; r < 5; r++) {
+    int q = min(lane + 32 * r, 23 * 6 - 1);
+    int k = q / 6, w = q - 6 * (q / 6);
+    uintptr_t a = (uintptr_t)(ref + (long)(oy - 2 + k) * stride + (ox - 2) + 4 * w);
+    const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
+    sh[r] = (uint32_t)(a & 3) * 8u;
+    lo[r] = b[0];
+    hi[r] = b[1];
+  }
+#pragma unroll
+  for (int r = 0; r < 5; r++) {
+    int q = lane + 32 * r;
+    if (q < 23 * 6) {
+      int k = q / 6, w = q - 6 * (q / 6);
+      *(uint32_t*)&sm.win[k * 24 + 4 * w] = __funnelshift_r(lo[r], hi[r], sh[r]);
+    }
   }
   __syncwarp();
 }
@@ -1475,18 +1478,25 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   const uint8_t* base = ref + (long)(y0 + (lane >> 1)) * stride + x0 + (lane & 1) * 8;
   int best0 = 0, best1 = 0;
   uint32_t best_cost = UMAX;
-  int seen[5][2];
-  for (int k = 0; k < n; k++) {
-    int mx = min(max((cand[k][0] + 2) >> 2, imin0), imax0);
-    int my = min(max((cand[k][1] + 2) >> 2, imin1), imax1);
-    bool dup = false;
-    for (int j = 0; j < k; j++) dup |= (seen[j][0] == mx && seen[j][1] == my);
-    seen[k][0] = dup ? 0x7fffffff : mx;
-    seen[k][1] = dup ? 0x7fffffff : my;
-    if (dup) continue;
-    uint32_t s = wsum(vsad8(sv, ldg8(base + (long)my * stride + mx)));
-    uint32_t cost = s + mvd_cost(mx * 4 - mvp0, lambda) + mvd_cost(my * 4 - mvp1, lambda);
-    if (cost < best_cost) { best_cost = cost; best0 = mx; best1 = my; }
+  // clamped full-pel candidates, their samples loaded together, then costed in order (a
+  // repeated position is skipped)
+  int cmx[5], cmy[5];
+  uint2 cref[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    int kk = min(k, n - 1);
+    cmx[k] = min(max((cand[kk][0] + 2) >> 2, imin0), imax0);
+    cmy[k] = min(max((cand[kk][1] + 2) >> 2, imin1), imax1);
+    cref[k] = ldg8(base + (long)cmy[k] * stride + cmx[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    bool dup = k >= n;
+#pragma unroll
+    for (int j = 0; j < k; j++) dup |= (cmx[j] == cmx[k] && cmy[j] == cmy[k]);
+    uint32_t s = wsum(dup ? 0u : vsad8(sv, cref[k]));
+    uint32_t cost = s + mvd_cost(cmx[k] * 4 - mvp0, lambda) + mvd_cost(cmy[k] * 4 - mvp1, lambda);
+    if (!dup && cost < best_cost) { best_cost = cost; best0 = cmx[k]; best1 = cmy[k]; }
   }
   // diamond (enc.rs:1207-1272)
   for (int it = 0; it < 16; it++) {
@@ -1945,19 +1955,41 @@ struct PipeParams {
                // extends the padding of the macroblocks it makes final
   const int2* tasks;  // {picture * S + stream, row << 16 | first macroblock << 1 | deblock}
   int n_tasks;
+  int n_ana;          // < n_tasks: tasks[0, n_ana) analysis, [n_ana, n_tasks) deblocking, two queues
+  int deblock_sms;    // SMs whose warps take the deblocking queue first
+  int role_by_sm;     // 0: warps of blocks 0, 9, 18, ... take it first (a grid too small to reach every SM)
   int seg;
   unsigned long long timeout_ns;
 };
+__device__ __forceinline__ unsigned sm_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
 
 __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
   __shared__ Smem sm;
   const int lane = lane_id();
   const int S = fp.n_streams, H = fp.mb_h, Wm = fp.mb_w;
+  // With two queues, warps on the first deblock_sms SMs prefer deblocking segments and the others
+  // analysis segments (each SM then runs a smaller code footprint); a warp whose queue is empty
+  // takes from the other one.
+  const bool split = pp.n_ana < pp.n_tasks;
+  const int pref = split && (pp.role_by_sm ? (int)sm_id() < pp.deblock_sms : blockIdx.x % 9 == 0) ? 1 : 0;
+  bool empty[2] = {false, !split};
   while (true) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(pp.ticket, 1);
+    int t = -1;
+    if (lane == 0) {
+      for (int k = 0; k < 2 && t < 0; k++) {
+        int q = pref ^ k;
+        if (empty[q]) continue;
+        int base = q ? pp.n_ana : 0, lim = q || !split ? pp.n_tasks : pp.n_ana;
+        int v = base + atomicAdd(q ? pp.ticket + 2 : pp.ticket, 1);
+        if (v < lim) t = v; else empty[q] = true;
+      }
+    }
     t = __shfl_sync(FULL, t, 0);
-    if (t >= pp.n_tasks) break;
+    if (t < 0) break;
     if (__shfl_sync(FULL, lane == 0 ? ld_relaxed(pp.error) : 0, 0)) break;
     int2 task = __ldg(pp.tasks + t);
     int ps = task.x, f = ps / S;
@@ -2093,11 +2125,19 @@ void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, in
   wavefront_step_kernel<<<grid, 32, 0, st>>>(fp, d_streams, step);
 }
 
-int pipeline_grid(int device) {
-  int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel, 32, 0);
+int pipeline_sms(int device) {
+  int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return per_sm * sms;
+  return sms;
+}
+
+// Resident warps of the pipelined mode: six per SM (fewer when they do not fit). More warps
+// overlap more waits but slow every macroblock on the critical path (measured on B200: 4-8 per
+// SM within 3 % of each other, 20 per SM 10 % slower).
+int pipeline_grid(int device) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel, 32, 0);
+  return (per_sm < 6 ? per_sm : 6) * pipeline_sms(device);
 }
 
 // Work list of the pipelined mode, written to `tasks` (pipeline_task_count entries): every
@@ -2112,40 +2152,46 @@ int pipeline_grid(int device) {
 // (x + 1, y - 1)), so warps taking tickets in order never wait for an untaken segment of the same
 // picture. The wait for the reference picture depends on the motion vectors: a search whose
 // window reaches r macroblocks beyond the co-located ones (r = 0 for zero motion) waits for a
-// smaller key when lag >= a * (4 + r) + seg + r + 3. lag <= 0 takes r = 6 (about 96 samples).
+// smaller key when lag >= a * (4 + r) + seg + r + 3. lag <= 0 takes r = 4 (about 64 samples).
 size_t pipeline_task_count(const FrameParams& fp, int frames, int seg) {
   size_t segs = (size_t)(fp.mb_w + seg - 1) / seg;
   return 2 * (size_t)frames * fp.n_streams * fp.mb_h * segs;
 }
 
-size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, int2* tasks) {
+size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, int2* tasks, size_t* n_ana) {
   int S = fp.n_streams, H = fp.mb_h, W = fp.mb_w;
   int segs = (W + seg - 1) / seg, a = seg > 2 ? seg : 2;
-  if (lag <= 0) lag = a * 10 + seg + 9;
+  if (lag <= 0) lag = a * 8 + seg + 7;
   auto key = [&](int f, int role, int y, int k) {
     return (size_t)a * (y + role) + (size_t)k * seg + role + (size_t)lag * f;
   };
-  size_t n_keys = key(frames - 1, 1, H - 1, segs - 1) + 1;
+  // split: analysis keys first, then deblocking keys shifted past them (two queues, each in
+  // key order)
+  size_t n_keys1 = key(frames - 1, 1, H - 1, segs - 1) + 1;
+  size_t shift = split ? n_keys1 : 0, n_keys = n_keys1 + shift;
+  auto slot = [&](int f, int role, int y, int k) { return key(f, role, y, k) + (role ? shift : 0); };
   std::vector<size_t> start(n_keys + 1, 0);
   for (int f = 0; f < frames; f++)
     for (int role = 0; role < 2; role++)
       for (int y = 0; y < H; y++)
-        for (int k = 0; k < segs; k++) start[key(f, role, y, k) + 1] += S;
+        for (int k = 0; k < segs; k++) start[slot(f, role, y, k) + 1] += S;
   for (size_t i = 0; i < n_keys; i++) start[i + 1] += start[i];
+  *n_ana = split ? start[n_keys1] : pipeline_task_count(fp, frames, seg);
   // placed in (picture, role, stream, row, segment) order within a key: a stable counting sort
   for (int f = 0; f < frames; f++)
     for (int role = 0; role < 2; role++)
       for (int s = 0; s < S; s++)
         for (int y = 0; y < H; y++)
           for (int k = 0; k < segs; k++) {
-            size_t at = start[key(f, role, y, k)]++;
+            size_t at = start[slot(f, role, y, k)]++;
             tasks[at] = make_int2(f * S + s, (y << 16) | ((k * seg) << 1) | role);
           }
   return pipeline_task_count(fp, frames, seg);
 }
 
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
-                     size_t n_tasks, int seg, int grid, unsigned long long timeout_ns, cudaStream_t st) {
+                     size_t n_tasks, size_t n_ana, int deblock_sms, int sms, int seg, int grid,
+                     unsigned long long timeout_ns, cudaStream_t st) {
   int S = fp.n_streams, H = fp.mb_h;
   PipeParams pp;
   pp.ticket = counters;
@@ -2154,6 +2200,9 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.db = pp.ana + frames * S * H;
   pp.tasks = d_tasks;
   pp.n_tasks = (int)n_tasks;
+  pp.n_ana = (int)n_ana;
+  pp.deblock_sms = deblock_sms;
+  pp.role_by_sm = grid >= sms;
   pp.seg = seg;
   pp.timeout_ns = timeout_ns;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;

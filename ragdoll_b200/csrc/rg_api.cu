@@ -21,7 +21,9 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the segment length
-constexpr int kDefaultSeg = 8;   // macroblocks per work segment
+constexpr int kDefaultSeg = 2;   // macroblocks per work segment
+// Deblocking is about a tenth of the work: one SM in nine takes its queue first (16 of 148).
+int default_deblock_sms(int sms) { return sms >= 9 ? (sms + 4) / 9 : 0; }
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -115,9 +117,11 @@ struct rg_ctx {
   int lag = kDefaultLag;           // macroblock-times between pictures of a stream in the work order
   int seg = kDefaultSeg;           // macroblocks per work segment
   unsigned long long timeout_ns = 2000000000ull;  // limit of one device wait
+  int deblock_sms = 0;             // SMs preferring deblocking segments (0 = one mixed queue)
+  int sms = 0;
   int2* d_tasks = nullptr;         // work list of the pipelined mode
-  size_t tasks_cap = 0, n_tasks = 0;
-  int tasks_frames = -1, tasks_lag = -1, tasks_seg = -1;  // what d_tasks holds
+  size_t tasks_cap = 0, n_tasks = 0, n_ana = 0;
+  int tasks_frames = -1, tasks_lag = -1, tasks_seg = -1, tasks_split = -1;  // what d_tasks holds
   std::vector<int2> h_tasks;
   // the pending pipelined call, kept to re-run it on the per-diagonal path after a failed wait
   std::vector<const uint8_t*> pend_planes;
@@ -240,6 +244,8 @@ rg_ctx* rg_create(const rg_config* cfg) {
   }
   *c->h_err = 0;
   c->grid = pipeline_grid(cfg->device);
+  c->sms = pipeline_sms(cfg->device);
+  c->deblock_sms = default_deblock_sms(c->sms);
   upload_tables();
   if (cudaDeviceSynchronize() != cudaSuccess) {
     fail(RG_ERR_CUDA, "rg_create: %s", cudaGetErrorString(cudaGetLastError()));
@@ -414,18 +420,20 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
   CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * S * frames, cudaMemcpyHostToDevice, c->stream));
   CK(cudaEventRecord(c->slot_done[slot], c->stream));
   CK(cudaMemsetAsync(c->counters, 0, sizeof(int) * pipeline_counter_ints(c->fp, frames), c->stream));
-  if (frames != c->tasks_frames || c->lag != c->tasks_lag || c->seg != c->tasks_seg) {
+  int split = c->deblock_sms > 0 && c->grid >= 2 ? 1 : 0;
+  if (frames != c->tasks_frames || c->lag != c->tasks_lag || c->seg != c->tasks_seg || split != c->tasks_split) {
     // rebuilt only when the call's shape or the tuning changes; the copy is stream-ordered
     // after any launch still reading the old list
     c->h_tasks.resize(pipeline_task_count(fp, frames, c->seg));
-    c->n_tasks = pipeline_task_list(fp, frames, c->lag, c->seg, c->h_tasks.data());
+    c->n_tasks = pipeline_task_list(fp, frames, c->lag, c->seg, split != 0, c->h_tasks.data(), &c->n_ana);
     CK(cudaMemcpyAsync(c->d_tasks, c->h_tasks.data(), sizeof(int2) * c->n_tasks, cudaMemcpyHostToDevice, c->stream));
     c->tasks_frames = frames;
     c->tasks_lag = c->lag;
     c->tasks_seg = c->seg;
+    c->tasks_split = split;
   }
-  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->seg, c->grid, c->timeout_ns,
-                  c->stream);
+  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->n_ana, c->deblock_sms, c->sms,
+                  c->seg, c->grid, c->timeout_ns, c->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_err, c->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   c->pend_planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
@@ -448,11 +456,13 @@ int rg_copy_records_gops(rg_ctx* c, int32_t frames, rg_mb_out* out) {
   return RG_OK;
 }
 
-int rg_set_pipeline_tuning(rg_ctx* c, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms) {
+int rg_set_pipeline_tuning(rg_ctx* c, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms,
+                           int32_t deblock_sms) {
   if (!c) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: null context");
   if (lag < 0 || lag > 4096) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: lag %d outside 0..4096", lag);
   if (seg < 0 || seg > c->fp.mb_w) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: seg %d outside 0..%d", seg, c->fp.mb_w);
-  if (grid < 0 || timeout_ms < 0) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: negative argument");
+  if (grid < 0 || timeout_ms < 0 || deblock_sms < -1)
+    return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: negative argument");
   CK(cudaStreamSynchronize(c->stream));
   int new_seg = seg > 0 ? seg : kDefaultSeg;
   if (new_seg > c->fp.mb_w) new_seg = c->fp.mb_w;
@@ -467,6 +477,7 @@ int rg_set_pipeline_tuning(rg_ctx* c, int32_t lag, int32_t seg, int32_t grid, in
   }
   c->lag = lag > 0 ? lag : kDefaultLag;
   c->seg = new_seg;
+  c->deblock_sms = deblock_sms < 0 ? 0 : (deblock_sms > 0 ? deblock_sms : default_deblock_sms(c->sms));
   c->tasks_frames = -1;
   if (grid > 0) c->grid = grid;
   else c->grid = pipeline_grid(c->cfg.device);

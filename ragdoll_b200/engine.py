@@ -101,7 +101,8 @@ def lib() -> ctypes.CDLL:
     L.rg_analyse_gops.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_analyse_gops_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32]
     L.rg_copy_records_gops.argtypes = [P, ctypes.c_int32, P]
-    L.rg_set_pipeline_tuning.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    L.rg_set_pipeline_tuning.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.c_int32]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
     _lib = L
@@ -202,11 +203,12 @@ class Engine:
         k = (ctypes.c_int32 * len(kinds))(*kinds)
         _check(lib().rg_analyse_gops_device(self.h, planes, stride_y, stride_uv, k, frames))
 
-    def set_pipeline_tuning(self, lag: int = 0, seg: int = 0, grid: int = 0, timeout_ms: int = 0) -> None:
+    def set_pipeline_tuning(self, lag: int = 0, seg: int = 0, grid: int = 0, timeout_ms: int = 0,
+                            deblock_sms: int = 0) -> None:
         """Pipelined-mode work order (0 = library defaults): lag macroblock-times between the
-        pictures of a stream, seg macroblocks per work segment, grid resident warps, and the limit
-        of one device wait."""
-        _check(lib().rg_set_pipeline_tuning(self.h, lag, seg, grid, timeout_ms))
+        pictures of a stream, seg macroblocks per work segment, grid resident warps, the limit
+        of one device wait, and the SMs that take deblocking segments first (-1 = one mixed queue)."""
+        _check(lib().rg_set_pipeline_tuning(self.h, lag, seg, grid, timeout_ms, deblock_sms))
 
     def records_gops(self, frames: int) -> np.ndarray:
         out = np.zeros((frames, self.num_streams, self.n_mb), RECORD_DTYPE)

@@ -61,20 +61,26 @@ def test_batched_streams_match_single():
             assert all(np.array_equal(a, b) for a, b in zip(batch.recon(s), solo[s].recon()))
 
 
-@pytest.mark.parametrize("w,h,qp,profile,streams,frames", [
-    (176, 144, 26, 2, 3, 5),
-    (250, 138, 30, 0, 2, 4),
-    (64, 32, 22, 1, 4, 6),
+@pytest.mark.parametrize("w,h,qp,profile,streams,frames,tuning", [
+    (176, 144, 26, 2, 3, 5, {}),
+    (250, 138, 30, 0, 2, 4, {}),
+    (64, 32, 22, 1, 4, 6, {}),
+    (176, 144, 26, 2, 3, 5, {"deblock_sms": -1, "seg": 8}),
+    (208, 120, 24, 2, 2, 5, {"deblock_sms": 16, "grid": 64, "lag": 40}),
 ])
-def test_pipelined_gops_match_oracle(w, h, qp, profile, streams, frames):
+def test_pipelined_gops_match_oracle(w, h, qp, profile, streams, frames, tuning):
     """One persistent launch for all pictures of several GOPs (pictures of a GOP overlapping)
-    gives the oracle's records and deblocked reconstruction for every picture."""
+    gives the oracle's records and deblocked reconstruction for every picture -- with separate
+    analysis / deblocking queues (default) or one mixed queue, at several segment lengths, lags
+    and grid sizes."""
     from oracle_lib import OracleEncoder
     from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
     from gpu_parity_util import first_record_mismatch, first_pixel_mismatch
 
     clips = [grating_clip(w, h, frames, seed=100 + 7 * s + w, motion=6.0, rects=2) for s in range(streams)]
     eng = Engine(w, h, qp, profile=profile, num_streams=streams, max_frames=frames)
+    if tuning:
+        eng.set_pipeline_tuning(**tuning)
     kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * streams for f in range(frames)]
     recs = eng.analyse_gops([[clips[s][f] for s in range(streams)] for f in range(frames)], kinds)
     for s in range(streams):
