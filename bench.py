@@ -42,6 +42,9 @@ MOTION, RECTS = 24.0, 12
 METRIC = "1080p H.264 encode frames/s (plain GPU form: analysis + reconstruction + deblocking)"
 UNIT = "frames/s"
 BYTES_PER_FRAME = 7.5 * W * H  # source 1.5 + reference 1.5 + recon 1.5 + deblock read/write 3.0 (x W*H)
+# DRAM bytes per picture of pipeline_kernel measured by ncu (dram__bytes_read + write) on a launch
+# of 8 streams x 4 pictures of this workload: 481.4 MB / 32 (scaled to a launch by its pictures).
+TRAFFIC_PER_FRAME = 481.4e6 / 32
 
 
 def dist_env():
@@ -298,7 +301,8 @@ def run_engine(args, rank, world, local):
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
                     "d2h_bytes_per_step": GOP * gops * eng.n_mb * 852},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 5), "traffic": None,
+                         "frac": round(achieved / peak, 5),
+                         "traffic": round(TRAFFIC_PER_FRAME * FRAMES) if args.mode == "pipelined" else None,
                          "kernel": kernel_name, "launch_ms": round(launch_ms, 5),
                          "bytes_per_launch": round(bytes_per_launch)},
             "cpu_baseline": cpu,
