@@ -195,15 +195,27 @@ def run_engine(args, rank, world, local):
         for g in range(gops):
             gop_ptrs += planes(g * GOP + i)
             gop_kinds.append(RG_FRAME_IDR if i == 0 else RG_FRAME_P)
-    frames_host = [[clip[g * GOP + i] for g in range(gops)] for i in range(GOP)]
+    # end-to-end inputs and outputs in pinned host memory, allocated once (the public host-buffer
+    # API copies from / to them every step)
+    pinned = torch.from_numpy(host).pin_memory()
+    ph = pinned.numpy()
+
+    def host_planes(i):
+        return (ph[i, :W * H].reshape(H, W), ph[i, W * H:W * H + cw * ch].reshape(ch, cw),
+                ph[i, W * H + cw * ch:].reshape(ch, cw))
+
+    frames_host = [[host_planes(g * GOP + i) for g in range(gops)] for i in range(GOP)]
     kinds_host = [[RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops for i in range(GOP)]
+    from ragdoll_b200.engine import RECORD_DTYPE
+    rec_pinned = torch.empty(GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    rec_host = rec_pinned.numpy().view(RECORD_DTYPE).reshape(GOP, gops, eng.n_mb)
 
     if args.mode == "pipelined":
         def device_step():
             eng.analyse_gops_device(gop_ptrs, W, cw, gop_kinds, GOP)
 
         def host_step():
-            eng.analyse_gops(frames_host, kinds_host)
+            eng.analyse_gops(frames_host, kinds_host, out=rec_host)
     else:
         def device_step():
             for i in range(GOP):

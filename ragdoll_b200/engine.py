@@ -176,9 +176,10 @@ class Engine:
         k = (ctypes.c_int32 * self.num_streams)(*kinds)
         _check(lib().rg_analyse_batch_device(self.h, planes, stride_y, stride_uv, k))
 
-    def analyse_gops(self, frames, kinds) -> np.ndarray:
+    def analyse_gops(self, frames, kinds, out: np.ndarray | None = None) -> np.ndarray:
         """Pipelined form: ``frames[f][s]`` is picture f of stream s (host planes), ``kinds[f][s]``
-        its kind; all pictures in one persistent launch. Returns records ``[F, S, n_mb]``."""
+        its kind; all pictures in one persistent launch. Returns records ``[F, S, n_mb]``, written
+        into ``out`` when given (e.g. a view of pinned memory reused across calls)."""
         F, S = len(frames), self.num_streams
         planes = (ctypes.c_void_p * (3 * S * F))()
         keep = []
@@ -186,14 +187,17 @@ class Engine:
         for f in range(F):
             assert len(frames[f]) == S
             for s, (y, u, v) in enumerate(frames[f]):
-                y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (y, u, v))
+                y, u, v = (p if p.dtype == np.uint8 and p.strides[-1] == 1 else np.ascontiguousarray(p, dtype=np.uint8)
+                           for p in (y, u, v))
                 keep += [y, u, v]
                 if sy is None:
                     sy, suv = y.strides[0], u.strides[0]
                 i = (f * S + s) * 3
                 planes[i], planes[i + 1], planes[i + 2] = y.ctypes.data, u.ctypes.data, v.ctypes.data
         k = (ctypes.c_int32 * (S * F))(*[kinds[f][s] for f in range(F) for s in range(S)])
-        out = np.zeros((F, S, self.n_mb), RECORD_DTYPE)
+        if out is None:
+            out = np.zeros((F, S, self.n_mb), RECORD_DTYPE)
+        assert out.shape == (F, S, self.n_mb) and out.dtype == RECORD_DTYPE and out.flags.c_contiguous
         _check(lib().rg_analyse_gops(self.h, planes, sy, suv, k, F, out.ctypes.data))
         return out
 
