@@ -207,15 +207,20 @@ def run_engine(args, rank, world, local):
     frames_host = [[host_planes(g * GOP + i) for g in range(gops)] for i in range(GOP)]
     kinds_host = [[RG_FRAME_IDR if i == 0 else RG_FRAME_P] * gops for i in range(GOP)]
     from ragdoll_b200.engine import RECORD_DTYPE
-    rec_pinned = torch.empty(GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
-    rec_host = rec_pinned.numpy().view(RECORD_DTYPE).reshape(GOP, gops, eng.n_mb)
+    rec_pinned = [torch.empty(GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+                  for _ in range(2)]
+    rec_host = [r.numpy().view(RECORD_DTYPE).reshape(GOP, gops, eng.n_mb) for r in rec_pinned]
+    e2e_calls = [0]
 
     if args.mode == "pipelined":
         def device_step():
             eng.analyse_gops_device(gop_ptrs, W, cw, gop_kinds, GOP)
 
         def host_step():
-            eng.analyse_gops(frames_host, kinds_host, out=rec_host)
+            # asynchronous host-buffer calls: copy-in of this step and copy-out of the last one
+            # overlap the launches; records land in alternating pinned buffers
+            eng.analyse_gops_async(frames_host, kinds_host, rec_host[e2e_calls[0] % 2])
+            e2e_calls[0] += 1
     else:
         def device_step():
             for i in range(GOP):
@@ -261,11 +266,13 @@ def run_engine(args, rank, world, local):
 
     # end to end through the host-buffer C ABI (records copied back every batch)
     host_step()
+    eng.sync()
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         host_step()
+    eng.sync()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps)
 

@@ -162,8 +162,22 @@ int rg_analyse_gops_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t
 int rg_analyse_gops(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
                     const int32_t* kinds, int32_t frames, rg_mb_out* out);
 
-/* Copies the records of the last `frames` pictures of an rg_analyse_gops* call. */
+/* Copies the records of the last `frames` pictures of an rg_analyse_gops / _device call. */
 int rg_copy_records_gops(rg_ctx* ctx, int32_t frames, rg_mb_out* out);
+
+/*
+ * Asynchronous host-buffer form of rg_analyse_gops, for a caller that encodes batch after batch
+ * (GopRingEncoder::encode_wave, crates/ragdoll-pipeline/src/lib.rs:543, one wave per call): the
+ * call queues the copy of the sources in, the launch, and the copy of the records out into `out`
+ * (frames * num_streams * mb_w * mb_h records, picture-major) and returns. The copy in of one call
+ * overlaps the launch of the previous call and its copy out the launch of the next, when `planes`
+ * and `out` are in pinned host memory (cudaHostAlloc). The sources may be reused, and `out` read,
+ * after rg_sync. Two calls' staging are kept on the device (allocated by the first call). A call
+ * whose device wait gave up is re-run on the per-diagonal path before the next call starts (or in
+ * rg_sync) and its records copied again, so results are always exact.
+ */
+int rg_analyse_gops_async(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                          const int32_t* kinds, int32_t frames, rg_mb_out* out);
 
 /*
  * Tuning / test hook of the pipelined mode: lag = macroblock-times between consecutive pictures

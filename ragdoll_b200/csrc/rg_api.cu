@@ -129,6 +129,17 @@ struct rg_ctx {
   std::vector<int> pend_start;
   int pend_frames = 0;
   size_t pend_sy = 0, pend_suv = 0;
+  rg_mb_out* pend_rec = nullptr;   // where the pending call's records go
+  rg_mb_out* pend_out = nullptr;   // host copy of them queued by an asynchronous call
+  size_t pend_out_bytes = 0;
+  // asynchronous host-buffer calls (rg_analyse_gops_async): two slots of source staging and
+  // records, a copy-in and a copy-out stream; allocated on the first such call
+  uint8_t* a_srcs[2] = {nullptr, nullptr};
+  rg_mb_out* a_recs[2] = {nullptr, nullptr};
+  cudaStream_t a_in = nullptr, a_out = nullptr;
+  cudaEvent_t a_in_done[2] = {nullptr, nullptr}, a_kern_done[2] = {nullptr, nullptr};
+  cudaEvent_t a_out_done[2] = {nullptr, nullptr};
+  int a_slot = 0;
   std::vector<int> frames;         // frames analysed per stream
   // metrics scratch
   float* m_rows = nullptr;
@@ -274,6 +285,16 @@ void rg_destroy(rg_ctx* c) {
   cudaFree(c->m_src);
   cudaFree(c->counters);
   cudaFree(c->d_tasks);
+  if (c->a_in) cudaStreamSynchronize(c->a_in);
+  if (c->a_out) cudaStreamSynchronize(c->a_out);
+  for (int i = 0; i < 2; i++) {
+    cudaFree(c->a_srcs[i]);
+    cudaFree(c->a_recs[i]);
+    for (cudaEvent_t e : {c->a_in_done[i], c->a_kern_done[i], c->a_out_done[i]})
+      if (e) cudaEventDestroy(e);
+  }
+  if (c->a_in) cudaStreamDestroy(c->a_in);
+  if (c->a_out) cudaStreamDestroy(c->a_out);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->h_streams[0]) cudaFreeHost(c->h_streams[0]);
   if (c->h_streams[1]) cudaFreeHost(c->h_streams[1]);
@@ -304,9 +325,13 @@ void* rg_cuda_stream(rg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                              const int32_t* kinds, rg_mb_out* rec_base);
+static int resolve_pending(rg_ctx* c, bool wait_out);
 
 int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                             const int32_t* kinds) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_analyse_batch_device: null context");
+  int r = resolve_pending(c, false);
+  if (r) return r;
   return enqueue_wavefront(c, dev_planes, stride_y, stride_uv, kinds, nullptr);
 }
 
@@ -369,8 +394,11 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
   return RG_OK;
 }
 
-int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                           const int32_t* kinds, int32_t frames) {
+// One persistent launch for `frames` pictures of every stream; records at rec_base. The previous
+// pipelined call is resolved first (waited for, and re-run on the per-diagonal path if one of its
+// waits gave up), so a call never starts from the pictures of a failed one.
+static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
+                        const int32_t* kinds, int32_t frames, rg_mb_out* rec_base) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null argument");
   if (frames < 1 || frames > c->max_frames)
     return fail(RG_ERR_INVALID, "rg_analyse_gops_device: frames %d outside 1..%d (rg_config.max_frames)", frames,
@@ -378,6 +406,10 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
   if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
     return fail(RG_ERR_INVALID, "rg_analyse_gops_device: stride too small");
   int S = c->S;
+  {
+    int r = resolve_pending(c, false);
+    if (r) return r;
+  }
   for (int f = 0; f < frames; f++)
     for (int s = 0; s < S; s++) {
       int k = kinds[f * S + s];
@@ -409,7 +441,7 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
       d.ref_v = c->pic_plane(s, prv, 2);
       d.info = c->infos + ((size_t)s * c->nslots + cur) * c->n_mb;
       d.prev_info = c->infos + ((size_t)s * c->nslots + prv) * c->n_mb;
-      d.rec = c->recs + ((size_t)f * S + s) * c->n_mb;
+      d.rec = rec_base + ((size_t)f * S + s) * c->n_mb;
       d.unf_y = d.unf_u = d.unf_v = nullptr;
       d.kind = kinds[f * S + s];
       d.pad_ = 0;
@@ -442,8 +474,16 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
   c->pend_frames = frames;
   c->pend_sy = stride_y;
   c->pend_suv = stride_uv;
+  c->pend_rec = rec_base;
+  c->pend_out = nullptr;
   for (int s = 0; s < S; s++) c->frames[s] += frames;
   return RG_OK;
+}
+
+int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
+                           const int32_t* kinds, int32_t frames) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null context");
+  return enqueue_gops(c, dev_planes, stride_y, stride_uv, kinds, frames, c->recs);
 }
 
 int rg_copy_records_gops(rg_ctx* c, int32_t frames, rg_mb_out* out) {
@@ -512,27 +552,89 @@ int rg_analyse_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, si
   return rg_sync(c);
 }
 
-int rg_sync(rg_ctx* c) {
-  if (!c) return fail(RG_ERR_INVALID, "rg_sync: null context");
+// Waits for the queued work of the context. If a wait of the last pipelined launch gave up (a
+// search reaching further than the picture lag allows, or another warp failing), every picture of
+// that call wrote its own ring slot and the reference it started from is untouched, so the call is
+// re-run, picture by picture, on the per-diagonal path, which has no waits; results are identical.
+// An asynchronous call's host copy of its records is then made again. wait_out: also wait for the
+// copy-out stream of asynchronous calls.
+static int resolve_pending(rg_ctx* c, bool wait_out) {
   CK(cudaStreamSynchronize(c->stream));
   if (*c->h_err) {
-    // A wait of the pipelined launch gave up (a search reaching further than the picture lag
-    // allows, or a fault of another warp). Every picture of the call wrote its own ring slot and
-    // the reference it started from is untouched, so the call is re-run, picture by picture, on
-    // the per-diagonal path, which has no waits. Results are identical.
     *c->h_err = 0;
     if (c->pend_frames == 0) return fail(RG_ERR_TIMEOUT, "rg_sync: a device wait gave up");
+    if (c->a_out) CK(cudaStreamSynchronize(c->a_out));  // its copy of the failed records may run
     int S = c->S, F = c->pend_frames;
     c->frames = c->pend_start;
     c->pend_frames = 0;
     for (int f = 0; f < F; f++) {
       int r = enqueue_wavefront(c, c->pend_planes.data() + (size_t)f * S * 3, c->pend_sy, c->pend_suv,
-                                c->pend_kinds.data() + (size_t)f * S, c->recs + (size_t)f * S * c->n_mb);
+                                c->pend_kinds.data() + (size_t)f * S, c->pend_rec + (size_t)f * S * c->n_mb);
       if (r) return r;
     }
     CK(cudaStreamSynchronize(c->stream));
+    if (c->pend_out) CK(cudaMemcpy(c->pend_out, c->pend_rec, c->pend_out_bytes, cudaMemcpyDeviceToHost));
   }
+  if (wait_out && c->a_out) CK(cudaStreamSynchronize(c->a_out));
   c->pend_frames = 0;
+  c->pend_out = nullptr;
+  return RG_OK;
+}
+
+int rg_sync(rg_ctx* c) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_sync: null context");
+  return resolve_pending(c, true);
+}
+
+int rg_analyse_gops_async(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                          const int32_t* kinds, int32_t frames, rg_mb_out* out) {
+  if (!c || !planes || !kinds || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: null argument");
+  if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: frames %d", frames);
+  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: stride too small");
+  int S = c->S;
+  for (int i = 0; i < 3 * S * frames; i++)
+    if (!planes[i]) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: picture %d stream %d null plane", i / 3 / S, (i / 3) % S);
+  if (!c->a_in) {
+    size_t nsrc = c->src_bytes() * S * c->max_frames, nrec = sizeof(rg_mb_out) * c->n_mb * S * c->max_frames;
+    for (int i = 0; i < 2; i++) {
+      if (cudaMalloc((void**)&c->a_srcs[i], nsrc) != cudaSuccess || cudaMalloc((void**)&c->a_recs[i], nrec) != cudaSuccess)
+        return fail(RG_ERR_OOM, "rg_analyse_gops_async: staging of %zu + %zu bytes", nsrc, nrec);
+      for (cudaEvent_t* e : {&c->a_in_done[i], &c->a_kern_done[i], &c->a_out_done[i]})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    CK(cudaStreamCreateWithFlags(&c->a_out, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->a_in, cudaStreamNonBlocking));
+  }
+  int slot = c->a_slot;
+  c->a_slot ^= 1;
+  // sources into this slot's staging once the launch that last read it is done
+  CK(cudaStreamWaitEvent(c->a_in, c->a_kern_done[slot], 0));
+  std::vector<const uint8_t*> dev(3 * (size_t)S * frames);
+  for (int i = 0; i < S * frames; i++) {
+    const uint8_t* const* pl = planes + 3 * i;
+    uint8_t* d = c->a_srcs[slot] + c->src_bytes() * i;
+    CK(cudaMemcpy2DAsync(d, w, pl[0], stride_y, w, h, cudaMemcpyHostToDevice, c->a_in));
+    CK(cudaMemcpy2DAsync(d + (size_t)w * h, cw, pl[1], stride_uv, cw, ch, cudaMemcpyHostToDevice, c->a_in));
+    CK(cudaMemcpy2DAsync(d + (size_t)w * h + (size_t)cw * ch, cw, pl[2], stride_uv, cw, ch, cudaMemcpyHostToDevice,
+                         c->a_in));
+    dev[3 * i] = d;
+    dev[3 * i + 1] = d + (size_t)w * h;
+    dev[3 * i + 2] = d + (size_t)w * h + (size_t)cw * ch;
+  }
+  CK(cudaEventRecord(c->a_in_done[slot], c->a_in));
+  // the launch waits for its sources and for the copy-out of this slot's previous records
+  CK(cudaStreamWaitEvent(c->stream, c->a_in_done[slot], 0));
+  CK(cudaStreamWaitEvent(c->stream, c->a_out_done[slot], 0));
+  int r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot]);
+  if (r) return r;
+  CK(cudaEventRecord(c->a_kern_done[slot], c->stream));
+  size_t bytes = sizeof(rg_mb_out) * c->n_mb * S * frames;
+  CK(cudaStreamWaitEvent(c->a_out, c->a_kern_done[slot], 0));
+  CK(cudaMemcpyAsync(out, c->a_recs[slot], bytes, cudaMemcpyDeviceToHost, c->a_out));
+  CK(cudaEventRecord(c->a_out_done[slot], c->a_out));
+  c->pend_out = out;
+  c->pend_out_bytes = bytes;
   return RG_OK;
 }
 
@@ -557,6 +659,10 @@ static int upload_planes(rg_ctx* c, int s, const uint8_t* y, const uint8_t* u, c
 int rg_analyse_batch(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
                      rg_mb_out* out) {
   if (!c || !planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_batch: null argument");
+  {
+    int r = resolve_pending(c, false);
+    if (r) return r;
+  }
   int w = c->cfg.width, cw = (w + 1) / 2;
   if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "rg_analyse_batch: stride too small");
   std::vector<const uint8_t*> dev(3 * c->S);

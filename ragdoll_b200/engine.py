@@ -38,7 +38,7 @@ EXPORTS = [
     "rg_analyse_batch", "rg_analyse_batch_device", "rg_sync", "rg_copy_records", "rg_get_recon",
     "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
     "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc", "rg_analyse_gops",
-    "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning",
+    "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_analyse_gops_async",
 ]
 
 
@@ -101,6 +101,7 @@ def lib() -> ctypes.CDLL:
     L.rg_analyse_gops.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_analyse_gops_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32]
     L.rg_copy_records_gops.argtypes = [P, ctypes.c_int32, P]
+    L.rg_analyse_gops_async.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_set_pipeline_tuning.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                          ctypes.c_int32]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
@@ -200,6 +201,26 @@ class Engine:
         assert out.shape == (F, S, self.n_mb) and out.dtype == RECORD_DTYPE and out.flags.c_contiguous
         _check(lib().rg_analyse_gops(self.h, planes, sy, suv, k, F, out.ctypes.data))
         return out
+
+    def analyse_gops_async(self, frames, kinds, out: np.ndarray) -> None:
+        """Queues ``analyse_gops`` and returns: the records land in ``out`` ([F, S, n_mb]) and the
+        sources may be reused after ``sync()``. Pinned ``frames``/``out`` let the copies overlap the
+        launches of neighbouring calls."""
+        F, S = len(frames), self.num_streams
+        assert out.shape == (F, S, self.n_mb) and out.dtype == RECORD_DTYPE and out.flags.c_contiguous
+        planes = (ctypes.c_void_p * (3 * S * F))()
+        sy = suv = None
+        for f in range(F):
+            assert len(frames[f]) == S
+            for s, (y, u, v) in enumerate(frames[f]):
+                for p in (y, u, v):
+                    assert p.dtype == np.uint8 and p.strides[-1] == 1
+                if sy is None:
+                    sy, suv = y.strides[0], u.strides[0]
+                i = (f * S + s) * 3
+                planes[i], planes[i + 1], planes[i + 2] = y.ctypes.data, u.ctypes.data, v.ctypes.data
+        k = (ctypes.c_int32 * (S * F))(*[kinds[f][s] for f in range(F) for s in range(S)])
+        _check(lib().rg_analyse_gops_async(self.h, planes, sy, suv, k, F, out.ctypes.data))
 
     def analyse_gops_device(self, dev_planes, stride_y: int, stride_uv: int, kinds, frames: int) -> None:
         """Queues ``frames`` pictures of every stream from device planes ([f][s][y,u,v])."""

@@ -119,3 +119,31 @@ def test_pipelined_wait_timeout_falls_back_to_exact_path():
     eng.set_pipeline_tuning()
     more = grating_clip(w, h, 2, seed=78, motion=4.0, rects=1)
     eng.analyse_gops([[more[0]], [more[1]]], [[RG_FRAME_P], [RG_FRAME_P]])
+
+
+def test_async_gops_match_sync_and_recover_from_timeout():
+    """Asynchronous host-buffer calls, queued back to back into alternating output buffers, give
+    the records of the synchronous call; a call whose wait is made to run out (one warp, lag 1)
+    is re-run before the next call starts, and its records in the caller's buffer are exact."""
+    from ragdoll_b200.engine import RECORD_DTYPE, RG_FRAME_IDR, RG_FRAME_P, Engine
+    w, h, qp, S, F = 176, 144, 26, 3, 4
+    clips = [grating_clip(w, h, 2 * F, seed=500 + s, motion=5.0, rects=2) for s in range(S)]
+    batches = [[[clips[s][b * F + f] for s in range(S)] for f in range(F)] for b in range(2)]
+    kinds = [[[RG_FRAME_IDR if (b == 0 and f == 0) else RG_FRAME_P] * S for f in range(F)] for b in range(2)]
+
+    sync = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+    want = [sync.analyse_gops(batches[b], kinds[b]) for b in range(2)]
+
+    for tuning in ({}, {"lag": 1, "grid": 1, "timeout_ms": 300}):
+        eng = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+        if tuning:
+            eng.set_pipeline_tuning(**tuning)
+        outs = [np.zeros((F, S, eng.n_mb), RECORD_DTYPE) for _ in range(2)]
+        for b in range(2):
+            eng.analyse_gops_async(batches[b], kinds[b], outs[b])
+        eng.sync()
+        for b in range(2):
+            assert outs[b].tobytes() == want[b].tobytes(), f"{tuning} batch {b}"
+        for s in range(S):
+            for a, c in zip(sync.recon_coded(s), eng.recon_coded(s)):
+                assert np.array_equal(a, c)
