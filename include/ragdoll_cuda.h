@@ -268,6 +268,25 @@ int rg_ssim_plane_device_noalloc(const uint8_t* dev_a, size_t stride_a, const ui
                                  size_t stride_b, int32_t width, int32_t height, double* dev_out,
                                  void* cuda_stream);
 
+/* ---- CAVLC bitstream writer (host) ------------------------------------------------------ */
+/*
+ * The serial half of encode_frame_body (crates/ragdoll-codec/src/h264/enc.rs:2234) for the
+ * Baseline profile: turns one picture's records into its Annex-B access unit -- SPS and PPS
+ * before an IDR (h264.rs:556-660, 806-832), the slice header (h264.rs:1071), skip runs and the
+ * macroblock layer (enc.rs:989-1054, 3260-3285, 3540-3577, 3736-3750), CAVLC residual blocks
+ * (h264.rs:2215 encode_cavlc_block) and NAL packing with emulation prevention (h264.rs:189).
+ * Host code only; one writer per stream, usable from one thread each. Main / High use CABAC:
+ * rg_writer_create returns NULL (RG_ERR_UNSUPPORTED) for them.
+ */
+typedef struct rg_writer rg_writer;
+rg_writer* rg_writer_create(const rg_config* cfg, int32_t fps_num, int32_t fps_den);
+void rg_writer_destroy(rg_writer* writer);
+/* A buffer size that always holds one access unit of this writer. */
+size_t rg_writer_bound(const rg_writer* writer);
+/* Writes the access unit of one picture (records: mb_w * mb_h, raster order; kind RG_FRAME_*)
+ * into out; returns its size in bytes, or a negative RG_ERR_* (the buffer too small included). */
+int64_t rg_writer_picture(rg_writer* writer, const rg_mb_out* records, int32_t kind, uint8_t* out, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,6 +39,7 @@ EXPORTS = [
     "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
     "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc", "rg_analyse_gops",
     "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_analyse_gops_async",
+    "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture",
 ]
 
 
@@ -102,6 +103,13 @@ def lib() -> ctypes.CDLL:
     L.rg_analyse_gops_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32]
     L.rg_copy_records_gops.argtypes = [P, ctypes.c_int32, P]
     L.rg_analyse_gops_async.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
+    L.rg_writer_create.restype = P
+    L.rg_writer_create.argtypes = [ctypes.POINTER(RgConfig), ctypes.c_int32, ctypes.c_int32]
+    L.rg_writer_destroy.argtypes = [P]
+    L.rg_writer_bound.restype = ctypes.c_size_t
+    L.rg_writer_bound.argtypes = [P]
+    L.rg_writer_picture.restype = ctypes.c_int64
+    L.rg_writer_picture.argtypes = [P, P, ctypes.c_int32, P, ctypes.c_size_t]
     L.rg_set_pipeline_tuning.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                          ctypes.c_int32]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
@@ -297,3 +305,29 @@ def ssim_plane_device_noalloc(dev_a: int, stride_a: int, dev_b: int, stride_b: i
     ``stream`` without any device allocation (rg_ssim_plane_device_noalloc)."""
     _check(lib().rg_ssim_plane_device_noalloc(dev_a, stride_a, dev_b, stride_b, width, height, dev_out,
                                                stream or None))
+
+
+class CavlcWriter:
+    """Annex-B writer of one Baseline stream from engine records (rg_writer_*; host code)."""
+
+    def __init__(self, width: int, height: int, qp: int, fps=(30, 1)):
+        cfg = RgConfig(width, height, RG_PROFILE_BASELINE, qp, 1, 0, 1)
+        self.h = lib().rg_writer_create(ctypes.byref(cfg), fps[0], fps[1])
+        if not self.h:
+            raise RgError(-1, lib().rg_last_error().decode())
+        self.buf = np.zeros(lib().rg_writer_bound(self.h), np.uint8)
+
+    def picture(self, records: np.ndarray, kind: int) -> bytes:
+        records = np.ascontiguousarray(records, dtype=RECORD_DTYPE)
+        n = lib().rg_writer_picture(self.h, records.ctypes.data, kind, self.buf.ctypes.data, self.buf.size)
+        if n < 0:
+            raise RgError(n, lib().rg_last_error().decode())
+        return self.buf[:n].tobytes()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().rg_writer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
