@@ -74,6 +74,7 @@ struct __align__(16) Smem {
   uint8_t i4all[9 * 16];    // its nine predictions, mode-major, raster
   int32_t red[32];
 };
+static_assert(offsetof(Smem, coef) % 4 == 0 && offsetof(Smem, ccoef) % 4 == 0, "level arrays cleared by words");
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ MbInfo ld_info(const MbInfo* p) {
@@ -224,6 +225,27 @@ __device__ __forceinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_
     s += abs(s03 + s12) + abs(d03 + d12) + abs(s03 - s12) + abs(d03 - d12);
   }
   return s;  // caller halves the sum of the blocks
+}
+
+// One pass of the 4x4 forward core transform along the axis whose lanes are `step` apart in a
+// 16-lane group (i = position along it): [1 1 1 1; 2 1 -1 -2; 1 -1 -1 1; 1 -2 2 -1].
+__device__ __forceinline__ int fwd4_pass(int v, int step, int i) {
+  int b = __shfl_xor_sync(FULL, v, 3 * step);
+  int s = v + b, dd = v - b;
+  int ps = __shfl_xor_sync(FULL, s, step), pd = __shfl_xor_sync(FULL, dd, step);
+  return i == 0 ? s + ps : (i == 1 ? 2 * pd + dd : (i == 2 ? ps - s : 2 * pd - dd));
+}
+// One pass of the inverse core transform (fixed.rs:192): e0 = c0 + c2, e1 = c0 - c2,
+// e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1); out = e0 + e3, e1 + e2, e1 - e2, e0 - e3.
+__device__ __forceinline__ int inv4_pass(int v, int step, int i) {
+  int b = __shfl_xor_sync(FULL, v, 2 * step);
+  int ea, eb;
+  if (i == 0) { ea = v + b; eb = v - b; }
+  else if (i == 2) { ea = b + v; eb = b - v; }
+  else if (i == 1) { ea = (v >> 1) - b; eb = v + (b >> 1); }
+  else { ea = (b >> 1) - v; eb = b + (v >> 1); }
+  int pa = __shfl_xor_sync(FULL, ea, step), pb = __shfl_xor_sync(FULL, eb, step);
+  return i == 0 ? ea + pb : (i == 1 ? pb + ea : (i == 2 ? eb - pa : pa - eb));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -387,38 +409,78 @@ __device__ __forceinline__ int quant_level(int c, uint32_t mf, uint32_t bias, ui
   return c < 0 ? -(int)l : (int)l;
 }
 
+// Zig-zag index of each raster position of a 4x4 block, 4 bits per position (inverse of the
+// frame scan, Table 8-12).
+constexpr unsigned long long kZigzagIndex4 = 0xfea9db83c7426510ull;
+
+// Forward 4x4 core transform (fixed.rs:104, int16 output) and quantisation of `nblocks` 4x4
+// residual blocks (src - pred): luma blocks in decoding order (chroma = false) or the eight chroma
+// blocks, U then V (chroma = true). Lane = coefficient (raster p = lane & 15); half-warp h takes
+// block 2 it + h, two blocks per step. Levels go to out[16 b + p]; the raw DC of each block to
+// dc_raw[b] when given. Lane b then holds block b's: any level (among zig-zag indices >= first),
+// any |level| > 1 (same), and the decimation score of its zig-zag levels from index `first`
+// (enc.rs:559 decimate_score without its |level| > 1 rule; the caller applies it).
+__device__ __noinline__ void quant4x4_blocks(Smem& sm, bool chroma, int nblocks, int first, int qp, uint32_t shift,
+                                             uint32_t bias, int16_t* out, int16_t* dc_raw, int& my_nz, int& my_big,
+                                             int& my_score) {
+  int lane = lane_id(), p = lane & 15, h = lane >> 4, xl = p & 3, yl = p >> 2;
+  int zi = (int)((kZigzagIndex4 >> (4 * p)) & 15);
+  uint32_t mf = c_mf4[qp % 6][pos4(p)];
+  bool counted = zi >= first;
+  my_nz = my_big = my_score = 0;
+#pragma unroll 2
+  for (int it = 0; it < nblocks / 2; it++) {
+    int b = 2 * it + h;
+    const uint8_t *s, *pr;
+    int stride;
+    if (chroma) {
+      int off = ((b & 3) >> 1) * 32 + (b & 1) * 4;
+      s = ((b >> 2) ? sm.src_v : sm.src_u) + off;
+      pr = ((b >> 2) ? sm.pred_v : sm.pred_u) + off;
+      stride = 8;
+    } else {
+      int off = blk_y(b) * 64 + blk_x(b) * 4;
+      s = sm.src_y + off;
+      pr = sm.pred_y + off;
+      stride = 16;
+    }
+    int d = (int)s[yl * stride + xl] - (int)pr[yl * stride + xl];
+    int c = (int16_t)fwd4_pass(fwd4_pass(d, 1, xl), 4, yl);
+    if (dc_raw && p == 0) dc_raw[b] = (int16_t)c;
+    int l = quant_level(c, mf, bias, shift);
+    out[b * 16 + p] = (int16_t)l;
+    bool nz = l != 0 && counted;
+    uint32_t nzm = __ballot_sync(FULL, nz);
+    uint32_t bigm = __ballot_sync(FULL, nz && (l > 1 || l < -1));
+    uint32_t zm = __reduce_or_sync(FULL, nz ? 1u << (zi + 16 * h) : 0u);
+    uint32_t mine = (zm >> (16 * h)) & 0xffffu;
+    uint32_t contrib = 0;
+    if ((mine >> p) & 1u) {  // this lane as zig-zag index p: the run of zeros below it
+      uint32_t below = mine & ((1u << p) - 1u);
+      int prev = below ? 31 - __clz(below) : first - 1;
+      int run = p - prev - 1;
+      contrib = run == 0 ? 3u : (run <= 2 ? 2u : (run <= 5 ? 1u : 0u));
+    }
+    uint32_t sc = __reduce_add_sync(FULL, contrib << (16 * h));
+    if (lane == 2 * it || lane == 2 * it + 1) {
+      int k = lane & 1;
+      my_nz = ((nzm >> (16 * k)) & 0xffffu) != 0;
+      my_big = ((bigm >> (16 * k)) & 0xffffu) != 0;
+      my_score = (int)((sc >> (16 * k)) & 0xffffu);
+    }
+  }
+  __syncwarp();
+}
+
 // Luma 4x4 residual of pred_y, quantised (inter) and decimated into sm.coef
-// (enc.rs:1810 quant_luma_4x4_inter). Returns cbp; lanes 0..15 own block lane.
+// (enc.rs:1810 quant_luma_4x4_inter). Returns cbp; lanes 0..15 report block lane's "any level".
 __device__ __noinline__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_out) {
   int lane = lane_id();
   int qp = fp.qp;
   uint32_t shift, bias;
   quant4_params(qp, false, shift, bias);
-  int my_nz = 0, my_big = 0;
-  uint32_t my_score = 0;
-  if (lane < 16) {
-    int bx = blk_x(lane), by = blk_y(lane);
-    int d[16], c[16];
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        int o = (by * 4 + y) * 16 + bx * 4 + x;
-        d[y * 4 + x] = (int)sm.src_y[o] - (int)sm.pred_y[o];
-      }
-    fdct4(d, c);
-    int16_t zz[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      int l = quant_level(c[i], c_mf4[qp % 6][pos4(i)], bias, shift);
-      sm.coef[lane * 16 + i] = (int16_t)l;
-      if (l) my_nz = 1;
-      if (l > 1 || l < -1) my_big = 1;
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++) zz[i] = sm.coef[lane * 16 + c_scan4[i]];
-    my_score = decimate_score(zz, 16, c_dec4);
-  }
+  int my_nz, my_big, my_score;
+  quant4x4_blocks(sm, false, 16, 0, qp, shift, bias, sm.coef, nullptr, my_nz, my_big, my_score);
   // per-8x8 aggregates (lanes 4g..4g+3)
   int g_nz = my_nz | __shfl_xor_sync(FULL, my_nz, 1);
   g_nz |= __shfl_xor_sync(FULL, g_nz, 2);
@@ -438,10 +500,10 @@ __device__ __noinline__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint3
     total += sc;
   }
   if (total < 6 && cbp) cbp = 0;
-  if (lane < 16 && !((cbp >> (lane >> 2)) & 1)) {
+  // clear the levels of dropped 8x8 groups: word lane + 32 k of sm.coef lies in group k
 #pragma unroll
-    for (int i = 0; i < 16; i++) sm.coef[lane * 16 + i] = 0;
-  }
+  for (int k = 0; k < 4; k++)
+    if (!((cbp >> k) & 1)) ((uint32_t*)sm.coef)[lane + 32 * k] = 0u;
   __syncwarp();
   if (nz_lane_out) *nz_lane_out = (lane < 16 && ((cbp >> (lane >> 2)) & 1)) ? (uint32_t)my_nz : 0u;
   return cbp;
@@ -525,29 +587,10 @@ __device__ __noinline__ void chroma_quant(int qpc, bool intra, Smem& sm, uint32_
   int lane = lane_id();
   uint32_t shift, bias;
   quant4_params(qpc, intra, shift, bias);
-  uint32_t my_ac = 0, my_score = 0;
-  if (lane < 8) {
-    int p = lane >> 2, b = lane & 3;
-    const uint8_t* s = p ? sm.src_v : sm.src_u;
-    const uint8_t* pr = p ? sm.pred_v : sm.pred_u;
-    int o = (b >> 1) * 32 + (b & 1) * 4;
-    int d[16], c[16];
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) d[y * 4 + x] = (int)s[o + y * 8 + x] - (int)pr[o + y * 8 + x];
-    fdct4(d, c);
-    sm.cdcraw[lane] = (int16_t)c[0];
-    int16_t zz[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) sm.ccoef[lane * 16 + i] = (int16_t)quant_level(c[i], c_mf4[qpc % 6][pos4(i)], bias, shift);
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      zz[i] = sm.ccoef[lane * 16 + c_scan4[i]];
-      if (i && zz[i]) my_ac = 1;
-    }
-    my_score = decimate_score(zz + 1, 15, c_dec4);
-  }
+  int ac, big, sc;
+  quant4x4_blocks(sm, true, 8, 1, qpc, shift, bias, sm.ccoef, sm.cdcraw, ac, big, sc);
+  uint32_t my_ac = lane < 8 ? (uint32_t)ac : 0u;
+  uint32_t my_score = lane < 8 ? (big ? 9u : (uint32_t)sc) : 0u;  // decimate_score's |level| > 1 rule
   __syncwarp();
   // 2x2 DC transform + quantisation (enc.rs:1938 quant_chroma_dc; f = 2^qbits / 3 always)
   if (lane == 0 || lane == 4) {
@@ -578,32 +621,44 @@ __device__ __forceinline__ bool chroma_dc_any(const Smem& sm) {
   return a;
 }
 
-// Adds the dequantised chroma residual to pred_u / pred_v (enc.rs:1992 recon_chroma).
+// Adds the dequantised chroma residual to pred_u / pred_v (enc.rs:1992 recon_chroma): the DC of
+// each block from the 2x2 inverse (h264.rs:1674 dequantize_idct_chroma_dc2x2), its AC dequantised
+// when cbpc == 2, then the inverse core transform. Lane = coefficient, two blocks per step.
 __device__ __noinline__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
-  int lane = lane_id();
   if (cbpc == 0) return;
-  if (lane < 8) {
-    int p = lane >> 2, b = lane & 3;
-    // dequantize_idct_chroma_dc2x2 (h264.rs:1674)
-    int qmul = (c_dq4[qpc % 6][0] * 16) << (qpc / 6 + 2);
-    int a = sm.cdc[p * 4], bb = sm.cdc[p * 4 + 1], c = sm.cdc[p * 4 + 2], d = sm.cdc[p * 4 + 3];
-    int e = a - bb, apb = a + bb, cmd = c - d, cpd = c + d;
-    int dcr[4] = {((apb + cpd) * qmul) >> 7, ((e + cmd) * qmul) >> 7, ((apb - cpd) * qmul) >> 7, ((e - cmd) * qmul) >> 7};
-    int blk[16], res[16];
-    int scale_shift = qpc / 6;
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      int v = 0;
-      if (cbpc >= 2) v = clamp_i16((int)sm.ccoef[lane * 16 + i] * ((int)c_dq4[qpc % 6][pos4(i)] << scale_shift));
-      blk[i] = v;
+  int lane = lane_id(), p = lane & 15, h = lane >> 4, xl = p & 3, yl = p >> 2;
+  int qmul = (c_dq4[qpc % 6][0] * 16) << (qpc / 6 + 2);
+  int dqs = (int)c_dq4[qpc % 6][pos4(p)] << (qpc / 6);
+#pragma unroll 2
+  for (int it = 0; it < 4; it++) {
+    int b = 2 * it + h, pl = b >> 2, bb = b & 3;
+    int a = sm.cdc[pl * 4], bv = sm.cdc[pl * 4 + 1], c = sm.cdc[pl * 4 + 2], d = sm.cdc[pl * 4 + 3];
+    int e = a - bv, apb = a + bv, cmd = c - d, cpd = c + d;
+    int dcv = bb == 0 ? apb + cpd : (bb == 1 ? e + cmd : (bb == 2 ? apb - cpd : e - cmd));
+    int v = p == 0 ? (int)(int16_t)((dcv * qmul) >> 7)
+                   : (cbpc >= 2 ? (int)clamp_i16((int)sm.ccoef[b * 16 + p] * dqs) : 0);
+    int r = (int16_t)((inv4_pass(inv4_pass(v, 1, xl), 4, yl) + 32) >> 6);
+    uint8_t* pr = (pl ? sm.pred_v : sm.pred_u) + (bb >> 1) * 32 + (bb & 1) * 4 + yl * 8 + xl;
+    *pr = (uint8_t)clip255(*pr + r);
+  }
+  __syncwarp();
+}
+
+// Adds the dequantised luma 4x4 residual of the coded 8x8 groups of sm.coef to pred_y
+// (enc.rs:1978 recon_luma_4x4). Lane = coefficient, two blocks per step.
+__device__ __noinline__ void recon_luma4x4(Smem& sm, int qp, int cbp) {
+  int lane = lane_id(), p = lane & 15, h = lane >> 4, xl = p & 3, yl = p >> 2;
+  int dqs = (int)c_dq4[qp % 6][pos4(p)] << (qp / 6);
+#pragma unroll 2
+  for (int it = 0; it < 8; it++) {
+    int b = 2 * it + h;
+    bool coded = (cbp >> (b >> 2)) & 1;
+    int v = coded ? (int)clamp_i16((int)sm.coef[b * 16 + p] * dqs) : 0;
+    int r = (int16_t)((inv4_pass(inv4_pass(v, 1, xl), 4, yl) + 32) >> 6);
+    if (coded) {
+      int o = (blk_y(b) * 4 + yl) * 16 + blk_x(b) * 4 + xl;
+      sm.pred_y[o] = (uint8_t)clip255(sm.pred_y[o] + r);
     }
-    blk[0] = (int16_t)dcr[b];
-    idct4(blk, res);
-    uint8_t* pr = (p ? sm.pred_v : sm.pred_u) + (b >> 1) * 32 + (b & 1) * 4;
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) pr[y * 8 + x] = (uint8_t)clip255(pr[y * 8 + x] + res[y * 4 + x]);
   }
   __syncwarp();
 }
@@ -798,27 +853,6 @@ __device__ __forceinline__ int i4_tap(int m, int x, int y) {
     }
   }
 }
-// One pass of the 4x4 forward core transform along the axis whose lanes are `step` apart in a
-// 16-lane group (i = position along it): [1 1 1 1; 2 1 -1 -2; 1 -1 -1 1; 1 -2 2 -1].
-__device__ __forceinline__ int fwd4_pass(int v, int step, int i) {
-  int b = __shfl_xor_sync(FULL, v, 3 * step);
-  int s = v + b, dd = v - b;
-  int ps = __shfl_xor_sync(FULL, s, step), pd = __shfl_xor_sync(FULL, dd, step);
-  return i == 0 ? s + ps : (i == 1 ? 2 * pd + dd : (i == 2 ? ps - s : 2 * pd - dd));
-}
-// One pass of the inverse core transform (fixed.rs:192): e0 = c0 + c2, e1 = c0 - c2,
-// e2 = (c1 >> 1) - c3, e3 = c1 + (c3 >> 1); out = e0 + e3, e1 + e2, e1 - e2, e0 - e3.
-__device__ __forceinline__ int inv4_pass(int v, int step, int i) {
-  int b = __shfl_xor_sync(FULL, v, 2 * step);
-  int ea, eb;
-  if (i == 0) { ea = v + b; eb = v - b; }
-  else if (i == 2) { ea = b + v; eb = b - v; }
-  else if (i == 1) { ea = (v >> 1) - b; eb = v + (b >> 1); }
-  else { ea = (b >> 1) - v; eb = b + (v >> 1); }
-  int pa = __shfl_xor_sync(FULL, ea, step), pb = __shfl_xor_sync(FULL, eb, step);
-  return i == 0 ? ea + pb : (i == 1 ? pb + ea : (i == 2 ? eb - pa : pa - eb));
-}
-
 // ---------------------------------------------------------------------------------------------
 struct Ctx {
   const FrameParams* fp;
@@ -1241,32 +1275,11 @@ __device__ __noinline__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
   int lane = lane_id();
   uint32_t shift, bias;
   quant4_params(fp.qp, false, shift, bias);
-  uint32_t big = 0, score = 0;
-  if (lane < 16) {
-    int bx = blk_x(lane), by = blk_y(lane);
-    int d[16], cc[16];
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        int o = (by * 4 + y) * 16 + bx * 4 + x;
-        d[y * 4 + x] = (int)sm.src_y[o] - (int)sm.pred_y[o];
-      }
-    fdct4(d, cc);
-    int16_t lv[16], zz[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      int l = quant_level(cc[i], c_mf4[fp.qp % 6][pos4(i)], bias, shift);
-      lv[i] = (int16_t)l;
-      if (l > 1 || l < -1) big = 1;
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++) zz[i] = lv[c_scan4[i]];
-    score = decimate_score(zz, 16, c_dec4);
-  }
-  big = wor(big);
-  score = wsum(score);
-  return !big && score < 6;
+  int nz, big, sc;  // levels go to sm.coef as scratch: a skipped macroblock records none
+  quant4x4_blocks(sm, false, 16, 0, fp.qp, shift, bias, sm.coef, nullptr, nz, big, sc);
+  uint32_t b = wor(lane < 16 ? (uint32_t)big : 0u);
+  uint32_t score = wsum(lane < 16 ? (uint32_t)sc : 0u);
+  return !b && score < 6;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1680,19 +1693,8 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
         sm.pred_y[off] = (uint8_t)clip255((int)((unsigned)sm.pred_y[off] + (unsigned)v));
       }
     }
-  } else if (lane < 16 && ((cbpl >> (lane >> 2)) & 1)) {
-    int bx = blk_x(lane), by = blk_y(lane);
-    int blk[16], res[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) blk[i] = clamp_i16((int)sm.coef[lane * 16 + i] * ((int)c_dq4[qp % 6][pos4(i)] << (qp / 6)));
-    idct4(blk, res);
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        int o = (by * 4 + y) * 16 + bx * 4 + x;
-        sm.pred_y[o] = (uint8_t)clip255(sm.pred_y[o] + res[y * 4 + x]);
-      }
+  } else if (cbpl) {
+    recon_luma4x4(sm, qp, cbpl);
   }
   __syncwarp();
   chroma_recon(qpc, cbpc, sm);
