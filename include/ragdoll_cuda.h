@@ -184,9 +184,9 @@ int rg_analyse_gops_async(rg_ctx* ctx, const uint8_t* const* planes, size_t stri
  * of a stream in the work order (1..4096; 0 = 8 * max(seg, 2) + seg + 7, which orders every
  * wait of a search reaching up to 4 macroblock rows beyond zero motion after the work it waits
  * for; larger is safer for long motion, smaller favours newer pictures), seg = macroblocks per
- * work segment (1..mb_w, 0 = 2), grid = resident warps (0 = six per SM, fewer if they do not
+ * work segment (1..mb_w, 0 = 2), grid = resident warps (0 = seven per SM, fewer if they do not
  * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take
- * deblocking segments first from a queue of their own (0 = one SM in nine, -1 = one mixed queue
+ * deblocking segments first from a queue of their own (0 = one SM in six, -1 = one mixed queue
  * for all warps). A wait that runs out makes the launch stop and rg_sync re-run the call on the
  * per-diagonal path, which has no waits. No counterpart in the reference (its GOP threads have
  * no device schedule).

@@ -2133,13 +2133,13 @@ int pipeline_sms(int device) {
   return sms;
 }
 
-// Resident warps of the pipelined mode: six per SM (fewer when they do not fit). More warps
-// overlap more waits but slow every macroblock on the critical path (measured on B200: 4-8 per
+// Resident warps of the pipelined mode: seven per SM (fewer when they do not fit). More warps
+// overlap more waits but slow every macroblock on the critical path (measured on B200: 5-8 per
 // SM within 3 % of each other, 20 per SM 10 % slower).
 int pipeline_grid(int device) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel, 32, 0);
-  return (per_sm < 6 ? per_sm : 6) * pipeline_sms(device);
+  return (per_sm < 7 ? per_sm : 7) * pipeline_sms(device);
 }
 
 // Work list of the pipelined mode, written to `tasks` (pipeline_task_count entries): every

@@ -22,8 +22,9 @@ thread_local std::string g_last_error;
 
 constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the segment length
 constexpr int kDefaultSeg = 2;   // macroblocks per work segment
-// Deblocking is about a tenth of the work: one SM in nine takes its queue first (16 of 148).
-int default_deblock_sms(int sms) { return sms >= 9 ? (sms + 4) / 9 : 0; }
+// Deblocking is about a sixth of the work once analysis runs at full speed: one SM in six takes
+// its queue first (25 of 148; measured on B200: 16 SMs 1326 frames/s, 20-30 SMs 1394-1417).
+int default_deblock_sms(int sms) { return sms >= 6 ? (sms + 3) / 6 : 0; }
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
