@@ -187,7 +187,8 @@ def run_engine(args, rank, world, local):
         return [p, p + W * H, p + W * H + cw * ch]
 
     eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
-    eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms)
+    eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms,
+                            intra_sms=args.intra_sms)
     stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
     torch.cuda.synchronize()
     gop_ptrs, gop_kinds = [], []
@@ -356,7 +357,8 @@ def run_profile_case(args, local):
     if args.profile_case == "pipelined":
         nf = args.profile_frames
         eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=nf)
-        eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms)
+        eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms,
+                                intra_sms=args.intra_sms)
         stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
         ptrs, kinds = [], []
         for f in range(nf):
@@ -420,6 +422,8 @@ def main():
                     help="pipelined mode: resident warps (0 = default)")
     ap.add_argument("--deblock-sms", type=int, default=0,
                     help="pipelined mode: SMs taking deblocking segments first (0 = default, -1 = one mixed queue)")
+    ap.add_argument("--intra-sms", type=int, default=0,
+                    help="pipelined mode: SMs taking IDR-picture analysis first (0 = default, -1 = none)")
     ap.add_argument("--lag", type=int, default=0,
                     help="pipelined mode: macroblock-times between consecutive pictures in the work order (0 = default)")
     ap.add_argument("--seg", type=int, default=0,

@@ -179,20 +179,30 @@ int rg_copy_records_gops(rg_ctx* ctx, int32_t frames, rg_mb_out* out);
 int rg_analyse_gops_async(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
                           const int32_t* kinds, int32_t frames, rg_mb_out* out);
 
+/* Tuning of the pipelined mode (rg_set_pipeline_tuning); 0 in any field selects the default. */
+typedef struct rg_pipeline_tuning {
+    int32_t lag;          /* macroblock-times between consecutive pictures in the work order    */
+    int32_t seg;          /* macroblocks per work segment                                         */
+    int32_t grid;         /* resident warps                                                       */
+    int32_t timeout_ms;   /* limit of one device wait                                             */
+    int32_t deblock_sms;  /* SMs taking deblocking segments first (-1: no deblocking queue)       */
+    int32_t intra_sms;    /* next SMs taking IDR-picture analysis first (-1: no such queue)       */
+} rg_pipeline_tuning;
+
 /*
- * Tuning / test hook of the pipelined mode: lag = macroblock-times between consecutive pictures
+ * Tuning / test hook of the pipelined mode (tuning NULL: all defaults): lag = macroblock-times between consecutive pictures
  * of a stream in the work order (1..4096; 0 = 8 * max(seg, 2) + seg + 7, which orders every
  * wait of a search reaching up to 4 macroblock rows beyond zero motion after the work it waits
  * for; larger is safer for long motion, smaller favours newer pictures), seg = macroblocks per
  * work segment (1..mb_w, 0 = 2), grid = resident warps (0 = seven per SM, fewer if they do not
  * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take
  * deblocking segments first from a queue of their own (0 = one SM in six, -1 = one mixed queue
- * for all warps). A wait that runs out makes the launch stop and rg_sync re-run the call on the
- * per-diagonal path, which has no waits. No counterpart in the reference (its GOP threads have
- * no device schedule).
+ * for all warps), intra_sms = the next SMs, whose warps take the analysis of IDR pictures first
+ * from a queue of their own. A wait that runs out makes the launch stop and rg_sync re-run the
+ * call on the per-diagonal path, which has no waits. No counterpart in the reference (its GOP
+ * threads have no device schedule).
  */
-int rg_set_pipeline_tuning(rg_ctx* ctx, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms,
-                           int32_t deblock_sms);
+int rg_set_pipeline_tuning(rg_ctx* ctx, const rg_pipeline_tuning* tuning);
 
 /* Waits for queued device work of the context. */
 int rg_sync(rg_ctx* ctx);

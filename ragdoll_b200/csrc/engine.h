@@ -79,11 +79,12 @@ size_t pipeline_counter_ints(const FrameParams& fp, int frames);
 // Work list: every analysis / deblocking segment of `seg` macroblocks, in expected-ready order
 // with `lag` macroblock-times between consecutive pictures of a stream.
 size_t pipeline_task_count(const FrameParams& fp, int frames, int seg);
-// split: analysis segments first, then deblocking segments, as two queues (*n_ana analysis).
-size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, int2* tasks, size_t* n_ana);
+// Queues: 0 analysis, 1 deblocking (split), 2 analysis of IDR pictures (kinds != null; [f][s]).
+size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, const int32_t* kinds,
+                          int2* tasks, int qbeg[3], int qend[3]);
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
-                     size_t n_tasks, size_t n_ana, int deblock_sms, int sms, int seg, int grid,
-                     unsigned long long timeout_ns, cudaStream_t st);
+                     size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
+                     int seg, int grid, unsigned long long timeout_ns, cudaStream_t st);
 void upload_tables();
 
 }  // namespace rg

@@ -1957,9 +1957,10 @@ struct PipeParams {
                // extends the padding of the macroblocks it makes final
   const int2* tasks;  // {picture * S + stream, row << 16 | first macroblock << 1 | deblock}
   int n_tasks;
-  int n_ana;          // < n_tasks: tasks[0, n_ana) analysis, [n_ana, n_tasks) deblocking, two queues
-  int deblock_sms;    // SMs whose warps take the deblocking queue first
-  int role_by_sm;     // 0: warps of blocks 0, 9, 18, ... take it first (a grid too small to reach every SM)
+  int qbeg[3], qend[3];  // queue q = tasks[qbeg[q], qend[q]): 0 analysis, 1 deblocking, 2 IDR analysis
+  int deblock_sms;    // SMs whose warps take queue 1 first
+  int intra_sms;      // the next SMs, whose warps take queue 2 first
+  int role_by_sm;     // 0: by block index instead (a grid too small to reach every SM)
   int seg;
   unsigned long long timeout_ns;
 };
@@ -1973,21 +1974,26 @@ __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const 
   __shared__ Smem sm;
   const int lane = lane_id();
   const int S = fp.n_streams, H = fp.mb_h, Wm = fp.mb_w;
-  // With two queues, warps on the first deblock_sms SMs prefer deblocking segments and the others
-  // analysis segments (each SM then runs a smaller code footprint); a warp whose queue is empty
-  // takes from the other one.
-  const bool split = pp.n_ana < pp.n_tasks;
-  const int pref = split && (pp.role_by_sm ? (int)sm_id() < pp.deblock_sms : blockIdx.x % 9 == 0) ? 1 : 0;
-  bool empty[2] = {false, !split};
+  // Warps on the first deblock_sms SMs take deblocking segments first, on the next intra_sms SMs
+  // segments of IDR pictures (the critical path of a GOP), and the others the remaining analysis
+  // (each SM then runs a smaller code footprint); a warp whose queue is empty takes from the next.
+  int role = 0;
+  if (pp.role_by_sm) {
+    int id = (int)sm_id();
+    role = id < pp.deblock_sms ? 1 : (id < pp.deblock_sms + pp.intra_sms ? 2 : 0);
+  } else {
+    int k = blockIdx.x % 9;
+    role = k == 0 ? 1 : (k == 1 ? 2 : 0);
+  }
+  bool empty[3] = {pp.qbeg[0] >= pp.qend[0], pp.qbeg[1] >= pp.qend[1], pp.qbeg[2] >= pp.qend[2]};
   while (true) {
     int t = -1;
     if (lane == 0) {
-      for (int k = 0; k < 2 && t < 0; k++) {
-        int q = pref ^ k;
+      for (int k = 0; k < 3 && t < 0; k++) {
+        int q = role + k >= 3 ? role + k - 3 : role + k;
         if (empty[q]) continue;
-        int base = q ? pp.n_ana : 0, lim = q || !split ? pp.n_tasks : pp.n_ana;
-        int v = base + atomicAdd(q ? pp.ticket + 2 : pp.ticket, 1);
-        if (v < lim) t = v; else empty[q] = true;
+        int v = pp.qbeg[q] + atomicAdd(pp.ticket + (q ? q + 1 : 0), 1);
+        if (v < pp.qend[q]) t = v; else empty[q] = true;
       }
     }
     t = __shfl_sync(FULL, t, 0);
@@ -2160,40 +2166,48 @@ size_t pipeline_task_count(const FrameParams& fp, int frames, int seg) {
   return 2 * (size_t)frames * fp.n_streams * fp.mb_h * segs;
 }
 
-size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, int2* tasks, size_t* n_ana) {
+size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, const int32_t* kinds,
+                          int2* tasks, int qbeg[3], int qend[3]) {
   int S = fp.n_streams, H = fp.mb_h, W = fp.mb_w;
   int segs = (W + seg - 1) / seg, a = seg > 2 ? seg : 2;
   if (lag <= 0) lag = a * 8 + seg + 7;
   auto key = [&](int f, int role, int y, int k) {
     return (size_t)a * (y + role) + (size_t)k * seg + role + (size_t)lag * f;
   };
-  // split: analysis keys first, then deblocking keys shifted past them (two queues, each in
-  // key order)
-  size_t n_keys1 = key(frames - 1, 1, H - 1, segs - 1) + 1;
-  size_t shift = split ? n_keys1 : 0, n_keys = n_keys1 + shift;
-  auto slot = [&](int f, int role, int y, int k) { return key(f, role, y, k) + (role ? shift : 0); };
+  // queue of a segment: deblocking (1) when split, analysis of an IDR picture (2) when kinds are
+  // given, else 0; each queue occupies its own range of keys, so each is in key order
+  auto queue = [&](int f, int s, int role) {
+    if (role) return split ? 1 : 0;
+    return kinds && kinds[f * S + s] == RG_FRAME_IDR ? 2 : 0;
+  };
+  size_t n_keys1 = key(frames - 1, 1, H - 1, segs - 1) + 1, n_keys = 3 * n_keys1;
+  auto slot = [&](int f, int s, int role, int y, int k) { return key(f, role, y, k) + queue(f, s, role) * n_keys1; };
   std::vector<size_t> start(n_keys + 1, 0);
   for (int f = 0; f < frames; f++)
     for (int role = 0; role < 2; role++)
-      for (int y = 0; y < H; y++)
-        for (int k = 0; k < segs; k++) start[slot(f, role, y, k) + 1] += S;
+      for (int s = 0; s < S; s++)
+        for (int y = 0; y < H; y++)
+          for (int k = 0; k < segs; k++) start[slot(f, s, role, y, k) + 1]++;
   for (size_t i = 0; i < n_keys; i++) start[i + 1] += start[i];
-  *n_ana = split ? start[n_keys1] : pipeline_task_count(fp, frames, seg);
+  for (int q = 0; q < 3; q++) {
+    qbeg[q] = (int)start[q * n_keys1];
+    qend[q] = (int)start[(q + 1) * n_keys1];
+  }
   // placed in (picture, role, stream, row, segment) order within a key: a stable counting sort
   for (int f = 0; f < frames; f++)
     for (int role = 0; role < 2; role++)
       for (int s = 0; s < S; s++)
         for (int y = 0; y < H; y++)
           for (int k = 0; k < segs; k++) {
-            size_t at = start[slot(f, role, y, k)]++;
+            size_t at = start[slot(f, s, role, y, k)]++;
             tasks[at] = make_int2(f * S + s, (y << 16) | ((k * seg) << 1) | role);
           }
   return pipeline_task_count(fp, frames, seg);
 }
 
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
-                     size_t n_tasks, size_t n_ana, int deblock_sms, int sms, int seg, int grid,
-                     unsigned long long timeout_ns, cudaStream_t st) {
+                     size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
+                     int seg, int grid, unsigned long long timeout_ns, cudaStream_t st) {
   int S = fp.n_streams, H = fp.mb_h;
   PipeParams pp;
   pp.ticket = counters;
@@ -2202,8 +2216,12 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.db = pp.ana + frames * S * H;
   pp.tasks = d_tasks;
   pp.n_tasks = (int)n_tasks;
-  pp.n_ana = (int)n_ana;
+  for (int q = 0; q < 3; q++) {
+    pp.qbeg[q] = qbeg[q];
+    pp.qend[q] = qend[q];
+  }
   pp.deblock_sms = deblock_sms;
+  pp.intra_sms = intra_sms;
   pp.role_by_sm = grid >= sms;
   pp.seg = seg;
   pp.timeout_ns = timeout_ns;

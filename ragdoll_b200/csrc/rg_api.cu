@@ -25,6 +25,10 @@ constexpr int kDefaultSeg = 2;   // macroblocks per work segment
 // Deblocking is about a sixth of the work once analysis runs at full speed: one SM in six takes
 // its queue first (25 of 148; measured on B200: 16 SMs 1326 frames/s, 20-30 SMs 1394-1417).
 int default_deblock_sms(int sms) { return sms >= 6 ? (sms + 3) / 6 : 0; }
+// The analysis of IDR pictures is the critical path of every GOP (each P picture trails it): one
+// SM in three takes it first (49 of 148; measured on B200: none 1412 frames/s, 20 SMs 1355,
+// 35-65 SMs 1473-1481). Those warps continue with P pictures once the IDR queue is empty.
+int default_intra_sms(int sms) { return sms >= 3 ? sms / 3 : 0; }
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -119,10 +123,13 @@ struct rg_ctx {
   int seg = kDefaultSeg;           // macroblocks per work segment
   unsigned long long timeout_ns = 2000000000ull;  // limit of one device wait
   int deblock_sms = 0;             // SMs preferring deblocking segments (0 = one mixed queue)
+  int intra_sms = 0;               // SMs preferring IDR-picture analysis (0 = no such queue)
   int sms = 0;
   int2* d_tasks = nullptr;         // work list of the pipelined mode
-  size_t tasks_cap = 0, n_tasks = 0, n_ana = 0;
+  size_t tasks_cap = 0, n_tasks = 0;
+  int qbeg[3] = {0, 0, 0}, qend[3] = {0, 0, 0};
   int tasks_frames = -1, tasks_lag = -1, tasks_seg = -1, tasks_split = -1;  // what d_tasks holds
+  std::vector<int32_t> tasks_kinds;
   std::vector<int2> h_tasks;
   // the pending pipelined call, kept to re-run it on the per-diagonal path after a failed wait
   std::vector<const uint8_t*> pend_planes;
@@ -258,6 +265,7 @@ rg_ctx* rg_create(const rg_config* cfg) {
   c->grid = pipeline_grid(cfg->device);
   c->sms = pipeline_sms(cfg->device);
   c->deblock_sms = default_deblock_sms(c->sms);
+  c->intra_sms = default_intra_sms(c->sms);
   upload_tables();
   if (cudaDeviceSynchronize() != cudaSuccess) {
     fail(RG_ERR_CUDA, "rg_create: %s", cudaGetErrorString(cudaGetLastError()));
@@ -454,19 +462,25 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   CK(cudaEventRecord(c->slot_done[slot], c->stream));
   CK(cudaMemsetAsync(c->counters, 0, sizeof(int) * pipeline_counter_ints(c->fp, frames), c->stream));
   int split = c->deblock_sms > 0 && c->grid >= 2 ? 1 : 0;
-  if (frames != c->tasks_frames || c->lag != c->tasks_lag || c->seg != c->tasks_seg || split != c->tasks_split) {
-    // rebuilt only when the call's shape or the tuning changes; the copy is stream-ordered
-    // after any launch still reading the old list
+  // IDR pictures get their own queue when SMs are set aside for them
+  std::vector<int32_t> kinds_key;
+  if (c->intra_sms > 0 && c->grid >= 3) kinds_key.assign(kinds, kinds + (size_t)frames * S);
+  if (frames != c->tasks_frames || c->lag != c->tasks_lag || c->seg != c->tasks_seg || split != c->tasks_split ||
+      kinds_key != c->tasks_kinds) {
+    // rebuilt only when the call's shape, its picture kinds or the tuning change; the copy is
+    // stream-ordered after any launch still reading the old list
     c->h_tasks.resize(pipeline_task_count(fp, frames, c->seg));
-    c->n_tasks = pipeline_task_list(fp, frames, c->lag, c->seg, split != 0, c->h_tasks.data(), &c->n_ana);
+    c->n_tasks = pipeline_task_list(fp, frames, c->lag, c->seg, split != 0,
+                                    kinds_key.empty() ? nullptr : kinds_key.data(), c->h_tasks.data(), c->qbeg, c->qend);
+    c->tasks_kinds = kinds_key;
     CK(cudaMemcpyAsync(c->d_tasks, c->h_tasks.data(), sizeof(int2) * c->n_tasks, cudaMemcpyHostToDevice, c->stream));
     c->tasks_frames = frames;
     c->tasks_lag = c->lag;
     c->tasks_seg = c->seg;
     c->tasks_split = split;
   }
-  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->n_ana, c->deblock_sms, c->sms,
-                  c->seg, c->grid, c->timeout_ns, c->stream);
+  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->qbeg, c->qend, c->deblock_sms,
+                  c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, c->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->h_err, c->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   c->pend_planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
@@ -497,12 +511,15 @@ int rg_copy_records_gops(rg_ctx* c, int32_t frames, rg_mb_out* out) {
   return RG_OK;
 }
 
-int rg_set_pipeline_tuning(rg_ctx* c, int32_t lag, int32_t seg, int32_t grid, int32_t timeout_ms,
-                           int32_t deblock_sms) {
+int rg_set_pipeline_tuning(rg_ctx* c, const rg_pipeline_tuning* t) {
   if (!c) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: null context");
+  rg_pipeline_tuning zero{};
+  if (!t) t = &zero;
+  int lag = t->lag, seg = t->seg, grid = t->grid, timeout_ms = t->timeout_ms, deblock_sms = t->deblock_sms,
+      intra_sms = t->intra_sms;
   if (lag < 0 || lag > 4096) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: lag %d outside 0..4096", lag);
   if (seg < 0 || seg > c->fp.mb_w) return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: seg %d outside 0..%d", seg, c->fp.mb_w);
-  if (grid < 0 || timeout_ms < 0 || deblock_sms < -1)
+  if (grid < 0 || timeout_ms < 0 || deblock_sms < -1 || intra_sms < -1)
     return fail(RG_ERR_INVALID, "rg_set_pipeline_tuning: negative argument");
   CK(cudaStreamSynchronize(c->stream));
   int new_seg = seg > 0 ? seg : kDefaultSeg;
@@ -519,6 +536,7 @@ int rg_set_pipeline_tuning(rg_ctx* c, int32_t lag, int32_t seg, int32_t grid, in
   c->lag = lag > 0 ? lag : kDefaultLag;
   c->seg = new_seg;
   c->deblock_sms = deblock_sms < 0 ? 0 : (deblock_sms > 0 ? deblock_sms : default_deblock_sms(c->sms));
+  c->intra_sms = intra_sms < 0 ? 0 : (intra_sms > 0 ? intra_sms : default_intra_sms(c->sms));
   c->tasks_frames = -1;
   if (grid > 0) c->grid = grid;
   else c->grid = pipeline_grid(c->cfg.device);

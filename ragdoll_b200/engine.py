@@ -57,6 +57,10 @@ class RgConfig(ctypes.Structure):
                 ("max_frames", ctypes.c_int32)]
 
 
+class RgPipelineTuning(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("lag", "seg", "grid", "timeout_ms", "deblock_sms", "intra_sms")]
+
+
 class RgQuality(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ("ssim_y", "ssim_u", "ssim_v", "ssim_avg", "ms_ssim", "psnr_y", "psnr_u", "psnr_v")]
@@ -110,8 +114,7 @@ def lib() -> ctypes.CDLL:
     L.rg_writer_bound.argtypes = [P]
     L.rg_writer_picture.restype = ctypes.c_int64
     L.rg_writer_picture.argtypes = [P, P, ctypes.c_int32, P, ctypes.c_size_t]
-    L.rg_set_pipeline_tuning.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                                         ctypes.c_int32]
+    L.rg_set_pipeline_tuning.argtypes = [P, ctypes.POINTER(RgPipelineTuning)]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
     _lib = L
@@ -237,11 +240,13 @@ class Engine:
         _check(lib().rg_analyse_gops_device(self.h, planes, stride_y, stride_uv, k, frames))
 
     def set_pipeline_tuning(self, lag: int = 0, seg: int = 0, grid: int = 0, timeout_ms: int = 0,
-                            deblock_sms: int = 0) -> None:
+                            deblock_sms: int = 0, intra_sms: int = 0) -> None:
         """Pipelined-mode work order (0 = library defaults): lag macroblock-times between the
         pictures of a stream, seg macroblocks per work segment, grid resident warps, the limit
-        of one device wait, and the SMs that take deblocking segments first (-1 = one mixed queue)."""
-        _check(lib().rg_set_pipeline_tuning(self.h, lag, seg, grid, timeout_ms, deblock_sms))
+        of one device wait, the SMs that take deblocking segments first and the next SMs that
+        take IDR-picture analysis first (-1 = no such queue)."""
+        t = RgPipelineTuning(lag, seg, grid, timeout_ms, deblock_sms, intra_sms)
+        _check(lib().rg_set_pipeline_tuning(self.h, ctypes.byref(t)))
 
     def records_gops(self, frames: int) -> np.ndarray:
         out = np.zeros((frames, self.num_streams, self.n_mb), RECORD_DTYPE)

@@ -67,6 +67,8 @@ def test_batched_streams_match_single():
     (64, 32, 22, 1, 4, 6, {}),
     (176, 144, 26, 2, 3, 5, {"deblock_sms": -1, "seg": 8}),
     (208, 120, 24, 2, 2, 5, {"deblock_sms": 16, "grid": 64, "lag": 40}),
+    (176, 144, 26, 2, 3, 5, {"deblock_sms": 20, "intra_sms": 40}),
+    (176, 144, 26, 2, 3, 5, {"deblock_sms": 3, "intra_sms": 2, "grid": 100}),
 ])
 def test_pipelined_gops_match_oracle(w, h, qp, profile, streams, frames, tuning):
     """One persistent launch for all pictures of several GOPs (pictures of a GOP overlapping)
