@@ -278,6 +278,17 @@ int rg_ssim_plane_device_noalloc(const uint8_t* dev_a, size_t stride_a, const ui
                                  size_t stride_b, int32_t width, int32_t height, double* dev_out,
                                  void* cuda_stream);
 
+/*
+ * Diagnostic: the work list of the pipelined mode for a shape (host code, no GPU), as the
+ * kernel receives it -- per segment {picture * streams + stream, row << 16 | first macroblock
+ * << 1 | deblocking} -- and each queue's range [queues[2q], queues[2q+1]) (queues: analysis,
+ * deblocking, IDR-picture analysis; kinds[f * streams + s] or NULL). lag 0 = the default.
+ * Returns the number of segments. Used by the tests that check the order never makes a
+ * wait depend on a segment that no warp can take. No counterpart in the reference.
+ */
+int64_t rg_pipeline_work_list(int32_t mb_w, int32_t mb_h, int32_t streams, int32_t frames, int32_t lag, int32_t seg,
+                              int32_t split, const int32_t* kinds, int32_t* tasks, int64_t cap, int32_t* queues);
+
 /* ---- CAVLC bitstream writer (host) ------------------------------------------------------ */
 /*
  * The serial half of encode_frame_body (crates/ragdoll-codec/src/h264/enc.rs:2234) for the

@@ -80,6 +80,7 @@ size_t pipeline_counter_ints(const FrameParams& fp, int frames);
 // with `lag` macroblock-times between consecutive pictures of a stream.
 size_t pipeline_task_count(const FrameParams& fp, int frames, int seg);
 // Queues: 0 analysis, 1 deblocking (split), 2 analysis of IDR pictures (kinds != null; [f][s]).
+constexpr int kPipeQueues = 3;
 size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, const int32_t* kinds,
                           int2* tasks, int qbeg[3], int qend[3]);
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,

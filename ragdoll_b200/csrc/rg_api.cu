@@ -955,4 +955,28 @@ int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8
   return r;
 }
 
+int64_t rg_pipeline_work_list(int32_t mb_w, int32_t mb_h, int32_t streams, int32_t frames, int32_t lag, int32_t seg,
+                              int32_t split, const int32_t* kinds, int32_t* tasks, int64_t cap, int32_t* queues) {
+  if (mb_w < 1 || mb_h < 1 || streams < 1 || frames < 1 || seg < 1 || lag < 0 || !tasks || !queues)
+    return fail(RG_ERR_INVALID, "rg_pipeline_work_list: bad argument");
+  FrameParams fp{};
+  fp.mb_w = mb_w;
+  fp.mb_h = mb_h;
+  fp.n_streams = streams;
+  size_t n = pipeline_task_count(fp, frames, seg);
+  if ((int64_t)n > cap) return fail(RG_ERR_INVALID, "rg_pipeline_work_list: %zu segments exceed cap %lld", n, (long long)cap);
+  std::vector<int2> list(n);
+  int qb[kPipeQueues], qe[kPipeQueues];
+  pipeline_task_list(fp, frames, lag, seg, split != 0, kinds, list.data(), qb, qe);
+  for (size_t i = 0; i < n; i++) {
+    tasks[2 * i] = list[i].x;
+    tasks[2 * i + 1] = list[i].y;
+  }
+  for (int q = 0; q < kPipeQueues; q++) {
+    queues[2 * q] = qb[q];
+    queues[2 * q + 1] = qe[q];
+  }
+  return (int64_t)n;
+}
+
 }  // extern "C"

@@ -39,7 +39,7 @@ EXPORTS = [
     "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
     "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc", "rg_analyse_gops",
     "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_analyse_gops_async",
-    "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture",
+    "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture", "rg_pipeline_work_list",
 ]
 
 
@@ -107,6 +107,8 @@ def lib() -> ctypes.CDLL:
     L.rg_analyse_gops_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32]
     L.rg_copy_records_gops.argtypes = [P, ctypes.c_int32, P]
     L.rg_analyse_gops_async.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
+    L.rg_pipeline_work_list.restype = ctypes.c_int64
+    L.rg_pipeline_work_list.argtypes = [ctypes.c_int32] * 7 + [P, P, ctypes.c_int64, P]
     L.rg_writer_create.restype = P
     L.rg_writer_create.argtypes = [ctypes.POINTER(RgConfig), ctypes.c_int32, ctypes.c_int32]
     L.rg_writer_destroy.argtypes = [P]
