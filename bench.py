@@ -54,6 +54,29 @@ def dist_env():
     return rank, world, local
 
 
+def bench_config(world: int, mode: str = "pipelined") -> dict:
+    """The workload both arms report (the engine arm and --impl reference)."""
+    return {"workload": "1080p High QP26 Balanced, 120 frames = 8 GOPs x 15 (IDR + 14 P) side by side",
+            "mode": mode, "width": W, "height": H, "frames_per_gpu": FRAMES, "gop": GOP, "qp": QP,
+            "profile": "high", "motion_px": MOTION, "rects": RECTS, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (373 MB source clip per GPU)"}
+
+
+def clip_seed(rank: int) -> int:
+    """Each rank encodes its own clip (replicas, weak scaling): distinct content per GPU."""
+    return 2000 + 97 * rank
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's time (every multi-GPU number is the max over ranks)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_clip(seed: int, frames: int = FRAMES):
     from ragdoll_b200.synth import grating_clip
     return grating_clip(W, H, frames, seed=seed, motion=MOTION, rects=RECTS)
@@ -146,9 +169,8 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings)",
-        "config": {"workload": "1080p High QP26, 8 GOPs x 15 frames (Balanced); step = 3 frames of each GOP",
-                   "width": W, "height": H, "qp": QP, "profile": "high", "gops": gops},
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
+        "config": bench_config(world),
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": min(cores, gops), "kind": "port",
                          "sample": f"{gops} GOPs x {fpg} frames of the 1080p clip, GOP-parallel"},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -170,7 +192,7 @@ def run_engine(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     gops = FRAMES // GOP
-    clip = make_clip(2000 + 97 * rank, FRAMES)
+    clip = make_clip(clip_seed(rank), FRAMES)
     # source clip resident in HBM: one contiguous buffer per frame (Y | U | V)
     cw, ch = (W + 1) // 2, (H + 1) // 2
     fbytes = W * H + 2 * cw * ch
@@ -238,12 +260,6 @@ def run_engine(args, rank, world, local):
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     # warm-up
     for _ in range(args.warmup):
@@ -263,7 +279,7 @@ def run_engine(args, rank, world, local):
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    dev_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    dev_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, f"cuda:{local}")
 
     # end to end through the host-buffer C ABI (records copied back every batch)
     host_step()
@@ -275,7 +291,7 @@ def run_engine(args, rank, world, local):
         host_step()
     eng.sync()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps, dist, f"cuda:{local}")
 
     # per-launch duration of the dominant kernel
     steps_per_frame = (eng.mb_w - 1) + 2 * (eng.mb_h - 1) + 1 + 3
@@ -312,12 +328,8 @@ def run_engine(args, rank, world, local):
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev_ms, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings, BASELINE config 2 shape)",
-            "config": {"workload": "1080p High QP26 Balanced, 120 frames = 8 GOPs x 15 (IDR + 14 P) side by side",
-                       "mode": args.mode,
-                       "width": W, "height": H, "frames_per_gpu": FRAMES, "gop": GOP, "qp": QP, "profile": "high",
-                       "motion_px": MOTION, "rects": RECTS, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (373 MB source clip per GPU)"},
+            "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
+            "config": bench_config(world, args.mode),
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
                     "d2h_bytes_per_step": GOP * gops * eng.n_mb * 852},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
