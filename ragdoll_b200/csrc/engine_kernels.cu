@@ -509,8 +509,19 @@ __device__ __noinline__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint3
   return cbp;
 }
 
+// Zig-zag index of (row y, column x) of an 8x8 block (frame scan, Table 8-13): diagonal s = x + y,
+// walked up-right on even s and down-left on odd s.
+__device__ __forceinline__ int zigzag8(int y, int x) {
+  int s = x + y;
+  if (s < 8) return s * (s + 1) / 2 + ((s & 1) ? y : x);
+  return 64 - (16 - s) * (15 - s) / 2 + ((s & 1) ? 7 - x : 7 - y);
+}
+
 // Luma 8x8 residual of pred_y, quantised (inter) and decimated into sm.coef8
-// (enc.rs:2041 quant_luma_8x8_inter). Lanes 8b..8b+7 own block b. Returns cbp; *nnz8 = count.
+// (enc.rs:2041 quant_luma_8x8_inter). Lanes 8b..8b+7 own block b: a row each in the first pass,
+// column q each in the second. The decimation score of a block comes from the bitmask of its
+// nonzero zig-zag positions (run of zeros below each, weights 3 / 2 / 1 / 0 for runs of
+// 0-3 / 4-11 / 12-23 / longer, enc.rs:559 with the 8x8 table). Returns cbp; *nnz8 = count.
 __device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint32_t* nnz8) {
   int lane = lane_id();
   int b = lane >> 3, q = lane & 7;
@@ -529,35 +540,47 @@ __device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint3
     for (int x = 0; x < 8; x++) sm.t8[b * 64 + q * 8 + x] = o[x];
   }
   __syncwarp();
-  int my_nz = 0, my_big = 0;
-  {  // column pass: column q
+  uint32_t mf6[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) mf6[k] = c_mf8[qp % 6][k];
+  int any = 0, big = 0;
+  unsigned long long zmask = 0;
+  {  // column pass: column q, then quantisation
     int a[8], o[8];
 #pragma unroll
     for (int y = 0; y < 8; y++) a[y] = sm.t8[b * 64 + y * 8 + q];
     fdct8_1d(a, o);
 #pragma unroll
     for (int y = 0; y < 8; y++) {
-      int i = y * 8 + q;
-      int l = quant_level((int16_t)o[y], c_mf8[qp % 6][pos8(i)], bias, shift);
+      int i = y * 8 + q, cls = pos8(i);
+      uint32_t mf = cls == 0 ? mf6[0] : cls == 1 ? mf6[1] : cls == 2 ? mf6[2] : cls == 3 ? mf6[3] : cls == 4 ? mf6[4] : mf6[5];
+      int l = quant_level((int16_t)o[y], mf, bias, shift);
       sm.coef8[b * 64 + i] = (int16_t)l;
-      if (l) my_nz = 1;
-      if (l > 1 || l < -1) my_big = 1;
+      any |= l != 0;
+      big |= l > 1 || l < -1;
+      if (l) zmask |= 1ull << zigzag8(y, q);
     }
   }
-  __syncwarp();
-  int bnz = my_nz, bbig = my_big;
 #pragma unroll
-  for (int o = 1; o < 8; o <<= 1) { bnz |= __shfl_xor_sync(FULL, bnz, o); bbig |= __shfl_xor_sync(FULL, bbig, o); }
-  uint32_t score = 0;
-  if (q == 0) {
-    if (!bnz) score = 0;
-    else if (bbig) score = 9;
-    else {
-      int16_t zz[64];
-      for (int i = 0; i < 64; i++) zz[i] = sm.coef8[b * 64 + c_scan8[i]];
-      score = decimate_score(zz, 64, c_dec8);
+  for (int o = 1; o < 8; o <<= 1) {
+    any |= __shfl_xor_sync(FULL, any, o);
+    big |= __shfl_xor_sync(FULL, big, o);
+    zmask |= __shfl_xor_sync(FULL, zmask, o);
+  }
+  // lane q scores zig-zag positions 8q .. 8q + 7
+  uint32_t part = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int z = 8 * q + k;
+    if ((zmask >> z) & 1ull) {
+      unsigned long long below = zmask & ((1ull << z) - 1ull);
+      int run = z - (below ? 63 - __clzll((long long)below) : -1) - 1;
+      part += run < 4 ? 3u : (run < 12 ? 2u : (run < 24 ? 1u : 0u));
     }
   }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) part += __shfl_xor_sync(FULL, part, o);
+  uint32_t score = !any ? 0u : (big ? 9u : part);
   int cbp = 0;
   uint32_t total = 0;
 #pragma unroll
@@ -572,8 +595,7 @@ __device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint3
 #pragma unroll
     for (int y = 0; y < 8; y++) sm.coef8[b * 64 + y * 8 + q] = 0;
   } else {
-#pragma unroll
-    for (int y = 0; y < 8; y++) cnt += sm.coef8[b * 64 + y * 8 + q] != 0;
+    cnt = __popcll(zmask) * (q == 0);
   }
   __syncwarp();
   *nnz8 = wsum(cnt);
@@ -1609,9 +1631,12 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   int cbpl = cbp4;
   bool use8 = false;
   if (fp.t8x8 && cbp4) {
-    uint32_t nnz4 = 0;
-    if (lane < 16)
-      for (int i = 0; i < 16; i++) nnz4 += sm.coef[lane * 16 + i] != 0;
+    uint32_t nnz4 = 0;  // nonzero levels of the 4x4 coding: four words (eight levels) per lane
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t w = ((const uint32_t*)sm.coef)[lane + 32 * k];
+      nnz4 += ((w & 0xffffu) != 0) + ((w >> 16) != 0);
+    }
     nnz4 = wsum(nnz4);
     uint32_t nnz8;
     int cbp8 = luma8x8_inter(fp, sm, &nnz8);
@@ -1639,9 +1664,9 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   bool t8flag = use8 && cbpl != 0;
   uint16_t nzm;
   if (use8) {
-    int b = lane >> 3, q = lane & 7;
+    int b = lane >> 3, q = lane & 7;  // column q of block b, each level to its zig-zag slot
 #pragma unroll
-    for (int k = 0; k < 8; k++) rec->luma[b * 64 + q * 8 + k] = sm.coef8[b * 64 + c_scan8[q * 8 + k]];
+    for (int y = 0; y < 8; y++) rec->luma[b * 64 + zigzag8(y, q)] = sm.coef8[b * 64 + y * 8 + q];
     nzm = 0;
     for (int k = 0; k < 4; k++) if ((cbpl >> k) & 1) nzm |= (uint16_t)(0xF << (4 * k));
   } else {
