@@ -360,6 +360,17 @@ __device__ __forceinline__ uint2 qpel8(const QSrc& q) {
   uint2 b = lds8(q.b + i * q.sb + j0);
   return make_uint2(__vavgu4(a.x, b.x), __vavgu4(a.y, b.y));
 }
+// Cost of a full-pel position (mx, my): the warp's SAD of the 16x16 block (this lane's 8 source
+// samples sv against its 8 reference samples r) plus lambda * bits of the vector difference to
+// the predictor (enc.rs:1207 cost). Shared by the candidates and the diamond steps.
+__device__ __noinline__ uint32_t fullpel_cost(uint2 sv, uint2 r, int mx, int my, int mvp0, int mvp1, uint32_t lambda) {
+  return wsum(vsad8(sv, r)) + mvd_cost(mx * 4 - mvp0, lambda) + mvd_cost(my * 4 - mvp1, lambda);
+}
+// This lane's SAD against the quarter-sample prediction at window position (wx, wy), phase
+// (fx, fy): shared by the candidates of the sub-pel search.
+__device__ __noinline__ uint32_t qpel_sad(const Smem& sm, uint2 sv, int wx, int wy, int fx, int fy) {
+  return vsad8(sv, qpel8(qpel_src(sm, wx, wy, fx, fy)));
+}
 __device__ __forceinline__ uint2 src8(const Smem& sm) {
   int lane = lane_id();
   return *(const uint2*)&sm.src_y[(lane >> 1) * 16 + (lane & 1) * 8];
@@ -1501,13 +1512,8 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   // 2. motion search (enc.rs:3084-3117)
   const uint8_t* ref = sd.ref_y;
   int stride = fp.stride_y;
-  int cand[5][2];
-  int n = 0;
-  cand[n][0] = mvp0; cand[n][1] = mvp1; n++;
-  cand[n][0] = 0; cand[n][1] = 0; n++;
-  if (mbx > 0) { cand[n][0] = a0; cand[n][1] = a1; n++; }
-  if (mby > 0) { cand[n][0] = b0; cand[n][1] = b1; n++; }
-  cand[n][0] = prevmb.mv[0]; cand[n][1] = prevmb.mv[1]; n++;
+  // candidates in order: predictor, zero, left (if any), top (if any), co-located of the previous
+  // picture -- five fixed slots, the left / top ones skipped when absent
   int imin0 = (bmin0 + 3) >> 2, imin1 = (bmin1 + 3) >> 2, imax0 = bmax0 >> 2, imax1 = bmax1 >> 2;
   uint2 sv = src8(sm);
   const uint8_t* base = ref + (long)(y0 + (lane >> 1)) * stride + x0 + (lane & 1) * 8;
@@ -1516,46 +1522,55 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   // clamped full-pel candidates, their samples loaded together, then costed in order (a
   // repeated position is skipped)
   int cmx[5], cmy[5];
+  bool cval[5];
   uint2 cref[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) {
-    int kk = min(k, n - 1);
-    cmx[k] = min(max((cand[kk][0] + 2) >> 2, imin0), imax0);
-    cmy[k] = min(max((cand[kk][1] + 2) >> 2, imin1), imax1);
+    int vx = k == 0 ? mvp0 : k == 1 ? 0 : k == 2 ? a0 : k == 3 ? b0 : prevmb.mv[0];
+    int vy = k == 0 ? mvp1 : k == 1 ? 0 : k == 2 ? a1 : k == 3 ? b1 : prevmb.mv[1];
+    cval[k] = k == 2 ? mbx > 0 : (k == 3 ? mby > 0 : true);
+    cmx[k] = min(max((vx + 2) >> 2, imin0), imax0);
+    cmy[k] = min(max((vy + 2) >> 2, imin1), imax1);
     cref[k] = ldg8(base + (long)cmy[k] * stride + cmx[k]);
   }
 #pragma unroll
   for (int k = 0; k < 5; k++) {
-    bool dup = k >= n;
+    bool use = cval[k];  // absent, or at the position of an earlier candidate: skipped
 #pragma unroll
-    for (int j = 0; j < k; j++) dup |= (cmx[j] == cmx[k] && cmy[j] == cmy[k]);
-    uint32_t s = wsum(dup ? 0u : vsad8(sv, cref[k]));
-    uint32_t cost = s + mvd_cost(cmx[k] * 4 - mvp0, lambda) + mvd_cost(cmy[k] * 4 - mvp1, lambda);
-    if (!dup && cost < best_cost) { best_cost = cost; best0 = cmx[k]; best1 = cmy[k]; }
+    for (int j = 0; j < k; j++) use &= !(cval[j] && cmx[j] == cmx[k] && cmy[j] == cmy[k]);
+    if (!use) continue;  // uniform across the warp
+    uint32_t cost = fullpel_cost(sv, cref[k], cmx[k], cmy[k], mvp0, mvp1, lambda);
+    if (cost < best_cost) { best_cost = cost; best0 = cmx[k]; best1 = cmy[k]; }
   }
-  // diamond (enc.rs:1207-1272)
+  // diamond (enc.rs:1207-1272): up, left, right, down around the best, first strict minimum
+  // wins; each step's four loads are issued together
+#pragma unroll 1
   for (int it = 0; it < 16; it++) {
-    int pts[4][2] = {{best0, best1 - 1}, {best0 - 1, best1}, {best0 + 1, best1}, {best0, best1 + 1}};
-    int moved = -1;
-    uint32_t costs[4];
     const uint8_t* cp = base + (long)best1 * stride + best0;
+    uint2 r[4];
     bool in[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) in[k] = pts[k][0] >= imin0 && pts[k][0] <= imax0 && pts[k][1] >= imin1 && pts[k][1] <= imax1;
-    uint32_t s0 = in[0] ? vsad8(sv, ldg8(cp - stride)) : 0;
-    uint32_t s1 = in[1] ? vsad8(sv, ldg8(cp - 1)) : 0;
-    uint32_t s2 = in[2] ? vsad8(sv, ldg8(cp + 1)) : 0;
-    uint32_t s3 = in[3] ? vsad8(sv, ldg8(cp + stride)) : 0;
-    s0 = wsum(s0); s1 = wsum(s1); s2 = wsum(s2); s3 = wsum(s3);
-    uint32_t sads[4] = {s0, s1, s2, s3};
+    for (int k = 0; k < 4; k++) {
+      int dx = k == 1 ? -1 : (k == 2 ? 1 : 0), dy = k == 0 ? -1 : (k == 3 ? 1 : 0);
+      int px = best0 + dx, py = best1 + dy;
+      in[k] = px >= imin0 && px <= imax0 && py >= imin1 && py <= imax1;
+      r[k] = in[k] ? ldg8(cp + dy * stride + dx) : make_uint2(0u, 0u);
+    }
+    int nb0 = best0, nb1 = best1;
 #pragma unroll
-    for (int k = 0; k < 4; k++)
-      costs[k] = in[k] ? sads[k] + mvd_cost(pts[k][0] * 4 - mvp0, lambda) + mvd_cost(pts[k][1] * 4 - mvp1, lambda) : UMAX;
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-      if (in[k] && costs[k] < best_cost) { best_cost = costs[k]; moved = k; }
-    if (moved < 0) break;
-    best0 = pts[moved][0]; best1 = pts[moved][1];
+    for (int k = 0; k < 4; k++) {
+      int dx = k == 1 ? -1 : (k == 2 ? 1 : 0), dy = k == 0 ? -1 : (k == 3 ? 1 : 0);
+      if (!in[k]) continue;  // uniform across the warp
+      uint32_t cost = fullpel_cost(sv, r[k], best0 + dx, best1 + dy, mvp0, mvp1, lambda);
+      if (cost < best_cost) {
+        best_cost = cost;
+        nb0 = best0 + dx;
+        nb1 = best1 + dy;
+      }
+    }
+    if (nb0 == best0 && nb1 == best1) break;
+    best0 = nb0;
+    best1 = nb1;
   }
   int mv0, mv1;
   {
@@ -1573,8 +1588,10 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
       build_hpel(sm, 7);
       int q0 = fm0, q1 = fm1;
       uint32_t bc = best_cost;
+#pragma unroll 1
       for (int si = 0; si < 2; si++) {
         int st = si == 0 ? 2 : 1, iters = si == 0 ? 1 : 2;
+#pragma unroll 1
         for (int it = 0; it < iters; it++) {
           int f0 = q0, f1 = q1;
           int dd[4][2] = {{0, -st}, {-st, 0}, {st, 0}, {0, st}};
@@ -1583,11 +1600,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
           for (int k = 0; k < 4; k++) {
             int cx = f0 + dd[k][0], cy = f1 + dd[k][1];
             bool ok = abs(cx - fm0) <= 3 && abs(cy - fm1) <= 3 && cx >= bmin0 && cx <= bmax0 && cy >= bmin1 && cy <= bmax1;
-            uint32_t s = 0;
-            if (ok) {
-              int wx = (cx >> 2) - best0 + 1, wy = (cy >> 2) - best1 + 1;
-              s = vsad8(sv, qpel8(qpel_src(sm, wx, wy, cx & 3, cy & 3)));
-            }
+            uint32_t s = ok ? qpel_sad(sm, sv, (cx >> 2) - best0 + 1, (cy >> 2) - best1 + 1, cx & 3, cy & 3) : 0u;
             s = wsum(s);
             cc[k] = ok ? s + mvd_cost(cx - mvp0, lambda) + mvd_cost(cy - mvp1, lambda) : UMAX;
           }
