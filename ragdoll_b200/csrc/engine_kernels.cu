@@ -439,7 +439,7 @@ __device__ __noinline__ void quant4x4_blocks(Smem& sm, bool chroma, int nblocks,
   uint32_t mf = c_mf4[qp % 6][pos4(p)];
   bool counted = zi >= first;
   my_nz = my_big = my_score = 0;
-#pragma unroll 2
+#pragma unroll 1
   for (int it = 0; it < nblocks / 2; it++) {
     int b = 2 * it + h;
     const uint8_t *s, *pr;
@@ -556,21 +556,23 @@ __device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint3
   for (int k = 0; k < 6; k++) mf6[k] = c_mf8[qp % 6][k];
   int any = 0, big = 0;
   unsigned long long zmask = 0;
-  {  // column pass: column q, then quantisation
+  {  // column pass: column q (back into t8), then quantisation row by row
     int a[8], o[8];
 #pragma unroll
     for (int y = 0; y < 8; y++) a[y] = sm.t8[b * 64 + y * 8 + q];
     fdct8_1d(a, o);
 #pragma unroll
-    for (int y = 0; y < 8; y++) {
-      int i = y * 8 + q, cls = pos8(i);
-      uint32_t mf = cls == 0 ? mf6[0] : cls == 1 ? mf6[1] : cls == 2 ? mf6[2] : cls == 3 ? mf6[3] : cls == 4 ? mf6[4] : mf6[5];
-      int l = quant_level((int16_t)o[y], mf, bias, shift);
-      sm.coef8[b * 64 + i] = (int16_t)l;
-      any |= l != 0;
-      big |= l > 1 || l < -1;
-      if (l) zmask |= 1ull << zigzag8(y, q);
-    }
+    for (int y = 0; y < 8; y++) sm.t8[b * 64 + y * 8 + q] = o[y];
+  }
+#pragma unroll 1
+  for (int y = 0; y < 8; y++) {
+    int i = y * 8 + q, cls = pos8(i);
+    uint32_t mf = cls == 0 ? mf6[0] : cls == 1 ? mf6[1] : cls == 2 ? mf6[2] : cls == 3 ? mf6[3] : cls == 4 ? mf6[4] : mf6[5];
+    int l = quant_level((int16_t)sm.t8[b * 64 + i], mf, bias, shift);
+    sm.coef8[b * 64 + i] = (int16_t)l;
+    any |= l != 0;
+    big |= l > 1 || l < -1;
+    if (l) zmask |= 1ull << zigzag8(y, q);
   }
 #pragma unroll
   for (int o = 1; o < 8; o <<= 1) {
@@ -580,7 +582,7 @@ __device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint3
   }
   // lane q scores zig-zag positions 8q .. 8q + 7
   uint32_t part = 0;
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < 8; k++) {
     int z = 8 * q + k;
     if ((zmask >> z) & 1ull) {
@@ -662,7 +664,7 @@ __device__ __noinline__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
   int lane = lane_id(), p = lane & 15, h = lane >> 4, xl = p & 3, yl = p >> 2;
   int qmul = (c_dq4[qpc % 6][0] * 16) << (qpc / 6 + 2);
   int dqs = (int)c_dq4[qpc % 6][pos4(p)] << (qpc / 6);
-#pragma unroll 2
+#pragma unroll 1
   for (int it = 0; it < 4; it++) {
     int b = 2 * it + h, pl = b >> 2, bb = b & 3;
     int a = sm.cdc[pl * 4], bv = sm.cdc[pl * 4 + 1], c = sm.cdc[pl * 4 + 2], d = sm.cdc[pl * 4 + 3];
@@ -682,7 +684,7 @@ __device__ __noinline__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
 __device__ __noinline__ void recon_luma4x4(Smem& sm, int qp, int cbp) {
   int lane = lane_id(), p = lane & 15, h = lane >> 4, xl = p & 3, yl = p >> 2;
   int dqs = (int)c_dq4[qp % 6][pos4(p)] << (qp / 6);
-#pragma unroll 2
+#pragma unroll 1
   for (int it = 0; it < 8; it++) {
     int b = 2 * it + h;
     bool coded = (cbp >> (b >> 2)) & 1;
