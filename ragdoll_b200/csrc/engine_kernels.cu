@@ -75,6 +75,7 @@ struct __align__(16) Smem {
   int32_t red[32];
 };
 static_assert(offsetof(Smem, coef) % 4 == 0 && offsetof(Smem, ccoef) % 4 == 0, "level arrays cleared by words");
+static_assert(offsetof(rg_mb_out, luma) % 4 == 0 && sizeof(rg_mb_out) % 4 == 0, "record levels written by words");
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ MbInfo ld_info(const MbInfo* p) {
@@ -520,6 +521,17 @@ __device__ __noinline__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint3
   return cbp;
 }
 
+// The 1-D forward 8x8 transform in place on p[0], p[stride], ..., p[7 * stride] (row and column
+// passes share it).
+__device__ __noinline__ void fdct8_inplace(int* p, int stride) {
+  int a[8], o[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = p[k * stride];
+  fdct8_1d(a, o);
+#pragma unroll
+  for (int k = 0; k < 8; k++) p[k * stride] = o[k];
+}
+
 // Zig-zag index of (row y, column x) of an 8x8 block (frame scan, Table 8-13): diagonal s = x + y,
 // walked up-right on even s and down-left on odd s.
 __device__ __forceinline__ int zigzag8(int y, int x) {
@@ -539,31 +551,20 @@ __device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint3
   int bx = (b & 1) * 8, by = (b >> 1) * 8;
   int qp = fp.qp;
   uint32_t shift = 16 + qp / 6, bias = (1u << shift) / 6u;
-  {  // row pass: row q of block b
-    int a[8], o[8];
-#pragma unroll
-    for (int x = 0; x < 8; x++) {
-      int off = (by + q) * 16 + bx + x;
-      a[x] = (int)sm.src_y[off] - (int)sm.pred_y[off];
-    }
-    fdct8_1d(a, o);
-#pragma unroll
-    for (int x = 0; x < 8; x++) sm.t8[b * 64 + q * 8 + x] = o[x];
+  // residual of row q, then the row pass and (after all rows) the column pass in place
+#pragma unroll 1
+  for (int x = 0; x < 8; x++) {
+    int off = (by + q) * 16 + bx + x;
+    sm.t8[b * 64 + q * 8 + x] = (int)sm.src_y[off] - (int)sm.pred_y[off];
   }
+  fdct8_inplace(&sm.t8[b * 64 + q * 8], 1);
   __syncwarp();
   uint32_t mf6[6];
 #pragma unroll
   for (int k = 0; k < 6; k++) mf6[k] = c_mf8[qp % 6][k];
   int any = 0, big = 0;
   unsigned long long zmask = 0;
-  {  // column pass: column q (back into t8), then quantisation row by row
-    int a[8], o[8];
-#pragma unroll
-    for (int y = 0; y < 8; y++) a[y] = sm.t8[b * 64 + y * 8 + q];
-    fdct8_1d(a, o);
-#pragma unroll
-    for (int y = 0; y < 8; y++) sm.t8[b * 64 + y * 8 + q] = o[y];
-  }
+  fdct8_inplace(&sm.t8[b * 64 + q], 8);  // column q; then quantisation row by row
 #pragma unroll 1
   for (int y = 0; y < 8; y++) {
     int i = y * 8 + q, cls = pos8(i);
@@ -675,6 +676,55 @@ __device__ __noinline__ void chroma_recon(int qpc, int cbpc, Smem& sm) {
     int r = (int16_t)((inv4_pass(inv4_pass(v, 1, xl), 4, yl) + 32) >> 6);
     uint8_t* pr = (pl ? sm.pred_v : sm.pred_u) + (bb >> 1) * 32 + (bb & 1) * 4 + yl * 8 + xl;
     *pr = (uint8_t)clip255(*pr + r);
+  }
+  __syncwarp();
+}
+
+// Raster position of each 4x4 zig-zag index, 4 bits per index (frame scan, Table 8-12).
+constexpr unsigned long long kScan4Packed = 0xfeb7adc963258410ull;
+
+// The 1-D inverse 8x8 transform in place on p[0], p[stride], ..., p[7 * stride] (rows and columns
+// of the 8x8 reconstruction share it).
+__device__ __noinline__ void idct8_inplace(int* p, int stride) {
+  int d[8], o[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) d[k] = p[k * stride];
+  idct8_1d(d, o);
+#pragma unroll
+  for (int k = 0; k < 8; k++) p[k * stride] = o[k];
+}
+
+// Adds the dequantised 8x8 residual of the coded blocks of sm.coef8 to pred_y (enc.rs:2013
+// recon_8x8: dequantize_block8x8, h264.rs:1403, then h264_idct8_add, h264_idct.rs:207).
+// Lanes 8b..8b+7 own block b: row q, then column q.
+__device__ __noinline__ void recon_luma8x8(Smem& sm, int qp, int cbp) {
+  int lane = lane_id(), b = lane >> 3, q = lane & 7;
+  bool coded = (cbp >> b) & 1;
+  int qdiv = qp / 6, rem = qp % 6;
+  int dq6[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) dq6[k] = c_dq8[rem][k];
+  if (coded) {
+#pragma unroll 1
+    for (int x = 0; x < 8; x++) {
+      int i = q * 8 + x, cls = pos8(i);
+      int v = cls == 0 ? dq6[0] : cls == 1 ? dq6[1] : cls == 2 ? dq6[2] : cls == 3 ? dq6[3] : cls == 4 ? dq6[4] : dq6[5];
+      int l = sm.coef8[b * 64 + i];
+      int dv = qdiv >= 2 ? l * (v << (qdiv - 2)) : ((l * v + (1 << (1 - qdiv))) >> (2 - qdiv));
+      sm.t8[b * 64 + i] = clamp_i16(dv);
+    }
+    idct8_inplace(&sm.t8[b * 64 + q * 8], 1);
+  }
+  __syncwarp();
+  if (coded) {
+    idct8_inplace(&sm.t8[b * 64 + q], 8);
+    int bx = (b & 1) * 8, by = (b >> 1) * 8;
+#pragma unroll 1
+    for (int y = 0; y < 8; y++) {
+      int off = (by + y) * 16 + bx + q;
+      int v = (int)((unsigned)sm.t8[b * 64 + y * 8 + q] + 32u) >> 6;
+      sm.pred_y[off] = (uint8_t)clip255((int)((unsigned)sm.pred_y[off] + (unsigned)v));
+    }
   }
   __syncwarp();
 }
@@ -1680,21 +1730,26 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   uint16_t nzm;
   if (use8) {
     int b = lane >> 3, q = lane & 7;  // column q of block b, each level to its zig-zag slot
-#pragma unroll
+#pragma unroll 1
     for (int y = 0; y < 8; y++) rec->luma[b * 64 + zigzag8(y, q)] = sm.coef8[b * 64 + y * 8 + q];
     nzm = 0;
     for (int k = 0; k < 4; k++) if ((cbpl >> k) & 1) nzm |= (uint16_t)(0xF << (4 * k));
   } else {
-    uint32_t bnz = 0;
-    if (lane < 16) {
+    // word w of the 4x4 levels (zig-zag order) holds levels 2(w & 7), 2(w & 7) + 1 of block w / 8;
+    // lanes 8j..8j+7 of step k cover block 4k + j
+    uint32_t nz = 0;
+#pragma unroll 1
+    for (int k = 0; k < 4; k++) {
+      int w = lane + 32 * k, b = w >> 3, i = (w & 7) * 2;
+      int r0 = (int)((kScan4Packed >> (4 * i)) & 15), r1 = (int)((kScan4Packed >> (4 * i + 4)) & 15);
+      int16_t v0 = sm.coef[b * 16 + r0], v1 = sm.coef[b * 16 + r1];
+      ((uint32_t*)rec->luma)[w] = (uint32_t)(uint16_t)v0 | ((uint32_t)(uint16_t)v1 << 16);
+      uint32_t bal = __ballot_sync(FULL, (v0 | v1) != 0);
 #pragma unroll
-      for (int i = 0; i < 16; i++) {
-        int16_t v = sm.coef[lane * 16 + c_scan4[i]];
-        rec->luma[lane * 16 + i] = v;
-        bnz |= v != 0;
-      }
+      for (int j = 0; j < 4; j++)
+        if ((bal >> (8 * j)) & 0xffu) nz |= 1u << (4 * k + j);
     }
-    nzm = (uint16_t)__ballot_sync(FULL, lane < 16 && bnz);
+    nzm = (uint16_t)nz;
   }
   if (lane < 16) { rec->luma_dc[lane] = 0; rec->i4_modes[lane] = 2; }
   record_chroma(rec, sm, cbpc);
@@ -1704,35 +1759,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   }
   // reconstruction
   if (use8) {
-    int b = lane >> 3, q = lane & 7;
-    bool coded = (cbpl >> b) & 1;
-    if (coded) {  // dequantize_block8x8 (h264.rs:1403) then rows of the inverse transform
-      int qdiv = qp / 6, rem = qp % 6;
-      int d[8], o[8];
-#pragma unroll
-      for (int x = 0; x < 8; x++) {
-        int i = q * 8 + x, v = c_dq8[rem][pos8(i)], l = sm.coef8[b * 64 + i];
-        int dv = qdiv >= 2 ? l * (v << (qdiv - 2)) : ((l * v + (1 << (1 - qdiv))) >> (2 - qdiv));
-        d[x] = clamp_i16(dv);
-      }
-      idct8_1d(d, o);
-#pragma unroll
-      for (int x = 0; x < 8; x++) sm.t8[b * 64 + q * 8 + x] = o[x];
-    }
-    __syncwarp();
-    if (coded) {
-      int d[8], o[8];
-#pragma unroll
-      for (int y = 0; y < 8; y++) d[y] = sm.t8[b * 64 + y * 8 + q];
-      idct8_1d(d, o);
-      int bx = (b & 1) * 8, by = (b >> 1) * 8;
-#pragma unroll
-      for (int y = 0; y < 8; y++) {
-        int off = (by + y) * 16 + bx + q;
-        int v = (int)((unsigned)o[y] + 32u) >> 6;
-        sm.pred_y[off] = (uint8_t)clip255((int)((unsigned)sm.pred_y[off] + (unsigned)v));
-      }
-    }
+    recon_luma8x8(sm, qp, cbpl);
   } else if (cbpl) {
     recon_luma4x4(sm, qp, cbpl);
   }
