@@ -76,6 +76,7 @@ struct __align__(16) Smem {
 };
 static_assert(offsetof(Smem, coef) % 4 == 0 && offsetof(Smem, ccoef) % 4 == 0, "level arrays cleared by words");
 static_assert(offsetof(rg_mb_out, luma) % 4 == 0 && sizeof(rg_mb_out) % 4 == 0, "record levels written by words");
+static_assert(offsetof(Smem, pred_y) % 8 == 0 && offsetof(Smem, tmp_y) % 8 == 0, "16x16 predictions written 8 bytes per lane");
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ MbInfo ld_info(const MbInfo* p) {
@@ -210,7 +211,7 @@ __device__ __forceinline__ uint32_t decimate_score(const int16_t* s, int n, cons
   return score;
 }
 // SATD of a 4x4 block (metrics.rs:705, halved).
-__device__ __forceinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
+__device__ __noinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
   int t[4][4];
 #pragma unroll
   for (int y = 0; y < 4; y++) {
@@ -782,12 +783,23 @@ __device__ __forceinline__ int dc16(const Smem& sm, bool ht, bool hl) {
 }
 __device__ __noinline__ void pred16_into(int mode, Smem& sm, uint8_t* dst, bool ht, bool hl, int tl) {
   int lane = lane_id();
-  int dc = mode == 2 ? dc16(sm, ht, hl) : 0;
-  int pa = 0, pb = 0, pc = 0;
-  if (mode == 3) plane16_params(sm, ht, hl, tl, pa, pb, pc);
   int y = lane >> 1, x0 = (lane & 1) * 8;
-#pragma unroll
-  for (int k = 0; k < 8; k++) dst[y * 16 + x0 + k] = (uint8_t)pred16_sample(mode, sm, ht, hl, tl, dc, pa, pb, pc, x0 + k, y);
+  uint8_t* o = dst + y * 16 + x0;  // this lane's 8 samples (8-byte aligned)
+  if (mode == 3) {
+    int pa, pb, pc;
+    plane16_params(sm, ht, hl, tl, pa, pb, pc);
+#pragma unroll 1
+    for (int k = 0; k < 8; k++) o[k] = (uint8_t)pred16_sample(3, sm, ht, hl, tl, 0, pa, pb, pc, x0 + k, y);
+  } else {
+    uint2 v;
+    if (mode == 0) {
+      v = ht ? lds8(&sm.top[x0]) : make_uint2(0x80808080u, 0x80808080u);
+    } else {
+      uint32_t b = mode == 1 ? (hl ? sm.left[y] : 128u) : (uint32_t)dc16(sm, ht, hl);
+      v = make_uint2(b * 0x01010101u, b * 0x01010101u);
+    }
+    *(uint2*)o = v;
+  }
   __syncwarp();
 }
 // Intra 16x16 analysis (enc.rs:1637 analyse_i16_edges): SATD per mode; returns best mode.
