@@ -149,3 +149,35 @@ def test_async_gops_match_sync_and_recover_from_timeout():
         for s in range(S):
             for a, c in zip(sync.recon_coded(s), eng.recon_coded(s)):
                 assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("w,h,qp,profile", [
+    (16, 16, 26, 2),     # one macroblock
+    (48, 16, 30, 0),     # one row of three
+    (16, 64, 22, 1),     # one column of four
+    (33, 17, 1, 2),      # ragged in both directions, lowest QP
+    (72, 40, 51, 2),     # highest QP
+    (80, 48, 1, 0),      # lowest QP, Baseline
+])
+def test_edge_shapes_and_qps(w, h, qp, profile):
+    frames = grating_clip(w, h, 4, seed=w * 7 + h + qp, motion=5.0, rects=1)
+    eng = _engine(w, h, qp, profile)
+    fails = run_parity(frames, w, h, qp, profile, keyint=3, engine=eng)
+    assert not fails, "\n".join(fails)
+
+
+def test_pipelined_many_small_streams():
+    """32 streams of 48x32 pictures in one persistent launch: every picture equals the oracle."""
+    from oracle_lib import OracleEncoder
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
+    from gpu_parity_util import first_record_mismatch
+    w, h, qp, S, F = 48, 32, 28, 32, 4
+    clips = [grating_clip(w, h, F, seed=3000 + s, motion=3.0, rects=1) for s in range(S)]
+    eng = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)]
+    recs = eng.analyse_gops([[clips[s][f] for s in range(S)] for f in range(F)], kinds)
+    for s in range(S):
+        orc = OracleEncoder(w, h, qp, profile=2, keyint=F + 1)
+        for f in range(F):
+            _, ref = orc.encode(clips[s][f])
+            assert first_record_mismatch(ref, recs[f, s], orc.mb_w) is None, f"stream {s} picture {f}"
