@@ -308,6 +308,52 @@ size_t rg_writer_bound(const rg_writer* writer);
  * into out; returns its size in bytes, or a negative RG_ERR_* (the buffer too small included). */
 int64_t rg_writer_picture(rg_writer* writer, const rg_mb_out* records, int32_t kind, uint8_t* out, size_t cap);
 
+/* ---- Containers (host) ------------------------------------------------------------------ */
+/*
+ * The muxers `ragdoll transcode` writes its H.264 output with: fast-start MP4
+ * (crates/ragdoll-format/src/mp4.rs:1668 Mp4Muxer, :1746 finish) and Matroska
+ * (crates/ragdoll-format/src/mkv.rs:840 MkvMuxer, :906 finish), one H.264 video track.
+ * Access units go in as Annex-B (what rg_writer_picture returns); SPS and PPS move into the avcC
+ * record (crates/ragdoll-format/src/mpegts.rs:273 build_avcc_from_sps_pps) and samples are
+ * 4-byte length-prefixed (mpegts.rs:123 h264_annex_b_to_avcc_au). Given the same access units,
+ * frame rate and size, the output is the reference's file byte for byte. Host code only.
+ */
+#define RG_CONTAINER_MP4 0
+#define RG_CONTAINER_MKV 1
+
+typedef struct rg_mux rg_mux;
+/* fps_num / fps_den: the frame rate (pictures are evenly spaced on a 90 kHz clock). */
+rg_mux* rg_mux_create(int32_t container, int32_t width, int32_t height, int32_t fps_num, int32_t fps_den);
+void rg_mux_destroy(rg_mux* mux);
+/* Adds one access unit in decoding order. The first must be an IDR picture carrying SPS and PPS;
+ * parameter sets that change later are RG_ERR_UNSUPPORTED. */
+int rg_mux_write(rg_mux* mux, const uint8_t* access_unit, size_t size);
+/* The whole file: returns its size; with out non-NULL also writes it (cap must hold it).
+ * May be called more than once (a size query first). */
+int64_t rg_mux_finish(rg_mux* mux, uint8_t* out, size_t cap);
+
+/*
+ * Demuxers of the same two containers (mp4.rs:186 Mp4Demuxer, mkv.rs MkvDemuxer), for the first
+ * H.264 video track, back to Annex-B access units (SPS and PPS in front of every IDR picture,
+ * as the writer emits them). The data is copied at open. Laced Matroska blocks and files
+ * without an H.264 track are RG_ERR_UNSUPPORTED.
+ */
+typedef struct rg_stream_info {
+  int32_t container;      /* RG_CONTAINER_* */
+  int32_t width, height;  /* from the sample entry / track entry */
+  int32_t fps_num, fps_den;
+  int32_t profile_idc;    /* from the SPS */
+  int64_t access_units;
+  int64_t keyframes;      /* access units holding an IDR slice */
+} rg_stream_info;
+
+typedef struct rg_demux rg_demux;
+rg_demux* rg_demux_open(const uint8_t* data, size_t size);
+void rg_demux_destroy(rg_demux* demux);
+int rg_demux_info(const rg_demux* demux, rg_stream_info* info);
+/* Access unit `index` as Annex-B: returns its size; with out non-NULL also writes it. */
+int64_t rg_demux_access_unit(const rg_demux* demux, int64_t index, uint8_t* out, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

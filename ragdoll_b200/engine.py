@@ -40,6 +40,8 @@ EXPORTS = [
     "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc", "rg_analyse_gops",
     "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_analyse_gops_async",
     "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture", "rg_pipeline_work_list",
+    "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
+    "rg_demux_info", "rg_demux_access_unit",
 ]
 
 
@@ -59,6 +61,12 @@ class RgConfig(ctypes.Structure):
 
 class RgPipelineTuning(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in ("lag", "seg", "grid", "timeout_ms", "deblock_sms", "intra_sms")]
+
+
+class RgStreamInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("container", "width", "height", "fps_num", "fps_den", "profile_idc")] + \
+               [("access_units", ctypes.c_int64), ("keyframes", ctypes.c_int64)]
 
 
 class RgQuality(ctypes.Structure):
@@ -119,6 +127,18 @@ def lib() -> ctypes.CDLL:
     L.rg_set_pipeline_tuning.argtypes = [P, ctypes.POINTER(RgPipelineTuning)]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
+    L.rg_mux_create.restype = P
+    L.rg_mux_create.argtypes = [ctypes.c_int32] * 5
+    L.rg_mux_destroy.argtypes = [P]
+    L.rg_mux_write.argtypes = [P, P, ctypes.c_size_t]
+    L.rg_mux_finish.restype = ctypes.c_int64
+    L.rg_mux_finish.argtypes = [P, P, ctypes.c_size_t]
+    L.rg_demux_open.restype = P
+    L.rg_demux_open.argtypes = [P, ctypes.c_size_t]
+    L.rg_demux_destroy.argtypes = [P]
+    L.rg_demux_info.argtypes = [P, ctypes.POINTER(RgStreamInfo)]
+    L.rg_demux_access_unit.restype = ctypes.c_int64
+    L.rg_demux_access_unit.argtypes = [P, ctypes.c_int64, P, ctypes.c_size_t]
     _lib = L
     return L
 
