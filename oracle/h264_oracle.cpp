@@ -1,7 +1,7 @@
 // TEST INFRASTRUCTURE ONLY -- not part of the product path.
 //
 // CPU oracle: a scalar C++ restatement of ragdoll's Balanced H.264 encoder (analysis,
-// reconstruction, deblocking, CAVLC slice writer, SPS/PPS/slice headers, NAL packing). The GPU
+// reconstruction, deblocking, CAVLC and CABAC slice writers, SPS/PPS/slice headers, NAL packing). The GPU
 // engine's decisions, levels and reconstructions are checked against it, and it is itself pinned
 // byte for byte to the reference's committed encoder output (qa/corpus/synth/clip_160x90_30fps.mp4)
 // by tests/test_oracle_golden.py. Only tests/, __graft_entry__.smoke() and bench.py's CPU
@@ -646,6 +646,219 @@ static void append_nal(std::vector<uint8_t>& dst, int ref_idc, int type, const s
     zeros = b == 0 ? zeros + 1 : 0;
   }
 }
+
+// ---------------------------------------------------------------------------------------------
+// CABAC (crates/ragdoll-codec/src/cabac.rs): the x264-style M-coder and the binarisations of the
+// syntax elements the Balanced encoder writes.
+struct CabacEnc {
+  uint32_t low = 0, range = 510;
+  int queue = -9;
+  uint32_t outstanding = 0;
+  std::vector<uint8_t> out;
+  uint8_t ctx[460];  // 2 * pStateIdx + valMPS (cabac.rs:324)
+
+  // cabac.rs:427 init_cabac_contexts, :354 CabacContext::from_mn_qp
+  void init(int slice_qp, bool islice, int idc) {
+    int t = islice ? 0 : 1 + std::min(idc, 2);
+    for (int i = 0; i < 460; i++) {
+      int m = kCabacInitMN[(t * 460 + i) * 2], n = kCabacInitMN[(t * 460 + i) * 2 + 1];
+      int pre = std::max(1, std::min(126, ((m * std::min(slice_qp, 51)) >> 4) + n));
+      ctx[i] = pre <= 63 ? (uint8_t)((63 - pre) << 1) : (uint8_t)(((pre - 64) << 1) | 1);
+    }
+  }
+  // cabac.rs:524 putbyte
+  void putbyte() {
+    if (queue < 0) return;
+    uint32_t o = low >> (queue + 10);
+    low &= (0x400u << queue) - 1;
+    queue -= 8;
+    if ((o & 0xFF) == 0xFF) {
+      outstanding++;
+    } else {
+      uint32_t carry = o >> 8;
+      if (!out.empty()) out.back() = (uint8_t)(out.back() + carry);
+      uint8_t fill = carry ? 0x00 : 0xFF;
+      for (; outstanding; outstanding--) out.push_back(fill);
+      out.push_back((uint8_t)(o & 0xFF));
+    }
+  }
+  // cabac.rs:549 renormalize
+  void renorm() {
+    int shift = __builtin_clz(range) - 23;
+    range <<= shift;
+    low <<= shift;
+    queue += shift;
+    if (queue >= 0) putbyte();
+  }
+  // cabac.rs:562 encode_decision (9.3.3.2.1)
+  void decision(int ci, int bin) {
+    int st = ctx[ci] >> 1, mps = ctx[ci] & 1;
+    uint32_t rl = kCabacRangeLps[st * 4 + ((range >> 6) & 3)];
+    range -= rl;
+    if (bin != mps) {
+      low += range;
+      range = rl;
+      if (st == 0) mps ^= 1;
+      st = kCabacTransLps[st];
+    } else {
+      st = std::min(st + 1, 62);
+    }
+    ctx[ci] = (uint8_t)((st << 1) | mps);
+    renorm();
+  }
+  // cabac.rs:578 encode_bypass
+  void bypass(int bin) {
+    low <<= 1;
+    if (bin) low += range;
+    queue++;
+    if (queue >= 0) putbyte();
+  }
+  // cabac.rs:591 encode_terminate
+  void terminate(int bin) {
+    range -= 2;
+    if (bin) {
+      low += range;
+      low = (low << 9) | 0x200;
+      queue += 9;
+      putbyte();
+      putbyte();
+      low <<= -queue;
+      queue = 0;
+      putbyte();
+      for (; outstanding; outstanding--) out.push_back(0xFF);
+    } else {
+      renorm();
+    }
+  }
+  // cabac.rs:738 encode_intra_mb_type (ctx_base 3: I slice, 17: suffix in a P slice)
+  void intra_mb_type(int ctx_base, int ca, int cb, int t) {
+    bool islice = ctx_base == 3;
+    int c0 = islice ? 3 + ca + cb : ctx_base;
+    if (t == 0) { decision(c0, 0); return; }
+    decision(c0, 1);
+    terminate(0);  // never I_PCM here (QP >= 1)
+    int code = t - 1, luma_mode = code % 4, cbpc = (code / 4) % 3, cbpl = code >= 12;
+    if (islice) {
+      decision(6, cbpl);
+      decision(7, cbpc > 0);
+      if (cbpc > 0) decision(8, cbpc == 2);
+      decision(9, (luma_mode >> 1) & 1);
+      decision(10, luma_mode & 1);
+    } else {
+      decision(ctx_base + 1, cbpl);
+      decision(ctx_base + 2, cbpc > 0);
+      if (cbpc > 0) decision(ctx_base + 2, cbpc == 2);
+      decision(ctx_base + 3, (luma_mode >> 1) & 1);
+      decision(ctx_base + 3, luma_mode & 1);
+    }
+  }
+  // cabac.rs:787 encode_p_mb_type (0 = P_L0_16x16, >= 5 intra)
+  void p_mb_type(int t) {
+    if (t >= 5) { decision(14, 1); intra_mb_type(17, 0, 0, t - 5); return; }
+    decision(14, 0);
+    decision(15, 0);
+    decision(16, 0);
+  }
+  // cabac.rs:819 encode_intra4x4_pred_mode
+  void i4_mode(bool prev, int rem) {
+    if (prev) { decision(68, 1); return; }
+    decision(68, 0);
+    decision(69, rem & 1);
+    decision(69, (rem >> 1) & 1);
+    decision(69, (rem >> 2) & 1);
+  }
+  // cabac.rs:836 encode_chroma_pred_mode
+  void chroma_mode(int ca, int cb, int mode) {
+    int c0 = 64 + ca + cb;
+    if (mode == 0) { decision(c0, 0); return; }
+    decision(c0, 1);
+    if (mode == 1) { decision(67, 0); return; }
+    decision(67, 1);
+    decision(67, mode >= 3);
+  }
+  // cabac.rs:891 encode_mb_qp_delta
+  void qp_delta(int prev_nz, int d) {
+    int c0 = 60 + (prev_nz != 0);
+    if (d == 0) { decision(c0, 0); return; }
+    unsigned code = d > 0 ? 2 * d - 1 : -2 * d;
+    decision(c0, 1);
+    if (code == 1) { decision(62, 0); return; }
+    decision(62, 1);
+    for (unsigned k = 2; k < code; k++) decision(63, 1);
+    decision(63, 0);
+  }
+  // cabac.rs:940 encode_mvd
+  void mvd(int comp, uint32_t abs_sum, int v) {
+    int base = comp == 0 ? 40 : 47;
+    int inc0 = abs_sum < 3 ? 0 : (abs_sum <= 32 ? 1 : 2);
+    uint32_t a = (uint32_t)std::abs(v);
+    if (a == 0) { decision(base + inc0, 0); return; }
+    decision(base + inc0, 1);
+    uint32_t prefix = std::min(a, 9u);
+    for (uint32_t i = 1; i < prefix; i++) decision(base + 3 + std::min((int)i - 1, 3), 1);
+    if (a < 9) {
+      decision(base + 3 + std::min((int)a - 1, 3), 0);
+    } else {
+      uint32_t rem = a - 9;
+      int k = 3;
+      while (rem >= (1u << k)) { bypass(1); rem -= 1u << k; k++; }
+      bypass(0);
+      for (int b = k - 1; b >= 0; b--) bypass((rem >> b) & 1);
+    }
+    bypass(v < 0);
+  }
+  // cabac.rs:981 encode_residual_block_cat, :1030 encode_sig_and_levels, :1059 sig_map, :1090 levels
+  void residual(int cat, int cbf_inc, const int16_t* c, int n) {
+    static const int kCbf[5] = {85, 89, 93, 97, 101};
+    static const int kSig[6] = {105, 120, 134, 149, 152, 402};
+    static const int kLast[6] = {166, 181, 195, 210, 213, 417};
+    static const int kLvl[6] = {227, 237, 247, 257, 266, 426};
+    int last = -1;
+    for (int i = n - 1; i >= 0; i--) if (c[i]) { last = i; break; }
+    if (cat < 5) {
+      if (last < 0) { decision(kCbf[cat] + cbf_inc, 0); return; }
+      decision(kCbf[cat] + cbf_inc, 1);
+    } else if (last < 0) {
+      last = 0;
+    }
+    int flagged = std::min(last, n - 2);
+    for (int i = 0; i <= flagged; i++) {
+      int so = cat == 5 ? kCabacSigOff8x8[i] : i, lo = cat == 5 ? kCabacLastOff8x8[i] : i;
+      if (c[i] == 0) {
+        decision(kSig[cat] + so, 0);
+      } else {
+        decision(kSig[cat] + so, 1);
+        decision(kLast[cat] + lo, i == last);
+      }
+    }
+    int gt_max = cat == 3 ? 3 : 4, eq1 = 0, gt1 = 0, lv = kLvl[cat];
+    for (int i = last; i >= 0; i--) {
+      if (c[i] == 0) continue;
+      uint32_t m1 = (uint32_t)std::abs(c[i]) - 1;
+      int c0 = gt1 > 0 ? 0 : std::min(1 + eq1, 4);
+      if (m1 == 0) {
+        decision(lv + c0, 0);
+        eq1++;
+      } else {
+        decision(lv + c0, 1);
+        int c1 = 5 + std::min(gt1, gt_max);
+        uint32_t prefix = std::min(m1, 14u);
+        for (uint32_t k = 1; k < prefix; k++) decision(lv + c1, 1);
+        if (m1 < 14) {
+          decision(lv + c1, 0);
+        } else {
+          uint32_t rem = m1 - 14;
+          int k = 0;
+          while (rem >= (1u << k)) { bypass(1); rem -= 1u << k; k++; }
+          bypass(0);
+          for (int b = k - 1; b >= 0; b--) bypass((rem >> b) & 1);
+        }
+        gt1++;
+      }
+      bypass(c[i] < 0);
+    }
+  }
+};
 
 // h264.rs:2215 encode_cavlc_block
 static void cavlc_block(BitWriter& w, const int16_t* sc, int max_coeff, int nc, bool chroma_dc) {
@@ -1316,6 +1529,199 @@ struct Encoder {
     }
   }
 
+  // ---- CABAC macroblock layer (enc.rs:2779 begin_coded_mb, :2877 code_skip, :3196 code_inter,
+  // :3442 code_i4, :3587 code_i16; h264.rs:3293-3553 the coded_block_pattern / residual glue).
+  // Neighbour state as EncState keeps it for the CABAC writer (enc.rs:218-276).
+  CabacEnc ce;
+  std::vector<uint8_t> cb_nnz, cb_cnnz[2], cb_intra, cb_i16, cb_skip, cb_cbpl, cb_cbpc, cb_cmode, cb_ldc, cb_cdc[2], cb_t8;
+  std::vector<int16_t> cb_mvd;
+  bool prev_qp_delta_nz = false;
+
+  void cabac_prepare() {
+    int n = mb_w * mb_h, n4 = n * 16;
+    cb_nnz.assign(n4, 0);
+    cb_cnnz[0].assign(n * 4, 0); cb_cnnz[1].assign(n * 4, 0);
+    for (auto* v : {&cb_intra, &cb_i16, &cb_skip, &cb_cbpl, &cb_cbpc, &cb_cmode, &cb_ldc, &cb_cdc[0], &cb_cdc[1], &cb_t8})
+      v->assign(n, 0);
+    cb_mvd.assign(n4 * 2, 0);
+    prev_qp_delta_nz = false;
+    ce = CabacEnc();
+    ce.init(qp, is_idr, 0);
+  }
+  // h264.rs:2139 cabac_cbf_ctx_inc (-1: neighbour unavailable)
+  static int cbf_inc(int l, int t, bool intra) {
+    int a = l < 0 ? intra : l, b = t < 0 ? intra : t;
+    return a + 2 * b;
+  }
+  // h264.rs:3293 luma_neighbor_cbf
+  int luma_nb(int gx, int gy, bool left) const {
+    if (left ? gx == 0 : gy == 0) return -1;
+    int ngx = left ? gx - 1 : gx, ngy = left ? gy : gy - 1;
+    int nm = (ngy / 4) * mb_w + ngx / 4;
+    if (cb_skip[nm]) return 0;
+    if (!cb_i16[nm]) {
+      int n8 = (ngy & 2) + ((ngx & 2) >> 1);
+      if (!((cb_cbpl[nm] >> n8) & 1) && !cb_intra[nm]) return 0;
+    }
+    return cb_nnz[ngy * gstride() + ngx] > 0;
+  }
+  // h264.rs:3492 encode_cabac_chroma_residuals
+  void cabac_chroma(int mbx, int mby, bool intra, int cbpc, const rg_mb_out& r) {
+    int m = mby * mb_w + mbx, cg = mb_w * 2;
+    if (cbpc >= 1)
+      for (int p = 0; p < 2; p++) {
+        int l = mbx > 0 ? (!cb_skip[m - 1] && cb_cdc[p][m - 1]) : -1;
+        int t = mby > 0 ? (!cb_skip[m - mb_w] && cb_cdc[p][m - mb_w]) : -1;
+        ce.residual(3, cbf_inc(l, t, intra), r.chroma_dc[p], 4);
+        cb_cdc[p][m] = r.chroma_dc[p][0] || r.chroma_dc[p][1] || r.chroma_dc[p][2] || r.chroma_dc[p][3];
+      }
+    if (cbpc >= 2)
+      for (int p = 0; p < 2; p++)
+        for (int b = 0; b < 4; b++) {
+          int cx = mbx * 2 + (b & 1), cy = mby * 2 + (b >> 1);
+          int l = cx > 0 ? cb_cnnz[p][cy * cg + cx - 1] > 0 : -1;
+          int t = cy > 0 ? cb_cnnz[p][(cy - 1) * cg + cx] > 0 : -1;
+          const int16_t* ac = r.chroma_ac[p][b] + 1;
+          ce.residual(4, cbf_inc(l, t, intra), ac, 15);
+          int cnt = 0;
+          for (int i = 0; i < 15; i++) cnt += ac[i] != 0;
+          cb_cnnz[p][cy * cg + cx] = (uint8_t)cnt;
+        }
+  }
+  // h264.rs:3327 encode_cabac_cbp_and_residuals
+  void cabac_cbp_residuals(int mbx, int mby, bool intra, bool write8, const rg_mb_out& r) {
+    int m = mby * mb_w + mbx, g = gstride();
+    int cbpl = r.cbp & 15, cbpc = r.cbp >> 4;
+    for (int i8 = 0; i8 < 4; i8++) {
+      int bx8 = i8 & 1, by8 = i8 >> 1;
+      bool lnz = bx8 ? (cbpl >> (i8 - 1)) & 1 : (mbx > 0 ? !cb_skip[m - 1] && ((cb_cbpl[m - 1] >> (by8 * 2 + 1)) & 1) : true);
+      bool tnz = by8 ? (cbpl >> (i8 - 2)) & 1 : (mby > 0 ? !cb_skip[m - mb_w] && ((cb_cbpl[m - mb_w] >> (2 + bx8)) & 1) : true);
+      ce.decision(73 + !lnz + 2 * !tnz, (cbpl >> i8) & 1);
+    }
+    int lc = mbx > 0 && !cb_skip[m - 1] ? cb_cbpc[m - 1] : 0;
+    int tc = mby > 0 && !cb_skip[m - mb_w] ? cb_cbpc[m - mb_w] : 0;
+    int c0 = 77 + (lc != 0) + 2 * (tc != 0);
+    if (cbpc == 0) {
+      ce.decision(c0, 0);
+    } else {
+      ce.decision(c0, 1);
+      ce.decision(81 + (lc == 2) + 2 * (tc == 2), cbpc == 2);
+    }
+    cb_cbpl[m] = (uint8_t)cbpl;
+    cb_cbpc[m] = (uint8_t)cbpc;
+    if (cbpl == 0 && cbpc == 0) { prev_qp_delta_nz = false; return; }
+    if (write8 && cbpl && !intra) {
+      int l8 = mbx > 0 && cb_t8[m - 1], t8 = mby > 0 && cb_t8[m - mb_w];
+      ce.decision(399 + l8 + t8, r.transform_8x8 != 0);
+    }
+    ce.qp_delta(prev_qp_delta_nz, r.qp_delta);
+    prev_qp_delta_nz = r.qp_delta != 0;
+    if (r.transform_8x8) {
+      for (int i8 = 0; i8 < 4; i8++) {
+        int gx = mbx * 4 + (i8 & 1) * 2, gy = mby * 4 + (i8 >> 1) * 2;
+        bool coded = (cbpl >> i8) & 1;
+        if (coded) ce.residual(5, 0, r.luma + i8 * 64, 64);
+        for (int y = 0; y < 2; y++)
+          for (int x = 0; x < 2; x++) cb_nnz[(gy + y) * g + gx + x] = coded;
+      }
+    } else {
+      for (int b = 0; b < 16; b++) {
+        int bx, by; blk_xy(b, bx, by);
+        int gx = mbx * 4 + bx, gy = mby * 4 + by;
+        if ((cbpl >> (b >> 2)) & 1) {
+          const int16_t* c = r.luma + b * 16;
+          ce.residual(2, cbf_inc(luma_nb(gx, gy, true), luma_nb(gx, gy, false), intra), c, 16);
+          int cnt = 0;
+          for (int i = 0; i < 16; i++) cnt += c[i] != 0;
+          cb_nnz[gy * g + gx] = (uint8_t)cnt;
+        } else {
+          cb_nnz[gy * g + gx] = 0;
+        }
+      }
+    }
+    cabac_chroma(mbx, mby, intra, cbpc, r);
+  }
+  void write_mb_cabac(int mbx, int mby, const rg_mb_out& r) {
+    int m = mby * mb_w + mbx, g = gstride();
+    int sl = mbx > 0 && !cb_skip[m - 1], st = mby > 0 && !cb_skip[m - mb_w];
+    if (r.mb_type == RG_MB_P_SKIP) {
+      ce.decision(11 + sl + st, 1);
+      cb_skip[m] = 1;
+      prev_qp_delta_nz = false;
+      return;
+    }
+    if (!is_idr) ce.decision(11 + sl + st, 0);
+    int li = mbx > 0 && cb_i16[m - 1], ti = mby > 0 && cb_i16[m - mb_w];
+    if (r.mb_type == RG_MB_P_L0_16X16) {
+      if (r.transform_8x8) cb_t8[m] = 1;
+      ce.p_mb_type(0);
+      uint32_t ax = 0, ay = 0;
+      int gx0 = mbx * 4, gy0 = mby * 4;
+      if (gx0 > 0) { int i = gy0 * g + gx0 - 1; ax += std::abs(cb_mvd[2 * i]); ay += std::abs(cb_mvd[2 * i + 1]); }
+      if (gy0 > 0) { int i = (gy0 - 1) * g + gx0; ax += std::abs(cb_mvd[2 * i]); ay += std::abs(cb_mvd[2 * i + 1]); }
+      ce.mvd(0, ax, r.mvd[0]);
+      ce.mvd(1, ay, r.mvd[1]);
+      cabac_cbp_residuals(mbx, mby, false, t8x8, r);
+      for (int y = 0; y < 4; y++)
+        for (int x = 0; x < 4; x++) {
+          int i = (gy0 + y) * g + gx0 + x;
+          cb_mvd[2 * i] = r.mvd[0];
+          cb_mvd[2 * i + 1] = r.mvd[1];
+        }
+      return;
+    }
+    cb_intra[m] = 1;
+    cb_cmode[m] = r.chroma_mode;
+    int lcm = mbx > 0 && cb_intra[m - 1] && cb_cmode[m - 1] != 0;
+    int tcm = mby > 0 && cb_intra[m - mb_w] && cb_cmode[m - mb_w] != 0;
+    if (r.mb_type == RG_MB_I4X4) {
+      for (int b = 0; b < 16; b++) {
+        int bx, by; blk_xy(b, bx, by);
+        intra4x4_modes[(mby * 4 + by) * g + mbx * 4 + bx] = 2;
+      }
+      if (!is_idr) ce.p_mb_type(5);
+      else ce.intra_mb_type(3, li, ti, 0);
+      if (t8x8) ce.decision(399 + (mbx > 0 && cb_t8[m - 1]) + (mby > 0 && cb_t8[m - mb_w]), 0);
+      for (int b = 0; b < 16; b++) {
+        int bx, by; blk_xy(b, bx, by);
+        int gx = mbx * 4 + bx, gy = mby * 4 + by;
+        int pm = pred_i4_mode(gx, gy), md = r.i4_modes[b];
+        ce.i4_mode(md == pm, md < pm ? md : std::max(md - 1, 0));
+        intra4x4_modes[gy * g + gx] = (uint8_t)md;
+      }
+      ce.chroma_mode(lcm, tcm, r.chroma_mode);
+      cabac_cbp_residuals(mbx, mby, true, false, r);
+      return;
+    }
+    // I_16x16
+    int cbpl = r.cbp & 15, cbpc = r.cbp >> 4;
+    cb_i16[m] = 1;
+    cb_cbpl[m] = (uint8_t)cbpl;
+    cb_cbpc[m] = (uint8_t)cbpc;
+    int mbt = 1 + r.i16_mode + 4 * cbpc + (cbpl ? 12 : 0);
+    if (!is_idr) ce.p_mb_type(5 + mbt);
+    else ce.intra_mb_type(3, li, ti, mbt);
+    ce.chroma_mode(lcm, tcm, r.chroma_mode);
+    ce.qp_delta(prev_qp_delta_nz, r.qp_delta);
+    prev_qp_delta_nz = r.qp_delta != 0;
+    int ldc = mbx > 0 ? cb_ldc[m - 1] : -1, tdc = mby > 0 ? cb_ldc[m - mb_w] : -1;
+    ce.residual(0, cbf_inc(ldc, tdc, true), r.luma_dc, 16);
+    bool any = false;
+    for (int i = 0; i < 16; i++) any |= r.luma_dc[i] != 0;
+    cb_ldc[m] = any;
+    if (cbpl)
+      for (int b = 0; b < 16; b++) {
+        int bx, by; blk_xy(b, bx, by);
+        int gx = mbx * 4 + bx, gy = mby * 4 + by;
+        const int16_t* ac = r.luma + b * 16 + 1;
+        ce.residual(1, cbf_inc(luma_nb(gx, gy, true), luma_nb(gx, gy, false), true), ac, 15);
+        int cnt = 0;
+        for (int i = 0; i < 15; i++) cnt += ac[i] != 0;
+        cb_nnz[gy * g + gx] = (uint8_t)cnt;
+      }
+    cabac_chroma(mbx, mby, true, cbpc, r);
+  }
+
   // ---- macroblock coding ----
   void store_mb(int mbx, int mby, const uint8_t* y, const uint8_t* u, const uint8_t* v) {
     for (int r = 0; r < 16; r++) memcpy(cur.y.ptr(mbx * 16, mby * 16 + r), y + r * 16, 16);
@@ -1816,6 +2222,10 @@ struct Encoder {
     w.se(0);
     w.ue(qp == 0 ? 1 : 0);
     if (qp != 0) { w.se(0); w.se(0); }
+    if (cabac) {  // enc.rs:2347: cabac_alignment_one_bits, contexts for this slice
+      if (w.bits() & 7) w.put((1u << (8 - (w.bits() & 7))) - 1, 8 - (int)(w.bits() & 7));
+      cabac_prepare();
+    }
 
     for (int mby = 0; mby < mb_h; mby++)
       for (int mbx = 0; mbx < mb_w; mbx++) {
@@ -1825,11 +2235,22 @@ struct Encoder {
         r.qp = (uint8_t)qp;
         if (is_idr) code_intra(mbx, mby, src, r);
         else code_p_mb(mbx, mby, src, r);
-        if (!cabac) write_mb_cavlc(w, mbx, mby, r);
+        if (!cabac) {
+          write_mb_cavlc(w, mbx, mby, r);
+        } else {
+          write_mb_cabac(mbx, mby, r);
+          ce.terminate(mby == mb_h - 1 && mbx == mb_w - 1);  // end_of_slice_flag (enc.rs:2430)
+        }
       }
-    if (!is_idr && skip_run > 0) w.ue(skip_run);
-    w.trailing();
-    std::vector<uint8_t> rbsp = w.finish();
+    std::vector<uint8_t> rbsp;
+    if (cabac) {
+      rbsp = w.finish();
+      rbsp.insert(rbsp.end(), ce.out.begin(), ce.out.end());
+    } else {
+      if (!is_idr && skip_run > 0) w.ue(skip_run);
+      w.trailing();
+      rbsp = w.finish();
+    }
 
     for (int p = 0; p < 3; p++) {
       const Plane& pl = p == 0 ? cur.y : (p == 1 ? cur.u : cur.v);
@@ -1849,7 +2270,6 @@ struct Encoder {
       }
     frame_count++;
     std::vector<uint8_t> out;
-    if (cabac) return out;
     if (is_idr) {
       append_nal(out, 3, 7, sps_rbsp());
       append_nal(out, 3, 8, pps_rbsp());

@@ -1,9 +1,11 @@
-// Host-side CAVLC writer: turns the per-macroblock records of the engine into the Annex-B access
-// units of ragdoll's Balanced encoder in the Baseline profile (the serial half of
-// encode_frame_body, crates/ragdoll-codec/src/h264/enc.rs:2234: the slice header, skip runs and
-// macroblock layer of enc.rs:989-1054 / 3260-3285 / 3540-3577 / 3736-3750, the residual blocks of
-// h264.rs:2215 encode_cavlc_block, SPS / PPS of h264.rs:556-660 and 806-832, and the NAL packing
-// with emulation prevention of h264.rs:189). One writer per stream (GOP); no CUDA.
+// Host-side bitstream writer: turns the per-macroblock records of the engine into the Annex-B
+// access units of ragdoll's Balanced encoder (the serial half of encode_frame_body,
+// crates/ragdoll-codec/src/h264/enc.rs:2234): SPS / PPS of h264.rs:556-660 and 806-832 for the
+// Baseline, Main and High profiles, the slice header, and the NAL packing with emulation
+// prevention of h264.rs:189. Baseline slices are CAVLC, written here (skip runs and macroblock
+// layer of enc.rs:989-1054 / 3260-3285 / 3540-3577 / 3736-3750, residual blocks of h264.rs:2215
+// encode_cavlc_block); Main and High slices are CABAC, written by cabac_writer.cpp after the
+// cabac_alignment_one_bits. One writer per stream (GOP); no CUDA.
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -15,6 +17,8 @@
 
 namespace rg {
 void set_last_error(const char* msg);
+int cabac_slice_data(int mb_w, int mb_h, int qp, bool idr, bool transform_8x8, const rg_mb_out* recs,
+                     std::vector<uint8_t>& out);
 }
 
 namespace {
@@ -57,6 +61,11 @@ class Rbsp {
     }
   }
   void se(int32_t v) { ue(v > 0 ? 2u * (uint32_t)v - 1u : 2u * (uint32_t)(-(int64_t)v)); }
+  // cabac_alignment_one_bit up to the byte boundary; the bytes so far.
+  std::vector<uint8_t>& align_ones() {
+    while (fill_) put(1, 1);
+    return bytes_;
+  }
   // rbsp_trailing_bits: a stop bit, then zeros to the byte boundary.
   const std::vector<uint8_t>& close() {
     put(1, 1);
@@ -157,6 +166,7 @@ inline int by4(int b) { return ((b >> 1) & 1) | ((b >> 2) & 2); }
 
 struct rg_writer {
   int width = 0, height = 0, qp = 26, fps_num = 30, fps_den = 1;
+  int profile = RG_PROFILE_BASELINE;  // Main / High: CABAC; High: 8x8 transform
   int mb_w = 0, mb_h = 0;
   uint32_t since_idr = 0;  // pictures since the last IDR (frame_num, POC)
   uint32_t idrs = 0;       // IDR pictures written (idr_pic_id)
@@ -166,10 +176,20 @@ struct rg_writer {
 
   std::vector<uint8_t> sps() const {
     Rbsp w;
-    w.put(66, 8);    // profile_idc: Baseline
-    w.put(0xC0, 8);  // constraint_set0/1 (Constrained Baseline)
+    // profile_idc and constraint flags (h264.rs:247): Constrained Baseline 66 / set0+set1,
+    // Main 77 / set1, High 100
+    const int idc = profile == RG_PROFILE_BASELINE ? 66 : (profile == RG_PROFILE_MAIN ? 77 : 100);
+    w.put(idc, 8);
+    w.put(profile == RG_PROFILE_BASELINE ? 0xC0 : (profile == RG_PROFILE_MAIN ? 0x40 : 0x00), 8);
     w.put(40, 8);    // level_idc 4.0
     w.ue(0);         // seq_parameter_set_id
+    if (idc == 100) {
+      w.ue(1);       // chroma_format_idc 4:2:0
+      w.ue(0);       // bit_depth_luma_minus8
+      w.ue(0);       // bit_depth_chroma_minus8
+      w.flag(false); // qpprime_y_zero_transform_bypass_flag
+      w.flag(false); // seq_scaling_matrix_present_flag
+    }
     w.ue(0);         // log2_max_frame_num_minus4
     w.ue(0);         // pic_order_cnt_type
     w.ue(2);         // log2_max_pic_order_cnt_lsb_minus4
@@ -213,7 +233,7 @@ struct rg_writer {
     Rbsp w;
     w.ue(0);         // pic_parameter_set_id
     w.ue(0);         // seq_parameter_set_id
-    w.flag(false);   // entropy_coding_mode_flag: CAVLC
+    w.flag(profile != RG_PROFILE_BASELINE);  // entropy_coding_mode_flag: CABAC beyond Baseline
     w.flag(false);   // bottom_field_pic_order_in_frame_present_flag
     w.ue(0);         // num_slice_groups_minus1
     w.ue(0);         // num_ref_idx_l0_default_active_minus1
@@ -226,6 +246,11 @@ struct rg_writer {
     w.flag(true);    // deblocking_filter_control_present_flag
     w.flag(false);   // constrained_intra_pred_flag
     w.flag(false);   // redundant_pic_cnt_present_flag
+    if (profile == RG_PROFILE_HIGH) {
+      w.flag(true);  // transform_8x8_mode_flag
+      w.flag(false); // pic_scaling_matrix_present_flag
+      w.se(0);       // second_chroma_qp_index_offset
+    }
     return w.close();
   }
 
@@ -336,8 +361,8 @@ rg_writer* rg_writer_create(const rg_config* cfg, int32_t fps_num, int32_t fps_d
     wfail(RG_ERR_INVALID, "rg_writer_create: null config");
     return nullptr;
   }
-  if (cfg->profile != RG_PROFILE_BASELINE) {
-    wfail(RG_ERR_UNSUPPORTED, "rg_writer_create: profile %d uses CABAC; this writer is CAVLC (Baseline)", cfg->profile);
+  if (cfg->profile != RG_PROFILE_BASELINE && cfg->profile != RG_PROFILE_MAIN && cfg->profile != RG_PROFILE_HIGH) {
+    wfail(RG_ERR_INVALID, "rg_writer_create: profile %d", cfg->profile);
     return nullptr;
   }
   if (cfg->width < 1 || cfg->height < 1 || cfg->width > 8192 || cfg->height > 8192 || cfg->qp < 1 || cfg->qp > 51 ||
@@ -350,6 +375,7 @@ rg_writer* rg_writer_create(const rg_config* cfg, int32_t fps_num, int32_t fps_d
   w->width = cfg->width;
   w->height = cfg->height;
   w->qp = cfg->qp;
+  w->profile = cfg->profile;
   w->fps_num = fps_num;
   w->fps_den = fps_den;
   w->mb_w = (cfg->width + 15) / 16;
@@ -396,23 +422,34 @@ int64_t rg_writer_picture(rg_writer* w, const rg_mb_out* records, int32_t kind, 
   } else {
     s.flag(false);                  // adaptive_ref_pic_marking_mode_flag
   }
+  const bool cabac = w->profile != RG_PROFILE_BASELINE;
+  if (cabac && !idr) s.ue(0);       // cabac_init_idc
   s.se(0);                          // slice_qp_delta
   s.ue(0);                          // disable_deblocking_filter_idc (QP >= 1)
   s.se(0);                          // slice_alpha_c0_offset_div2
   s.se(0);                          // slice_beta_offset_div2
-  uint32_t skip_run = 0;
-  for (int mby = 0; mby < w->mb_h; mby++)
-    for (int mbx = 0; mbx < w->mb_w; mbx++) {
-      int r = w->mb_layer(s, mbx, mby, records[mby * w->mb_w + mbx], idr, skip_run);
-      if (r) return r;
-    }
-  if (!idr && skip_run) s.ue(skip_run);
+  const std::vector<uint8_t>* rbsp;
+  if (cabac) {
+    std::vector<uint8_t>& bytes = s.align_ones();
+    if (rg::cabac_slice_data(w->mb_w, w->mb_h, w->qp, idr, w->profile == RG_PROFILE_HIGH, records, bytes))
+      return wfail(RG_ERR_INVALID, "rg_writer_picture: a record no %s slice holds", idr ? "IDR" : "P");
+    rbsp = &bytes;
+  } else {
+    uint32_t skip_run = 0;
+    for (int mby = 0; mby < w->mb_h; mby++)
+      for (int mbx = 0; mbx < w->mb_w; mbx++) {
+        int r = w->mb_layer(s, mbx, mby, records[mby * w->mb_w + mbx], idr, skip_run);
+        if (r) return r;
+      }
+    if (!idr && skip_run) s.ue(skip_run);
+    rbsp = &s.close();
+  }
   std::vector<uint8_t> au;
   if (idr) {
     emit_nal(au, 3, 7, w->sps());
     emit_nal(au, 3, 8, w->pps());
   }
-  emit_nal(au, 3, idr ? 5 : 1, s.close());
+  emit_nal(au, 3, idr ? 5 : 1, *rbsp);
   if (au.size() > cap)
     return wfail(RG_ERR_INVALID, "rg_writer_picture: access unit of %zu bytes exceeds the %zu-byte buffer", au.size(), cap);
   memcpy(out, au.data(), au.size());

@@ -334,11 +334,12 @@ def ssim_plane_device_noalloc(dev_a: int, stride_a: int, dev_b: int, stride_b: i
                                                stream or None))
 
 
-class CavlcWriter:
-    """Annex-B writer of one Baseline stream from engine records (rg_writer_*; host code)."""
+class BitstreamWriter:
+    """Annex-B writer of one stream from engine records (rg_writer_*; host code): CAVLC slices
+    for Baseline, CABAC slices for Main and High."""
 
-    def __init__(self, width: int, height: int, qp: int, fps=(30, 1)):
-        cfg = RgConfig(width, height, RG_PROFILE_BASELINE, qp, 1, 0, 1)
+    def __init__(self, width: int, height: int, qp: int, fps=(30, 1), profile: int = RG_PROFILE_BASELINE):
+        cfg = RgConfig(width, height, profile, qp, 1, 0, 1)
         self.h = lib().rg_writer_create(ctypes.byref(cfg), fps[0], fps[1])
         if not self.h:
             raise RgError(-1, lib().rg_last_error().decode())
@@ -358,3 +359,10 @@ class CavlcWriter:
 
     def __del__(self):
         self.close()
+
+
+class CavlcWriter(BitstreamWriter):
+    """The Baseline (CAVLC) writer."""
+
+    def __init__(self, width: int, height: int, qp: int, fps=(30, 1)):
+        super().__init__(width, height, qp, fps, RG_PROFILE_BASELINE)

@@ -1,10 +1,15 @@
-"""The library's CAVLC writer (host code, no GPU) against the reference corpus.
+"""The library's bitstream writer (host code, no GPU) against the reference corpus and the oracle.
 
-Fed the macroblock records the oracle chose for the reference corpus clips, the product writer
-must emit exactly the pinned SPS, PPS and slice NAL units of qa/corpus/synth/clip_160x90_30fps.mp4
-and clip_320x180_25fps.mkv (two / one 15-picture GOPs, QP 20, Baseline), and exactly the oracle's
-bytes on grating clips with every macroblock kind at several QPs and sizes. GPU records go through
-the same writer in test_gpu_bitstream.py.
+* CAVLC (Baseline): fed the macroblock records the oracle chose for the reference corpus clips,
+  the product writer must emit exactly the pinned SPS, PPS and slice NAL units of
+  qa/corpus/synth/clip_160x90_30fps.mp4 and clip_320x180_25fps.mkv (two / one 15-picture GOPs,
+  QP 20), and exactly the oracle's bytes on grating clips at several QPs and sizes.
+* CABAC (Main, High with 8x8 transforms): the product writer (the arithmetic coder of the
+  standard, per-macroblock context summaries) and the oracle (a restatement of the reference's
+  cabac.rs engine and h264.rs / enc.rs glue) must give the same bytes; the reference holds no
+  CABAC output of its own encoder, so both are further pinned by decoding: FFmpeg's H.264 decoder
+  must turn the stream into exactly the oracle's reconstruction, every plane of every picture.
+GPU records go through the same writer in test_gpu_bitstream.py.
 """
 from pathlib import Path
 
@@ -12,7 +17,7 @@ import numpy as np
 import pytest
 
 from oracle_lib import OracleEncoder, read_nal_fixture, split_annex_b
-from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, CavlcWriter, RgError
+from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, BitstreamWriter, CavlcWriter, RgError
 from ragdoll_b200.synth import grating_clip, synth_video_frame
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -54,12 +59,66 @@ def test_writer_matches_oracle_bytes(w, h, qp):
     writer_gops(w, h, frames, qp, (30, 1), gop=4)
 
 
-def test_writer_rejects_cabac_profiles_and_bad_calls():
+def test_writer_rejects_bad_calls():
     from ragdoll_b200.engine import RECORD_DTYPE, RgConfig, lib
     import ctypes
-    cfg = RgConfig(64, 64, 2, 26, 1, 0, 1)
+    cfg = RgConfig(64, 64, 7, 26, 1, 0, 1)
     assert not lib().rg_writer_create(ctypes.byref(cfg), 30, 1)
-    assert b"CABAC" in lib().rg_last_error()
-    wr = CavlcWriter(64, 64, 26)
-    with pytest.raises(RgError):
-        wr.picture(np.zeros(16, RECORD_DTYPE), RG_FRAME_P)  # P before any IDR
+    assert b"profile" in lib().rg_last_error()
+    for profile in (0, 2):
+        wr = BitstreamWriter(64, 64, 26, profile=profile)
+        with pytest.raises(RgError):
+            wr.picture(np.zeros(16, RECORD_DTYPE), RG_FRAME_P)  # P before any IDR
+        recs = np.zeros(16, RECORD_DTYPE)
+        recs["mb_type"] = 0  # P_Skip
+        with pytest.raises(RgError):
+            wr.picture(recs, RG_FRAME_IDR)                    # P_Skip in an IDR picture
+
+
+def cabac_gop(w, h, qp, profile, frames, keyint):
+    """Oracle decisions and bytes, product bytes, oracle reconstructions."""
+    orc = OracleEncoder(w, h, qp, profile=profile, keyint=keyint)
+    wr = BitstreamWriter(w, h, qp, profile=profile)
+    aus, recons = [], []
+    for i, fr in enumerate(frames):
+        want, recs = orc.encode(fr)
+        got = wr.picture(recs, RG_FRAME_IDR if orc.last_idr else RG_FRAME_P)
+        assert got == want, f"picture {i}: writer {len(got)} B, oracle {len(want)} B"
+        aus.append(got)
+        recons.append([p.copy() for p in orc.recon()])
+    return aus, recons
+
+
+@pytest.mark.parametrize("w,h,qp,profile", [
+    (176, 144, 26, 1), (176, 144, 26, 2), (208, 120, 12, 2), (250, 138, 30, 2),
+    (96, 64, 40, 1), (64, 48, 51, 2), (48, 32, 1, 2), (16, 16, 22, 2),
+])
+def test_cabac_writer_matches_oracle_and_decodes(w, h, qp, profile):
+    import ffmpeg_decode
+    frames = grating_clip(w, h, 7, seed=5 + w + qp, motion=6.0, rects=2)
+    aus, recons = cabac_gop(w, h, qp, profile, frames, keyint=4)
+    for n in split_annex_b(aus[0])[:1]:
+        assert n[1] == (77 if profile == 1 else 100)          # profile_idc
+    if not ffmpeg_decode.available():
+        pytest.skip("FFmpeg libraries not found")
+    pics = ffmpeg_decode.decode(aus)
+    assert len(pics) == len(recons)
+    for i, (p, r) in enumerate(zip(pics, recons)):
+        for k in range(3):
+            assert np.array_equal(p[k], r[k][:p[k].shape[0], :p[k].shape[1]]), f"picture {i} plane {k}"
+
+
+def test_cabac_streams_use_every_syntax_path():
+    """The clips above reach 8x8 transforms, I_4x4 / I_16x16 / P_Skip / P_L0_16x16 macroblocks,
+    levels beyond the unary prefix (>= 15) and vectors beyond the mvd prefix (|mvd| >= 9)."""
+    seen = {"t8": 0, "big_level": 0, "big_mvd": 0, "types": set()}
+    for w, h, qp in ((208, 120, 12), (176, 144, 26), (48, 32, 1)):
+        orc = OracleEncoder(w, h, qp, profile=2, keyint=4)
+        for fr in grating_clip(w, h, 7, seed=5 + w + qp, motion=6.0, rects=2):
+            _, recs = orc.encode(fr)
+            seen["t8"] += int((recs["transform_8x8"] != 0).sum())
+            seen["big_level"] += int((np.abs(recs["luma"]) >= 15).sum())
+            seen["big_mvd"] += int((np.abs(recs["mvd"]) >= 9).sum())
+            seen["types"] |= set(int(t) for t in recs["mb_type"])
+    assert seen["t8"] and seen["big_level"] and seen["big_mvd"]
+    assert len(seen["types"]) == 4

@@ -1,6 +1,8 @@
-"""Bitstreams from GPU decisions (GPU tests): the engine's records, written by the library's CAVLC
-writer, must give the reference corpus's NAL units byte for byte, and the oracle's access units
-on the 1280x720 Baseline QP 30 configuration and on batched streams of the pipelined launch.
+"""Bitstreams from GPU decisions (GPU tests): the engine's records, written by the library's
+writer, must give the reference corpus's NAL units byte for byte (CAVLC), and the oracle's access
+units on the 1280x720 Baseline QP 30 configuration, on the 1920x1080 High QP 26 configuration
+(CABAC, 8x8 transforms) and on batched Main-profile streams of the pipelined launch. The High
+stream must also decode, through FFmpeg's H.264 decoder, to exactly the engine's reconstruction.
 """
 from pathlib import Path
 
@@ -61,6 +63,44 @@ def test_gpu_pipelined_streams_bitstreams_match_oracle():
     for s in range(S):
         orc = OracleEncoder(w, h, qp, profile=0, keyint=F + 1)
         wr = CavlcWriter(w, h, qp)
+        for f in range(F):
+            want, _ = orc.encode(clips[s][f])
+            assert wr.picture(recs[f, s], kinds[f][s]) == want, f"stream {s} picture {f}"
+
+
+def test_gpu_1080p_high_cabac_bitstream_matches_oracle_and_decodes():
+    import ffmpeg_decode
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, BitstreamWriter, Engine
+    w, h, qp = 1920, 1080, 26
+    frames = grating_clip(w, h, 3, seed=2001, motion=24.0, rects=12)
+    eng = Engine(w, h, qp, profile=2)
+    orc = OracleEncoder(w, h, qp, profile=2, keyint=15)
+    wr = BitstreamWriter(w, h, qp, profile=2)
+    aus, recons = [], []
+    for i, fr in enumerate(frames):
+        want, _ = orc.encode(fr)
+        kind = RG_FRAME_IDR if orc.last_idr else RG_FRAME_P
+        got = wr.picture(eng.analyse([fr], [kind])[0], kind)
+        assert got == want, f"picture {i}: {len(got)} vs {len(want)} bytes"
+        aus.append(got)
+        recons.append([p.copy() for p in eng.recon_coded(0)])
+    if not ffmpeg_decode.available():
+        pytest.skip("FFmpeg libraries not found")
+    for i, (p, r) in enumerate(zip(ffmpeg_decode.decode(aus), recons)):
+        for k in range(3):
+            assert np.array_equal(p[k], r[k][:p[k].shape[0], :p[k].shape[1]]), f"picture {i} plane {k}"
+
+
+def test_gpu_pipelined_main_streams_bitstreams_match_oracle():
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, BitstreamWriter, Engine
+    w, h, qp, S, F = 320, 180, 28, 4, 6
+    clips = [grating_clip(w, h, F, seed=50 + s, motion=8.0, rects=3) for s in range(S)]
+    eng = Engine(w, h, qp, profile=1, num_streams=S, max_frames=F)
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)]
+    recs = eng.analyse_gops([[clips[s][f] for s in range(S)] for f in range(F)], kinds)
+    for s in range(S):
+        orc = OracleEncoder(w, h, qp, profile=1, keyint=F + 1)
+        wr = BitstreamWriter(w, h, qp, profile=1)
         for f in range(F):
             want, _ = orc.encode(clips[s][f])
             assert wr.picture(recs[f, s], kinds[f][s]) == want, f"stream {s} picture {f}"
