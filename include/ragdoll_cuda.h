@@ -121,7 +121,8 @@ int rg_mb_dims(const rg_ctx* ctx, int32_t* mb_w, int32_t* mb_h);
  * Analyses, reconstructs and deblocks one frame of one stream from host planes (replaces
  * encode_frame_body's macroblock loop, deblock and border extension, enc.rs:2382-2503).
  * kind: RG_FRAME_IDR or RG_FRAME_P (a P frame needs an earlier frame of the stream).
- * out: mb_w * mb_h records in raster order (may be NULL to skip the copy).
+ * out: mb_w * mb_h records in raster order (may be NULL to skip the copy). In a context of
+ * several streams only `stream` is analysed (its own wavefront launches); the others stay put.
  */
 int rg_analyse_frame(rg_ctx* ctx, int32_t stream, const uint8_t* y, const uint8_t* u,
                      const uint8_t* v, size_t stride_y, size_t stride_uv, int32_t kind,
@@ -178,6 +179,11 @@ int rg_copy_records_gops(rg_ctx* ctx, int32_t frames, rg_mb_out* out);
  */
 int rg_analyse_gops_async(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
                           const int32_t* kinds, int32_t frames, rg_mb_out* out);
+
+/* Waits until the records of the rg_analyse_gops_async call that copies into `out` are in host
+ * memory and final (for the latest call: everything queued, as rg_sync; for the one before it:
+ * its copy out only, so the latest call's launch keeps running). No counterpart in the reference. */
+int rg_analyse_gops_wait(rg_ctx* ctx, const rg_mb_out* out);
 
 /* Tuning of the pipelined mode (rg_set_pipeline_tuning); 0 in any field selects the default. */
 typedef struct rg_pipeline_tuning {
@@ -307,6 +313,37 @@ size_t rg_writer_bound(const rg_writer* writer);
 /* Writes the access unit of one picture (records: mb_w * mb_h, raster order; kind RG_FRAME_*)
  * into out; returns its size in bytes, or a negative RG_ERR_* (the buffer too small included). */
 int64_t rg_writer_picture(rg_writer* writer, const rg_mb_out* records, int32_t kind, uint8_t* out, size_t cap);
+
+/* ---- Encoder (host + GPU) ---------------------------------------------------------------- */
+/*
+ * H264Encoder (crates/ragdoll-codec/src/h264.rs:2996) with the macroblock loop on the GPU: the
+ * engine analyses, reconstructs and deblocks each picture and the host writes its access unit
+ * (rg_writer_* coding: CAVLC for Baseline, CABAC for Main / High). Stream s is an independent
+ * encoder (GOP); its picture k is an IDR picture when k % keyint == 0 (enc.rs:2245). threads <= 0:
+ * one per host core.
+ */
+typedef struct rg_encoder rg_encoder;
+rg_encoder* rg_encoder_create(const rg_config* cfg, int32_t fps_num, int32_t fps_den, int32_t keyint, int32_t threads);
+void rg_encoder_destroy(rg_encoder* enc);
+int32_t rg_encoder_threads(const rg_encoder* enc);
+/* H264Encoder::encode_frame (h264.rs:3153) for one stream: the Annex-B access unit of the next
+ * picture into out; returns its size or a negative RG_ERR_*. Not while waves are in flight. */
+int64_t rg_encode_frame(rg_encoder* enc, int32_t stream, const uint8_t* y, const uint8_t* u, const uint8_t* v,
+                        size_t stride_y, size_t stride_uv, uint8_t* out, size_t cap);
+/*
+ * One wave of GopRingEncoder::encode_wave (crates/ragdoll-pipeline/src/lib.rs:543): the next
+ * `frames` pictures of every stream (planes: frames * num_streams * 3 host pointers, [f][s][y,u,v];
+ * frames <= cfg.max_frames) are queued for the GPU and the call returns. At most two waves are in
+ * flight: while the host writes one (rg_encoder_collect) the GPU analyses the next. The sources
+ * may be reused after the wave is collected; pinned sources copy fastest.
+ */
+int rg_encoder_submit(rg_encoder* enc, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, int32_t frames);
+/*
+ * The access units of the oldest wave, written on the pool's threads: concatenated picture-major
+ * ([f][s]) into out, sizes[f * num_streams + s] their sizes; returns the total. With out NULL only
+ * the sizes and the total are returned and the wave stays to be collected.
+ */
+int64_t rg_encoder_collect(rg_encoder* enc, uint8_t* out, size_t cap, int64_t* sizes);
 
 /* ---- Containers (host) ------------------------------------------------------------------ */
 /*

@@ -4,8 +4,8 @@
 // prediction modes, mvd, coded_block_pattern, mb_qp_delta, the residual blocks of categories 0-5
 // and end_of_slice_flag.
 //
-// The arithmetic coder is the encoding process of ITU-T H.264 9.3.4 written bit by bit
-// (RenormE / PutBit with bitsOutstanding / EncodeFlush), and the context indices come from the
+// The arithmetic coder follows the encoding process of ITU-T H.264 9.3.4 a byte at a time
+// (carries resolved when the slice is done), and the context indices come from the
 // derivations of 9.3.3.1.1 evaluated on a small per-macroblock summary (flags, coded block
 // pattern, a 16-bit mask of the luma 4x4 blocks holding levels, 4-bit masks per chroma plane,
 // |mvd|) kept for the row above and the macroblock to the left. The reference uses the same
@@ -16,7 +16,7 @@
 #include <cstring>
 #include <vector>
 
-#include "../../include/ragdoll_cuda.h"
+#include "bitstream.h"
 #include "cabac_tables.h"
 
 namespace rg {
@@ -25,35 +25,16 @@ namespace {
 
 using cabac::kContexts;
 
-// MSB-first bits into bytes.
-class Bits {
- public:
-  explicit Bits(std::vector<uint8_t>& out) : out_(out) {}
-  void bit(unsigned b) {
-    acc_ = (acc_ << 1) | (b & 1u);
-    if (++n_ == 8) {
-      out_.push_back((uint8_t)acc_);
-      acc_ = 0;
-      n_ = 0;
-    }
-  }
-  void run(unsigned b, uint32_t count) {
-    for (uint32_t i = 0; i < count; i++) bit(b);
-  }
-  void align_zero() {
-    while (n_) bit(0);
-  }
-
- private:
-  std::vector<uint8_t>& out_;
-  uint32_t acc_ = 0;
-  int n_ = 0;
-};
-
-// ITU-T H.264 9.3.4.2-9.3.4.5. Context models are packed as pStateIdx << 1 | valMPS.
+// The arithmetic coder of ITU-T H.264 9.3.4.2-9.3.4.5, a byte at a time. `low` holds the code
+// value's bits from the highest one not yet written (position `top`) down to the 10-bit window
+// of the standard's codILow; a byte is split off once its 8 bits lie above the window. An
+// addition to `low` may carry into bytes already split off: each byte is kept with the carry it
+// received (up to 9 bits) and the carries are resolved, last byte first, when the slice is done.
+// The first bit of the code value (the standard's firstBitFlag) is always 0 and never written.
+// Context models are packed as pStateIdx << 1 | valMPS.
 class Arith {
  public:
-  explicit Arith(Bits& bits) : bits_(bits) {}
+  explicit Arith(std::vector<uint8_t>& out) : out_(out) {}
 
   void decision(uint8_t& model, unsigned bin) {
     unsigned state = model >> 1, mps = model & 1u;
@@ -68,62 +49,67 @@ class Arith {
       state++;
     }
     model = (uint8_t)(state << 1 | mps);
-    renorm();
+    const int shift = __builtin_clz(range_) - 23;  // range_ < 512: doubles it to 256..511
+    range_ <<= shift;
+    low_ <<= shift;
+    top_ += shift;
+    split();
   }
   void bypass(unsigned bin) {
     low_ <<= 1;
     if (bin) low_ += range_;
-    if (low_ >= 1024) {
-      put(1);
-      low_ -= 1024;
-    } else if (low_ < 512) {
-      put(0);
-    } else {
-      low_ -= 512;
-      outstanding_++;
-    }
+    top_++;
+    split();
   }
-  // end_of_slice_flag; 1 flushes the coder (its last written bit is rbsp_stop_one_bit).
+  // end_of_slice_flag; 1 flushes the coder (9.3.4.5): the rest of the code value down to bit 8
+  // of the window, then rbsp_stop_one_bit, zeros to the byte boundary, and the carries resolved.
   void terminate(unsigned bin) {
     range_ -= 2;
     if (!bin) {
-      renorm();
+      if (range_ < 256) {
+        range_ <<= 1;
+        low_ <<= 1;
+        top_++;
+        split();
+      }
       return;
     }
     low_ += range_;
-    range_ = 2;
-    renorm();
-    put((low_ >> 9) & 1u);
-    bits_.bit((low_ >> 8) & 1u);
-    bits_.bit(1);
-  }
-
- private:
-  void put(unsigned b) {
-    if (first_) first_ = false;
-    else bits_.bit(b);
-    bits_.run(b ^ 1u, outstanding_);
-    outstanding_ = 0;
-  }
-  void renorm() {
-    while (range_ < 256) {
-      if (low_ < 256) {
-        put(0);
-      } else if (low_ >= 512) {
-        low_ -= 512;
-        put(1);
-      } else {
-        low_ -= 256;
-        outstanding_++;
-      }
-      range_ <<= 1;
-      low_ <<= 1;
+    low_ <<= 7;  // range 2 renormalised
+    top_ += 7;
+    split();
+    uint32_t v = (low_ >> 8) << 1 | 1u;  // bits top_..8, the stop bit; a carry above them
+    int n = top_ - 6;
+    const int pad = (8 - n % 8) % 8;
+    v <<= pad;
+    n += pad;
+    for (; n > 0; n -= 8) {
+      pend_.push_back((uint16_t)(v >> (n - 8)));
+      v &= (1u << (n - 8)) - 1;
+    }
+    size_t at = out_.size();
+    out_.resize(at + pend_.size());
+    unsigned carry = 0;
+    for (size_t i = pend_.size(); i-- > 0;) {
+      const unsigned b = pend_[i] + carry;
+      out_[at + i] = (uint8_t)b;
+      carry = b >> 8;
     }
   }
 
-  Bits& bits_;
-  uint32_t low_ = 0, range_ = 510, outstanding_ = 0;
-  bool first_ = true;
+ private:
+  void split() {
+    if (top_ >= 17) {  // bits top_..top_-7 are above the window
+      pend_.push_back((uint16_t)(low_ >> (top_ - 7)));
+      low_ &= (1u << (top_ - 7)) - 1;
+      top_ -= 8;
+    }
+  }
+
+  std::vector<uint8_t>& out_;
+  std::vector<uint16_t> pend_;
+  uint32_t low_ = 0, range_ = 510;
+  int top_ = 8;
 };
 
 // What later macroblocks read of a coded one.
@@ -153,7 +139,7 @@ inline int blk_y(int b) { return ((b >> 1) & 1) | ((b >> 2) & 2); }
 class SliceCoder {
  public:
   SliceCoder(int mb_w, int mb_h, int qp, bool idr, bool t8x8, std::vector<uint8_t>& out)
-      : mb_w_(mb_w), mb_h_(mb_h), idr_(idr), t8x8_(t8x8), bits_(out), ar_(bits_), above_(mb_w), modes_(mb_w * 4) {
+      : mb_w_(mb_w), mb_h_(mb_h), idr_(idr), t8x8_(t8x8), ar_(out), above_(mb_w), modes_(mb_w * 4) {
     const int table = idr ? 0 : 1;  // cabac_init_idc 0
     for (int i = 0; i < kContexts; i++) {
       const cabac::MN mn = cabac::kInit[table][i];
@@ -179,7 +165,6 @@ class SliceCoder {
         left_ = cur;
       }
     }
-    bits_.align_zero();
     return 0;
   }
 
@@ -439,7 +424,6 @@ class SliceCoder {
 
   int mb_w_, mb_h_;
   bool idr_, t8x8_;
-  Bits bits_;
   Arith ar_;
   uint8_t ctx_[kContexts];
   std::vector<MbSummary> above_;

@@ -15,11 +15,7 @@
 #include "../../include/ragdoll_cuda.h"
 #include "cavlc_tables.h"
 
-namespace rg {
-void set_last_error(const char* msg);
-int cabac_slice_data(int mb_w, int mb_h, int qp, bool idr, bool transform_8x8, const rg_mb_out* recs,
-                     std::vector<uint8_t>& out);
-}
+#include "bitstream.h"
 
 namespace {
 
@@ -354,6 +350,69 @@ struct rg_writer {
   }
 };
 
+namespace rg {
+
+// The access unit of one picture (SPS and PPS first for an IDR) with explicit frame_num / POC
+// (pictures since the IDR) and idr_pic_id; uses the writer's configuration and scratch only, so
+// writers of the same configuration can write pictures of one stream on several threads.
+int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_t since_idr, uint32_t idr_id,
+                       std::vector<uint8_t>& au) {
+  int n4 = w->mb_w * w->mb_h * 16;
+  w->nnz.assign(n4, 0);
+  w->cnnz[0].assign(w->mb_w * w->mb_h * 4, 0);
+  w->cnnz[1].assign(w->mb_w * w->mb_h * 4, 0);
+  w->mode4.assign(n4, 2);
+
+  Rbsp s;
+  s.ue(0);                          // first_mb_in_slice
+  s.ue(idr ? 7 : 5);                // slice_type: I or P, all slices of the picture alike
+  s.ue(0);                          // pic_parameter_set_id
+  s.put(since_idr & 15, 4);         // frame_num
+  if (idr) s.ue(idr_id);            // idr_pic_id
+  s.put((since_idr * 2) & 63, 6);   // pic_order_cnt_lsb
+  if (!idr) {
+    s.flag(false);                  // num_ref_idx_active_override_flag
+    s.flag(false);                  // ref_pic_list_modification_flag_l0
+  }
+  if (idr) {
+    s.flag(false);                  // no_output_of_prior_pics_flag
+    s.flag(false);                  // long_term_reference_flag
+  } else {
+    s.flag(false);                  // adaptive_ref_pic_marking_mode_flag
+  }
+  const bool cabac = w->profile != RG_PROFILE_BASELINE;
+  if (cabac && !idr) s.ue(0);       // cabac_init_idc
+  s.se(0);                          // slice_qp_delta
+  s.ue(0);                          // disable_deblocking_filter_idc (QP >= 1)
+  s.se(0);                          // slice_alpha_c0_offset_div2
+  s.se(0);                          // slice_beta_offset_div2
+  const std::vector<uint8_t>* rbsp;
+  if (cabac) {
+    std::vector<uint8_t>& bytes = s.align_ones();
+    if (rg::cabac_slice_data(w->mb_w, w->mb_h, w->qp, idr, w->profile == RG_PROFILE_HIGH, records, bytes))
+      return wfail(RG_ERR_INVALID, "rg_writer_picture: a record no %s slice holds", idr ? "IDR" : "P");
+    rbsp = &bytes;
+  } else {
+    uint32_t skip_run = 0;
+    for (int mby = 0; mby < w->mb_h; mby++)
+      for (int mbx = 0; mbx < w->mb_w; mbx++) {
+        int r = w->mb_layer(s, mbx, mby, records[mby * w->mb_w + mbx], idr, skip_run);
+        if (r) return r;
+      }
+    if (!idr && skip_run) s.ue(skip_run);
+    rbsp = &s.close();
+  }
+  au.clear();
+  if (idr) {
+    emit_nal(au, 3, 7, w->sps());
+    emit_nal(au, 3, 8, w->pps());
+  }
+  emit_nal(au, 3, idr ? 5 : 1, *rbsp);
+  return 0;
+}
+
+}  // namespace rg
+
 extern "C" {
 
 rg_writer* rg_writer_create(const rg_config* cfg, int32_t fps_num, int32_t fps_den) {
@@ -399,57 +458,9 @@ int64_t rg_writer_picture(rg_writer* w, const rg_mb_out* records, int32_t kind, 
   if (kind == RG_FRAME_P && !w->have_idr) return wfail(RG_ERR_STATE, "rg_writer_picture: P picture before an IDR");
   bool idr = kind == RG_FRAME_IDR;
   if (idr) w->since_idr = 0;
-  int n4 = w->mb_w * w->mb_h * 16;
-  w->nnz.assign(n4, 0);
-  w->cnnz[0].assign(w->mb_w * w->mb_h * 4, 0);
-  w->cnnz[1].assign(w->mb_w * w->mb_h * 4, 0);
-  w->mode4.assign(n4, 2);
-
-  Rbsp s;
-  s.ue(0);                          // first_mb_in_slice
-  s.ue(idr ? 7 : 5);                // slice_type: I or P, all slices of the picture alike
-  s.ue(0);                          // pic_parameter_set_id
-  s.put(w->since_idr & 15, 4);      // frame_num
-  if (idr) s.ue(w->idrs);           // idr_pic_id
-  s.put((w->since_idr * 2) & 63, 6);  // pic_order_cnt_lsb
-  if (!idr) {
-    s.flag(false);                  // num_ref_idx_active_override_flag
-    s.flag(false);                  // ref_pic_list_modification_flag_l0
-  }
-  if (idr) {
-    s.flag(false);                  // no_output_of_prior_pics_flag
-    s.flag(false);                  // long_term_reference_flag
-  } else {
-    s.flag(false);                  // adaptive_ref_pic_marking_mode_flag
-  }
-  const bool cabac = w->profile != RG_PROFILE_BASELINE;
-  if (cabac && !idr) s.ue(0);       // cabac_init_idc
-  s.se(0);                          // slice_qp_delta
-  s.ue(0);                          // disable_deblocking_filter_idc (QP >= 1)
-  s.se(0);                          // slice_alpha_c0_offset_div2
-  s.se(0);                          // slice_beta_offset_div2
-  const std::vector<uint8_t>* rbsp;
-  if (cabac) {
-    std::vector<uint8_t>& bytes = s.align_ones();
-    if (rg::cabac_slice_data(w->mb_w, w->mb_h, w->qp, idr, w->profile == RG_PROFILE_HIGH, records, bytes))
-      return wfail(RG_ERR_INVALID, "rg_writer_picture: a record no %s slice holds", idr ? "IDR" : "P");
-    rbsp = &bytes;
-  } else {
-    uint32_t skip_run = 0;
-    for (int mby = 0; mby < w->mb_h; mby++)
-      for (int mbx = 0; mbx < w->mb_w; mbx++) {
-        int r = w->mb_layer(s, mbx, mby, records[mby * w->mb_w + mbx], idr, skip_run);
-        if (r) return r;
-      }
-    if (!idr && skip_run) s.ue(skip_run);
-    rbsp = &s.close();
-  }
   std::vector<uint8_t> au;
-  if (idr) {
-    emit_nal(au, 3, 7, w->sps());
-    emit_nal(au, 3, 8, w->pps());
-  }
-  emit_nal(au, 3, idr ? 5 : 1, *rbsp);
+  int r = rg::writer_access_unit(w, records, idr, w->since_idr, w->idrs, au);
+  if (r) return r;
   if (au.size() > cap)
     return wfail(RG_ERR_INVALID, "rg_writer_picture: access unit of %zu bytes exceeds the %zu-byte buffer", au.size(), cap);
   memcpy(out, au.data(), au.size());

@@ -147,6 +147,7 @@ struct rg_ctx {
   cudaStream_t a_in = nullptr, a_out = nullptr;
   cudaEvent_t a_in_done[2] = {nullptr, nullptr}, a_kern_done[2] = {nullptr, nullptr};
   cudaEvent_t a_out_done[2] = {nullptr, nullptr};
+  rg_mb_out* a_out_ptr[2] = {nullptr, nullptr};  // host buffer each slot's call copies into
   int a_slot = 0;
   std::vector<int> frames;         // frames analysed per stream
   // metrics scratch
@@ -333,7 +334,7 @@ int rg_keep_unfiltered(rg_ctx* c, int32_t enable) {
 void* rg_cuda_stream(rg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                             const int32_t* kinds, rg_mb_out* rec_base);
+                             const int32_t* kinds, rg_mb_out* rec_base, int only = -1);
 static int resolve_pending(rg_ctx* c, bool wait_out);
 
 int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
@@ -344,19 +345,22 @@ int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t 
   return enqueue_wavefront(c, dev_planes, stride_y, stride_uv, kinds, nullptr);
 }
 
-// One picture of every stream, one launch per anti-diagonal step; records at rec_base
-// (default: the first picture's records).
+// One picture of every stream (or of stream `only`), one launch per anti-diagonal step; records
+// at rec_base (default: the first picture's records). dev_planes and kinds hold one entry per
+// stream launched.
 static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                             const int32_t* kinds, rg_mb_out* rec_base) {
+                             const int32_t* kinds, rg_mb_out* rec_base, int only) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_batch_device: null argument");
   if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
     return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stride too small");
-  for (int s = 0; s < c->S; s++) {
-    if (kinds[s] != RG_FRAME_IDR && kinds[s] != RG_FRAME_P)
-      return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stream %d kind %d", s, kinds[s]);
-    if (kinds[s] == RG_FRAME_P && c->frames[s] == 0)
+  const int n = only >= 0 ? 1 : c->S;
+  for (int i = 0; i < n; i++) {
+    int s = only >= 0 ? only : i;
+    if (kinds[i] != RG_FRAME_IDR && kinds[i] != RG_FRAME_P)
+      return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stream %d kind %d", s, kinds[i]);
+    if (kinds[i] == RG_FRAME_P && c->frames[s] == 0)
       return fail(RG_ERR_STATE, "rg_analyse_batch_device: stream %d P frame without a reference", s);
-    if (!dev_planes[3 * s] || !dev_planes[3 * s + 1] || !dev_planes[3 * s + 2])
+    if (!dev_planes[3 * i] || !dev_planes[3 * i + 1] || !dev_planes[3 * i + 2])
       return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stream %d null plane", s);
   }
   int slot = c->slot;
@@ -364,12 +368,13 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
   CK(cudaEventSynchronize(c->slot_done[slot]));  // the pinned descriptor slot is free again
   StreamDev* h = c->h_streams[slot];
   size_t unf = c->unf_bytes();
-  for (int s = 0; s < c->S; s++) {
+  for (int i = 0; i < n; i++) {
+    int s = only >= 0 ? only : i;
     int par = c->frames[s] % c->nslots, prv = (c->frames[s] + c->nslots - 1) % c->nslots;
-    StreamDev& d = h[s];
-    d.src_y = dev_planes[3 * s];
-    d.src_u = dev_planes[3 * s + 1];
-    d.src_v = dev_planes[3 * s + 2];
+    StreamDev& d = h[i];
+    d.src_y = dev_planes[3 * i];
+    d.src_u = dev_planes[3 * i + 1];
+    d.src_v = dev_planes[3 * i + 2];
     d.cur_y = c->pic_plane(s, par, 0);
     d.cur_u = c->pic_plane(s, par, 1);
     d.cur_v = c->pic_plane(s, par, 2);
@@ -387,19 +392,20 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
     } else {
       d.unf_y = d.unf_u = d.unf_v = nullptr;
     }
-    d.kind = kinds[s];
+    d.kind = kinds[i];
     d.pad_ = 0;
   }
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
   fp.src_stride_uv = (int)stride_uv;
-  CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * c->S, cudaMemcpyHostToDevice, c->stream));
+  fp.n_streams = n;
+  CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * n, cudaMemcpyHostToDevice, c->stream));
   CK(cudaEventRecord(c->slot_done[slot], c->stream));
   int steps = wavefront_steps(fp);
   for (int t = 0; t < steps; t++) launch_wavefront_step(fp, c->d_streams[slot], t, c->stream);
   launch_extend_borders(fp, c->d_streams[slot], c->stream);
   CK(cudaGetLastError());
-  for (int s = 0; s < c->S; s++) c->frames[s]++;
+  for (int i = 0; i < n; i++) c->frames[only >= 0 ? only : i]++;
   return RG_OK;
 }
 
@@ -652,9 +658,22 @@ int rg_analyse_gops_async(rg_ctx* c, const uint8_t* const* planes, size_t stride
   CK(cudaStreamWaitEvent(c->a_out, c->a_kern_done[slot], 0));
   CK(cudaMemcpyAsync(out, c->a_recs[slot], bytes, cudaMemcpyDeviceToHost, c->a_out));
   CK(cudaEventRecord(c->a_out_done[slot], c->a_out));
+  c->a_out_ptr[slot] = out;
   c->pend_out = out;
   c->pend_out_bytes = bytes;
   return RG_OK;
+}
+
+int rg_analyse_gops_wait(rg_ctx* c, const rg_mb_out* out) {
+  if (!c || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_wait: null argument");
+  if (c->pend_out == out) return resolve_pending(c, true);  // the latest call: wait for everything
+  for (int i = 0; i < 2; i++)
+    if (c->a_in && c->a_out_ptr[i] == out) {
+      // an earlier call: resolved when the latest one was queued; only its copy out may run
+      CK(cudaEventSynchronize(c->a_out_done[i]));
+      return RG_OK;
+    }
+  return RG_OK;  // no call in flight writes into out
 }
 
 int rg_copy_records(rg_ctx* c, rg_mb_out* out) {
@@ -704,10 +723,29 @@ int rg_analyse_batch(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, s
 int rg_analyse_frame(rg_ctx* c, int32_t stream, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t stride_y,
                      size_t stride_uv, int32_t kind, rg_mb_out* out) {
   if (!c) return fail(RG_ERR_INVALID, "rg_analyse_frame: null context");
-  if (c->S != 1) return fail(RG_ERR_INVALID, "rg_analyse_frame: context has %d streams; use rg_analyse_batch", c->S);
-  if (stream != 0) return fail(RG_ERR_INVALID, "rg_analyse_frame: stream %d", stream);
-  const uint8_t* planes[3] = {y, u, v};
-  return rg_analyse_batch(c, planes, stride_y, stride_uv, &kind, out);
+  if (stream < 0 || stream >= c->S) return fail(RG_ERR_INVALID, "rg_analyse_frame: stream %d of %d", stream, c->S);
+  if (!y || !u || !v) return fail(RG_ERR_INVALID, "rg_analyse_frame: null plane");
+  if (c->S == 1) {
+    const uint8_t* planes[3] = {y, u, v};
+    return rg_analyse_batch(c, planes, stride_y, stride_uv, &kind, out);
+  }
+  // one stream of a multi-stream context: its own wavefront launches
+  int r = resolve_pending(c, false);
+  if (r) return r;
+  int w = c->cfg.width, cw = (w + 1) / 2;
+  if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "rg_analyse_frame: stride too small");
+  r = upload_planes(c, stream, y, u, v, stride_y, stride_uv);
+  if (r) return r;
+  uint8_t* d = c->srcs + c->src_bytes() * stream;
+  const uint8_t* dev[3] = {d, d + (size_t)w * c->cfg.height, d + (size_t)w * c->cfg.height + (size_t)cw * ((c->cfg.height + 1) / 2)};
+  r = enqueue_wavefront(c, dev, w, cw, &kind, nullptr, stream);
+  if (r) return r;
+  if (out) {
+    CK(cudaMemcpyAsync(out, c->recs + (size_t)stream * c->n_mb, sizeof(rg_mb_out) * c->n_mb, cudaMemcpyDeviceToHost,
+                       c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return RG_OK;
 }
 
 int rg_get_recon(rg_ctx* c, int32_t s, uint8_t* y, uint8_t* u, uint8_t* v, size_t sy, size_t suv) {

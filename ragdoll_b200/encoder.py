@@ -1,0 +1,96 @@
+"""H264Encoder with the macroblock loop on the GPU (rg_encoder_*, C++ host code around the engine).
+
+``H264Encoder`` mirrors ragdoll's encoder (crates/ragdoll-codec/src/h264.rs:2996): ``encode_frame``
+returns the Annex-B access unit of the next picture of a stream (an IDR picture every ``keyint``
+pictures, SPS and PPS in front of it). ``submit`` / ``collect`` are the batched form, one wave of
+GopRingEncoder::encode_wave (crates/ragdoll-pipeline/src/lib.rs:543): the next ``frames`` pictures
+of every stream go to the GPU in one persistent launch, and their access units are written on the
+host cores; with two waves in flight the GPU analyses one while the host writes the other.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from .engine import RG_PROFILE_HIGH, RgConfig, RgError, _u8, lib
+
+Frame = Tuple[np.ndarray, np.ndarray, np.ndarray]
+
+
+class H264Encoder:
+    def __init__(self, width: int, height: int, qp: int, profile: int = RG_PROFILE_HIGH, fps=(30, 1),
+                 keyint: int = 30, streams: int = 1, max_frames: int = 1, device: int = 0, threads: int = 0):
+        cfg = RgConfig(width, height, profile, qp, streams, device, max_frames)
+        self.h = lib().rg_encoder_create(ctypes.byref(cfg), fps[0], fps[1], keyint, threads)
+        if not self.h:
+            raise RgError(-1, lib().rg_last_error().decode())
+        self.width, self.height, self.streams, self.max_frames = width, height, streams, max_frames
+        cw, ch = (width + 15) // 16 * 16, (height + 15) // 16 * 16
+        self.bound = (cw * ch * 3 // 2) * 4 + (1 << 16)   # one access unit, generously
+        self.buf = np.zeros(self.bound, np.uint8)
+        self._inflight: List[list] = []                     # sources of waves not yet collected
+        self._out = np.zeros(0, np.uint8)
+
+    @property
+    def threads(self) -> int:
+        return lib().rg_encoder_threads(self.h)
+
+    def encode_frame(self, frame: Frame, stream: int = 0) -> bytes:
+        y, u, v = (np.ascontiguousarray(p, np.uint8) for p in frame)
+        n = lib().rg_encode_frame(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],
+                                  self.buf.ctypes.data, self.buf.size)
+        if n < 0:
+            raise RgError(n, lib().rg_last_error().decode())
+        return self.buf[:n].tobytes()
+
+    def submit(self, frames: Sequence[Sequence[Frame]]) -> None:
+        """frames[f][s]: the next len(frames) pictures of every stream."""
+        keep, ptrs = [], []
+        for pics in frames:
+            if len(pics) != self.streams:
+                raise RgError(-1, f"submit: {len(pics)} pictures for {self.streams} streams")
+            for y, u, v in pics:
+                planes = [np.ascontiguousarray(p, np.uint8) for p in (y, u, v)]
+                keep.append(planes)
+                ptrs += [p.ctypes.data for p in planes]
+        sy, suv = keep[0][0].strides[0], keep[0][1].strides[0]
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        rc = lib().rg_encoder_submit(self.h, arr, sy, suv, len(frames))
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+        self._inflight.append((keep, len(frames)))
+
+    def collect(self) -> List[List[bytes]]:
+        """Access units of the oldest submitted wave, [f][s]."""
+        if not self._inflight:
+            raise RgError(-6, "collect: no wave in flight")
+        frames = self._inflight[0][1]
+        sizes = np.zeros(frames * self.streams, np.int64)
+        total = lib().rg_encoder_collect(self.h, None, 0, sizes.ctypes.data)
+        if total < 0:
+            raise RgError(total, lib().rg_last_error().decode())
+        if self._out.size < total:
+            self._out = np.zeros(int(total * 1.25) + 1024, np.uint8)
+        got = lib().rg_encoder_collect(self.h, self._out.ctypes.data, self._out.size, sizes.ctypes.data)
+        if got != total:
+            raise RgError(got if got < 0 else -1, lib().rg_last_error().decode())
+        self._inflight.pop(0)
+        data, at, out = self._out[:total].tobytes(), 0, []
+        for f in range(frames):
+            row = []
+            for s in range(self.streams):
+                n = int(sizes[f * self.streams + s])
+                row.append(data[at:at + n])
+                at += n
+            out.append(row)
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().rg_encoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -41,7 +41,8 @@ EXPORTS = [
     "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_analyse_gops_async",
     "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture", "rg_pipeline_work_list",
     "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
-    "rg_demux_info", "rg_demux_access_unit",
+    "rg_demux_info", "rg_demux_access_unit", "rg_analyse_gops_wait", "rg_encoder_create", "rg_encoder_destroy",
+    "rg_encoder_threads", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect",
 ]
 
 
@@ -127,6 +128,18 @@ def lib() -> ctypes.CDLL:
     L.rg_set_pipeline_tuning.argtypes = [P, ctypes.POINTER(RgPipelineTuning)]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
+    L.rg_analyse_gops_wait.argtypes = [P, P]
+    L.rg_encoder_create.restype = P
+    L.rg_encoder_create.argtypes = [ctypes.POINTER(RgConfig)] + [ctypes.c_int32] * 4
+    L.rg_encoder_destroy.argtypes = [P]
+    L.rg_encoder_threads.restype = ctypes.c_int32
+    L.rg_encoder_threads.argtypes = [P]
+    L.rg_encode_frame.restype = ctypes.c_int64
+    L.rg_encode_frame.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, P,
+                                  ctypes.c_size_t]
+    L.rg_encoder_submit.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int32]
+    L.rg_encoder_collect.restype = ctypes.c_int64
+    L.rg_encoder_collect.argtypes = [P, P, ctypes.c_size_t, P]
     L.rg_mux_create.restype = P
     L.rg_mux_create.argtypes = [ctypes.c_int32] * 5
     L.rg_mux_destroy.argtypes = [P]
