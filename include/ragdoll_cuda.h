@@ -89,11 +89,13 @@ typedef struct rg_mb_out {
     int16_t chroma_ac[2][4][16]; /* zig-zag; slot 0 (the DC position) is unused              */
 } rg_mb_out;
 
-/* SSIM / MS-SSIM of a reconstruction against its source (QualityReport subset,
- * crates/ragdoll-pix/src/metrics.rs:13). */
+/* Quality of a reconstruction against its source (QualityReport, crates/ragdoll-pix/src/metrics.rs:13;
+ * evaluate_frame_quality :328): SSIM per plane and (4Y + U + V) / 6, 5-scale MS-SSIM of luma, PSNR
+ * per plane, over all samples (psnr_avg) and 6:1:1 weighted, SSIM in dB, VMAF-Lite of luma. */
 typedef struct rg_quality {
     double ssim_y, ssim_u, ssim_v, ssim_avg, ms_ssim;
     double psnr_y, psnr_u, psnr_v;
+    double psnr_avg, psnr_yuv_611, ssim_db, vmaf_lite;
 } rg_quality;
 
 typedef struct rg_ctx rg_ctx;
@@ -253,6 +255,18 @@ void* rg_cuda_stream(rg_ctx* ctx);
  */
 int rg_quality_frame(rg_ctx* ctx, int32_t stream, const uint8_t* y, const uint8_t* u,
                      const uint8_t* v, size_t stride_y, size_t stride_uv, rg_quality* q);
+
+/* rg_quality_frame with the previous source frame's luma (stride_prev), for VMAF-Lite's motion
+ * term (evaluate_frame_quality's prev_reference); prev_y NULL is rg_quality_frame. */
+int rg_quality_frame_prev(rg_ctx* ctx, int32_t stream, const uint8_t* y, const uint8_t* u,
+                          const uint8_t* v, size_t stride_y, size_t stride_uv, const uint8_t* prev_y,
+                          size_t stride_prev, rg_quality* q);
+
+/* VMAF-Lite (crates/ragdoll-pix/src/metrics.rs:218 vmaf_lite_plane_u8) of host planes on `device`:
+ * ref against dist, prev the previous reference plane or NULL. Result in *score (0..100). */
+int rg_vmaf_lite_plane(int32_t device, const uint8_t* ref, size_t stride_ref, const uint8_t* dist,
+                       size_t stride_dist, int32_t width, int32_t height, const uint8_t* prev,
+                       size_t stride_prev, double* score);
 
 /*
  * Stand-alone plane metrics on host planes (ssim_plane_u8 / ms_ssim_plane_u8,

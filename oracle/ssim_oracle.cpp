@@ -1,10 +1,13 @@
 // TEST INFRASTRUCTURE ONLY -- not part of the product path.
 //
-// CPU oracle of ragdoll's SSIM / MS-SSIM / PSNR (FFmpeg vf_ssim 4x4-sum reuse):
+// CPU oracle of ragdoll's SSIM / MS-SSIM / PSNR / VMAF-Lite (FFmpeg vf_ssim 4x4-sum reuse):
 //   crates/ragdoll-simd/src/metrics.rs:409-423  SSIM_C1_8BIT, SSIM_C2_8BIT, ssim_end1_8bit
 //   crates/ragdoll-simd/src/metrics.rs:505      ssim_4x4xn_u8_scalar
 //   crates/ragdoll-simd/src/metrics.rs:637      ssim_plane_8bit (f32 per row, f64 across rows)
 //   crates/ragdoll-pix/src/metrics.rs:87,154    decimate_2x2_u8_scalar, ms_ssim_plane_u8
+//   crates/ragdoll-pix/src/metrics.rs:218       vmaf_lite_plane_u8 (per-4x4 SSIM / VIF terms, f64
+//                                               sums in raster order, motion term from the plane SAD)
+//   crates/ragdoll-simd/src/metrics.rs:60,221   sad_plane_u8_scalar, sse_plane_u8_scalar
 // Built with -ffp-contract=off so no product is fused into an add, as in the reference.
 #include <algorithm>
 #include <cmath>
@@ -118,6 +121,73 @@ double oracle_psnr_plane(const uint8_t* a, long sa, const uint8_t* b, long sb, i
   if (sse == 0) return INFINITY;
   double mse = (double)sse / ((double)width * height);
   return 10.0 * std::log10((255.0 * 255.0) / mse);
+}
+
+// crates/ragdoll-simd/src/metrics.rs:221 sse_plane_u8_scalar
+uint64_t oracle_sse_plane(const uint8_t* a, long sa, const uint8_t* b, long sb, int width, int height) {
+  uint64_t sse = 0;
+  for (int y = 0; y < height; y++)
+    for (int x = 0; x < width; x++) {
+      int d = (int)a[y * sa + x] - (int)b[y * sb + x];
+      sse += (uint64_t)(d * d);
+    }
+  return sse;
+}
+
+// crates/ragdoll-pix/src/metrics.rs:218 vmaf_lite_plane_u8; prev may be NULL (no motion term).
+double oracle_vmaf_lite_plane(const uint8_t* ref, long sr, const uint8_t* dist, long sd, int width, int height,
+                              const uint8_t* prev, long sp) {
+  int bw = width >> 2, bh = height >> 2;
+  if (bw == 0 || bh == 0) return 100.0;
+  const double kSigmaNsq = 2.0 * 256.0, kEps = 1.0e-10, kGainLimit = 100.0;
+  std::vector<int> sums((size_t)bw * 4);
+  double info_num = 0.0, info_den = 0.0, ssim_acc = 0.0;
+  long blocks = 0;
+  for (int by = 0; by < bh; by++) {
+    sums4x4(ref + (long)by * 4 * sr, sr, dist + (long)by * 4 * sd, sd, bw, (int(*)[4])sums.data());
+    for (int bx = 0; bx < bw; bx++) {
+      int s1 = sums[bx * 4], s2 = sums[bx * 4 + 1], ss = sums[bx * 4 + 2], s12 = sums[bx * 4 + 3];
+      double mean_sq_sum = (double)(s1 * s1 + s2 * s2);
+      double total_var = (double)std::max(ss * 16 - s1 * s1 - s2 * s2, 0);
+      double covar = (double)(s12 * 16 - s1 * s2);
+      const double c1 = 26.0, c2 = 234.0;
+      double blk = ((2.0 * (double)s1 * (double)s2 + c1) * (2.0 * covar + c2)) / ((mean_sq_sum + c1) * (total_var + c2));
+      ssim_acc += std::min(1.0, std::max(0.0, blk));
+      double err_var = (double)std::max(ss - 2 * s12, 0) * 16.0 - (double)((s1 - s2) * (s1 - s2));
+      err_var = std::max(err_var, 0.0);
+      double sigma1_sq = std::max((total_var - err_var) * 0.5, std::max(covar, 0.0));
+      double sigma2_sq = std::max(total_var - sigma1_sq, 0.0);
+      double sigma12 = std::max(covar, 0.0);
+      double g, sv_sq;
+      if (sigma1_sq < kEps) {
+        g = 0.0; sv_sq = sigma2_sq;
+      } else if (sigma2_sq < kEps) {
+        g = 0.0; sv_sq = 0.0;
+      } else {
+        double g_raw = sigma12 / (sigma1_sq + kEps);
+        if (g_raw < 0.0) { g = 0.0; sv_sq = sigma2_sq; }
+        else { g = std::min(g_raw, kGainLimit); sv_sq = std::max(sigma2_sq - g_raw * sigma12, kEps); }
+      }
+      sv_sq = std::max(sv_sq, kEps);
+      g = std::min(g, kGainLimit);
+      info_num += std::log2(1.0 + (g * g * sigma1_sq) / (sv_sq + kSigmaNsq));
+      info_den += std::log2(1.0 + sigma1_sq / kSigmaNsq);
+      blocks++;
+    }
+  }
+  double mean_ssim = ssim_acc / (double)std::max(blocks, 1L);
+  if (std::fabs(1.0 - mean_ssim) < 1e-9) return 100.0;
+  double vif = info_den <= 1e-9 ? mean_ssim : std::min(1.0, std::max(0.0, info_num / info_den));
+  double boost = 0.0;
+  if (prev) {
+    uint64_t sad = 0;
+    for (int y = 0; y < height; y++)
+      for (int x = 0; x < width; x++) sad += (uint64_t)std::abs((int)ref[y * sr + x] - (int)prev[y * sp + x]);
+    double mad = (double)sad / ((double)width * height);
+    boost = std::min(mad / 255.0 * 0.08, 0.05);
+  }
+  double raw = (0.65 * std::pow(mean_ssim, 0.85) + 0.35 * vif + boost) * 100.0;
+  return std::min(100.0, std::max(0.0, raw));
 }
 
 }  // extern "C"

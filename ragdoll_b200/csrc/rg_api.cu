@@ -849,6 +849,7 @@ int device_metrics(const std::vector<PlanePair>& pairs, const std::vector<bool>&
   size_t rofs = 0, pofs = 0;
   int maxw = 0, maxh = 0;
   std::vector<int> job_of(n * 5, -1);
+  // the n full-size planes first (jobs 0..n-1: the SSE launch reads those), pyramid levels after
   for (int i = 0; i < n; i++) {
     const PlanePair& p = pairs[i];
     SsimJob j{p.a, p.b, p.sa, p.sb, p.w, p.h, rows + rofs, outs + jobs.size(), sses + i};
@@ -857,6 +858,9 @@ int device_metrics(const std::vector<PlanePair>& pairs, const std::vector<bool>&
     jobs.push_back(j);
     maxw = std::max(maxw, p.w);
     maxh = std::max(maxh, p.h);
+  }
+  for (int i = 0; i < n; i++) {
+    const PlanePair& p = pairs[i];
     if (want_ms[i]) {
       const uint8_t* sa = p.a;
       const uint8_t* sb = p.b;
@@ -927,12 +931,49 @@ double psnr_of(unsigned long long sse, long n) {
   return 10.0 * std::log10((255.0 * 255.0) / mse);
 }
 
+// VMAF-Lite of one plane pair on the device (prev may be null); scores via vmaf_lite_score.
+int device_vmaf(const uint8_t* a, long sa, const uint8_t* b, long sb, const uint8_t* prev, long sp, int w, int h,
+                cudaStream_t st, double* score) {
+  int bw = w >> 2, bh = h >> 2;
+  if (bw == 0 || bh == 0) {
+    *score = 100.0;
+    return RG_OK;
+  }
+  double* buf = nullptr;
+  VmafJob* d_job = nullptr;
+  if (cudaMalloc(&buf, (3 * (size_t)bh + 3) * sizeof(double) + sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&d_job, sizeof(VmafJob)) != cudaSuccess) {
+    cudaFree(buf);
+    return fail(RG_ERR_OOM, "vmaf: device allocation failed");
+  }
+  unsigned long long* sad = (unsigned long long*)(buf + 3 * (size_t)bh + 3);
+  VmafJob j{a, b, prev, sa, sb, sp, w, h, buf, buf + 3 * (size_t)bh, prev ? sad : nullptr};
+  double res[3];
+  unsigned long long sad_h = 0;
+  cudaMemsetAsync(sad, 0, sizeof(unsigned long long), st);
+  cudaMemcpyAsync(d_job, &j, sizeof j, cudaMemcpyHostToDevice, st);
+  launch_vmaf(d_job, 1, h, st);
+  cudaMemcpyAsync(res, buf + 3 * (size_t)bh, sizeof res, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&sad_h, sad, sizeof sad_h, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(buf);
+  cudaFree(d_job);
+  if (e != cudaSuccess) return fail(RG_ERR_CUDA, "vmaf: %s", cudaGetErrorString(e));
+  *score = vmaf_lite_score(res[0], res[1], res[2], (long)bw * bh, prev != nullptr, sad_h, (long)w * h);
+  return RG_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 int rg_quality_frame(rg_ctx* c, int32_t s, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t sy, size_t suv,
                      rg_quality* q) {
+  return rg_quality_frame_prev(c, s, y, u, v, sy, suv, nullptr, 0, q);
+}
+
+int rg_quality_frame_prev(rg_ctx* c, int32_t s, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t sy,
+                          size_t suv, const uint8_t* prev_y, size_t stride_prev, rg_quality* q) {
   if (!c || !y || !u || !v || !q) return fail(RG_ERR_INVALID, "rg_quality_frame: null argument");
   if (s < 0 || s >= c->S || c->frames[s] == 0) return fail(RG_ERR_STATE, "rg_quality_frame: stream %d", s);
   int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
@@ -958,7 +999,47 @@ int rg_quality_frame(rg_ctx* c, int32_t s, const uint8_t* y, const uint8_t* u, c
   q->psnr_y = psnr_of(sse[0], (long)w * h);
   q->psnr_u = psnr_of(sse[1], (long)cw * ch);
   q->psnr_v = psnr_of(sse[2], (long)cw * ch);
-  return RG_OK;
+  // the rest of evaluate_frame_quality (crates/ragdoll-pix/src/metrics.rs:374-392)
+  q->psnr_avg = psnr_of(sse[0] + sse[1] + sse[2], (long)w * h + 2L * cw * ch);
+  if (std::isinf(q->psnr_y) && std::isinf(q->psnr_u) && std::isinf(q->psnr_v))
+    q->psnr_yuv_611 = INFINITY;
+  else
+    q->psnr_yuv_611 = (6.0 * std::fmin(q->psnr_y, 100.0) + std::fmin(q->psnr_u, 100.0) + std::fmin(q->psnr_v, 100.0)) / 8.0;
+  q->ssim_db = q->ssim_avg >= 1.0 ? INFINITY : -10.0 * std::log10(1.0 - q->ssim_avg);
+  uint8_t* d_prev = nullptr;
+  if (prev_y) {
+    if (cudaMalloc(&d_prev, (size_t)w * h) != cudaSuccess) return fail(RG_ERR_OOM, "rg_quality_frame: allocation failed");
+    CK(cudaMemcpy2DAsync(d_prev, w, prev_y, stride_prev, w, h, cudaMemcpyHostToDevice, c->stream));
+  }
+  r = device_vmaf(c->m_src, w, c->pic_plane(s, par, 0), c->fp.stride_y, d_prev, w, w, h, c->stream, &q->vmaf_lite);
+  cudaFree(d_prev);
+  return r;
+}
+
+int rg_vmaf_lite_plane(int32_t device, const uint8_t* ref, size_t stride_ref, const uint8_t* dist, size_t stride_dist,
+                       int32_t width, int32_t height, const uint8_t* prev, size_t stride_prev, double* score) {
+  if (!ref || !dist || !score || width < 1 || height < 1) return fail(RG_ERR_INVALID, "rg_vmaf_lite_plane: bad argument");
+  CK(cudaSetDevice(device));
+  size_t n = (size_t)width * height;
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, 3 * n) != cudaSuccess) return fail(RG_ERR_OOM, "rg_vmaf_lite_plane: allocation failed");
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(d);
+    return fail(RG_ERR_CUDA, "rg_vmaf_lite_plane: stream creation failed");
+  }
+  int r = RG_OK;
+  if (cudaMemcpy2DAsync(d, width, ref, stride_ref, width, height, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpy2DAsync(d + n, width, dist, stride_dist, width, height, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      (prev && cudaMemcpy2DAsync(d + 2 * n, width, prev, stride_prev, width, height, cudaMemcpyHostToDevice, st) != cudaSuccess)) {
+    r = fail(RG_ERR_CUDA, "rg_vmaf_lite_plane: copy failed");
+  } else {
+    r = device_vmaf(d, width, d + n, width, prev ? d + 2 * n : nullptr, width, width, height, st, score);
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaFree(d);
+  return r;
 }
 
 int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8_t* b, size_t stride_b, int32_t width,

@@ -42,7 +42,8 @@ EXPORTS = [
     "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture", "rg_pipeline_work_list",
     "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
     "rg_demux_info", "rg_demux_access_unit", "rg_analyse_gops_wait", "rg_encoder_create", "rg_encoder_destroy",
-    "rg_encoder_threads", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect",
+    "rg_encoder_threads", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_quality_frame_prev",
+    "rg_vmaf_lite_plane",
 ]
 
 
@@ -72,7 +73,8 @@ class RgStreamInfo(ctypes.Structure):
 
 class RgQuality(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
-                ("ssim_y", "ssim_u", "ssim_v", "ssim_avg", "ms_ssim", "psnr_y", "psnr_u", "psnr_v")]
+                ("ssim_y", "ssim_u", "ssim_v", "ssim_avg", "ms_ssim", "psnr_y", "psnr_u", "psnr_v",
+                 "psnr_avg", "psnr_yuv_611", "ssim_db", "vmaf_lite")]
 
 
 _lib = None
@@ -129,6 +131,10 @@ def lib() -> ctypes.CDLL:
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
     L.rg_analyse_gops_wait.argtypes = [P, P]
+    L.rg_quality_frame_prev.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, u8p,
+                                        ctypes.c_size_t, ctypes.POINTER(RgQuality)]
+    L.rg_vmaf_lite_plane.argtypes = [ctypes.c_int32, u8p, ctypes.c_size_t, u8p, ctypes.c_size_t, ctypes.c_int32,
+                                     ctypes.c_int32, u8p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
     L.rg_encoder_create.restype = P
     L.rg_encoder_create.argtypes = [ctypes.POINTER(RgConfig)] + [ctypes.c_int32] * 4
     L.rg_encoder_destroy.argtypes = [P]
@@ -321,11 +327,18 @@ class Engine:
         _check(lib().rg_get_recon_unfiltered(self.h, stream, _u8(y), _u8(u), _u8(v)))
         return y, u, v
 
-    def quality(self, frame, stream: int = 0) -> dict:
+    def quality(self, frame, stream: int = 0, prev=None) -> dict:
+        """evaluate_frame_quality of the stream's last reconstruction against its source ``frame``;
+        ``prev`` (the previous source frame) adds VMAF-Lite's motion term."""
         y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in frame)
         q = RgQuality()
-        _check(lib().rg_quality_frame(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],
-                                      ctypes.byref(q)))
+        if prev is None:
+            _check(lib().rg_quality_frame(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],
+                                          ctypes.byref(q)))
+        else:
+            py = np.ascontiguousarray(prev[0], dtype=np.uint8)
+            _check(lib().rg_quality_frame_prev(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],
+                                               _u8(py), py.strides[0], ctypes.byref(q)))
         return {n: getattr(q, n) for n, _ in RgQuality._fields_}
 
 
@@ -337,6 +350,21 @@ def ssim_plane(a: np.ndarray, b: np.ndarray, device: int = 0):
     _check(lib().rg_ssim_plane(device, _u8(a), a.strides[0], _u8(b), b.strides[0], a.shape[1], a.shape[0],
                                ctypes.byref(s), ctypes.byref(m)))
     return s.value, m.value
+
+
+def vmaf_lite_plane(ref: np.ndarray, dist: np.ndarray, prev: np.ndarray = None, device: int = 0) -> float:
+    """VMAF-Lite of two 8-bit planes on the GPU (vmaf_lite_plane_u8); prev: previous reference plane."""
+    r = np.ascontiguousarray(ref, dtype=np.uint8)
+    d = np.ascontiguousarray(dist, dtype=np.uint8)
+    out = ctypes.c_double()
+    if prev is None:
+        _check(lib().rg_vmaf_lite_plane(device, _u8(r), r.strides[0], _u8(d), d.strides[0], r.shape[1], r.shape[0],
+                                        None, 0, ctypes.byref(out)))
+    else:
+        q = np.ascontiguousarray(prev, dtype=np.uint8)
+        _check(lib().rg_vmaf_lite_plane(device, _u8(r), r.strides[0], _u8(d), d.strides[0], r.shape[1], r.shape[0],
+                                        _u8(q), q.strides[0], ctypes.byref(out)))
+    return out.value
 
 
 def ssim_plane_device_noalloc(dev_a: int, stride_a: int, dev_b: int, stride_b: int, width: int, height: int,

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import re
 import struct
 import sys
 from pathlib import Path
@@ -163,10 +164,20 @@ def main(ref_root: str) -> None:
         (HERE / out).write_bytes(pack(nals))
         meta[out] = {"source": "qa/corpus/synth/" + name, "source_size": len(data),
                      "source_sha256": hashlib.sha256(data).hexdigest(), "nal_units": len(nals)}
+    golden = ref / "crates/ragdoll-cli/tests/golden"
+    text = (golden / "metrics.txt").read_text()
+    num = r"([0-9]+\.[0-9]+)"
+    pm = re.search(r"Y=" + num + r" dB \| U=" + num + r" dB \| V=" + num + r" dB \| Avg=" + num +
+                   r" dB \(6:1:1=" + num + r" dB\)", text)
+    sm = re.search(r"Y=" + num + r" \(" + num + r" dB\) \| Avg=" + num + r" \| 5-Scale MS-SSIM=" + num, text)
+    vm = re.search(r"VMAF-Lite\s*: " + num, text)
+    tm = re.search(r"out=([0-9]+) B", (golden / "transcode.txt").read_text())
     meta["cli_snapshots"] = {
-        "transcode_qp30_mp4_bytes": 2382,
-        "metrics": {"psnr_y": 43.28, "psnr_u": 50.27, "psnr_v": 49.79, "ssim_y": 0.99100,
-                    "ssim_avg": 0.99300, "ms_ssim": 0.99247},
+        "transcode_qp30_mp4_bytes": int(tm.group(1)),
+        "metrics": {"psnr_y": float(pm.group(1)), "psnr_u": float(pm.group(2)), "psnr_v": float(pm.group(3)),
+                    "psnr_avg": float(pm.group(4)), "psnr_yuv_611": float(pm.group(5)),
+                    "ssim_y": float(sm.group(1)), "ssim_db": float(sm.group(2)), "ssim_avg": float(sm.group(3)),
+                    "ms_ssim": float(sm.group(4)), "vmaf_lite": float(vm.group(1))},
         "source": "crates/ragdoll-cli/tests/golden/transcode.txt, metrics.txt",
     }
     (HERE / "golden.json").write_text(json.dumps(meta, indent=2) + "\n")

@@ -64,6 +64,11 @@ def lib():
             f = getattr(L, fn)
             f.restype = ctypes.c_double
             f.argtypes = [u8p, ctypes.c_long, u8p, ctypes.c_long, ctypes.c_int, ctypes.c_int]
+        L.oracle_sse_plane.restype = ctypes.c_uint64
+        L.oracle_sse_plane.argtypes = [u8p, ctypes.c_long, u8p, ctypes.c_long, ctypes.c_int, ctypes.c_int]
+        L.oracle_vmaf_lite_plane.restype = ctypes.c_double
+        L.oracle_vmaf_lite_plane.argtypes = [u8p, ctypes.c_long, u8p, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                             u8p, ctypes.c_long]
         assert L.oracle_record_size() == RECORD_DTYPE.itemsize
         _lib = L
     return _lib
@@ -124,6 +129,40 @@ def ms_ssim_plane(a, b):
 def psnr_plane(a, b):
     a = np.ascontiguousarray(a); b = np.ascontiguousarray(b)
     return lib().oracle_psnr_plane(_p(a), a.strides[0], _p(b), b.strides[0], a.shape[1], a.shape[0])
+
+
+def sse_plane(a, b):
+    a = np.ascontiguousarray(a); b = np.ascontiguousarray(b)
+    return lib().oracle_sse_plane(_p(a), a.strides[0], _p(b), b.strides[0], a.shape[1], a.shape[0])
+
+
+def vmaf_lite_plane(ref, dist, prev=None):
+    r = np.ascontiguousarray(ref); d = np.ascontiguousarray(dist)
+    if prev is None:
+        return lib().oracle_vmaf_lite_plane(_p(r), r.strides[0], _p(d), d.strides[0], r.shape[1], r.shape[0], None, 0)
+    q = np.ascontiguousarray(prev)
+    return lib().oracle_vmaf_lite_plane(_p(r), r.strides[0], _p(d), d.strides[0], r.shape[1], r.shape[0],
+                                        _p(q), q.strides[0])
+
+
+def quality_report(ref, dist, prev=None):
+    """evaluate_frame_quality (crates/ragdoll-pix/src/metrics.rs:328) from the oracle's plane metrics."""
+    import math
+    psnr = [psnr_plane(ref[p], dist[p]) for p in range(3)]
+    ssim = [ssim_plane(ref[p], dist[p]) for p in range(3)]
+    sse = sum(sse_plane(ref[p], dist[p]) for p in range(3))
+    n = sum(ref[p].size for p in range(3))
+    psnr_avg = math.inf if sse == 0 else 10.0 * math.log10((255.0 * 255.0) / (sse / n))
+    if all(math.isinf(v) for v in psnr):
+        psnr_611 = math.inf
+    else:
+        psnr_611 = (6.0 * min(psnr[0], 100.0) + min(psnr[1], 100.0) + min(psnr[2], 100.0)) / 8.0
+    ssim_avg = (4.0 * ssim[0] + ssim[1] + ssim[2]) / 6.0
+    ssim_db = math.inf if ssim_avg >= 1.0 else -10.0 * math.log10(1.0 - ssim_avg)
+    return {"psnr_y": psnr[0], "psnr_u": psnr[1], "psnr_v": psnr[2], "psnr_avg": psnr_avg,
+            "psnr_yuv_611": psnr_611, "ssim_y": ssim[0], "ssim_u": ssim[1], "ssim_v": ssim[2],
+            "ssim_avg": ssim_avg, "ssim_db": ssim_db, "ms_ssim": ms_ssim_plane(ref[0], dist[0]),
+            "vmaf_lite": vmaf_lite_plane(ref[0], dist[0], None if prev is None else prev[0])}
 
 
 def split_annex_b(data: bytes) -> list[bytes]:

@@ -80,7 +80,7 @@ def test_oracle_matches_cli_transcode_and_metrics_snapshots():
     2382-byte MP4 (ftyp 32 + moov 919 + mdat 8 + length-prefixed slices: the avcC and tables
     have equal sizes at both QPs) and the pinned PSNR / SSIM / MS-SSIM averages.
     """
-    from oracle_lib import ms_ssim_plane, psnr_plane, ssim_plane
+    from oracle_lib import ms_ssim_plane, psnr_plane, quality_report, ssim_plane
 
     meta = json.loads((GOLDEN / "golden.json").read_text())["cli_snapshots"]
     w, h = 160, 90
@@ -109,3 +109,8 @@ def test_oracle_matches_cli_transcode_and_metrics_snapshots():
     assert round(ssim[0], 5) == m["ssim_y"]
     assert round((4 * ssim[0] + ssim[1] + ssim[2]) / 6, 5) == m["ssim_avg"]
     assert round(ms, 5) == m["ms_ssim"]
+    # the rest of the report (evaluate_media_metrics, crates/ragdoll-pipeline/src/lib.rs:2879: each
+    # frame against the previous reference frame for VMAF-Lite's motion term, then the mean)
+    reps = [quality_report(a, b, r1[i - 1] if i else None) for i, (a, b) in enumerate(zip(r1, r2))]
+    for key, digits in (("psnr_avg", 2), ("psnr_yuv_611", 2), ("ssim_db", 2), ("vmaf_lite", 2)):
+        assert round(sum(r[key] for r in reps) / n, digits) == m[key], key
