@@ -120,6 +120,15 @@ void rg_destroy(rg_ctx* ctx);
 int rg_mb_dims(const rg_ctx* ctx, int32_t* mb_w, int32_t* mb_h);
 
 /*
+ * Sets the fixed QP (1..51) of one stream; the others keep theirs (cfg.qp by default). Streams of
+ * different QPs share every launch. Pictures queued before the call keep the QP they were queued
+ * with. A stream's bitstream has one QP (the writer's, in its PPS), so set it before the stream's
+ * first picture or at an IDR with a writer of the new QP. No counterpart in the reference (one
+ * H264Encoder per stream, each with its own rate control).
+ */
+int rg_set_stream_qp(rg_ctx* ctx, int32_t stream, int32_t qp);
+
+/*
  * Analyses, reconstructs and deblocks one frame of one stream from host planes (replaces
  * encode_frame_body's macroblock loop, deblock and border extension, enc.rs:2382-2503).
  * kind: RG_FRAME_IDR or RG_FRAME_P (a P frame needs an earlier frame of the stream).
@@ -340,6 +349,9 @@ typedef struct rg_encoder rg_encoder;
 rg_encoder* rg_encoder_create(const rg_config* cfg, int32_t fps_num, int32_t fps_den, int32_t keyint, int32_t threads);
 void rg_encoder_destroy(rg_encoder* enc);
 int32_t rg_encoder_threads(const rg_encoder* enc);
+/* The fixed QP (1..51) of one stream, before its first picture (default cfg.qp): streams of
+ * different QPs are analysed in the same launches and written with their own PPS. */
+int rg_encoder_set_stream_qp(rg_encoder* enc, int32_t stream, int32_t qp);
 /* H264Encoder::encode_frame (h264.rs:3153) for one stream: the Annex-B access unit of the next
  * picture into out; returns its size or a negative RG_ERR_*. Not while waves are in flight. */
 int64_t rg_encode_frame(rg_encoder* enc, int32_t stream, const uint8_t* y, const uint8_t* u, const uint8_t* v,

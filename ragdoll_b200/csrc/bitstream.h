@@ -17,6 +17,6 @@ int cabac_slice_data(int mb_w, int mb_h, int qp, bool idr, bool transform_8x8, c
 // The access unit of one picture with explicit frame counters (cavlc_writer.cpp); the writer
 // supplies configuration and scratch only. 0 or a negative RG_ERR_* code.
 int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_t since_idr, uint32_t idr_id,
-                       std::vector<uint8_t>& au);
+                       int qp, std::vector<uint8_t>& au);
 
 }  // namespace rg

@@ -225,7 +225,7 @@ struct rg_writer {
     w.flag(false);                  // bitstream_restriction_flag
     return w.close();
   }
-  std::vector<uint8_t> pps() const {
+  std::vector<uint8_t> pps(int qp) const {
     Rbsp w;
     w.ue(0);         // pic_parameter_set_id
     w.ue(0);         // seq_parameter_set_id
@@ -353,10 +353,10 @@ struct rg_writer {
 namespace rg {
 
 // The access unit of one picture (SPS and PPS first for an IDR) with explicit frame_num / POC
-// (pictures since the IDR) and idr_pic_id; uses the writer's configuration and scratch only, so
+// (pictures since the IDR), idr_pic_id and QP; uses the writer's configuration and scratch only, so
 // writers of the same configuration can write pictures of one stream on several threads.
 int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_t since_idr, uint32_t idr_id,
-                       std::vector<uint8_t>& au) {
+                       int qp, std::vector<uint8_t>& au) {
   int n4 = w->mb_w * w->mb_h * 16;
   w->nnz.assign(n4, 0);
   w->cnnz[0].assign(w->mb_w * w->mb_h * 4, 0);
@@ -389,7 +389,7 @@ int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_
   const std::vector<uint8_t>* rbsp;
   if (cabac) {
     std::vector<uint8_t>& bytes = s.align_ones();
-    if (rg::cabac_slice_data(w->mb_w, w->mb_h, w->qp, idr, w->profile == RG_PROFILE_HIGH, records, bytes))
+    if (rg::cabac_slice_data(w->mb_w, w->mb_h, qp, idr, w->profile == RG_PROFILE_HIGH, records, bytes))
       return wfail(RG_ERR_INVALID, "rg_writer_picture: a record no %s slice holds", idr ? "IDR" : "P");
     rbsp = &bytes;
   } else {
@@ -405,7 +405,7 @@ int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_
   au.clear();
   if (idr) {
     emit_nal(au, 3, 7, w->sps());
-    emit_nal(au, 3, 8, w->pps());
+    emit_nal(au, 3, 8, w->pps(qp));
   }
   emit_nal(au, 3, idr ? 5 : 1, *rbsp);
   return 0;
@@ -459,7 +459,7 @@ int64_t rg_writer_picture(rg_writer* w, const rg_mb_out* records, int32_t kind, 
   bool idr = kind == RG_FRAME_IDR;
   if (idr) w->since_idr = 0;
   std::vector<uint8_t> au;
-  int r = rg::writer_access_unit(w, records, idr, w->since_idr, w->idrs, au);
+  int r = rg::writer_access_unit(w, records, idr, w->since_idr, w->idrs, w->qp, au);
   if (r) return r;
   if (au.size() > cap)
     return wfail(RG_ERR_INVALID, "rg_writer_picture: access unit of %zu bytes exceeds the %zu-byte buffer", au.size(), cap);

@@ -50,10 +50,14 @@ struct StreamDev {
   uint8_t* unf_u;
   uint8_t* unf_v;
   int32_t kind;           // RG_FRAME_IDR or RG_FRAME_P
+  int32_t qp, qpc;        // the stream's QP and chroma QP
+  // SkipBounds (enc.rs:2104) of the stream's QP
+  uint32_t sb_luma, sb_luma_ssd, sb_chroma, sb_chroma_ssd, sb_probe;
   int32_t pad_;
 };
 
-// Frame-constant parameters of one wavefront (all streams share the size and QP).
+// Frame-constant parameters of one wavefront (all streams share the size; qp / qpc / sb_* are the
+// context's default QP -- the kernels read each stream's own from its StreamDev).
 struct FrameParams {
   int32_t width, height;      // display size
   int32_t mb_w, mb_h;

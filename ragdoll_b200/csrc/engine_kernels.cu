@@ -487,9 +487,8 @@ __device__ __noinline__ void quant4x4_blocks(Smem& sm, bool chroma, int nblocks,
 
 // Luma 4x4 residual of pred_y, quantised (inter) and decimated into sm.coef
 // (enc.rs:1810 quant_luma_4x4_inter). Returns cbp; lanes 0..15 report block lane's "any level".
-__device__ __noinline__ int luma4x4_inter(const FrameParams& fp, Smem& sm, uint32_t* nz_lane_out) {
+__device__ __noinline__ int luma4x4_inter(int qp, Smem& sm, uint32_t* nz_lane_out) {
   int lane = lane_id();
-  int qp = fp.qp;
   uint32_t shift, bias;
   quant4_params(qp, false, shift, bias);
   int my_nz, my_big, my_score;
@@ -546,11 +545,10 @@ __device__ __forceinline__ int zigzag8(int y, int x) {
 // column q each in the second. The decimation score of a block comes from the bitmask of its
 // nonzero zig-zag positions (run of zeros below each, weights 3 / 2 / 1 / 0 for runs of
 // 0-3 / 4-11 / 12-23 / longer, enc.rs:559 with the 8x8 table). Returns cbp; *nnz8 = count.
-__device__ __noinline__ int luma8x8_inter(const FrameParams& fp, Smem& sm, uint32_t* nnz8) {
+__device__ __noinline__ int luma8x8_inter(int qp, Smem& sm, uint32_t* nnz8) {
   int lane = lane_id();
   int b = lane >> 3, q = lane & 7;
   int bx = (b & 1) * 8, by = (b >> 1) * 8;
-  int qp = fp.qp;
   uint32_t shift = 16 + qp / 6, bias = (1u << shift) / 6u;
   // residual of row q, then the row pass and (after all rows) the column pass in place
 #pragma unroll 1
@@ -1057,7 +1055,7 @@ __device__ __noinline__ void write_info(const Ctx& c, int flags, int cbpl, int m
   inf.ref = (int8_t)ref;
   inf.flags = (uint8_t)flags;
   inf.cbp_luma = (uint8_t)cbpl;
-  inf.qp = (uint8_t)c.fp->qp;
+  inf.qp = (uint8_t)c.sd->qp;
   inf.nz16 = nz;
   inf.i4_bottom = 0;
   inf.i4_right = 0;
@@ -1076,7 +1074,7 @@ __device__ __noinline__ void write_info(const Ctx& c, int flags, int cbpl, int m
 __device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
-  int qp = fp.qp, qpc = fp.qpc;
+  int qp = c.sd->qp, qpc = c.sd->qpc;
   pred16_into(mode, sm, sm.pred_y, ht, hl, tl);
   int cmode = analyse_chroma(sm, ht, hl, ctl);
   uint32_t shift, bias;
@@ -1204,7 +1202,7 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int p = lane & 15, xl = p & 3, yl = p >> 2;
-  int qp = fp.qp;
+  int qp = c.sd->qp;
   uint32_t lambda = c_lambda[qp];
   uint32_t shift, bias;
   quant4_params(qp, true, shift, bias);
@@ -1300,7 +1298,7 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
 __device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
-  int qpc = fp.qpc;
+  int qpc = c.sd->qpc;
   int cmode = analyse_chroma(sm, ht, hl, ctl);
   uint32_t ac_any[2], ac_sc[2];
   chroma_quant(qpc, true, sm, ac_any, ac_sc);
@@ -1319,7 +1317,7 @@ __device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, 
   }
   uint16_t nzm = (uint16_t)__ballot_sync(FULL, lane < 16 && bnz);
   record_chroma(rec, sm, cbpc);
-  if (lane == 0) record_header(rec, RG_MB_I4X4, 0, cmode, cbpl | (cbpc << 4), 0, fp.qp, 0, 0, 0, 0, nzm);
+  if (lane == 0) record_header(rec, RG_MB_I4X4, 0, cmode, cbpl | (cbpc << 4), 0, c.sd->qp, 0, 0, 0, 0, nzm);
   chroma_recon(qpc, cbpc, sm);
   store_recon(c, sm.tmp_y, sm);
   if (lane == 0) write_info(c, kFlagIntra, cbpl, 0, 0, -1, nzm, sm.i4m);
@@ -1331,7 +1329,7 @@ __device__ __noinline__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
   int tl, ctl[2];
   load_edges(c, sm, true, tl, ctl);
   bool ht = c.mby > 0, hl = c.mbx > 0;
-  uint32_t lambda = c_lambda[fp.qp];
+  uint32_t lambda = c_lambda[c.sd->qp];
   uint32_t i16c;
   int i16m = analyse_i16(sm, ht, hl, tl, &i16c);
   if (i16c > 40 * lambda) {
@@ -1360,7 +1358,7 @@ __device__ __noinline__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy)
     rec->chroma_dc[lane >> 2][lane & 3] = 0;
   }
   if (lane == 0) {
-    record_header(rec, RG_MB_P_SKIP, 0, 0, 0, 0, c.fp->qp, mvx, mvy, 0, 0, 0);
+    record_header(rec, RG_MB_P_SKIP, 0, 0, 0, 0, c.sd->qp, mvx, mvy, 0, 0, 0);
     write_info(c, kFlagSkip, 0, mvx, mvy, 0, 0, nullptr);
   }
   store_recon(c, sm.pred_y, sm);
@@ -1368,12 +1366,12 @@ __device__ __noinline__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy)
 
 // Probe of the skip residual (enc.rs:2163 probe_skip_luma): no level above 1 and a total
 // decimation score below 6.
-__device__ __noinline__ bool probe_skip_luma(const FrameParams& fp, Smem& sm) {
+__device__ __noinline__ bool probe_skip_luma(int qp, Smem& sm) {
   int lane = lane_id();
   uint32_t shift, bias;
-  quant4_params(fp.qp, false, shift, bias);
+  quant4_params(qp, false, shift, bias);
   int nz, big, sc;  // levels go to sm.coef as scratch: a skipped macroblock records none
-  quant4x4_blocks(sm, false, 16, 0, fp.qp, shift, bias, sm.coef, nullptr, nz, big, sc);
+  quant4x4_blocks(sm, false, 16, 0, qp, shift, bias, sm.coef, nullptr, nz, big, sc);
   uint32_t b = wor(lane < 16 ? (uint32_t)big : 0u);
   uint32_t score = wsum(lane < 16 ? (uint32_t)sc : 0u);
   return !b && score < 6;
@@ -1464,7 +1462,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   int lane = lane_id();
   int mbx = c.mbx, mby = c.mby, mb_w = fp.mb_w;
   int x0 = mbx * 16, y0 = mby * 16;
-  int qp = fp.qp;
+  int qp = c.sd->qp;
   uint32_t lambda = c_lambda[qp];
   int cw = fp.mb_w * 16, chh = fp.mb_h * 16;
   // MvBounds (enc.rs:1105)
@@ -1494,7 +1492,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   int ps0 = mvp0, ps1 = mvp1;
   if (mbx == 0 || mby == 0 || (lref == 0 && a0 == 0 && a1 == 0) || (tref == 0 && b0 == 0 && b1 == 0)) { ps0 = 0; ps1 = 0; }
   load_source(c, sm);
-  int qpc = fp.qpc;
+  int qpc = c.sd->qpc;
   // co-located vector of the previous picture: a search candidate (enc.rs:3094)
   if (pw && !wait_seen(pw->ana_prev + mby, mbx + 1, pw->seen_ana, pw->error, pw->timeout_ns)) {
     pw->failed = true;
@@ -1533,8 +1531,8 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
     mc_luma16(sd.ref_y, fp.stride_y, x0, y0, ps0, ps1, sm);
     uint2 s = src8(sm), p = *(const uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8];
     uint32_t sad = wsum(vsad8(s, p));
-    if (sad < fp.sb_probe) {
-      bool lz = sad <= fp.sb_luma;
+    if (sad < c.sd->sb_probe) {
+      bool lz = sad <= c.sd->sb_luma;
       if (!lz) {
         uint32_t ssd = 0;
 #pragma unroll
@@ -1543,9 +1541,9 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
           int d1 = (int)((s.y >> (8 * k)) & 255) - (int)((p.y >> (8 * k)) & 255);
           ssd += d0 * d0 + d1 * d1;
         }
-        lz = wsum(ssd) <= fp.sb_luma_ssd;
+        lz = wsum(ssd) <= c.sd->sb_luma_ssd;
       }
-      if (!lz) lz = probe_skip_luma(fp, sm);
+      if (!lz) lz = probe_skip_luma(qp, sm);
       if (lz) {
         mc_chroma8(sd.ref_u, sd.ref_v, fp.stride_c, mbx, mby, ps0, ps1, sm);
         // per plane SAD / SSD bounds (lanes 0..15 U, 16..31 V, 4 samples each)
@@ -1557,8 +1555,8 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
         for (int k = 0; k < 4; k++) { int d = (int)ss[k] - (int)pp[k]; sadp += abs(d); ssdp += d * d; }
         uint32_t sad_u = wsum(plane == 0 ? sadp : 0), sad_v = wsum(plane == 1 ? sadp : 0);
         uint32_t ssd_u = wsum(plane == 0 ? ssdp : 0), ssd_v = wsum(plane == 1 ? ssdp : 0);
-        bool zu = sad_u <= fp.sb_chroma || ssd_u <= fp.sb_chroma_ssd;
-        bool zv = sad_v <= fp.sb_chroma || ssd_v <= fp.sb_chroma_ssd;
+        bool zu = sad_u <= c.sd->sb_chroma || ssd_u <= c.sd->sb_chroma_ssd;
+        bool zv = sad_v <= c.sd->sb_chroma || ssd_v <= c.sd->sb_chroma_ssd;
         bool cz = zu && zv;
         if (!cz) {
           uint32_t ac_any[2], ac_sc[2];
@@ -1640,7 +1638,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   {
     int fm0 = best0 * 4, fm1 = best1 * 4;
     uint32_t full_mvc = mvd_cost(fm0 - mvp0, lambda) + mvd_cost(fm1 - mvp1, lambda);
-    if (best_cost - full_mvc <= fp.sb_luma) {
+    if (best_cost - full_mvc <= c.sd->sb_luma) {
       mv0 = fm0; mv1 = fm1;
       uint2 v = ldg8(base + (long)best1 * stride + best0);
       *(uint2*)&sm.pred_y[(lane >> 1) * 16 + (lane & 1) * 8] = v;
@@ -1704,7 +1702,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
   // 4. P_L0_16x16 residual (enc.rs:3158-3190)
   mc_chroma8(sd.ref_u, sd.ref_v, fp.stride_c, mbx, mby, mv0, mv1, sm);
   uint32_t nz_lane;
-  int cbp4 = luma4x4_inter(fp, sm, &nz_lane);
+  int cbp4 = luma4x4_inter(qp, sm, &nz_lane);
   int cbpl = cbp4;
   bool use8 = false;
   if (fp.t8x8 && cbp4) {
@@ -1716,7 +1714,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
     }
     nnz4 = wsum(nnz4);
     uint32_t nnz8;
-    int cbp8 = luma8x8_inter(fp, sm, &nnz8);
+    int cbp8 = luma8x8_inter(qp, sm, &nnz8);
     if (nnz8 <= nnz4) { use8 = true; cbpl = cbp8; }
   }
   uint32_t ac_any[2], ac_sc[2];

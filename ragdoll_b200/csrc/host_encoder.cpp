@@ -99,6 +99,7 @@ class Pool {
 struct Wave {
   rg_mb_out* recs = nullptr;  // pinned, frames * streams * n_mb, picture-major
   int frames = 0;
+  std::vector<int> qp;        // per stream
   bool written = false;       // its access units are in rg_encoder::aus, not yet handed out
   std::vector<uint8_t> idr;
   std::vector<uint32_t> since, idr_id;
@@ -114,6 +115,7 @@ struct rg_encoder {
   std::vector<int64_t> coded;    // per stream: pictures so far
   std::vector<uint32_t> idrs;    // per stream: IDR pictures so far
   std::vector<uint32_t> since;   // per stream: pictures since its last IDR
+  std::vector<int> qp;           // per stream: fixed QP
   Wave waves[2];
   int head = 0, pending = 0;     // oldest wave in flight, waves in flight
   Pool* pool = nullptr;
@@ -162,6 +164,7 @@ rg_encoder* rg_encoder_create(const rg_config* cfg, int32_t fps_num, int32_t fps
   e->coded.assign(S, 0);
   e->idrs.assign(S, 0);
   e->since.assign(S, 0);
+  e->qp.assign(S, cfg->qp);
   if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
   e->pool = new Pool(threads);
   for (int i = 0; i < threads; i++) e->writers.push_back(rg_writer_create(cfg, fps_num, fps_den));
@@ -181,6 +184,16 @@ void rg_encoder_destroy(rg_encoder* e) {
 
 int32_t rg_encoder_threads(const rg_encoder* e) { return e ? e->pool->size() : 0; }
 
+int rg_encoder_set_stream_qp(rg_encoder* e, int32_t stream, int32_t qp) {
+  if (!e) return efail(RG_ERR_INVALID, "rg_encoder_set_stream_qp: null encoder");
+  if (stream < 0 || stream >= (int)e->coded.size()) return efail(RG_ERR_INVALID, "rg_encoder_set_stream_qp: stream %d", stream);
+  if (e->coded[stream]) return efail(RG_ERR_STATE, "rg_encoder_set_stream_qp: stream %d has pictures already", stream);
+  int r = rg_set_stream_qp(e->ctx, stream, qp);
+  if (r) return r;
+  e->qp[stream] = qp;
+  return RG_OK;
+}
+
 int64_t rg_encode_frame(rg_encoder* e, int32_t stream, const uint8_t* y, const uint8_t* u, const uint8_t* v,
                         size_t stride_y, size_t stride_uv, uint8_t* out, size_t cap) {
   if (!e || !out) return efail(RG_ERR_INVALID, "rg_encode_frame: null argument");
@@ -194,7 +207,7 @@ int64_t rg_encode_frame(rg_encoder* e, int32_t stream, const uint8_t* y, const u
   e->next_picture(stream, idr, since_idr, idr_id);
   int r = rg_analyse_frame(e->ctx, stream, y, u, v, stride_y, stride_uv, idr ? RG_FRAME_IDR : RG_FRAME_P, e->one.data());
   std::vector<uint8_t> au;
-  if (!r) r = rg::writer_access_unit(e->writers[0], e->one.data(), idr, since_idr, idr_id, au);
+  if (!r) r = rg::writer_access_unit(e->writers[0], e->one.data(), idr, since_idr, idr_id, e->qp[stream], au);
   if (r) {  // the picture was not coded: the stream's counters stay where they were
     e->coded[stream] = coded;
     e->idrs[stream] = idrs;
@@ -223,6 +236,7 @@ int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride
       }
   }
   w.frames = frames;
+  w.qp = e->qp;
   w.idr.resize((size_t)frames * S);
   w.since.resize((size_t)frames * S);
   w.idr_id.resize((size_t)frames * S);
@@ -258,7 +272,7 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
     std::atomic<int> err{0};
     e->pool->run(n, [&](int i, int worker) {
       int rc = rg::writer_access_unit(e->writers[worker], w.recs + (size_t)i * e->n_mb, w.idr[i], w.since[i],
-                                      w.idr_id[i], e->aus[i]);
+                                      w.idr_id[i], w.qp[i % S], e->aus[i]);
       if (rc) err.store(rc);
     });
     if (err.load()) return err.load();

@@ -90,6 +90,27 @@ void skip_bounds(int qp, int qpc, FrameParams& fp) {
   fp.sb_probe = 16 * (((1u << q.shift) - q.bias) / q.mf[0] + 1);
 }
 
+// The per-stream QP fields of a StreamDev at qp.
+struct StreamQp {
+  int32_t qp, qpc;
+  uint32_t sb_luma, sb_luma_ssd, sb_chroma, sb_chroma_ssd, sb_probe;
+};
+StreamQp stream_qp(int qp) {
+  FrameParams t{};
+  int qpc = tables::kChromaQp[qp];
+  skip_bounds(qp, qpc, t);
+  return {qp, qpc, t.sb_luma, t.sb_luma_ssd, t.sb_chroma, t.sb_chroma_ssd, t.sb_probe};
+}
+void apply_qp(StreamDev& d, const StreamQp& q) {
+  d.qp = q.qp;
+  d.qpc = q.qpc;
+  d.sb_luma = q.sb_luma;
+  d.sb_luma_ssd = q.sb_luma_ssd;
+  d.sb_chroma = q.sb_chroma;
+  d.sb_chroma_ssd = q.sb_chroma_ssd;
+  d.sb_probe = q.sb_probe;
+}
+
 }  // namespace
 
 namespace rg {
@@ -150,6 +171,7 @@ struct rg_ctx {
   rg_mb_out* a_out_ptr[2] = {nullptr, nullptr};  // host buffer each slot's call copies into
   int a_slot = 0;
   std::vector<int> frames;         // frames analysed per stream
+  std::vector<StreamQp> qps;       // QP of each stream (rg_set_stream_qp; default cfg.qp)
   // metrics scratch
   float* m_rows = nullptr;
   double* m_out = nullptr;
@@ -224,6 +246,7 @@ rg_ctx* rg_create(const rg_config* cfg) {
   c->pic_y = (size_t)fp.stride_y * c->rows_y;
   c->pic_c = (size_t)fp.stride_c * c->rows_c;
   c->frames.assign(c->S, 0);
+  c->qps.assign(c->S, stream_qp(cfg->qp));
   c->max_frames = cfg->max_frames > 1 ? cfg->max_frames : 1;
   if (c->max_frames > 64) {
     fail(RG_ERR_INVALID, "rg_create: max_frames %d outside 0..64", cfg->max_frames);
@@ -393,6 +416,7 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
       d.unf_y = d.unf_u = d.unf_v = nullptr;
     }
     d.kind = kinds[i];
+    apply_qp(d, c->qps[s]);
     d.pad_ = 0;
   }
   FrameParams fp = c->fp;
@@ -459,6 +483,7 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
       d.rec = rec_base + ((size_t)f * S + s) * c->n_mb;
       d.unf_y = d.unf_u = d.unf_v = nullptr;
       d.kind = kinds[f * S + s];
+      apply_qp(d, c->qps[s]);
       d.pad_ = 0;
     }
   FrameParams fp = c->fp;
@@ -718,6 +743,16 @@ int rg_analyse_batch(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, s
   if (r) return r;
   if (out) return rg_copy_records(c, out);
   return rg_sync(c);
+}
+
+int rg_set_stream_qp(rg_ctx* c, int32_t stream, int32_t qp) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_stream_qp: null context");
+  if (stream < 0 || stream >= c->S) return fail(RG_ERR_INVALID, "rg_set_stream_qp: stream %d of %d", stream, c->S);
+  if (qp < 1 || qp > 51) return fail(RG_ERR_UNSUPPORTED, "rg_set_stream_qp: qp %d outside 1..51", qp);
+  int r = resolve_pending(c, false);  // calls already queued keep the QP they were queued with
+  if (r) return r;
+  c->qps[stream] = stream_qp(qp);
+  return RG_OK;
 }
 
 int rg_analyse_frame(rg_ctx* c, int32_t stream, const uint8_t* y, const uint8_t* u, const uint8_t* v, size_t stride_y,

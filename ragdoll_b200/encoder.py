@@ -33,6 +33,12 @@ class H264Encoder:
         self._inflight: List[list] = []                     # sources of waves not yet collected
         self._out = np.zeros(0, np.uint8)
 
+    def set_stream_qp(self, stream: int, qp: int) -> None:
+        """Fixed QP of one stream, before its first picture (rg_encoder_set_stream_qp)."""
+        rc = lib().rg_encoder_set_stream_qp(self.h, stream, qp)
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+
     @property
     def threads(self) -> int:
         return lib().rg_encoder_threads(self.h)

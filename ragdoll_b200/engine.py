@@ -43,7 +43,7 @@ EXPORTS = [
     "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
     "rg_demux_info", "rg_demux_access_unit", "rg_analyse_gops_wait", "rg_encoder_create", "rg_encoder_destroy",
     "rg_encoder_threads", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_quality_frame_prev",
-    "rg_vmaf_lite_plane",
+    "rg_vmaf_lite_plane", "rg_set_stream_qp", "rg_encoder_set_stream_qp",
 ]
 
 
@@ -131,6 +131,8 @@ def lib() -> ctypes.CDLL:
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
     L.rg_analyse_gops_wait.argtypes = [P, P]
+    L.rg_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
+    L.rg_encoder_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_quality_frame_prev.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, u8p,
                                         ctypes.c_size_t, ctypes.POINTER(RgQuality)]
     L.rg_vmaf_lite_plane.argtypes = [ctypes.c_int32, u8p, ctypes.c_size_t, u8p, ctypes.c_size_t, ctypes.c_int32,
@@ -326,6 +328,10 @@ class Engine:
         v = np.zeros((ch // 2, cw // 2), np.uint8)
         _check(lib().rg_get_recon_unfiltered(self.h, stream, _u8(y), _u8(u), _u8(v)))
         return y, u, v
+
+    def set_stream_qp(self, stream: int, qp: int) -> None:
+        """Fixed QP of one stream (rg_set_stream_qp); streams of different QPs share launches."""
+        _check(lib().rg_set_stream_qp(self.h, stream, qp))
 
     def quality(self, frame, stream: int = 0, prev=None) -> dict:
         """evaluate_frame_quality of the stream's last reconstruction against its source ``frame``;

@@ -78,3 +78,26 @@ def test_out_of_order_calls_are_refused():
     orc = OracleEncoder(w, h, 28, profile=1, keyint=30)
     for i, row in enumerate(a + b):
         assert row[0] == orc.encode(clip[i])[0], f"picture {i}"
+
+
+def test_mixed_sizes_and_qps_like_the_batched_configuration():
+    """The batched-streams configuration scaled down: four picture sizes, four streams each,
+    Main profile (CABAC), a QP drawn from 20..36 per stream -- one encoder per size, each stream at
+    its own QP in the same launches; every access unit equals the oracle's."""
+    from ragdoll_b200.encoder import H264Encoder
+    rng = np.random.default_rng(64)
+    sizes, per_size, F = [(64, 48), (160, 96), (320, 180), (352, 288)], 4, 3
+    for (w, h) in sizes:
+        qps = [int(q) for q in rng.integers(20, 37, per_size)]
+        clips = [grating_clip(w, h, F, seed=w + h + s, motion=4.0, rects=2) for s in range(per_size)]
+        enc = H264Encoder(w, h, 28, profile=1, keyint=30, streams=per_size, max_frames=F, threads=4)
+        for s, q in enumerate(qps):
+            enc.set_stream_qp(s, q)
+        enc.submit([[clips[s][f] for s in range(per_size)] for f in range(F)])
+        got = enc.collect()
+        for s, q in enumerate(qps):
+            orc = OracleEncoder(w, h, q, profile=1, keyint=30)
+            for f in range(F):
+                assert got[f][s] == orc.encode(clips[s][f])[0], f"{w}x{h} stream {s} (QP {q}) picture {f}"
+        with pytest.raises(Exception):
+            enc.set_stream_qp(0, 30)              # the stream has pictures already

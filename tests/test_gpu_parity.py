@@ -181,3 +181,29 @@ def test_pipelined_many_small_streams():
         for f in range(F):
             _, ref = orc.encode(clips[s][f])
             assert first_record_mismatch(ref, recs[f, s], orc.mb_w) is None, f"stream {s} picture {f}"
+
+
+@pytest.mark.parametrize("pipelined", [False, True])
+def test_streams_of_different_qps_in_one_launch(pipelined):
+    """Four streams at QP 20 / 26 / 31 / 36 (rg_set_stream_qp) analysed together, per-diagonal
+    and in one persistent launch: each equals the oracle at its own QP."""
+    from oracle_lib import OracleEncoder
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
+    from gpu_parity_util import first_record_mismatch
+    w, h, F, qps = 160, 96, 4, [20, 26, 31, 36]
+    S = len(qps)
+    clips = [grating_clip(w, h, F, seed=600 + s, motion=5.0, rects=2) for s in range(S)]
+    eng = Engine(w, h, 28, profile=2, num_streams=S, max_frames=F if pipelined else 1)
+    for s, q in enumerate(qps):
+        eng.set_stream_qp(s, q)
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)]
+    if pipelined:
+        recs = eng.analyse_gops([[clips[s][f] for s in range(S)] for f in range(F)], kinds)
+    else:
+        recs = np.stack([eng.analyse([clips[s][f] for s in range(S)], kinds[f]) for f in range(F)])
+    for s, q in enumerate(qps):
+        orc = OracleEncoder(w, h, q, profile=2, keyint=F + 1)
+        for f in range(F):
+            _, ref = orc.encode(clips[s][f])
+            assert first_record_mismatch(ref, recs[f, s], orc.mb_w) is None, f"stream {s} (QP {q}) picture {f}"
+        assert np.array_equal(orc.recon()[0], eng.recon_coded(s)[0]), f"stream {s} reference picture"
