@@ -196,6 +196,21 @@ int rg_analyse_gops_async(rg_ctx* ctx, const uint8_t* const* planes, size_t stri
  * its copy out only, so the latest call's launch keeps running). No counterpart in the reference. */
 int rg_analyse_gops_wait(rg_ctx* ctx, const rg_mb_out* out);
 
+/*
+ * rg_analyse_gops_async without the copy of all records at the end: the launch flags each picture
+ * (index f * num_streams + s) in mapped host memory once its records are final, and
+ * rg_analyse_gops_fetch copies that picture's records into out -- while the launch still runs.
+ * rg_analyse_gops_wait(ctx, out) then waits for the launch; if one of its waits gave up, it re-runs
+ * the call and copies every record into out. Fetch every picture of a call before the call two
+ * calls later is queued. No counterpart in the reference.
+ */
+int rg_analyse_gops_stream(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                           const int32_t* kinds, int32_t frames, rg_mb_out* out);
+/* 1: the picture's records are copied into out; 0: not final yet; 2: the launch ended without
+ * finishing it (call rg_analyse_gops_wait); negative RG_ERR_*. Safe to call from several host threads
+ * at once (for different pictures) while the context's own thread is not in another call. */
+int rg_analyse_gops_fetch(rg_ctx* ctx, rg_mb_out* out, int32_t picture);
+
 /* Tuning of the pipelined mode (rg_set_pipeline_tuning); 0 in any field selects the default. */
 typedef struct rg_pipeline_tuning {
     int32_t lag;          /* macroblock-times between consecutive pictures in the work order    */

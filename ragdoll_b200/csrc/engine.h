@@ -76,7 +76,10 @@ void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, in
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st);
 int wavefront_steps(const FrameParams& fp);
 // Pipelined mode: d_streams holds frames x n_streams descriptors (picture-major); counters is
-// pipeline_counter_ints() zeroed ints; counters[1] is non-zero after a failed wait.
+// pipeline_counter_ints() zeroed ints; counters[1] is non-zero after a failed wait. ready (device
+// address of mapped host memory, or null): frames x n_streams ints, each set to seq once that
+// picture's records are final. host_err: mapped host int receiving the launch's error word (zero
+// it before the launch).
 int pipeline_grid(int device);
 int pipeline_sms(int device);
 size_t pipeline_counter_ints(const FrameParams& fp, int frames);
@@ -89,7 +92,8 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
                           int2* tasks, int qbeg[3], int qend[3]);
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
                      size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
-                     int seg, int grid, unsigned long long timeout_ns, cudaStream_t st);
+                     int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
+                     cudaStream_t st);
 void upload_tables();
 
 }  // namespace rg

@@ -1394,6 +1394,14 @@ __device__ __forceinline__ int ld_relaxed(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ int atom_add_acq_rel(int* p, int v) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void st_release_sys(int* p, int v) {
+  asm volatile("st.release.sys.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -2040,11 +2048,27 @@ struct PipeParams {
   int role_by_sm;     // 0: by block index instead (a grid too small to reach every SM)
   int seg;
   unsigned long long timeout_ns;
+  int* rows_done;     // [F][S] rows of a picture fully analysed
+  int* ready;         // [F][S] in mapped host memory (or null): seq once a picture's records are final
+  int seq;
+  int* host_err;      // mapped host memory: the error word as the launch ends (no copy to wait for)
 };
 __device__ __forceinline__ unsigned sm_id() {
   unsigned r;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
   return r;
+}
+
+// Counts a picture's fully analysed row; the warp completing its last row tells the host that the
+// picture's records are final. Each row's records were ordered before its count by the release
+// chain of the row's segments; the acq_rel count gathers all rows, and the system-scope release
+// store orders them before the flag the host polls.
+__device__ __noinline__ void picture_row_done(int* rows_done, int* ready, int seq, int H) {
+  if (lane_id() == 0) {
+    int before = atom_add_acq_rel(rows_done, 1);
+    if (before == H - 1) st_release_sys(ready, seq);
+  }
+  __syncwarp();
 }
 
 __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
@@ -2115,6 +2139,7 @@ __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const 
         }
         publish(ana_rows + y, x + 1);
       }
+      if (!failed && x1 == Wm && pp.ready) picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
     } else {
       int seen_own = 0, seen_a0 = 0, seen_a1 = 0, seen_up = 0;
       if (x0 > 0 && !wait_seen(db_rows + y, x0, seen_own, pp.error, pp.timeout_ns)) failed = true;
@@ -2138,6 +2163,10 @@ __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const 
       }
     }
     if (failed) break;
+  }
+  if (lane == 0) {
+    int e = ld_relaxed(pp.error);
+    if (e) st_release_sys(pp.host_err, e);
   }
 }
 
@@ -2284,7 +2313,8 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
                      size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
-                     int seg, int grid, unsigned long long timeout_ns, cudaStream_t st) {
+                     int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
+                     cudaStream_t st) {
   int S = fp.n_streams, H = fp.mb_h;
   PipeParams pp;
   pp.ticket = counters;
@@ -2302,12 +2332,16 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.role_by_sm = grid >= sms;
   pp.seg = seg;
   pp.timeout_ns = timeout_ns;
+  pp.rows_done = pp.db + frames * S * H;
+  pp.ready = ready;
+  pp.seq = seq;
+  pp.host_err = host_err;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;
   pipeline_kernel<<<g, 32, 0, st>>>(fp, d_streams, pp);
 }
 
 size_t pipeline_counter_ints(const FrameParams& fp, int frames) {
-  return 4 + 2 * (size_t)frames * fp.n_streams * fp.mb_h;
+  return 4 + 2 * (size_t)frames * fp.n_streams * fp.mb_h + (size_t)frames * fp.n_streams;
 }
 
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st) {

@@ -3,14 +3,16 @@
 // with the macroblock loop on the GPU. A picture is analysed, reconstructed and deblocked by the
 // engine, and its access unit is written on the host from the engine's records.
 //
-// Waves: rg_encoder_submit queues the copy in, the persistent launch and the copy out of the records
-// of `frames` pictures of every stream, and returns; rg_encoder_collect waits for the oldest wave's
-// records and writes all of its pictures at once on a pool of threads. Every picture is one slice
-// whose entropy coder starts afresh, and its frame_num / POC / idr_pic_id are known when it is
-// submitted, so the pictures of one stream are written in parallel too. With two waves in flight
-// the GPU analyses one while the host writes the other.
+// Waves: rg_encoder_submit queues the copy in and the persistent launch of `frames` pictures of every
+// stream behind the wave in flight, and returns; rg_encoder_collect writes the wave's pictures on a
+// pool of threads, each as soon as the launch flags its records final (rg_analyse_gops_stream /
+// _fetch), so the writing overlaps the launch. Every picture is one slice whose entropy coder
+// starts afresh, and its frame_num / POC / idr_pic_id are known when it is submitted, so the
+// pictures of one stream are written in parallel too. With two waves in flight the GPU goes from
+// one launch to the next while the host writes.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
@@ -249,7 +251,7 @@ int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride
       e->next_picture(s, w.idr[i], w.since[i], w.idr_id[i]);
       kinds[i] = w.idr[i] ? RG_FRAME_IDR : RG_FRAME_P;
     }
-  int r = rg_analyse_gops_async(e->ctx, planes, stride_y, stride_uv, kinds.data(), frames, w.recs);
+  int r = rg_analyse_gops_stream(e->ctx, planes, stride_y, stride_uv, kinds.data(), frames, w.recs);
   if (r) {
     e->coded = coded;
     e->idrs = idrs;
@@ -266,15 +268,34 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
   Wave& w = e->waves[e->head];
   const int S = (int)e->coded.size(), n = w.frames * S;
   if (!w.written) {
-    int r = rg_analyse_gops_wait(e->ctx, w.recs);
-    if (r) return r;
+    // Pictures are written as the launch finishes them (picture-major order is roughly the order
+    // they become final); one the launch could not finish is written after the call is re-run.
     if ((int)e->aus.size() < n) e->aus.resize(n);
+    std::vector<uint8_t> later(n, 0);
     std::atomic<int> err{0};
-    e->pool->run(n, [&](int i, int worker) {
+    auto write = [&](int i, int worker) {
       int rc = rg::writer_access_unit(e->writers[worker], w.recs + (size_t)i * e->n_mb, w.idr[i], w.since[i],
                                       w.idr_id[i], w.qp[i % S], e->aus[i]);
       if (rc) err.store(rc);
+    };
+    e->pool->run(n, [&](int i, int worker) {
+      for (int spins = 0;; spins++) {
+        int st = rg_analyse_gops_fetch(e->ctx, w.recs, i);
+        if (st == 1) break;
+        if (st != 0) {
+          later[i] = 1;
+          return;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(spins < 64 ? 20 : 200));
+      }
+      write(i, worker);
     });
+    int r = rg_analyse_gops_wait(e->ctx, w.recs);  // the launch's end; a re-run if a wait gave up
+    if (r) return r;
+    std::vector<int> rest;
+    for (int i = 0; i < n; i++)
+      if (later[i]) rest.push_back(i);
+    if (!rest.empty()) e->pool->run((int)rest.size(), [&](int k, int worker) { write(rest[k], worker); });
     if (err.load()) return err.load();
     w.written = true;
   }

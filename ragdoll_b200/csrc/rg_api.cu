@@ -138,7 +138,8 @@ struct rg_ctx {
   int max_frames = 1, nslots = 2;  // pictures per pipelined call; picture ring per stream
   int* counters = nullptr;         // pipelined-mode progress counters
   size_t n_counters = 0;
-  int* h_err = nullptr;            // pinned copy of the device error word
+  int* h_err = nullptr;            // mapped host memory: each pending launch's error word
+  int* d_err = nullptr;            // the same, as the device sees it
   int grid = 0;
   int lag = kDefaultLag;           // macroblock-times between pictures of a stream in the work order
   int seg = kDefaultSeg;           // macroblocks per work segment
@@ -153,14 +154,21 @@ struct rg_ctx {
   std::vector<int32_t> tasks_kinds;
   std::vector<int2> h_tasks;
   // the pending pipelined call, kept to re-run it on the per-diagonal path after a failed wait
-  std::vector<const uint8_t*> pend_planes;
-  std::vector<int32_t> pend_kinds;
-  std::vector<int> pend_start;
-  int pend_frames = 0;
-  size_t pend_sy = 0, pend_suv = 0;
-  rg_mb_out* pend_rec = nullptr;   // where the pending call's records go
-  rg_mb_out* pend_out = nullptr;   // host copy of them queued by an asynchronous call
-  size_t pend_out_bytes = 0;
+  // Pipelined calls queued and not yet resolved (at most two, oldest first): what a re-run needs.
+  struct Pending {
+    std::vector<const uint8_t*> planes;  // device planes, [f][s][y,u,v]
+    std::vector<int32_t> kinds;
+    std::vector<int> start;              // frames analysed per stream before the call
+    int frames = 0;
+    size_t sy = 0, suv = 0;
+    rg_mb_out* rec = nullptr;            // device records
+    rg_mb_out* out = nullptr;            // host copy queued by an asynchronous call, or null
+    size_t out_bytes = 0;
+    int* h_err = nullptr;                // mapped host: the launch's error word
+    cudaEvent_t done = nullptr;          // after the launch
+  };
+  Pending pend[2];
+  int pend_head = 0, pend_count = 0;
   // asynchronous host-buffer calls (rg_analyse_gops_async): two slots of source staging and
   // records, a copy-in and a copy-out stream; allocated on the first such call
   uint8_t* a_srcs[2] = {nullptr, nullptr};
@@ -169,6 +177,10 @@ struct rg_ctx {
   cudaEvent_t a_in_done[2] = {nullptr, nullptr}, a_kern_done[2] = {nullptr, nullptr};
   cudaEvent_t a_out_done[2] = {nullptr, nullptr};
   rg_mb_out* a_out_ptr[2] = {nullptr, nullptr};  // host buffer each slot's call copies into
+  int* h_ready[2] = {nullptr, nullptr};  // mapped host memory: per picture, the launch seq once final
+  int* d_ready[2] = {nullptr, nullptr};  // the same, as the device sees it
+  int a_seq[2] = {0, 0}, a_frames[2] = {0, 0};
+  int launch_seq = 0;
   int a_slot = 0;
   std::vector<int> frames;         // frames analysed per stream
   std::vector<StreamQp> qps;       // QP of each stream (rg_set_stream_qp; default cfg.qp)
@@ -277,7 +289,10 @@ rg_ctx* rg_create(const rg_config* cfg) {
   }
   if (cudaMallocHost((void**)&c->h_streams[0], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
       cudaMallocHost((void**)&c->h_streams[1], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
-      cudaMallocHost((void**)&c->h_err, sizeof(int)) != cudaSuccess ||
+      cudaHostAlloc((void**)&c->h_err, 2 * sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void**)&c->d_err, c->h_err, 0) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->pend[0].done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->pend[1].done, cudaEventDisableTiming) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->slot_done[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->slot_done[1], cudaEventDisableTiming) != cudaSuccess) {
@@ -285,7 +300,9 @@ rg_ctx* rg_create(const rg_config* cfg) {
     rg_destroy(c);
     return nullptr;
   }
-  *c->h_err = 0;
+  c->h_err[0] = c->h_err[1] = 0;
+  c->pend[0].h_err = c->h_err;
+  c->pend[1].h_err = c->h_err + 1;
   c->grid = pipeline_grid(cfg->device);
   c->sms = pipeline_sms(cfg->device);
   c->deblock_sms = default_deblock_sms(c->sms);
@@ -323,12 +340,15 @@ void rg_destroy(rg_ctx* c) {
   for (int i = 0; i < 2; i++) {
     cudaFree(c->a_srcs[i]);
     cudaFree(c->a_recs[i]);
+    if (c->h_ready[i]) cudaFreeHost(c->h_ready[i]);
     for (cudaEvent_t e : {c->a_in_done[i], c->a_kern_done[i], c->a_out_done[i]})
       if (e) cudaEventDestroy(e);
   }
   if (c->a_in) cudaStreamDestroy(c->a_in);
   if (c->a_out) cudaStreamDestroy(c->a_out);
   if (c->h_err) cudaFreeHost(c->h_err);
+  for (auto& p : c->pend)
+    if (p.done) cudaEventDestroy(p.done);
   if (c->h_streams[0]) cudaFreeHost(c->h_streams[0]);
   if (c->h_streams[1]) cudaFreeHost(c->h_streams[1]);
   for (auto& e : c->slot_done) if (e) cudaEventDestroy(e);
@@ -359,6 +379,7 @@ void* rg_cuda_stream(rg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                              const int32_t* kinds, rg_mb_out* rec_base, int only = -1);
 static int resolve_pending(rg_ctx* c, bool wait_out);
+static int resolve_oldest(rg_ctx* c);
 
 int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                             const int32_t* kinds) {
@@ -435,9 +456,12 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
 
 // One persistent launch for `frames` pictures of every stream; records at rec_base. The previous
 // pipelined call is resolved first (waited for, and re-run on the per-diagonal path if one of its
-// waits gave up), so a call never starts from the pictures of a failed one.
+// waits gave up), so a call never starts from the pictures of a failed one. (Queueing it behind
+// the previous launch without waiting measured slower end to end: the host's writing of the
+// previous wave then runs during that wave's own launch and slows it.) ready / seq: per-picture
+// flags in mapped host memory (rg_analyse_gops_stream), or null.
 static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                        const int32_t* kinds, int32_t frames, rg_mb_out* rec_base) {
+                        const int32_t* kinds, int32_t frames, rg_mb_out* rec_base, int* ready = nullptr, int seq = 0) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null argument");
   if (frames < 1 || frames > c->max_frames)
     return fail(RG_ERR_INVALID, "rg_analyse_gops_device: frames %d outside 1..%d (rg_config.max_frames)", frames,
@@ -510,18 +534,26 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
     c->tasks_seg = c->seg;
     c->tasks_split = split;
   }
+  // The launch writes its error word into mapped host memory itself: a device-to-host copy queued
+  // behind the launch would hold up, until the launch ends, every later device-to-host copy of the
+  // context (the copy engine takes them in order), such as a picture fetched while it runs.
+  int pslot = (c->pend_head + c->pend_count) & 1;
+  rg_ctx::Pending& p = c->pend[pslot];
+  *(volatile int*)p.h_err = 0;  // the launch that used this word before was resolved
   launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->qbeg, c->qend, c->deblock_sms,
-                  c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, c->stream);
+                  c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq, c->d_err + pslot, c->stream);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c->h_err, c->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  c->pend_planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
-  c->pend_kinds.assign(kinds, kinds + (size_t)frames * S);
-  c->pend_start = c->frames;
-  c->pend_frames = frames;
-  c->pend_sy = stride_y;
-  c->pend_suv = stride_uv;
-  c->pend_rec = rec_base;
-  c->pend_out = nullptr;
+  CK(cudaEventRecord(p.done, c->stream));
+  p.planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
+  p.kinds.assign(kinds, kinds + (size_t)frames * S);
+  p.start = c->frames;
+  p.frames = frames;
+  p.sy = stride_y;
+  p.suv = stride_uv;
+  p.rec = rec_base;
+  p.out = nullptr;
+  p.out_bytes = 0;
+  c->pend_count++;
   for (int s = 0; s < S; s++) c->frames[s] += frames;
   return RG_OK;
 }
@@ -602,32 +634,49 @@ int rg_analyse_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, si
   return rg_sync(c);
 }
 
-// Waits for the queued work of the context. If a wait of the last pipelined launch gave up (a
-// search reaching further than the picture lag allows, or another warp failing), every picture of
-// that call wrote its own ring slot and the reference it started from is untouched, so the call is
-// re-run, picture by picture, on the per-diagonal path, which has no waits; results are identical.
-// An asynchronous call's host copy of its records is then made again. wait_out: also wait for the
-// copy-out stream of asynchronous calls.
-static int resolve_pending(rg_ctx* c, bool wait_out) {
+// Resolves the oldest pending pipelined call: waits for its launch and, if a wait of it gave up
+// (a search reaching further than the picture lag allows, or another warp failing), re-runs it,
+// picture by picture, on the per-diagonal path, which has no waits: each picture wrote its own
+// ring slot and the reference it started from is untouched, so the results are identical. The
+// host copy of an asynchronous call's records is made again.
+static int resolve_oldest(rg_ctx* c) {
+  if (!c->pend_count) return RG_OK;
+  rg_ctx::Pending& p = c->pend[c->pend_head];
+  CK(cudaEventSynchronize(p.done));
+  if (*(volatile int*)p.h_err == 0) {
+    c->pend_head ^= 1;
+    c->pend_count--;
+    return RG_OK;
+  }
   CK(cudaStreamSynchronize(c->stream));
-  if (*c->h_err) {
-    *c->h_err = 0;
-    if (c->pend_frames == 0) return fail(RG_ERR_TIMEOUT, "rg_sync: a device wait gave up");
-    if (c->a_out) CK(cudaStreamSynchronize(c->a_out));  // its copy of the failed records may run
-    int S = c->S, F = c->pend_frames;
-    c->frames = c->pend_start;
-    c->pend_frames = 0;
-    for (int f = 0; f < F; f++) {
-      int r = enqueue_wavefront(c, c->pend_planes.data() + (size_t)f * S * 3, c->pend_sy, c->pend_suv,
-                                c->pend_kinds.data() + (size_t)f * S, c->pend_rec + (size_t)f * S * c->n_mb);
+  if (c->a_out) CK(cudaStreamSynchronize(c->a_out));  // its copy of the failed records may still run
+  int S = c->S;
+  c->frames = p.start;
+  for (int k = 0; k < c->pend_count; k++) {
+    rg_ctx::Pending& q = c->pend[(c->pend_head + k) & 1];
+    for (int f = 0; f < q.frames; f++) {
+      int r = enqueue_wavefront(c, q.planes.data() + (size_t)f * S * 3, q.sy, q.suv, q.kinds.data() + (size_t)f * S,
+                                q.rec + (size_t)f * S * c->n_mb);
       if (r) return r;
     }
     CK(cudaStreamSynchronize(c->stream));
-    if (c->pend_out) CK(cudaMemcpy(c->pend_out, c->pend_rec, c->pend_out_bytes, cudaMemcpyDeviceToHost));
+    if (q.out) CK(cudaMemcpy(q.out, q.rec, q.out_bytes, cudaMemcpyDeviceToHost));
+    *(volatile int*)q.h_err = 0;
   }
+  c->pend_head = 0;
+  c->pend_count = 0;
+  return RG_OK;
+}
+
+// Waits for the queued work of the context, resolving every pending pipelined call. wait_out: also
+// wait for the copy-out stream of asynchronous calls.
+static int resolve_pending(rg_ctx* c, bool wait_out) {
+  while (c->pend_count) {
+    int r = resolve_oldest(c);
+    if (r) return r;
+  }
+  CK(cudaStreamSynchronize(c->stream));
   if (wait_out && c->a_out) CK(cudaStreamSynchronize(c->a_out));
-  c->pend_frames = 0;
-  c->pend_out = nullptr;
   return RG_OK;
 }
 
@@ -636,8 +685,10 @@ int rg_sync(rg_ctx* c) {
   return resolve_pending(c, true);
 }
 
-int rg_analyse_gops_async(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
-                          const int32_t* kinds, int32_t frames, rg_mb_out* out) {
+// rg_analyse_gops_async (bulk: the records copied out after the launch) and rg_analyse_gops_stream
+// (the host fetches each picture's records once the launch flags them final).
+static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
+                      int32_t frames, rg_mb_out* out, bool bulk) {
   if (!c || !planes || !kinds || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: null argument");
   if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: frames %d", frames);
   int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
@@ -652,6 +703,11 @@ int rg_analyse_gops_async(rg_ctx* c, const uint8_t* const* planes, size_t stride
         return fail(RG_ERR_OOM, "rg_analyse_gops_async: staging of %zu + %zu bytes", nsrc, nrec);
       for (cudaEvent_t* e : {&c->a_in_done[i], &c->a_kern_done[i], &c->a_out_done[i]})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+      size_t nflags = sizeof(int) * S * c->max_frames;
+      if (cudaHostAlloc((void**)&c->h_ready[i], nflags, cudaHostAllocMapped) != cudaSuccess)
+        return fail(RG_ERR_OOM, "rg_analyse_gops_async: %zu bytes of mapped host memory", nflags);
+      memset(c->h_ready[i], 0, nflags);
+      CK(cudaHostGetDevicePointer((void**)&c->d_ready[i], c->h_ready[i], 0));
     }
     CK(cudaStreamCreateWithFlags(&c->a_out, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->a_in, cudaStreamNonBlocking));
@@ -676,29 +732,70 @@ int rg_analyse_gops_async(rg_ctx* c, const uint8_t* const* planes, size_t stride
   // the launch waits for its sources and for the copy-out of this slot's previous records
   CK(cudaStreamWaitEvent(c->stream, c->a_in_done[slot], 0));
   CK(cudaStreamWaitEvent(c->stream, c->a_out_done[slot], 0));
-  int r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot]);
+  int seq = ++c->launch_seq;
+  int r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot], bulk ? nullptr : c->d_ready[slot], seq);
   if (r) return r;
+  c->a_seq[slot] = seq;
+  c->a_frames[slot] = frames;
   CK(cudaEventRecord(c->a_kern_done[slot], c->stream));
   size_t bytes = sizeof(rg_mb_out) * c->n_mb * S * frames;
   CK(cudaStreamWaitEvent(c->a_out, c->a_kern_done[slot], 0));
-  CK(cudaMemcpyAsync(out, c->a_recs[slot], bytes, cudaMemcpyDeviceToHost, c->a_out));
+  if (bulk) CK(cudaMemcpyAsync(out, c->a_recs[slot], bytes, cudaMemcpyDeviceToHost, c->a_out));
   CK(cudaEventRecord(c->a_out_done[slot], c->a_out));
   c->a_out_ptr[slot] = out;
-  c->pend_out = out;
-  c->pend_out_bytes = bytes;
+  rg_ctx::Pending& p = c->pend[(c->pend_head + c->pend_count - 1) & 1];  // the call just queued
+  p.out = out;
+  p.out_bytes = bytes;
   return RG_OK;
+}
+
+int rg_analyse_gops_async(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                          const int32_t* kinds, int32_t frames, rg_mb_out* out) {
+  return async_gops(c, planes, stride_y, stride_uv, kinds, frames, out, true);
+}
+
+int rg_analyse_gops_stream(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                           const int32_t* kinds, int32_t frames, rg_mb_out* out) {
+  return async_gops(c, planes, stride_y, stride_uv, kinds, frames, out, false);
+}
+
+int rg_analyse_gops_fetch(rg_ctx* c, rg_mb_out* out, int32_t picture) {
+  if (!c || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_fetch: null argument");
+  int slot = c->a_out_ptr[0] == out ? 0 : (c->a_out_ptr[1] == out ? 1 : -1);
+  if (slot < 0 || !c->h_ready[slot]) return fail(RG_ERR_STATE, "rg_analyse_gops_fetch: no call in flight writes into out");
+  if (picture < 0 || picture >= c->a_frames[slot] * c->S)
+    return fail(RG_ERR_INVALID, "rg_analyse_gops_fetch: picture %d of %d", picture, c->a_frames[slot] * c->S);
+  volatile int* flag = c->h_ready[slot] + picture;
+  if (*flag != c->a_seq[slot]) {
+    // the launch flags a picture before it ends: after the end, an unflagged picture means a wait
+    // gave up, and rg_analyse_gops_wait re-runs the call
+    if (cudaEventQuery(c->a_kern_done[slot]) != cudaSuccess) return 0;
+    if (*flag != c->a_seq[slot]) return 2;
+  }
+  CK(cudaSetDevice(c->cfg.device));
+  thread_local cudaStream_t streams[16] = {};
+  int dev = c->cfg.device & 15;
+  if (!streams[dev]) CK(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+  size_t n = (size_t)c->n_mb;
+  CK(cudaMemcpyAsync(out + (size_t)picture * n, c->a_recs[slot] + (size_t)picture * n, sizeof(rg_mb_out) * n,
+                     cudaMemcpyDeviceToHost, streams[dev]));
+  CK(cudaStreamSynchronize(streams[dev]));
+  return 1;
 }
 
 int rg_analyse_gops_wait(rg_ctx* c, const rg_mb_out* out) {
   if (!c || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_wait: null argument");
-  if (c->pend_out == out) return resolve_pending(c, true);  // the latest call: wait for everything
+  // resolve the pending calls up to the one copying into out
+  int idx = -1;
+  for (int k = 0; k < c->pend_count; k++)
+    if (c->pend[(c->pend_head + k) & 1].out == out) idx = k;
+  for (int k = 0; k <= idx && c->pend_count; k++) {
+    int r = resolve_oldest(c);
+    if (r) return r;
+  }
   for (int i = 0; i < 2; i++)
-    if (c->a_in && c->a_out_ptr[i] == out) {
-      // an earlier call: resolved when the latest one was queued; only its copy out may run
-      CK(cudaEventSynchronize(c->a_out_done[i]));
-      return RG_OK;
-    }
-  return RG_OK;  // no call in flight writes into out
+    if (c->a_in && c->a_out_ptr[i] == out) CK(cudaEventSynchronize(c->a_out_done[i]));  // its copy out
+  return RG_OK;
 }
 
 int rg_copy_records(rg_ctx* c, rg_mb_out* out) {

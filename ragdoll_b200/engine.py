@@ -43,7 +43,8 @@ EXPORTS = [
     "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
     "rg_demux_info", "rg_demux_access_unit", "rg_analyse_gops_wait", "rg_encoder_create", "rg_encoder_destroy",
     "rg_encoder_threads", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_quality_frame_prev",
-    "rg_vmaf_lite_plane", "rg_set_stream_qp", "rg_encoder_set_stream_qp",
+    "rg_vmaf_lite_plane", "rg_set_stream_qp", "rg_encoder_set_stream_qp", "rg_analyse_gops_stream",
+    "rg_analyse_gops_fetch",
 ]
 
 
@@ -132,6 +133,8 @@ def lib() -> ctypes.CDLL:
                                                ctypes.c_int32, P, P]
     L.rg_analyse_gops_wait.argtypes = [P, P]
     L.rg_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
+    L.rg_analyse_gops_stream.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
+    L.rg_analyse_gops_fetch.argtypes = [P, P, ctypes.c_int32]
     L.rg_encoder_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_quality_frame_prev.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, u8p,
                                         ctypes.c_size_t, ctypes.POINTER(RgQuality)]

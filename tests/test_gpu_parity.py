@@ -207,3 +207,43 @@ def test_streams_of_different_qps_in_one_launch(pipelined):
             _, ref = orc.encode(clips[s][f])
             assert first_record_mismatch(ref, recs[f, s], orc.mb_w) is None, f"stream {s} (QP {q}) picture {f}"
         assert np.array_equal(orc.recon()[0], eng.recon_coded(s)[0]), f"stream {s} reference picture"
+
+
+@pytest.mark.parametrize("give_up", [False, True])
+def test_streamed_records_arrive_per_picture_and_match(give_up):
+    """rg_analyse_gops_stream / _fetch: every picture's records, fetched as soon as the launch flags
+    them final (while it still runs), equal those of the bulk call; fetching out of range or
+    without a call is refused. give_up: one warp and a lag of one macroblock-time make a wait run
+    out (no fault); fetch then reports the unfinished pictures (2) and rg_analyse_gops_wait re-runs
+    the call, after which every record is exact."""
+    import ctypes
+    from ragdoll_b200.engine import RECORD_DTYPE, RG_FRAME_IDR, RG_FRAME_P, Engine, lib
+    w, h, qp, S, F = 320, 180, 26, 4, 6
+    clips = [grating_clip(w, h, F, seed=700 + s, motion=6.0, rects=2) for s in range(S)]
+    pics = [[clips[s][f] for s in range(S)] for f in range(F)]
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)]
+    bulk = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F).analyse_gops(pics, kinds)
+    eng = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+    if give_up:
+        eng.set_pipeline_tuning(lag=1, grid=1, timeout_ms=300)
+    out = np.zeros((F, S, eng.n_mb), RECORD_DTYPE)
+    planes = [np.ascontiguousarray(p) for f in range(F) for s in range(S) for p in pics[f][s]]
+    ptrs = (ctypes.c_void_p * len(planes))(*[p.ctypes.data for p in planes])
+    k = (ctypes.c_int32 * (F * S))(*[kinds[f][s] for f in range(F) for s in range(S)])
+    L = lib()
+    assert L.rg_analyse_gops_fetch(eng.h, out.ctypes.data, 0) < 0          # no call yet
+    assert L.rg_analyse_gops_stream(eng.h, ptrs, w, (w + 1) // 2, k, F, out.ctypes.data) == 0
+    assert L.rg_analyse_gops_fetch(eng.h, out.ctypes.data, F * S) < 0      # out of range
+    done, unfinished = set(), set()
+    while len(done) + len(unfinished) < F * S:
+        for i in range(F * S):
+            if i not in done and i not in unfinished:
+                st = L.rg_analyse_gops_fetch(eng.h, out.ctypes.data, i)
+                assert st in (0, 1, 2), st
+                if st == 1:
+                    done.add(i)
+                elif st == 2:
+                    unfinished.add(i)
+    assert bool(unfinished) == give_up
+    assert L.rg_analyse_gops_wait(eng.h, out.ctypes.data) == 0
+    assert out.tobytes() == bulk.tobytes()
