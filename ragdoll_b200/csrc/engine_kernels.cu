@@ -2164,11 +2164,11 @@ __global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const 
     }
     if (failed) break;
   }
-  if (lane == 0) {
-    int e = ld_relaxed(pp.error);
-    if (e) st_release_sys(pp.host_err, e);
-  }
 }
+
+// The launch's error word into mapped host memory, queued after the launch (a kernel, not a copy:
+// a device-to-host copy waiting for a launch would stall later copies of the context).
+__global__ void error_to_host_kernel(const int* error, int* host_err) { st_release_sys(host_err, *error); }
 
 // Border extension (enc.rs:165 extend_borders): every padding sample takes the value of the
 // nearest picture sample. One thread per 16-byte chunk of a padded row.
@@ -2338,6 +2338,7 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.host_err = host_err;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;
   pipeline_kernel<<<g, 32, 0, st>>>(fp, d_streams, pp);
+  error_to_host_kernel<<<1, 1, 0, st>>>(pp.error, host_err);
 }
 
 size_t pipeline_counter_ints(const FrameParams& fp, int frames) {
