@@ -338,7 +338,9 @@ def run_engine(args, rank, world, local):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = bytes_per_launch / (launch_ms / 1000) / 1e9
-    launches = args.steps * launches_per_step
+    # kernels of this library per timed step: the pipelined launch and the one-thread kernel that
+    # hands its error word to the host; per-diagonal mode: the diagonal steps and the padding
+    launches = args.steps * (2 if args.mode == "pipelined" else launches_per_step)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
