@@ -926,7 +926,7 @@ __device__ __noinline__ int analyse_chroma(Smem& sm, bool ht, bool hl, const int
 // Q[i+2]) with i a function of (mode, x, y) -- e.g. diagonal down-right is avg3 at 4 + x - y,
 // horizontal-up at z = x + 2y is avg2 at 3 - z/2 (z even), avg3 at 2 - z/2 (z odd) and l3 past z = 5.
 // Returns kind (0 copy, 1 avg2, 2 avg3) << 8 | i.
-__device__ __forceinline__ int i4_tap(int m, int x, int y) {
+__host__ __device__ __forceinline__ int i4_tap(int m, int x, int y) {
   switch (m) {
     case 0: return 6 + x;
     case 1: return 4 - y;
@@ -948,6 +948,9 @@ __device__ __forceinline__ int i4_tap(int m, int x, int y) {
     }
   }
 }
+// The taps of every (mode, sample) for the nine-prediction loop: i | min(i + 1, 15) << 4 |
+// min(i + 2, 15) << 8 | kind << 12, at [16 m + 4 y + x] (filled from i4_tap by upload_tables).
+__device__ uint16_t g_i4tap[9 * 16];
 // ---------------------------------------------------------------------------------------------
 struct Ctx {
   const FrameParams* fp;
@@ -1213,6 +1216,13 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
   const MbInfo* info = c.sd->info;
   uint32_t lmodes = hl_mb ? ld_info(&info[c.mb - 1]).i4_right : 0x2222u;
   uint32_t tmodes = ht_mb ? ld_info(&info[c.mb - fp.mb_w]).i4_bottom : 0x2222u;
+  // this lane's taps for its predictions (modes lane / 16 + 2 k, sample p): the same for every block
+  uint32_t taps[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    int m = (lane >> 4) + 2 * k;
+    taps[k] = m < 9 ? __ldg(&g_i4tap[m * 16 + p]) : 0u;
+  }
   for (int b = 0; b < 16; b++) {
     int bx = blk_x(b), by = blk_y(b), px = bx * 4, py = by * 4;
     bool ht = by > 0 || ht_mb, hl = bx > 0 || hl_mb;
@@ -1248,11 +1258,15 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
     }
     __syncwarp();
     // nine predictions: half-warp h builds modes h, h + 2, ...
-    for (int m = lane >> 4; m < 9; m += 2) {
-      int tap = i4_tap(m, xl, yl), i = tap & 0xff;
-      int a0 = sm.i4q[i], a1 = sm.i4q[min(i + 1, 15)], a2 = sm.i4q[min(i + 2, 15)];
-      int v = (tap >> 8) == 0 ? a0 : ((tap >> 8) == 1 ? (a0 + a1 + 1) >> 1 : (a0 + 2 * a1 + a2 + 2) >> 2);
-      sm.i4all[m * 16 + p] = (uint8_t)v;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      int m = (lane >> 4) + 2 * k;
+      if (m < 9) {
+        uint32_t tp = taps[k], kind = tp >> 12;
+        int a0 = sm.i4q[tp & 15], a1 = sm.i4q[(tp >> 4) & 15], a2 = sm.i4q[(tp >> 8) & 15];
+        int v = kind == 0 ? a0 : (kind == 1 ? (a0 + a1 + 1) >> 1 : (a0 + 2 * a1 + a2 + 2) >> 2);
+        sm.i4all[m * 16 + p] = (uint8_t)v;
+      }
     }
     __syncwarp();
     // lanes 0..8: one mode each
@@ -2216,6 +2230,13 @@ void upload_tables() {
   cudaMemcpyToSymbol(c_alpha, kAlpha, sizeof(kAlpha));
   cudaMemcpyToSymbol(c_beta, kBeta, sizeof(kBeta));
   cudaMemcpyToSymbol(c_tc0, kTc0, sizeof(kTc0));
+  uint16_t taps[9 * 16];
+  for (int m = 0; m < 9; m++)
+    for (int q = 0; q < 16; q++) {
+      int t = i4_tap(m, q & 3, q >> 2), i = t & 0xff;
+      taps[m * 16 + q] = (uint16_t)(i | (i + 1 < 15 ? i + 1 : 15) << 4 | (i + 2 < 15 ? i + 2 : 15) << 8 | (t >> 8) << 12);
+    }
+  cudaMemcpyToSymbol(g_i4tap, taps, sizeof(taps));
 }
 
 int wavefront_steps(const FrameParams& fp) {
