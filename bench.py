@@ -19,6 +19,8 @@ e2e_analysis: the host-buffer analysis call alone (rg_analyse_gops_async, record
         bitstream), for comparison.
 --impl reference: the CPU restatement of ragdoll's encoder (the oracle) on the same workload
         sample, GOP-parallel across the host cores (parallel_gop_map semantics).
+--workload batched: the batched-streams configuration instead (64 streams of four sizes, a QP
+        per stream; aggregate frames/s and per-frame latency percentiles; see run_batched).
 
 Multi-GPU (torchrun): every rank encodes its own 120-frame clip (weak scaling, no collective on
 the data path); the timing is the max over ranks.
@@ -158,6 +160,130 @@ def oracle_gops(clip, gops: int, frames_per_gop: int, threads: int) -> float:
     return time.perf_counter() - t0
 
 
+def oracle_sample(clip, gops: int, fpg: int, cores: int) -> dict:
+    """The CPU figures beside the GPU numbers: the oracle GOP-parallel on `cores` threads over
+    `gops` GOPs x `fpg` frames, the same on one thread over one GOP, and the integer work the
+    oracle's decisions evaluate per frame (pixel differences of every SAD / SSD / SATD)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_lib import pixel_ops
+    pixel_ops(reset=True)
+    t = oracle_gops(clip, gops, fpg, cores)
+    ops = pixel_ops(reset=True)
+    t1 = oracle_gops(clip, 1, fpg, 1)
+    return {"value": round(gops * fpg / t, 3), "unit": UNIT, "cores": min(cores, gops), "kind": "port",
+            "single_thread": round(fpg / t1, 3),
+            "oracle_pixel_ops_per_frame": round(ops / (gops * fpg)),
+            "sample": f"{gops} GOPs x {fpg} frames (IDR + P) of the clip, oracle GOP-parallel; "
+                      f"single_thread: 1 GOP x {fpg} frames on one thread"}
+
+
+BATCH_SIZES = [(320, 240), (640, 360), (1280, 720), (1920, 1080)]
+BATCH_STREAMS, BATCH_FRAMES, BATCH_WAVE = 16, 30, 10
+
+
+def run_batched(args, rank, world, local):
+    """The batched-streams configuration: 64 concurrent streams, 16 each at 320x240, 640x360,
+    1280x720 and 1920x1080, 30 frames each (one GOP: IDR + 29 P) from independent seeds, Main
+    profile (CABAC), a QP drawn uniformly from 20..36 per stream, Balanced analysis. One encoder
+    per size, the four driven concurrently from host threads (each with its own persistent
+    launches on its own CUDA stream and its own writer threads), waves of 10 pictures of all its
+    streams, two waves in flight. A step is the whole encode of the 1920 pictures: host frames in
+    (pinned), access units out. Reports the aggregate frames/s and the per-frame latency
+    percentiles (a picture's latency: its wave's submit to its access unit written)."""
+    import torch
+
+    from ragdoll_b200.encoder import H264Encoder
+    from ragdoll_b200.engine import RG_PROFILE_MAIN
+    from ragdoll_b200.synth import grating_clip
+
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(4)
+    cores = os.cpu_count() or 1
+    areas = [w * h for w, h in BATCH_SIZES]
+    jobs = []
+    for k, (w, h) in enumerate(BATCH_SIZES):
+        cw, ch = (w + 1) // 2, (h + 1) // 2
+        fb = w * h + 2 * cw * ch
+        host = torch.empty((BATCH_STREAMS, BATCH_FRAMES, fb), dtype=torch.uint8).pin_memory()
+        hn = host.numpy()
+        for s in range(BATCH_STREAMS):
+            clip = grating_clip(w, h, BATCH_FRAMES, seed=4000 + 100 * k + s, motion=8.0, rects=6)
+            for f, (y, u, v) in enumerate(clip):
+                hn[s, f] = np.concatenate([y.reshape(-1), u.reshape(-1), v.reshape(-1)])
+        qps = [int(q) for q in rng.integers(20, 37, BATCH_STREAMS)]
+        threads = max(2, round(cores * areas[k] / sum(areas)))
+        enc = H264Encoder(w, h, 26, profile=RG_PROFILE_MAIN, keyint=BATCH_FRAMES, streams=BATCH_STREAMS,
+                          max_frames=BATCH_WAVE, device=local, threads=threads)
+        for s, q in enumerate(qps):
+            enc.set_stream_qp(s, q)
+        frames = [[(hn[s, f, :w * h].reshape(h, w), hn[s, f, w * h:w * h + cw * ch].reshape(ch, cw),
+                    hn[s, f, w * h + cw * ch:].reshape(ch, cw)) for s in range(BATCH_STREAMS)]
+                  for f in range(BATCH_FRAMES)]
+        jobs.append({"size": f"{w}x{h}", "enc": enc, "frames": frames, "host": host, "qps": qps,
+                     "threads": threads})
+
+    def encode_all(job, out):
+        enc, frames, lat, nbytes = job["enc"], job["frames"], [], 0
+        waves = [frames[i:i + BATCH_WAVE] for i in range(0, BATCH_FRAMES, BATCH_WAVE)]
+        t0 = time.perf_counter()
+        for i, wave in enumerate(waves):
+            enc.submit(wave)
+            if i:
+                nbytes += sum(len(au) for row in enc.collect() for au in row)
+                lat.append(enc.latencies().reshape(-1))
+        nbytes += sum(len(au) for row in enc.collect() for au in row)
+        lat.append(enc.latencies().reshape(-1))
+        out[job["size"]] = (time.perf_counter() - t0, np.concatenate(lat), nbytes)
+
+    def step():
+        out = {}
+        ts = [threading.Thread(target=encode_all, args=(j, out)) for j in jobs]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0, out
+
+    for _ in range(max(args.warmup, 1)):      # every stream continues with a new GOP each step
+        step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    walls, lats, per = [], [], {}
+    for _ in range(args.steps):
+        wall, out = step()
+        walls.append(wall)
+        lats.append(np.concatenate([out[j["size"]][1] for j in jobs]))
+        for j in jobs:
+            t, _, nb = out[j["size"]]
+            per.setdefault(j["size"], []).append((t, nb))
+    clk = clocks.stop()
+    pictures = len(BATCH_SIZES) * BATCH_STREAMS * BATCH_FRAMES
+    wall = statistics.median(walls)
+    lat = np.concatenate(lats)
+    line = {
+        "metric": "batched streams: aggregate encode frames/s (64 streams of mixed size, one GPU)",
+        "value": round(pictures / wall, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1),
+        "ms_per_step": round(1000 * wall, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/int32", "data": "synthetic (seeded gratings, +-8 px global motion, 6 moving rectangles, independent seed per stream)",
+        "config": {"workload": "batched streams: 16 x 320x240, 16 x 640x360, 16 x 1280x720, 16 x 1920x1080, "
+                               "30 frames each (one GOP), Main CABAC, QP U[20,36] per stream, Balanced",
+                   "encoders": "one per size, driven concurrently; waves of 10 pictures x 16 streams, two in flight",
+                   "host_threads": {j["size"]: j["threads"] for j in jobs}},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2), "p99": round(float(np.percentile(lat, 99)), 2),
+                       "max": round(float(lat.max()), 2), "definition": "a wave's submit to the picture's access unit written"},
+        "per_size": {k: {"frames_per_s": round(BATCH_STREAMS * BATCH_FRAMES / statistics.median(t for t, _ in v), 1),
+                         "bitstream_bytes": int(statistics.median(nb for _, nb in v))} for k, v in per.items()},
+        "clocks": clk,
+        "gpu_launches": args.steps * len(jobs) * (BATCH_FRAMES // BATCH_WAVE) * 2,
+    }
+    print(json.dumps(line), flush=True)
+    for j in jobs:
+        j["enc"].close()
+
+
 def run_reference(args, rank, world):
     """CPU arm: the oracle (C++ restatement of ragdoll's Balanced encoder) on the host cores."""
     if rank != 0:
@@ -170,13 +296,17 @@ def run_reference(args, rank, world):
     times = [oracle_gops(clip, gops, fpg, cores) for _ in range(args.steps)]
     t = statistics.median(times)
     value = gops * fpg / t
+    sample = oracle_sample(clip, gops, fpg, cores)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
         "config": bench_config(world),
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": min(cores, gops), "kind": "port",
-                         "sample": f"{gops} GOPs x {fpg} frames of the 1080p clip, GOP-parallel"},
+                         "single_thread": sample["single_thread"],
+                         "oracle_pixel_ops_per_frame": sample["oracle_pixel_ops_per_frame"],
+                         "sample": f"{gops} GOPs x {fpg} frames of the 1080p clip, GOP-parallel; "
+                                   f"single_thread: 1 GOP x {fpg} frames on one thread"},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -344,11 +474,7 @@ def run_engine(args, rank, world, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cores = os.cpu_count() or 1
-        fpg = 2
-        t = oracle_gops(clip, gops, fpg, cores)
-        cpu = {"value": round(gops * fpg / t, 3), "unit": UNIT, "cores": min(cores, gops), "kind": "port",
-               "sample": f"{gops} GOPs x {fpg} frames (IDR + P) of the same clip, oracle GOP-parallel"}
+        cpu = oracle_sample(clip, gops, 2, os.cpu_count() or 1)
 
     if rank == 0:
         line = {
@@ -454,6 +580,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched"],
+                    help="the 1080p 8-GOP workload, or the batched-streams configuration (64 mixed-size streams)")
     ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],
                     help="one persistent launch for all 15 pictures of the 8 GOPs, or one launch per anti-diagonal")
     ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
@@ -478,6 +606,9 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batched":
+        run_batched(args, rank, world, local)
         return
     run_engine(args, rank, world, local)
 

@@ -385,6 +385,13 @@ int rg_encoder_submit(rg_encoder* enc, const uint8_t* const* planes, size_t stri
  * the sizes and the total are returned and the wave stays to be collected.
  */
 int64_t rg_encoder_collect(rg_encoder* enc, uint8_t* out, size_t cap, int64_t* sizes);
+/*
+ * Per-picture latency of the wave collected last, [f * num_streams + s]: milliseconds from its
+ * rg_encoder_submit to its access unit being written (up to n values into ms); returns the
+ * wave's picture count (0 before the first collect). Telemetry of this library; no counterpart
+ * in the reference.
+ */
+int32_t rg_encoder_latencies(const rg_encoder* enc, double* ms, int32_t n);
 
 /* ---- Containers (host) ------------------------------------------------------------------ */
 /*

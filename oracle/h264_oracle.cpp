@@ -9,6 +9,7 @@
 //
 // Each function cites the reference code it restates (paths inside oddurs/ragdoll).
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -96,14 +97,24 @@ static uint32_t decimate_score(const int16_t* s, int n) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Integer work actually evaluated by the decisions: pixel differences of every SAD, SSD and SATD
+// (a SATD of n samples counts n; the three-way I16 SATD counts 3 x 256). Counted per encoding
+// thread and added to the process total after each frame (a measurement, not part of the
+// algorithm).
+static thread_local uint64_t t_pixel_ops = 0;
+static std::atomic<uint64_t> g_pixel_ops{0};
+
+// ---------------------------------------------------------------------------------------------
 // Pixel kernels (crates/ragdoll-simd, the _scalar functions)
 static uint32_t sad(const uint8_t* a, int sa, const uint8_t* b, int sb, int w, int h) {
+  t_pixel_ops += (uint64_t)w * h;
   uint32_t s = 0;
   for (int y = 0; y < h; y++)
     for (int x = 0; x < w; x++) s += (uint32_t)iabs((int)a[y * sa + x] - (int)b[y * sb + x]);
   return s;
 }
 static uint32_t ssd(const uint8_t* a, int sa, const uint8_t* b, int sb, int n) {
+  t_pixel_ops += (uint64_t)n * n;
   uint32_t s = 0;
   for (int y = 0; y < n; y++)
     for (int x = 0; x < n; x++) {
@@ -249,6 +260,7 @@ static void idct8_add(uint8_t* dst, int stride, const int32_t* d) {
 }
 // metrics.rs:705 satd_4x4_u8_scalar (halved)
 static uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
+  t_pixel_ops += 16;
   int t[4][4];
   for (int y = 0; y < 4; y++) {
     int d0 = a[y * sa] - b[y * sb], d1 = a[y * sa + 1] - b[y * sb + 1];
@@ -265,6 +277,7 @@ static uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
 }
 // h264_enc.rs:167 pixel_satd_16x16_scalar (sum of 4x4 transforms, halved once)
 static uint32_t satd16(const uint8_t* a, int sa, const uint8_t* b, int sb) {
+  t_pixel_ops += 256;
   uint32_t sum = 0;
   for (int by = 0; by < 4; by++)
     for (int bx = 0; bx < 4; bx++) {
@@ -481,6 +494,7 @@ static void hadamard_edge(const uint8_t* x, int* o) {
 }
 // h264_enc.rs:628 intra_satd_x3_16x16_scalar -> [v, h, dc]
 static void intra_satd_x3_16(const uint8_t* src, const uint8_t* top, const uint8_t* left, int dc, uint32_t out[3]) {
+  t_pixel_ops += 3 * 256;
   int tv[4][4], th[4][4];
   for (int b = 0; b < 4; b++) { hadamard_edge(top + b * 4, tv[b]); hadamard_edge(left + b * 4, th[b]); }
   uint32_t s[3] = {0, 0, 0};
@@ -2299,6 +2313,8 @@ long oracle_enc_frame(void* h, const uint8_t* y, const uint8_t* u, const uint8_t
                       rg_mb_out* recs, uint8_t* bits, long cap, int* is_idr) {
   auto* e = (oracle::Encoder*)h;
   std::vector<uint8_t> out = e->encode(y, u, v, sy, suv);
+  oracle::g_pixel_ops.fetch_add(oracle::t_pixel_ops, std::memory_order_relaxed);
+  oracle::t_pixel_ops = 0;
   if (is_idr) *is_idr = e->is_idr ? 1 : 0;
   if (recs) memcpy(recs, e->recs.data(), e->recs.size() * sizeof(rg_mb_out));
   if ((long)out.size() > cap) return -(long)out.size();
@@ -2325,5 +2341,10 @@ void oracle_mb_dims(void* h, int* mb_w, int* mb_h) {
   *mb_w = e->mb_w; *mb_h = e->mb_h;
 }
 int oracle_record_size(void) { return (int)sizeof(rg_mb_out); }
+// Pixel differences evaluated by the SAD / SSD / SATD of every frame encoded so far in this
+// process (all threads); reset = 1 also sets the total back to 0.
+unsigned long long oracle_pixel_ops(int reset) {
+  return reset ? oracle::g_pixel_ops.exchange(0) : oracle::g_pixel_ops.load();
+}
 
 }  // extern "C"

@@ -105,6 +105,8 @@ struct Wave {
   bool written = false;       // its access units are in rg_encoder::aus, not yet handed out
   std::vector<uint8_t> idr;
   std::vector<uint32_t> since, idr_id;
+  std::chrono::steady_clock::time_point submitted;
+  std::vector<double> latency_ms;  // per picture: submit -> access unit written
 };
 
 }  // namespace
@@ -124,6 +126,7 @@ struct rg_encoder {
   std::vector<rg_writer*> writers;               // one per pool thread
   std::vector<std::vector<uint8_t>> aus;         // access units of the wave being written
   std::vector<rg_mb_out> one;                    // records of rg_encode_frame
+  std::vector<double> last_latency_ms;           // of the wave collected last
 
   // Counters of the next picture of stream s, then advances them.
   void next_picture(int s, uint8_t& idr, uint32_t& since_idr, uint32_t& idr_id) {
@@ -237,6 +240,7 @@ int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride
         return efail(RG_ERR_OOM, "rg_encoder_submit: %zu bytes of pinned host memory", bytes);
       }
   }
+  w.submitted = std::chrono::steady_clock::now();
   w.frames = frames;
   w.qp = e->qp;
   w.idr.resize((size_t)frames * S);
@@ -271,12 +275,15 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
     // Pictures are written as the launch finishes them (picture-major order is roughly the order
     // they become final); one the launch could not finish is written after the call is re-run.
     if ((int)e->aus.size() < n) e->aus.resize(n);
+    w.latency_ms.assign(n, 0.0);
     std::vector<uint8_t> later(n, 0);
     std::atomic<int> err{0};
     auto write = [&](int i, int worker) {
       int rc = rg::writer_access_unit(e->writers[worker], w.recs + (size_t)i * e->n_mb, w.idr[i], w.since[i],
                                       w.idr_id[i], w.qp[i % S], e->aus[i]);
       if (rc) err.store(rc);
+      w.latency_ms[i] =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w.submitted).count();
     };
     e->pool->run(n, [&](int i, int worker) {
       for (int spins = 0;; spins++) {
@@ -312,9 +319,18 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
     at += e->aus[i].size();
   }
   w.written = false;
+  e->last_latency_ms = w.latency_ms;
   e->head ^= 1;
   e->pending--;
   return (int64_t)total;
+}
+
+int32_t rg_encoder_latencies(const rg_encoder* e, double* ms, int32_t n) {
+  if (!e) return efail(RG_ERR_INVALID, "rg_encoder_latencies: null encoder");
+  int32_t k = (int32_t)e->last_latency_ms.size();
+  if (ms)
+    for (int32_t i = 0; i < std::min(n, k); i++) ms[i] = e->last_latency_ms[i];
+  return k;
 }
 
 }  // extern "C"

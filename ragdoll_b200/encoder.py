@@ -93,6 +93,16 @@ class H264Encoder:
             out.append(row)
         return out
 
+    def latencies(self) -> np.ndarray:
+        """Milliseconds from submit to access unit written, per picture ([f][s]) of the wave
+        collected last (rg_encoder_latencies)."""
+        n = lib().rg_encoder_latencies(self.h, None, 0)
+        if n < 0:
+            raise RgError(n, lib().rg_last_error().decode())
+        out = np.zeros(n, np.float64)
+        lib().rg_encoder_latencies(self.h, out.ctypes.data, n)
+        return out.reshape(-1, self.streams) if n else out
+
     def close(self) -> None:
         if getattr(self, "h", None):
             lib().rg_encoder_destroy(self.h)

@@ -60,6 +60,8 @@ def lib():
         L.oracle_enc_recon.argtypes = [ctypes.c_void_p, u8p, u8p, u8p, ctypes.c_int]
         L.oracle_mb_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.oracle_record_size.restype = ctypes.c_int
+        L.oracle_pixel_ops.restype = ctypes.c_ulonglong
+        L.oracle_pixel_ops.argtypes = [ctypes.c_int]
         for fn in ("oracle_ssim_plane", "oracle_ms_ssim_plane", "oracle_psnr_plane"):
             f = getattr(L, fn)
             f.restype = ctypes.c_double
@@ -114,6 +116,12 @@ class OracleEncoder:
         v = np.zeros((ch // 2, cw // 2), np.uint8)
         lib().oracle_enc_recon(self.h, _p(y), _p(u), _p(v), 1 if filtered else 0)
         return y, u, v
+
+
+def pixel_ops(reset=False) -> int:
+    """Pixel differences evaluated by the oracle's SAD / SSD / SATD over the frames encoded so far
+    (all threads of the process); reset=True also zeroes the count."""
+    return int(lib().oracle_pixel_ops(1 if reset else 0))
 
 
 def ssim_plane(a, b):

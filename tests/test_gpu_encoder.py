@@ -4,7 +4,8 @@
   (CAVLC Baseline and CABAC High).
 * submit / collect with two waves in flight (the GPU analyses one wave while the host writes the
   other): every access unit of every stream equals the oracle's, and one stream, muxed to MP4 and
-  demuxed, decodes through FFmpeg to exactly the oracle's reconstruction.
+  demuxed, decodes through FFmpeg to exactly the oracle's reconstruction; every picture's
+  submit-to-written latency is reported and bounded by the wall time since its submit.
 * Calls out of order are refused without disturbing the streams.
 """
 import numpy as np
@@ -36,11 +37,16 @@ def test_waves_in_flight_match_oracle_and_decode():
     w, h, qp, S, F, waves, keyint = 320, 180, 26, 3, 5, 3, 8
     clips = [grating_clip(w, h, F * waves, seed=90 + s, motion=8.0, rects=3) for s in range(S)]
     enc = H264Encoder(w, h, qp, profile=2, keyint=keyint, streams=S, max_frames=F, threads=4)
-    got = []
+    got, t_sub = [], []
+    import time
     for k in range(waves):
+        t_sub.append(time.perf_counter())
         enc.submit([[clips[s][k * F + f] for s in range(S)] for f in range(F)])
         if k >= 1:
             got += enc.collect()
+            lat = enc.latencies()   # of wave k - 1: submit -> access unit written, per picture
+            assert lat.shape == (F, S) and (lat > 0).all()
+            assert lat.max() <= 1000 * (time.perf_counter() - t_sub[k - 1]) + 1
     got += enc.collect()
     assert len(got) == F * waves
     for s in range(S):

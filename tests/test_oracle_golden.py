@@ -114,3 +114,24 @@ def test_oracle_matches_cli_transcode_and_metrics_snapshots():
     reps = [quality_report(a, b, r1[i - 1] if i else None) for i, (a, b) in enumerate(zip(r1, r2))]
     for key, digits in (("psnr_avg", 2), ("psnr_yuv_611", 2), ("ssim_db", 2), ("vmaf_lite", 2)):
         assert round(sum(r[key] for r in reps) / n, digits) == m[key], key
+
+
+def test_pixel_op_counter():
+    """The oracle's count of integer work (pixel differences of every SAD / SSD / SATD its
+    decisions evaluate -- the denominator of the kernel's integer-pipe figures) is deterministic
+    and covers at least the three-way 16x16 SATD of every intra macroblock."""
+    from oracle_lib import pixel_ops
+    w, h = 96, 64
+    frames = [synth_video_frame(w, h, i) for i in range(3)]
+    counts = []
+    for _ in range(2):
+        enc = OracleEncoder(w, h, 26, profile=2, keyint=30)
+        pixel_ops(reset=True)
+        per = []
+        for f in frames:
+            enc.encode(f)
+            per.append(pixel_ops(reset=True))
+        counts.append(per)
+    assert counts[0] == counts[1]
+    assert counts[0][0] >= (w // 16) * (h // 16) * 3 * 256
+    assert all(c > 0 for c in counts[0])
