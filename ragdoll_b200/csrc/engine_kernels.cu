@@ -195,21 +195,6 @@ __device__ __forceinline__ void idct8_1d(const int* d, int* o) {
   o[0] = (int)(b0 + b7); o[1] = (int)(b2 + b5); o[2] = (int)(b4 + b3); o[3] = (int)(b6 + b1);
   o[4] = (int)(b6 - b1); o[5] = (int)(b4 - b3); o[6] = (int)(b2 - b5); o[7] = (int)(b0 - b7);
 }
-// Decimation score of n zig-zag levels (enc.rs:559 decimate_score).
-__device__ __forceinline__ uint32_t decimate_score(const int16_t* s, int n, const uint8_t* table) {
-  int idx = n;
-  while (idx > 0 && s[idx - 1] == 0) idx--;
-  uint32_t score = 0;
-  while (idx > 0) {
-    idx--;
-    int v = s[idx];
-    if (v > 1 || v < -1) return 9;
-    int run = 0;
-    while (idx > 0 && s[idx - 1] == 0) { idx--; run++; }
-    score += table[run];
-  }
-  return score;
-}
 // SATD of a 4x4 block (metrics.rs:705, halved).
 __device__ __noinline__ uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
   int t[4][4];
@@ -1075,7 +1060,6 @@ __device__ __noinline__ void write_info(const Ctx& c, int flags, int cbpl, int m
 
 // I16x16 coding and reconstruction (enc.rs:3587 code_i16) with prediction mode `mode`.
 __device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
-  const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int qp = c.sd->qp, qpc = c.sd->qpc;
   pred16_into(mode, sm, sm.pred_y, ht, hl, tl);
@@ -1310,7 +1294,6 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
 }
 
 __device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
-  const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int qpc = c.sd->qpc;
   int cmode = analyse_chroma(sm, ht, hl, ctl);
@@ -1339,7 +1322,6 @@ __device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, 
 
 // One macroblock of an I slice (enc.rs:3311 code_intra).
 __device__ __noinline__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
-  const FrameParams& fp = *c.fp;
   int tl, ctl[2];
   load_edges(c, sm, true, tl, ctl);
   bool ht = c.mby > 0, hl = c.mbx > 0;
