@@ -71,7 +71,6 @@ struct __align__(16) Smem {
   uint8_t cleft[2][8];
   uint8_t i4m[16];          // Intra4x4PredMode of this macroblock (decoding order)
   uint8_t i4q[16];          // edge samples of the current 4x4 block (i4_edge_index)
-  uint8_t i4all[9 * 16];    // its nine predictions, mode-major, raster
   int32_t red[32];
 };
 static_assert(offsetof(Smem, coef) % 4 == 0 && offsetof(Smem, ccoef) % 4 == 0, "level arrays cleared by words");
@@ -86,7 +85,6 @@ __device__ __forceinline__ MbInfo ld_info(const MbInfo* p) {
   return m;
 }
 __device__ __forceinline__ uint32_t wsum(uint32_t v) { return __reduce_add_sync(FULL, v); }
-__device__ __forceinline__ uint32_t wmin(uint32_t v) { return __reduce_min_sync(FULL, v); }
 __device__ __forceinline__ uint32_t wor(uint32_t v) { return __reduce_or_sync(FULL, v); }
 __device__ __forceinline__ int clip255(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
 __device__ __forceinline__ int16_t clamp_i16(int v) { return (int16_t)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v)); }
@@ -1241,37 +1239,47 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
       pm = min(ml, mt);
     }
     __syncwarp();
-    // nine predictions: half-warp h builds modes h, h + 2, ...
+    // nine predictions and their SATDs: half-warp h takes modes h, h + 2, ... (k = 0..4), lane p
+    // sample p; the 4x4 Hadamard of the difference (metrics.rs:705) by four shuffle butterflies,
+    // both halves' sums of magnitudes in one reduction (each below 2^16). Every lane ends with
+    // the same key, the least cost first and the lower mode on a tie.
+    int srcp = sm.src_y[(py + yl) * 16 + px + xl];
+    int pv[5];
+    uint32_t key = UMAX;
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-      int m = (lane >> 4) + 2 * k;
-      if (m < 9) {
-        uint32_t tp = taps[k], kind = tp >> 12;
-        int a0 = sm.i4q[tp & 15], a1 = sm.i4q[(tp >> 4) & 15], a2 = sm.i4q[(tp >> 8) & 15];
-        int v = kind == 0 ? a0 : (kind == 1 ? (a0 + a1 + 1) >> 1 : (a0 + 2 * a1 + a2 + 2) >> 2);
-        sm.i4all[m * 16 + p] = (uint8_t)v;
+      uint32_t tp = taps[k], kind = tp >> 12;
+      int a0 = sm.i4q[tp & 15], a1 = sm.i4q[(tp >> 4) & 15], a2 = sm.i4q[(tp >> 8) & 15];
+      int v = kind == 0 ? a0 : (kind == 1 ? (a0 + a1 + 1) >> 1 : (a0 + 2 * a1 + a2 + 2) >> 2);
+      pv[k] = v;
+      int d = srcp - v;
+#pragma unroll
+      for (int b = 1; b < 16; b <<= 1) {
+        int o = __shfl_xor_sync(FULL, d, b);
+        d = (lane & b) ? o - d : d + o;
+      }
+      uint32_t sums = __reduce_add_sync(FULL, (uint32_t)(d < 0 ? -d : d) << (16 * (lane >> 4)));
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        int m = 2 * k + h;
+        if (m > 8) continue;
+        bool av = (m == 0 || m == 3 || m == 7) ? ht : ((m == 1 || m == 8) ? hl : (m == 2 ? true : (ht && hl)));
+        uint32_t cost = (((sums >> (16 * h)) & 0xffffu) >> 1) + lambda * (m == pm ? 1u : 4u);
+        if (av) key = min(key, (cost << 4) | (uint32_t)m);
       }
     }
-    __syncwarp();
-    // lanes 0..8: one mode each
-    uint32_t key = UMAX;
-    if (lane < 9) {
-      int m = lane;
-      bool av = (m == 0 || m == 3 || m == 7) ? ht : ((m == 1 || m == 8) ? hl : (m == 2 ? true : (ht && hl)));
-      if (av) {
-        uint32_t s = satd4(&sm.src_y[py * 16 + px], 16, &sm.i4all[m * 16], 4) >> 1;
-        uint32_t cost = s + lambda * (m == pm ? 1u : 4u);
-        key = (cost << 4) | (uint32_t)m;
-      }
-    }
-    key = wmin(key);
     int bm = (int)(key & 15);
     total += key >> 4;
     if (total >= budget) return false;
     if (lane == 0) sm.i4m[b] = (uint8_t)bm;
-    // residual transform and quantisation, lane p -> coefficient p (raster)
-    int pred = sm.i4all[bm * 16 + p];
-    int acc = fwd4_pass(fwd4_pass((int)sm.src_y[(py + yl) * 16 + px + xl] - pred, 1, xl), 4, yl);
+    // residual transform and quantisation, lane p -> coefficient p (raster); the chosen mode's
+    // sample p is in lane 16 (bm & 1) + p
+    int kb = bm >> 1, mine = pv[0];
+#pragma unroll
+    for (int k = 1; k < 5; k++)
+      if (kb == k) mine = pv[k];
+    int pred = __shfl_sync(FULL, mine, (bm & 1) * 16 + p);
+    int acc = fwd4_pass(fwd4_pass(srcp - pred, 1, xl), 4, yl);
     acc = (int16_t)acc;
     uint32_t aa = (uint32_t)(acc < 0 ? -acc : acc);
     int l = (int)((aa * mf + bias) >> shift);
