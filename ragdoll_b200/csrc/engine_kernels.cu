@@ -732,31 +732,29 @@ __device__ __noinline__ void recon_luma4x4(Smem& sm, int qp, int cbp) {
 
 // ---------------------------------------------------------------------------------------------
 // Intra prediction (h264.rs:1715 predict_intra_16x16_scalar, :1967 chroma; enc.rs:1561,1586)
-__device__ __forceinline__ int pred16_sample(int mode, const Smem& sm, bool ht, bool hl, int tl, int dc,
-                                             int pa, int pb, int pc, int x, int y) {
-  switch (mode) {
-    case 0: return ht ? sm.top[x] : 128;
-    case 1: return hl ? sm.left[y] : 128;
-    case 2: return dc;
-    default: return clip255((pa + pb * (x - 7) + pc * (y - 7) + 16) >> 5);
-  }
-}
+// Plane-mode parameters; called by the whole warp: lanes 0..7 take the terms of H
+// ((q + 1) (top[8 + q] - top[6 - q])), lanes 8..15 those of V down the left column.
 __device__ void plane16_params(const Smem& sm, bool ht, bool hl, int tl, int& pa, int& pb, int& pc) {
-  int H = 0, V = 0;
-  for (int q = 0; q < 8; q++) {
-    int t8 = ht ? sm.top[8 + q] : 128, l8 = hl ? sm.left[8 + q] : 128;
-    int pt = q == 7 ? tl : (ht ? sm.top[6 - q] : 128), pl = q == 7 ? tl : (hl ? sm.left[6 - q] : 128);
-    H += (q + 1) * (t8 - pt);
-    V += (q + 1) * (l8 - pl);
+  int lane = lane_id(), q = lane & 7;
+  int term = 0;
+  if (lane < 16) {
+    bool top = lane < 8, av = top ? ht : hl;
+    const uint8_t* e = top ? sm.top : sm.left;
+    int e8 = av ? e[8 + q] : 128, ep = q == 7 ? tl : (av ? e[6 - q] : 128);
+    term = (q + 1) * (e8 - ep);
   }
+  int H = (int)wsum(lane < 8 ? (uint32_t)term : 0u), V = (int)wsum(lane >= 8 ? (uint32_t)term : 0u);
   int t15 = ht ? sm.top[15] : 128, l15 = hl ? sm.left[15] : 128;
   pa = 16 * (t15 + l15);
   pb = (5 * H + 32) >> 6;
   pc = (5 * V + 32) >> 6;
 }
+// DC of the 16x16 prediction; called by the whole warp: lane q < 16 adds top[q], lane 16 + q
+// left[q] (both sums below 2^16, one reduction).
 __device__ __forceinline__ int dc16(const Smem& sm, bool ht, bool hl) {
-  uint32_t st = 0, sl = 0;
-  for (int q = 0; q < 16; q++) { st += ht ? sm.top[q] : 0; sl += hl ? sm.left[q] : 0; }
+  int lane = lane_id();
+  uint32_t v = lane < 16 ? (ht ? (uint32_t)sm.top[lane] : 0u) : (hl ? (uint32_t)sm.left[lane - 16] << 16 : 0u);
+  uint32_t both = wsum(v), st = both & 0xffffu, sl = both >> 16;
   if (ht && hl) return (int)((st + sl + 16) >> 5);
   if (ht) return (int)((st + 8) >> 4);
   if (hl) return (int)((sl + 8) >> 4);
@@ -769,8 +767,11 @@ __device__ __noinline__ void pred16_into(int mode, Smem& sm, uint8_t* dst, bool 
   if (mode == 3) {
     int pa, pb, pc;
     plane16_params(sm, ht, hl, tl, pa, pb, pc);
-#pragma unroll 1
-    for (int k = 0; k < 8; k++) o[k] = (uint8_t)pred16_sample(3, sm, ht, hl, tl, 0, pa, pb, pc, x0 + k, y);
+    uint32_t w[2] = {0u, 0u};
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      w[k >> 2] |= (uint32_t)clip255((pa + pb * (x0 + k - 7) + pc * (y - 7) + 16) >> 5) << (8 * (k & 3));
+    *(uint2*)o = make_uint2(w[0], w[1]);
   } else {
     uint2 v;
     if (mode == 0) {
@@ -850,11 +851,18 @@ __device__ __forceinline__ int predc_sample(int mode, const Smem& sm, int p, boo
     default: return clip255((pa + pb * (x - 3) + pc * (y - 3) + 16) >> 5);
   }
 }
+// DC and plane parameters of plane p's chroma prediction; called by the whole warp with p =
+// lane / 16. In each half-warp lanes 0..7 hold top[0..7], lanes 8..15 left[0..7] (DC sums of four
+// by two butterflies), then lanes 0..3 the terms of H, lanes 4..7 those of V.
 __device__ void chroma_pred_params(const Smem& sm, int p, bool ht, bool hl, int tl, int* dcv, int& pa, int& pb, int& pc) {
   const uint8_t* t = sm.ctop[p];
   const uint8_t* l = sm.cleft[p];
-  int st0 = ht ? t[0] + t[1] + t[2] + t[3] : 0, st1 = ht ? t[4] + t[5] + t[6] + t[7] : 0;
-  int sl0 = hl ? l[0] + l[1] + l[2] + l[3] : 0, sl1 = hl ? l[4] + l[5] + l[6] + l[7] : 0;
+  int lane = lane_id(), j = lane & 15, base = lane & 16;
+  int e = j < 8 ? (ht ? t[j] : 0) : (hl ? l[j - 8] : 0);
+  e += __shfl_xor_sync(FULL, e, 1);
+  e += __shfl_xor_sync(FULL, e, 2);
+  int st0 = __shfl_sync(FULL, e, base), st1 = __shfl_sync(FULL, e, base + 4);
+  int sl0 = __shfl_sync(FULL, e, base + 8), sl1 = __shfl_sync(FULL, e, base + 12);
   if (ht && hl) {
     dcv[0] = (st0 + sl0 + 4) >> 3; dcv[1] = (st1 + 2) >> 2; dcv[2] = (sl1 + 2) >> 2; dcv[3] = (st1 + sl1 + 4) >> 3;
   } else if (ht) {
@@ -864,13 +872,14 @@ __device__ void chroma_pred_params(const Smem& sm, int p, bool ht, bool hl, int 
   } else {
     dcv[0] = dcv[1] = dcv[2] = dcv[3] = 128;
   }
-  int H = 0, V = 0;
-  for (int q = 0; q < 4; q++) {
-    int t4 = ht ? t[4 + q] : 128, l4 = hl ? l[4 + q] : 128;
-    int pt = q == 3 ? tl : (ht ? t[2 - q] : 128), pl = q == 3 ? tl : (hl ? l[2 - q] : 128);
-    H += (q + 1) * (t4 - pt);
-    V += (q + 1) * (l4 - pl);
-  }
+  int q = j & 3;
+  bool top = j < 4, av = top ? ht : hl;
+  const uint8_t* ed = top ? t : l;
+  int e4 = av ? ed[4 + q] : 128, ep = q == 3 ? tl : (av ? ed[2 - q] : 128);
+  int term = j < 8 ? (q + 1) * (e4 - ep) : 0;
+  term += __shfl_xor_sync(FULL, term, 1);
+  term += __shfl_xor_sync(FULL, term, 2);
+  int H = __shfl_sync(FULL, term, base), V = __shfl_sync(FULL, term, base + 4);
   pa = 16 * ((ht ? t[7] : 128) + (hl ? l[7] : 128));
   pb = (17 * H + 16) >> 5;
   pc = (17 * V + 16) >> 5;
