@@ -37,7 +37,7 @@ def work_list(mb_w, mb_h, streams, frames, lag, seg, split, kinds):
     return tasks[:2 * n].reshape(n, 2), [(int(queues[2 * q]), int(queues[2 * q + 1])) for q in range(3)]
 
 
-ORDER = {0: (0, 1, 2), 1: (1, 0, 2), 2: (2, 0, 1)}  # queue order per warp role (kernel)
+ORDER = {0: (0, 1, 2), 1: (1, 2, 0), 2: (2, 0, 1)}  # queue order per warp role, as in the kernel
 
 
 def simulate(mb_w, mb_h, streams, frames, lag, seg, reach, warps, idr_every=None):
@@ -102,9 +102,11 @@ def simulate(mb_w, mb_h, streams, frames, lag, seg, reach, warps, idr_every=None
                     if t is not None:
                         w[2] = (int(tasks[t, 1]) >> 1) & 0x7FFF
         for arr, i, v in pub:
-            arr[i] = max(arr[i], v)
+            assert arr[i] == v - 1      # every macroblock once, in order along its row
+            arr[i] = v
         if not moved:
             return None
+    assert (ana == W).all() and (db == W).all()
     return steps
 
 
