@@ -74,7 +74,9 @@ struct __align__(16) Smem {
   int32_t red[32];
 };
 static_assert(offsetof(Smem, coef) % 4 == 0 && offsetof(Smem, ccoef) % 4 == 0, "level arrays cleared by words");
-static_assert(offsetof(rg_mb_out, luma) % 4 == 0 && sizeof(rg_mb_out) % 4 == 0, "record levels written by words");
+static_assert(offsetof(rg_mb_out, luma) % 4 == 0 && offsetof(rg_mb_out, chroma_dc) % 4 == 0 &&
+                  offsetof(rg_mb_out, chroma_ac) % 4 == 0 && sizeof(rg_mb_out) % 4 == 0,
+              "record levels written by words");
 static_assert(offsetof(Smem, pred_y) % 8 == 0 && offsetof(Smem, tmp_y) % 8 == 0, "16x16 predictions written 8 bytes per lane");
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -1016,15 +1018,41 @@ __device__ __noinline__ void store_recon(const Ctx& c, const uint8_t* ly, Smem& 
 }
 
 // Writes the chroma part of the record (chroma levels in zig-zag) and clears the rest.
+// The chroma levels of the record, a word (two zig-zag levels) per lane and store: word w of the
+// AC levels holds slots 2 (w & 7), 2 (w & 7) + 1 of block w / 8 (plane * 4 + block); slot 0 (the
+// DC position) stays 0. Lanes 0..3 write the DC levels.
 __device__ __noinline__ void record_chroma(rg_mb_out* rec, Smem& sm, int cbpc) {
   int lane = lane_id();
-  if (lane < 8) {
-    int p = lane >> 2, b = lane & 3;
-#pragma unroll
-    for (int i = 0; i < 16; i++) rec->chroma_ac[p][b][i] = (i && cbpc >= 2) ? sm.ccoef[lane * 16 + c_scan4[i]] : 0;
-    if (b == 0)
-      for (int i = 0; i < 4; i++) rec->chroma_dc[p][i] = cbpc >= 1 ? sm.cdc[p * 4 + i] : 0;
+#pragma unroll 1
+  for (int k = 0; k < 2; k++) {
+    int w = lane + 32 * k, blk = w >> 3, i = (w & 7) * 2;
+    int r0 = (int)((kScan4Packed >> (4 * i)) & 15), r1 = (int)((kScan4Packed >> (4 * i + 4)) & 15);
+    int16_t v0 = (i && cbpc >= 2) ? sm.ccoef[blk * 16 + r0] : 0, v1 = cbpc >= 2 ? sm.ccoef[blk * 16 + r1] : 0;
+    ((uint32_t*)rec->chroma_ac)[w] = (uint32_t)(uint16_t)v0 | ((uint32_t)(uint16_t)v1 << 16);
   }
+  if (lane < 4) {
+    int16_t d0 = cbpc >= 1 ? sm.cdc[2 * lane] : 0, d1 = cbpc >= 1 ? sm.cdc[2 * lane + 1] : 0;
+    ((uint32_t*)rec->chroma_dc)[lane] = (uint32_t)(uint16_t)d0 | ((uint32_t)(uint16_t)d1 << 16);
+  }
+}
+// The 4x4 luma levels of the record in zig-zag order, a word per lane and store: word w holds
+// levels 2 (w & 7), 2 (w & 7) + 1 of block w / 8; lanes 8j..8j+7 of step k cover block 4k + j.
+// Returns the blocks holding levels (bit b: block b).
+__device__ __noinline__ uint16_t record_luma4x4(rg_mb_out* rec, const Smem& sm) {
+  int lane = lane_id();
+  uint32_t nz = 0;
+#pragma unroll 1
+  for (int k = 0; k < 4; k++) {
+    int w = lane + 32 * k, b = w >> 3, i = (w & 7) * 2;
+    int r0 = (int)((kScan4Packed >> (4 * i)) & 15), r1 = (int)((kScan4Packed >> (4 * i + 4)) & 15);
+    int16_t v0 = sm.coef[b * 16 + r0], v1 = sm.coef[b * 16 + r1];
+    ((uint32_t*)rec->luma)[w] = (uint32_t)(uint16_t)v0 | ((uint32_t)(uint16_t)v1 << 16);
+    uint32_t bal = __ballot_sync(FULL, (v0 | v1) != 0);
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if ((bal >> (8 * j)) & 0xffu) nz |= 1u << (4 * k + j);
+  }
+  return (uint16_t)nz;
 }
 __device__ __noinline__ void record_header(rg_mb_out* rec, int type, int i16_mode, int cmode, int cbp, int t8, int qp, int mvx, int mvy,
                               int mvdx, int mvdy, uint16_t nz) {
@@ -1318,18 +1346,11 @@ __device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, 
   chroma_quant(qpc, true, sm, ac_any, ac_sc);
   int cbpc = (ac_any[0] | ac_any[1]) ? 2 : (chroma_dc_any(sm) ? 1 : 0);
   rg_mb_out* rec = c.sd->rec + c.mb;
-  uint32_t bnz = 0;
+  uint16_t nzm = record_luma4x4(rec, sm);
   if (lane < 16) {
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      int16_t v = sm.coef[lane * 16 + c_scan4[i]];
-      rec->luma[lane * 16 + i] = v;
-      bnz |= v != 0;
-    }
     rec->luma_dc[lane] = 0;
     rec->i4_modes[lane] = sm.i4m[lane];
   }
-  uint16_t nzm = (uint16_t)__ballot_sync(FULL, lane < 16 && bnz);
   record_chroma(rec, sm, cbpc);
   if (lane == 0) record_header(rec, RG_MB_I4X4, 0, cmode, cbpl | (cbpc << 4), 0, c.sd->qp, 0, 0, 0, 0, nzm);
   chroma_recon(qpc, cbpc, sm);
@@ -1766,21 +1787,7 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
     nzm = 0;
     for (int k = 0; k < 4; k++) if ((cbpl >> k) & 1) nzm |= (uint16_t)(0xF << (4 * k));
   } else {
-    // word w of the 4x4 levels (zig-zag order) holds levels 2(w & 7), 2(w & 7) + 1 of block w / 8;
-    // lanes 8j..8j+7 of step k cover block 4k + j
-    uint32_t nz = 0;
-#pragma unroll 1
-    for (int k = 0; k < 4; k++) {
-      int w = lane + 32 * k, b = w >> 3, i = (w & 7) * 2;
-      int r0 = (int)((kScan4Packed >> (4 * i)) & 15), r1 = (int)((kScan4Packed >> (4 * i + 4)) & 15);
-      int16_t v0 = sm.coef[b * 16 + r0], v1 = sm.coef[b * 16 + r1];
-      ((uint32_t*)rec->luma)[w] = (uint32_t)(uint16_t)v0 | ((uint32_t)(uint16_t)v1 << 16);
-      uint32_t bal = __ballot_sync(FULL, (v0 | v1) != 0);
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if ((bal >> (8 * j)) & 0xffu) nz |= 1u << (4 * k + j);
-    }
-    nzm = (uint16_t)nz;
+    nzm = record_luma4x4(rec, sm);
   }
   if (lane < 16) { rec->luma_dc[lane] = 0; rec->i4_modes[lane] = 2; }
   record_chroma(rec, sm, cbpc);
