@@ -2272,13 +2272,14 @@ int pipeline_sms(int device) {
   return sms;
 }
 
-// Resident warps of the pipelined mode: seven per SM (fewer when they do not fit). More warps
-// overlap more waits but slow every macroblock on the critical path (measured on B200: 5-8 per
-// SM within 3 % of each other, 20 per SM 10 % slower).
+// Resident warps of the pipelined mode: sixteen per SM (fewer when they do not fit). More warps
+// overlap more of each other's waits, until the SM's front end saturates and every macroblock on
+// the critical path slows (measured on B200, 1080p 8 x 15 pictures, launch time: 7 per SM
+// 62.9 ms, 8 61.0, 10 59.1, 12 57.4, 14 56.0, 16 55.8, 18 56.2, 20-21 56.3).
 int pipeline_grid(int device) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel, 32, 0);
-  return (per_sm < 7 ? per_sm : 7) * pipeline_sms(device);
+  return (per_sm < 16 ? per_sm : 16) * pipeline_sms(device);
 }
 
 // Work list of the pipelined mode, written to `tasks` (pipeline_task_count entries): every
