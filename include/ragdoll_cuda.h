@@ -226,7 +226,7 @@ typedef struct rg_pipeline_tuning {
  * of a stream in the work order (1..4096; 0 = 8 * max(seg, 2) + seg + 7, which orders every
  * wait of a search reaching up to 4 macroblock rows beyond zero motion after the work it waits
  * for; larger is safer for long motion, smaller favours newer pictures), seg = macroblocks per
- * work segment (1..mb_w, 0 = 2), grid = resident warps (0 = sixteen per SM, fewer if they do not
+ * work segment (1..mb_w, 0 = 1), grid = resident warps (0 = sixteen per SM, fewer if they do not
  * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take
  * deblocking segments first from a queue of their own (0 = one SM in six, -1 = one mixed queue
  * for all warps), intra_sms = the next SMs, whose warps take the analysis of IDR pictures first

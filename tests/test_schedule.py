@@ -117,9 +117,10 @@ def simulate(mb_w, mb_h, streams, frames, lag, seg, reach, warps, idr_every=None
 ])
 @pytest.mark.parametrize("warps", [(1, 0, 0), (3, 1, 1), (12, 4, 6), (40, 10, 20), (2, 1, 0)])
 @pytest.mark.parametrize("reach", [0, 2, 4])
-def test_default_order_never_stalls(shape, warps, reach):
+@pytest.mark.parametrize("seg", [1, 2])
+def test_default_order_never_stalls(shape, warps, reach, seg):
     W, H, S, F = shape
-    assert simulate(W, H, S, F, 0, 2, reach, warps) is not None
+    assert simulate(W, H, S, F, 0, seg, reach, warps) is not None
 
 
 def test_longer_segments_and_gops_in_one_call():
