@@ -2091,7 +2091,9 @@ __device__ __noinline__ void picture_row_done(int* rows_done, int* ready, int se
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(32, 20) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
+// At least 16 warps per SM: up to 128 registers a thread, so nothing spills (4.5 % faster than 20,
+// which held it to 96 registers with spills).
+__global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
   __shared__ Smem sm;
   const int lane = lane_id();
   const int S = fp.n_streams, H = fp.mb_h, Wm = fp.mb_w;
