@@ -461,7 +461,8 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
 // previous wave then runs during that wave's own launch and slows it.) ready / seq: per-picture
 // flags in mapped host memory (rg_analyse_gops_stream), or null.
 static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                        const int32_t* kinds, int32_t frames, rg_mb_out* rec_base, int* ready = nullptr, int seq = 0) {
+                        const int32_t* kinds, int32_t frames, rg_mb_out* rec_base, int* ready = nullptr, int seq = 0,
+                        bool resolved = false) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null argument");
   if (frames < 1 || frames > c->max_frames)
     return fail(RG_ERR_INVALID, "rg_analyse_gops_device: frames %d outside 1..%d (rg_config.max_frames)", frames,
@@ -469,7 +470,7 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
     return fail(RG_ERR_INVALID, "rg_analyse_gops_device: stride too small");
   int S = c->S;
-  {
+  if (!resolved) {
     int r = resolve_pending(c, false);
     if (r) return r;
   }
@@ -607,6 +608,25 @@ int rg_set_pipeline_tuning(rg_ctx* c, const rg_pipeline_tuning* t) {
   return RG_OK;
 }
 
+// One source picture (host planes pl[3]) into device staging d (Y | U | V, unpadded rows): one copy
+// when the planes lie back to back with unpadded rows, else one per plane; 2-D copies only for
+// padded rows (they run at a fraction of the link's rate).
+static cudaError_t copy_picture_in(uint8_t* d, const uint8_t* const* pl, int w, int h, size_t stride_y,
+                                   size_t stride_uv, cudaStream_t st) {
+  const int cw = (w + 1) / 2, ch = (h + 1) / 2;
+  const size_t ny = (size_t)w * h, nc = (size_t)cw * ch;
+  cudaError_t e = cudaSuccess;
+  if (stride_y == (size_t)w && stride_uv == (size_t)cw) {
+    if (pl[1] == pl[0] + ny && pl[2] == pl[1] + nc) return cudaMemcpyAsync(d, pl[0], ny + 2 * nc, cudaMemcpyHostToDevice, st);
+    if ((e = cudaMemcpyAsync(d, pl[0], ny, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(d + ny, pl[1], nc, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    return cudaMemcpyAsync(d + ny + nc, pl[2], nc, cudaMemcpyHostToDevice, st);
+  }
+  if ((e = cudaMemcpy2DAsync(d, w, pl[0], stride_y, w, h, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpy2DAsync(d + ny, cw, pl[1], stride_uv, cw, ch, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  return cudaMemcpy2DAsync(d + ny + nc, cw, pl[2], stride_uv, cw, ch, cudaMemcpyHostToDevice, st);
+}
+
 int rg_analyse_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
                     int32_t frames, rg_mb_out* out) {
   if (!c || !planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops: null argument");
@@ -620,10 +640,7 @@ int rg_analyse_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, si
       const uint8_t* const* pl = planes + (f * S + s) * 3;
       if (!pl[0] || !pl[1] || !pl[2]) return fail(RG_ERR_INVALID, "rg_analyse_gops: picture %d stream %d null plane", f, s);
       uint8_t* d = c->srcs + c->src_bytes() * ((size_t)f * S + s);
-      CK(cudaMemcpy2DAsync(d, w, pl[0], stride_y, w, h, cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemcpy2DAsync(d + (size_t)w * h, cw, pl[1], stride_uv, cw, ch, cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemcpy2DAsync(d + (size_t)w * h + (size_t)cw * ch, cw, pl[2], stride_uv, cw, ch, cudaMemcpyHostToDevice,
-                           c->stream));
+      CK(copy_picture_in(d, pl, w, h, stride_y, stride_uv, c->stream));
       dev[(f * S + s) * 3] = d;
       dev[(f * S + s) * 3 + 1] = d + (size_t)w * h;
       dev[(f * S + s) * 3 + 2] = d + (size_t)w * h + (size_t)cw * ch;
@@ -717,23 +734,26 @@ static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, 
   // sources into this slot's staging once the launch that last read it is done
   CK(cudaStreamWaitEvent(c->a_in, c->a_kern_done[slot], 0));
   std::vector<const uint8_t*> dev(3 * (size_t)S * frames);
+  const size_t ny = (size_t)w * h, nc = (size_t)cw * ch;
   for (int i = 0; i < S * frames; i++) {
     const uint8_t* const* pl = planes + 3 * i;
     uint8_t* d = c->a_srcs[slot] + c->src_bytes() * i;
-    CK(cudaMemcpy2DAsync(d, w, pl[0], stride_y, w, h, cudaMemcpyHostToDevice, c->a_in));
-    CK(cudaMemcpy2DAsync(d + (size_t)w * h, cw, pl[1], stride_uv, cw, ch, cudaMemcpyHostToDevice, c->a_in));
-    CK(cudaMemcpy2DAsync(d + (size_t)w * h + (size_t)cw * ch, cw, pl[2], stride_uv, cw, ch, cudaMemcpyHostToDevice,
-                         c->a_in));
+    CK(copy_picture_in(d, pl, w, h, stride_y, stride_uv, c->a_in));
     dev[3 * i] = d;
-    dev[3 * i + 1] = d + (size_t)w * h;
-    dev[3 * i + 2] = d + (size_t)w * h + (size_t)cw * ch;
+    dev[3 * i + 1] = d + ny;
+    dev[3 * i + 2] = d + ny + nc;
   }
   CK(cudaEventRecord(c->a_in_done[slot], c->a_in));
+  // The previous launch is resolved (waited for, re-run if it failed) before the launch stream is
+  // told to wait for this copy: resolving ends with a synchronisation of that stream, which would
+  // otherwise wait for the copy too and hold the caller for its whole duration.
+  int r = resolve_pending(c, false);
+  if (r) return r;
   // the launch waits for its sources and for the copy-out of this slot's previous records
   CK(cudaStreamWaitEvent(c->stream, c->a_in_done[slot], 0));
   CK(cudaStreamWaitEvent(c->stream, c->a_out_done[slot], 0));
   int seq = ++c->launch_seq;
-  int r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot], bulk ? nullptr : c->d_ready[slot], seq);
+  r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot], bulk ? nullptr : c->d_ready[slot], seq, true);
   if (r) return r;
   c->a_seq[slot] = seq;
   c->a_frames[slot] = frames;

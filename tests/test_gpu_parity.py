@@ -247,3 +247,40 @@ def test_streamed_records_arrive_per_picture_and_match(give_up):
     assert bool(unfinished) == give_up
     assert L.rg_analyse_gops_wait(eng.h, out.ctypes.data) == 0
     assert out.tobytes() == bulk.tobytes()
+
+
+def test_source_layouts_give_the_same_records():
+    """Host sources as separate planes, as one Y|U|V buffer per picture (copied in one piece) and
+    with padded rows (2-D copies), through the synchronous and the asynchronous host-buffer calls:
+    the same records every time."""
+    from ragdoll_b200.engine import RECORD_DTYPE, RG_FRAME_IDR, RG_FRAME_P, Engine
+    w, h, qp, S, F = 96, 64, 27, 2, 3
+    cw, ch = w // 2, h // 2
+    clips = [grating_clip(w, h, F, seed=321 + s, motion=5.0, rects=1) for s in range(S)]
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)]
+
+    def packed(y, u, v):
+        buf = np.concatenate([y.reshape(-1), u.reshape(-1), v.reshape(-1)])
+        return buf[:w * h].reshape(h, w), buf[w * h:w * h + cw * ch].reshape(ch, cw), buf[w * h + cw * ch:].reshape(ch, cw)
+
+    def padded(y, u, v):
+        out = []
+        for p in (y, u, v):
+            wide = np.zeros((p.shape[0], p.shape[1] + 32), np.uint8)
+            wide[:, :p.shape[1]] = p
+            out.append(wide[:, :p.shape[1]])
+        return tuple(out)
+
+    layouts = {"planes": lambda y, u, v: (y, u, v), "packed": packed, "padded": padded}
+    got = {}
+    for name, lay in layouts.items():
+        frames = [[lay(*clips[s][f]) for s in range(S)] for f in range(F)]
+        got[name + "/sync"] = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F).analyse_gops(frames, kinds)
+        eng = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+        out = np.zeros((F, S, eng.n_mb), RECORD_DTYPE)
+        eng.analyse_gops_async(frames, kinds, out)
+        eng.sync()
+        got[name + "/async"] = out
+    ref = got["planes/sync"]
+    for k, v in got.items():
+        assert v.tobytes() == ref.tobytes(), k
