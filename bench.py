@@ -187,13 +187,15 @@ def run_batched(args, rank, world, local):
     profile (CABAC), a QP drawn uniformly from 20..36 per stream, Balanced analysis. One encoder
     per size, the four driven concurrently from host threads (each with its own persistent
     launches on its own CUDA stream and its own writer threads), waves of 10 pictures of all its
-    streams, two waves in flight. A step is the whole encode of the 1920 pictures: host frames in
-    (pinned), access units out. Reports the aggregate frames/s and the per-frame latency
-    percentiles (a picture's latency: its wave's submit to its access unit written)."""
+    streams, two waves in flight; each size's launch shape (warps per SM, segment length) picked by
+    ragdoll_b200.autotune on its first wave before timing (--no-autotune: library defaults). A
+    step is the whole encode of the 1920 pictures: host frames in (pinned), access units out.
+    Reports the aggregate frames/s and the per-frame latency percentiles (a picture's latency: its
+    wave's submit to its access unit written)."""
     import torch
 
     from ragdoll_b200.encoder import H264Encoder
-    from ragdoll_b200.engine import RG_PROFILE_MAIN
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_MAIN
     from ragdoll_b200.synth import grating_clip
 
     if rank != 0:
@@ -221,8 +223,15 @@ def run_batched(args, rank, world, local):
         frames = [[(hn[s, f, :w * h].reshape(h, w), hn[s, f, w * h:w * h + cw * ch].reshape(ch, cw),
                     hn[s, f, w * h + cw * ch:].reshape(ch, cw)) for s in range(BATCH_STREAMS)]
                   for f in range(BATCH_FRAMES)]
+        tuning = None
+        if args.autotune:
+            # the launch shape of this size, timed on its first wave (outside the timed region)
+            from ragdoll_b200.autotune import autotune_pipeline
+            kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * BATCH_STREAMS for f in range(BATCH_WAVE)]
+            tuning, _ = autotune_pipeline(w, h, 26, RG_PROFILE_MAIN, frames[:BATCH_WAVE], kinds, device=local)
+            enc.set_pipeline_tuning(**tuning)
         jobs.append({"size": f"{w}x{h}", "enc": enc, "frames": frames, "host": host, "qps": qps,
-                     "threads": threads})
+                     "threads": threads, "tuning": tuning})
 
     def encode_all(job, out):
         enc, frames, lat, nbytes = job["enc"], job["frames"], [], 0
@@ -271,7 +280,8 @@ def run_batched(args, rank, world, local):
         "config": {"workload": "batched streams: 16 x 320x240, 16 x 640x360, 16 x 1280x720, 16 x 1920x1080, "
                                "30 frames each (one GOP), Main CABAC, QP U[20,36] per stream, Balanced",
                    "encoders": "one per size, driven concurrently; waves of 10 pictures x 16 streams, two in flight",
-                   "host_threads": {j["size"]: j["threads"] for j in jobs}},
+                   "host_threads": {j["size"]: j["threads"] for j in jobs},
+                   "launch_shape": {j["size"]: j["tuning"] or "library defaults" for j in jobs}},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2), "p99": round(float(np.percentile(lat, 99)), 2),
                        "max": round(float(lat.max()), 2), "definition": "a wave's submit to the picture's access unit written"},
         "per_size": {k: {"frames_per_s": round(BATCH_STREAMS * BATCH_FRAMES / statistics.median(t for t, _ in v), 1),
@@ -580,6 +590,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="batched workload: keep the library's default launch shape for every size")
     ap.add_argument("--workload", default="1080p", choices=["1080p", "batched"],
                     help="the 1080p 8-GOP workload, or the batched-streams configuration (64 mixed-size streams)")
     ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],

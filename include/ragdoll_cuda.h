@@ -364,6 +364,9 @@ typedef struct rg_encoder rg_encoder;
 rg_encoder* rg_encoder_create(const rg_config* cfg, int32_t fps_num, int32_t fps_den, int32_t keyint, int32_t threads);
 void rg_encoder_destroy(rg_encoder* enc);
 int32_t rg_encoder_threads(const rg_encoder* enc);
+/* The engine context the encoder analyses with, for rg_set_pipeline_tuning (owned by the
+ * encoder). No counterpart in the reference. */
+rg_ctx* rg_encoder_context(rg_encoder* enc);
 /* The fixed QP (1..51) of one stream, before its first picture (default cfg.qp): streams of
  * different QPs are analysed in the same launches and written with their own PPS. */
 int rg_encoder_set_stream_qp(rg_encoder* enc, int32_t stream, int32_t qp);

@@ -189,6 +189,8 @@ void rg_encoder_destroy(rg_encoder* e) {
 
 int32_t rg_encoder_threads(const rg_encoder* e) { return e ? e->pool->size() : 0; }
 
+rg_ctx* rg_encoder_context(rg_encoder* e) { return e ? e->ctx : nullptr; }
+
 int rg_encoder_set_stream_qp(rg_encoder* e, int32_t stream, int32_t qp) {
   if (!e) return efail(RG_ERR_INVALID, "rg_encoder_set_stream_qp: null encoder");
   if (stream < 0 || stream >= (int)e->coded.size()) return efail(RG_ERR_INVALID, "rg_encoder_set_stream_qp: stream %d", stream);

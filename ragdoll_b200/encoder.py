@@ -43,6 +43,18 @@ class H264Encoder:
     def threads(self) -> int:
         return lib().rg_encoder_threads(self.h)
 
+    def set_pipeline_tuning(self, **tuning) -> None:
+        """Work order of the encoder's persistent launches (rg_set_pipeline_tuning on its context;
+        keywords as Engine.set_pipeline_tuning), e.g. what ragdoll_b200.autotune picked; not while
+        waves are in flight."""
+        from .engine import RgPipelineTuning
+        if self._inflight:
+            raise RgError(-6, "set_pipeline_tuning: waves in flight")
+        t = RgPipelineTuning(*(int(tuning.get(k, 0)) for k, _ in RgPipelineTuning._fields_))
+        rc = lib().rg_set_pipeline_tuning(lib().rg_encoder_context(self.h), ctypes.byref(t))
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+
     def encode_frame(self, frame: Frame, stream: int = 0) -> bytes:
         y, u, v = (np.ascontiguousarray(p, np.uint8) for p in frame)
         n = lib().rg_encode_frame(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],

@@ -42,7 +42,7 @@ EXPORTS = [
     "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture", "rg_pipeline_work_list",
     "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
     "rg_demux_info", "rg_demux_access_unit", "rg_analyse_gops_wait", "rg_encoder_create", "rg_encoder_destroy",
-    "rg_encoder_threads", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_encoder_latencies",
+    "rg_encoder_threads", "rg_encoder_context", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_encoder_latencies",
     "rg_quality_frame_prev",
     "rg_vmaf_lite_plane", "rg_set_stream_qp", "rg_encoder_set_stream_qp", "rg_analyse_gops_stream",
     "rg_analyse_gops_fetch",
@@ -146,6 +146,8 @@ def lib() -> ctypes.CDLL:
     L.rg_encoder_destroy.argtypes = [P]
     L.rg_encoder_threads.restype = ctypes.c_int32
     L.rg_encoder_threads.argtypes = [P]
+    L.rg_encoder_context.restype = P
+    L.rg_encoder_context.argtypes = [P]
     L.rg_encode_frame.restype = ctypes.c_int64
     L.rg_encode_frame.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, P,
                                   ctypes.c_size_t]
