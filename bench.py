@@ -439,8 +439,11 @@ def run_engine(args, rank, world, local):
 
     # end to end: the whole encode through the public encoder, host frames in, access units out
     from ragdoll_b200.encoder import H264Encoder
+    # the host cores shared among the ranks of this node (one writer pool per rank)
+    local_world = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+    enc_threads = max(2, (os.cpu_count() or 1) // max(local_world, 1))
     enc = H264Encoder(W, H, QP, profile=RG_PROFILE_HIGH, keyint=GOP, streams=gops, max_frames=GOP,
-                      device=local, threads=0)
+                      device=local, threads=enc_threads)
     for _ in range(2):                         # both wave slots once
         enc.submit(frames_host)
     enc.collect()
