@@ -69,6 +69,9 @@ def test_batched_streams_match_single():
     (208, 120, 24, 2, 2, 5, {"deblock_sms": 16, "grid": 64, "lag": 40}),
     (176, 144, 26, 2, 3, 5, {"deblock_sms": 20, "intra_sms": 40}),
     (176, 144, 26, 2, 3, 5, {"deblock_sms": 3, "intra_sms": 2, "grid": 100}),
+    (16, 16, 26, 2, 2, 3, {}),                  # one macroblock
+    (48, 16, 28, 1, 2, 3, {}),                  # one row
+    (16, 64, 30, 0, 2, 3, {"grid": 8}),         # one column
 ])
 def test_pipelined_gops_match_oracle(w, h, qp, profile, streams, frames, tuning):
     """One persistent launch for all pictures of several GOPs (pictures of a GOP overlapping)
