@@ -15,6 +15,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+#if defined(__AVX2__) && defined(__BMI2__)
+#include <immintrin.h>
+#endif
 
 #include "bitstream.h"
 #include "cabac_tables.h"
@@ -136,6 +139,22 @@ constexpr int kAbs[6] = {227, 237, 247, 257, 266, 426};
 inline int blk_x(int b) { return (b & 1) | ((b >> 1) & 2); }
 inline int blk_y(int b) { return ((b >> 1) & 1) | ((b >> 2) & 2); }
 
+// Bit i set where level i of c[0..n) (n <= 64) is not 0.
+inline uint64_t nonzero_mask(const int16_t* c, int n) {
+  uint64_t m = 0;
+  int i = 0;
+#if defined(__AVX2__) && defined(__BMI2__)
+  const __m256i zero = _mm256_setzero_si256();
+  for (; i + 16 <= n; i += 16) {
+    const __m256i v = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(c + i));
+    const uint32_t eq = (uint32_t)_mm256_movemask_epi8(_mm256_cmpeq_epi16(v, zero));  // 2 bits per level
+    m |= (uint64_t)(_pext_u32(~eq, 0x55555555u)) << i;
+  }
+#endif
+  for (; i < n; i++) m |= (uint64_t)(c[i] != 0) << i;
+  return m;
+}
+
 class SliceCoder {
  public:
   SliceCoder(int mb_w, int mb_h, int qp, bool idr, bool t8x8, std::vector<uint8_t>& out)
@@ -238,22 +257,22 @@ class SliceCoder {
   // One residual block in scan order (9.3.2.3 / 9.3.3.1.3); cat 5 has no coded_block_flag.
   // Returns whether it holds levels.
   bool block(int cat, int cbf_inc, const int16_t* c, int n) {
-    int last = n - 1;
-    while (last >= 0 && !c[last]) last--;
+    const uint64_t nz = nonzero_mask(c, n);
     if (cat < 5) {
-      bin(kCbf[cat] + cbf_inc, last >= 0);
-      if (last < 0) return false;
+      bin(kCbf[cat] + cbf_inc, nz != 0);
+      if (!nz) return false;
     }
-    if (last < 0) last = 0;
+    const int last = nz ? 63 - __builtin_clzll(nz) : 0;
     for (int i = 0; i <= std::min(last, n - 2); i++) {
       const int sig = cat == 5 ? cabac::kSig8x8[i] : i, lst = cat == 5 ? cabac::kLast8x8[i] : i;
-      bin(kSig[cat] + sig, c[i] != 0);
-      if (c[i]) bin(kLast[cat] + lst, i == last);
+      const unsigned s = (unsigned)(nz >> i) & 1u;
+      bin(kSig[cat] + sig, s);
+      if (s) bin(kLast[cat] + lst, i == last);
     }
     const int lvl = kAbs[cat], gt_cap = cat == 3 ? 3 : 4;
     int ones = 0, bigger = 0;
-    for (int i = last; i >= 0; i--) {
-      if (!c[i]) continue;
+    for (uint64_t left = nz; left; left &= ~(1ull << (63 - __builtin_clzll(left)))) {
+      const int i = 63 - __builtin_clzll(left);
       const unsigned m1 = (unsigned)std::abs(c[i]) - 1;
       bin(lvl + (bigger ? 0 : std::min(1 + ones, 4)), m1 != 0);
       if (!m1) {
