@@ -35,23 +35,38 @@ using cabac::kContexts;
 // received (up to 9 bits) and the carries are resolved, last byte first, when the slice is done.
 // The first bit of the code value (the standard's firstBitFlag) is always 0 and never written.
 // Context models are packed as pStateIdx << 1 | valMPS.
+// The model after coding bin b with model m (pStateIdx << 1 | valMPS), at [2 m + b]: the
+// transitions of 9.3.3.2.2 in one table.
+struct ModelNext {
+  uint8_t v[256];
+  constexpr ModelNext() : v() {
+    for (int m = 0; m < 128; m++)
+      for (int b = 0; b < 2; b++) {
+        int state = m >> 1, mps = m & 1;
+        if (b != mps) {
+          if (state == 0) mps ^= 1;
+          state = cabac::kNextLps[state];
+        } else if (state < 62) {
+          state++;
+        }
+        v[2 * m + b] = (uint8_t)(state << 1 | mps);
+      }
+  }
+};
+constexpr ModelNext kModelNext{};
+
 class Arith {
  public:
-  explicit Arith(std::vector<uint8_t>& out) : out_(out) {}
+  explicit Arith(std::vector<uint8_t>& out) : out_(out) { pend_.reserve(1 << 16); }
 
   void decision(uint8_t& model, unsigned bin) {
-    unsigned state = model >> 1, mps = model & 1u;
+    const unsigned m = model, state = m >> 1, lpsb = bin ^ (m & 1u);
     const uint32_t lps = cabac::kRangeLps[state][(range_ >> 6) & 3];
-    range_ -= lps;
-    if (bin != mps) {
-      low_ += range_;
-      range_ = lps;
-      if (state == 0) mps ^= 1u;
-      state = cabac::kNextLps[state];
-    } else if (state < 62) {
-      state++;
-    }
-    model = (uint8_t)(state << 1 | mps);
+    const uint32_t rmps = range_ - lps;
+    // the least probable symbol adds the MPS sub-range to low and keeps the LPS sub-range
+    low_ += lpsb ? rmps : 0u;
+    range_ = lpsb ? lps : rmps;
+    model = kModelNext.v[2 * m + bin];
     const int shift = __builtin_clz(range_) - 23;  // range_ < 512: doubles it to 256..511
     range_ <<= shift;
     low_ <<= shift;
