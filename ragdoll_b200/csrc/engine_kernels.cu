@@ -50,16 +50,20 @@ struct __align__(16) Smem {
   uint8_t pred_u[64];
   uint8_t pred_v[64];
   uint8_t tmp_y[256];       // plane prediction / I4x4 reconstruction
-  uint8_t cand_u[64];       // chroma intra candidates
-  uint8_t cand_v[64];
   uint8_t win[23 * 24];     // integer samples of a half-sample window (rows -2.., cols -2..)
-  uint8_t hph[18 * 20];     // b samples (horizontal half)
-  uint8_t hpv[18 * 20];     // h samples (vertical half)
-  uint8_t hpj[18 * 20];     // j samples (centre)
-  int16_t hr[23 * 18];      // unrounded horizontal 6-tap sums
+  // The half-sample planes live until the sub-pel search ends; the 8x8 transform's intermediates
+  // are needed only after it (the residual), so they share the space.
+  union {
+    struct {
+      uint8_t hph[18 * 20];  // b samples (horizontal half)
+      uint8_t hpv[18 * 20];  // h samples (vertical half)
+      uint8_t hpj[18 * 20];  // j samples (centre)
+      int16_t hr[23 * 18];   // unrounded horizontal 6-tap sums
+    };
+    int32_t t8[256];         // 8x8 transform intermediates
+  };
   int16_t coef[256];        // luma 4x4 levels: block b (decoding order) at [16 b], raster
   int16_t coef8[256];       // luma 8x8 levels: block b at [64 b], raster
-  int32_t t8[256];          // 8x8 transform intermediates
   int16_t ccoef[128];       // chroma levels: block (plane * 4 + b) at [16 *], raster
   int16_t cdcraw[8];
   int16_t cdc[8];
@@ -71,7 +75,6 @@ struct __align__(16) Smem {
   uint8_t cleft[2][8];
   uint8_t i4m[16];          // Intra4x4PredMode of this macroblock (decoding order)
   uint8_t i4q[16];          // edge samples of the current 4x4 block (i4_edge_index)
-  int32_t red[32];
 };
 static_assert(offsetof(Smem, coef) % 4 == 0 && offsetof(Smem, ccoef) % 4 == 0, "level arrays cleared by words");
 static_assert(offsetof(rg_mb_out, luma) % 4 == 0 && offsetof(rg_mb_out, chroma_dc) % 4 == 0 &&
