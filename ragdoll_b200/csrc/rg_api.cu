@@ -22,13 +22,15 @@ thread_local std::string g_last_error;
 
 constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the segment length
 constexpr int kDefaultSeg = 1;   // macroblocks per work segment (16 warps per SM: 1 is 2 % faster than 2)
-// Deblocking is about a sixth of the work once analysis runs at full speed: one SM in six takes
-// its queue first (25 of 148; measured on B200: 16 SMs 1326 frames/s, 20-30 SMs 1394-1417).
-int default_deblock_sms(int sms) { return sms >= 6 ? (sms + 3) / 6 : 0; }
-// The analysis of IDR pictures is the critical path of every GOP (each P picture trails it): one
-// SM in three takes it first (49 of 148; measured on B200: none 1412 frames/s, 20 SMs 1355,
-// 35-65 SMs 1473-1481). Those warps continue with P pictures once the IDR queue is empty.
-int default_intra_sms(int sms) { return sms >= 3 ? sms / 3 : 0; }
+// Deblocking SMs: one in five takes the deblocking queue first (30 of 148). Measured on B200 with
+// 16 warps per SM, 1080p 8 x 15 launch: 25 SMs 52.3-53.2 ms, 30 51.4-52.3, 35-40 52.6-52.8
+// (at 7 warps per SM, before the IDR path got faster: 16 SMs 1326 frames/s, 20-30 1394-1417).
+int default_deblock_sms(int sms) { return sms >= 5 ? (sms + 4) / 5 : 0; }
+// The analysis of IDR pictures heads every GOP (each P picture trails it): the next one SM in
+// seven takes it first (21 of 148; with 30 deblocking SMs: 20 IDR SMs 51.6 ms, 30 51.8, 49 52.3;
+// at 7 warps per SM one in three was best). Those warps continue with P pictures once the IDR
+// queue is empty.
+int default_intra_sms(int sms) { return sms >= 7 ? sms / 7 : 0; }
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
