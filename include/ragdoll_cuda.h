@@ -228,9 +228,9 @@ typedef struct rg_pipeline_tuning {
  * for; larger is safer for long motion, smaller favours newer pictures), seg = macroblocks per
  * work segment (1..mb_w, 0 = 1), grid = resident warps (0 = sixteen per SM, fewer if they do not
  * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take
- * deblocking segments first from a queue of their own (0 = one SM in six, -1 = one mixed queue
+ * deblocking segments first from a queue of their own (0 = one SM in five, -1 = one mixed queue
  * for all warps), intra_sms = the next SMs, whose warps take the analysis of IDR pictures first
- * from a queue of their own. A wait that runs out makes the launch stop and rg_sync re-run the
+ * from a queue of their own (0 = one SM in seven, -1 = none). A wait that runs out makes the launch stop and rg_sync re-run the
  * call on the per-diagonal path, which has no waits. No counterpart in the reference (its GOP
  * threads have no device schedule).
  */
