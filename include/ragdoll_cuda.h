@@ -223,9 +223,12 @@ typedef struct rg_pipeline_tuning {
 
 /*
  * Tuning / test hook of the pipelined mode (tuning NULL: all defaults): lag = macroblock-times between consecutive pictures
- * of a stream in the work order (1..4096; 0 = 8 * max(seg, 2) + seg + 7, which orders every
- * wait of a search reaching up to 4 macroblock rows beyond zero motion after the work it waits
- * for; larger is safer for long motion, smaller favours newer pictures), seg = macroblocks per
+ * of a stream in the work order (1..4096; 0 = derived from the searches: max(seg, 2) * (4 + ry)
+ * + seg + rx + 3, which orders every wait of a search reaching up to ry macroblock rows and rx
+ * columns beyond zero motion after the work it waits for; ry = rx = 4 until the context's
+ * launches have shown their reach, raised as soon as a launch reaches further, lowered after four
+ * launches in a row that all reached less; larger is safer for long motion, smaller favours newer
+ * pictures), seg = macroblocks per
  * work segment (1..mb_w, 0 = 1), grid = resident warps (0 = sixteen per SM, fewer if they do not
  * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take
  * deblocking segments first from a queue of their own (0 = one SM in five, -1 = one mixed queue
@@ -235,6 +238,11 @@ typedef struct rg_pipeline_tuning {
  * threads have no device schedule).
  */
 int rg_set_pipeline_tuning(rg_ctx* ctx, const rg_pipeline_tuning* tuning);
+
+/* The picture lag the next pipelined launch of the context uses (the set one, or the one derived
+ * from the reach of its searches); negative RG_ERR_* on a null context. No counterpart in the
+ * reference. */
+int32_t rg_pipeline_lag(const rg_ctx* ctx);
 
 /* Waits for queued device work of the context. */
 int rg_sync(rg_ctx* ctx);

@@ -29,6 +29,7 @@ class Muxer:
     """One H.264 track: ``write(access_unit)`` per picture in decoding order, then ``finish()``."""
 
     def __init__(self, container: str, width: int, height: int, fps: Tuple[int, int] = (30, 1)):
+        self._destroy = lib().rg_mux_destroy  # kept: the module's globals may go first at exit
         self.h = lib().rg_mux_create(CONTAINERS[container], width, height, fps[0], fps[1])
         if not self.h:
             raise _err(-1)
@@ -51,7 +52,7 @@ class Muxer:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            lib().rg_mux_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -74,6 +75,7 @@ class Demuxer:
 
     def __init__(self, data: bytes):
         buf = (ctypes.c_uint8 * len(data)).from_buffer_copy(data)
+        self._destroy = lib().rg_demux_destroy  # kept: the module's globals may go first at exit
         self.h = lib().rg_demux_open(buf, len(data))
         if not self.h:
             raise _err(-1)
@@ -106,7 +108,7 @@ class Demuxer:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            lib().rg_demux_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):

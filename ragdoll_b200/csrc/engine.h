@@ -79,7 +79,10 @@ int wavefront_steps(const FrameParams& fp);
 // pipeline_counter_ints() zeroed ints; counters[1] is non-zero after a failed wait. ready (device
 // address of mapped host memory, or null): frames x n_streams ints, each set to seq once that
 // picture's records are final. host_err: mapped host int receiving the launch's error word (zero
-// it before the launch).
+// it before the launch). host_reach (mapped host, or null): two ints receiving 1 + the largest
+// reach, in macroblock rows and columns beyond zero motion, of the launch's waits for a reference
+// picture (0: no such wait); the work order never waits for an untaken segment when
+// lag >= max(seg, 2) * (4 + rows) + seg + columns + 3.
 int pipeline_grid(int device);
 int pipeline_sms(int device);
 size_t pipeline_counter_ints(const FrameParams& fp, int frames);
@@ -93,7 +96,7 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
                      size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
                      int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
-                     cudaStream_t st);
+                     int* host_reach, cudaStream_t st);
 void upload_tables();
 
 }  // namespace rg

@@ -1495,6 +1495,7 @@ struct PipeWait {
   unsigned long long timeout_ns;
   int seen_ana;          // last acquired ana_prev[row of this segment]
   int db_row, seen_db;   // last acquired db_prev[db_row]
+  int reach_y, reach_x;  // 1 + the largest reach waited for beyond zero motion, in macroblocks
   bool failed;
 };
 
@@ -1561,6 +1562,9 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
     // rows above the last are final where the row below is deblocked; the last row where its
     // right neighbour is
     int row = rr < fp.mb_h - 1 ? rr + 1 : rr, need = rr < fp.mb_h - 1 ? xx + 1 : min(xx + 2, fp.mb_w);
+    // zero motion reaches (mbx + 2, mby + 2); the host sizes the picture lag from the maximum
+    pw->reach_y = max(pw->reach_y, max(rr - mby - 2, 0) + 1);
+    pw->reach_x = max(pw->reach_x, max(xx - mbx - 2, 0) + 1);
     if (row != pw->db_row) {
       pw->db_row = row;
       pw->seen_db = 0;
@@ -2075,6 +2079,7 @@ struct PipeParams {
   int* ready;         // [F][S] in mapped host memory (or null): seq once a picture's records are final
   int seq;
   int* host_err;      // mapped host memory: the error word as the launch ends (no copy to wait for)
+  int* reach;         // [2] 1 + the largest reach of a reference wait beyond zero motion (rows, columns)
 };
 __device__ __forceinline__ unsigned sm_id() {
   unsigned r;
@@ -2112,6 +2117,7 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
     role = k == 0 ? 1 : (k == 1 ? 2 : 0);
   }
   bool empty[3] = {pp.qbeg[0] >= pp.qend[0], pp.qbeg[1] >= pp.qend[1], pp.qbeg[2] >= pp.qend[2]};
+  int reach_y = 0, reach_x = 0;  // this warp's, published once as it exits
   while (true) {
     int t = -1;
     if (lane == 0) {
@@ -2145,6 +2151,8 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
       pw.seen_ana = 0;
       pw.db_row = -1;
       pw.seen_db = 0;
+      pw.reach_y = reach_y;
+      pw.reach_x = reach_x;
       pw.failed = false;
       int seen_own = 0, seen_up = 0;
       // the previous segment of this row, then per macroblock the row above two ahead
@@ -2165,6 +2173,8 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
         publish(ana_rows + y, x + 1);
       }
       if (!failed && x1 == Wm && pp.ready) picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
+      reach_y = pw.reach_y;
+      reach_x = pw.reach_x;
     } else {
       int seen_own = 0, seen_a0 = 0, seen_a1 = 0, seen_up = 0;
       if (x0 > 0 && !wait_seen(db_rows + y, x0, seen_own, pp.error, pp.timeout_ns)) failed = true;
@@ -2189,11 +2199,22 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
     }
     if (failed) break;
   }
+  if (lane == 0 && reach_y) {
+    atomicMax(pp.reach, reach_y);
+    atomicMax(pp.reach + 1, reach_x);
+  }
 }
 
-// The launch's error word into mapped host memory, queued after the launch (a kernel, not a copy:
-// a device-to-host copy waiting for a launch would stall later copies of the context).
-__global__ void error_to_host_kernel(const int* error, int* host_err) { st_release_sys(host_err, *error); }
+// The launch's error word (and the reach its reference waits saw) into mapped host memory, queued
+// after the launch (a kernel, not a copy: a device-to-host copy waiting for a launch would stall
+// later copies of the context).
+__global__ void error_to_host_kernel(const int* error, const int* reach, int* host_err, int* host_reach) {
+  if (host_reach) {
+    host_reach[0] = reach[0];
+    host_reach[1] = reach[1];
+  }
+  st_release_sys(host_err, *error);
+}
 
 // Border extension (enc.rs:165 extend_borders): every padding sample takes the value of the
 // nearest picture sample. One thread per 16-byte chunk of a padded row.
@@ -2347,7 +2368,7 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
                      size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
                      int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
-                     cudaStream_t st) {
+                     int* host_reach, cudaStream_t st) {
   int S = fp.n_streams, H = fp.mb_h;
   PipeParams pp;
   pp.ticket = counters;
@@ -2369,13 +2390,14 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.ready = ready;
   pp.seq = seq;
   pp.host_err = host_err;
+  pp.reach = pp.rows_done + frames * S;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;
   pipeline_kernel<<<g, 32, 0, st>>>(fp, d_streams, pp);
-  error_to_host_kernel<<<1, 1, 0, st>>>(pp.error, host_err);
+  error_to_host_kernel<<<1, 1, 0, st>>>(pp.error, pp.reach, host_err, host_reach);
 }
 
 size_t pipeline_counter_ints(const FrameParams& fp, int frames) {
-  return 4 + 2 * (size_t)frames * fp.n_streams * fp.mb_h + (size_t)frames * fp.n_streams;
+  return 4 + 2 * (size_t)frames * fp.n_streams * fp.mb_h + (size_t)frames * fp.n_streams + 2;
 }
 
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st) {

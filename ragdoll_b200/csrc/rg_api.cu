@@ -20,7 +20,7 @@ namespace {
 
 thread_local std::string g_last_error;
 
-constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the segment length
+constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the reach of the searches
 constexpr int kDefaultSeg = 1;   // macroblocks per work segment (16 warps per SM: 1 is 2 % faster than 2)
 // Deblocking SMs: one in five takes the deblocking queue first (30 of 148). Measured on B200 with
 // 16 warps per SM, 1080p 8 x 15 launch: 25 SMs 52.3-53.2 ms, 30 51.4-52.3, 35-40 52.6-52.8
@@ -144,6 +144,11 @@ struct rg_ctx {
   int* d_err = nullptr;            // the same, as the device sees it
   int grid = 0;
   int lag = kDefaultLag;           // macroblock-times between pictures of a stream in the work order
+  // Reach of the searches the lag is derived from when lag is 0 (macroblock rows / columns beyond
+  // zero motion): 4 until launches show otherwise; lowered only after kReachLowRuns launches that
+  // all reached less (a new work list costs ~50 ms of host time at 1080p x 120 pictures).
+  int reach_y = 4, reach_x = 4;
+  int reach_low = 0, low_y = 0, low_x = 0;
   int seg = kDefaultSeg;           // macroblocks per work segment
   unsigned long long timeout_ns = 2000000000ull;  // limit of one device wait
   int deblock_sms = 0;             // SMs preferring deblocking segments (0 = one mixed queue)
@@ -167,6 +172,7 @@ struct rg_ctx {
     rg_mb_out* out = nullptr;            // host copy queued by an asynchronous call, or null
     size_t out_bytes = 0;
     int* h_err = nullptr;                // mapped host: the launch's error word
+    int* h_reach = nullptr;              // mapped host: 1 + the reach its reference waits saw [2]
     cudaEvent_t done = nullptr;          // after the launch
   };
   Pending pend[2];
@@ -291,7 +297,7 @@ rg_ctx* rg_create(const rg_config* cfg) {
   }
   if (cudaMallocHost((void**)&c->h_streams[0], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
       cudaMallocHost((void**)&c->h_streams[1], sizeof(StreamDev) * c->S * c->max_frames) != cudaSuccess ||
-      cudaHostAlloc((void**)&c->h_err, 2 * sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostAlloc((void**)&c->h_err, 6 * sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer((void**)&c->d_err, c->h_err, 0) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->pend[0].done, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->pend[1].done, cudaEventDisableTiming) != cudaSuccess ||
@@ -302,9 +308,11 @@ rg_ctx* rg_create(const rg_config* cfg) {
     rg_destroy(c);
     return nullptr;
   }
-  c->h_err[0] = c->h_err[1] = 0;
+  for (int k = 0; k < 6; k++) c->h_err[k] = 0;
   c->pend[0].h_err = c->h_err;
   c->pend[1].h_err = c->h_err + 1;
+  c->pend[0].h_reach = c->h_err + 2;
+  c->pend[1].h_reach = c->h_err + 4;
   c->grid = pipeline_grid(cfg->device);
   c->sms = pipeline_sms(cfg->device);
   c->deblock_sms = default_deblock_sms(c->sms);
@@ -382,6 +390,7 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
                              const int32_t* kinds, rg_mb_out* rec_base, int only = -1);
 static int resolve_pending(rg_ctx* c, bool wait_out);
 static int resolve_oldest(rg_ctx* c);
+static int auto_lag(const rg_ctx* c);
 
 int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                             const int32_t* kinds) {
@@ -523,17 +532,18 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   // IDR pictures get their own queue when SMs are set aside for them
   std::vector<int32_t> kinds_key;
   if (c->intra_sms > 0 && c->grid >= 3) kinds_key.assign(kinds, kinds + (size_t)frames * S);
-  if (frames != c->tasks_frames || c->lag != c->tasks_lag || c->seg != c->tasks_seg || split != c->tasks_split ||
+  const int lag = c->lag > 0 ? c->lag : auto_lag(c);
+  if (frames != c->tasks_frames || lag != c->tasks_lag || c->seg != c->tasks_seg || split != c->tasks_split ||
       kinds_key != c->tasks_kinds) {
     // rebuilt only when the call's shape, its picture kinds or the tuning change; the copy is
     // stream-ordered after any launch still reading the old list
     c->h_tasks.resize(pipeline_task_count(fp, frames, c->seg));
-    c->n_tasks = pipeline_task_list(fp, frames, c->lag, c->seg, split != 0,
+    c->n_tasks = pipeline_task_list(fp, frames, lag, c->seg, split != 0,
                                     kinds_key.empty() ? nullptr : kinds_key.data(), c->h_tasks.data(), c->qbeg, c->qend);
     c->tasks_kinds = kinds_key;
     CK(cudaMemcpyAsync(c->d_tasks, c->h_tasks.data(), sizeof(int2) * c->n_tasks, cudaMemcpyHostToDevice, c->stream));
     c->tasks_frames = frames;
-    c->tasks_lag = c->lag;
+    c->tasks_lag = lag;
     c->tasks_seg = c->seg;
     c->tasks_split = split;
   }
@@ -544,7 +554,8 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   rg_ctx::Pending& p = c->pend[pslot];
   *(volatile int*)p.h_err = 0;  // the launch that used this word before was resolved
   launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->qbeg, c->qend, c->deblock_sms,
-                  c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq, c->d_err + pslot, c->stream);
+                  c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq, c->d_err + pslot,
+                  c->d_err + 2 + 2 * pslot, c->stream);
   CK(cudaGetLastError());
   CK(cudaEventRecord(p.done, c->stream));
   p.planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
@@ -600,6 +611,8 @@ int rg_set_pipeline_tuning(rg_ctx* c, const rg_pipeline_tuning* t) {
     c->tasks_cap = need;
   }
   c->lag = lag > 0 ? lag : kDefaultLag;
+  c->reach_y = c->reach_x = 4;
+  c->reach_low = 0;
   c->seg = new_seg;
   c->deblock_sms = deblock_sms < 0 ? 0 : (deblock_sms > 0 ? deblock_sms : default_deblock_sms(c->sms));
   c->intra_sms = intra_sms < 0 ? 0 : (intra_sms > 0 ? intra_sms : default_intra_sms(c->sms));
@@ -608,6 +621,11 @@ int rg_set_pipeline_tuning(rg_ctx* c, const rg_pipeline_tuning* t) {
   else c->grid = pipeline_grid(c->cfg.device);
   c->timeout_ns = timeout_ms > 0 ? (unsigned long long)timeout_ms * 1000000ull : 2000000000ull;
   return RG_OK;
+}
+
+int32_t rg_pipeline_lag(const rg_ctx* c) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_pipeline_lag: null context");
+  return c->lag > 0 ? c->lag : auto_lag(c);
 }
 
 // One source picture (host planes pl[3]) into device staging d (Y | U | V, unpadded rows): one copy
@@ -653,6 +671,42 @@ int rg_analyse_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, si
   return rg_sync(c);
 }
 
+// Picture lag of the work order when none is set: the smallest under which no wait for the
+// reference picture goes to a later segment of the work list, for the reach the context's searches
+// have shown (the bound of pipeline_task_list: lag >= max(seg, 2) * (4 + rows) + seg + columns + 3).
+// With reach 4 x 4 (about 64 samples) this is the work list's own default. A search reaching
+// further only waits longer; if a wait gives up, the call is re-run exactly.
+static int auto_lag(const rg_ctx* c) {
+  const int a = c->seg > 2 ? c->seg : 2;
+  return a * (4 + c->reach_y) + c->seg + c->reach_x + 3;
+}
+
+constexpr int kReachLowRuns = 4;
+
+// The reach a completed launch's reference waits saw (1 + macroblocks, 0 = none): a larger one
+// raises the derived lag at once; a smaller one lowers it after kReachLowRuns launches in a row,
+// to the largest of them.
+static void observe_reach(rg_ctx* c, int oy, int ox) {
+  if (oy <= 0) return;  // no P picture waited for a reference picture in that launch
+  oy--;
+  ox = ox > 0 ? ox - 1 : 0;
+  if (oy > c->reach_y || ox > c->reach_x) {
+    c->reach_y = std::max(c->reach_y, oy);
+    c->reach_x = std::max(c->reach_x, ox);
+    c->reach_low = 0;
+  } else if (oy == c->reach_y && ox == c->reach_x) {
+    c->reach_low = 0;
+  } else {
+    c->low_y = c->reach_low ? std::max(c->low_y, oy) : oy;
+    c->low_x = c->reach_low ? std::max(c->low_x, ox) : ox;
+    if (++c->reach_low >= kReachLowRuns) {
+      c->reach_y = c->low_y;
+      c->reach_x = c->low_x;
+      c->reach_low = 0;
+    }
+  }
+}
+
 // Resolves the oldest pending pipelined call: waits for its launch and, if a wait of it gave up
 // (a search reaching further than the picture lag allows, or another warp failing), re-runs it,
 // picture by picture, on the per-diagonal path, which has no waits: each picture wrote its own
@@ -662,11 +716,17 @@ static int resolve_oldest(rg_ctx* c) {
   if (!c->pend_count) return RG_OK;
   rg_ctx::Pending& p = c->pend[c->pend_head];
   CK(cudaEventSynchronize(p.done));
+  const int oy = ((volatile int*)p.h_reach)[0], ox = ((volatile int*)p.h_reach)[1];
   if (*(volatile int*)p.h_err == 0) {
+    observe_reach(c, oy, ox);
     c->pend_head ^= 1;
     c->pend_count--;
     return RG_OK;
   }
+  // a wait gave up: order the next launches for at least the reach it saw, and no less than 4
+  c->reach_y = std::max(std::max(c->reach_y, oy - 1), 4);
+  c->reach_x = std::max(std::max(c->reach_x, ox - 1), 4);
+  c->reach_low = 0;
   CK(cudaStreamSynchronize(c->stream));
   if (c->a_out) CK(cudaStreamSynchronize(c->a_out));  // its copy of the failed records may still run
   int S = c->S;

@@ -23,6 +23,7 @@ class H264Encoder:
     def __init__(self, width: int, height: int, qp: int, profile: int = RG_PROFILE_HIGH, fps=(30, 1),
                  keyint: int = 30, streams: int = 1, max_frames: int = 1, device: int = 0, threads: int = 0):
         cfg = RgConfig(width, height, profile, qp, streams, device, max_frames)
+        self._destroy = lib().rg_encoder_destroy  # kept: the module's globals may go first at exit
         self.h = lib().rg_encoder_create(ctypes.byref(cfg), fps[0], fps[1], keyint, threads)
         if not self.h:
             raise RgError(-1, lib().rg_last_error().decode())
@@ -117,7 +118,7 @@ class H264Encoder:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            lib().rg_encoder_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):

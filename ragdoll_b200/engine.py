@@ -38,7 +38,7 @@ EXPORTS = [
     "rg_analyse_batch", "rg_analyse_batch_device", "rg_sync", "rg_copy_records", "rg_get_recon",
     "rg_get_recon_unfiltered", "rg_get_recon_coded", "rg_keep_unfiltered", "rg_cuda_stream",
     "rg_quality_frame", "rg_ssim_plane", "rg_ssim_plane_device_noalloc", "rg_analyse_gops",
-    "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_analyse_gops_async",
+    "rg_analyse_gops_device", "rg_copy_records_gops", "rg_set_pipeline_tuning", "rg_pipeline_lag", "rg_analyse_gops_async",
     "rg_writer_create", "rg_writer_destroy", "rg_writer_bound", "rg_writer_picture", "rg_pipeline_work_list",
     "rg_mux_create", "rg_mux_destroy", "rg_mux_write", "rg_mux_finish", "rg_demux_open", "rg_demux_destroy",
     "rg_demux_info", "rg_demux_access_unit", "rg_analyse_gops_wait", "rg_encoder_create", "rg_encoder_destroy",
@@ -130,6 +130,8 @@ def lib() -> ctypes.CDLL:
     L.rg_writer_picture.restype = ctypes.c_int64
     L.rg_writer_picture.argtypes = [P, P, ctypes.c_int32, P, ctypes.c_size_t]
     L.rg_set_pipeline_tuning.argtypes = [P, ctypes.POINTER(RgPipelineTuning)]
+    L.rg_pipeline_lag.restype = ctypes.c_int32
+    L.rg_pipeline_lag.argtypes = [P]
     L.rg_ssim_plane_device_noalloc.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                                ctypes.c_int32, P, P]
     L.rg_analyse_gops_wait.argtypes = [P, P]
@@ -194,6 +196,8 @@ class Engine:
         if not h:
             raise RgError(-1, lib().rg_last_error().decode())
         self.h = h
+        # kept on the instance: a context closed as the interpreter exits may outlive the module's globals
+        self._destroy = lib().rg_destroy
         mw, mh = ctypes.c_int32(), ctypes.c_int32()
         _check(lib().rg_mb_dims(h, ctypes.byref(mw), ctypes.byref(mh)))
         self.mb_w, self.mb_h = mw.value, mh.value
@@ -201,7 +205,7 @@ class Engine:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            lib().rg_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -299,6 +303,13 @@ class Engine:
         t = RgPipelineTuning(lag, seg, grid, timeout_ms, deblock_sms, intra_sms)
         _check(lib().rg_set_pipeline_tuning(self.h, ctypes.byref(t)))
 
+    def pipeline_lag(self) -> int:
+        """The picture lag the next pipelined launch uses: the set one, or with lag 0 the one
+        derived from the reach of the searches of the launches so far."""
+        r = lib().rg_pipeline_lag(self.h)
+        _check(r if r < 0 else 0)
+        return r
+
     def records_gops(self, frames: int) -> np.ndarray:
         out = np.zeros((frames, self.num_streams, self.n_mb), RECORD_DTYPE)
         _check(lib().rg_copy_records_gops(self.h, frames, out.ctypes.data))
@@ -395,6 +406,7 @@ class BitstreamWriter:
 
     def __init__(self, width: int, height: int, qp: int, fps=(30, 1), profile: int = RG_PROFILE_BASELINE):
         cfg = RgConfig(width, height, profile, qp, 1, 0, 1)
+        self._destroy = lib().rg_writer_destroy  # kept: the module's globals may go first at exit
         self.h = lib().rg_writer_create(ctypes.byref(cfg), fps[0], fps[1])
         if not self.h:
             raise RgError(-1, lib().rg_last_error().decode())
@@ -409,7 +421,7 @@ class BitstreamWriter:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            lib().rg_writer_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     def __del__(self):

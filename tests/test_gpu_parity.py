@@ -287,3 +287,33 @@ def test_source_layouts_give_the_same_records():
     ref = got["planes/sync"]
     for k, v in got.items():
         assert v.tobytes() == ref.tobytes(), k
+
+
+def test_derived_lag_follows_the_reach_of_the_searches():
+    """With lag 0 the work order's picture lag follows the reach of the searches: 24 (reach 4 x 4,
+    one-macroblock segments) for the first launch, 12 (no reach beyond zero motion) after four
+    launches of still pictures, raised at once by a launch with motion. The records and the
+    deblocked references equal those of a context with the lag fixed at 24."""
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, Engine
+
+    w, h, qp, S, F = 176, 144, 26, 2, 4
+    still = [grating_clip(w, h, 1, seed=300 + s, motion=0.0, rects=0)[0] for s in range(S)]
+    moving = [grating_clip(w, h, F, seed=310 + s, motion=24.0, rects=2) for s in range(S)]
+    auto = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+    fixed = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+    fixed.set_pipeline_tuning(lag=24)
+    assert auto.pipeline_lag() == 24 and fixed.pipeline_lag() == 24
+    calls = [([[still[s] for s in range(S)]] * F, [[RG_FRAME_IDR] * S] + [[RG_FRAME_P] * S] * (F - 1))]
+    calls += [([[still[s] for s in range(S)]] * F, [[RG_FRAME_P] * S] * F)] * 3
+    calls += [([[moving[s][f] for s in range(S)] for f in range(F)], [[RG_FRAME_P] * S] * F)]
+    lags = []
+    for pics, kinds in calls:
+        a = auto.analyse_gops(pics, kinds)
+        b = fixed.analyse_gops(pics, kinds)
+        assert a.tobytes() == b.tobytes()
+        lags.append(auto.pipeline_lag())
+    assert lags[:3] == [24, 24, 24] and lags[3] == 12, lags
+    assert lags[4] > 12, lags
+    assert fixed.pipeline_lag() == 24
+    for s in range(S):
+        assert all(np.array_equal(x, y) for x, y in zip(auto.recon_coded(s), fixed.recon_coded(s)))
