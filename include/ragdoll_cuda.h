@@ -226,8 +226,8 @@ typedef struct rg_pipeline_tuning {
  * of a stream in the work order (1..4096; 0 = derived from the searches: max(seg, 2) * (4 + ry)
  * + seg + rx + 3, which orders every wait of a search reaching up to ry macroblock rows and rx
  * columns beyond zero motion after the work it waits for; ry = rx = 4 until the context's
- * launches have shown their reach, raised as soon as a launch reaches further, lowered after four
- * launches in a row that all reached less; larger is safer for long motion, smaller favours newer
+ * launches have shown their reach, raised as soon as a launch reaches further, lowered after two
+ * launches in a row that both reached less; larger is safer for long motion, smaller favours newer
  * pictures), seg = macroblocks per
  * work segment (1..mb_w, 0 = 1), grid = resident warps (0 = sixteen per SM, fewer if they do not
  * fit), timeout_ms = limit of one device wait (0 = 2000), deblock_sms = SMs whose warps take

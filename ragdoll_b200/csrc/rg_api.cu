@@ -146,7 +146,7 @@ struct rg_ctx {
   int lag = kDefaultLag;           // macroblock-times between pictures of a stream in the work order
   // Reach of the searches the lag is derived from when lag is 0 (macroblock rows / columns beyond
   // zero motion): 4 until launches show otherwise; lowered only after kReachLowRuns launches that
-  // all reached less (a new work list costs ~50 ms of host time at 1080p x 120 pictures).
+  // all reached less (a new work list costs ~10 ms of host time at 1080p x 120 pictures).
   int reach_y = 4, reach_x = 4;
   int reach_low = 0, low_y = 0, low_x = 0;
   int seg = kDefaultSeg;           // macroblocks per work segment
@@ -681,7 +681,7 @@ static int auto_lag(const rg_ctx* c) {
   return a * (4 + c->reach_y) + c->seg + c->reach_x + 3;
 }
 
-constexpr int kReachLowRuns = 4;
+constexpr int kReachLowRuns = 2;
 
 // The reach a completed launch's reference waits saw (1 + macroblocks, 0 = none): a larger one
 // raises the derived lag at once; a smaller one lowers it after kReachLowRuns launches in a row,
