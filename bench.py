@@ -49,8 +49,8 @@ METRIC = "1080p H.264 encode frames/s (plain GPU form)"
 UNIT = "frames/s"
 BYTES_PER_FRAME = 7.5 * W * H  # source 1.5 + reference 1.5 + recon 1.5 + deblock read/write 3.0 (x W*H)
 # DRAM bytes per picture of pipeline_kernel measured by ncu (dram__bytes_read + write) on a launch
-# of 8 streams x 4 pictures of this workload: 521.3 MB / 32 (scaled to a launch by its pictures).
-TRAFFIC_PER_FRAME = 521.3e6 / 32
+# of 8 streams x 4 pictures of this workload: 490.2 MB / 32 (scaled to a launch by its pictures).
+TRAFFIC_PER_FRAME = 490.2e6 / 32
 
 
 def dist_env():
