@@ -133,13 +133,15 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------------
-def oracle_gops(clip, gops: int, frames_per_gop: int, threads: int) -> float:
-    """Encodes `gops` GOPs of the clip with the oracle on `threads` host threads; returns seconds."""
+def oracle_gops(clip, gops: int, frames_per_gop: int, threads: int, keep: bool = False):
+    """Encodes `gops` GOPs of the clip with the oracle on `threads` host threads. Returns the
+    seconds taken and (keep=True) each GOP's access units."""
     sys.path.insert(0, str(ROOT / "tests"))
     from oracle_lib import OracleEncoder
 
     work = list(range(gops))
     lock = threading.Lock()
+    aus = [None] * gops
 
     def worker():
         while True:
@@ -147,9 +149,13 @@ def oracle_gops(clip, gops: int, frames_per_gop: int, threads: int) -> float:
                 if not work:
                     return
                 g = work.pop(0)
-            enc = OracleEncoder(W, H, QP, profile=2, keyint=GOP + 1)
+            enc = OracleEncoder(W, H, QP, profile=2, keyint=GOP)
+            out = []
             for i in range(frames_per_gop):
-                enc.encode(clip[g * GOP + i])
+                au, _ = enc.encode(clip[g * GOP + i])
+                if keep:
+                    out.append(au)
+            aus[g] = out
 
     t0 = time.perf_counter()
     ts = [threading.Thread(target=worker) for _ in range(min(threads, gops))]
@@ -157,24 +163,38 @@ def oracle_gops(clip, gops: int, frames_per_gop: int, threads: int) -> float:
         t.start()
     for t in ts:
         t.join()
-    return time.perf_counter() - t0
+    return time.perf_counter() - t0, aus
 
 
-def oracle_sample(clip, gops: int, fpg: int, cores: int) -> dict:
-    """The CPU figures beside the GPU numbers: the oracle GOP-parallel on `cores` threads over
-    `gops` GOPs x `fpg` frames, the same on one thread over one GOP, and the integer work the
-    oracle's decisions evaluate per frame (pixel differences of every SAD / SSD / SATD)."""
+def oracle_sample(clip, gops: int, cores: int) -> dict:
+    """The CPU figures beside the GPU numbers: the oracle encoding the whole step (every GOP, all
+    its pictures) GOP-parallel on the host cores, the same for one GOP on one thread, and the
+    integer work the oracle's decisions evaluate per frame (pixel differences of every SAD / SSD /
+    SATD). Also returns the oracle's access units of the step (key "aus", [g][f]) for the parity
+    check of the GPU's bitstream."""
     sys.path.insert(0, str(ROOT / "tests"))
     from oracle_lib import pixel_ops
     pixel_ops(reset=True)
-    t = oracle_gops(clip, gops, fpg, cores)
+    t, aus = oracle_gops(clip, gops, GOP, cores, keep=True)
     ops = pixel_ops(reset=True)
-    t1 = oracle_gops(clip, 1, fpg, 1)
-    return {"value": round(gops * fpg / t, 3), "unit": UNIT, "cores": min(cores, gops), "kind": "port",
-            "single_thread": round(fpg / t1, 3),
-            "oracle_pixel_ops_per_frame": round(ops / (gops * fpg)),
-            "sample": f"{gops} GOPs x {fpg} frames (IDR + P) of the clip, oracle GOP-parallel; "
-                      f"single_thread: 1 GOP x {fpg} frames on one thread"}
+    t1, _ = oracle_gops(clip, 1, GOP, 1)
+    return {"value": round(gops * GOP / t, 3), "unit": UNIT, "cores": min(cores, gops), "host_cores": cores,
+            "kind": "port", "single_thread": round(GOP / t1, 3),
+            "oracle_pixel_ops_per_frame": round(ops / (gops * GOP)),
+            "sample": f"the whole step: {gops} GOPs x {GOP} frames (IDR + {GOP - 1} P), one oracle encoder per "
+                      f"GOP on {min(cores, gops)} threads ({cores} host cores; one thread per GOP); "
+                      f"single_thread: 1 GOP x {GOP} frames on one thread",
+            "aus": aus}
+
+
+def bitstream_digest(aus_by_gop) -> str:
+    """SHA-256 of the GOPs' access units, GOP by GOP in display order."""
+    import hashlib
+    h = hashlib.sha256()
+    for g in aus_by_gop:
+        for au in g:
+            h.update(au)
+    return h.hexdigest()
 
 
 BATCH_SIZES = [(320, 240), (640, 360), (1280, 720), (1920, 1080)]
@@ -295,28 +315,35 @@ def run_batched(args, rank, world, local):
 
 
 def run_reference(args, rank, world):
-    """CPU arm: the oracle (C++ restatement of ragdoll's Balanced encoder) on the host cores."""
+    """CPU arm: the oracle (C++ restatement of ragdoll's Balanced encoder) on the host cores, each
+    step the whole workload -- 8 GOPs x 15 pictures, one oracle encoder per GOP (parallel_gop_map
+    semantics: as many threads as GOPs, up to the host's cores)."""
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    gops, fpg = FRAMES // GOP, 3  # bounded sample: 3 frames (IDR + 2 P) of each of the 8 GOPs
+    gops = FRAMES // GOP
     clip = make_clip(2000, FRAMES)
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_lib import pixel_ops
     for _ in range(args.warmup):
         oracle_gops(clip, gops, 1, cores)
-    times = [oracle_gops(clip, gops, fpg, cores) for _ in range(args.steps)]
+    pixel_ops(reset=True)
+    times = [oracle_gops(clip, gops, GOP, cores)[0] for _ in range(args.steps)]
+    ops = pixel_ops(reset=True)
     t = statistics.median(times)
-    value = gops * fpg / t
-    sample = oracle_sample(clip, gops, fpg, cores)
+    value = gops * GOP / t
+    t1, _ = oracle_gops(clip, 1, GOP, 1)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
         "config": bench_config(world),
-        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": min(cores, gops), "kind": "port",
-                         "single_thread": sample["single_thread"],
-                         "oracle_pixel_ops_per_frame": sample["oracle_pixel_ops_per_frame"],
-                         "sample": f"{gops} GOPs x {fpg} frames of the 1080p clip, GOP-parallel; "
-                                   f"single_thread: 1 GOP x {fpg} frames on one thread"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": min(cores, gops), "host_cores": cores,
+                         "kind": "port", "single_thread": round(GOP / t1, 3),
+                         "oracle_pixel_ops_per_frame": round(ops / (args.steps * gops * GOP)),
+                         "sample": f"each step the whole workload: {gops} GOPs x {GOP} frames, one oracle encoder per "
+                                   f"GOP on {min(cores, gops)} threads ({cores} host cores); single_thread: 1 GOP "
+                                   f"x {GOP} frames on one thread"},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -455,7 +482,8 @@ def run_engine(args, rank, world, local):
         enc.submit(frames_host)
         if k:
             out_bytes += sum(len(au) for row in enc.collect() for au in row)
-    out_bytes += sum(len(au) for row in enc.collect() for au in row)
+    last_aus = enc.collect()
+    out_bytes += sum(len(au) for row in last_aus for au in row)
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps, dist, f"cuda:{local}")
     enc_threads = enc.threads
     enc.close()
@@ -485,9 +513,15 @@ def run_engine(args, rank, world, local):
     # hands its error word to the host; per-diagonal mode: the diagonal steps and the padding
     launches = args.steps * (2 if args.mode == "pipelined" else launches_per_step)
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = oracle_sample(clip, gops, 2, os.cpu_count() or 1)
+        # outside the timed regions: the oracle encodes the same step, which is both the CPU
+        # baseline and the parity check of the step's bitstream (every access unit of every GOP)
+        cpu = oracle_sample(clip, gops, os.cpu_count() or 1)
+        want = bitstream_digest(cpu.pop("aus"))
+        got = bitstream_digest([[last_aus[f][g] for f in range(GOP)] for g in range(gops)])
+        parity = {"bitstream_equals_oracle": got == want, "sha256": got,
+                  "checked": f"every access unit of the last timed e2e step ({gops} GOPs x {GOP} pictures)"}
 
     if rank == 0:
         line = {
@@ -496,7 +530,7 @@ def run_engine(args, rank, world, local):
             "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
             "config": bench_config(world, args.mode),
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
-                    "d2h_bytes_per_step": GOP * gops * eng.n_mb * 852,
+                    "d2h_bytes_per_step": GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize,
                     "bitstream_bytes_per_step": round(out_bytes / args.steps),
                     "host_threads": enc_threads,
                     "path": "rg_encoder_submit/collect: copy in, persistent launch, records out, CABAC on the host"},
@@ -508,6 +542,7 @@ def run_engine(args, rank, world, local):
                          "kernel": kernel_name, "launch_ms": round(launch_ms, 5),
                          "bytes_per_launch": round(bytes_per_launch)},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clk,
             "gpu_launches": launches,
         }

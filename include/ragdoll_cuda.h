@@ -312,7 +312,9 @@ int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8
  * reference: it exists for callers that may not call cudaMalloc / cudaFree when they measure --
  * a frame loop whose device memory is all reserved by another allocator (a framework's caching
  * pool), or a latency-critical loop where an allocation would synchronise the device and stall
- * its other streams. Results equal rg_ssim_plane's (same arithmetic order).
+ * its other streams. SSIM is bit-identical to rg_ssim_plane's (same f32 row order); MS-SSIM is
+ * combined on the device (pow / fmin / fmax there, std::pow on the host in rg_ssim_plane) and
+ * agrees with rg_ssim_plane's within 1e-6.
  *
  * dev_a / dev_b: device planes (8-bit, given strides); dev_out: caller-owned device memory for two
  * doubles, written as {SSIM, MS-SSIM}; cuda_stream: the cudaStream_t to run on (NULL = legacy
@@ -323,8 +325,10 @@ int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8
  * and at most 1920 x 1088 samples; larger ones get RG_ERR_INVALID (use rg_ssim_plane). Every call
  * on a device shares that array: calls that overlap on the GPU (other streams, other threads)
  * race and must be serialised by the caller. The first call on each device looks the array up
- * (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture begins.
+ * (cudaGetSymbolAddress) with that device current and keeps the address for the life of the
+ * process; make that first call before any stream capture begins. Resetting a device
+ * (cudaDeviceReset, or any teardown of its primary context) after that first call is not
+ * supported: the kept address and the kernel's shared-memory attribute would be stale.
  */
 int rg_ssim_plane_device_noalloc(const uint8_t* dev_a, size_t stride_a, const uint8_t* dev_b,
                                  size_t stride_b, int32_t width, int32_t height, double* dev_out,

@@ -1237,9 +1237,9 @@ struct Encoder {
     return cbp;
   }
   // enc.rs:2041 quant_luma_8x8_inter -> cbp8, q8 (raster per 8x8 block)
-  int quant_luma_8x8(const uint8_t* src, const uint8_t* pred, int q_, int16_t q8[4][64]) const {
+  static int quant_luma_8x8(const uint8_t* src, const uint8_t* pred, int q_, int16_t q8[4][64], bool fine = false) {
     int qq = std::min(q_, 51);
-    uint32_t shift = 16 + qq / 6, bias = (1u << shift) / 6;
+    uint32_t shift = 16 + qq / 6, bias = (1u << shift) / (fine ? 3 : 6);
     int cbp = 0; uint32_t total = 0;
     for (int b = 0; b < 4; b++) {
       int o = (b >> 1) * 128 + (b & 1) * 8;
@@ -2345,6 +2345,24 @@ int oracle_record_size(void) { return (int)sizeof(rg_mb_out); }
 // process (all threads); reset = 1 also sets the total back to 0.
 unsigned long long oracle_pixel_ops(int reset) {
   return reset ? oracle::g_pixel_ops.exchange(0) : oracle::g_pixel_ops.load();
+}
+
+// Kernels behind the reference's own property tests (crates/ragdoll-codec/src/h264/enc.rs:4119
+// transform_8x8_paths_match_the_reference, :4189 decimation_scores_follow_x264), exposed so the
+// tests can restate them against this oracle.
+// decimate_score (enc.rs:559) of n = 16 or 64 levels in zig-zag order.
+unsigned oracle_decimate_score(const int16_t* zz, int n) { return oracle::decimate_score(zz, n == 64 ? 64 : 16); }
+// quant_luma_8x8_inter (enc.rs:2041) of a 16x16 source / prediction pair (stride 16): raster levels
+// of the four 8x8 blocks into q8 (4 x 64), returns cbp8; fine = the intra rounding (f = 2^s / 3).
+int oracle_quant_luma_8x8(const uint8_t* src, const uint8_t* pred, int qp, int fine, int16_t* q8) {
+  return oracle::Encoder::quant_luma_8x8(src, pred, qp, (int16_t(*)[64])q8, fine != 0);
+}
+// recon_8x8 (enc.rs:2020): dequantises 64 raster levels (dequantize_block8x8, h264.rs:1403) and adds
+// their inverse transform (h264_idct8_add, h264_idct.rs:207) onto dst (stride).
+void oracle_recon_8x8(uint8_t* dst, int stride, const int16_t* levels, int qp) {
+  int32_t d[64];
+  oracle::dequant8(levels, qp, d);
+  oracle::idct8_add(dst, stride, d);
 }
 
 }  // extern "C"

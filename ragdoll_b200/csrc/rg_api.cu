@@ -682,10 +682,15 @@ static int auto_lag(const rg_ctx* c) {
 }
 
 constexpr int kReachLowRuns = 2;
+// The derived reach never goes below one macroblock row and column beyond zero motion: a diamond
+// of at most 16 one-sample steps from still candidates reaches 16 samples further, so the first
+// launch with motion after still pictures stays within the order's bound instead of waiting for
+// segments no warp has taken (and re-running after the wait limit).
+constexpr int kReachFloor = 1;
 
 // The reach a completed launch's reference waits saw (1 + macroblocks, 0 = none): a larger one
 // raises the derived lag at once; a smaller one lowers it after kReachLowRuns launches in a row,
-// to the largest of them.
+// to the largest of them (not below kReachFloor).
 static void observe_reach(rg_ctx* c, int oy, int ox) {
   if (oy <= 0) return;  // no P picture waited for a reference picture in that launch
   oy--;
@@ -700,8 +705,8 @@ static void observe_reach(rg_ctx* c, int oy, int ox) {
     c->low_y = c->reach_low ? std::max(c->low_y, oy) : oy;
     c->low_x = c->reach_low ? std::max(c->low_x, ox) : ox;
     if (++c->reach_low >= kReachLowRuns) {
-      c->reach_y = c->low_y;
-      c->reach_x = c->low_x;
+      c->reach_y = std::max(c->low_y, kReachFloor);
+      c->reach_x = std::max(c->low_x, kReachFloor);
       c->reach_low = 0;
     }
   }
