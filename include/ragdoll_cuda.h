@@ -63,6 +63,12 @@ typedef struct rg_config {
 #define RG_MB_P_L0_16X16 1
 #define RG_MB_I16X16 2
 #define RG_MB_I4X4 3
+/* Partitioned inter macroblocks, coded only by the search forms (rg_set_analysis_form): two 16x8
+ * or 8x16 partitions, or four 8x8 sub-macroblocks (P_8x8, every sub_mb_type P_L0_8x8). Their
+ * vectors are part_mv / part_mvd below. */
+#define RG_MB_P_L0_16X8 4
+#define RG_MB_P_L0_8X16 5
+#define RG_MB_P_8X8 6
 
 /*
  * One macroblock's decisions and levels, everything the entropy coder reads
@@ -87,6 +93,16 @@ typedef struct rg_mb_out {
     int16_t luma_dc[16];   /* Intra16x16 DC levels, zig-zag                                     */
     int16_t chroma_dc[2][4];
     int16_t chroma_ac[2][4][16]; /* zig-zag; slot 0 (the DC position) is unused              */
+    /* Written by the search forms only (zero in the plain form): the vector of each 8x8 quadrant
+     * (raster order: top-left, top-right, bottom-left, bottom-right), the vector differences of
+     * the partitions in coding order (16x8: top, bottom; 8x16: left, right; 8x8: the four
+     * sub-macroblocks; one for 16x16), and the partition type the search found cheapest before
+     * the skip and intra decisions (0 16x16, 1 16x8, 2 8x16, 3 8x8; 255 when not searched) --
+     * the label the learned form's network is trained on. */
+    int16_t part_mv[4][2];
+    int16_t part_mvd[4][2];
+    uint8_t part_type;
+    uint8_t reserved2[3];
 } rg_mb_out;
 
 /* Quality of a reconstruction against its source (QualityReport, crates/ragdoll-pix/src/metrics.rs:13;
@@ -243,6 +259,50 @@ int rg_set_pipeline_tuning(rg_ctx* ctx, const rg_pipeline_tuning* tuning);
  * from the reach of its searches); negative RG_ERR_* on a null context. No counterpart in the
  * reference. */
 int32_t rg_pipeline_lag(const rg_ctx* ctx);
+
+/* ---- analysis forms ------------------------------------------------------------------------ */
+/*
+ * Two forms beside the plain one (the Balanced preset, byte-identical to the reference), neither
+ * of which exists in the reference; both need CABAC (Main / High profile):
+ *
+ * RG_FORM_FULLSEARCH: P macroblocks search every integer vector within +-search_range samples of
+ *   the 16x16 predictor (the sum of absolute differences of each 8x8 quadrant at every position,
+ *   plus lambda times the vector bits), refine the best vector of every partition of the four
+ *   partition types (16x16, 16x8, 8x16, 8x8) to quarter samples by SATD with each partition's own
+ *   predictor, and code the type of least cost. Intra and the residual follow the plain form.
+ * RG_FORM_LEARNED: the same decisions restricted by a per-macroblock hint (rg_mb_hint, from the
+ *   candidate network of rg_predict_hints): the integer search covers +-2 samples around the
+ *   predictor plus the hinted offset (the full +-search_range search when the best vector lies on
+ *   that window's edge), only the hinted partition types are refined, and intra 4x4 blocks of IDR
+ *   pictures try only their hinted prediction modes.
+ */
+#define RG_FORM_PLAIN 0
+#define RG_FORM_FULLSEARCH 1
+#define RG_FORM_LEARNED 2
+
+/* Per-macroblock hint of the learned form (raster order, one per macroblock of a picture). */
+typedef struct rg_mb_hint {
+    uint8_t part_mask;      /* bit t: partition type t is tried (t as rg_mb_out.part_type)       */
+    uint8_t reserved;
+    int8_t mv_off[2];       /* offset of the integer search's centre from the 16x16 predictor,
+                               quarter samples                                                   */
+    uint16_t i4_mask[16];   /* bit m: Intra4x4PredMode m is tried for 4x4 block b (decoding order) */
+} rg_mb_hint;
+
+/*
+ * Selects the analysis form of the context's next calls (RG_FORM_*) and the integer search range
+ * of the search forms (1..128 samples; ignored by the plain form). The learned form needs hints
+ * for every analysed picture (rg_set_hints). Returns RG_ERR_UNSUPPORTED for a search form in a
+ * Baseline (CAVLC) context. No counterpart in the reference.
+ */
+int rg_set_analysis_form(rg_ctx* ctx, int32_t form, int32_t search_range);
+
+/*
+ * Device hints of the learned form for the next pipelined or batched call: dev_hints[f * S + s] is
+ * the device address of picture f of stream s's mb_w * mb_h rg_mb_hint records (the order of the
+ * call's planes). They must stay valid until the call is resolved. No counterpart in the reference.
+ */
+int rg_set_hints(rg_ctx* ctx, const rg_mb_hint* const* dev_hints, int32_t count);
 
 /* Waits for queued device work of the context. */
 int rg_sync(rg_ctx* ctx);

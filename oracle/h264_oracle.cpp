@@ -275,6 +275,23 @@ static uint32_t satd4(const uint8_t* a, int sa, const uint8_t* b, int sb) {
   }
   return s >> 1;
 }
+// The unhalved sum of one 4x4 transform (the search forms halve the sum over a partition's blocks).
+static uint32_t satd4_raw(const uint8_t* a, int sa, const uint8_t* b, int sb) {
+  t_pixel_ops += 16;
+  int t[4][4];
+  for (int y = 0; y < 4; y++) {
+    int d0 = a[y * sa] - b[y * sb], d1 = a[y * sa + 1] - b[y * sb + 1];
+    int d2 = a[y * sa + 2] - b[y * sb + 2], d3 = a[y * sa + 3] - b[y * sb + 3];
+    int s03 = d0 + d3, s12 = d1 + d2, d03 = d0 - d3, d12 = d1 - d2;
+    t[y][0] = s03 + s12; t[y][1] = d03 + d12; t[y][2] = s03 - s12; t[y][3] = d03 - d12;
+  }
+  uint32_t s = 0;
+  for (int x = 0; x < 4; x++) {
+    int s03 = t[0][x] + t[3][x], s12 = t[1][x] + t[2][x], d03 = t[0][x] - t[3][x], d12 = t[1][x] - t[2][x];
+    s += iabs(s03 + s12) + iabs(d03 + d12) + iabs(s03 - s12) + iabs(d03 - d12);
+  }
+  return s;
+}
 // h264_enc.rs:167 pixel_satd_16x16_scalar (sum of 4x4 transforms, halved once)
 static uint32_t satd16(const uint8_t* a, int sa, const uint8_t* b, int sb) {
   t_pixel_ops += 256;
@@ -1367,11 +1384,13 @@ struct Encoder {
       for (int mbx = 0; mbx < mb_w; mbx++) {
         int m = mby * mb_w + mbx;
         auto same_mv = [&](int ox, int oy) { return mv_of(ox, oy, 0) == mv_of(mbx, mby, 0) && mv_of(ox, oy, 1) == mv_of(mbx, mby, 1); };
-        if (quiet(m) && (mbx == 0 || (quiet(m - 1) && same_mv(mbx - 1, mby))) &&
+        bool split = form && mb_split[m];
+        bool nsplit = form && ((mbx > 0 && mb_split[m - 1]) || (mby > 0 && mb_split[m - mb_w]));
+        if (!split && !nsplit && quiet(m) && (mbx == 0 || (quiet(m - 1) && same_mv(mbx - 1, mby))) &&
             (mby == 0 || (quiet(m - mb_w) && same_mv(mbx, mby - 1))))
           continue;
         bool intra = mb_intra[m];
-        bool internal = intra || mb_cbp_luma[m] != 0;
+        bool internal = intra || mb_cbp_luma[m] != 0 || split;
         bool skip_odd = mb_t8[m];
         int qpq = mb_qp[m], qpcq = chroma_qp(qpq, 0);
         for (int dir = 0; dir < 2; dir++)
@@ -1397,15 +1416,19 @@ struct Encoder {
                 if (dir == 0) coded[k] = nzq(e, k) | (e == 0 ? nzp(pm, 3, k) : nzq(e - 1, k));
                 else coded[k] = nzq(k, e) | (e == 0 ? nzp(pm, k, 3) : nzq(k, e - 1));
               }
-              bool motion = false;
-              if (e == 0) {
-                int gq = (mby * 4) * g + mbx * 4;
+              bool mot[4] = {false, false, false, false};
+              for (int k = 0; k < 4; k++) {
+                // 4x4 blocks q (this side) and p (across the edge) of segment k; the plain form's
+                // vectors are one per macroblock, so only its edge 0 can differ
+                if (!form && (e != 0 || k != 0)) { mot[k] = mot[0]; continue; }
+                int qx = dir == 0 ? e : k, qy = dir == 0 ? k : e;
+                int gq = (mby * 4 + qy) * g + mbx * 4 + qx;
                 int gp = dir == 0 ? gq - 1 : gq - g;
-                motion = ref_grid[gq] != ref_grid[gp] || iabs(mv_grid[2 * gq] - mv_grid[2 * gp]) >= 4 ||
+                mot[k] = ref_grid[gq] != ref_grid[gp] || iabs(mv_grid[2 * gq] - mv_grid[2 * gp]) >= 4 ||
                          iabs(mv_grid[2 * gq + 1] - mv_grid[2 * gp + 1]) >= 4;
               }
-              if (!coded[0] && !coded[1] && !coded[2] && !coded[3] && !motion) continue;
-              for (int k = 0; k < 4; k++) bs[k] = coded[k] ? 2 : (motion ? 1 : 0);
+              if (!coded[0] && !coded[1] && !coded[2] && !coded[3] && !mot[0] && !mot[1] && !mot[2] && !mot[3]) continue;
+              for (int k = 0; k < 4; k++) bs[k] = coded[k] ? 2 : (mot[k] ? 1 : 0);
             }
             int qpv, qpc;
             if (pm == m) { qpv = qpq; qpc = qpcq; }
@@ -1819,7 +1842,8 @@ struct Encoder {
   }
 
   // enc.rs:3336 analyse_i4; returns false when the budget is exceeded. Writes recon into cur.y.
-  bool analyse_i4(int mbx, int mby, const MbSrc& src, uint32_t budget, rg_mb_out& r, uint8_t* recon, int16_t q4[16][16], int& cbpl) {
+  bool analyse_i4(int mbx, int mby, const MbSrc& src, uint32_t budget, rg_mb_out& r, uint8_t* recon, int16_t q4[16][16], int& cbpl,
+                  const uint16_t* masks = nullptr) {
     int g = gstride();
     int q_ = cur_qp;
     uint32_t lambda = kLambda[q_];
@@ -1864,9 +1888,16 @@ struct Encoder {
       if (hl) { int p[4]; hadamard_edge(left, p); sh = total_abs; for (int k = 0; k < 4; k++) sh += iabs(h[4 * k] - p[k]) - iabs(h[4 * k]); }
       uint32_t s3[3] = {(uint32_t)(sv >> 1), (uint32_t)(sh >> 1), (uint32_t)(sd >> 1)};
       uint32_t best = UINT32_MAX; int bm = 2;
+      // learned form: only the hinted modes available here (DC when none is)
+      uint32_t allow = 0x1ff;
+      if (masks) {
+        uint32_t avail = 0x4u | (ht ? 0x89u : 0u) | (hl ? 0x102u : 0u) | (ht && hl ? 0x70u : 0u);
+        allow = masks[b] & avail;
+        if (!allow) allow = 0x4u;
+      }
       bool ok3[3] = {ht, hl, true};
       for (int md = 0; md < 3; md++)
-        if (ok3[md] && s3[md] + bits(md) < best) { best = s3[md] + bits(md); bm = md; }
+        if (ok3[md] && ((allow >> md) & 1) && s3[md] + bits(md) < best) { best = s3[md] + bits(md); bm = md; }
       uint8_t t8[8], l4[4];
       for (int k = 0; k < 8; k++) t8[k] = ht ? top[k] : 128;
       for (int k = 0; k < 4; k++) l4[k] = hl ? left[k] : 128;
@@ -1874,7 +1905,7 @@ struct Encoder {
       for (int md = 3; md <= 8; md++) pred4x4(md, t8, l4, tl, dirs[md - 3]);
       for (int md = 3; md <= 8; md++) {
         bool av = (md == 3 || md == 7) ? ht : (md == 8 ? hl : (ht && hl));
-        if (!av) continue;
+        if (!av || !((allow >> md) & 1)) continue;
         uint32_t cst = satd4(src.y + by * 64 + bx * 4, 16, dirs[md - 3], 4) + bits(md);
         if (cst < best) { best = cst; bm = md; }
       }
@@ -1921,7 +1952,8 @@ struct Encoder {
     analyse_i16(mbx, mby, src, i16c, i16m);
     if (i16c > 40 * lambda) {
       uint8_t recon[256]; int16_t q4[16][16]; int cbpl;
-      if (analyse_i4(mbx, mby, src, i16c + lambda * 4, r, recon, q4, cbpl)) {
+      const uint16_t* masks = form == 2 && hints ? hints[mby * mb_w + mbx].i4_mask : nullptr;
+      if (analyse_i4(mbx, mby, src, i16c + lambda * 4, r, recon, q4, cbpl, masks)) {
         code_i4(mbx, mby, src, r, recon, q4, cbpl);
         return;
       }
@@ -2205,6 +2237,324 @@ struct Encoder {
     sb_probe = 16 * (((1u << q.shift) - q.bias) / q.mf[0] + 1);
   }
 
+
+  // ---- search forms: full search (form 1) and learned (form 2); no counterpart in the reference.
+  // The same decisions as the GPU engine's search forms: the skip probe of the plain form, an
+  // integer search over a window (quadrant SADs, nine partition parts, cost SAD + lambda * vector
+  // bits against the 16x16 predictor, first minimum in raster order), quarter-sample refinement of
+  // each part of every tried partition type (centre and 8 neighbours at distance 2, then 8 at
+  // distance 1; cost SATD/2 + lambda * vector bits against the part's own H.264 8.4.1.3 predictor),
+  // the type of least total cost (+ lambda * {1, 3, 3, 7}), then the plain form's intra check,
+  // residual and late skip. Learned: +-2 around the predictor plus the hinted offset (the full
+  // window when the 16x16 best lies on that window's edge), only the hinted types, and intra 4x4
+  // blocks of IDR pictures restricted to their hinted modes.
+  int form = 0, search_range = 32;
+  const rg_mb_hint* hints = nullptr;    // learned form: this picture's hints
+  std::vector<uint8_t> mb_split;        // per MB: quadrant vectors differ
+
+  struct NbS { int ref, x, y; };
+  NbS nb4s(int mbx, int mby, int bx, int by, const int own[4][2], int done) const {
+    if (bx >= 0 && bx < 4 && by >= 0 && by < 4) {
+      int q = (by >> 1) * 2 + (bx >> 1);
+      if ((done >> q) & 1) return {0, own[q][0], own[q][1]};
+      return {-2, 0, 0};
+    }
+    if ((bx == 4 && by >= 0) || by >= 4) return {-2, 0, 0};
+    int g = gstride(), gx = mbx * 4 + bx, gy = mby * 4 + by;
+    if (gx < 0 || gy < 0 || gx >= g) return {-2, 0, 0};
+    int i = gy * g + gx;
+    int ref = ref_grid[i];
+    if (ref != 0) return {ref, 0, 0};
+    return {0, mv_grid[2 * i], mv_grid[2 * i + 1]};
+  }
+  // H.264 8.4.1.3 (dir: 1 16x8 top, 2 16x8 bottom, 3 8x16 left, 4 8x16 right, 0 median)
+  void mv_pred_s(int mbx, int mby, int bx, int by, int pw, int dir, const int own[4][2], int done, int mvp[2]) const {
+    NbS A = nb4s(mbx, mby, bx - 1, by, own, done), B = nb4s(mbx, mby, bx, by - 1, own, done);
+    NbS C = nb4s(mbx, mby, bx + pw, by - 1, own, done);
+    if (C.ref == -2) C = nb4s(mbx, mby, bx - 1, by - 1, own, done);
+    if (dir == 1 && B.ref == 0) { mvp[0] = B.x; mvp[1] = B.y; return; }
+    if ((dir == 2 || dir == 3) && A.ref == 0) { mvp[0] = A.x; mvp[1] = A.y; return; }
+    if (dir == 4 && C.ref == 0) { mvp[0] = C.x; mvp[1] = C.y; return; }
+    if (B.ref == -2 && C.ref == -2 && A.ref != -2) { mvp[0] = A.x; mvp[1] = A.y; return; }
+    int m = (A.ref == 0) + (B.ref == 0) + (C.ref == 0);
+    if (m == 1) {
+      const NbS& o = A.ref == 0 ? A : (B.ref == 0 ? B : C);
+      mvp[0] = o.x; mvp[1] = o.y;
+      return;
+    }
+    auto med = [](int x, int y, int z) { return std::min(std::max(x, y), std::max(std::min(x, y), z)); };
+    mvp[0] = med(A.x, B.x, C.x);
+    mvp[1] = med(A.y, B.y, C.y);
+  }
+  // integer search over [xlo, xhi] x [ylo, yhi]: best vector and cost of each of the nine parts
+  void int_search_s(int x0, int y0, const MbSrc& src, int xlo, int xhi, int ylo, int yhi, const int mvp[2], uint32_t lambda,
+                    int bx[9], int by[9]) const {
+    uint32_t bc[9];
+    for (int k = 0; k < 9; k++) { bc[k] = UINT32_MAX; bx[k] = xlo; by[k] = ylo; }
+    for (int y = ylo; y <= yhi; y++)
+      for (int x = xlo; x <= xhi; x++) {
+        uint32_t q[4];
+        for (int k = 0; k < 4; k++)
+          q[k] = sad(src.y + (k >> 1) * 128 + (k & 1) * 8, 16, refp.y.ptr(x0 + x + (k & 1) * 8, y0 + y + (k >> 1) * 8),
+                     refp.y.stride, 8, 8);
+        uint32_t part[9] = {q[0] + q[1] + q[2] + q[3], q[0] + q[1], q[2] + q[3], q[0] + q[2], q[1] + q[3], q[0], q[1], q[2], q[3]};
+        uint32_t mc = lambda * (se_bits(4 * x - mvp[0]) + se_bits(4 * y - mvp[1]));
+        for (int k = 0; k < 9; k++)
+          if (part[k] + mc < bc[k]) { bc[k] = part[k] + mc; bx[k] = x; by[k] = y; }
+      }
+  }
+  // SATD cost of a part's prediction at vector (mx, my)
+  uint32_t part_cost(int x0, int y0, const MbSrc& src, int px, int py, int pw, int ph, int mx, int my, const int mvp[2],
+                     uint32_t lambda) const {
+    uint8_t pred[256];
+    luma_mc(refp.y.ptr(x0 + px + (mx >> 2), y0 + py + (my >> 2)), refp.y.stride, pw, ph, mx & 3, my & 3, pred, 16);
+    uint32_t s = 0;
+    for (int by = 0; by < ph; by += 4)
+      for (int bx = 0; bx < pw; bx += 4) s += satd4_raw(src.y + (py + by) * 16 + px + bx, 16, pred + by * 16 + bx, 16);
+    return (s >> 1) + lambda * (se_bits(mx - mvp[0]) + se_bits(my - mvp[1]));
+  }
+  uint32_t refine_part_s(int x0, int y0, const MbSrc& src, const Bounds& bd, int px, int py, int pw, int ph, int ix, int iy,
+                         const int mvp[2], uint32_t lambda, int mv[2]) const {
+    static const int st[8][2] = {{0, -2}, {-2, 0}, {2, 0}, {0, 2}, {-2, -2}, {2, -2}, {-2, 2}, {2, 2}};
+    int cx = 4 * ix, cy = 4 * iy;
+    uint32_t best = part_cost(x0, y0, src, px, py, pw, ph, cx, cy, mvp, lambda);
+    for (int step = 0; step < 2; step++) {
+      int fx = cx, fy = cy;
+      for (int k = 0; k < 8; k++) {
+        int vx = fx + (step == 0 ? st[k][0] : st[k][0] / 2), vy = fy + (step == 0 ? st[k][1] : st[k][1] / 2);
+        if (!in_bounds(bd, vx, vy)) continue;
+        uint32_t c = part_cost(x0, y0, src, px, py, pw, ph, vx, vy, mvp, lambda);
+        if (c < best) { best = c; cx = vx; cy = vy; }
+      }
+    }
+    mv[0] = cx; mv[1] = cy;
+    return best;
+  }
+  void fill_motion_q(int mbx, int mby, const int qmv[4][2]) {
+    int g = gstride();
+    for (int y = 0; y < 4; y++)
+      for (int x = 0; x < 4; x++) {
+        int i = (mby * 4 + y) * g + mbx * 4 + x, q = (y >> 1) * 2 + (x >> 1);
+        ref_grid[i] = 0;
+        mv_grid[2 * i] = (int16_t)qmv[q][0];
+        mv_grid[2 * i + 1] = (int16_t)qmv[q][1];
+      }
+    mb_split[mby * mb_w + mbx] = !(qmv[0][0] == qmv[1][0] && qmv[0][0] == qmv[2][0] && qmv[0][0] == qmv[3][0] &&
+                                   qmv[0][1] == qmv[1][1] && qmv[0][1] == qmv[2][1] && qmv[0][1] == qmv[3][1]);
+  }
+  static void set_parts(rg_mb_out& r, int ptype, const int qmv[4][2], const int pmvd[4][2]) {
+    for (int q = 0; q < 4; q++)
+      for (int c = 0; c < 2; c++) { r.part_mv[q][c] = (int16_t)qmv[q][c]; r.part_mvd[q][c] = (int16_t)pmvd[q][c]; }
+    r.part_type = (uint8_t)ptype;
+  }
+
+  void code_p_mb_search(int mbx, int mby, const MbSrc& src, rg_mb_out& r) {
+    static const int parts[9][9] = {{0, 0, 16, 16, 0, 0, 4, 0, 0}, {0, 0, 16, 8, 0, 0, 4, 1, 1}, {0, 8, 16, 8, 0, 2, 4, 2, 2},
+                                    {0, 0, 8, 16, 0, 0, 2, 3, 3}, {8, 0, 8, 16, 2, 0, 2, 4, 4}, {0, 0, 8, 8, 0, 0, 2, 0, 5},
+                                    {8, 0, 8, 8, 2, 0, 2, 0, 6}, {0, 8, 8, 8, 0, 2, 2, 0, 7}, {8, 8, 8, 8, 2, 2, 2, 0, 8}};
+    static const int first[4] = {0, 1, 3, 5}, nparts[4] = {1, 2, 2, 4};
+    static const int quads[9] = {15, 3, 12, 5, 10, 1, 2, 4, 8};
+    int m = mby * mb_w + mbx, x0 = mbx * 16, y0 = mby * 16;
+    int q_ = cur_qp, qpc = chroma_qp(q_, 0);
+    uint32_t lambda = kLambda[q_];
+    Bounds bd = mv_bounds(x0, y0);
+    int imin[2] = {(bd.min[0] + 3) >> 2, (bd.min[1] + 3) >> 2}, imax[2] = {bd.max[0] >> 2, bd.max[1] >> 2};
+    const int none[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    int mvp16[2];
+    mv_pred_s(mbx, mby, 0, 0, 4, 0, none, 0, mvp16);
+    int ps[2] = {mvp16[0], mvp16[1]};
+    {
+      NbS A = nb4s(mbx, mby, -1, 0, none, 0), B = nb4s(mbx, mby, 0, -1, none, 0);
+      if (mbx == 0 || mby == 0 || (A.ref == 0 && A.x == 0 && A.y == 0) || (B.ref == 0 && B.x == 0 && B.y == 0)) ps[0] = ps[1] = 0;
+    }
+    uint8_t py[256], pu[64], pv[64];
+    // 1. skip probe (enc.rs:2906 try_p_skip)
+    if (in_bounds(bd, ps[0], ps[1])) {
+      mc_luma16(x0, y0, ps[0], ps[1], py);
+      uint32_t s0 = sad(src.y, 16, py, 16, 16, 16);
+      if (s0 < sb_probe) {
+        bool luma_zero = s0 <= sb_luma || ssd(src.y, 16, py, 16, 16) <= sb_luma_ssd;
+        if (!luma_zero) luma_zero = probe_skip_luma(src, py, q_);
+        if (luma_zero) {
+          mc_chroma8(mbx, mby, ps[0], ps[1], pu, pv);
+          auto plane_zero = [&](const uint8_t* s8, const uint8_t* p8) {
+            return sad(s8, 8, p8, 8, 8, 8) <= sb_chroma || ssd(s8, 8, p8, 8, 8) <= sb_chroma_ssd;
+          };
+          bool chroma_zero = plane_zero(src.u, pu) && plane_zero(src.v, pv);
+          if (!chroma_zero) chroma_zero = probe_skip_chroma(src, pu, pv, qpc);
+          if (chroma_zero) {
+            int16_t p16[2] = {(int16_t)ps[0], (int16_t)ps[1]};
+            code_skip(mbx, mby, p16, r);
+            store_mb(mbx, mby, py, pu, pv);
+            int qmv[4][2] = {{ps[0], ps[1]}, {ps[0], ps[1]}, {ps[0], ps[1]}, {ps[0], ps[1]}};
+            set_parts(r, 255, qmv, none);
+            mb_split[m] = 0;
+            return;
+          }
+        }
+      }
+    }
+    // 2. integer search
+    const rg_mb_hint* h = form == 2 && hints ? &hints[m] : nullptr;
+    int R = search_range;
+    int fc[2] = {std::min(std::max((mvp16[0] + 2) >> 2, imin[0]), imax[0]), std::min(std::max((mvp16[1] + 2) >> 2, imin[1]), imax[1])};
+    int lo[2] = {std::max(fc[0] - R, imin[0]), std::max(fc[1] - R, imin[1])};
+    int hi[2] = {std::min(fc[0] + R, imax[0]), std::min(fc[1] + R, imax[1])};
+    int part_mask = 15;
+    if (h) {
+      int lc[2];
+      for (int c = 0; c < 2; c++) {
+        lc[c] = std::min(std::max((mvp16[c] + h->mv_off[c] + 2) >> 2, imin[c]), imax[c]);
+        lo[c] = std::max(lc[c] - 2, imin[c]);
+        hi[c] = std::min(lc[c] + 2, imax[c]);
+      }
+      part_mask = h->part_mask & 15;
+      if (!part_mask) part_mask = 1;
+    }
+    int ibx[9], iby[9];
+    int_search_s(x0, y0, src, lo[0], hi[0], lo[1], hi[1], mvp16, lambda, ibx, iby);
+    if (h) {
+      bool edge = (ibx[0] == lo[0] && lo[0] > imin[0]) || (ibx[0] == hi[0] && hi[0] < imax[0]) ||
+                  (iby[0] == lo[1] && lo[1] > imin[1]) || (iby[0] == hi[1] && hi[1] < imax[1]);
+      if (edge) {
+        for (int c = 0; c < 2; c++) { lo[c] = std::max(fc[c] - R, imin[c]); hi[c] = std::min(fc[c] + R, imax[c]); }
+        int_search_s(x0, y0, src, lo[0], hi[0], lo[1], hi[1], mvp16, lambda, ibx, iby);
+      }
+    }
+    // 3-4. refinement and the partition type
+    int best_t = -1;
+    uint32_t best_j = UINT32_MAX;
+    int bmv[4][2] = {}, bmvd[4][2] = {};
+    for (int t = 0; t < 4; t++) {
+      if (!((part_mask >> t) & 1)) continue;
+      int own[4][2] = {}, done = 0, pm[4][2] = {}, pd[4][2] = {};
+      uint32_t J = lambda * (t == 0 ? 1u : (t == 3 ? 7u : 3u));
+      for (int k = 0; k < nparts[t]; k++) {
+        const int* g = parts[first[t] + k];
+        int mvp[2], mv[2];
+        mv_pred_s(mbx, mby, g[4], g[5], g[6], g[7], own, done, mvp);
+        J += refine_part_s(x0, y0, src, bd, g[0], g[1], g[2], g[3], ibx[g[8]], iby[g[8]], mvp, lambda, mv);
+        pm[k][0] = mv[0]; pm[k][1] = mv[1];
+        pd[k][0] = mv[0] - mvp[0]; pd[k][1] = mv[1] - mvp[1];
+        for (int q = 0; q < 4; q++)
+          if ((quads[first[t] + k] >> q) & 1) { own[q][0] = mv[0]; own[q][1] = mv[1]; }
+        done |= quads[first[t] + k];
+      }
+      if (J < best_j) {
+        best_j = J; best_t = t;
+        memcpy(bmv, pm, sizeof pm);
+        memcpy(bmvd, pd, sizeof pd);
+      }
+    }
+    int qmv[4][2];
+    for (int k = 0; k < nparts[best_t]; k++) {
+      const int* g = parts[first[best_t] + k];
+      for (int q = 0; q < 4; q++)
+        if ((quads[first[best_t] + k] >> q) & 1) { qmv[q][0] = bmv[k][0]; qmv[q][1] = bmv[k][1]; }
+      luma_mc(refp.y.ptr(x0 + g[0] + (bmv[k][0] >> 2), y0 + g[1] + (bmv[k][1] >> 2)), refp.y.stride, g[2], g[3],
+              bmv[k][0] & 3, bmv[k][1] & 3, py + g[1] * 16 + g[0], 16);
+    }
+    // 5. intra 16x16 check (the plain form's rule)
+    uint32_t inter_satd = satd16(src.y, 16, py, 16);
+    if (inter_satd > 24 * lambda) {
+      uint32_t i16c; int i16m;
+      analyse_i16(mbx, mby, src, i16c, i16m);
+      if (i16c + lambda * 8 < best_j) {
+        code_i16(mbx, mby, src, i16m, r);
+        set_parts(r, best_t, none, none);
+        mb_split[m] = 0;
+        return;
+      }
+    }
+    // chroma per quadrant vector, residual, late skip
+    for (int q = 0; q < 4; q++) {
+      uint8_t tu[64], tv[64];
+      mc_chroma8(mbx, mby, qmv[q][0], qmv[q][1], tu, tv);
+      int ox = (q & 1) * 4, oy = (q >> 1) * 4;
+      for (int yy = 0; yy < 4; yy++)
+        for (int xx = 0; xx < 4; xx++) {
+          pu[(oy + yy) * 8 + ox + xx] = tu[(oy + yy) * 8 + ox + xx];
+          pv[(oy + yy) * 8 + ox + xx] = tv[(oy + yy) * 8 + ox + xx];
+        }
+    }
+    int16_t q4[16][16];
+    int cbp4 = quant_luma_inter(src.y, py, q_, q4);
+    int cbpl = cbp4;
+    bool use8 = false;
+    int16_t q8[4][64];
+    if (t8x8 && cabac && cbp4) {
+      int cbp8 = quant_luma_8x8(src.y, py, q_, q8);
+      int nnz4 = 0, nnz8 = 0;
+      for (int b = 0; b < 16; b++) for (int i = 0; i < 16; i++) nnz4 += q4[b][i] != 0;
+      for (int b = 0; b < 4; b++) for (int i = 0; i < 64; i++) nnz8 += q8[b][i] != 0;
+      if (nnz8 <= nnz4) { use8 = true; cbpl = cbp8; }
+    }
+    Chroma c;
+    quant_chroma(src, pu, pv, qpc, false, c);
+    for (int p = 0; p < 2; p++) {
+      bool anym = c.mask[p][0] | c.mask[p][1] | c.mask[p][2] | c.mask[p][3];
+      if (anym && chroma_ac_score(c, p) < 7) {
+        memset(c.ac[p], 0, sizeof c.ac[p]);
+        memset(c.mask[p], 0, sizeof c.mask[p]);
+        memset(c.raster[p], 0, sizeof c.raster[p]);
+      }
+    }
+    int cbpc = chroma_cbp(c);
+    if (best_t == 0 && cbpl == 0 && cbpc == 0 && bmv[0][0] == ps[0] && bmv[0][1] == ps[1]) {
+      int16_t p16[2] = {(int16_t)ps[0], (int16_t)ps[1]};
+      code_skip(mbx, mby, p16, r);
+      store_mb(mbx, mby, py, pu, pv);
+      set_parts(r, best_t, qmv, none);
+      mb_split[m] = 0;
+      return;
+    }
+    static const uint8_t types[4] = {RG_MB_P_L0_16X16, RG_MB_P_L0_16X8, RG_MB_P_L0_8X16, RG_MB_P_8X8};
+    r.mb_type = types[best_t];
+    r.mv[0] = (int16_t)bmv[0][0]; r.mv[1] = (int16_t)bmv[0][1];
+    r.mvd[0] = (int16_t)bmvd[0][0]; r.mvd[1] = (int16_t)bmvd[0][1];
+    r.cbp = (uint8_t)(cbpl | (cbpc << 4));
+    bool t8flag = use8 && cbpl != 0;
+    r.transform_8x8 = t8flag;
+    uint16_t nzm = 0;
+    if (use8) {
+      for (int b = 0; b < 4; b++) {
+        for (int i = 0; i < 64; i++) r.luma[b * 64 + i] = q8[b][kZigzag8[i]];
+        if (cbpl & (1 << b)) nzm |= 0xF << (4 * b);
+      }
+    } else {
+      for (int b = 0; b < 16; b++) {
+        zigzag16(q4[b], r.luma + b * 16);
+        for (int i = 0; i < 16; i++) if (q4[b][i]) nzm |= 1 << b;
+      }
+    }
+    memcpy(r.chroma_dc, c.dc, sizeof c.dc);
+    memcpy(r.chroma_ac, c.ac, sizeof c.ac);
+    set_mb_state(m, false, cbpl, t8flag, nzm);
+    if (use8) {
+      for (int b = 0; b < 4; b++)
+        if (cbpl & (1 << b)) {
+          int32_t d[64];
+          dequant8(q8[b], q_, d);
+          idct8_add(py + (b >> 1) * 128 + (b & 1) * 8, 16, d);
+        }
+    } else {
+      int32_t sc[16];
+      dequant4_scale(q_, sc);
+      for (int b = 0; b < 16; b++)
+        if (cbpl & (1 << (b >> 2))) {
+          int16_t blk[16];
+          memcpy(blk, q4[b], 32);
+          dequant_block(blk, sc);
+          int bx, by; blk_xy(b, bx, by);
+          add_idct4(py + by * 64 + bx * 4, 16, blk);
+        }
+    }
+    recon_chroma(pu, pv, c, cbpc, qpc);
+    fill_motion_q(mbx, mby, qmv);
+    store_mb(mbx, mby, py, pu, pv);
+    set_parts(r, best_t, qmv, bmvd);
+  }
+
   // enc.rs:2234 encode_frame_body (fixed QP, Balanced); returns Annex-B bytes (CAVLC only).
   std::vector<uint8_t> encode(const uint8_t* Y, const uint8_t* U, const uint8_t* V, int sy, int suv) {
     int n = mb_w * mb_h, n4 = n * 16;
@@ -2217,6 +2567,7 @@ struct Encoder {
     intra4x4_modes.assign(n4, 2);
     nz16.assign(n, 0);
     mb_intra.assign(n, 0); mb_cbp_luma.assign(n, 0); mb_t8.assign(n, 0); mb_qp.assign(n, (uint8_t)qp); mb_skip.assign(n, 0);
+    mb_split.assign(n, 0);
     for (auto& r : recs) memset(&r, 0, sizeof r);
     cur_qp = qp;
     skip_run = 0;
@@ -2247,6 +2598,12 @@ struct Encoder {
         load_src(Y, U, V, sy, suv, mbx, mby, src);
         rg_mb_out& r = recs[mby * mb_w + mbx];
         r.qp = (uint8_t)qp;
+        if (form) {  // search forms: decisions and reconstruction only (no bitstream)
+          r.part_type = 255;
+          if (is_idr) code_intra(mbx, mby, src, r);
+          else code_p_mb_search(mbx, mby, src, r);
+          continue;
+        }
         if (is_idr) code_intra(mbx, mby, src, r);
         else code_p_mb(mbx, mby, src, r);
         if (!cabac) {
@@ -2257,7 +2614,9 @@ struct Encoder {
         }
       }
     std::vector<uint8_t> rbsp;
-    if (cabac) {
+    if (form) {
+      rbsp.clear();
+    } else if (cabac) {
       rbsp = w.finish();
       rbsp.insert(rbsp.end(), ce.out.begin(), ce.out.end());
     } else {
@@ -2284,6 +2643,7 @@ struct Encoder {
       }
     frame_count++;
     std::vector<uint8_t> out;
+    if (form) return out;
     if (is_idr) {
       append_nal(out, 3, 7, sps_rbsp());
       append_nal(out, 3, 8, pps_rbsp());
@@ -2341,6 +2701,14 @@ void oracle_mb_dims(void* h, int* mb_w, int* mb_h) {
   *mb_w = e->mb_w; *mb_h = e->mb_h;
 }
 int oracle_record_size(void) { return (int)sizeof(rg_mb_out); }
+// Search forms (1 full search, 2 learned) with the integer search range; the learned form reads the
+// hints set for the next frame (mb_w * mb_h records, host memory, kept until the next call).
+void oracle_enc_set_form(void* h, int form, int search_range) {
+  auto* e = (oracle::Encoder*)h;
+  e->form = form;
+  e->search_range = search_range;
+}
+void oracle_enc_set_hints(void* h, const rg_mb_hint* hints) { ((oracle::Encoder*)h)->hints = hints; }
 // Pixel differences evaluated by the SAD / SSD / SATD of every frame encoded so far in this
 // process (all threads); reset = 1 also sets the total back to 0.
 unsigned long long oracle_pixel_ops(int reset) {

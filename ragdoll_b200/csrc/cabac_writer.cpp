@@ -138,11 +138,11 @@ struct MbSummary {
   uint8_t cdc = 0;              // bit p: chroma DC levels present in plane p
   uint16_t luma = 0;            // bit 4 * y + x: luma 4x4 block (x, y) holds levels (8x8: the whole 8x8)
   uint8_t chroma[2] = {0, 0};   // bit 2 * y + x: chroma AC block (x, y) holds levels
-  uint16_t amvd[2] = {0, 0};    // |mvd| per component
+  uint16_t amvd[4][2] = {};     // |mvd| per 8x8 quadrant (raster) and component
 };
 
 // Context index offsets (Table 9-34) and the coded_block_flag / residual offsets per category.
-constexpr int kSkipP = 11, kMbTypeI = 3, kMbTypeP = 14, kMbTypePIntra = 17, kMvdX = 40, kMvdY = 47;
+constexpr int kSkipP = 11, kMbTypeI = 3, kMbTypeP = 14, kMbTypePIntra = 17, kSubMbTypeP = 21, kMvdX = 40, kMvdY = 47;
 constexpr int kQpDelta = 60, kChromaPred = 64, kPrevI4 = 68, kRemI4 = 69, kCbpLuma = 73, kCbpChroma = 77;
 constexpr int kTransform8x8 = 399;
 constexpr int kCbf[5] = {85, 89, 93, 97, 101};
@@ -257,6 +257,14 @@ class SliceCoder {
       exp_golomb(a - 9, 3);
     }
     ar_.bypass(v < 0);
+  }
+
+  // |mvd| component c of the 4x4 block (bx, by) relative to the current macroblock (-1: the left /
+  // top neighbour's): 0 when not available, skipped or intra (9.3.3.1.1.7).
+  unsigned amvd_at(const MbSummary& cur, const MbSummary& top, int bx, int by, int c) const {
+    if (bx < 0) return left_.avail ? left_.amvd[(by >> 1) * 2 + 1][c] : 0u;
+    if (by < 0) return top.avail ? top.amvd[2 + (bx >> 1)][c] : 0u;
+    return cur.amvd[(by >> 1) * 2 + (bx >> 1)][c];
   }
 
   void exp_golomb(unsigned v, unsigned k) {
@@ -387,14 +395,34 @@ class SliceCoder {
     if (!idr_) bin(kSkipP + skip_inc, 0);
     cur.cbpl = r.cbp & 15;
     cur.cbpc = r.cbp >> 4;
-    if (r.mb_type == RG_MB_P_L0_16X16) {
+    if (r.mb_type == RG_MB_P_L0_16X16 || (r.mb_type >= RG_MB_P_L0_16X8 && r.mb_type <= RG_MB_P_8X8)) {
       if (idr_) return -1;
       cur.t8 = r.transform_8x8 && cur.cbpl;
-      for (int k = 0; k < 3; k++) bin(kMbType + k, 0);  // P_L0_16x16: bins 0 0 0 at 14, 15, 16
-      for (int c = 0; c < 2; c++) {
-        const unsigned sum = (left_.avail ? left_.amvd[c] : 0u) + (top.avail ? top.amvd[c] : 0u);
-        mvd(c ? kMvdY : kMvdX, sum, r.mvd[c]);
-        cur.amvd[c] = (uint16_t)std::min(std::abs((int)r.mvd[c]), 65535);
+      // mb_type (Table 9-37 binarisation; bin 2 at ctxIdx 16 after a 0, 17 after a 1):
+      // P_L0_16x16 000, P_L0_L0_16x8 011, P_L0_L0_8x16 010, P_8x8 001
+      const int t = r.mb_type == RG_MB_P_L0_16X16 ? 0 : r.mb_type - RG_MB_P_L0_16X8 + 1;
+      static const uint8_t kBins[4][2] = {{0, 0}, {1, 1}, {1, 0}, {0, 1}};
+      bin(kMbType, 0);
+      bin(kMbType + 1, kBins[t][0]);
+      bin(kMbType + 2 + kBins[t][0], kBins[t][1]);
+      if (t == 3)
+        for (int k = 0; k < 4; k++) bin(kSubMbTypeP, 1);  // sub_mb_type P_L0_8x8: "1"
+      // partitions in coding order: top-left 4x4 block and the quadrants each covers
+      static const int8_t kParts[4][4][3] = {{{0, 0, 15}},
+                                             {{0, 0, 3}, {0, 2, 12}},
+                                             {{0, 0, 5}, {2, 0, 10}},
+                                             {{0, 0, 1}, {2, 0, 2}, {0, 2, 4}, {2, 2, 8}}};
+      static const int kNum[4] = {1, 2, 2, 4};
+      for (int k = 0; k < kNum[t]; k++) {
+        const int bx = kParts[t][k][0], by = kParts[t][k][1], qm = kParts[t][k][2];
+        for (int c = 0; c < 2; c++) {
+          const int v = t == 0 ? r.mvd[c] : r.part_mvd[k][c];
+          const unsigned sum = amvd_at(cur, top, bx - 1, by, c) + amvd_at(cur, top, bx, by - 1, c);
+          mvd(c ? kMvdY : kMvdX, sum, v);
+          const uint16_t a = (uint16_t)std::min(std::abs(v), 65535);
+          for (int q = 0; q < 4; q++)
+            if ((qm >> q) & 1) cur.amvd[q][c] = a;
+        }
       }
       residual(r, top, cur, false);
       std::fill(left_modes_, left_modes_ + 4, 2);

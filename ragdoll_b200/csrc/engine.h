@@ -32,6 +32,15 @@ static_assert(sizeof(MbInfo) == 16, "MbInfo layout");
 
 constexpr uint8_t kFlagIntra = 1, kFlagSkip = 2, kFlagT8 = 4;
 
+// Quadrant vectors of a macroblock of the search forms (raster: top-left, top-right, bottom-left,
+// bottom-right), read by later macroblocks' predictors and by the deblocking filter.
+struct __align__(16) MbMv4 {
+  int16_t mv[4][2];
+};
+
+// Integer search range limit of the search forms (samples).
+constexpr int kMaxSearchRange = 64;
+
 // Device view of one stream for one picture.
 struct StreamDev {
   const uint8_t* src_y;   // source planes (display size, any stride)
@@ -54,6 +63,11 @@ struct StreamDev {
   // SkipBounds (enc.rs:2104) of the stream's QP
   uint32_t sb_luma, sb_luma_ssd, sb_chroma, sb_chroma_ssd, sb_probe;
   int32_t pad_;
+  // search forms only (null / 0 in the plain form)
+  MbMv4* mv4;              // this picture's quadrant vectors
+  const rg_mb_hint* hint;  // learned form: this picture's hints (null: full search)
+  int32_t search_range;    // integer search range of the full search (samples)
+  int32_t pad2_;
 };
 
 // Frame-constant parameters of one wavefront (all streams share the size; qp / qpc / sb_* are the
@@ -72,7 +86,9 @@ struct FrameParams {
 };
 
 // Host launchers (engine_kernels.cu).
-void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st);
+// form: 0 the plain (Balanced) analysis, 1 the search forms (full search; learned where a stream's
+// descriptor carries hints).
+void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st, int form = 0);
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st);
 int wavefront_steps(const FrameParams& fp);
 // Pipelined mode: d_streams holds frames x n_streams descriptors (picture-major); counters is
@@ -83,7 +99,7 @@ int wavefront_steps(const FrameParams& fp);
 // reach, in macroblock rows and columns beyond zero motion, of the launch's waits for a reference
 // picture (0: no such wait); the work order never waits for an untaken segment when
 // lag >= max(seg, 2) * (4 + rows) + seg + columns + 3.
-int pipeline_grid(int device);
+int pipeline_grid(int device, int form = 0);
 int pipeline_sms(int device);
 size_t pipeline_counter_ints(const FrameParams& fp, int frames);
 // Work list: every analysis / deblocking segment of `seg` macroblocks, in expected-ready order
@@ -96,7 +112,7 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
                      size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
                      int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
-                     int* host_reach, cudaStream_t st);
+                     int* host_reach, cudaStream_t st, int form = 0);
 void upload_tables();
 
 }  // namespace rg

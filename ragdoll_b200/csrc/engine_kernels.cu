@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -1223,7 +1224,11 @@ __device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht,
 // Q[k]), builds all nine predictions (lane -> pixel, the two half-warps taking even / odd modes),
 // costs the modes (lane -> mode), and transforms the chosen residual with shuffles (lane ->
 // coefficient). Gives up (false) as soon as the running cost reaches `budget`.
-__device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out) {
+// kMask: only the modes of masks[b] (bit m: Intra4x4PredMode m) that are available at block b are
+// tried -- DC alone when none is (the learned form); the plain form tries every available mode.
+template <bool kMask>
+__device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out,
+                                        const uint16_t* masks) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int p = lane & 15, xl = p & 3, yl = p >> 2;
@@ -1286,8 +1291,17 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
     int srcp = sm.src_y[(py + yl) * 16 + px + xl];
     int pv[5];
     uint32_t key = UMAX;
+    uint32_t allow = 0x1ffu;
+    if constexpr (kMask) {
+      uint32_t avail = 0x4u | (ht ? 0x89u : 0u) | (hl ? 0x102u : 0u) | (ht && hl ? 0x70u : 0u);
+      allow = masks[b] & avail;
+      if (!allow) allow = 0x4u;
+    }
 #pragma unroll
     for (int k = 0; k < 5; k++) {
+      if constexpr (kMask) {
+        if (!((allow >> (2 * k)) & 3u)) { pv[k] = 0; continue; }  // neither mode of this step is tried
+      }
       uint32_t tp = taps[k], kind = tp >> 12;
       int a0 = sm.i4q[tp & 15], a1 = sm.i4q[(tp >> 4) & 15], a2 = sm.i4q[(tp >> 8) & 15];
       int v = kind == 0 ? a0 : (kind == 1 ? (a0 + a1 + 1) >> 1 : (a0 + 2 * a1 + a2 + 2) >> 2);
@@ -1304,6 +1318,7 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
         int m = 2 * k + h;
         if (m > 8) continue;
         bool av = (m == 0 || m == 3 || m == 7) ? ht : ((m == 1 || m == 8) ? hl : (m == 2 ? true : (ht && hl)));
+        if constexpr (kMask) av = av && ((allow >> m) & 1u);
         uint32_t cost = (((sums >> (16 * h)) & 0xffffu) >> 1) + lambda * (m == pm ? 1u : 4u);
         if (av) key = min(key, (cost << 4) | (uint32_t)m);
       }
@@ -1371,7 +1386,7 @@ __device__ __noinline__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
   int i16m = analyse_i16(sm, ht, hl, tl, &i16c);
   if (i16c > 40 * lambda) {
     int cbpl;
-    if (analyse_i4(c, sm, i16c + lambda * 4, ht, hl, tl, &cbpl)) {
+    if (analyse_i4<false>(c, sm, i16c + lambda * 4, ht, hl, tl, &cbpl, nullptr)) {
       code_i4(c, sm, cbpl, ht, hl, ctl);
       return;
     }
@@ -1815,6 +1830,10 @@ __device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) 
 }
 
 // ---------------------------------------------------------------------------------------------
+// The full-search and learned forms' analysis (neither exists in the reference).
+#include "search_form.cuh"
+
+// ---------------------------------------------------------------------------------------------
 // Deblocking of one macroblock (enc.rs:3776 deblock, h264_deblock.rs:71,187): vertical edges
 // then horizontal ones, on a shared-memory tile with 4 samples of the left / top neighbours.
 struct EdgeParams {
@@ -1885,7 +1904,11 @@ __device__ __forceinline__ int nz_at(uint16_t nz, int bx, int by) {
   return (nz >> b) & 1;
 }
 // Boundary strengths of edge e in direction dir (0 vertical); returns false to skip the edge.
-__device__ bool edge_bs(const MbInfo& q, const MbInfo* p, int dir, int e, int* bs) {
+// kMv4 (search forms): the motion term compares the quadrant vectors on either side of each
+// 4-sample segment (qm: this macroblock's, pm4: the neighbour's across edge 0), so the internal
+// edge between partitions gets strength 1 where their vectors differ by 4 quarter samples.
+template <bool kMv4>
+__device__ bool edge_bs(const MbInfo& q, const MbInfo* p, int dir, int e, int* bs, const MbMv4* qm, const MbMv4* pm4) {
   bool qi = q.flags & kFlagIntra;
   bool pi = p ? (p->flags & kFlagIntra) : qi;
   if (qi || pi) {
@@ -1897,13 +1920,34 @@ __device__ bool edge_bs(const MbInfo& q, const MbInfo* p, int dir, int e, int* b
     if (dir == 0) coded[k] = nz_at(q.nz16, e, k) | (e == 0 ? nz_at(p->nz16, 3, k) : nz_at(q.nz16, e - 1, k));
     else coded[k] = nz_at(q.nz16, k, e) | (e == 0 ? nz_at(p->nz16, k, 3) : nz_at(q.nz16, k, e - 1));
   }
-  bool motion = false;
-  if (e == 0) motion = q.ref != p->ref || abs(q.mv[0] - p->mv[0]) >= 4 || abs(q.mv[1] - p->mv[1]) >= 4;
-  if (!coded[0] && !coded[1] && !coded[2] && !coded[3] && !motion) return false;
-  for (int k = 0; k < 4; k++) bs[k] = coded[k] ? 2 : (motion ? 1 : 0);
-  return true;
+  if constexpr (!kMv4) {
+    bool motion = false;
+    if (e == 0) motion = q.ref != p->ref || abs(q.mv[0] - p->mv[0]) >= 4 || abs(q.mv[1] - p->mv[1]) >= 4;
+    if (!coded[0] && !coded[1] && !coded[2] && !coded[3] && !motion) return false;
+    for (int k = 0; k < 4; k++) bs[k] = coded[k] ? 2 : (motion ? 1 : 0);
+    return true;
+  } else {
+    bool any = false;
+    for (int k = 0; k < 4; k++) {
+      int qq = dir == 0 ? (k >> 1) * 2 + (e >> 1) : (e >> 1) * 2 + (k >> 1);
+      int pq = e == 0 ? (dir == 0 ? (k >> 1) * 2 + 1 : 2 + (k >> 1))
+                      : (dir == 0 ? (k >> 1) * 2 + ((e - 1) >> 1) : ((e - 1) >> 1) * 2 + (k >> 1));
+      const MbMv4* pmm = e == 0 ? pm4 : qm;
+      bool motion = (e == 0 && q.ref != p->ref) || abs(qm->mv[qq][0] - pmm->mv[pq][0]) >= 4 ||
+                    abs(qm->mv[qq][1] - pmm->mv[pq][1]) >= 4;
+      bs[k] = coded[k] ? 2 : (motion ? 1 : 0);
+      any |= bs[k] != 0;
+    }
+    return any;
+  }
+}
+// Whether a search-form macroblock's quadrants share one vector.
+__device__ __forceinline__ bool one_vector(const MbMv4& m) {
+  const uint32_t* w = (const uint32_t*)&m;
+  return w[0] == w[1] && w[0] == w[2] && w[0] == w[3];
 }
 
+template <bool kMv4>
 __device__ __noinline__ void deblock_mb(const FrameParams& fp, const StreamDev& sd, int mbx, int mby, Smem& sm) {
   int lane = lane_id();
   int m = mby * fp.mb_w + mbx;
@@ -1913,9 +1957,22 @@ __device__ __noinline__ void deblock_mb(const FrameParams& fp, const StreamDev& 
   if (hasl) lf = ld_info(&sd.info[m - 1]);
   if (hast) tp = ld_info(&sd.info[m - fp.mb_w]);
   auto quiet = [](const MbInfo& i) { return !(i.flags & kFlagIntra) && i.cbp_luma == 0; };
-  if (quiet(q) && (!hasl || (quiet(lf) && lf.mv[0] == q.mv[0] && lf.mv[1] == q.mv[1])) &&
-      (!hast || (quiet(tp) && tp.mv[0] == q.mv[0] && tp.mv[1] == q.mv[1])))
-    return;
+  MbMv4 qm, lm, tm;
+  bool split = false;
+  if constexpr (kMv4) {
+    qm = sd.mv4[m];
+    if (hasl) lm = sd.mv4[m - 1];
+    if (hast) tm = sd.mv4[m - fp.mb_w];
+    split = !one_vector(qm);
+    const uint32_t qv = *(const uint32_t*)&qm;
+    if (quiet(q) && !split && (!hasl || (quiet(lf) && one_vector(lm) && *(const uint32_t*)&lm == qv)) &&
+        (!hast || (quiet(tp) && one_vector(tm) && *(const uint32_t*)&tm == qv)))
+      return;
+  } else {
+    if (quiet(q) && (!hasl || (quiet(lf) && lf.mv[0] == q.mv[0] && lf.mv[1] == q.mv[1])) &&
+        (!hast || (quiet(tp) && tp.mv[0] == q.mv[0] && tp.mv[1] == q.mv[1])))
+      return;
+  }
   // tiles: luma 20x20 at (x0-4, y0-4) stride 20 in win; chroma 12x12 each in hph / hpv
   uint8_t* ty = sm.win;
   uint8_t* tc[2] = {sm.hph, sm.hpv};
@@ -1933,7 +1990,7 @@ __device__ __noinline__ void deblock_mb(const FrameParams& fp, const StreamDev& 
   }
   __syncwarp();
   bool intra = q.flags & kFlagIntra;
-  bool internal = intra || q.cbp_luma != 0;
+  bool internal = intra || q.cbp_luma != 0 || split;
   bool skip_odd = q.flags & kFlagT8;
   int qpq = q.qp, qpcq = chroma_qp(qpq);
   for (int dir = 0; dir < 2; dir++) {
@@ -1947,7 +2004,7 @@ __device__ __noinline__ void deblock_mb(const FrameParams& fp, const StreamDev& 
         pm = nullptr;
       }
       int bs[4];
-      if (!edge_bs(q, pm ? pm : &q, dir, e, bs)) continue;
+      if (!edge_bs<kMv4>(q, pm ? pm : &q, dir, e, bs, &qm, dir == 0 ? &lm : &tm)) continue;
       int qpl, qpc;
       if (!pm) { qpl = qpq; qpc = qpcq; }
       else { qpl = (qpq + pm->qp + 1) >> 1; qpc = (qpcq + chroma_qp(pm->qp) + 1) >> 1; }
@@ -1994,8 +2051,14 @@ __device__ __forceinline__ int diag_len(const FrameParams& fp, int d) {
   return hi >= lo ? hi - lo + 1 : 0;
 }
 
+struct NoSearchSmem {};
+template <int kForm>
+using FormSmem = typename std::conditional<kForm != 0, SearchSmem, NoSearchSmem>::type;
+
+template <int kForm>
 __global__ void __launch_bounds__(32) wavefront_step_kernel(FrameParams fp, const StreamDev* __restrict__ streams, int step) {
   __shared__ Smem sm;
+  __shared__ FormSmem<kForm> ss;
   const StreamDev& sd = streams[blockIdx.y];
   int na = diag_len(fp, step);
   int nd = fp.deblock ? diag_len(fp, step - 3) : 0;
@@ -2005,15 +2068,18 @@ __global__ void __launch_bounds__(32) wavefront_step_kernel(FrameParams fp, cons
     Ctx c{&fp, &sd, mbx, mby, mby * fp.mb_w + mbx};
     if (sd.kind == RG_FRAME_IDR) {
       load_source(c, sm);
-      analyse_intra_mb(c, sm);
+      if constexpr (kForm != 0) analyse_intra_mb_search(c, sm);
+      else analyse_intra_mb(c, sm);
     } else {
-      analyse_p_mb(c, sm, nullptr);
+      if constexpr (kForm != 0) analyse_p_mb_search(c, sm, ss, nullptr);
+      else analyse_p_mb(c, sm, nullptr);
     }
   } else if (k - na < nd) {
     int d = step - 3;
     int mby = diag_first(fp, d) + (k - na), mbx = d - 2 * mby;
-    deblock_mb(fp, sd, mbx, mby, sm);
+    deblock_mb<kForm != 0>(fp, sd, mbx, mby, sm);
   }
+  (void)ss;
 }
 
 // Border extension (enc.rs:165 extend_borders) of the padding that takes its values from
@@ -2101,8 +2167,10 @@ __device__ __noinline__ void picture_row_done(int* rows_done, int* ready, int se
 
 // At least 16 warps per SM: up to 128 registers a thread, so nothing spills (4.5 % faster than 20,
 // which held it to 96 registers with spills).
+template <int kForm>
 __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
   __shared__ Smem sm;
+  __shared__ FormSmem<kForm> ss;
   const int lane = lane_id();
   const int S = fp.n_streams, H = fp.mb_h, Wm = fp.mb_w;
   // Warps on the first deblock_sms SMs take deblocking segments first, on the next intra_sms SMs
@@ -2165,9 +2233,11 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
         Ctx c{&fp, &sd, x, y, y * Wm + x};
         if (sd.kind == RG_FRAME_IDR) {
           load_source(c, sm);
-          analyse_intra_mb(c, sm);
+          if constexpr (kForm != 0) analyse_intra_mb_search(c, sm);
+          else analyse_intra_mb(c, sm);
         } else {
-          analyse_p_mb(c, sm, has_prev ? &pw : nullptr);
+          if constexpr (kForm != 0) analyse_p_mb_search(c, sm, ss, has_prev ? &pw : nullptr);
+          else analyse_p_mb(c, sm, has_prev ? &pw : nullptr);
           if (pw.failed) { failed = true; break; }
         }
         publish(ana_rows + y, x + 1);
@@ -2185,7 +2255,7 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
           failed = true;
           break;
         }
-        deblock_mb(fp, sd, x, y, sm);
+        deblock_mb<kForm != 0>(fp, sd, x, y, sm);
         // Macroblock (x, y - 1) is final now: (x + 1, y - 1) was deblocked before this one. In
         // the last row, so is (x - 1, y), and the last macroblock is final after its own pass.
         __syncwarp();
@@ -2203,6 +2273,7 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
     atomicMax(pp.reach, reach_y);
     atomicMax(pp.reach + 1, reach_x);
   }
+  (void)ss;
 }
 
 // The launch's error word (and the reach its reference waits saw) into mapped host memory, queued
@@ -2287,9 +2358,10 @@ static int max_diag_len(const FrameParams& fp) {
   return best;
 }
 
-void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st) {
+void launch_wavefront_step(const FrameParams& fp, const StreamDev* d_streams, int step, cudaStream_t st, int form) {
   dim3 grid(2 * max_diag_len(fp), fp.n_streams);
-  wavefront_step_kernel<<<grid, 32, 0, st>>>(fp, d_streams, step);
+  if (form) wavefront_step_kernel<1><<<grid, 32, 0, st>>>(fp, d_streams, step);
+  else wavefront_step_kernel<0><<<grid, 32, 0, st>>>(fp, d_streams, step);
 }
 
 int pipeline_sms(int device) {
@@ -2302,9 +2374,10 @@ int pipeline_sms(int device) {
 // overlap more of each other's waits, until the SM's front end saturates and every macroblock on
 // the critical path slows (measured on B200, 1080p 8 x 15 pictures, launch time: 7 per SM
 // 62.9 ms, 8 61.0, 10 59.1, 12 57.4, 14 56.0, 16 55.8, 18 56.2, 20-21 56.3).
-int pipeline_grid(int device) {
+int pipeline_grid(int device, int form) {
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel, 32, 0);
+  if (form) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel<1>, 32, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel<0>, 32, 0);
   return (per_sm < 16 ? per_sm : 16) * pipeline_sms(device);
 }
 
@@ -2368,7 +2441,7 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
                      size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
                      int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
-                     int* host_reach, cudaStream_t st) {
+                     int* host_reach, cudaStream_t st, int form) {
   int S = fp.n_streams, H = fp.mb_h;
   PipeParams pp;
   pp.ticket = counters;
@@ -2392,7 +2465,8 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.host_err = host_err;
   pp.reach = pp.rows_done + frames * S;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;
-  pipeline_kernel<<<g, 32, 0, st>>>(fp, d_streams, pp);
+  if (form) pipeline_kernel<1><<<g, 32, 0, st>>>(fp, d_streams, pp);
+  else pipeline_kernel<0><<<g, 32, 0, st>>>(fp, d_streams, pp);
   error_to_host_kernel<<<1, 1, 0, st>>>(pp.error, pp.reach, host_err, host_reach);
 }
 

@@ -174,6 +174,7 @@ struct rg_ctx {
     int* h_err = nullptr;                // mapped host: the launch's error word
     int* h_reach = nullptr;              // mapped host: 1 + the reach its reference waits saw [2]
     cudaEvent_t done = nullptr;          // after the launch
+    std::vector<const rg_mb_hint*> hints;  // learned form: [f][s] (empty otherwise)
   };
   Pending pend[2];
   int pend_head = 0, pend_count = 0;
@@ -190,6 +191,10 @@ struct rg_ctx {
   int a_seq[2] = {0, 0}, a_frames[2] = {0, 0};
   int launch_seq = 0;
   int a_slot = 0;
+  int form = RG_FORM_PLAIN;        // analysis form (rg_set_analysis_form)
+  int search_range = 32;           // integer search range of the search forms
+  MbMv4* mv4s = nullptr;           // [S][nslots][n_mb] quadrant vectors (search forms; on first use)
+  std::vector<const rg_mb_hint*> hints;  // learned form: the next call's hints (rg_set_hints)
   std::vector<int> frames;         // frames analysed per stream
   std::vector<StreamQp> qps;       // QP of each stream (rg_set_stream_qp; default cfg.qp)
   // metrics scratch
@@ -331,6 +336,7 @@ void rg_destroy(rg_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->pics);
   cudaFree(c->infos);
+  cudaFree(c->mv4s);
   cudaFree(c->recs);
   cudaFree(c->srcs);
   cudaFree(c->unf);
@@ -387,7 +393,9 @@ int rg_keep_unfiltered(rg_ctx* c, int32_t enable) {
 void* rg_cuda_stream(rg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                             const int32_t* kinds, rg_mb_out* rec_base, int only = -1);
+                             const int32_t* kinds, rg_mb_out* rec_base, int only = -1,
+                             const rg_mb_hint* const* hints = nullptr);
+static int take_hints(rg_ctx* c, int count, const char* who, std::vector<const rg_mb_hint*>& out);
 static int resolve_pending(rg_ctx* c, bool wait_out);
 static int resolve_oldest(rg_ctx* c);
 static int auto_lag(const rg_ctx* c);
@@ -397,14 +405,35 @@ int rg_analyse_batch_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t 
   if (!c) return fail(RG_ERR_INVALID, "rg_analyse_batch_device: null context");
   int r = resolve_pending(c, false);
   if (r) return r;
-  return enqueue_wavefront(c, dev_planes, stride_y, stride_uv, kinds, nullptr);
+  std::vector<const rg_mb_hint*> hv;
+  r = take_hints(c, c->S, "rg_analyse_batch_device", hv);
+  if (r) return r;
+  return enqueue_wavefront(c, dev_planes, stride_y, stride_uv, kinds, nullptr, -1, hv.empty() ? nullptr : hv.data());
+}
+
+// The learned form's hints for a call of `count` pictures (rg_set_hints before the call); none for
+// the other forms.
+static int take_hints(rg_ctx* c, int count, const char* who, std::vector<const rg_mb_hint*>& out) {
+  out.clear();
+  if (c->form != RG_FORM_LEARNED) {
+    c->hints.clear();
+    return RG_OK;
+  }
+  if ((int)c->hints.size() != count)
+    return fail(RG_ERR_STATE, "%s: the learned form needs %d hint arrays (rg_set_hints), %d set", who, count,
+                (int)c->hints.size());
+  for (int i = 0; i < count; i++)
+    if (!c->hints[i]) return fail(RG_ERR_INVALID, "%s: null hint array %d", who, i);
+  out.swap(c->hints);
+  c->hints.clear();
+  return RG_OK;
 }
 
 // One picture of every stream (or of stream `only`), one launch per anti-diagonal step; records
 // at rec_base (default: the first picture's records). dev_planes and kinds hold one entry per
 // stream launched.
 static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
-                             const int32_t* kinds, rg_mb_out* rec_base, int only) {
+                             const int32_t* kinds, rg_mb_out* rec_base, int only, const rg_mb_hint* const* hints) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_batch_device: null argument");
   if (stride_y < (size_t)c->cfg.width || stride_uv < (size_t)(c->cfg.width + 1) / 2)
     return fail(RG_ERR_INVALID, "rg_analyse_batch_device: stride too small");
@@ -450,6 +479,10 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
     d.kind = kinds[i];
     apply_qp(d, c->qps[s]);
     d.pad_ = 0;
+    d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + par) * c->n_mb : nullptr;
+    d.hint = hints ? hints[i] : nullptr;
+    d.search_range = c->search_range;
+    d.pad2_ = 0;
   }
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
@@ -458,7 +491,7 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
   CK(cudaMemcpyAsync(c->d_streams[slot], h, sizeof(StreamDev) * n, cudaMemcpyHostToDevice, c->stream));
   CK(cudaEventRecord(c->slot_done[slot], c->stream));
   int steps = wavefront_steps(fp);
-  for (int t = 0; t < steps; t++) launch_wavefront_step(fp, c->d_streams[slot], t, c->stream);
+  for (int t = 0; t < steps; t++) launch_wavefront_step(fp, c->d_streams[slot], t, c->stream, c->form != RG_FORM_PLAIN);
   launch_extend_borders(fp, c->d_streams[slot], c->stream);
   CK(cudaGetLastError());
   for (int i = 0; i < n; i++) c->frames[only >= 0 ? only : i]++;
@@ -496,6 +529,11 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
         if (!dev_planes[(f * S + s) * 3 + p])
           return fail(RG_ERR_INVALID, "rg_analyse_gops_device: picture %d stream %d null plane", f, s);
     }
+  std::vector<const rg_mb_hint*> hv;
+  {
+    int r = take_hints(c, frames * S, "rg_analyse_gops_device", hv);
+    if (r) return r;
+  }
   int slot = c->slot;
   c->slot ^= 1;
   CK(cudaEventSynchronize(c->slot_done[slot]));
@@ -521,6 +559,10 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
       d.kind = kinds[f * S + s];
       apply_qp(d, c->qps[s]);
       d.pad_ = 0;
+      d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + cur) * c->n_mb : nullptr;
+      d.hint = hv.empty() ? nullptr : hv[f * S + s];
+      d.search_range = c->search_range;
+      d.pad2_ = 0;
     }
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
@@ -555,7 +597,7 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   *(volatile int*)p.h_err = 0;  // the launch that used this word before was resolved
   launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->qbeg, c->qend, c->deblock_sms,
                   c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq, c->d_err + pslot,
-                  c->d_err + 2 + 2 * pslot, c->stream);
+                  c->d_err + 2 + 2 * pslot, c->stream, c->form != RG_FORM_PLAIN);
   CK(cudaGetLastError());
   CK(cudaEventRecord(p.done, c->stream));
   p.planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
@@ -567,6 +609,7 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   p.rec = rec_base;
   p.out = nullptr;
   p.out_bytes = 0;
+  p.hints = hv;
   c->pend_count++;
   for (int s = 0; s < S; s++) c->frames[s] += frames;
   return RG_OK;
@@ -618,7 +661,7 @@ int rg_set_pipeline_tuning(rg_ctx* c, const rg_pipeline_tuning* t) {
   c->intra_sms = intra_sms < 0 ? 0 : (intra_sms > 0 ? intra_sms : default_intra_sms(c->sms));
   c->tasks_frames = -1;
   if (grid > 0) c->grid = grid;
-  else c->grid = pipeline_grid(c->cfg.device);
+  else c->grid = pipeline_grid(c->cfg.device, c->form != RG_FORM_PLAIN);
   c->timeout_ns = timeout_ms > 0 ? (unsigned long long)timeout_ms * 1000000ull : 2000000000ull;
   return RG_OK;
 }
@@ -740,7 +783,8 @@ static int resolve_oldest(rg_ctx* c) {
     rg_ctx::Pending& q = c->pend[(c->pend_head + k) & 1];
     for (int f = 0; f < q.frames; f++) {
       int r = enqueue_wavefront(c, q.planes.data() + (size_t)f * S * 3, q.sy, q.suv, q.kinds.data() + (size_t)f * S,
-                                q.rec + (size_t)f * S * c->n_mb);
+                                q.rec + (size_t)f * S * c->n_mb, -1,
+                                q.hints.empty() ? nullptr : q.hints.data() + (size_t)f * S);
       if (r) return r;
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -761,6 +805,37 @@ static int resolve_pending(rg_ctx* c, bool wait_out) {
   }
   CK(cudaStreamSynchronize(c->stream));
   if (wait_out && c->a_out) CK(cudaStreamSynchronize(c->a_out));
+  return RG_OK;
+}
+
+int rg_set_analysis_form(rg_ctx* c, int32_t form, int32_t search_range) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_analysis_form: null context");
+  if (form != RG_FORM_PLAIN && form != RG_FORM_FULLSEARCH && form != RG_FORM_LEARNED)
+    return fail(RG_ERR_INVALID, "rg_set_analysis_form: form %d", form);
+  if (form != RG_FORM_PLAIN && c->cfg.profile == RG_PROFILE_BASELINE)
+    return fail(RG_ERR_UNSUPPORTED, "rg_set_analysis_form: the search forms code partitions with CABAC (Main / High)");
+  if (form != RG_FORM_PLAIN && (search_range < 1 || search_range > kMaxSearchRange))
+    return fail(RG_ERR_INVALID, "rg_set_analysis_form: search range %d outside 1..%d", search_range, kMaxSearchRange);
+  int r = resolve_pending(c, true);
+  if (r) return r;
+  if (form != RG_FORM_PLAIN && !c->mv4s) {
+    size_t n = sizeof(MbMv4) * c->n_mb * c->nslots * c->S;
+    if (cudaMalloc((void**)&c->mv4s, n) != cudaSuccess) return fail(RG_ERR_OOM, "rg_set_analysis_form: %zu bytes", n);
+    CK(cudaMemset(c->mv4s, 0, n));
+  }
+  bool default_grid = c->grid == pipeline_grid(c->cfg.device, c->form != RG_FORM_PLAIN);
+  c->form = form;
+  if (form != RG_FORM_PLAIN) c->search_range = search_range;
+  if (default_grid) c->grid = pipeline_grid(c->cfg.device, form != RG_FORM_PLAIN);
+  c->hints.clear();
+  return RG_OK;
+}
+
+int rg_set_hints(rg_ctx* c, const rg_mb_hint* const* dev_hints, int32_t count) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_hints: null context");
+  if (count < 0 || (count > 0 && !dev_hints)) return fail(RG_ERR_INVALID, "rg_set_hints: %d hint arrays", count);
+  if (c->form != RG_FORM_LEARNED) return fail(RG_ERR_STATE, "rg_set_hints: the context is not in the learned form");
+  c->hints.assign(dev_hints, dev_hints + count);
   return RG_OK;
 }
 
@@ -785,6 +860,7 @@ static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, 
     for (int i = 0; i < 2; i++) {
       if (cudaMalloc((void**)&c->a_srcs[i], nsrc) != cudaSuccess || cudaMalloc((void**)&c->a_recs[i], nrec) != cudaSuccess)
         return fail(RG_ERR_OOM, "rg_analyse_gops_async: staging of %zu + %zu bytes", nsrc, nrec);
+      CK(cudaMemset(c->a_recs[i], 0, nrec));
       for (cudaEvent_t* e : {&c->a_in_done[i], &c->a_kern_done[i], &c->a_out_done[i]})
         CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
       size_t nflags = sizeof(int) * S * c->max_frames;
@@ -957,7 +1033,10 @@ int rg_analyse_frame(rg_ctx* c, int32_t stream, const uint8_t* y, const uint8_t*
   if (r) return r;
   uint8_t* d = c->srcs + c->src_bytes() * stream;
   const uint8_t* dev[3] = {d, d + (size_t)w * c->cfg.height, d + (size_t)w * c->cfg.height + (size_t)cw * ((c->cfg.height + 1) / 2)};
-  r = enqueue_wavefront(c, dev, w, cw, &kind, nullptr, stream);
+  std::vector<const rg_mb_hint*> hv;
+  r = take_hints(c, 1, "rg_analyse_frame", hv);
+  if (r) return r;
+  r = enqueue_wavefront(c, dev, w, cw, &kind, nullptr, stream, hv.empty() ? nullptr : hv.data());
   if (r) return r;
   if (out) {
     CK(cudaMemcpyAsync(out, c->recs + (size_t)stream * c->n_mb, sizeof(rg_mb_out) * c->n_mb, cudaMemcpyDeviceToHost,

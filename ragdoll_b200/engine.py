@@ -29,8 +29,15 @@ RECORD_DTYPE = np.dtype([
     ("mv", "<i2", (2,)), ("mvd", "<i2", (2,)), ("i4_modes", "u1", (16,)),
     ("nz_mask", "<u2"), ("reserved1", "<u2"), ("luma", "<i2", (256,)), ("luma_dc", "<i2", (16,)),
     ("chroma_dc", "<i2", (2, 4)), ("chroma_ac", "<i2", (2, 4, 16)),
+    ("part_mv", "<i2", (4, 2)), ("part_mvd", "<i2", (4, 2)), ("part_type", "u1"), ("reserved2", "u1", (3,)),
 ])
-assert RECORD_DTYPE.itemsize == 852
+assert RECORD_DTYPE.itemsize == 888
+
+# Analysis forms (rg_set_analysis_form) and the learned form's per-macroblock hint (rg_mb_hint).
+RG_FORM_PLAIN, RG_FORM_FULLSEARCH, RG_FORM_LEARNED = 0, 1, 2
+RG_MB_P_L0_16X8, RG_MB_P_L0_8X16, RG_MB_P_8X8 = 4, 5, 6
+HINT_DTYPE = np.dtype([("part_mask", "u1"), ("reserved", "u1"), ("mv_off", "i1", (2,)), ("i4_mask", "<u2", (16,))])
+assert HINT_DTYPE.itemsize == 36
 
 # Every symbol include/ragdoll_cuda.h declares.
 EXPORTS = [
@@ -45,7 +52,7 @@ EXPORTS = [
     "rg_encoder_threads", "rg_encoder_context", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_encoder_latencies",
     "rg_quality_frame_prev",
     "rg_vmaf_lite_plane", "rg_set_stream_qp", "rg_encoder_set_stream_qp", "rg_analyse_gops_stream",
-    "rg_analyse_gops_fetch",
+    "rg_analyse_gops_fetch", "rg_set_analysis_form", "rg_set_hints",
 ]
 
 
@@ -138,6 +145,8 @@ def lib() -> ctypes.CDLL:
     L.rg_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_analyse_gops_stream.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_analyse_gops_fetch.argtypes = [P, P, ctypes.c_int32]
+    L.rg_set_analysis_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
+    L.rg_set_hints.argtypes = [P, P, ctypes.c_int32]
     L.rg_encoder_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_quality_frame_prev.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, u8p,
                                         ctypes.c_size_t, ctypes.POINTER(RgQuality)]
@@ -293,6 +302,17 @@ class Engine:
         planes = (ctypes.c_void_p * len(dev_planes))(*dev_planes)
         k = (ctypes.c_int32 * len(kinds))(*kinds)
         _check(lib().rg_analyse_gops_device(self.h, planes, stride_y, stride_uv, k, frames))
+
+    def set_analysis_form(self, form: int, search_range: int = 32) -> None:
+        """Plain (byte-identical Balanced), full-search or learned analysis of the next calls
+        (rg_set_analysis_form); the search forms need a Main or High profile context."""
+        _check(lib().rg_set_analysis_form(self.h, form, search_range))
+
+    def set_hints_device(self, dev_hints) -> None:
+        """The learned form's hints of the next call: device addresses of one rg_mb_hint array
+        (n_mb records, HINT_DTYPE) per picture and stream, in the call's [f][s] order."""
+        arr = (ctypes.c_void_p * len(dev_hints))(*dev_hints)
+        _check(lib().rg_set_hints(self.h, arr, len(dev_hints)))
 
     def set_pipeline_tuning(self, lag: int = 0, seg: int = 0, grid: int = 0, timeout_ms: int = 0,
                             deblock_sms: int = 0, intra_sms: int = 0) -> None:

@@ -8,12 +8,14 @@ from oracle_lib import OracleEncoder
 
 FIELDS = ["mb_type", "i16_mode", "chroma_mode", "cbp", "transform_8x8", "qp", "mv", "mvd",
           "i4_modes", "luma", "luma_dc", "chroma_dc", "chroma_ac"]
+# the search forms' partition fields
+SEARCH_FIELDS = FIELDS + ["part_mv", "part_mvd", "part_type"]
 
 
-def first_record_mismatch(a: np.ndarray, b: np.ndarray, mb_w: int):
+def first_record_mismatch(a: np.ndarray, b: np.ndarray, mb_w: int, fields=FIELDS):
     """(mb_x, mb_y, field, oracle value, engine value) of the first difference, else None."""
     for i in range(len(a)):
-        for f in FIELDS:
+        for f in fields:
             if f == "i4_modes" and a[i]["mb_type"] != 3:
                 continue
             if not np.array_equal(a[i][f], b[i][f]):

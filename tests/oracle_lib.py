@@ -16,7 +16,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[1]
 LIB_PATH = ROOT / "oracle" / "liboracle.so"
 
-MB_TYPES = {0: "P_Skip", 1: "P_L0_16x16", 2: "I16x16", 3: "I4x4"}
+MB_TYPES = {0: "P_Skip", 1: "P_L0_16x16", 2: "I16x16", 3: "I4x4", 4: "P_L0_16x8", 5: "P_L0_8x16", 6: "P_8x8"}
 
 
 class MbOut(ctypes.Structure):
@@ -29,6 +29,8 @@ class MbOut(ctypes.Structure):
         ("i4_modes", ctypes.c_uint8 * 16), ("nz_mask", ctypes.c_uint16), ("reserved1", ctypes.c_uint16),
         ("luma", ctypes.c_int16 * 256), ("luma_dc", ctypes.c_int16 * 16),
         ("chroma_dc", ctypes.c_int16 * 8), ("chroma_ac", ctypes.c_int16 * 128),
+        ("part_mv", ctypes.c_int16 * 8), ("part_mvd", ctypes.c_int16 * 8), ("part_type", ctypes.c_uint8),
+        ("reserved2", ctypes.c_uint8 * 3),
     ]
 
 
@@ -38,6 +40,7 @@ RECORD_DTYPE = np.dtype([
     ("mv", "<i2", (2,)), ("mvd", "<i2", (2,)), ("i4_modes", "u1", (16,)),
     ("nz_mask", "<u2"), ("reserved1", "<u2"), ("luma", "<i2", (256,)), ("luma_dc", "<i2", (16,)),
     ("chroma_dc", "<i2", (2, 4)), ("chroma_ac", "<i2", (2, 4, 16)),
+    ("part_mv", "<i2", (4, 2)), ("part_mvd", "<i2", (4, 2)), ("part_type", "u1"), ("reserved2", "u1", (3,)),
 ])
 assert RECORD_DTYPE.itemsize == ctypes.sizeof(MbOut)
 
@@ -60,6 +63,8 @@ def lib():
         L.oracle_enc_recon.argtypes = [ctypes.c_void_p, u8p, u8p, u8p, ctypes.c_int]
         L.oracle_mb_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.oracle_record_size.restype = ctypes.c_int
+        L.oracle_enc_set_form.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.oracle_enc_set_hints.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_pixel_ops.restype = ctypes.c_ulonglong
         L.oracle_pixel_ops.argtypes = [ctypes.c_int]
         for fn in ("oracle_ssim_plane", "oracle_ms_ssim_plane", "oracle_psnr_plane"):
@@ -95,6 +100,15 @@ class OracleEncoder:
         if getattr(self, "h", None):
             lib().oracle_enc_destroy(self.h)
             self.h = None
+
+    def set_form(self, form, search_range=32):
+        """Search forms (1 full search, 2 learned): decisions and reconstruction only, no bitstream."""
+        lib().oracle_enc_set_form(self.h, form, search_range)
+
+    def set_hints(self, hints):
+        """The learned form's hints of the next frame (a HINT_DTYPE array of mb_w * mb_h records)."""
+        self._hints = np.ascontiguousarray(hints)
+        lib().oracle_enc_set_hints(self.h, self._hints.ctypes.data)
 
     def encode(self, frame):
         """Returns (annex_b_bytes, records[mb_h*mb_w])."""
