@@ -349,6 +349,176 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+LEARNED_METRIC = "1080p H.264 encode frames/s: learned vs plain GPU, equal PSNR, <=2% bit cost"
+QPS = (22, 26, 30, 34)
+CNN_FLOP_PER_MB = 2 * (22 * 22 * 32 * 18 + 20 * 20 * 32 * 288 + 18 * 18 * 32 * 288)  # 24x24 crop, three 3x3 convs
+
+
+def bd_rate(r1, p1, r2, p2) -> float:
+    """Bjontegaard delta rate (%) of curve 2 against curve 1: mean log-rate difference over the PSNR
+    range both cover, each curve interpolated piecewise-cubically (monotone) in PSNR."""
+    from scipy.interpolate import PchipInterpolator
+    p1, p2, l1, l2 = map(np.asarray, (p1, p2, np.log10(r1), np.log10(r2)))
+    o1, o2 = np.argsort(p1), np.argsort(p2)
+    lo, hi = max(p1.min(), p2.min()), min(p1.max(), p2.max())
+    if hi <= lo:
+        return float("nan")
+    xs = np.linspace(lo, hi, 401)
+    d = PchipInterpolator(p2[o2], l2[o2])(xs) - PchipInterpolator(p1[o1], l1[o1])(xs)
+    return float((10 ** (np.trapezoid(d, xs) / (hi - lo)) - 1) * 100)
+
+
+def run_learned(args, rank, world, local):
+    """The learned form against the plain and full-search forms on the 1080p workload (8 GOPs x 15,
+    High profile): device frames/s of each form at QP 26 (one persistent launch of the 120 pictures;
+    the learned form's network inference included), then bits and luma PSNR of every form at QP 22,
+    26, 30 and 34 (records written by the host CABAC writer, reconstructions compared with the
+    source) and the Bjontegaard delta rates. `no_net` is the learned form with fixed candidates
+    instead of the network's (what the network gains)."""
+    import torch
+
+    from ragdoll_b200.engine import (RG_FORM_FULLSEARCH, RG_FORM_LEARNED, RG_FORM_PLAIN, RG_FRAME_IDR, RG_FRAME_P,
+                                     RG_PROFILE_HIGH, BitstreamWriter, Engine)
+    from ragdoll_b200.learned import WEIGHTS, CandidateNet, hints_for, prior_hints
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    gops = FRAMES // GOP
+    clip = make_clip(clip_seed(0), FRAMES)
+    cw, ch = (W + 1) // 2, (H + 1) // 2
+    fbytes = W * H + 2 * cw * ch
+    host = np.empty((FRAMES, fbytes), np.uint8)
+    for i, (y, u, v) in enumerate(clip):
+        host[i] = np.concatenate([y.reshape(-1), u.reshape(-1), v.reshape(-1)])
+    dev = torch.from_numpy(host).to(f"cuda:{local}")
+    base = dev.data_ptr()
+
+    def planes(i):
+        p = base + i * fbytes
+        return [p, p + W * H, p + W * H + cw * ch]
+
+    net = CandidateNet.trained(local)
+    idx = [g * GOP + f for g in range(gops) for f in range(GOP)]
+    prev = [i if i % GOP == 0 else i - 1 for i in idx]
+    hints, _ = hints_for(net, [base + i * fbytes for i in idx], [base + i * fbytes for i in prev], W, H, W)
+    hint_of = {i: hints[k] for k, i in enumerate(idx)}
+    n_mb = ((W + 15) // 16) * ((H + 15) // 16)
+    prior = torch.from_numpy(prior_hints(n_mb).view(np.uint8)).to(f"cuda:{local}")
+    forms = {"plain": RG_FORM_PLAIN, "fullsearch": RG_FORM_FULLSEARCH, "learned": RG_FORM_LEARNED,
+             "no_net": RG_FORM_LEARNED}
+    torch.cuda.synchronize()
+
+    # network inference alone: the 120 pictures' hints
+    st = torch.cuda.Stream(device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        net.predict_hints([base + i * fbytes for i in idx], [base + i * fbytes for i in prev], W, H, W,
+                          [h.data_ptr() for h in hints], None, st.cuda_stream)
+    e0.record(st)
+    reps = 5
+    for _ in range(reps):
+        net.predict_hints([base + i * fbytes for i in idx], [base + i * fbytes for i in prev], W, H, W,
+                          [h.data_ptr() for h in hints], None, st.cuda_stream)
+    e1.record(st)
+    e1.synchronize()
+    net.check(st.cuda_stream)
+    cnn_ms = e0.elapsed_time(e1) / reps
+
+    # 1. speed at QP 26: persistent launches, sources resident
+    speed = {}
+    for name, form in forms.items():
+        if name == "no_net":
+            continue
+        eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
+        if form != RG_FORM_PLAIN:
+            eng.set_analysis_form(form, 32)
+        if form == RG_FORM_LEARNED:
+            eng.set_hint_net(net)   # each launch first runs the network on its own sources
+        stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+        ptrs, kinds = [], []
+        for f in range(GOP):
+            for g in range(gops):
+                ptrs += planes(g * GOP + f)
+                kinds.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+        steps = args.steps if form != RG_FORM_FULLSEARCH else max(1, min(args.steps, 3))
+        for _ in range(max(args.warmup, 1)):
+            eng.analyse_gops_device(ptrs, W, cw, kinds, GOP)
+        eng.sync()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            eng.analyse_gops_device(ptrs, W, cw, kinds, GOP)
+        b.record(stream)
+        b.synchronize()
+        eng.sync()
+        ms = a.elapsed_time(b) / steps
+        speed[name] = {"frames_per_s": round(FRAMES / (ms / 1000), 2), "ms_per_step": round(ms, 3), "steps": steps}
+        eng.close()
+
+    # 2. rate and distortion at four QPs (per-picture calls; every access unit written)
+    rd = {name: {} for name in forms}
+    for qp in QPS:
+        for name, form in forms.items():
+            eng = Engine(W, H, qp, profile=RG_PROFILE_HIGH, num_streams=gops, device=local)
+            if form != RG_FORM_PLAIN:
+                eng.set_analysis_form(form, 32)
+            writers = [BitstreamWriter(W, H, qp, profile=RG_PROFILE_HIGH) for _ in range(gops)]
+            bits, psnr = 0, []
+            for f in range(GOP):
+                kind = RG_FRAME_IDR if f == 0 else RG_FRAME_P
+                ptrs = []
+                for g in range(gops):
+                    ptrs += planes(g * GOP + f)
+                if name == "learned":
+                    eng.set_hints_device([hint_of[g * GOP + f].data_ptr() for g in range(gops)])
+                elif name == "no_net":
+                    eng.set_hints_device([prior.data_ptr()] * gops)
+                eng.analyse_device(ptrs, W, cw, [kind] * gops)
+                recs = eng.records()
+                for g in range(gops):
+                    bits += 8 * len(writers[g].picture(recs[g], kind))
+                    y = eng.recon_coded(g)[0][:H, :W].astype(np.int32)
+                    mse = float(np.mean((y - clip[g * GOP + f][0].astype(np.int32)) ** 2))
+                    psnr.append(10 * np.log10(255.0 ** 2 / max(mse, 1e-9)))
+            rd[name][qp] = {"kbits": round(bits / 1000, 1), "psnr_y": round(float(np.mean(psnr)), 4)}
+            eng.close()
+
+    def curve(name):
+        return [rd[name][q]["kbits"] for q in QPS], [rd[name][q]["psnr_y"] for q in QPS]
+
+    bd = {}
+    for a, b in (("plain", "learned"), ("fullsearch", "learned"), ("plain", "fullsearch"), ("fullsearch", "no_net"),
+                 ("no_net", "learned")):
+        ra, pa = curve(a)
+        rb, pb = curve(b)
+        bd[f"{b}_vs_{a}"] = round(bd_rate(ra, pa, rb, pb), 3)
+    tflops = n_mb * FRAMES * CNN_FLOP_PER_MB / (cnn_ms / 1000) / 1e12
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    line = {
+        "metric": LEARNED_METRIC, "value": speed["learned"]["frames_per_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": speed["learned"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network / u8,int32 analysis",
+        "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
+        "config": {**bench_config(1), "workload": "1080p High, 120 frames = 8 GOPs x 15, QP 26 for speed; QP 22/26/30/34 "
+                                                 "for rate and PSNR; +-32 integer search of the search forms",
+                   "network_weights": WEIGHTS.name},
+        "speed": speed,
+        "learned_over_plain": round(speed["learned"]["frames_per_s"] / speed["plain"]["frames_per_s"], 4),
+        "learned_over_fullsearch": round(speed["learned"]["frames_per_s"] / speed["fullsearch"]["frames_per_s"], 4),
+        "bd_rate_pct": bd, "rd": rd,
+        "network": {"ms_per_120_pictures": round(cnn_ms, 3), "tflops": round(tflops, 1),
+                    "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
+                                 "frac": round(tflops / peak, 4),
+                                 "flop_per_mb": CNN_FLOP_PER_MB, "kernel": "cnn_infer_kernel"}},
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------------------------------------
 def run_engine(args, rank, world, local):
     import torch
@@ -471,7 +641,10 @@ def run_engine(args, rank, world, local):
     enc_threads = max(2, (os.cpu_count() or 1) // max(local_world, 1))
     enc = H264Encoder(W, H, QP, profile=RG_PROFILE_HIGH, keyint=GOP, streams=gops, max_frames=GOP,
                       device=local, threads=enc_threads)
+    # every wave is the workload's 8 GOP chunks, each coded as by a fresh encoder per chunk (the
+    # pipeline's own shape: IDR with idr_pic_id 0, then 14 P pictures)
     for _ in range(2):                         # both wave slots once
+        enc.new_gops()
         enc.submit(frames_host)
     enc.collect()
     enc.collect()
@@ -479,6 +652,7 @@ def run_engine(args, rank, world, local):
     t0 = time.perf_counter()
     out_bytes = 0
     for k in range(args.steps):
+        enc.new_gops()
         enc.submit(frames_host)
         if k:
             out_bytes += sum(len(au) for row in enc.collect() for au in row)
@@ -630,7 +804,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched workload: keep the library's default launch shape for every size")
-    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched"],
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched", "learned"],
                     help="the 1080p 8-GOP workload, or the batched-streams configuration (64 mixed-size streams)")
     ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],
                     help="one persistent launch for all 15 pictures of the 8 GOPs, or one launch per anti-diagonal")
@@ -659,6 +833,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args, rank, world, local)
+        return
+    if args.workload == "learned":
+        run_learned(args, rank, world, local)
         return
     run_engine(args, rank, world, local)
 

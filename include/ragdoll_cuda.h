@@ -289,6 +289,53 @@ typedef struct rg_mb_hint {
     uint16_t i4_mask[16];   /* bit m: Intra4x4PredMode m is tried for 4x4 block b (decoding order) */
 } rg_mb_hint;
 
+/* ---- the learned form's candidate network (no counterpart in the reference) ----------------- */
+/*
+ * A small CNN over each macroblock and a 4-sample border (24 x 24 luma of the picture and of the
+ * previous picture): three 3x3 convolutions of 32 channels with ReLU, then heads over the 18 x 18
+ * map's mean (4 partition-type logits, a 2-component offset of the integer search's centre in units
+ * of 16 quarter samples) and over each 4x4 block's mean (9 intra 4x4 mode logits). Inference runs
+ * in BF16 on the tensor cores; training in f32 on the CUDA cores. Parameters are rg_net_param_count()
+ * floats: conv weights [32][in][3][3] and biases of the three layers, then the partition head
+ * [4][32] + 4, the offset head [2][32] + 2 and the intra head [9][32] + 9.
+ */
+typedef struct rg_net rg_net;
+int32_t rg_net_param_count(void);
+/* A network on `device` with parameters drawn from `seed` (He-uniform). NULL on failure. */
+rg_net* rg_net_create(int32_t device, uint64_t seed);
+void rg_net_destroy(rg_net* net);
+int rg_net_set_params(rg_net* net, const float* params, int32_t count);
+int rg_net_get_params(const rg_net* net, float* params, int32_t count);
+/*
+ * Hints of n_pictures pictures on the device: dev_cur[k] / dev_prev[k] the luma planes (display
+ * size width x height, row stride `stride`; prev = cur for an IDR picture), dev_hints[k] receives
+ * mb_w * mb_h rg_mb_hint (the top three partition types, the rounded offset, the top three intra
+ * 4x4 modes of each block), dev_logits[k] (or dev_logits NULL) mb_w * mb_h * 150 floats (partition
+ * 4, offset 2, intra 4x4 9 per block in raster order). Asynchronous on `stream`; rg_net_check
+ * reports a wait on the tensor cores that gave up.
+ */
+int rg_net_predict_hints(rg_net* net, const uint8_t* const* dev_cur, const uint8_t* const* dev_prev, int32_t n_pictures,
+                         int32_t width, int32_t height, size_t stride, rg_mb_hint* const* dev_hints,
+                         float* const* dev_logits, void* stream);
+int rg_net_check(rg_net* net, void* stream);
+/* Training crops: sample k is macroblock (mb_xy[2k], mb_xy[2k+1]) of the luma planes cur[k] /
+ * prev[k] (device, display size): 2 x 24 x 24 bytes each into dev_out. */
+int rg_net_crops(rg_net* net, const uint8_t* const* cur, const uint8_t* const* prev, const int32_t* mb_xy, int32_t n,
+                 int32_t width, int32_t height, size_t stride, uint8_t* dev_out, void* stream);
+/*
+ * One forward and backward pass over n crops (device arrays): labels dev_part [n] (partition type,
+ * -1 none), dev_i4 [n][16] (intra 4x4 mode of each raster 4x4 block, -1 none), dev_mv [n][2] (the
+ * offset target in units of 16 quarter samples) with dev_mvv [n] (0: none). Loss = mean
+ * cross-entropy of the partition labels + mean cross-entropy of the block labels + mv_weight * mean
+ * Huber loss of the offsets. dev_logits (n * 150 floats), loss_out and grads_out (host, the
+ * parameters' layout) may be NULL. The gradients stay for rg_net_adam_step.
+ */
+int rg_net_forward_backward(rg_net* net, const uint8_t* dev_crops, int32_t n, const int32_t* dev_part,
+                            const int32_t* dev_i4, const float* dev_mv, const int32_t* dev_mvv, float mv_weight,
+                            float* dev_logits, float* loss_out, float* grads_out);
+/* Adam (beta 0.9 / 0.999) step of the last gradients with learning rate lr. */
+int rg_net_adam_step(rg_net* net, float lr);
+
 /*
  * Selects the analysis form of the context's next calls (RG_FORM_*) and the integer search range
  * of the search forms (1..128 samples; ignored by the plain form). The learned form needs hints
@@ -303,6 +350,15 @@ int rg_set_analysis_form(rg_ctx* ctx, int32_t form, int32_t search_range);
  * call's planes). They must stay valid until the call is resolved. No counterpart in the reference.
  */
 int rg_set_hints(rg_ctx* ctx, const rg_mb_hint* const* dev_hints, int32_t count);
+
+/*
+ * The network the learned form predicts its hints with (NULL: none): a pipelined call
+ * (rg_analyse_gops*) without rg_set_hints first runs `net` on its own sources -- each picture's luma
+ * with the previous picture's of the same call (the picture itself for an IDR picture and for the
+ * call's first picture) -- on the context's stream, into hint buffers of the context. The network
+ * must outlive its use. No counterpart in the reference.
+ */
+int rg_set_hint_net(rg_ctx* ctx, rg_net* net);
 
 /* Waits for queued device work of the context. */
 int rg_sync(rg_ctx* ctx);
@@ -460,6 +516,17 @@ int rg_encoder_submit(rg_encoder* enc, const uint8_t* const* planes, size_t stri
  * the sizes and the total are returned and the wave stays to be collected.
  */
 int64_t rg_encoder_collect(rg_encoder* enc, uint8_t* out, size_t cap, int64_t* sizes);
+/*
+ * Starts a new GOP on every stream with the next submitted picture, as the pipeline's fresh
+ * H264Encoder per chunk does (GopRingEncoder::encode_wave, crates/ragdoll-pipeline/src/lib.rs:580-585):
+ * the streams' picture counters restart, so that picture is an IDR picture with idr_pic_id 0 and
+ * frame_num / POC from 0. Waves already submitted keep their counters.
+ */
+int rg_encoder_new_gops(rg_encoder* enc);
+/* The analysis form of the encoder's next waves (rg_set_analysis_form on its context); the learned
+ * form with its candidate network `net` (rg_set_hint_net), which must outlive its use. Not while
+ * waves are in flight. No counterpart in the reference. */
+int rg_encoder_set_form(rg_encoder* enc, int32_t form, int32_t search_range, rg_net* net);
 /*
  * Per-picture latency of the wave collected last, [f * num_streams + s]: milliseconds from its
  * rg_encoder_submit to its access unit being written (up to n values into ms); returns the

@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libragdoll_cuda.so"
 BUILD = PKG / "_build"
 
-SOURCES = ["engine_kernels.cu", "ssim_kernels.cu", "rg_api.cu", "ssim_noalloc.cu", "cavlc_writer.cpp",
+SOURCES = ["engine_kernels.cu", "ssim_kernels.cu", "rg_api.cu", "ssim_noalloc.cu", "candidate_net.cu", "cavlc_writer.cpp",
            "cabac_writer.cpp", "containers.cpp", "host_encoder.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

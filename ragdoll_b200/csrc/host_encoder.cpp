@@ -327,6 +327,22 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
   return (int64_t)total;
 }
 
+int rg_encoder_set_form(rg_encoder* e, int32_t form, int32_t search_range, rg_net* net) {
+  if (!e) return efail(RG_ERR_INVALID, "rg_encoder_set_form: null encoder");
+  if (e->pending) return efail(RG_ERR_STATE, "rg_encoder_set_form: waves in flight");
+  int r = rg_set_analysis_form(e->ctx, form, search_range);
+  if (r) return r;
+  return rg_set_hint_net(e->ctx, form == RG_FORM_LEARNED ? net : nullptr);
+}
+
+int rg_encoder_new_gops(rg_encoder* e) {
+  if (!e) return efail(RG_ERR_INVALID, "rg_encoder_new_gops: null encoder");
+  std::fill(e->coded.begin(), e->coded.end(), 0);
+  std::fill(e->idrs.begin(), e->idrs.end(), 0u);
+  std::fill(e->since.begin(), e->since.end(), 0u);
+  return RG_OK;
+}
+
 int32_t rg_encoder_latencies(const rg_encoder* e, double* ms, int32_t n) {
   if (!e) return efail(RG_ERR_INVALID, "rg_encoder_latencies: null encoder");
   int32_t k = (int32_t)e->last_latency_ms.size();

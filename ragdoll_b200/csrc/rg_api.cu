@@ -195,6 +195,9 @@ struct rg_ctx {
   int search_range = 32;           // integer search range of the search forms
   MbMv4* mv4s = nullptr;           // [S][nslots][n_mb] quadrant vectors (search forms; on first use)
   std::vector<const rg_mb_hint*> hints;  // learned form: the next call's hints (rg_set_hints)
+  rg_net* net = nullptr;           // learned form: the network that predicts a call's hints itself
+  rg_mb_hint* d_hints = nullptr;   // [2][max_frames][S][n_mb] hints the context predicted (two calls)
+  int hint_slot = 0;
   std::vector<int> frames;         // frames analysed per stream
   std::vector<StreamQp> qps;       // QP of each stream (rg_set_stream_qp; default cfg.qp)
   // metrics scratch
@@ -337,6 +340,7 @@ void rg_destroy(rg_ctx* c) {
   cudaFree(c->pics);
   cudaFree(c->infos);
   cudaFree(c->mv4s);
+  cudaFree(c->d_hints);
   cudaFree(c->recs);
   cudaFree(c->srcs);
   cudaFree(c->unf);
@@ -530,7 +534,25 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
           return fail(RG_ERR_INVALID, "rg_analyse_gops_device: picture %d stream %d null plane", f, s);
     }
   std::vector<const rg_mb_hint*> hv;
-  {
+  if (c->form == RG_FORM_LEARNED && c->net && c->hints.empty()) {
+    // the network reads each picture's luma and the previous picture's of the same call (the picture
+    // itself for the first one and for IDR pictures)
+    rg_mb_hint* base = c->d_hints + (size_t)c->hint_slot * c->max_frames * S * c->n_mb;
+    c->hint_slot ^= 1;
+    std::vector<const uint8_t*> cur((size_t)frames * S), prev((size_t)frames * S);
+    std::vector<rg_mb_hint*> dst((size_t)frames * S);
+    for (int f = 0; f < frames; f++)
+      for (int s = 0; s < S; s++) {
+        const size_t i = (size_t)f * S + s;
+        cur[i] = dev_planes[i * 3];
+        prev[i] = (f > 0 && kinds[i] == RG_FRAME_P) ? dev_planes[(i - S) * 3] : cur[i];
+        dst[i] = base + i * c->n_mb;
+      }
+    int r = rg_net_predict_hints(c->net, cur.data(), prev.data(), frames * S, c->cfg.width, c->cfg.height, stride_y,
+                                 dst.data(), nullptr, c->stream);
+    if (r) return r;
+    hv.assign(dst.begin(), dst.end());
+  } else {
     int r = take_hints(c, frames * S, "rg_analyse_gops_device", hv);
     if (r) return r;
   }
@@ -828,6 +850,18 @@ int rg_set_analysis_form(rg_ctx* c, int32_t form, int32_t search_range) {
   if (form != RG_FORM_PLAIN) c->search_range = search_range;
   if (default_grid) c->grid = pipeline_grid(c->cfg.device, form != RG_FORM_PLAIN);
   c->hints.clear();
+  return RG_OK;
+}
+
+int rg_set_hint_net(rg_ctx* c, rg_net* net) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_hint_net: null context");
+  int r = resolve_pending(c, true);
+  if (r) return r;
+  if (net && !c->d_hints) {
+    size_t n = sizeof(rg_mb_hint) * 2 * (size_t)c->max_frames * c->S * c->n_mb;
+    if (cudaMalloc((void**)&c->d_hints, n) != cudaSuccess) return fail(RG_ERR_OOM, "rg_set_hint_net: %zu bytes", n);
+  }
+  c->net = net;
   return RG_OK;
 }
 

@@ -106,6 +106,21 @@ class H264Encoder:
             out.append(row)
         return out
 
+    def set_form(self, form: int, search_range: int = 32, net=None) -> None:
+        """Analysis form of the next waves (rg_encoder_set_form): plain, full search, or learned with
+        its candidate network (ragdoll_b200.learned.CandidateNet)."""
+        rc = lib().rg_encoder_set_form(self.h, form, search_range, net.h if net is not None else None)
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+        self._net = net
+
+    def new_gops(self) -> None:
+        """The next submitted picture of every stream starts a new GOP (an IDR picture with
+        idr_pic_id 0), as a fresh encoder per GOP chunk of the pipeline (rg_encoder_new_gops)."""
+        rc = lib().rg_encoder_new_gops(self.h)
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+
     def latencies(self) -> np.ndarray:
         """Milliseconds from submit to access unit written, per picture ([f][s]) of the wave
         collected last (rg_encoder_latencies)."""

@@ -52,7 +52,10 @@ EXPORTS = [
     "rg_encoder_threads", "rg_encoder_context", "rg_encode_frame", "rg_encoder_submit", "rg_encoder_collect", "rg_encoder_latencies",
     "rg_quality_frame_prev",
     "rg_vmaf_lite_plane", "rg_set_stream_qp", "rg_encoder_set_stream_qp", "rg_analyse_gops_stream",
-    "rg_analyse_gops_fetch", "rg_set_analysis_form", "rg_set_hints",
+    "rg_analyse_gops_fetch", "rg_set_analysis_form", "rg_set_hints", "rg_encoder_new_gops",
+    "rg_net_param_count", "rg_net_create", "rg_net_destroy", "rg_net_set_params", "rg_net_get_params",
+    "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
+    "rg_set_hint_net", "rg_encoder_set_form",
 ]
 
 
@@ -147,6 +150,21 @@ def lib() -> ctypes.CDLL:
     L.rg_analyse_gops_fetch.argtypes = [P, P, ctypes.c_int32]
     L.rg_set_analysis_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_set_hints.argtypes = [P, P, ctypes.c_int32]
+    L.rg_encoder_new_gops.argtypes = [P]
+    L.rg_set_hint_net.argtypes = [P, P]
+    L.rg_encoder_set_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32, P]
+    L.rg_net_param_count.restype = ctypes.c_int32
+    L.rg_net_create.restype = P
+    L.rg_net_create.argtypes = [ctypes.c_int32, ctypes.c_uint64]
+    L.rg_net_destroy.argtypes = [P]
+    L.rg_net_set_params.argtypes = [P, P, ctypes.c_int32]
+    L.rg_net_get_params.argtypes = [P, P, ctypes.c_int32]
+    L.rg_net_predict_hints.argtypes = [P, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_size_t,
+                                       P, P, P]
+    L.rg_net_check.argtypes = [P, P]
+    L.rg_net_crops.argtypes = [P, P, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_size_t, P, P]
+    L.rg_net_forward_backward.argtypes = [P, P, ctypes.c_int32, P, P, P, P, ctypes.c_float, P, P, P]
+    L.rg_net_adam_step.argtypes = [P, ctypes.c_float]
     L.rg_encoder_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_quality_frame_prev.argtypes = [P, ctypes.c_int32, u8p, u8p, u8p, ctypes.c_size_t, ctypes.c_size_t, u8p,
                                         ctypes.c_size_t, ctypes.POINTER(RgQuality)]
@@ -307,6 +325,12 @@ class Engine:
         """Plain (byte-identical Balanced), full-search or learned analysis of the next calls
         (rg_set_analysis_form); the search forms need a Main or High profile context."""
         _check(lib().rg_set_analysis_form(self.h, form, search_range))
+
+    def set_hint_net(self, net) -> None:
+        """The candidate network (ragdoll_b200.learned.CandidateNet or None) the learned form runs
+        on each pipelined call's own sources when no hints were set (rg_set_hint_net)."""
+        _check(lib().rg_set_hint_net(self.h, net.h if net is not None else None))
+        self._hint_net = net
 
     def set_hints_device(self, dev_hints) -> None:
         """The learned form's hints of the next call: device addresses of one rg_mb_hint array

@@ -1,0 +1,154 @@
+"""The learned form's candidate network on the GPU against its CPU oracle (GPU tests).
+
+* Training kernels (f32, CUDA cores): loss, logits and the gradient of every parameter of one
+  forward / backward pass equal the float64 oracle's (oracle/candidate_net_oracle.py, itself pinned
+  by finite differences) within f32 rounding.
+* Tensor-core inference (BF16 tcgen05 MMAs, strips of three macroblocks, pictures whose width is no
+  multiple of the strip): every logit equals the oracle's BF16 arithmetic within the stated
+  tolerance, and the hints are the top three of the GPU's own logits.
+* Training on full-search labels lowers the loss.
+* End to end: hints from the network drive the learned form; its records equal the oracle's with
+  the same hints, and its CABAC stream decodes (FFmpeg) to the engine's reconstruction.
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+import candidate_net_oracle as cno  # noqa: E402
+
+from gpu_parity_util import SEARCH_FIELDS, first_record_mismatch  # noqa: E402
+from oracle_lib import OracleEncoder  # noqa: E402
+from ragdoll_b200.synth import grating_clip  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+# BF16 inputs, weights and activations; f32 accumulation on the GPU against float64 in the oracle
+INFER_ATOL, INFER_RTOL = 0.03, 0.03
+
+
+def _params(seed):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(cno.N_PARAMS)
+    at = 0
+    for name, shape in cno.SHAPES:
+        n = int(np.prod(shape))
+        fan = np.prod(shape[1:]) if len(shape) > 1 else 32
+        p[at:at + n] = rng.normal(0, np.sqrt(2.0 / fan), n) if name[0] == "W" else rng.normal(0, 0.05, n)
+        at += n
+    return p.astype(np.float32)
+
+
+def test_training_pass_matches_oracle():
+    import torch
+
+    from ragdoll_b200.learned import CandidateNet
+    rng = np.random.default_rng(3)
+    n = 6
+    crops = rng.integers(0, 256, (n, 2, 24, 24)).astype(np.uint8)
+    part = rng.integers(-1, 4, n).astype(np.int32)
+    i4 = rng.integers(-1, 9, (n, 16)).astype(np.int32)
+    mv = rng.normal(0, 1.5, (n, 2)).astype(np.float32)
+    mvv = rng.integers(0, 2, n).astype(np.int32)
+    part[0], mvv[0] = 1, 1
+    p = _params(4)
+    net = CandidateNet(0, params=p)
+    d = {k: torch.from_numpy(v).cuda() for k, v in dict(c=crops, p=part, i=i4, m=mv, v=mvv).items()}
+    logits = torch.zeros(n * 150, dtype=torch.float32, device="cuda")
+    loss, grads = net.forward_backward(d["c"].data_ptr(), n, d["p"].data_ptr(), d["i"].data_ptr(), d["m"].data_ptr(),
+                                       d["v"].data_ptr(), 0.5, logits.data_ptr(), want_grads=True)
+    want_loss, want_grads, want_logits = cno.forward_backward(p.astype(np.float64), crops, part, i4, mv, mvv, 0.5)
+    assert abs(loss - want_loss) <= 1e-4 * max(1.0, abs(want_loss))
+    np.testing.assert_allclose(logits.cpu().numpy().reshape(n, 150), want_logits, rtol=1e-4, atol=1e-4)
+    scale = np.abs(want_grads).max()
+    err = np.abs(grads - want_grads)
+    assert err.max() <= 1e-3 * scale, (err.max(), scale, int(err.argmax()))
+    # every parameter group carries gradient
+    at = 0
+    for name, shape in cno.SHAPES:
+        k = int(np.prod(shape))
+        assert np.abs(want_grads[at:at + k]).max() > 0, name
+        at += k
+
+
+@pytest.mark.parametrize("w,h", [(80, 48), (200, 72)])
+def test_tensor_core_inference_matches_oracle(w, h):
+    import torch
+
+    from ragdoll_b200.engine import HINT_DTYPE
+    from ragdoll_b200.learned import CandidateNet, hints_for
+    rng = np.random.default_rng(w)
+    cur = rng.integers(0, 256, (h, w)).astype(np.uint8)
+    prev = np.clip(cur.astype(int) + rng.integers(-30, 31, (h, w)), 0, 255).astype(np.uint8)
+    p = _params(5)
+    net = CandidateNet(0, params=p)
+    tc, tp = torch.from_numpy(cur).cuda(), torch.from_numpy(prev).cuda()
+    hints, logits = hints_for(net, [tc.data_ptr()], [tp.data_ptr()], w, h, w, with_logits=True)
+    net.check()
+    torch.cuda.synchronize()
+    got = logits[0].cpu().numpy().reshape(-1, 150)
+    mb_w, mb_h = (w + 15) // 16, (h + 15) // 16
+    crops = np.zeros((mb_w * mb_h, 2, 24, 24), np.uint8)
+    for my in range(mb_h):
+        for mx in range(mb_w):
+            ys = np.clip(np.arange(24) + my * 16 - 4, 0, h - 1)
+            xs = np.clip(np.arange(24) + mx * 16 - 4, 0, w - 1)
+            crops[my * mb_w + mx, 0] = cur[np.ix_(ys, xs)]
+            crops[my * mb_w + mx, 1] = prev[np.ix_(ys, xs)]
+    want = cno.forward_bf16(p.astype(np.float64), crops)
+    err = np.abs(got - want)
+    assert (err <= INFER_ATOL + INFER_RTOL * np.abs(want)).all(), (err.max(), np.unravel_index(err.argmax(), err.shape))
+    hh = hints[0].cpu().numpy().view(HINT_DTYPE)
+    for m in range(mb_w * mb_h):
+        top = np.argsort(-got[m, :4], kind="stable")[:3]
+        assert hh["part_mask"][m] == sum(1 << int(t) for t in top)
+        assert tuple(hh["mv_off"][m]) == tuple(np.clip(np.rint(16 * got[m, 4:6]), -127, 127).astype(int))
+
+
+def test_training_on_full_search_labels_lowers_the_loss():
+    from ragdoll_b200.learned import CandidateNet, generate_training_set, train
+    data = generate_training_set(8, 160, 96, 4, search_range=16, streams=4)
+    assert int((data[1] >= 0).sum()) > 50 and int((data[2] >= 0).sum()) > 50
+    net = CandidateNet(0, seed=7)
+    losses = train(net, data, epochs=3, batch=64, lr=3e-3, lr_end=3e-4)
+    assert losses[-1] < losses[0], losses
+
+
+def test_learned_form_with_network_hints_matches_oracle_and_decodes():
+    import torch
+
+    import ffmpeg_decode
+    from ragdoll_b200.engine import RG_FORM_LEARNED, RG_FRAME_IDR, RG_FRAME_P, BitstreamWriter, Engine, HINT_DTYPE
+    from ragdoll_b200.learned import WEIGHTS, CandidateNet, hints_for
+    w, h, qp, F = 240, 128, 26, 5
+    frames = grating_clip(w, h, F, seed=1234, motion=10.0, rects=3)
+    net = CandidateNet.trained(0) if WEIGHTS.exists() else CandidateNet(0, seed=3)
+    luma = [torch.from_numpy(np.ascontiguousarray(fr[0])).cuda() for fr in frames]
+    hints, _ = hints_for(net, [l.data_ptr() for l in luma], [luma[max(f - 1, 0)].data_ptr() if f else luma[0].data_ptr()
+                                                             for f, l in enumerate(luma)], w, h, w)
+    net.check()
+    torch.cuda.synchronize()
+    eng = Engine(w, h, qp, profile=2, max_frames=F)
+    eng.set_analysis_form(RG_FORM_LEARNED, 32)
+    eng.set_hints_device([x.data_ptr() for x in hints])
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] for f in range(F)]
+    recs = eng.analyse_gops([[fr] for fr in frames], kinds)
+    orc = OracleEncoder(w, h, qp, profile=2, keyint=F + 1)
+    orc.set_form(2, 32)
+    wr = BitstreamWriter(w, h, qp, profile=2)
+    aus = []
+    for f in range(F):
+        orc.set_hints(hints[f].cpu().numpy().view(HINT_DTYPE))
+        _, want = orc.encode(frames[f])
+        m = first_record_mismatch(want, recs[f, 0], orc.mb_w, SEARCH_FIELDS)
+        assert m is None, f"picture {f}: {m}"
+        aus.append(wr.picture(recs[f, 0], kinds[f][0]))
+    final = [p.copy() for p in eng.recon_coded(0)]
+    for a, b in zip(orc.recon(), final):
+        assert np.array_equal(a, b)
+    if not ffmpeg_decode.available():
+        pytest.skip("FFmpeg libraries not found")
+    dec = ffmpeg_decode.decode(aus)
+    for k in range(3):
+        assert np.array_equal(dec[-1][k], final[k][:dec[-1][k].shape[0], :dec[-1][k].shape[1]])
