@@ -662,6 +662,28 @@ def run_engine(args, rank, world, local):
     enc_threads = enc.threads
     enc.close()
 
+    # SSIM and MS-SSIM of 120 luma plane pairs in one batched call (shared launches over every
+    # pair and pyramid level); the pairs are pictures of the step's clip (their values do not change
+    # the work). Algorithmic bytes per 1080p pair: both planes read at the five levels, and four
+    # decimations reading one level and writing the next: ~5.98 W H.
+    from ragdoll_b200.engine import ssim_batch_device
+    qstream = torch.cuda.Stream(device=local)
+    pa = [base + i * fbytes for i in range(FRAMES)]
+    pb = [base + ((i + 1) % FRAMES) * fbytes for i in range(FRAMES)]
+    ssim_batch_device(pa, pb, W, H, W, W, device=local, stream=qstream.cuda_stream)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q_reps = 3
+    tq = time.perf_counter()
+    q0.record(qstream)
+    for _ in range(q_reps):
+        ssim_batch_device(pa, pb, W, H, W, W, device=local, stream=qstream.cuda_stream)
+    q1.record(qstream)
+    q1.synchronize()
+    q_wall_ms = (time.perf_counter() - tq) * 1000 / q_reps
+    q_ms = q0.elapsed_time(q1) / q_reps
+    lv = sum(4.0 ** -k for k in range(5))
+    q_bytes = FRAMES * W * H * (2 * lv + 2 * (lv - 4.0 ** -4) + 2 * (lv - 1))
+
     # per-launch duration of the dominant kernel
     steps_per_frame = (eng.mb_w - 1) + 2 * (eng.mb_h - 1) + 1 + 3
     if args.mode == "pipelined":
@@ -715,6 +737,12 @@ def run_engine(args, rank, world, local):
                          "traffic": round(TRAFFIC_PER_FRAME * FRAMES) if args.mode == "pipelined" else None,
                          "kernel": kernel_name, "launch_ms": round(launch_ms, 5),
                          "bytes_per_launch": round(bytes_per_launch)},
+            "quality": {"what": "SSIM + 5-scale MS-SSIM of 120 1080p luma plane pairs, one rg_ssim_batch_device call",
+                        "ms_device": round(q_ms, 3), "ms_call": round(q_wall_ms, 3),
+                        "pairs_per_s": round(FRAMES / (q_ms / 1000), 1),
+                        "roofline": {"bound": "hbm", "achieved": round(q_bytes / (q_ms / 1000) / 1e9, 1), "peak": peak,
+                                     "unit": "GB/s", "frac": round(q_bytes / (q_ms / 1000) / 1e9 / peak, 4),
+                                     "bytes_per_call": round(q_bytes)}},
             "cpu_baseline": cpu,
             "parity": parity,
             "clocks": clk,

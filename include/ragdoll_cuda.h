@@ -424,6 +424,18 @@ int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8
                   size_t stride_b, int32_t width, int32_t height, double* ssim, double* ms_ssim);
 
 /*
+ * SSIM and (if ms_ssim) 5-scale MS-SSIM of n plane pairs of one size already on the device --
+ * e.g. every reconstructed picture of a job against its source -- in shared launches: one 2x2
+ * decimation launch per pyramid level for all pairs, then one SSIM launch over every pair and
+ * level, then one for the row totals. Same arithmetic as rg_ssim_plane. dev_a[i] / dev_b[i]: device
+ * planes with the given strides; ssim / ms_ssim: host arrays of n doubles (either may be NULL).
+ * Synchronous on cuda_stream (NULL: legacy default stream); allocates its working memory.
+ */
+int rg_ssim_batch_device(int32_t device, const uint8_t* const* dev_a, const uint8_t* const* dev_b, int32_t n,
+                         int32_t width, int32_t height, size_t stride_a, size_t stride_b, double* ssim, double* ms_ssim,
+                         void* cuda_stream);
+
+/*
  * Allocation-free SSIM / MS-SSIM of two planes already on the device. No counterpart in the
  * reference: it exists for callers that may not call cudaMalloc / cudaFree when they measure --
  * a frame loop whose device memory is all reserved by another allocator (a framework's caching

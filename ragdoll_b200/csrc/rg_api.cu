@@ -1406,6 +1406,29 @@ int rg_ssim_plane(int32_t device, const uint8_t* a, size_t stride_a, const uint8
   return r;
 }
 
+int rg_ssim_batch_device(int32_t device, const uint8_t* const* dev_a, const uint8_t* const* dev_b, int32_t n,
+                         int32_t width, int32_t height, size_t stride_a, size_t stride_b, double* ssim, double* ms_ssim,
+                         void* cuda_stream) {
+  if (!dev_a || !dev_b || n < 1 || (!ssim && !ms_ssim)) return fail(RG_ERR_INVALID, "rg_ssim_batch_device: bad argument");
+  if (width < 8 || height < 8) return fail(RG_ERR_INVALID, "rg_ssim_batch_device: plane smaller than one 8x8 window");
+  if (stride_a < (size_t)width || stride_b < (size_t)width) return fail(RG_ERR_INVALID, "rg_ssim_batch_device: stride");
+  CK(cudaSetDevice(device));
+  std::vector<PlanePair> pairs;
+  for (int i = 0; i < n; i++) {
+    if (!dev_a[i] || !dev_b[i]) return fail(RG_ERR_INVALID, "rg_ssim_batch_device: null plane %d", i);
+    pairs.push_back({dev_a[i], (long)stride_a, dev_b[i], (long)stride_b, width, height});
+  }
+  std::vector<double> ss, ms;
+  std::vector<unsigned long long> sse;
+  int r = device_metrics(pairs, std::vector<bool>(n, ms_ssim != nullptr), (cudaStream_t)cuda_stream, ss, ms, sse);
+  if (r) return r;
+  for (int i = 0; i < n; i++) {
+    if (ssim) ssim[i] = ss[i];
+    if (ms_ssim) ms_ssim[i] = ms[i];
+  }
+  return RG_OK;
+}
+
 int64_t rg_pipeline_work_list(int32_t mb_w, int32_t mb_h, int32_t streams, int32_t frames, int32_t lag, int32_t seg,
                               int32_t split, const int32_t* kinds, int32_t* tasks, int64_t cap, int32_t* queues) {
   if (mb_w < 1 || mb_h < 1 || streams < 1 || frames < 1 || seg < 1 || lag < 0 || !tasks || !queues)

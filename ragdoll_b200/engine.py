@@ -55,7 +55,7 @@ EXPORTS = [
     "rg_analyse_gops_fetch", "rg_set_analysis_form", "rg_set_hints", "rg_encoder_new_gops",
     "rg_net_param_count", "rg_net_create", "rg_net_destroy", "rg_net_set_params", "rg_net_get_params",
     "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
-    "rg_set_hint_net", "rg_encoder_set_form",
+    "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device",
 ]
 
 
@@ -152,6 +152,8 @@ def lib() -> ctypes.CDLL:
     L.rg_set_hints.argtypes = [P, P, ctypes.c_int32]
     L.rg_encoder_new_gops.argtypes = [P]
     L.rg_set_hint_net.argtypes = [P, P]
+    L.rg_ssim_batch_device.argtypes = [ctypes.c_int32, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_size_t, ctypes.c_size_t, P, P, P]
     L.rg_encoder_set_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32, P]
     L.rg_net_param_count.restype = ctypes.c_int32
     L.rg_net_create.restype = P
@@ -434,6 +436,18 @@ def vmaf_lite_plane(ref: np.ndarray, dist: np.ndarray, prev: np.ndarray = None, 
         _check(lib().rg_vmaf_lite_plane(device, _u8(r), r.strides[0], _u8(d), d.strides[0], r.shape[1], r.shape[0],
                                         _u8(q), q.strides[0], ctypes.byref(out)))
     return out.value
+
+
+def ssim_batch_device(dev_a, dev_b, width: int, height: int, stride_a: int, stride_b: int, device: int = 0,
+                      stream: int = 0, ms: bool = True):
+    """SSIM and MS-SSIM of len(dev_a) device plane pairs in shared launches (rg_ssim_batch_device);
+    returns two numpy arrays (MS-SSIM None when ms is False)."""
+    n = len(dev_a)
+    A = ctypes.c_void_p * n
+    s, m = np.zeros(n), (np.zeros(n) if ms else None)
+    _check(lib().rg_ssim_batch_device(device, A(*dev_a), A(*dev_b), n, width, height, stride_a, stride_b,
+                                      s.ctypes.data, m.ctypes.data if ms else None, stream or None))
+    return s, m
 
 
 def ssim_plane_device_noalloc(dev_a: int, stride_a: int, dev_b: int, stride_b: int, width: int, height: int,

@@ -90,3 +90,26 @@ def test_quality_report_of_reconstruction_matches_oracle():
             assert abs(q[key] - want[key]) <= TOL, key
         assert abs(q["ssim_db"] - want["ssim_db"]) <= 1e-4 and math.isfinite(q["ssim_db"])
         assert abs(q["vmaf_lite"] - want["vmaf_lite"]) <= VMAF_TOL
+
+
+def test_batched_ssim_of_many_pairs_matches_oracle():
+    """rg_ssim_batch_device: every pair of a batch (device planes, padded stride) equals the
+    oracle's SSIM and MS-SSIM within 1e-6, in one set of shared launches."""
+    import torch
+
+    from oracle_lib import ms_ssim_plane
+    from oracle_lib import ssim_plane as oracle_ssim
+    from ragdoll_b200.engine import ssim_batch_device
+    w, h, pad, n = 333, 197, 32, 6
+    rng = np.random.default_rng(9)
+    a = rng.integers(0, 256, (n, h, w)).astype(np.uint8)
+    b = np.clip(a.astype(int) + rng.integers(-25, 26, (n, h, w)), 0, 255).astype(np.uint8)
+    da = torch.zeros((n, h, w + pad), dtype=torch.uint8, device="cuda")
+    db = torch.zeros((n, h, w + pad), dtype=torch.uint8, device="cuda")
+    da[:, :, :w] = torch.from_numpy(a).cuda()
+    db[:, :, :w] = torch.from_numpy(b).cuda()
+    s, m = ssim_batch_device([da[i].data_ptr() for i in range(n)], [db[i].data_ptr() for i in range(n)], w, h,
+                             w + pad, w + pad)
+    for i in range(n):
+        assert abs(s[i] - oracle_ssim(a[i], b[i])) <= 1e-6
+        assert abs(m[i] - ms_ssim_plane(a[i], b[i])) <= 1e-6
