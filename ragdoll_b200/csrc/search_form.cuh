@@ -251,12 +251,25 @@ __device__ __forceinline__ void qpel4(const Smem& sm, int wx, int wy, int fx, in
 }
 __device__ __constant__ int8_t c_hstep[8][2] = {{0, -2}, {-2, 0}, {2, 0}, {0, 2}, {-2, -2}, {2, -2}, {-2, 2}, {2, 2}};
 
-__device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, int px, int py, int pw, int ph, int bx, int by,
-                                             const int* mvp, uint32_t lambda, const Bounds& bd, int* mv) {
-  const FrameParams& fp = *c.fp;
-  const int lane = lane_id();
-  stage_window(c.sd->ref_y, fp.stride_y, c.mbx * 16 + px + bx - 1, c.mby * 16 + py + by - 1, sm);
+// The half-sample planes in shared memory serve every part whose integer vector they were built
+// around: a macroblock-level window (origin one sample above-left of the macroblock displaced by the
+// vector) covers every 4x4 block of the macroblock at quarter-sample offsets -3..3.
+struct WinState {
+  int bx, by;  // integer vector of the planes held, or kNoWin
+};
+constexpr int kNoWin = 1 << 20;
+__device__ __forceinline__ void ensure_window(const Ctx& c, Smem& sm, WinState& ws, int bx, int by) {
+  if (ws.bx == bx && ws.by == by) return;
+  stage_window(c.sd->ref_y, c.fp->stride_y, c.mbx * 16 + bx - 1, c.mby * 16 + by - 1, sm);
   build_hpel(sm, 7);
+  ws.bx = bx;
+  ws.by = by;
+}
+
+__device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
+                                             int by, const int* mvp, uint32_t lambda, const Bounds& bd, int* mv) {
+  const int lane = lane_id();
+  ensure_window(c, sm, ws, bx, by);
   const int bw4 = pw >> 2, nblk = bw4 * (ph >> 2);
   const int m0x = 4 * bx, m0y = 4 * by;
   int cx = m0x, cy = m0y;
@@ -278,7 +291,7 @@ __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, int px, int
       if (ok) {
         const int ox = 4 * (blk % bw4), oy = 4 * (blk / bw4);
         uint32_t pa[4], sa[4];
-        qpel4(sm, (vx >> 2) - bx + 1 + ox, (vy >> 2) - by + 1 + oy, vx & 3, vy & 3, pa);
+        qpel4(sm, (vx >> 2) - bx + 1 + px + ox, (vy >> 2) - by + 1 + py + oy, vx & 3, vy & 3, pa);
 #pragma unroll
         for (int r = 0; r < 4; r++) sa[r] = *(const uint32_t*)&sm.src_y[(py + oy + r) * 16 + px + ox];
         s = satd4_regs(sa, pa);
@@ -307,14 +320,13 @@ __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, int px, int
   return best_key >> 4;
 }
 
-// The luma prediction of a part at quarter-sample vector mv into pred_y.
-__device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, int px, int py, int pw, int ph, const int* mv) {
-  const FrameParams& fp = *c.fp;
+// The luma prediction of a part at quarter-sample vector mv (within 3 quarter samples of 4 (bx, by),
+// the integer vector its refinement started from) into pred_y.
+__device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
+                                          int by, const int* mv) {
   const int lane = lane_id();
-  const int ix = mv[0] >> 2, iy = mv[1] >> 2, fx = mv[0] & 3, fy = mv[1] & 3;
-  stage_window(c.sd->ref_y, fp.stride_y, c.mbx * 16 + px + ix, c.mby * 16 + py + iy, sm);
-  build_hpel(sm, planes_needed(fx, fy));
-  QSrc q = qpel_src(sm, 0, 0, fx, fy);
+  ensure_window(c, sm, ws, bx, by);
+  QSrc q = qpel_src(sm, (mv[0] >> 2) - bx + 1 + px, (mv[1] >> 2) - by + 1 + py, mv[0] & 3, mv[1] & 3);
   for (int i = lane; i < pw * ph; i += 32) {
     const int r = i / pw, x = i - r * pw;
     int v = q.a[r * q.sa + x];
@@ -515,6 +527,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   int best_t = -1;
   uint32_t best_j = UMAX;
   int bmv[4][2], bmvd[4][2];  // per part (coding order) of the best type
+  WinState ws{kNoWin, kNoWin};  // the skip probe's window is not a refinement window
   for (int t = 0; t < 4; t++) {
     if (!((part_mask >> t) & 1)) continue;
     int own[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
@@ -526,7 +539,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
       const int8_t* g = c_parts[first + k];
       int mvp[2], mv[2];
       mv_pred(nb, g[4], g[5], g[6], g[7], own, done, mvp);
-      uint32_t cost = refine_part(c, sm, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv);
+      uint32_t cost = refine_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv);
       J += cost;
       pm[k][0] = mv[0]; pm[k][1] = mv[1];
       pd[k][0] = mv[0] - mvp[0]; pd[k][1] = mv[1] - mvp[1];
@@ -553,7 +566,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
       for (int q = 0; q < 4; q++)
         if ((qm >> q) & 1) { qmv[q][0] = bmv[k][0]; qmv[q][1] = bmv[k][1]; }
       const int8_t* g = c_parts[first + k];
-      predict_part(c, sm, g[0], g[1], g[2], g[3], bmv[k]);
+      predict_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], bmv[k]);
     }
   }
   // 5. intra 16x16 when the inter prediction is poor (the plain form's rule, enc.rs:3121-3156)
