@@ -519,6 +519,84 @@ def run_learned(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_4k(args, rank, world, local):
+    """The 4K configuration: 8 streams of 3840x2160 (+-48 px global motion, 24 rectangles), High
+    profile, QP 28, the learned form with a +-64 integer search -- its network run by the engine on
+    each call's sources, then one persistent launch of all streams' pictures -- and SSIM / MS-SSIM of
+    every reconstructed picture against its source in batched launches. One GOP (IDR + 14 P) per
+    stream per step (the configuration's 60 frames are four such steps)."""
+    import torch
+
+    from ragdoll_b200.engine import (RG_FORM_LEARNED, RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_HIGH, Engine,
+                                     ssim_batch_device)
+    from ragdoll_b200.learned import CandidateNet
+    from ragdoll_b200.synth import grating_clip
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    w4, h4, S, F, qp = 3840, 2160, 8, GOP, 28
+    cw, ch = w4 // 2, h4 // 2
+    fbytes = w4 * h4 + 2 * cw * ch
+    dev = torch.empty((S, F, fbytes), dtype=torch.uint8, device=f"cuda:{local}")
+    for s_ in range(S):
+        for f, (y, u, v) in enumerate(grating_clip(w4, h4, F, seed=5000 + s_, motion=48.0, rects=24)):
+            dev[s_, f] = torch.from_numpy(np.concatenate([y.reshape(-1), u.reshape(-1), v.reshape(-1)]))
+    base = dev.data_ptr()
+
+    def pic(s_, f):
+        p = base + (s_ * F + f) * fbytes
+        return [p, p + w4 * h4, p + w4 * h4 + cw * ch]
+
+    net = CandidateNet.trained(local)
+    eng = Engine(w4, h4, qp, profile=RG_PROFILE_HIGH, num_streams=S, device=local, max_frames=F)
+    eng.set_analysis_form(RG_FORM_LEARNED, 64)
+    eng.set_hint_net(net)
+    ptrs, kinds = [], []
+    for f in range(F):
+        for s_ in range(S):
+            ptrs += pic(s_, f)
+            kinds.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+    stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    for _ in range(max(args.warmup, 1)):
+        eng.analyse_gops_device(ptrs, w4, cw, kinds, F)
+    eng.sync()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, min(args.steps, 4))
+    a.record(stream)
+    for _ in range(steps):
+        eng.analyse_gops_device(ptrs, w4, cw, kinds, F)
+    b.record(stream)
+    b.synchronize()
+    eng.sync()
+    ms = a.elapsed_time(b) / steps
+    # SSIM / MS-SSIM: the final reconstruction of every stream against its source, and the batched
+    # throughput over all S x F pictures of a step (each against the next picture of its stream)
+    recon = torch.stack([torch.from_numpy(np.ascontiguousarray(eng.recon(s_)[0])) for s_ in range(S)]).to(f"cuda:{local}")
+    fin, fin_ms = ssim_batch_device([recon[s_].data_ptr() for s_ in range(S)], [pic(s_, F - 1)[0] for s_ in range(S)],
+                                    w4, h4, w4, w4, device=local)
+    pa = [pic(s_, f)[0] for s_ in range(S) for f in range(F)]
+    pb = [pic(s_, (f + 1) % F)[0] for s_ in range(S) for f in range(F)]
+    qs = torch.cuda.Stream(device=local)
+    ssim_batch_device(pa, pb, w4, h4, w4, w4, device=local, stream=qs.cuda_stream)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(qs)
+    ssim_batch_device(pa, pb, w4, h4, w4, w4, device=local, stream=qs.cuda_stream)
+    q1.record(qs)
+    q1.synchronize()
+    line = {"metric": "4K learned + batched: encode frames/s (8 streams of 3840x2160, one GPU)",
+            "value": round(S * F / (ms / 1000), 2), "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 1),
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 network / u8,int32 analysis",
+            "data": "synthetic (seeded gratings, +-48 px global motion, 24 moving rectangles, 3840x2160 8-bit 4:2:0)",
+            "config": {"workload": "8 streams x 3840x2160, one GOP (IDR + 14 P) each per step, High, QP 28, learned form, "
+                                   "+-64 integer search, network and analysis launches on one stream",
+                       "l2": "inputs larger than L2"},
+            "ssim_final": [round(float(x), 6) for x in fin], "ms_ssim_final": [round(float(x), 6) for x in fin_ms],
+            "ssim_batch": {"pairs": len(pa), "ms": round(q0.elapsed_time(q1), 3)}}
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 # ------------------------------------------------------------------------------------------------
 def run_engine(args, rank, world, local):
     import torch
@@ -832,7 +910,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched workload: keep the library's default launch shape for every size")
-    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched", "learned"],
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "batched", "learned", "4k"],
                     help="the 1080p 8-GOP workload, or the batched-streams configuration (64 mixed-size streams)")
     ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],
                     help="one persistent launch for all 15 pictures of the 8 GOPs, or one launch per anti-diagonal")
@@ -864,6 +942,9 @@ def main():
         return
     if args.workload == "learned":
         run_learned(args, rank, world, local)
+        return
+    if args.workload == "4k":
+        run_4k(args, rank, world, local)
         return
     run_engine(args, rank, world, local)
 
