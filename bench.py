@@ -832,6 +832,30 @@ def run_engine(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_profile_case_cnn(args, local):
+    """Small case for ncu of the network kernel: the hints of 8 pictures of the 1080p clip (two
+    launches of cnn_infer_kernel, 65 280 macroblocks each)."""
+    import torch
+
+    from ragdoll_b200.learned import CandidateNet, hints_for
+    torch.cuda.set_device(local)
+    clip = make_clip(2000, 9)
+    luma = torch.from_numpy(np.stack([fr[0] for fr in clip])).to(f"cuda:{local}")
+    net = CandidateNet.trained(local)
+    ptrs = [luma[i].data_ptr() for i in range(1, 9)]
+    prev = [luma[i - 1].data_ptr() for i in range(1, 9)]
+    times = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        hints_for(net, ptrs, prev, W, H, W)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    net.check()
+    print(json.dumps({"profile_case": "network hints of 8 1080p pictures", "ms": [round(t, 3) for t in times]}), flush=True)
+
+
 def run_profile_case(args, local):
     """Small case for ncu: one IDR batch and one P batch of the 8-GOP 1080p workload (16 frames),
     with the device time of each batch -- per anti-diagonal launches, or (pipelined) the first
@@ -915,7 +939,7 @@ def main():
     ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],
                     help="one persistent launch for all 15 pictures of the 8 GOPs, or one launch per anti-diagonal")
     ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
-                    choices=["wavefront", "pipelined"],
+                    choices=["wavefront", "pipelined", "cnn"],
                     help="a small slice of the workload (the ncu capture case)")
     ap.add_argument("--profile-frames", type=int, default=3, choices=range(1, 9),
                     help="pictures per stream of the pipelined profile case")
@@ -931,6 +955,9 @@ def main():
                     help="pipelined mode: macroblocks per work segment (0 = default)")
     args = ap.parse_args()
     rank, world, local = dist_env()
+    if args.profile_case == "cnn":
+        run_profile_case_cnn(args, local)
+        return
     if args.profile_case:
         run_profile_case(args, local)
         return

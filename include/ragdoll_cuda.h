@@ -345,6 +345,14 @@ int rg_net_adam_step(rg_net* net, float lr);
 int rg_set_analysis_form(rg_ctx* ctx, int32_t form, int32_t search_range);
 
 /*
+ * Decision constants of the search forms (test and tuning hook): the bits charged per partition
+ * type (16x16, 16x8, 8x16, 8x8; type_bits NULL: the defaults), times lambda, and the learned form's
+ * re-centrings of its +-2 window before the full search (`walk`, 0..64). No counterpart in the
+ * reference.
+ */
+int rg_set_search_tuning(rg_ctx* ctx, const int32_t* type_bits, int32_t walk);
+
+/*
  * Device hints of the learned form for the next pipelined or batched call: dev_hints[f * S + s] is
  * the device address of picture f of stream s's mb_w * mb_h rg_mb_hint records (the order of the
  * call's planes). They must stay valid until the call is resolved. No counterpart in the reference.

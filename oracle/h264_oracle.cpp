@@ -2248,7 +2248,8 @@ struct Encoder {
   // residual and late skip. Learned: +-2 around the predictor plus the hinted offset (the full
   // window when the 16x16 best lies on that window's edge), only the hinted types, and intra 4x4
   // blocks of IDR pictures restricted to their hinted modes.
-  int form = 0, search_range = 32;
+  int form = 0, search_range = 32, walk = 4;
+  int type_bits[4] = {1, 3, 3, 7};      // bits charged per partition type (x lambda)
   const rg_mb_hint* hints = nullptr;    // learned form: this picture's hints
   std::vector<uint8_t> mb_split;        // per MB: quadrant vectors differ
 
@@ -2414,8 +2415,17 @@ struct Encoder {
     int ibx[9], iby[9];
     int_search_s(x0, y0, src, lo[0], hi[0], lo[1], hi[1], mvp16, lambda, ibx, iby);
     if (h) {
-      bool edge = (ibx[0] == lo[0] && lo[0] > imin[0]) || (ibx[0] == hi[0] && hi[0] < imax[0]) ||
-                  (iby[0] == lo[1] && lo[1] > imin[1]) || (iby[0] == hi[1] && hi[1] < imax[1]);
+      auto on_edge = [&]() {
+        return (ibx[0] == lo[0] && lo[0] > imin[0]) || (ibx[0] == hi[0] && hi[0] < imax[0]) ||
+               (iby[0] == lo[1] && lo[1] > imin[1]) || (iby[0] == hi[1] && hi[1] < imax[1]);
+      };
+      bool edge = on_edge();
+      for (int it = 0; edge && it < walk; it++) {  // centre the window on its best again
+        int cc[2] = {ibx[0], iby[0]};
+        for (int c = 0; c < 2; c++) { lo[c] = std::max(cc[c] - 2, imin[c]); hi[c] = std::min(cc[c] + 2, imax[c]); }
+        int_search_s(x0, y0, src, lo[0], hi[0], lo[1], hi[1], mvp16, lambda, ibx, iby);
+        edge = on_edge();
+      }
       if (edge) {
         for (int c = 0; c < 2; c++) { lo[c] = std::max(fc[c] - R, imin[c]); hi[c] = std::min(fc[c] + R, imax[c]); }
         int_search_s(x0, y0, src, lo[0], hi[0], lo[1], hi[1], mvp16, lambda, ibx, iby);
@@ -2428,7 +2438,7 @@ struct Encoder {
     for (int t = 0; t < 4; t++) {
       if (!((part_mask >> t) & 1)) continue;
       int own[4][2] = {}, done = 0, pm[4][2] = {}, pd[4][2] = {};
-      uint32_t J = lambda * (t == 0 ? 1u : (t == 3 ? 7u : 3u));
+      uint32_t J = lambda * (uint32_t)type_bits[t];
       for (int k = 0; k < nparts[t]; k++) {
         const int* g = parts[first[t] + k];
         int mvp[2], mv[2];
@@ -2709,6 +2719,12 @@ void oracle_enc_set_form(void* h, int form, int search_range) {
   e->search_range = search_range;
 }
 void oracle_enc_set_hints(void* h, const rg_mb_hint* hints) { ((oracle::Encoder*)h)->hints = hints; }
+// The search forms' decision constants (rg_set_search_tuning).
+void oracle_enc_set_search_tuning(void* h, const int* type_bits, int walk) {
+  auto* e = (oracle::Encoder*)h;
+  for (int k = 0; k < 4; k++) e->type_bits[k] = type_bits[k];
+  e->walk = walk;
+}
 // Pixel differences evaluated by the SAD / SSD / SATD of every frame encoded so far in this
 // process (all threads); reset = 1 also sets the total back to 0.
 unsigned long long oracle_pixel_ops(int reset) {

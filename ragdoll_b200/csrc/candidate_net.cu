@@ -50,6 +50,7 @@ constexpr int kTiles1 = (22 * kRow + 127) / 128, kTiles2 = (20 * kRow + 127) / 1
 constexpr int kPos0 = ((kTiles1 * 128 + 2 * kRow + 2) + 127) / 128 * 128;  // positions of the input map
 constexpr int kPos1 = kTiles1 * 128, kPos2 = kTiles2 * 128;
 static_assert(kPos1 >= kTiles2 * 128 + 2 * kRow + 2 && kPos2 >= kTiles3 * 128 + 2 * kRow + 2, "tap reach");
+static_assert(kPos0 % 128 == 0, "input map staged 128 positions per thread step");
 static_assert(kTiles1 * 32 <= 512, "accumulators of one layer fit the tensor memory");
 // shared memory (bytes): A1 (4 planes of 8 channels) | A2 or the input | B operands | the rest
 constexpr int kPlane1 = kPos1 * 16, kPlane2 = kPos2 * 16;
@@ -105,6 +106,26 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
     if (ok) return true;
   }
   return false;
+}
+// 64 consecutive columns of this thread's lane (two accumulator tiles).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+      "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
+        "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
+        "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]),
+        "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
+        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   uint32_t r[32];
@@ -188,16 +209,21 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
     // input map: position r * kRow + c is sample (x0 - 4 + c, y0 - 4 + r), clamped to the picture;
     // 16 bytes each: the two channels and six zero channels
     const int y0 = mby * 16 - 4, x0 = mbx0 * 16 - 4;
-    for (int p = tid; p < kPos0; p += 128) {
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (p < 24 * kRow) {
-        int r = p / kRow, c = p - r * kRow;
-        int yy = min(max(y0 + r, 0), ip.height - 1), xx = min(max(x0 + c, 0), ip.width - 1);
-        __nv_bfloat162 two = __floats2bfloat162_rn(pix_norm(jb.cur[(size_t)yy * ip.stride + xx]),
-                                                   pix_norm(jb.prev[(size_t)yy * ip.stride + xx]));
-        v.x = *(uint32_t*)&two;
-      }
-      ((uint4*)A2)[p] = v;
+    constexpr int kPer = kPos0 / 128;
+    uint8_t ca[kPer], pa[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {  // all of this thread's loads in flight together
+      const int p = tid + 128 * k;
+      const int r = p / kRow, c = p - r * kRow;
+      const int yy = min(max(y0 + r, 0), ip.height - 1), xx = min(max(x0 + c, 0), ip.width - 1);
+      const size_t o = (size_t)yy * ip.stride + xx;
+      ca[k] = p < 24 * kRow ? jb.cur[o] : 128;
+      pa[k] = p < 24 * kRow ? jb.prev[o] : 128;
+    }
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+      __nv_bfloat162 two = __floats2bfloat162_rn(pix_norm(ca[k]), pix_norm(pa[k]));
+      ((uint4*)A2)[tid + 128 * k] = make_uint4(*(uint32_t*)&two, 0u, 0u, 0u);
     }
     for (int layer = 0; layer < 3; layer++) {
       fence_async_smem();
@@ -240,21 +266,26 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
       // conv1 -> A1; conv2 -> A2; conv3 -> A1 again (dead once conv2's MMAs completed), for the pooling
       uint8_t* dst = layer == 1 ? A2 : A1;
       const uint32_t dplane = layer == 1 ? kPlane2 : kPlane1;
-      for (int t = 0; t < tiles; t++) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 32), v);
-        const int p = t * 128 + warp * 32 + lane;
+      for (int t = 0; t < tiles; t += 2) {  // two tiles (64 accumulator columns) per load
+        float v[64];
+        if (t + 1 < tiles) tmem_ld64(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 32), v);
+        else tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 32), v);
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          uint32_t w[4];
+        for (int h = 0; h < 2; h++) {
+          if (t + h >= tiles) break;
+          const int p = (t + h) * 128 + warp * 32 + lane;
 #pragma unroll
-          for (int k = 0; k < 4; k++) {
-            float a = fmaxf(v[8 * q + 2 * k] + ms.bias[layer][8 * q + 2 * k], 0.0f);
-            float b = fmaxf(v[8 * q + 2 * k + 1] + ms.bias[layer][8 * q + 2 * k + 1], 0.0f);
-            __nv_bfloat162 two = __floats2bfloat162_rn(a, b);
-            w[k] = *(uint32_t*)&two;
+          for (int q = 0; q < 4; q++) {
+            uint32_t w[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              float a = fmaxf(v[32 * h + 8 * q + 2 * k] + ms.bias[layer][8 * q + 2 * k], 0.0f);
+              float b = fmaxf(v[32 * h + 8 * q + 2 * k + 1] + ms.bias[layer][8 * q + 2 * k + 1], 0.0f);
+              __nv_bfloat162 two = __floats2bfloat162_rn(a, b);
+              w[k] = *(uint32_t*)&two;
+            }
+            *(uint4*)(dst + q * dplane + p * 16) = make_uint4(w[0], w[1], w[2], w[3]);
           }
-          *(uint4*)(dst + q * dplane + p * 16) = make_uint4(w[0], w[1], w[2], w[3]);
         }
       }
     }

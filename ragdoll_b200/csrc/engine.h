@@ -67,7 +67,9 @@ struct StreamDev {
   MbMv4* mv4;              // this picture's quadrant vectors
   const rg_mb_hint* hint;  // learned form: this picture's hints (null: full search)
   int32_t search_range;    // integer search range of the full search (samples)
-  int32_t pad2_;
+  int32_t walk;            // learned form: re-centrings of the seed's window before the full search
+  uint16_t type_bits[4];   // search forms: bits charged per partition type (x lambda)
+  uint16_t pad3_[4];
 };
 
 // Frame-constant parameters of one wavefront (all streams share the size; qp / qpc / sb_* are the

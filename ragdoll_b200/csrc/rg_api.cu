@@ -21,7 +21,11 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr int kDefaultLag = 0;   // pipelined work order: 0 = derived from the reach of the searches
-constexpr int kDefaultSeg = 1;   // macroblocks per work segment (16 warps per SM: 1 is 2 % faster than 2)
+constexpr int kDefaultSeg = 1;
+// Search forms: bits charged per partition type (16x16, 16x8, 8x16, 8x8), times lambda, and the
+// learned form's window re-centrings before it falls back to the full search.
+constexpr uint16_t kDefaultTypeBits[4] = {1, 3, 3, 7};
+constexpr int kDefaultWalk = 4;   // macroblocks per work segment (16 warps per SM: 1 is 2 % faster than 2)
 // Deblocking SMs: one in five takes the deblocking queue first (30 of 148). Measured on B200 with
 // 16 warps per SM, 1080p 8 x 15 launch: 25 SMs 52.3-53.2 ms, 30 51.4-52.3, 35-40 52.6-52.8
 // (at 7 warps per SM, before the IDR path got faster: 16 SMs 1326 frames/s, 20-30 1394-1417).
@@ -193,6 +197,8 @@ struct rg_ctx {
   int a_slot = 0;
   int form = RG_FORM_PLAIN;        // analysis form (rg_set_analysis_form)
   int search_range = 32;           // integer search range of the search forms
+  int walk = kDefaultWalk;         // learned form: re-centrings of the seed's window
+  uint16_t type_bits[4] = {kDefaultTypeBits[0], kDefaultTypeBits[1], kDefaultTypeBits[2], kDefaultTypeBits[3]};
   MbMv4* mv4s = nullptr;           // [S][nslots][n_mb] quadrant vectors (search forms; on first use)
   std::vector<const rg_mb_hint*> hints;  // learned form: the next call's hints (rg_set_hints)
   rg_net* net = nullptr;           // learned form: the network that predicts a call's hints itself
@@ -486,7 +492,8 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
     d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + par) * c->n_mb : nullptr;
     d.hint = hints ? hints[i] : nullptr;
     d.search_range = c->search_range;
-    d.pad2_ = 0;
+    d.walk = c->walk;
+    for (int k = 0; k < 4; k++) { d.type_bits[k] = c->type_bits[k]; d.pad3_[k] = 0; }
   }
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
@@ -584,7 +591,8 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
       d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + cur) * c->n_mb : nullptr;
       d.hint = hv.empty() ? nullptr : hv[f * S + s];
       d.search_range = c->search_range;
-      d.pad2_ = 0;
+      d.walk = c->walk;
+      for (int k = 0; k < 4; k++) { d.type_bits[k] = c->type_bits[k]; d.pad3_[k] = 0; }
     }
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
@@ -862,6 +870,20 @@ int rg_set_hint_net(rg_ctx* c, rg_net* net) {
     if (cudaMalloc((void**)&c->d_hints, n) != cudaSuccess) return fail(RG_ERR_OOM, "rg_set_hint_net: %zu bytes", n);
   }
   c->net = net;
+  return RG_OK;
+}
+
+int rg_set_search_tuning(rg_ctx* c, const int32_t* type_bits, int32_t walk) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_search_tuning: null context");
+  if (walk < 0 || walk > 64) return fail(RG_ERR_INVALID, "rg_set_search_tuning: walk %d outside 0..64", walk);
+  for (int k = 0; k < 4; k++) {
+    int b = type_bits ? type_bits[k] : kDefaultTypeBits[k];
+    if (b < 0 || b > 4096) return fail(RG_ERR_INVALID, "rg_set_search_tuning: type bits %d", b);
+  }
+  int r = resolve_pending(c, true);
+  if (r) return r;
+  for (int k = 0; k < 4; k++) c->type_bits[k] = (uint16_t)(type_bits ? type_bits[k] : kDefaultTypeBits[k]);
+  c->walk = walk;
   return RG_OK;
 }
 

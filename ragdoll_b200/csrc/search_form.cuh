@@ -9,15 +9,16 @@
 //      each of the nine partition parts (16x16; 16x8 top, bottom; 8x16 left, right; four 8x8) the
 //      vector of least SAD + lambda * (bits(4 vx - mvp.x) + bits(4 vy - mvp.y)) against the 16x16
 //      predictor, first in raster order on ties. Full search: the window is +-search_range around
-//      the 16x16 predictor. Learned: +-2 around the predictor plus the hinted offset, and the full
-//      window when the 16x16 part's best lies on the small window's edge (and not on the vector
-//      bounds);
+//      the 16x16 predictor. Learned: +-2 around the predictor plus the hinted offset; while the
+//      16x16 part's best lies on that window's edge (and not on the vector bounds) the window is
+//      centred on it again, up to `walk` times, and then the full window is searched;
 //   3. for every partition type tried (all four; learned: the hinted ones), each part in coding
 //      order from its integer best: half-sample step (centre, then 8 neighbours at distance 2,
 //      quarter units) and quarter-sample step (8 neighbours at distance 1), costs (SATD >> 1) +
 //      lambda * vector bits against the part's own predictor (H.264 8.4.1.3, directional for 16x8
 //      and 8x16), least cost first in candidate order;
-//   4. the type of least total cost, type bits {1, 3, 3, 7} * lambda added, first on ties;
+//   4. the type of least total cost, the stream's type bits (per partition type) * lambda added,
+//      first on ties;
 //   5. intra 16x16 check, residual, late skip and reconstruction exactly as the plain form.
 // IDR macroblock: the plain form's analysis; learned: intra 4x4 blocks try only their hinted modes
 // (those of them available at the block, DC when none is).
@@ -514,9 +515,20 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   IntBest ib;
   int_search(c, sm, ss, xlo, xhi, ylo, yhi, mvp16[0], mvp16[1], lambda, ib);
   if (hint) {
-    const bool edge = (ib.x[0] == xlo && xlo > imin0) || (ib.x[0] == xhi && xhi < imax0) ||
-                      (ib.y[0] == ylo && ylo > imin1) || (ib.y[0] == yhi && yhi < imax1);
-    if (edge) {  // the seed's window missed the minimum: full search
+    bool edge = (ib.x[0] == xlo && xlo > imin0) || (ib.x[0] == xhi && xhi < imax0) ||
+                (ib.y[0] == ylo && ylo > imin1) || (ib.y[0] == yhi && yhi < imax1);
+    for (int it = 0; edge && it < sd.walk; it++) {  // centre the window on its best again
+      const int cx = ib.x[0], cy = ib.y[0];
+      xlo = max(cx - kLearnedRange, imin0);
+      xhi = min(cx + kLearnedRange, imax0);
+      ylo = max(cy - kLearnedRange, imin1);
+      yhi = min(cy + kLearnedRange, imax1);
+      if (!wait_window(c, pw, xhi, yhi)) return;
+      int_search(c, sm, ss, xlo, xhi, ylo, yhi, mvp16[0], mvp16[1], lambda, ib);
+      edge = (ib.x[0] == xlo && xlo > imin0) || (ib.x[0] == xhi && xhi < imax0) ||
+             (ib.y[0] == ylo && ylo > imin1) || (ib.y[0] == yhi && yhi < imax1);
+    }
+    if (edge) {  // the walk did not reach the minimum: full search
       xlo = max(fcx - R, imin0); xhi = min(fcx + R, imax0);
       ylo = max(fcy - R, imin1); yhi = min(fcy + R, imax1);
       if (!wait_window(c, pw, xhi, yhi)) return;
@@ -532,7 +544,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
     if (!((part_mask >> t) & 1)) continue;
     int own[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
     int done = 0;
-    uint32_t J = lambda * (t == 0 ? 1u : (t == 3 ? 7u : 3u));  // type bits {1, 3, 3, 7}
+    uint32_t J = lambda * (uint32_t)sd.type_bits[t];
     int pm[4][2], pd[4][2];
     const int first = c_type_first[t], np = c_type_parts[t];
     for (int k = 0; k < np; k++) {

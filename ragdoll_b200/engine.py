@@ -55,7 +55,7 @@ EXPORTS = [
     "rg_analyse_gops_fetch", "rg_set_analysis_form", "rg_set_hints", "rg_encoder_new_gops",
     "rg_net_param_count", "rg_net_create", "rg_net_destroy", "rg_net_set_params", "rg_net_get_params",
     "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
-    "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device",
+    "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device", "rg_set_search_tuning",
 ]
 
 
@@ -152,6 +152,7 @@ def lib() -> ctypes.CDLL:
     L.rg_set_hints.argtypes = [P, P, ctypes.c_int32]
     L.rg_encoder_new_gops.argtypes = [P]
     L.rg_set_hint_net.argtypes = [P, P]
+    L.rg_set_search_tuning.argtypes = [P, P, ctypes.c_int32]
     L.rg_ssim_batch_device.argtypes = [ctypes.c_int32, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_size_t, ctypes.c_size_t, P, P, P]
     L.rg_encoder_set_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32, P]
@@ -327,6 +328,12 @@ class Engine:
         """Plain (byte-identical Balanced), full-search or learned analysis of the next calls
         (rg_set_analysis_form); the search forms need a Main or High profile context."""
         _check(lib().rg_set_analysis_form(self.h, form, search_range))
+
+    def set_search_tuning(self, type_bits=None, walk: int = 4) -> None:
+        """Search forms' partition type bits (16x16, 16x8, 8x16, 8x8; None: defaults) and the learned
+        form's window re-centrings (rg_set_search_tuning)."""
+        tb = (ctypes.c_int32 * 4)(*type_bits) if type_bits is not None else None
+        _check(lib().rg_set_search_tuning(self.h, tb, walk))
 
     def set_hint_net(self, net) -> None:
         """The candidate network (ragdoll_b200.learned.CandidateNet or None) the learned form runs

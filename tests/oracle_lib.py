@@ -65,6 +65,7 @@ def lib():
         L.oracle_record_size.restype = ctypes.c_int
         L.oracle_enc_set_form.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_enc_set_hints.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_enc_set_search_tuning.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.oracle_pixel_ops.restype = ctypes.c_ulonglong
         L.oracle_pixel_ops.argtypes = [ctypes.c_int]
         for fn in ("oracle_ssim_plane", "oracle_ms_ssim_plane", "oracle_psnr_plane"):
@@ -104,6 +105,10 @@ class OracleEncoder:
     def set_form(self, form, search_range=32):
         """Search forms (1 full search, 2 learned): decisions and reconstruction only, no bitstream."""
         lib().oracle_enc_set_form(self.h, form, search_range)
+
+    def set_search_tuning(self, type_bits=(1, 3, 3, 7), walk=4):
+        tb = (ctypes.c_int * 4)(*type_bits)
+        lib().oracle_enc_set_search_tuning(self.h, tb, walk)
 
     def set_hints(self, hints):
         """The learned form's hints of the next frame (a HINT_DTYPE array of mb_w * mb_h records)."""
