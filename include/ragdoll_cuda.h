@@ -309,8 +309,8 @@ int rg_net_get_params(const rg_net* net, float* params, int32_t count);
 /*
  * Hints of n_pictures pictures on the device: dev_cur[k] / dev_prev[k] the luma planes (display
  * size width x height, row stride `stride`; prev = cur for an IDR picture), dev_hints[k] receives
- * mb_w * mb_h rg_mb_hint (the top three partition types, the rounded offset, the top three intra
- * 4x4 modes of each block), dev_logits[k] (or dev_logits NULL) mb_w * mb_h * 150 floats (partition
+ * mb_w * mb_h rg_mb_hint (the candidate partition types and intra 4x4 modes of each block that
+ * rg_net_set_hint_policy keeps, the rounded offset), dev_logits[k] (or dev_logits NULL) mb_w * mb_h * 150 floats (partition
  * 4, offset 2, intra 4x4 9 per block in raster order). Asynchronous on `stream`; rg_net_check
  * reports a wait on the tensor cores that gave up.
  */
@@ -318,6 +318,13 @@ int rg_net_predict_hints(rg_net* net, const uint8_t* const* dev_cur, const uint8
                          int32_t width, int32_t height, size_t stride, rg_mb_hint* const* dev_hints,
                          float* const* dev_logits, void* stream);
 int rg_net_check(rg_net* net, void* stream);
+/*
+ * Which candidates rg_net_predict_hints keeps: per macroblock the partition type of the largest
+ * logit, then the next ones in logit order up to part_k types in all (1..4), each only while its
+ * logit is at least the largest minus part_margin (>= 0; INFINITY: no margin); per intra 4x4 block
+ * the same with i4_k (1..9) and i4_margin. Default: 3, INFINITY, 3, INFINITY (the top three).
+ */
+int rg_net_set_hint_policy(rg_net* net, int32_t part_k, float part_margin, int32_t i4_k, float i4_margin);
 /* Training crops: sample k is macroblock (mb_xy[2k], mb_xy[2k+1]) of the luma planes cur[k] /
  * prev[k] (device, display size): 2 x 24 x 24 bytes each into dev_out. */
 int rg_net_crops(rg_net* net, const uint8_t* const* cur, const uint8_t* const* prev, const int32_t* mb_xy, int32_t n,

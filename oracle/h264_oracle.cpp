@@ -2245,9 +2245,11 @@ struct Encoder {
   // each part of every tried partition type (centre and 8 neighbours at distance 2, then 8 at
   // distance 1; cost SATD/2 + lambda * vector bits against the part's own H.264 8.4.1.3 predictor),
   // the type of least total cost (+ lambda * {1, 3, 3, 7}), then the plain form's intra check,
-  // residual and late skip. Learned: +-2 around the predictor plus the hinted offset (the full
-  // window when the 16x16 best lies on that window's edge), only the hinted types, and intra 4x4
-  // blocks of IDR pictures restricted to their hinted modes.
+  // residual and late skip. Learned: +-2 around a centre chosen among six integer candidates
+  // (predictor plus the hinted offset, predictor, left / top / top-right (else top-left) neighbour
+  // vectors, zero) by 16x16 SAD + lambda * vector bits, first in that order on ties; re-centred on
+  // the 16x16 best while that lies on the window's edge (`walk` times), then the full window; only
+  // the hinted types, and intra 4x4 blocks of IDR pictures restricted to their hinted modes.
   int form = 0, search_range = 32, walk = 4;
   int type_bits[4] = {1, 3, 3, 7};      // bits charged per partition type (x lambda)
   const rg_mb_hint* hints = nullptr;    // learned form: this picture's hints
@@ -2403,9 +2405,22 @@ struct Encoder {
     int hi[2] = {std::min(fc[0] + R, imax[0]), std::min(fc[1] + R, imax[1])};
     int part_mask = 15;
     if (h) {
-      int lc[2];
+      NbS A = nb4s(mbx, mby, -1, 0, none, 0), B = nb4s(mbx, mby, 0, -1, none, 0), C = nb4s(mbx, mby, 4, -1, none, 0);
+      if (C.ref == -2) C = nb4s(mbx, mby, -1, -1, none, 0);
+      const int cv[6][2] = {{mvp16[0] + h->mv_off[0], mvp16[1] + h->mv_off[1]}, {mvp16[0], mvp16[1]}, {A.x, A.y}, {B.x, B.y},
+                            {C.x, C.y}, {0, 0}};
+      const bool use[6] = {true, true, A.ref == 0, B.ref == 0, C.ref == 0, true};
+      int lc[2] = {0, 0};
+      uint32_t best = UINT32_MAX;
+      for (int k = 0; k < 6; k++) {
+        if (!use[k]) continue;
+        int v[2];
+        for (int c = 0; c < 2; c++) v[c] = std::min(std::max((cv[k][c] + 2) >> 2, imin[c]), imax[c]);
+        uint32_t cost = sad(src.y, 16, refp.y.ptr(x0 + v[0], y0 + v[1]), refp.y.stride, 16, 16) +
+                        mvd_cost(4 * v[0] - mvp16[0], lambda) + mvd_cost(4 * v[1] - mvp16[1], lambda);
+        if (cost < best) { best = cost; lc[0] = v[0]; lc[1] = v[1]; }
+      }
       for (int c = 0; c < 2; c++) {
-        lc[c] = std::min(std::max((mvp16[c] + h->mv_off[c] + 2) >> 2, imin[c]), imax[c]);
         lo[c] = std::max(lc[c] - 2, imin[c]);
         hi[c] = std::min(lc[c] + 2, imax[c]);
       }

@@ -156,15 +156,21 @@ struct InferParams {
   const float* params;        // f32 parameters (biases and heads)
   int* counter;               // strip ticket
   int* error;                 // set when a wait on the tensor cores gives up
+  int part_k, i4_k;           // hint policy: candidates kept at most,
+  float part_margin, i4_margin;  // and only those within this logit margin of the best
 };
 
-// The top three of n logits as a bit mask (the lower index on ties).
-__device__ __forceinline__ uint32_t top3_mask(const float* l, int n) {
+// The candidates of n logits as a bit mask: the best, then the next ones in logit order (the lower
+// index on ties) up to k in all, each only while its logit is at least the best's minus `margin`.
+__device__ __forceinline__ uint32_t topk_mask(const float* l, int n, int k, float margin) {
   uint32_t m = 0;
-  for (int k = 0; k < 3; k++) {
+  float top = 0.0f;
+  for (int r = 0; r < k; r++) {
     int best = -1;
     for (int i = 0; i < n; i++)
       if (!((m >> i) & 1) && (best < 0 || l[i] > l[best])) best = i;
+    if (r == 0) top = l[best];
+    else if (l[best] < top - margin) break;
     m |= 1u << best;
   }
   return m;
@@ -290,24 +296,43 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
       }
     }
     if (!ok) break;
+    // pooling of the conv3 map (in A1; map column 16 j + i is sample x 16 (mbx0 + j) - 1 + i):
+    // item (macroblock j, 8-channel plane q, map row r) reads the row's 18 positions 16 bytes at a
+    // time, then adds its row total and its four block-row totals into the shared sums
+    for (int i = tid; i < kStripMbs * 17 * C; i += 128) (&ms.pool[0][0][0])[i] = 0.0f;
     __syncthreads();
-    // pooling of the conv3 map (in A1): thread (macroblock j, channel c), map column 16 j + i is
-    // sample x 16 (mbx0 + j) - 1 + i; the 18 x 18 mean and the 16 block means
-    if (tid < kStripMbs * C) {
-      const int j = tid / C, c = tid % C;
-      const uint8_t* pl = A1 + (c >> 3) * kPlane1 + (c & 7) * 2;
-      float all = 0.0f, blk[16];
+    for (int it = tid; it < kStripMbs * 4 * 18; it += 128) {
+      const int j = it / 72, q = (it / 18) % 4, r = it % 18;
+      const uint8_t* row = A1 + q * kPlane1 + (r * kRow + 16 * j) * 16;
+      float tot[8], blk[4][8];
 #pragma unroll
-      for (int b = 0; b < 16; b++) blk[b] = 0.0f;
-      for (int r = 0; r < 18; r++)
-        for (int i = 0; i < 18; i++) {
-          float x = __bfloat162float(*(const __nv_bfloat16*)(pl + (r * kRow + 16 * j + i) * 16));
-          all += x;
-          if (r >= 1 && r <= 16 && i >= 1 && i <= 16) blk[((r - 1) >> 2) * 4 + ((i - 1) >> 2)] += x;
+      for (int k = 0; k < 8; k++) {
+        tot[k] = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 4; b++) blk[b][k] = 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < 18; i++) {
+        const uint4 v = *(const uint4*)(row + i * 16);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const float2 f = __bfloat1622float2(*(const __nv_bfloat162*)&w[k]);
+          tot[2 * k] += f.x;
+          tot[2 * k + 1] += f.y;
+          if (i >= 1 && i <= 16) {
+            blk[(i - 1) >> 2][2 * k] += f.x;
+            blk[(i - 1) >> 2][2 * k + 1] += f.y;
+          }
         }
-      ms.pool[j][0][c] = all * (1.0f / 324.0f);
+      }
 #pragma unroll
-      for (int b = 0; b < 16; b++) ms.pool[j][1 + b][c] = blk[b] * (1.0f / 16.0f);
+      for (int k = 0; k < 8; k++) {
+        atomicAdd(&ms.pool[j][0][8 * q + k], tot[k] * (1.0f / 324.0f));
+        if (r >= 1 && r <= 16)
+#pragma unroll
+          for (int b = 0; b < 4; b++) atomicAdd(&ms.pool[j][1 + ((r - 1) >> 2) * 4 + b][8 * q + k], blk[b][k] * (1.0f / 16.0f));
+      }
     }
     __syncthreads();
     // heads and hints: threads 0..47 the intra 4x4 heads of (macroblock tid / 16, block tid % 16),
@@ -331,7 +356,7 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
           // 4x4 block b in raster order; the hint holds decoding order
           const int bx = b & 3, by = b >> 2;
           const int dec = ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1);
-          jb.hints[m].i4_mask[dec] = (uint16_t)top3_mask(li, 9);
+          jb.hints[m].i4_mask[dec] = (uint16_t)topk_mask(li, 9, ip.i4_k, ip.i4_margin);
           if (lg)
             for (int o = 0; o < 9; o++) lg[6 + b * 9 + o] = li[o];
         } else {
@@ -348,7 +373,7 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
             lm[o] = s;
           }
           rg_mb_hint& hh = jb.hints[m];
-          hh.part_mask = (uint8_t)top3_mask(lp, 4);
+          hh.part_mask = (uint8_t)topk_mask(lp, 4, ip.part_k, ip.part_margin);
           hh.reserved = 0;
           for (int o = 0; o < 2; o++) hh.mv_off[o] = (int8_t)max(-127, min(127, __float2int_rn(16.0f * lm[o])));
           if (lg) {
@@ -678,6 +703,8 @@ struct rg_net {
   int cap = 0;
   InferJob* jobs = nullptr;
   int jobs_cap = 0;
+  int part_k = 3, i4_k = 3;  // hint policy (rg_net_set_hint_policy)
+  float part_margin = INFINITY, i4_margin = INFINITY;
 };
 
 namespace {
@@ -913,12 +940,26 @@ int rg_net_predict_hints(rg_net* net, const uint8_t* const* dev_cur, const uint8
   ip.params = net->P;
   ip.counter = net->counter;
   ip.error = net->counter + 1;
+  ip.part_k = net->part_k;
+  ip.i4_k = net->i4_k;
+  ip.part_margin = net->part_margin;
+  ip.i4_margin = net->i4_margin;
   NCK(cudaFuncSetAttribute(cnn_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemInfer));
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int strips = n_pictures * ip.mb_h * ip.strips_per_row;
   cnn_infer_kernel<<<sms < strips ? sms : strips, 128, kSmemInfer, st>>>(ip);
   NCK(cudaGetLastError());
+  return RG_OK;
+}
+
+int rg_net_set_hint_policy(rg_net* net, int32_t part_k, float part_margin, int32_t i4_k, float i4_margin) {
+  if (!net || part_k < 1 || part_k > 4 || i4_k < 1 || i4_k > 9 || !(part_margin >= 0.0f) || !(i4_margin >= 0.0f))
+    return nfail(RG_ERR_INVALID, "rg_net_set_hint_policy: bad arguments");
+  net->part_k = part_k;
+  net->part_margin = part_margin;
+  net->i4_k = i4_k;
+  net->i4_margin = i4_margin;
   return RG_OK;
 }
 

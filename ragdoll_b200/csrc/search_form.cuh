@@ -9,9 +9,12 @@
 //      each of the nine partition parts (16x16; 16x8 top, bottom; 8x16 left, right; four 8x8) the
 //      vector of least SAD + lambda * (bits(4 vx - mvp.x) + bits(4 vy - mvp.y)) against the 16x16
 //      predictor, first in raster order on ties. Full search: the window is +-search_range around
-//      the 16x16 predictor. Learned: +-2 around the predictor plus the hinted offset; while the
-//      16x16 part's best lies on that window's edge (and not on the vector bounds) the window is
-//      centred on it again, up to `walk` times, and then the full window is searched;
+//      the 16x16 predictor. Learned: +-2 around a centre chosen among six integer candidates --
+//      predictor plus the hinted offset, predictor, the left, top and top-right (top-left where
+//      that is absent) neighbours' vectors, zero -- by the 16x16 SAD + lambda * vector bits, first
+//      in that order on ties; while the 16x16 part's best lies on that window's edge (and not on
+//      the vector bounds) the window is centred on it again, up to `walk` times, and then the full
+//      window is searched;
 //   3. for every partition type tried (all four; learned: the hinted ones), each part in coding
 //      order from its integer best: half-sample step (centre, then 8 neighbours at distance 2,
 //      quarter units) and quarter-sample step (8 neighbours at distance 1), costs (SATD >> 1) +
@@ -26,6 +29,7 @@
 constexpr int kBandRows = 8;               // integer vectors per band row
 constexpr int kBandBytes = (kBandRows + 15) * (2 * kMaxSearchRange + 28);
 constexpr int kLearnedRange = 2;           // learned form: integer window around the seed
+constexpr int kCentreCands = 6;            // learned form: candidates of the window's centre
 
 struct SearchSmem {
   uint8_t band[kBandBytes];
@@ -442,6 +446,28 @@ __device__ __noinline__ bool skip_probe(const Ctx& c, Smem& sm, int ps0, int ps1
   return cz;
 }
 
+// Learned form: the centre of the first +-2 window among n integer candidates (cx, cy; ok false:
+// absent) -- the first of least 16x16 SAD + lambda * vector bits against the 16x16 predictor.
+__device__ __noinline__ void learned_centre(const Ctx& c, const Smem& sm, const int* cx, const int* cy, const bool* ok,
+                                            int n, int mvp0, int mvp1, uint32_t lambda, int& bx, int& by) {
+  const int lane = lane_id();
+  const int stride = c.fp->stride_y;
+  const uint8_t* base = c.sd->ref_y + (long)(c.mby * 16 + (lane >> 1)) * stride + c.mbx * 16 + (lane & 1) * 8;
+  const uint2 sv = src8(sm);
+  uint2 r[kCentreCands];
+#pragma unroll
+  for (int k = 0; k < kCentreCands; k++) r[k] = k < n && ok[k] ? ldg8(base + (long)cy[k] * stride + cx[k]) : make_uint2(0u, 0u);
+  uint32_t best = UMAX;
+  bx = cx[0];
+  by = cy[0];
+#pragma unroll
+  for (int k = 0; k < kCentreCands; k++) {
+    if (k >= n || !ok[k]) continue;  // uniform across the warp
+    const uint32_t cost = fullpel_cost(sv, r[k], cx[k], cy[k], mvp0, mvp1, lambda);
+    if (cost < best) { best = cost; bx = cx[k]; by = cy[k]; }
+  }
+}
+
 // Partition geometry in coding order: {type, first part, parts}; part k: {px, py, pw, ph, bx, by,
 // pw4, dir, integer-search index}.
 __device__ __constant__ int8_t c_parts[9][9] = {
@@ -490,18 +516,31 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   int fcx = min(max((mvp16[0] + 2) >> 2, imin0), imax0), fcy = min(max((mvp16[1] + 2) >> 2, imin1), imax1);
   int xlo = max(fcx - R, imin0), xhi = min(fcx + R, imax0), ylo = max(fcy - R, imin1), yhi = min(fcy + R, imax1);
   int part_mask = 15;
+  // learned: the candidates of the first window's centre (integer, clamped to the bounds)
+  int ccx[kCentreCands], ccy[kCentreCands];
+  bool cok[kCentreCands];
   if (hint) {
-    const int off0 = hint->mv_off[0], off1 = hint->mv_off[1];
-    const int lcx = min(max((mvp16[0] + off0 + 2) >> 2, imin0), imax0);
-    const int lcy = min(max((mvp16[1] + off1 + 2) >> 2, imin1), imax1);
-    xlo = max(lcx - kLearnedRange, imin0);
-    xhi = min(lcx + kLearnedRange, imax0);
-    ylo = max(lcy - kLearnedRange, imin1);
-    yhi = min(lcy + kLearnedRange, imax1);
+    NbMv A = nb4(nb, -1, 0, none, 0), B = nb4(nb, 0, -1, none, 0), C = nb4(nb, 4, -1, none, 0);
+    if (C.ref == -2) C = nb4(nb, -1, -1, none, 0);
+    const int vx[kCentreCands] = {mvp16[0] + hint->mv_off[0], mvp16[0], A.x, B.x, C.x, 0};
+    const int vy[kCentreCands] = {mvp16[1] + hint->mv_off[1], mvp16[1], A.y, B.y, C.y, 0};
+    const bool use[kCentreCands] = {true, true, A.ref == 0, B.ref == 0, C.ref == 0, true};
+    xhi = -(1 << 20);
+    yhi = -(1 << 20);
+#pragma unroll
+    for (int k = 0; k < kCentreCands; k++) {
+      ccx[k] = min(max((vx[k] + 2) >> 2, imin0), imax0);
+      ccy[k] = min(max((vy[k] + 2) >> 2, imin1), imax1);
+      cok[k] = use[k];
+      if (use[k]) {
+        xhi = max(xhi, min(ccx[k] + kLearnedRange, imax0));
+        yhi = max(yhi, min(ccy[k] + kLearnedRange, imax1));
+      }
+    }
     part_mask = hint->part_mask & 15;
     if (!part_mask) part_mask = 1;
   }
-  // the reference region of the skip probe and the search window
+  // the reference region of the skip probe and the search window (learned: every candidate's)
   if (!wait_window(c, pw, max(xhi, (max(ps0, 0) + 3) >> 2), max(yhi, (max(ps1, 0) + 3) >> 2))) return;
   const int off4[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   // 1. skip probe
@@ -512,6 +551,14 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
     return;
   }
   // 2. integer search
+  if (hint) {
+    int lcx, lcy;
+    learned_centre(c, sm, ccx, ccy, cok, kCentreCands, mvp16[0], mvp16[1], lambda, lcx, lcy);
+    xlo = max(lcx - kLearnedRange, imin0);
+    xhi = min(lcx + kLearnedRange, imax0);
+    ylo = max(lcy - kLearnedRange, imin1);
+    yhi = min(lcy + kLearnedRange, imax1);
+  }
   IntBest ib;
   int_search(c, sm, ss, xlo, xhi, ylo, yhi, mvp16[0], mvp16[1], lambda, ib);
   if (hint) {

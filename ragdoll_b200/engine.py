@@ -56,6 +56,7 @@ EXPORTS = [
     "rg_net_param_count", "rg_net_create", "rg_net_destroy", "rg_net_set_params", "rg_net_get_params",
     "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
     "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device", "rg_set_search_tuning",
+    "rg_net_set_hint_policy",
 ]
 
 
@@ -165,6 +166,7 @@ def lib() -> ctypes.CDLL:
     L.rg_net_predict_hints.argtypes = [P, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_size_t,
                                        P, P, P]
     L.rg_net_check.argtypes = [P, P]
+    L.rg_net_set_hint_policy.argtypes = [P, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, ctypes.c_float]
     L.rg_net_crops.argtypes = [P, P, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_size_t, P, P]
     L.rg_net_forward_backward.argtypes = [P, P, ctypes.c_int32, P, P, P, P, ctypes.c_float, P, P, P]
     L.rg_net_adam_step.argtypes = [P, ctypes.c_float]

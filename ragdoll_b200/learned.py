@@ -69,6 +69,12 @@ class CandidateNet:
         _check(lib().rg_net_predict_hints(self.h, A(*cur), A(*prev), n, width, height, stride, A(*hints), lg,
                                           stream or None))
 
+    def set_hint_policy(self, part_k: int = 3, part_margin: float = float("inf"), i4_k: int = 3,
+                        i4_margin: float = float("inf")) -> None:
+        """Candidates the hints keep (rg_net_set_hint_policy): the best partition type, then the next
+        ones up to part_k while within part_margin of the best logit; intra 4x4 modes alike."""
+        _check(lib().rg_net_set_hint_policy(self.h, part_k, part_margin, i4_k, i4_margin))
+
     def check(self, stream: int = 0) -> None:
         _check(lib().rg_net_check(self.h, stream or None))
 

@@ -5,7 +5,8 @@
   by finite differences) within f32 rounding.
 * Tensor-core inference (BF16 tcgen05 MMAs, strips of three macroblocks, pictures whose width is no
   multiple of the strip): every logit equals the oracle's BF16 arithmetic within the stated
-  tolerance, and the hints are the top three of the GPU's own logits.
+  tolerance, and the hints are the top three of the GPU's own logits; under another hint policy
+  (fewer candidates, logit margins) the kept candidates are those of the same rule on the host.
 * Training on full-search labels lowers the loss.
 * End to end: hints from the network drive the learned form; its records equal the oracle's with
   the same hints, and its CABAC stream decodes (FFmpeg) to the engine's reconstruction.
@@ -104,6 +105,46 @@ def test_tensor_core_inference_matches_oracle(w, h):
         top = np.argsort(-got[m, :4], kind="stable")[:3]
         assert hh["part_mask"][m] == sum(1 << int(t) for t in top)
         assert tuple(hh["mv_off"][m]) == tuple(np.clip(np.rint(16 * got[m, 4:6]), -127, 127).astype(int))
+
+
+def _topk_mask(l, k, margin):
+    """The hint policy on the host: the best logit, then the next ones (lower index on ties) up to k
+    while within `margin` of the best (f32 arithmetic, as the kernel)."""
+    l = np.asarray(l, np.float32)
+    order = np.argsort(-l, kind="stable")
+    m = 1 << int(order[0])
+    for i in order[1:k]:
+        if l[i] < np.float32(l[order[0]] - np.float32(margin)):
+            break
+        m |= 1 << int(i)
+    return m
+
+
+def test_hint_policy_keeps_the_candidates_within_the_margin():
+    import torch
+
+    from ragdoll_b200.engine import HINT_DTYPE
+    from ragdoll_b200.learned import CandidateNet, hints_for
+    w, h = 144, 80
+    rng = np.random.default_rng(9)
+    cur = rng.integers(0, 256, (h, w)).astype(np.uint8)
+    prev = np.roll(cur, 3, axis=1)
+    net = CandidateNet(0, params=_params(6))
+    tc, tp = torch.from_numpy(cur).cuda(), torch.from_numpy(prev).cuda()
+    for part_k, part_margin, i4_k, i4_margin in ((1, np.inf, 1, np.inf), (2, 0.5, 4, 1.0), (4, 2.0, 9, 0.25)):
+        net.set_hint_policy(part_k, part_margin, i4_k, i4_margin)
+        hints, logits = hints_for(net, [tc.data_ptr()], [tp.data_ptr()], w, h, w, with_logits=True)
+        net.check()
+        torch.cuda.synchronize()
+        lg = logits[0].cpu().numpy().reshape(-1, 150)
+        hh = hints[0].cpu().numpy().view(HINT_DTYPE)
+        from ragdoll_b200.learned import DEC_TO_RASTER
+        for m in range(len(lg)):
+            assert hh["part_mask"][m] == _topk_mask(lg[m, :4], part_k, part_margin)
+            for d in range(16):
+                b = DEC_TO_RASTER[d]
+                assert hh["i4_mask"][m][d] == _topk_mask(lg[m, 6 + 9 * b:15 + 9 * b], i4_k, i4_margin)
+    net.set_hint_policy()
 
 
 def test_training_on_full_search_labels_lowers_the_loss():
