@@ -374,11 +374,11 @@ def run_learned(args, rank, world, local):
     the learned form's network inference included), then bits and luma PSNR of every form at QP 22,
     26, 30 and 34 (records written by the host CABAC writer, reconstructions compared with the
     source) and the Bjontegaard delta rates. `no_net` is the learned form with fixed candidates
-    instead of the network's (what the network gains)."""
+    instead of the network's (the coarse motion vectors kept): what the network gains."""
     import torch
 
-    from ragdoll_b200.engine import (RG_FORM_FULLSEARCH, RG_FORM_LEARNED, RG_FORM_PLAIN, RG_FRAME_IDR, RG_FRAME_P,
-                                     RG_PROFILE_HIGH, BitstreamWriter, Engine)
+    from ragdoll_b200.engine import (HINT_DTYPE, RG_FORM_FULLSEARCH, RG_FORM_LEARNED, RG_FORM_PLAIN, RG_FRAME_IDR,
+                                     RG_FRAME_P, RG_PROFILE_HIGH, BitstreamWriter, Engine)
     from ragdoll_b200.learned import WEIGHTS, CandidateNet, hints_for, prior_hints
     if rank != 0:
         return
@@ -403,7 +403,15 @@ def run_learned(args, rank, world, local):
     hints, _ = hints_for(net, [base + i * fbytes for i in idx], [base + i * fbytes for i in prev], W, H, W)
     hint_of = {i: hints[k] for k, i in enumerate(idx)}
     n_mb = ((W + 15) // 16) * ((H + 15) // 16)
-    prior = torch.from_numpy(prior_hints(n_mb).view(np.uint8)).to(f"cuda:{local}")
+    # the network's candidates replaced by fixed ones; the coarse motion vectors kept
+    fixed = prior_hints(n_mb)
+    prior_of = {}
+    torch.cuda.synchronize()
+    for i in idx:
+        h = hint_of[i].cpu().numpy().view(HINT_DTYPE).copy()
+        for field in ("part_mask", "mv_off", "i4_mask"):
+            h[field] = fixed[field]
+        prior_of[i] = torch.from_numpy(h.view(np.uint8)).to(f"cuda:{local}")
     forms = {"plain": RG_FORM_PLAIN, "fullsearch": RG_FORM_FULLSEARCH, "learned": RG_FORM_LEARNED,
              "no_net": RG_FORM_LEARNED}
     torch.cuda.synchronize()
@@ -472,7 +480,7 @@ def run_learned(args, rank, world, local):
                 if name == "learned":
                     eng.set_hints_device([hint_of[g * GOP + f].data_ptr() for g in range(gops)])
                 elif name == "no_net":
-                    eng.set_hints_device([prior.data_ptr()] * gops)
+                    eng.set_hints_device([prior_of[g * GOP + f].data_ptr() for g in range(gops)])
                 eng.analyse_device(ptrs, W, cw, [kind] * gops)
                 recs = eng.records()
                 for g in range(gops):

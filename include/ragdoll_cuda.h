@@ -271,10 +271,12 @@ int32_t rg_pipeline_lag(const rg_ctx* ctx);
  *   partition types (16x16, 16x8, 8x16, 8x8) to quarter samples by SATD with each partition's own
  *   predictor, and code the type of least cost. Intra and the residual follow the plain form.
  * RG_FORM_LEARNED: the same decisions restricted by a per-macroblock hint (rg_mb_hint, from the
- *   candidate network of rg_predict_hints): the integer search covers +-2 samples around the
- *   predictor plus the hinted offset (the full +-search_range search when the best vector lies on
- *   that window's edge), only the hinted partition types are refined, and intra 4x4 blocks of IDR
- *   pictures try only their hinted prediction modes.
+ *   candidate network of rg_net_predict_hints): the integer search covers +-2 samples around a
+ *   centre chosen among integer candidates (the predictor plus the hinted offset, the predictor,
+ *   the hint's coarse vector, the left / top / top-right neighbours' vectors, zero) by 16x16 SAD
+ *   plus vector bits, re-centred on its best up to `walk` times while that lies on the window's
+ *   edge, then the full +-search_range search; only the hinted partition types are refined, and
+ *   intra 4x4 blocks of IDR pictures try only their hinted prediction modes.
  */
 #define RG_FORM_PLAIN 0
 #define RG_FORM_FULLSEARCH 1
@@ -283,10 +285,12 @@ int32_t rg_pipeline_lag(const rg_ctx* ctx);
 /* Per-macroblock hint of the learned form (raster order, one per macroblock of a picture). */
 typedef struct rg_mb_hint {
     uint8_t part_mask;      /* bit t: partition type t is tried (t as rg_mb_out.part_type)       */
-    uint8_t reserved;
+    uint8_t flags;          /* bit 0: mv_coarse holds a vector                                   */
     int8_t mv_off[2];       /* offset of the integer search's centre from the 16x16 predictor,
                                quarter samples                                                   */
     uint16_t i4_mask[16];   /* bit m: Intra4x4PredMode m is tried for 4x4 block b (decoding order) */
+    int16_t mv_coarse[2];   /* coarse motion against the previous picture's source (quarter samples;
+                               rg_net_predict_hints, see rg_net_set_coarse_range)                */
 } rg_mb_hint;
 
 /* ---- the learned form's candidate network (no counterpart in the reference) ----------------- */
@@ -325,6 +329,15 @@ int rg_net_check(rg_net* net, void* stream);
  * the same with i4_k (1..9) and i4_margin. Default: 3, INFINITY, 3, INFINITY (the top three).
  */
 int rg_net_set_hint_policy(rg_net* net, int32_t part_k, float part_margin, int32_t i4_k, float i4_margin);
+/*
+ * Coarse motion of rg_net_predict_hints (range 0: off, the hints' flags bit 0 clear; else an even
+ * 2..64, default 32): per macroblock of a picture whose previous picture differs from it, the
+ * vector of least SAD of the 2:1 decimated macroblock (2x2 means, rounded) against the decimated
+ * previous picture (coordinates clamped to the picture) over +-range/2 decimated samples, ties to
+ * the least |x| + |y| and then the first in raster order; written as twice that vector in
+ * mv_coarse (quarter samples) with flags bit 0 set.
+ */
+int rg_net_set_coarse_range(rg_net* net, int32_t range);
 /* Training crops: sample k is macroblock (mb_xy[2k], mb_xy[2k+1]) of the luma planes cur[k] /
  * prev[k] (device, display size): 2 x 24 x 24 bytes each into dev_out. */
 int rg_net_crops(rg_net* net, const uint8_t* const* cur, const uint8_t* const* prev, const int32_t* mb_xy, int32_t n,

@@ -2244,14 +2244,15 @@ struct Encoder {
   // bits against the 16x16 predictor, first minimum in raster order), quarter-sample refinement of
   // each part of every tried partition type (centre and 8 neighbours at distance 2, then 8 at
   // distance 1; cost SATD/2 + lambda * vector bits against the part's own H.264 8.4.1.3 predictor),
-  // the type of least total cost (+ lambda * {1, 3, 3, 7}), then the plain form's intra check,
-  // residual and late skip. Learned: +-2 around a centre chosen among six integer candidates
-  // (predictor plus the hinted offset, predictor, left / top / top-right (else top-left) neighbour
-  // vectors, zero) by 16x16 SAD + lambda * vector bits, first in that order on ties; re-centred on
-  // the 16x16 best while that lies on the window's edge (`walk` times), then the full window; only
-  // the hinted types, and intra 4x4 blocks of IDR pictures restricted to their hinted modes.
+  // the type of least total cost (+ lambda * type bits, by default {1, 16, 16, 40}), then the plain
+  // form's intra check, residual and late skip. Learned: +-2 around a centre chosen among seven
+  // integer candidates (predictor plus the hinted offset, predictor, the hint's coarse vector when
+  // it has one, left / top / top-right (else top-left) neighbour vectors, zero) by 16x16 SAD +
+  // lambda * vector bits, first in that order on ties; re-centred on the 16x16 best while that lies
+  // on the window's edge (`walk` times), then the full window; only the hinted types, and intra 4x4
+  // blocks of IDR pictures restricted to their hinted modes.
   int form = 0, search_range = 32, walk = 4;
-  int type_bits[4] = {1, 3, 3, 7};      // bits charged per partition type (x lambda)
+  int type_bits[4] = {1, 16, 16, 40};   // bits charged per partition type (x lambda)
   const rg_mb_hint* hints = nullptr;    // learned form: this picture's hints
   std::vector<uint8_t> mb_split;        // per MB: quadrant vectors differ
 
@@ -2407,12 +2408,12 @@ struct Encoder {
     if (h) {
       NbS A = nb4s(mbx, mby, -1, 0, none, 0), B = nb4s(mbx, mby, 0, -1, none, 0), C = nb4s(mbx, mby, 4, -1, none, 0);
       if (C.ref == -2) C = nb4s(mbx, mby, -1, -1, none, 0);
-      const int cv[6][2] = {{mvp16[0] + h->mv_off[0], mvp16[1] + h->mv_off[1]}, {mvp16[0], mvp16[1]}, {A.x, A.y}, {B.x, B.y},
-                            {C.x, C.y}, {0, 0}};
-      const bool use[6] = {true, true, A.ref == 0, B.ref == 0, C.ref == 0, true};
+      const int cv[7][2] = {{mvp16[0] + h->mv_off[0], mvp16[1] + h->mv_off[1]}, {mvp16[0], mvp16[1]},
+                            {h->mv_coarse[0], h->mv_coarse[1]}, {A.x, A.y}, {B.x, B.y}, {C.x, C.y}, {0, 0}};
+      const bool use[7] = {true, true, (h->flags & 1) != 0, A.ref == 0, B.ref == 0, C.ref == 0, true};
       int lc[2] = {0, 0};
       uint32_t best = UINT32_MAX;
-      for (int k = 0; k < 6; k++) {
+      for (int k = 0; k < 7; k++) {
         if (!use[k]) continue;
         int v[2];
         for (int c = 0; c < 2; c++) v[c] = std::min(std::max((cv[k][c] + 2) >> 2, imin[c]), imax[c]);

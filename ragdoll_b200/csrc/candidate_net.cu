@@ -45,13 +45,15 @@ __device__ __forceinline__ float pix_norm(uint8_t v) { return ((float)v - 128.0f
 // ---------------------------------------------------------------------------------------------
 // Inference on the tensor cores.
 constexpr int kStripMbs = 3;
+constexpr int kThreads = 256;  // 8 warps: two per scheduler; warps w and w + 4 share TMEM lanes 32 (w % 4)..
 constexpr int kRow = 16 * kStripMbs + 8;  // row stride (positions) of every map of a strip: 56
 constexpr int kTiles1 = (22 * kRow + 127) / 128, kTiles2 = (20 * kRow + 127) / 128, kTiles3 = (18 * kRow + 127) / 128;
-constexpr int kPos0 = ((kTiles1 * 128 + 2 * kRow + 2) + 127) / 128 * 128;  // positions of the input map
+constexpr int kPos0 = ((kTiles1 * 128 + 2 * kRow + 2) + kThreads - 1) / kThreads * kThreads;  // input map positions
 constexpr int kPos1 = kTiles1 * 128, kPos2 = kTiles2 * 128;
 static_assert(kPos1 >= kTiles2 * 128 + 2 * kRow + 2 && kPos2 >= kTiles3 * 128 + 2 * kRow + 2, "tap reach");
-static_assert(kPos0 % 128 == 0, "input map staged 128 positions per thread step");
+static_assert(kPos0 % kThreads == 0, "input map staged one position per thread and step");
 static_assert(kTiles1 * 32 <= 512, "accumulators of one layer fit the tensor memory");
+static_assert(kStripMbs * 4 * 16 <= kThreads && (kStripMbs * 4 * 16) % 32 == 0, "pooling: whole warps of half-warps");
 // shared memory (bytes): A1 (4 planes of 8 channels) | A2 or the input | B operands | the rest
 constexpr int kPlane1 = kPos1 * 16, kPlane2 = kPos2 * 16;
 constexpr int kOffA1 = 0, kOffA2 = kOffA1 + 4 * kPlane1, kSizeA2 = (4 * kPlane2 > kPos0 * 16 ? 4 * kPlane2 : kPos0 * 16);
@@ -176,17 +178,17 @@ __device__ __forceinline__ uint32_t topk_mask(const float* l, int n, int k, floa
   return m;
 }
 
-__global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
+__global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) {
   extern __shared__ __align__(1024) uint8_t smem[];
   InferMisc& ms = *reinterpret_cast<InferMisc*>(smem + kOffMisc);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* A1 = smem + kOffA1;
   uint8_t* A2 = smem + kOffA2;  // the input map first, then conv2's output
   // B operands, biases and heads once per CTA
-  for (int i = tid; i < (kB1Mmas + 2 * kBMmas) * 1024 / 16; i += 128)
+  for (int i = tid; i < (kB1Mmas + 2 * kBMmas) * 1024 / 16; i += kThreads)
     ((uint4*)(smem + kOffB))[i] = ((const uint4*)ip.bops)[i];
-  for (int i = tid; i < 3 * C; i += 128) ms.bias[i / C][i % C] = ip.params[(i / C == 0 ? kB1 : (i / C == 1 ? kB2 : kB3)) + i % C];
-  for (int i = tid; i < kParams - kWp; i += 128) ms.head[i] = ip.params[kWp + i];
+  for (int i = tid; i < 3 * C; i += kThreads) ms.bias[i / C][i % C] = ip.params[(i / C == 0 ? kB1 : (i / C == 1 ? kB2 : kB3)) + i % C];
+  for (int i = tid; i < kParams - kWp; i += kThreads) ms.head[i] = ip.params[kWp + i];
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&ms.mbar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -204,33 +206,52 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
   uint32_t phase = 0;
   bool ok = true;
   const int total = ip.n_jobs * ip.mb_h * ip.strips_per_row;
-  while (true) {
-    if (tid == 0) ms.strip = atomicAdd(ip.counter, 1);
-    __syncthreads();
-    const int strip = ms.strip;
-    if (strip >= total || !ok) break;
-    const int job = strip / (ip.mb_h * ip.strips_per_row), rem = strip % (ip.mb_h * ip.strips_per_row);
-    const int mby = rem / ip.strips_per_row, mbx0 = (rem % ip.strips_per_row) * kStripMbs;
+  // The input map of a strip: position r * kRow + c is sample (x0 - 4 + c, y0 - 4 + r), clamped
+  // to the picture; 16 bytes each, the two channels and six zero channels. A strip's bytes are
+  // loaded into registers while the previous strip's MMAs run, and stored once its conv3 is done.
+  constexpr int kPer = kPos0 / kThreads;
+  uint8_t ca[kPer], pa[kPer];
+  auto load_input = [&](int st) {
+    const int job = st / (ip.mb_h * ip.strips_per_row), rem = st % (ip.mb_h * ip.strips_per_row);
+    const int y0 = (rem / ip.strips_per_row) * 16 - 4, x0 = (rem % ip.strips_per_row) * kStripMbs * 16 - 4;
     const InferJob jb = ip.jobs[job];
-    // input map: position r * kRow + c is sample (x0 - 4 + c, y0 - 4 + r), clamped to the picture;
-    // 16 bytes each: the two channels and six zero channels
-    const int y0 = mby * 16 - 4, x0 = mbx0 * 16 - 4;
-    constexpr int kPer = kPos0 / 128;
-    uint8_t ca[kPer], pa[kPer];
 #pragma unroll
     for (int k = 0; k < kPer; k++) {  // all of this thread's loads in flight together
-      const int p = tid + 128 * k;
+      const int p = tid + kThreads * k;
       const int r = p / kRow, c = p - r * kRow;
       const int yy = min(max(y0 + r, 0), ip.height - 1), xx = min(max(x0 + c, 0), ip.width - 1);
       const size_t o = (size_t)yy * ip.stride + xx;
       ca[k] = p < 24 * kRow ? jb.cur[o] : 128;
       pa[k] = p < 24 * kRow ? jb.prev[o] : 128;
     }
+  };
+  if (tid == 0) ms.strip = atomicAdd(ip.counter, 1);
+  __syncthreads();
+  int strip = ms.strip;
+  if (strip < total) load_input(strip);
+  // shared-memory descriptors: conv1's five tap pairs, the two channel halves of conv2's and
+  // conv3's operands, the B operands; a tile / tap adds its offset in 16-byte units
+  uint64_t a1d[kB1Mmas];
+#pragma unroll
+  for (int k = 0; k < kB1Mmas; k++) {
+    const int ta = c_pair[k][0], tb = c_pair[k][1];
+    const int oa = (ta / 3) * kRow + ta % 3, ob = tb < 9 ? (tb / 3) * kRow + tb % 3 : oa + 1;
+    a1d[k] = umma_desc(sA2 + (uint32_t)(oa * 16), (uint32_t)((ob - oa) * 16), 128);
+  }
+  const uint64_t b1d = umma_desc(sB1, 512, 128), b2d = umma_desc(sB2, 512, 128), b3d = umma_desc(sB3, 512, 128);
+  const uint64_t a2d0 = umma_desc(sA1, kPlane1, 128), a2d1 = umma_desc(sA1 + 2 * kPlane1, kPlane1, 128);
+  const uint64_t a3d0 = umma_desc(sA2, kPlane2, 128), a3d1 = umma_desc(sA2 + 2 * kPlane2, kPlane2, 128);
+  while (strip < total && ok) {
+    const int job = strip / (ip.mb_h * ip.strips_per_row), rem = strip % (ip.mb_h * ip.strips_per_row);
+    const int mby = rem / ip.strips_per_row, mbx0 = (rem % ip.strips_per_row) * kStripMbs;
+    const InferJob jb = ip.jobs[job];
 #pragma unroll
     for (int k = 0; k < kPer; k++) {
       __nv_bfloat162 two = __floats2bfloat162_rn(pix_norm(ca[k]), pix_norm(pa[k]));
-      ((uint4*)A2)[tid + 128 * k] = make_uint4(*(uint32_t*)&two, 0u, 0u, 0u);
+      ((uint4*)A2)[tid + kThreads * k] = make_uint4(*(uint32_t*)&two, 0u, 0u, 0u);
     }
+    if (tid == 0) ms.strip = atomicAdd(ip.counter, 1);  // read after the first layer's barrier
+    int next = total;
     for (int layer = 0; layer < 3; layer++) {
       fence_async_smem();
       fence_before_sync();
@@ -238,29 +259,31 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
       fence_after_sync();
       const int tiles = layer == 0 ? kTiles1 : (layer == 1 ? kTiles2 : kTiles3);
       if (tid == 0) {
-        for (int t = 0; t < tiles; t++) {
-          const uint32_t d = tmem + (uint32_t)(t * 32);
-          if (layer == 0) {
-            for (int k = 0; k < kB1Mmas; k++) {
-              int ta = c_pair[k][0], tb = c_pair[k][1];
-              int oa = (ta / 3) * kRow + ta % 3, ob = tb < 9 ? (tb / 3) * kRow + tb % 3 : oa + 1;
-              uint64_t a = umma_desc(sA2 + (uint32_t)((t * 128 + oa) * 16), (uint32_t)((ob - oa) * 16), 128);
-              uint64_t b = umma_desc(sB1 + k * 1024, 512, 128);
-              umma_bf16(d, a, b, k > 0);
-            }
-          } else {
-            const uint32_t src = layer == 1 ? sA1 : sA2, plane = layer == 1 ? kPlane1 : kPlane2;
-            const uint32_t bb = layer == 1 ? sB2 : sB3;
+        if (layer == 0) {
+#pragma unroll 1
+          for (int t = 0; t < tiles; t++)
+#pragma unroll
+            for (int k = 0; k < kB1Mmas; k++)
+              umma_bf16(tmem + (uint32_t)(t * 32), a1d[k] + (uint64_t)(t * 128), b1d + (uint64_t)(k * 64), k > 0);
+        } else {
+          const uint64_t ad0 = layer == 1 ? a2d0 : a3d0, ad1 = layer == 1 ? a2d1 : a3d1, bd = layer == 1 ? b2d : b3d;
+#pragma unroll 1
+          for (int t = 0; t < tiles; t++) {
+            const uint32_t d = tmem + (uint32_t)(t * 32);
+#pragma unroll
             for (int tap = 0; tap < 9; tap++)
+#pragma unroll
               for (int h = 0; h < 2; h++) {
-                int off = (tap / 3) * kRow + tap % 3;
-                uint64_t a = umma_desc(src + 2 * h * plane + (uint32_t)((t * 128 + off) * 16), plane, 128);
-                uint64_t b = umma_desc(bb + (tap * 2 + h) * 1024, 512, 128);
-                umma_bf16(d, a, b, tap > 0 || h > 0);
+                const uint64_t off = (uint64_t)(t * 128 + (tap / 3) * kRow + tap % 3);
+                umma_bf16(d, (h ? ad1 : ad0) + off, bd + (uint64_t)((tap * 2 + h) * 64), tap > 0 || h > 0);
               }
           }
         }
         umma_commit(&ms.mbar);
+      }
+      if (layer == 0) {  // the next strip's bytes, in flight while the tensor cores work
+        next = ms.strip;
+        if (next < total) load_input(next);
       }
       // every thread polls the barrier; the outcome is made uniform before anyone acts on it
       ok = __syncthreads_and(mbar_wait(&ms.mbar, phase) ? 1 : 0) != 0;
@@ -268,18 +291,20 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
       phase ^= 1;
       fence_after_sync();
       if (!ok) break;
-      // epilogue: warp w reads rows 32 w .. 32 w + 31 of each tile; bias, ReLU, BF16 -> next map
+      // epilogue: warp w reads rows 32 (w % 4) .. + 31 of the tile pairs 2 (w / 4), + 4, ..; bias,
+      // ReLU, BF16 -> next map
       // conv1 -> A1; conv2 -> A2; conv3 -> A1 again (dead once conv2's MMAs completed), for the pooling
       uint8_t* dst = layer == 1 ? A2 : A1;
       const uint32_t dplane = layer == 1 ? kPlane2 : kPlane1;
-      for (int t = 0; t < tiles; t += 2) {  // two tiles (64 accumulator columns) per load
+      const int wl = warp & 3;
+      for (int t = 2 * (warp >> 2); t < tiles; t += 4) {  // two tiles (64 accumulator columns) per load
         float v[64];
-        if (t + 1 < tiles) tmem_ld64(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 32), v);
-        else tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 32), v);
+        if (t + 1 < tiles) tmem_ld64(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)(t * 32), v);
+        else tmem_ld32(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)(t * 32), v);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           if (t + h >= tiles) break;
-          const int p = (t + h) * 128 + warp * 32 + lane;
+          const int p = (t + h) * 128 + wl * 32 + lane;
 #pragma unroll
           for (int q = 0; q < 4; q++) {
             uint32_t w[4];
@@ -296,14 +321,14 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
       }
     }
     if (!ok) break;
+    __syncthreads();  // conv3's map complete
     // pooling of the conv3 map (in A1; map column 16 j + i is sample x 16 (mbx0 + j) - 1 + i):
-    // item (macroblock j, 8-channel plane q, map row r) reads the row's 18 positions 16 bytes at a
-    // time, then adds its row total and its four block-row totals into the shared sums
-    for (int i = tid; i < kStripMbs * 17 * C; i += 128) (&ms.pool[0][0][0])[i] = 0.0f;
-    __syncthreads();
-    for (int it = tid; it < kStripMbs * 4 * 18; it += 128) {
-      const int j = it / 72, q = (it / 18) % 4, r = it % 18;
-      const uint8_t* row = A1 + q * kPlane1 + (r * kRow + 16 * j) * 16;
+    // half-warp h < 4 kStripMbs takes macroblock j = h / 4 and 8-channel plane q = h % 4; its lane l
+    // sums map row l + 1 (16-byte reads), lanes 0 and 15 also the border rows 0 and 17; the block
+    // sums are reduced over the block row's four lanes, the 18 x 18 sum over all sixteen
+    if (tid < kStripMbs * 4 * 16) {
+      const int j = tid >> 6, q = (tid >> 4) & 3, l = tid & 15;
+      const uint8_t* base = A1 + q * kPlane1 + (16 * j) * 16;
       float tot[8], blk[4][8];
 #pragma unroll
       for (int k = 0; k < 8; k++) {
@@ -311,28 +336,44 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
 #pragma unroll
         for (int b = 0; b < 4; b++) blk[b][k] = 0.0f;
       }
+      for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1 && l != 0 && l != 15) break;
+        const int r = pass == 0 ? l + 1 : (l == 0 ? 0 : 17);
+        const uint8_t* row = base + r * kRow * 16;
 #pragma unroll
-      for (int i = 0; i < 18; i++) {
-        const uint4 v = *(const uint4*)(row + i * 16);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        for (int i = 0; i < 18; i++) {
+          const uint4 v = *(const uint4*)(row + i * 16);
+          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const float2 f = __bfloat1622float2(*(const __nv_bfloat162*)&w[k]);
-          tot[2 * k] += f.x;
-          tot[2 * k + 1] += f.y;
-          if (i >= 1 && i <= 16) {
-            blk[(i - 1) >> 2][2 * k] += f.x;
-            blk[(i - 1) >> 2][2 * k + 1] += f.y;
+          for (int k = 0; k < 4; k++) {
+            const float2 f = __bfloat1622float2(*(const __nv_bfloat162*)&w[k]);
+            tot[2 * k] += f.x;
+            tot[2 * k + 1] += f.y;
+            if (pass == 0 && i >= 1 && i <= 16) {
+              blk[(i - 1) >> 2][2 * k] += f.x;
+              blk[(i - 1) >> 2][2 * k + 1] += f.y;
+            }
           }
         }
       }
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        atomicAdd(&ms.pool[j][0][8 * q + k], tot[k] * (1.0f / 324.0f));
-        if (r >= 1 && r <= 16)
 #pragma unroll
-          for (int b = 0; b < 4; b++) atomicAdd(&ms.pool[j][1 + ((r - 1) >> 2) * 4 + b][8 * q + k], blk[b][k] * (1.0f / 16.0f));
+        for (int b = 0; b < 4; b++) {
+          blk[b][k] += __shfl_xor_sync(0xffffffffu, blk[b][k], 1);
+          blk[b][k] += __shfl_xor_sync(0xffffffffu, blk[b][k], 2);
+        }
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], o);
       }
+      if ((l & 3) == 0)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+          for (int k = 0; k < 8; k++) ms.pool[j][1 + (l >> 2) * 4 + b][8 * q + k] = blk[b][k] * (1.0f / 16.0f);
+      if (l == 0)
+#pragma unroll
+        for (int k = 0; k < 8; k++) ms.pool[j][0][8 * q + k] = tot[k] * (1.0f / 324.0f);
     }
     __syncthreads();
     // heads and hints: threads 0..47 the intra 4x4 heads of (macroblock tid / 16, block tid % 16),
@@ -374,7 +415,8 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
           }
           rg_mb_hint& hh = jb.hints[m];
           hh.part_mask = (uint8_t)topk_mask(lp, 4, ip.part_k, ip.part_margin);
-          hh.reserved = 0;
+          hh.flags = 0;  // the coarse motion pass, when on, follows
+          hh.mv_coarse[0] = hh.mv_coarse[1] = 0;
           for (int o = 0; o < 2; o++) hh.mv_off[o] = (int8_t)max(-127, min(127, __float2int_rn(16.0f * lm[o])));
           if (lg) {
             for (int o = 0; o < 4; o++) lg[o] = lp[o];
@@ -384,10 +426,83 @@ __global__ void __launch_bounds__(128, 1) cnn_infer_kernel(InferParams ip) {
         }
       }
     }
+    strip = next;
   }
   fence_before_sync();
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Coarse motion (rg_net_set_coarse_range): a warp per macroblock, 8 per block. The decimated
+// picture's sample (x, y) is the rounded mean of the four samples (2x + i, 2y + j), coordinates
+// clamped to the picture; the macroblock's 8 x 8 decimated block is compared with the decimated
+// previous picture at every displacement of +-r (SAD), the least (SAD, |dx| + |dy|, raster index)
+// wins.
+constexpr int kCoarseMaxR = 32;
+constexpr int kCoarseRow = (8 + 2 * kCoarseMaxR + 3) / 4 * 4 + 4;  // window row stride (bytes)
+constexpr int kCoarseWarps = 8;
+struct CoarseParams {
+  const InferJob* jobs;
+  int n_jobs, width, height, stride, mb_w, mb_h, r;
+};
+__device__ __forceinline__ uint32_t dec_sample(const uint8_t* p, int stride, int w, int h, int x, int y) {
+  const int x0 = min(max(2 * x, 0), w - 1), x1 = min(max(2 * x + 1, 0), w - 1);
+  const int y0 = min(max(2 * y, 0), h - 1), y1 = min(max(2 * y + 1, 0), h - 1);
+  const uint8_t* r0 = p + (size_t)y0 * stride;
+  const uint8_t* r1 = p + (size_t)y1 * stride;
+  return ((uint32_t)r0[x0] + r0[x1] + r1[x0] + r1[x1] + 2u) >> 2;
+}
+__device__ __forceinline__ uint32_t lds4_unaligned(const uint8_t* p) {
+  const uintptr_t a = (uintptr_t)p;
+  const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
+  return __funnelshift_r(b[0], b[1], (uint32_t)(a & 3) * 8u);
+}
+__global__ void __launch_bounds__(32 * kCoarseWarps) coarse_motion_kernel(CoarseParams cp) {
+  __shared__ __align__(16) uint8_t win[kCoarseWarps][(8 + 2 * kCoarseMaxR) * kCoarseRow];
+  __shared__ __align__(16) uint8_t blk[kCoarseWarps][64];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int per_pic = cp.mb_w * cp.mb_h;
+  const long task = (long)blockIdx.x * kCoarseWarps + warp;
+  if (task >= (long)cp.n_jobs * per_pic) return;
+  const int job = (int)(task / per_pic), m = (int)(task % per_pic);
+  const InferJob jb = cp.jobs[job];
+  if (jb.cur == jb.prev) return;  // an IDR picture: no previous picture
+  const int mbx = m % cp.mb_w, mby = m / cp.mb_w, R = cp.r, side = 8 + 2 * R;
+  const int bx = 8 * mbx, by = 8 * mby;  // the block's decimated origin
+  uint8_t* w = win[warp];
+  for (int i = lane; i < side * side; i += 32) {
+    const int y = i / side, x = i - y * side;
+    w[y * kCoarseRow + x] = (uint8_t)dec_sample(jb.prev, cp.stride, cp.width, cp.height, bx - R + x, by - R + y);
+  }
+  for (int i = lane; i < 64; i += 32)
+    blk[warp][i] = (uint8_t)dec_sample(jb.cur, cp.stride, cp.width, cp.height, bx + (i & 7), by + (i >> 3));
+  __syncwarp();
+  uint32_t b[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) b[k] = ((const uint32_t*)blk[warp])[k];
+  const int n = (2 * R + 1) * (2 * R + 1);
+  uint64_t best = ~0ull;
+  for (int p = lane; p < n; p += 32) {
+    const int dyi = p / (2 * R + 1), dxi = p - dyi * (2 * R + 1);
+    const uint8_t* q = w + dyi * kCoarseRow + dxi;
+    uint32_t sad = 0;
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+      sad = __vsadu4(lds4_unaligned(q + r * kCoarseRow), b[2 * r]) +
+            __vsadu4(lds4_unaligned(q + r * kCoarseRow + 4), b[2 * r + 1]) + sad;
+    const uint32_t dist = (uint32_t)(abs(dxi - R) + abs(dyi - R));
+    best = min(best, ((uint64_t)sad << 32) | ((uint64_t)dist << 16) | (uint64_t)p);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) best = min(best, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)best, o));
+  if (lane == 0) {
+    const int p = (int)(best & 0xffffu), dyi = p / (2 * R + 1), dxi = p - dyi * (2 * R + 1);
+    rg_mb_hint& h = jb.hints[m];
+    h.mv_coarse[0] = (int16_t)(8 * (dxi - R));
+    h.mv_coarse[1] = (int16_t)(8 * (dyi - R));
+    h.flags |= 1;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -705,6 +820,7 @@ struct rg_net {
   int jobs_cap = 0;
   int part_k = 3, i4_k = 3;  // hint policy (rg_net_set_hint_policy)
   float part_margin = INFINITY, i4_margin = INFINITY;
+  int coarse_range = 32;      // rg_net_set_coarse_range
 };
 
 namespace {
@@ -948,8 +1064,20 @@ int rg_net_predict_hints(rg_net* net, const uint8_t* const* dev_cur, const uint8
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int strips = n_pictures * ip.mb_h * ip.strips_per_row;
-  cnn_infer_kernel<<<sms < strips ? sms : strips, 128, kSmemInfer, st>>>(ip);
+  cnn_infer_kernel<<<sms < strips ? sms : strips, kThreads, kSmemInfer, st>>>(ip);
   NCK(cudaGetLastError());
+  if (net->coarse_range > 0) {
+    CoarseParams cp{net->jobs, n_pictures, width, height, (int)stride, ip.mb_w, ip.mb_h, net->coarse_range / 2};
+    const long tasks = (long)n_pictures * ip.mb_w * ip.mb_h;
+    coarse_motion_kernel<<<(unsigned)((tasks + kCoarseWarps - 1) / kCoarseWarps), 32 * kCoarseWarps, 0, st>>>(cp);
+    NCK(cudaGetLastError());
+  }
+  return RG_OK;
+}
+
+int rg_net_set_coarse_range(rg_net* net, int32_t range) {
+  if (!net || range < 0 || range > 2 * kCoarseMaxR || (range & 1)) return nfail(RG_ERR_INVALID, "rg_net_set_coarse_range: bad arguments");
+  net->coarse_range = range;
   return RG_OK;
 }
 

@@ -9,10 +9,10 @@
 //      each of the nine partition parts (16x16; 16x8 top, bottom; 8x16 left, right; four 8x8) the
 //      vector of least SAD + lambda * (bits(4 vx - mvp.x) + bits(4 vy - mvp.y)) against the 16x16
 //      predictor, first in raster order on ties. Full search: the window is +-search_range around
-//      the 16x16 predictor. Learned: +-2 around a centre chosen among six integer candidates --
-//      predictor plus the hinted offset, predictor, the left, top and top-right (top-left where
-//      that is absent) neighbours' vectors, zero -- by the 16x16 SAD + lambda * vector bits, first
-//      in that order on ties; while the 16x16 part's best lies on that window's edge (and not on
+//      the 16x16 predictor. Learned: +-2 around a centre chosen among seven integer candidates --
+//      predictor plus the hinted offset, predictor, the hint's coarse vector (when it has one), the
+//      left, top and top-right (top-left where that is absent) neighbours' vectors, zero -- by the
+//      16x16 SAD + lambda * vector bits, first in that order on ties; while the 16x16 part's best lies on that window's edge (and not on
 //      the vector bounds) the window is centred on it again, up to `walk` times, and then the full
 //      window is searched;
 //   3. for every partition type tried (all four; learned: the hinted ones), each part in coding
@@ -29,7 +29,7 @@
 constexpr int kBandRows = 8;               // integer vectors per band row
 constexpr int kBandBytes = (kBandRows + 15) * (2 * kMaxSearchRange + 28);
 constexpr int kLearnedRange = 2;           // learned form: integer window around the seed
-constexpr int kCentreCands = 6;            // learned form: candidates of the window's centre
+constexpr int kCentreCands = 7;            // learned form: candidates of the window's centre
 
 struct SearchSmem {
   uint8_t band[kBandBytes];
@@ -137,8 +137,55 @@ __device__ __forceinline__ uint32_t lds4u(const uint8_t* p) {
   const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
   return __funnelshift_r(b[0], b[1], (uint32_t)(a & 3) * 8u);
 }
+// A window of at most 32 vectors (the learned form's): lane v takes vector v in raster order and
+// sums its four quadrant SADs over the staged band; the same costs and ties as the wide search.
+__device__ __noinline__ void int_search_small(const Ctx& c, const Smem& sm, SearchSmem& ss, int xlo, int xhi, int ylo,
+                                              int yhi, int mvp0, int mvp1, uint32_t lambda, IntBest& ib) {
+  const int lane = lane_id();
+  const int x0 = c.mbx * 16, y0 = c.mby * 16, stride = c.fp->stride_y;
+  const uint8_t* ref = c.sd->ref_y;
+  const int xs = (x0 + xlo) & ~3;
+  const int bw = ((x0 + xhi + 20 - xs) + 3) & ~3;
+  const int nwx = xhi - xlo + 1, nwy = yhi - ylo + 1, wpr = bw >> 2;
+  __syncwarp();
+  for (int w = lane; w < (nwy + 15) * wpr; w += 32) {
+    const int r = w / wpr, k = w - r * wpr;
+    ((uint32_t*)ss.band)[r * wpr + k] = ldw32(ref + (long)(y0 + ylo + r) * stride + xs + 4 * k);
+  }
+  __syncwarp();
+  const bool act = lane < nwx * nwy;
+  const int vx = act ? lane % nwx : 0, vy = act ? lane / nwx : 0;
+  const int dx = xlo + vx, dy = ylo + vy;
+  const uint8_t* rp = ss.band + vy * bw + (x0 + dx - xs);
+  uint32_t q[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    const uint32_t* sp = (const uint32_t*)&sm.src_y[r * 16];
+    const uint8_t* rr = rp + r * bw;
+    const int h = (r >> 3) * 2;
+    q[h] = __vsadu4(lds4u(rr), sp[0]) + __vsadu4(lds4u(rr + 4), sp[1]) + q[h];
+    q[h + 1] = __vsadu4(lds4u(rr + 8), sp[2]) + __vsadu4(lds4u(rr + 12), sp[3]) + q[h + 1];
+  }
+  const uint32_t mc = lambda * se_bits(4 * dx - mvp0) + lambda * se_bits(4 * dy - mvp1);
+  const uint32_t part[9] = {q[0] + q[1] + q[2] + q[3], q[0] + q[1], q[2] + q[3], q[0] + q[2], q[1] + q[3],
+                            q[0], q[1], q[2], q[3]};
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const uint32_t cost = act ? part[k] + mc : UMAX;
+    const uint32_t m = __reduce_min_sync(FULL, cost);
+    const uint32_t i = __reduce_min_sync(FULL, act && cost == m ? (uint32_t)lane : 0xffffffffu);
+    ib.c[k] = m;
+    ib.x[k] = xlo + (int)(i % (uint32_t)nwx);
+    ib.y[k] = ylo + (int)(i / (uint32_t)nwx);
+  }
+}
+
 __device__ __noinline__ void int_search(const Ctx& c, const Smem& sm, SearchSmem& ss, int xlo, int xhi, int ylo, int yhi,
                                         int mvp0, int mvp1, uint32_t lambda, IntBest& ib) {
+  if ((xhi - xlo + 1) * (yhi - ylo + 1) <= 32) {
+    int_search_small(c, sm, ss, xlo, xhi, ylo, yhi, mvp0, mvp1, lambda, ib);
+    return;
+  }
   const FrameParams& fp = *c.fp;
   const int lane = lane_id();
   const int x0 = c.mbx * 16, y0 = c.mby * 16, stride = fp.stride_y;
@@ -522,9 +569,9 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   if (hint) {
     NbMv A = nb4(nb, -1, 0, none, 0), B = nb4(nb, 0, -1, none, 0), C = nb4(nb, 4, -1, none, 0);
     if (C.ref == -2) C = nb4(nb, -1, -1, none, 0);
-    const int vx[kCentreCands] = {mvp16[0] + hint->mv_off[0], mvp16[0], A.x, B.x, C.x, 0};
-    const int vy[kCentreCands] = {mvp16[1] + hint->mv_off[1], mvp16[1], A.y, B.y, C.y, 0};
-    const bool use[kCentreCands] = {true, true, A.ref == 0, B.ref == 0, C.ref == 0, true};
+    const int vx[kCentreCands] = {mvp16[0] + hint->mv_off[0], mvp16[0], hint->mv_coarse[0], A.x, B.x, C.x, 0};
+    const int vy[kCentreCands] = {mvp16[1] + hint->mv_off[1], mvp16[1], hint->mv_coarse[1], A.y, B.y, C.y, 0};
+    const bool use[kCentreCands] = {true, true, (hint->flags & 1) != 0, A.ref == 0, B.ref == 0, C.ref == 0, true};
     xhi = -(1 << 20);
     yhi = -(1 << 20);
 #pragma unroll

@@ -36,8 +36,9 @@ assert RECORD_DTYPE.itemsize == 888
 # Analysis forms (rg_set_analysis_form) and the learned form's per-macroblock hint (rg_mb_hint).
 RG_FORM_PLAIN, RG_FORM_FULLSEARCH, RG_FORM_LEARNED = 0, 1, 2
 RG_MB_P_L0_16X8, RG_MB_P_L0_8X16, RG_MB_P_8X8 = 4, 5, 6
-HINT_DTYPE = np.dtype([("part_mask", "u1"), ("reserved", "u1"), ("mv_off", "i1", (2,)), ("i4_mask", "<u2", (16,))])
-assert HINT_DTYPE.itemsize == 36
+HINT_DTYPE = np.dtype([("part_mask", "u1"), ("flags", "u1"), ("mv_off", "i1", (2,)), ("i4_mask", "<u2", (16,)),
+                       ("mv_coarse", "<i2", (2,))])
+assert HINT_DTYPE.itemsize == 40
 
 # Every symbol include/ragdoll_cuda.h declares.
 EXPORTS = [
@@ -56,7 +57,7 @@ EXPORTS = [
     "rg_net_param_count", "rg_net_create", "rg_net_destroy", "rg_net_set_params", "rg_net_get_params",
     "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
     "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device", "rg_set_search_tuning",
-    "rg_net_set_hint_policy",
+    "rg_net_set_hint_policy", "rg_net_set_coarse_range",
 ]
 
 
@@ -167,6 +168,7 @@ def lib() -> ctypes.CDLL:
                                        P, P, P]
     L.rg_net_check.argtypes = [P, P]
     L.rg_net_set_hint_policy.argtypes = [P, ctypes.c_int32, ctypes.c_float, ctypes.c_int32, ctypes.c_float]
+    L.rg_net_set_coarse_range.argtypes = [P, ctypes.c_int32]
     L.rg_net_crops.argtypes = [P, P, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_size_t, P, P]
     L.rg_net_forward_backward.argtypes = [P, P, ctypes.c_int32, P, P, P, P, ctypes.c_float, P, P, P]
     L.rg_net_adam_step.argtypes = [P, ctypes.c_float]

@@ -75,6 +75,11 @@ class CandidateNet:
         ones up to part_k while within part_margin of the best logit; intra 4x4 modes alike."""
         _check(lib().rg_net_set_hint_policy(self.h, part_k, part_margin, i4_k, i4_margin))
 
+    def set_coarse_range(self, search_range: int = 32) -> None:
+        """Range (samples, even, 0: off) of the coarse motion pass that follows the network in
+        predict_hints and fills the hints' mv_coarse (rg_net_set_coarse_range)."""
+        _check(lib().rg_net_set_coarse_range(self.h, search_range))
+
     def check(self, stream: int = 0) -> None:
         _check(lib().rg_net_check(self.h, stream or None))
 

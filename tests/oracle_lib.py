@@ -106,7 +106,7 @@ class OracleEncoder:
         """Search forms (1 full search, 2 learned): decisions and reconstruction only, no bitstream."""
         lib().oracle_enc_set_form(self.h, form, search_range)
 
-    def set_search_tuning(self, type_bits=(1, 3, 3, 7), walk=4):
+    def set_search_tuning(self, type_bits=(1, 16, 16, 40), walk=4):
         tb = (ctypes.c_int * 4)(*type_bits)
         lib().oracle_enc_set_search_tuning(self.h, tb, walk)
 

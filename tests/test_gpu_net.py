@@ -7,6 +7,8 @@
   multiple of the strip): every logit equals the oracle's BF16 arithmetic within the stated
   tolerance, and the hints are the top three of the GPU's own logits; under another hint policy
   (fewer candidates, logit margins) the kept candidates are those of the same rule on the host.
+* The coarse motion pass that follows the network (2:1 decimated exhaustive SAD search) gives the
+  vectors of a numpy restatement; IDR pictures get none.
 * Training on full-search labels lowers the loss.
 * End to end: hints from the network drive the learned form; its records equal the oracle's with
   the same hints, and its CABAC stream decodes (FFmpeg) to the engine's reconstruction.
@@ -145,6 +147,59 @@ def test_hint_policy_keeps_the_candidates_within_the_margin():
                 b = DEC_TO_RASTER[d]
                 assert hh["i4_mask"][m][d] == _topk_mask(lg[m, 6 + 9 * b:15 + 9 * b], i4_k, i4_margin)
     net.set_hint_policy()
+
+
+def _coarse_motion(cur, prev, r):
+    """The coarse motion pass on the host: 2:1 decimation (rounded 2x2 means, coordinates clamped
+    to the picture), least (SAD, |dx| + |dy|, raster index) over +-r decimated samples, twice the
+    vector in quarter samples."""
+    h, w = cur.shape
+    mb_w, mb_h = (w + 15) // 16, (h + 15) // 16
+
+    def dec(p, x0, y0, nx, ny):
+        xs, ys = np.arange(x0, x0 + nx), np.arange(y0, y0 + ny)
+        c = lambda v, n: np.clip(v, 0, n - 1)
+        q = p.astype(np.int32)
+        return (q[np.ix_(c(2 * ys, h), c(2 * xs, w))] + q[np.ix_(c(2 * ys, h), c(2 * xs + 1, w))] +
+                q[np.ix_(c(2 * ys + 1, h), c(2 * xs, w))] + q[np.ix_(c(2 * ys + 1, h), c(2 * xs + 1, w))] + 2) >> 2
+    out = np.zeros((mb_w * mb_h, 2), np.int32)
+    for my in range(mb_h):
+        for mx in range(mb_w):
+            blk = dec(cur, 8 * mx, 8 * my, 8, 8)
+            win = dec(prev, 8 * mx - r, 8 * my - r, 8 + 2 * r, 8 + 2 * r)
+            sw = np.lib.stride_tricks.sliding_window_view(win, (8, 8))
+            sad = np.abs(sw - blk).sum(axis=(2, 3))
+            dy, dx = np.meshgrid(np.arange(-r, r + 1), np.arange(-r, r + 1), indexing="ij")
+            key = sad.astype(np.int64) * (1 << 32) + (np.abs(dx) + np.abs(dy)) * (1 << 16) + np.arange(sad.size).reshape(sad.shape)
+            i = int(np.argmin(key))
+            out[my * mb_w + mx] = (8 * dx.flat[i], 8 * dy.flat[i])
+    return out
+
+
+@pytest.mark.parametrize("search_range", [32, 10])
+def test_coarse_motion_matches_host_restatement(search_range):
+    import torch
+
+    from ragdoll_b200.engine import HINT_DTYPE
+    from ragdoll_b200.learned import CandidateNet, hints_for
+    w, h = 150, 84
+    frames = grating_clip(w, h, 2, seed=31, motion=9.0, rects=2)
+    cur, prev = frames[1][0], frames[0][0]
+    net = CandidateNet(0, params=_params(8))
+    net.set_coarse_range(search_range)
+    tc, tp = torch.from_numpy(np.ascontiguousarray(cur)).cuda(), torch.from_numpy(np.ascontiguousarray(prev)).cuda()
+    hints, _ = hints_for(net, [tc.data_ptr(), tc.data_ptr()], [tp.data_ptr(), tc.data_ptr()], w, h, w)
+    net.check()
+    torch.cuda.synchronize()
+    hp = hints[0].cpu().numpy().view(HINT_DTYPE)
+    hi = hints[1].cpu().numpy().view(HINT_DTYPE)
+    assert (hp["flags"] == 1).all() and (hi["flags"] == 0).all(), "an IDR picture (prev = cur) has no coarse vector"
+    want = _coarse_motion(cur, prev, search_range // 2)
+    assert np.array_equal(hp["mv_coarse"].astype(np.int32), want)
+    net.set_coarse_range(0)
+    hints, _ = hints_for(net, [tc.data_ptr()], [tp.data_ptr()], w, h, w)
+    torch.cuda.synchronize()
+    assert (hints[0].cpu().numpy().view(HINT_DTYPE)["flags"] == 0).all()
 
 
 def test_training_on_full_search_labels_lowers_the_loss():

@@ -30,6 +30,9 @@ def random_hints(n_mb, seed):
         parts = rng.choice(4, size=3, replace=False)
         h["part_mask"][i] = sum(1 << int(p) for p in parts)
         h["mv_off"][i] = rng.integers(-12, 13, 2)
+        if rng.random() < 0.7:  # a coarse vector (even integer samples) on most macroblocks
+            h["flags"][i] = 1
+            h["mv_coarse"][i] = 8 * rng.integers(-6, 7, 2)
         for b in range(16):
             modes = rng.choice(9, size=3, replace=False)
             h["i4_mask"][i, b] = sum(1 << int(m) for m in modes)

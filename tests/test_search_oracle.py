@@ -40,6 +40,8 @@ def test_search_form_streams_decode_to_the_oracle_reconstruction(profile, qp, fo
             hh = np.zeros(n, HINT_DTYPE)
             hh["part_mask"] = rng.integers(1, 16, n)
             hh["mv_off"] = rng.integers(-8, 9, (n, 2))
+            hh["flags"] = rng.integers(0, 2, n)
+            hh["mv_coarse"] = 8 * rng.integers(-5, 6, (n, 2))
             hh["i4_mask"] = rng.integers(1, 512, (n, 16))
             hints.append(hh)
     recs, recons = _encode(w, h, qp, profile, form, 16, frames, hints)
