@@ -841,8 +841,8 @@ def run_engine(args, rank, world, local):
 
 
 def run_profile_case_cnn(args, local):
-    """Small case for ncu of the network kernel: the hints of 8 pictures of the 1080p clip (two
-    launches of cnn_infer_kernel, 65 280 macroblocks each)."""
+    """Small case for ncu of the network kernel: the hints of 8 pictures of the 1080p clip (65 280
+    macroblocks a launch of cnn_infer_kernel): twice without the coarse motion pass, twice with it."""
     import torch
 
     from ragdoll_b200.learned import CandidateNet, hints_for
@@ -852,16 +852,20 @@ def run_profile_case_cnn(args, local):
     net = CandidateNet.trained(local)
     ptrs = [luma[i].data_ptr() for i in range(1, 9)]
     prev = [luma[i - 1].data_ptr() for i in range(1, 9)]
-    times = []
-    for _ in range(2):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        hints_for(net, ptrs, prev, W, H, W)
-        e1.record()
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+    times = {}
+    for coarse in (0, 32):   # the network alone, then with the coarse motion pass after it
+        net.set_coarse_range(coarse)
+        times[coarse] = []
+        for _ in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            hints_for(net, ptrs, prev, W, H, W)
+            e1.record()
+            e1.synchronize()
+            times[coarse].append(round(e0.elapsed_time(e1), 3))
     net.check()
-    print(json.dumps({"profile_case": "network hints of 8 1080p pictures", "ms": [round(t, 3) for t in times]}), flush=True)
+    print(json.dumps({"profile_case": "network hints of 8 1080p pictures", "ms_network": times[0],
+                      "ms_network_and_coarse_motion": times[32]}), flush=True)
 
 
 def run_profile_case(args, local):

@@ -275,8 +275,9 @@ int32_t rg_pipeline_lag(const rg_ctx* ctx);
  *   centre chosen among integer candidates (the predictor plus the hinted offset, the predictor,
  *   the hint's coarse vector, the left / top / top-right neighbours' vectors, zero) by 16x16 SAD
  *   plus vector bits, re-centred on its best up to `walk` times while that lies on the window's
- *   edge, then the full +-search_range search; only the hinted partition types are refined, and
- *   intra 4x4 blocks of IDR pictures try only their hinted prediction modes.
+ *   edge, then the full +-search_range search; only the hinted partition types are refined (by
+ *   SAD: a half-sample diamond step, then up to two quarter-sample diamond steps), and intra 4x4
+ *   blocks of IDR pictures try only their hinted prediction modes.
  */
 #define RG_FORM_PLAIN 0
 #define RG_FORM_FULLSEARCH 1

@@ -2249,8 +2249,9 @@ struct Encoder {
   // integer candidates (predictor plus the hinted offset, predictor, the hint's coarse vector when
   // it has one, left / top / top-right (else top-left) neighbour vectors, zero) by 16x16 SAD +
   // lambda * vector bits, first in that order on ties; re-centred on the 16x16 best while that lies
-  // on the window's edge (`walk` times), then the full window; only the hinted types, and intra 4x4
-  // blocks of IDR pictures restricted to their hinted modes.
+  // on the window's edge (`walk` times), then the full window; only the hinted types, refined by the
+  // SAD diamonds of refine_part_sad_s; intra 4x4 blocks of IDR pictures restricted to their hinted
+  // modes.
   int form = 0, search_range = 32, walk = 4;
   int type_bits[4] = {1, 16, 16, 40};   // bits charged per partition type (x lambda)
   const rg_mb_hint* hints = nullptr;    // learned form: this picture's hints
@@ -2331,6 +2332,34 @@ struct Encoder {
         if (c < best) { best = c; cx = vx; cy = vy; }
       }
     }
+    mv[0] = cx; mv[1] = cy;
+    return best;
+  }
+  // learned form: SAD diamonds (half-sample: up, left, right, down at distance 2, one step; then
+  // quarter-sample at distance 1, up to two steps), cost SAD + lambda * vector bits, within 3
+  // quarter samples of the integer start
+  uint32_t part_sad_cost(int x0, int y0, const MbSrc& src, int px, int py, int pw, int ph, int mx, int my, const int mvp[2],
+                         uint32_t lambda) const {
+    uint8_t pred[256];
+    luma_mc(refp.y.ptr(x0 + px + (mx >> 2), y0 + py + (my >> 2)), refp.y.stride, pw, ph, mx & 3, my & 3, pred, 16);
+    return sad(src.y + py * 16 + px, 16, pred, 16, pw, ph) + lambda * (se_bits(mx - mvp[0]) + se_bits(my - mvp[1]));
+  }
+  uint32_t refine_part_sad_s(int x0, int y0, const MbSrc& src, const Bounds& bd, int px, int py, int pw, int ph, int ix,
+                             int iy, const int mvp[2], uint32_t lambda, int mv[2]) const {
+    int cx = 4 * ix, cy = 4 * iy;
+    uint32_t best = part_sad_cost(x0, y0, src, px, py, pw, ph, cx, cy, mvp, lambda);
+    for (int st = 2; st >= 1; st--)
+      for (int it = 0; it < (st == 2 ? 1 : 2); it++) {
+        int fx = cx, fy = cy;
+        const int d[4][2] = {{0, -st}, {-st, 0}, {st, 0}, {0, st}};
+        for (int k = 0; k < 4; k++) {
+          int vx = fx + d[k][0], vy = fy + d[k][1];
+          if (std::abs(vx - 4 * ix) > 3 || std::abs(vy - 4 * iy) > 3 || !in_bounds(bd, vx, vy)) continue;
+          uint32_t c = part_sad_cost(x0, y0, src, px, py, pw, ph, vx, vy, mvp, lambda);
+          if (c < best) { best = c; cx = vx; cy = vy; }
+        }
+        if (cx == fx && cy == fy) break;
+      }
     mv[0] = cx; mv[1] = cy;
     return best;
   }
@@ -2459,7 +2488,8 @@ struct Encoder {
         const int* g = parts[first[t] + k];
         int mvp[2], mv[2];
         mv_pred_s(mbx, mby, g[4], g[5], g[6], g[7], own, done, mvp);
-        J += refine_part_s(x0, y0, src, bd, g[0], g[1], g[2], g[3], ibx[g[8]], iby[g[8]], mvp, lambda, mv);
+        J += h ? refine_part_sad_s(x0, y0, src, bd, g[0], g[1], g[2], g[3], ibx[g[8]], iby[g[8]], mvp, lambda, mv)
+               : refine_part_s(x0, y0, src, bd, g[0], g[1], g[2], g[3], ibx[g[8]], iby[g[8]], mvp, lambda, mv);
         pm[k][0] = mv[0]; pm[k][1] = mv[1];
         pd[k][0] = mv[0] - mvp[0]; pd[k][1] = mv[1] - mvp[1];
         for (int q = 0; q < 4; q++)

@@ -19,7 +19,8 @@
 //      order from its integer best: half-sample step (centre, then 8 neighbours at distance 2,
 //      quarter units) and quarter-sample step (8 neighbours at distance 1), costs (SATD >> 1) +
 //      lambda * vector bits against the part's own predictor (H.264 8.4.1.3, directional for 16x8
-//      and 8x16), least cost first in candidate order;
+//      and 8x16), least cost first in candidate order; learned: the SAD diamonds of
+//      refine_part_sad instead;
 //   4. the type of least total cost, the stream's type bits (per partition type) * lambda added,
 //      first on ties;
 //   5. intra 16x16 check, residual, late skip and reconstruction exactly as the plain form.
@@ -372,6 +373,47 @@ __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& w
   return best_key >> 4;
 }
 
+// Learned form: refinement of one part from its integer best (bx, by) by SAD -- the half-sample
+// diamond (up, left, right, down at distance 2, one step), then the quarter-sample diamond (the
+// same at distance 1, up to two steps, each from the step's start), cost SAD + lambda * vector bits
+// against the part's predictor, the first strict minimum in that order; lanes take the part's
+// 4-sample words, one candidate at a time.
+__device__ __noinline__ uint32_t part_sad(const Smem& sm, int px, int py, int pw, int ph, int bx, int by, int vx, int vy) {
+  const int lane = lane_id();
+  const QSrc q = qpel_src(sm, (vx >> 2) - bx + 1 + px, (vy >> 2) - by + 1 + py, vx & 3, vy & 3);
+  const int wpr = pw >> 2, nw = wpr * ph;
+  uint32_t s = 0;
+  for (int w = lane; w < nw; w += 32) {
+    const int r = w / wpr, x = (w - r * wpr) * 4;
+    uint32_t a = lds4u(q.a + r * q.sa + x);
+    if (q.avg) a = __vavgu4(a, lds4u(q.b + r * q.sb + x));
+    s = __vsadu4(a, *(const uint32_t*)&sm.src_y[(py + r) * 16 + px + x]) + s;
+  }
+  return wsum(s);
+}
+__device__ __noinline__ uint32_t refine_part_sad(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph,
+                                                 int bx, int by, const int* mvp, uint32_t lambda, const Bounds& bd,
+                                                 int* mv) {
+  ensure_window(c, sm, ws, bx, by);
+  int cx = 4 * bx, cy = 4 * by;
+  uint32_t best = part_sad(sm, px, py, pw, ph, bx, by, cx, cy) + vec_cost(cx - mvp[0], cy - mvp[1], lambda);
+  for (int st = 2; st >= 1; st--) {
+    for (int it = 0; it < (st == 2 ? 1 : 2); it++) {
+      const int fx = cx, fy = cy;
+      for (int k = 0; k < 4; k++) {
+        const int vx = fx + (k == 1 ? -st : (k == 2 ? st : 0)), vy = fy + (k == 0 ? -st : (k == 3 ? st : 0));
+        if (abs(vx - 4 * bx) > 3 || abs(vy - 4 * by) > 3 || !in_bounds(bd, vx, vy)) continue;  // uniform
+        const uint32_t cost = part_sad(sm, px, py, pw, ph, bx, by, vx, vy) + vec_cost(vx - mvp[0], vy - mvp[1], lambda);
+        if (cost < best) { best = cost; cx = vx; cy = vy; }
+      }
+      if (cx == fx && cy == fy) break;
+    }
+  }
+  mv[0] = cx;
+  mv[1] = cy;
+  return best;
+}
+
 // The luma prediction of a part at quarter-sample vector mv (within 3 quarter samples of 4 (bx, by),
 // the integer vector its refinement started from) into pred_y.
 __device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
@@ -645,7 +687,8 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
       const int8_t* g = c_parts[first + k];
       int mvp[2], mv[2];
       mv_pred(nb, g[4], g[5], g[6], g[7], own, done, mvp);
-      uint32_t cost = refine_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv);
+      uint32_t cost = hint ? refine_part_sad(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv)
+                           : refine_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv);
       J += cost;
       pm[k][0] = mv[0]; pm[k][1] = mv[1];
       pd[k][0] = mv[0] - mvp[0]; pd[k][1] = mv[1] - mvp[1];
