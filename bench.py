@@ -4,19 +4,21 @@
 Workload (one "step"): a seeded synthetic 1920x1080 4:2:0 clip of 120 frames (sum of four
 gratings + blurred noise, +-24 px quarter-sample global motion, 12 moving textured rectangles),
 encoded as ragdoll transcode cuts it -- 8 independent 15-frame GOPs (IDR + 14 P), High profile
-decisions (8x8 transform), fixed QP 26, Balanced analysis -- with the 8 GOPs analysed side by
-side in one persistent launch. The device step covers analysis, reconstruction, deblocking and
-border extension of all 120 frames.
+decisions (8x8 transform), fixed QP 26 -- with the 8 GOPs analysed side by side in one persistent
+launch. The device step covers analysis, reconstruction, deblocking and border extension of all
+120 frames; the learned form's step also runs the candidate network and the coarse motion pass.
 
-value:  frames/s of the device step with the source clip resident in HBM (device pointers into
-        the C ABI).
-e2e:    frames/s of the whole encode through the public encoder (rg_encoder_submit / _collect,
-        ragdoll_b200.encoder.H264Encoder): host->device copy of every frame from pinned host
-        memory, the persistent launch, device->host copy of every macroblock record, and the
-        CABAC access units of all 120 pictures written on the host cores -- two waves in flight,
-        so one is analysed while the other is written.
-e2e_analysis: the host-buffer analysis call alone (rg_analyse_gops_async, records out, no
-        bitstream), for comparison.
+The default line is the learned form against the plain (Balanced) form:
+value:  frames/s of the learned form's device step (network, coarse motion, persistent analysis
+        launch; sources resident in HBM).
+e2e:    frames/s of the learned form through the public encoder (rg_encoder_set_form, then
+        rg_encoder_submit / _collect): host->device copy of every frame from pinned host memory,
+        the launches, device->host copy of every macroblock record, and the CABAC access units of
+        all 120 pictures written on the host cores -- two waves in flight.
+bd_rate_vs_plain_pct: Bjontegaard delta rate of the learned form against the plain form (bits at
+        equal luma PSNR over QP 22 / 26 / 30 / 34, every access unit written); `rd` the points.
+plain:  the plain form's device frames/s, its e2e through the same encoder (and the analysis-only
+        host-buffer call), its HBM roofline, and the parity of its bitstream with the oracle.
 --impl reference: the CPU restatement of ragdoll's encoder (the oracle) on the same workload
         sample, GOP-parallel across the host cores (parallel_gop_map semantics).
 --workload batched: the batched-streams configuration instead (64 streams of four sizes, a QP
@@ -45,7 +47,7 @@ sys.path.insert(0, str(ROOT))
 
 W, H, FRAMES, GOP, QP = 1920, 1080, 120, 15, 26
 MOTION, RECTS = 24.0, 12
-METRIC = "1080p H.264 encode frames/s (plain GPU form)"
+METRIC = "1080p H.264 encode frames/s: learned vs plain GPU, equal PSNR, \u22642% bit cost"
 UNIT = "frames/s"
 BYTES_PER_FRAME = 7.5 * W * H  # source 1.5 + reference 1.5 + recon 1.5 + deblock read/write 3.0 (x W*H)
 # DRAM bytes per picture of pipeline_kernel measured by ncu (dram__bytes_read + write) on a launch
@@ -349,7 +351,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-LEARNED_METRIC = "1080p H.264 encode frames/s: learned vs plain GPU, equal PSNR, <=2% bit cost"
+LEARNED_METRIC = METRIC
 QPS = (22, 26, 30, 34)
 CNN_FLOP_PER_MB = 2 * (22 * 22 * 32 * 18 + 20 * 20 * 32 * 288 + 18 * 18 * 32 * 288)  # 24x24 crop, three 3x3 convs
 
@@ -606,6 +608,177 @@ def run_4k(args, rank, world, local):
 
 
 # ------------------------------------------------------------------------------------------------
+def rd_point(eng_factory, clip, planes, gops, qp, hints_of=None):
+    """Bits and mean luma PSNR of the 8 GOPs x 15 at one QP: per-picture calls of one engine, every
+    access unit written by the host CABAC writer, reconstructions compared with the source."""
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_HIGH, BitstreamWriter
+    eng = eng_factory(qp)
+    writers = [BitstreamWriter(W, H, qp, profile=RG_PROFILE_HIGH) for _ in range(gops)]
+    cw = (W + 1) // 2
+    bits, psnr = 0, []
+    for f in range(GOP):
+        kind = RG_FRAME_IDR if f == 0 else RG_FRAME_P
+        ptrs = []
+        for g in range(gops):
+            ptrs += planes(g * GOP + f)
+        if hints_of is not None:
+            eng.set_hints_device([hints_of[g * GOP + f].data_ptr() for g in range(gops)])
+        eng.analyse_device(ptrs, W, cw, [kind] * gops)
+        recs = eng.records()
+        for g in range(gops):
+            bits += 8 * len(writers[g].picture(recs[g], kind))
+            y = eng.recon_coded(g)[0][:H, :W].astype(np.int32)
+            mse = float(np.mean((y - clip[g * GOP + f][0].astype(np.int32)) ** 2))
+            psnr.append(10 * np.log10(255.0 ** 2 / max(mse, 1e-9)))
+    eng.close()
+    return {"kbits": round(bits / 1000, 1), "psnr_y": round(float(np.mean(psnr)), 4)}
+
+
+def measure_learned(args, local, dist, base, fbytes, planes, gops, frames_host, clip, rank, barrier):
+    """The learned form on the step's workload: device frames/s of the whole learned step (network
+    and coarse-motion launches, then the persistent analysis launch, one stream), the network alone
+    and the analysis alone (hints computed beforehand); end to end through the public encoder
+    (rg_encoder_set_form); on rank 0 the rate and PSNR of the plain and learned forms at QP 22 / 26
+    / 30 / 34 and the Bjontegaard delta rate of the learned form against the plain one."""
+    import torch
+
+    from ragdoll_b200.encoder import H264Encoder
+    from ragdoll_b200.engine import (RG_FORM_FULLSEARCH, RG_FORM_LEARNED, RG_FORM_PLAIN, RG_FRAME_IDR, RG_FRAME_P,
+                                     RG_PROFILE_HIGH, Engine)
+    from ragdoll_b200.learned import WEIGHTS, CandidateNet, hints_for
+    cw = (W + 1) // 2
+    net = CandidateNet.trained(local)
+    ptrs, kinds = [], []
+    for f in range(GOP):
+        for g in range(gops):
+            ptrs += planes(g * GOP + f)
+            kinds.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+    idx = [g * GOP + f for f in range(GOP) for g in range(gops)]          # the call's [f][s] order
+    prev = [i if i % GOP == 0 else i - 1 for i in idx]
+    cur_p, prev_p = [base + i * fbytes for i in idx], [base + i * fbytes for i in prev]
+
+    def learned_engine(qp, with_net=True):
+        e = Engine(W, H, qp, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
+        e.set_analysis_form(RG_FORM_LEARNED, 32)
+        if with_net:
+            e.set_hint_net(net)
+        return e
+
+    def timed(stream, fn, steps):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(a.elapsed_time(b) / steps, dist, f"cuda:{local}")
+
+    # 1. the learned step: network + coarse motion + analysis, one stream
+    eng = learned_engine(QP)
+    st = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    steps = max(1, min(args.steps, 8))
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms = timed(st, lambda: eng.analyse_gops_device(ptrs, W, cw, kinds, GOP), steps)
+    clk = clocks.stop()
+    eng.close()
+    # 2. the network (and coarse pass) alone, and 3. the analysis alone with those hints
+    hints, _ = hints_for(net, cur_p, prev_p, W, H, W, device=local)
+    hs = torch.cuda.Stream(device=local)
+
+    def predict():
+        net.predict_hints(cur_p, prev_p, W, H, W, [h.data_ptr() for h in hints], None, hs.cuda_stream)
+    net.set_coarse_range(0)
+    cnn_ms = timed(hs, predict, steps)
+    net.set_coarse_range(32)
+    net_ms = timed(hs, predict, steps)
+    net.check(hs.cuda_stream)
+    eng = learned_engine(QP, with_net=False)
+    st = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    hp = [h.data_ptr() for h in hints]
+
+    def analysis():
+        eng.set_hints_device(hp)
+        eng.analyse_gops_device(ptrs, W, cw, kinds, GOP)
+    ana_ms = timed(st, analysis, steps)
+    eng.close()
+    # the same step with one partition type per macroblock (hint policy top-1), and the full-search
+    # form (the learned form's fallback and judge)
+    net.set_hint_policy(1)
+    eng = learned_engine(QP)
+    st = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    top1_ms = timed(st, lambda: eng.analyse_gops_device(ptrs, W, cw, kinds, GOP), steps)
+    eng.close()
+    hints1, _ = hints_for(net, cur_p, prev_p, W, H, W, device=local)
+    net.set_hint_policy()
+    eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
+    eng.set_analysis_form(RG_FORM_FULLSEARCH, 32)
+    st = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    fs_ms = timed(st, lambda: eng.analyse_gops_device(ptrs, W, cw, kinds, GOP), max(1, min(steps, 3)))
+    eng.close()
+    # 4. end to end: host frames in, access units out, through the public encoder
+    local_world = int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+    enc = H264Encoder(W, H, QP, profile=RG_PROFILE_HIGH, keyint=GOP, streams=gops, max_frames=GOP, device=local,
+                      threads=max(2, (os.cpu_count() or 1) // max(local_world, 1)))
+    enc.set_form(RG_FORM_LEARNED, 32, net)
+    for _ in range(2):
+        enc.new_gops()
+        enc.submit(frames_host)
+    enc.collect()
+    enc.collect()
+    barrier()
+    t0 = time.perf_counter()
+    out_bytes = 0
+    for k in range(steps):
+        enc.new_gops()
+        enc.submit(frames_host)
+        if k:
+            out_bytes += sum(len(au) for row in enc.collect() for au in row)
+    out_bytes += sum(len(au) for row in enc.collect() for au in row)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / steps, dist, f"cuda:{local}")
+    enc.close()
+    out = {"step_ms": step_ms, "cnn_ms": cnn_ms, "network_ms": net_ms, "analysis_ms": ana_ms, "e2e_ms": e2e_ms, "steps": steps,
+           "top1_ms": top1_ms, "fullsearch_ms": fs_ms,
+           "clocks": clk, "bitstream_bytes_per_step": round(out_bytes / steps), "weights": WEIGHTS.name}
+    # 5. rate and distortion (rank 0, outside the timed regions)
+    if rank == 0:
+        def plain_engine(qp):
+            e = Engine(W, H, qp, profile=RG_PROFILE_HIGH, num_streams=gops, device=local)
+            e.set_analysis_form(RG_FORM_PLAIN, 32)
+            return e
+        def fs_engine(qp):
+            e = Engine(W, H, qp, profile=RG_PROFILE_HIGH, num_streams=gops, device=local)
+            e.set_analysis_form(RG_FORM_FULLSEARCH, 32)
+            return e
+        by_pic = {i: hints[k] for k, i in enumerate(idx)}
+        by_pic1 = {i: hints1[k] for k, i in enumerate(idx)}
+        rd = {"plain": {}, "learned": {}, "learned_top1": {}, "fullsearch": {}}
+        for qp in QPS:
+            rd["plain"][qp] = rd_point(plain_engine, clip, planes, gops, qp)
+            # the hints do not depend on the QP: the same ones serve every QP
+            rd["learned"][qp] = rd_point(lambda q: learned_engine(q, with_net=False), clip, planes, gops, qp, by_pic)
+            rd["learned_top1"][qp] = rd_point(lambda q: learned_engine(q, with_net=False), clip, planes, gops, qp,
+                                              by_pic1)
+            rd["fullsearch"][qp] = rd_point(fs_engine, clip, planes, gops, qp)
+
+        def curve(name):
+            return [rd[name][q]["kbits"] for q in QPS], [rd[name][q]["psnr_y"] for q in QPS]
+        out["rd"] = rd
+        out["bd_rate_vs_plain_pct"] = round(bd_rate(*curve("plain"), *curve("learned")), 3)
+        out["bd_rates_pct"] = {f"{b}_vs_{a}": round(bd_rate(*curve(a), *curve(b)), 3)
+                               for a, b in (("plain", "learned_top1"), ("fullsearch", "learned"),
+                                            ("fullsearch", "learned_top1"), ("plain", "fullsearch"))}
+    net.close()
+    return out
+
+
+# ------------------------------------------------------------------------------------------------
 def run_engine(args, rank, world, local):
     import torch
 
@@ -748,6 +921,9 @@ def run_engine(args, rank, world, local):
     enc_threads = enc.threads
     enc.close()
 
+    # the learned form on the same workload (the headline of the line)
+    learned = measure_learned(args, local, dist, base, fbytes, planes, gops, frames_host, clip, rank, barrier)
+
     # SSIM and MS-SSIM of 120 luma plane pairs in one batched call (shared launches over every
     # pair and pyramid level); the pairs are pictures of the step's clip (their values do not change
     # the work). Algorithmic bytes per 1080p pair: both planes read at the five levels, and four
@@ -806,14 +982,15 @@ def run_engine(args, rank, world, local):
                   "checked": f"every access unit of the last timed e2e step ({gops} GOPs x {GOP} pictures)"}
 
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(dev_ms, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
-            "config": bench_config(world, args.mode),
-            "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
-                    "d2h_bytes_per_step": GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize,
-                    "bitstream_bytes_per_step": round(out_bytes / args.steps),
+        l_value = frames_total / (learned["step_ms"] / 1000)
+        l_e2e = frames_total / (learned["e2e_ms"] / 1000)
+        l_ana = bytes_per_launch / (learned["analysis_ms"] / 1000) / 1e9 if args.mode == "pipelined" else None
+        n_mb = eng.n_mb
+        cnn_tflops = n_mb * FRAMES * CNN_FLOP_PER_MB / (learned["cnn_ms"] / 1000) / 1e12
+        tpeak = peaks.get("bf16_tflops", 1590.0)
+        plain = {
+            "value": round(value, 2), "ms_per_step": round(dev_ms, 3), "steps": args.steps,
+            "e2e": {"value": round(e2e, 2), "unit": UNIT, "bitstream_bytes_per_step": round(out_bytes / args.steps),
                     "host_threads": enc_threads,
                     "path": "rg_encoder_submit/collect: copy in, persistent launch, records out, CABAC on the host"},
             "e2e_analysis": {"value": round(frames_total / (ana_ms / 1000), 2), "unit": UNIT,
@@ -823,6 +1000,41 @@ def run_engine(args, rank, world, local):
                          "traffic": round(TRAFFIC_PER_FRAME * FRAMES) if args.mode == "pipelined" else None,
                          "kernel": kernel_name, "launch_ms": round(launch_ms, 5),
                          "bytes_per_launch": round(bytes_per_launch)},
+            "parity": parity, "clocks": clk, "gpu_launches": launches,
+        }
+        line = {
+            "metric": METRIC, "value": round(l_value, 2), "unit": UNIT, "n_gpus": world, "steps": learned["steps"],
+            "warmup": max(args.warmup, 1), "ms_per_step": round(learned["step_ms"], 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network / u8,int32 analysis",
+            "data": "synthetic (seeded gratings with global motion and moving rectangles, 1080p 8-bit 4:2:0)",
+            "config": bench_config(world, args.mode),
+            "form": {"headline": "learned: network hints, coarse motion, +-2 windows, full search +-32 fallback",
+                     "network_weights": learned["weights"], "compared_with": "plain (ragdoll's Balanced decisions)"},
+            "e2e": {"value": round(l_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
+                    "d2h_bytes_per_step": GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize,
+                    "bitstream_bytes_per_step": learned["bitstream_bytes_per_step"], "host_threads": enc_threads,
+                    "path": "rg_encoder_set_form(learned) + submit/collect: copy in, network and coarse-motion "
+                            "launches, persistent analysis launch, records out, CABAC on the host"},
+            "learned_over_plain": {"device": round(l_value / value, 4), "e2e": round(l_e2e / e2e, 4)},
+            "bd_rate_vs_plain_pct": learned.get("bd_rate_vs_plain_pct"),
+            "forms_frames_per_s": {"plain": round(value, 2), "learned": round(l_value, 2),
+                                   "learned_top1": round(frames_total / (learned["top1_ms"] / 1000), 2),
+                                   "fullsearch": round(frames_total / (learned["fullsearch_ms"] / 1000), 2)},
+            "bd_rates_pct": learned.get("bd_rates_pct"),
+            "rd": learned.get("rd"),
+            "target": "learned >= 3x plain frames/s at <= +2 % bits for equal PSNR (QP 22/26/30/34)",
+            "learned_breakdown_ms": {"step": round(learned["step_ms"], 3), "network": round(learned["cnn_ms"], 3),
+                                     "network_and_coarse_motion": round(learned["network_ms"], 3),
+                                     "analysis_with_hints": round(learned["analysis_ms"], 3)},
+            "roofline": {"bound": "hbm", "achieved": round(l_ana, 2) if l_ana else None, "peak": peak, "unit": "GB/s",
+                         "frac": round(l_ana / peak, 5) if l_ana else None, "traffic": None,
+                         "kernel": "pipeline_kernel (learned form)", "launch_ms": round(learned["analysis_ms"], 4),
+                         "bytes_per_launch": round(bytes_per_launch)},
+            "roofline_network": {"bound": "tensor", "achieved": round(cnn_tflops, 1), "peak": tpeak, "unit": "TFLOP/s",
+                                 "frac": round(cnn_tflops / tpeak, 4), "kernel": "cnn_infer_kernel",
+                                 "flop_per_launch": n_mb * FRAMES * CNN_FLOP_PER_MB,
+                                 "launch_ms": round(learned["cnn_ms"], 4)},
+            "plain": plain,
             "quality": {"what": "SSIM + 5-scale MS-SSIM of 120 1080p luma plane pairs, one rg_ssim_batch_device call",
                         "ms_device": round(q_ms, 3), "ms_call": round(q_wall_ms, 3),
                         "pairs_per_s": round(FRAMES / (q_ms / 1000), 1),
@@ -831,8 +1043,10 @@ def run_engine(args, rank, world, local):
                                      "bytes_per_call": round(q_bytes)}},
             "cpu_baseline": cpu,
             "parity": parity,
-            "clocks": clk,
-            "gpu_launches": launches,
+            "clocks": learned["clocks"],
+            # kernels of this library per timed learned step: the network, the coarse motion pass,
+            # the persistent analysis launch and the one-thread error hand-off
+            "gpu_launches": 4 * learned["steps"],
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -866,6 +1080,46 @@ def run_profile_case_cnn(args, local):
     net.check()
     print(json.dumps({"profile_case": "network hints of 8 1080p pictures", "ms_network": times[0],
                       "ms_network_and_coarse_motion": times[32]}), flush=True)
+
+
+def run_profile_case_learned(args, local):
+    """Launch list of the learned step (ncu, one metric): two learned steps of the default workload
+    (8 GOPs x 15 of 1080p) -- the network, the coarse motion pass and the persistent analysis
+    launch each time."""
+    import torch
+
+    from ragdoll_b200.engine import RG_FORM_LEARNED, RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_HIGH, Engine
+    from ragdoll_b200.learned import CandidateNet
+    torch.cuda.set_device(local)
+    gops = FRAMES // GOP
+    clip = make_clip(clip_seed(0), FRAMES)
+    cw, ch = (W + 1) // 2, (H + 1) // 2
+    fbytes = W * H + 2 * cw * ch
+    host = np.stack([np.concatenate([p.reshape(-1) for p in fr]) for fr in clip])
+    dev = torch.from_numpy(host).to(f"cuda:{local}")
+    base = dev.data_ptr()
+    net = CandidateNet.trained(local)
+    eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
+    eng.set_analysis_form(RG_FORM_LEARNED, 32)
+    eng.set_hint_net(net)
+    ptrs, kinds = [], []
+    for f in range(GOP):
+        for g in range(gops):
+            p = base + (g * GOP + f) * fbytes
+            ptrs += [p, p + W * H, p + W * H + cw * ch]
+            kinds.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+    times = []
+    stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.analyse_gops_device(ptrs, W, cw, kinds, GOP)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(round(e0.elapsed_time(e1), 3))
+    eng.sync()
+    eng.close()
+    print(json.dumps({"profile_case": "learned step, 1080p 8 GOPs x 15", "ms": times}), flush=True)
 
 
 def run_profile_case(args, local):
@@ -951,7 +1205,7 @@ def main():
     ap.add_argument("--mode", default="pipelined", choices=["pipelined", "wavefront"],
                     help="one persistent launch for all 15 pictures of the 8 GOPs, or one launch per anti-diagonal")
     ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
-                    choices=["wavefront", "pipelined", "cnn"],
+                    choices=["wavefront", "pipelined", "cnn", "learned"],
                     help="a small slice of the workload (the ncu capture case)")
     ap.add_argument("--profile-frames", type=int, default=3, choices=range(1, 9),
                     help="pictures per stream of the pipelined profile case")
@@ -967,6 +1221,9 @@ def main():
                     help="pipelined mode: macroblocks per work segment (0 = default)")
     args = ap.parse_args()
     rank, world, local = dist_env()
+    if args.profile_case == "learned":
+        run_profile_case_learned(args, local)
+        return
     if args.profile_case == "cnn":
         run_profile_case_cnn(args, local)
         return

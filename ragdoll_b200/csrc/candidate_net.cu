@@ -10,11 +10,12 @@
 //   intra 4x4 logits of block b = Wi f_b + bi (9)
 //
 // Inference (cnn_infer_kernel): BF16 implicit-GEMM convolutions on the 5th-generation tensor cores
-// (tcgen05.mma, accumulators in tensor memory), a strip of three macroblocks per step: every
-// activation map of the strip is stored with one row stride, so the 3x3 taps of a 128-position tile
-// are the same K-major operand shifted by whole rows of 16 bytes, and each tap is one descriptor of
-// the map -- no im2col copy. The epilogue adds the bias, applies the ReLU and stores the next
-// layer's BF16 operand; the heads run on the CUDA cores and write the hints.
+// (tcgen05.mma, accumulators in tensor memory), two CTAs per SM, each a strip of two macroblocks
+// per step: every activation map of the strip is stored with one row stride, so the 3x3 taps of a
+// 128-position tile are the same K-major operand shifted by whole rows of 16 bytes, and each tap is
+// one descriptor of the map -- no im2col copy. The epilogue adds the bias, applies the ReLU and
+// stores the next layer's BF16 operand over its input; the heads run on the CUDA cores and write
+// the hints. While one CTA's epilogue runs, the other's MMAs can.
 // Training (cnn_train_*): the same network in f32 on the CUDA cores -- forward, the losses, the
 // backward pass and Adam -- on per-macroblock crops.
 #include <cuda_bf16.h>
@@ -43,21 +44,25 @@ constexpr int kLogits = 4 + 2 + 16 * 9;  // per macroblock: partition, offset, i
 __device__ __forceinline__ float pix_norm(uint8_t v) { return ((float)v - 128.0f) * (1.0f / 64.0f); }
 
 // ---------------------------------------------------------------------------------------------
-// Inference on the tensor cores.
-constexpr int kStripMbs = 3;
-constexpr int kThreads = 256;  // 8 warps: two per scheduler; warps w and w + 4 share TMEM lanes 32 (w % 4)..
-constexpr int kRow = 16 * kStripMbs + 8;  // row stride (positions) of every map of a strip: 56
+// Inference on the tensor cores. Two CTAs per SM, each a strip of two macroblocks at a time; one
+// activation buffer per CTA holds every map of its strip in turn (the input in plane 0, then each
+// layer's output over its input: a layer's epilogue starts once all its MMAs have completed).
+constexpr int kStripMbs = 2;
+constexpr int kThreads = 256;  // 8 warps; warps w and w + 4 share TMEM lanes 32 (w % 4)..
+constexpr int kCtasPerSm = 2;
+constexpr int kRow = 16 * kStripMbs + 8;  // row stride (positions) of every map of a strip: 40
 constexpr int kTiles1 = (22 * kRow + 127) / 128, kTiles2 = (20 * kRow + 127) / 128, kTiles3 = (18 * kRow + 127) / 128;
-constexpr int kPos0 = ((kTiles1 * 128 + 2 * kRow + 2) + kThreads - 1) / kThreads * kThreads;  // input map positions
-constexpr int kPos1 = kTiles1 * 128, kPos2 = kTiles2 * 128;
-static_assert(kPos1 >= kTiles2 * 128 + 2 * kRow + 2 && kPos2 >= kTiles3 * 128 + 2 * kRow + 2, "tap reach");
-static_assert(kPos0 % kThreads == 0, "input map staged one position per thread and step");
-static_assert(kTiles1 * 32 <= 512, "accumulators of one layer fit the tensor memory");
-static_assert(kStripMbs * 4 * 16 <= kThreads && (kStripMbs * 4 * 16) % 32 == 0, "pooling: whole warps of half-warps");
-// shared memory (bytes): A1 (4 planes of 8 channels) | A2 or the input | B operands | the rest
-constexpr int kPlane1 = kPos1 * 16, kPlane2 = kPos2 * 16;
-constexpr int kOffA1 = 0, kOffA2 = kOffA1 + 4 * kPlane1, kSizeA2 = (4 * kPlane2 > kPos0 * 16 ? 4 * kPlane2 : kPos0 * 16);
-constexpr int kOffB = kOffA2 + kSizeA2;
+constexpr int kTap = 2 * kRow + 2;  // reach of the last tap
+constexpr int kPosBuf = ((kTiles1 * 128 + kTap > kTiles2 * 128 + kTap ? kTiles1 * 128 + kTap : kTiles2 * 128 + kTap) +
+                         kThreads - 1) / kThreads * kThreads;  // positions of the buffer
+static_assert(kPosBuf >= kTiles1 * 128 + kTap + 1 && kPosBuf >= kTiles3 * 128 + kTap,
+              "tap reach (conv1's last pair one position further) and outputs fit the buffer");
+static_assert(kPosBuf >= 24 * kRow, "the input map fits plane 0");
+static_assert(kTiles1 * 32 <= 256, "accumulators of one layer fit the CTA's 256 tensor-memory columns");
+static_assert(kStripMbs * 4 <= kThreads / 32, "pooling: a warp per (macroblock, 8-channel plane)");
+// shared memory (bytes): the buffer (4 planes of 8 channels) | B operands | the rest
+constexpr int kPlane = kPosBuf * 16;
+constexpr int kOffBuf = 0, kOffB = kOffBuf + 4 * kPlane;
 constexpr int kB1Mmas = 5, kBMmas = 18;  // conv1: taps paired; conv2/3: 9 taps x 2 channel halves
 constexpr int kOffB2 = kOffB + kB1Mmas * 1024, kOffB3 = kOffB2 + kBMmas * 1024, kOffMisc = kOffB3 + kBMmas * 1024;
 struct InferMisc {
@@ -69,8 +74,7 @@ struct InferMisc {
   int strip;
 };
 constexpr int kSmemInfer = kOffMisc + (int)sizeof(InferMisc);
-// conv1 tap pairs (second tap 9: a zero-weight pair with tap 8 one position on)
-__constant__ int8_t c_pair[kB1Mmas][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {8, 9}};
+static_assert(kSmemInfer <= 233472 / kCtasPerSm - 1024, "two CTAs' shared memory fit an SM");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 // Shared-memory matrix descriptor, K-major without swizzle: 8-row core matrices of 16-byte rows,
@@ -109,26 +113,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
   }
   return false;
 }
-// 64 consecutive columns of this thread's lane (two accumulator tiles).
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
-  uint32_t r[64];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
-      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
-      "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
-        "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
-        "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]),
-        "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
-        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
-}
+// 32 consecutive columns of this thread's lane (one accumulator tile).
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   uint32_t r[32];
   asm volatile(
@@ -178,12 +163,11 @@ __device__ __forceinline__ uint32_t topk_mask(const float* l, int n, int k, floa
   return m;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) cnn_infer_kernel(InferParams ip) {
   extern __shared__ __align__(1024) uint8_t smem[];
   InferMisc& ms = *reinterpret_cast<InferMisc*>(smem + kOffMisc);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  uint8_t* A1 = smem + kOffA1;
-  uint8_t* A2 = smem + kOffA2;  // the input map first, then conv2's output
+  uint8_t* buf = smem + kOffBuf;
   // B operands, biases and heads once per CTA
   for (int i = tid; i < (kB1Mmas + 2 * kBMmas) * 1024 / 16; i += kThreads)
     ((uint4*)(smem + kOffB))[i] = ((const uint4*)ip.bops)[i];
@@ -194,22 +178,22 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&ms.tmem)));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(&ms.tmem)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = ms.tmem;
-  const uint32_t sA1 = smem_u32(A1), sA2 = smem_u32(A2), sB1 = smem_u32(smem + kOffB), sB2 = smem_u32(smem + kOffB2),
+  const uint32_t sBuf = smem_u32(buf), sB1 = smem_u32(smem + kOffB), sB2 = smem_u32(smem + kOffB2),
                  sB3 = smem_u32(smem + kOffB3);
   uint32_t phase = 0;
   bool ok = true;
   const int total = ip.n_jobs * ip.mb_h * ip.strips_per_row;
-  // The input map of a strip: position r * kRow + c is sample (x0 - 4 + c, y0 - 4 + r), clamped
-  // to the picture; 16 bytes each, the two channels and six zero channels. A strip's bytes are
-  // loaded into registers while the previous strip's MMAs run, and stored once its conv3 is done.
-  constexpr int kPer = kPos0 / kThreads;
+  // The input map of a strip (plane 0 of the buffer): position r * kRow + c is sample (x0 - 4 + c,
+  // y0 - 4 + r), clamped to the picture; 16 bytes each, the two channels and six zero channels. A
+  // strip's bytes are loaded into registers while the previous strip's MMAs run.
+  constexpr int kPer = kPosBuf / kThreads;
   uint8_t ca[kPer], pa[kPer];
   auto load_input = [&](int st) {
     const int job = st / (ip.mb_h * ip.strips_per_row), rem = st % (ip.mb_h * ip.strips_per_row);
@@ -229,18 +213,10 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
   __syncthreads();
   int strip = ms.strip;
   if (strip < total) load_input(strip);
-  // shared-memory descriptors: conv1's five tap pairs, the two channel halves of conv2's and
-  // conv3's operands, the B operands; a tile / tap adds its offset in 16-byte units
-  uint64_t a1d[kB1Mmas];
-#pragma unroll
-  for (int k = 0; k < kB1Mmas; k++) {
-    const int ta = c_pair[k][0], tb = c_pair[k][1];
-    const int oa = (ta / 3) * kRow + ta % 3, ob = tb < 9 ? (tb / 3) * kRow + tb % 3 : oa + 1;
-    a1d[k] = umma_desc(sA2 + (uint32_t)(oa * 16), (uint32_t)((ob - oa) * 16), 128);
-  }
+  // shared-memory descriptors: conv1's five tap pairs on plane 0, the two channel halves of the
+  // buffer for conv2 and conv3, the B operands; a tile / tap adds its offset in 16-byte units
+  const uint64_t bufd0 = umma_desc(sBuf, kPlane, 128), bufd1 = umma_desc(sBuf + 2 * kPlane, kPlane, 128);
   const uint64_t b1d = umma_desc(sB1, 512, 128), b2d = umma_desc(sB2, 512, 128), b3d = umma_desc(sB3, 512, 128);
-  const uint64_t a2d0 = umma_desc(sA1, kPlane1, 128), a2d1 = umma_desc(sA1 + 2 * kPlane1, kPlane1, 128);
-  const uint64_t a3d0 = umma_desc(sA2, kPlane2, 128), a3d1 = umma_desc(sA2 + 2 * kPlane2, kPlane2, 128);
   while (strip < total && ok) {
     const int job = strip / (ip.mb_h * ip.strips_per_row), rem = strip % (ip.mb_h * ip.strips_per_row);
     const int mby = rem / ip.strips_per_row, mbx0 = (rem % ip.strips_per_row) * kStripMbs;
@@ -248,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
 #pragma unroll
     for (int k = 0; k < kPer; k++) {
       __nv_bfloat162 two = __floats2bfloat162_rn(pix_norm(ca[k]), pix_norm(pa[k]));
-      ((uint4*)A2)[tid + kThreads * k] = make_uint4(*(uint32_t*)&two, 0u, 0u, 0u);
+      ((uint4*)buf)[tid + kThreads * k] = make_uint4(*(uint32_t*)&two, 0u, 0u, 0u);
     }
     if (tid == 0) ms.strip = atomicAdd(ip.counter, 1);  // read after the first layer's barrier
     int next = total;
@@ -263,10 +239,16 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
 #pragma unroll 1
           for (int t = 0; t < tiles; t++)
 #pragma unroll
-            for (int k = 0; k < kB1Mmas; k++)
-              umma_bf16(tmem + (uint32_t)(t * 32), a1d[k] + (uint64_t)(t * 128), b1d + (uint64_t)(k * 64), k > 0);
+            for (int k = 0; k < kB1Mmas; k++) {
+              // taps 2k and 2k + 1 (tap 9: a zero-weight partner one position on) as the two
+              // 8-element halves of K, LBO their distance
+              const int ta = 2 * k, tb = 2 * k + 1;
+              const int oa = (ta / 3) * kRow + ta % 3, ob = tb < 9 ? (tb / 3) * kRow + tb % 3 : oa + 1;
+              const uint64_t a = umma_desc(sBuf + (uint32_t)((t * 128 + oa) * 16), (uint32_t)((ob - oa) * 16), 128);
+              umma_bf16(tmem + (uint32_t)(t * 32), a, b1d + (uint64_t)(k * 64), k > 0);
+            }
         } else {
-          const uint64_t ad0 = layer == 1 ? a2d0 : a3d0, ad1 = layer == 1 ? a2d1 : a3d1, bd = layer == 1 ? b2d : b3d;
+          const uint64_t bd = layer == 1 ? b2d : b3d;
 #pragma unroll 1
           for (int t = 0; t < tiles; t++) {
             const uint32_t d = tmem + (uint32_t)(t * 32);
@@ -275,7 +257,7 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
 #pragma unroll
               for (int h = 0; h < 2; h++) {
                 const uint64_t off = (uint64_t)(t * 128 + (tap / 3) * kRow + tap % 3);
-                umma_bf16(d, (h ? ad1 : ad0) + off, bd + (uint64_t)((tap * 2 + h) * 64), tap > 0 || h > 0);
+                umma_bf16(d, (h ? bufd1 : bufd0) + off, bd + (uint64_t)((tap * 2 + h) * 64), tap > 0 || h > 0);
               }
           }
         }
@@ -291,44 +273,36 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
       phase ^= 1;
       fence_after_sync();
       if (!ok) break;
-      // epilogue: warp w reads rows 32 (w % 4) .. + 31 of the tile pairs 2 (w / 4), + 4, ..; bias,
-      // ReLU, BF16 -> next map
-      // conv1 -> A1; conv2 -> A2; conv3 -> A1 again (dead once conv2's MMAs completed), for the pooling
-      uint8_t* dst = layer == 1 ? A2 : A1;
-      const uint32_t dplane = layer == 1 ? kPlane2 : kPlane1;
+      // epilogue over the layer's input (all its MMAs have completed): warp w reads rows 32 (w % 4)
+      // .. + 31 of tiles w / 4, + 2, ..; bias, ReLU, BF16 into the buffer's four planes
       const int wl = warp & 3;
-      for (int t = 2 * (warp >> 2); t < tiles; t += 4) {  // two tiles (64 accumulator columns) per load
-        float v[64];
-        if (t + 1 < tiles) tmem_ld64(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)(t * 32), v);
-        else tmem_ld32(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)(t * 32), v);
+      for (int t = warp >> 2; t < tiles; t += 2) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)(t * 32), v);
+        const int p = t * 128 + wl * 32 + lane;
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          if (t + h >= tiles) break;
-          const int p = (t + h) * 128 + wl * 32 + lane;
+        for (int q = 0; q < 4; q++) {
+          uint32_t w[4];
 #pragma unroll
-          for (int q = 0; q < 4; q++) {
-            uint32_t w[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-              float a = fmaxf(v[32 * h + 8 * q + 2 * k] + ms.bias[layer][8 * q + 2 * k], 0.0f);
-              float b = fmaxf(v[32 * h + 8 * q + 2 * k + 1] + ms.bias[layer][8 * q + 2 * k + 1], 0.0f);
-              __nv_bfloat162 two = __floats2bfloat162_rn(a, b);
-              w[k] = *(uint32_t*)&two;
-            }
-            *(uint4*)(dst + q * dplane + p * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+          for (int k = 0; k < 4; k++) {
+            const float a = fmaxf(v[8 * q + 2 * k] + ms.bias[layer][8 * q + 2 * k], 0.0f);
+            const float b = fmaxf(v[8 * q + 2 * k + 1] + ms.bias[layer][8 * q + 2 * k + 1], 0.0f);
+            __nv_bfloat162 two = __floats2bfloat162_rn(a, b);
+            w[k] = *(uint32_t*)&two;
           }
+          *(uint4*)(buf + q * kPlane + p * 16) = make_uint4(w[0], w[1], w[2], w[3]);
         }
       }
     }
     if (!ok) break;
     __syncthreads();  // conv3's map complete
-    // pooling of the conv3 map (in A1; map column 16 j + i is sample x 16 (mbx0 + j) - 1 + i):
-    // half-warp h < 4 kStripMbs takes macroblock j = h / 4 and 8-channel plane q = h % 4; its lane l
-    // sums map row l + 1 (16-byte reads), lanes 0 and 15 also the border rows 0 and 17; the block
-    // sums are reduced over the block row's four lanes, the 18 x 18 sum over all sixteen
-    if (tid < kStripMbs * 4 * 16) {
-      const int j = tid >> 6, q = (tid >> 4) & 3, l = tid & 15;
-      const uint8_t* base = A1 + q * kPlane1 + (16 * j) * 16;
+    // pooling of the conv3 map (map column 16 j + i is sample x 16 (mbx0 + j) - 1 + i): warp w
+    // takes macroblock j = w / 4 and 8-channel plane q = w % 4; lane l < 16 sums map column l + 1
+    // down the 18 rows (16-byte reads), lanes 16 and 17 the border columns 0 and 17; block sums
+    // over the four lanes of a block column, the 18 x 18 sum over the warp
+    if (warp < kStripMbs * 4) {
+      const int j = warp >> 2, q = warp & 3;
+      const int col = lane < 16 ? lane + 1 : (lane == 16 ? 0 : 17);
       float tot[8], blk[4][8];
 #pragma unroll
       for (int k = 0; k < 8; k++) {
@@ -336,22 +310,20 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
 #pragma unroll
         for (int b = 0; b < 4; b++) blk[b][k] = 0.0f;
       }
-      for (int pass = 0; pass < 2; pass++) {
-        if (pass == 1 && l != 0 && l != 15) break;
-        const int r = pass == 0 ? l + 1 : (l == 0 ? 0 : 17);
-        const uint8_t* row = base + r * kRow * 16;
+      if (lane < 18) {
+        const uint8_t* colp = buf + q * kPlane + (16 * j + col) * 16;
 #pragma unroll
-        for (int i = 0; i < 18; i++) {
-          const uint4 v = *(const uint4*)(row + i * 16);
+        for (int r = 0; r < 18; r++) {
+          const uint4 v = *(const uint4*)(colp + r * kRow * 16);
           const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const float2 f = __bfloat1622float2(*(const __nv_bfloat162*)&w[k]);
             tot[2 * k] += f.x;
             tot[2 * k + 1] += f.y;
-            if (pass == 0 && i >= 1 && i <= 16) {
-              blk[(i - 1) >> 2][2 * k] += f.x;
-              blk[(i - 1) >> 2][2 * k + 1] += f.y;
+            if (r >= 1 && r <= 16 && lane < 16) {
+              blk[(r - 1) >> 2][2 * k] += f.x;
+              blk[(r - 1) >> 2][2 * k + 1] += f.y;
             }
           }
         }
@@ -364,20 +336,20 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
           blk[b][k] += __shfl_xor_sync(0xffffffffu, blk[b][k], 2);
         }
 #pragma unroll
-        for (int o = 1; o < 16; o <<= 1) tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], o);
+        for (int o = 1; o < 32; o <<= 1) tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], o);
       }
-      if ((l & 3) == 0)
+      if (lane < 16 && (lane & 3) == 0)
 #pragma unroll
         for (int b = 0; b < 4; b++)
 #pragma unroll
-          for (int k = 0; k < 8; k++) ms.pool[j][1 + (l >> 2) * 4 + b][8 * q + k] = blk[b][k] * (1.0f / 16.0f);
-      if (l == 0)
+          for (int k = 0; k < 8; k++) ms.pool[j][1 + b * 4 + (lane >> 2)][8 * q + k] = blk[b][k] * (1.0f / 16.0f);
+      if (lane == 0)
 #pragma unroll
         for (int k = 0; k < 8; k++) ms.pool[j][0][8 * q + k] = tot[k] * (1.0f / 324.0f);
     }
     __syncthreads();
-    // heads and hints: threads 0..47 the intra 4x4 heads of (macroblock tid / 16, block tid % 16),
-    // threads 48..50 the partition and offset heads of macroblock tid - 48
+    // heads and hints: threads 0 .. 16 kStripMbs - 1 the intra 4x4 heads of (macroblock tid / 16,
+    // block tid % 16), the next kStripMbs threads the partition and offset heads of their macroblock
     if (tid < 16 * kStripMbs + kStripMbs) {
       const bool blockhead = tid < 16 * kStripMbs;
       const int j = blockhead ? tid / 16 : tid - 16 * kStripMbs, mbx = mbx0 + j;
@@ -430,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, 1) cnn_infer_kernel(InferParams ip) 
   }
   fence_before_sync();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1061,10 +1033,12 @@ int rg_net_predict_hints(rg_net* net, const uint8_t* const* dev_cur, const uint8
   ip.part_margin = net->part_margin;
   ip.i4_margin = net->i4_margin;
   NCK(cudaFuncSetAttribute(cnn_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemInfer));
+  NCK(cudaFuncSetAttribute(cnn_infer_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
   const int strips = n_pictures * ip.mb_h * ip.strips_per_row;
-  cnn_infer_kernel<<<sms < strips ? sms : strips, kThreads, kSmemInfer, st>>>(ip);
+  const int ctas = kCtasPerSm * sms < strips ? kCtasPerSm * sms : strips;
+  cnn_infer_kernel<<<ctas, kThreads, kSmemInfer, st>>>(ip);
   NCK(cudaGetLastError());
   if (net->coarse_range > 0) {
     CoarseParams cp{net->jobs, n_pictures, width, height, (int)stride, ip.mb_w, ip.mb_h, net->coarse_range / 2};
