@@ -1146,6 +1146,12 @@ def run_profile_case(args, local):
         eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=nf)
         eng.set_pipeline_tuning(lag=args.lag, seg=args.seg, grid=args.grid, deblock_sms=args.deblock_sms,
                                 intra_sms=args.intra_sms)
+        if args.profile_form == "learned":   # the learned form, its network run by each launch
+            from ragdoll_b200.engine import RG_FORM_LEARNED
+            from ragdoll_b200.learned import CandidateNet
+            net = CandidateNet.trained(local)
+            eng.set_analysis_form(RG_FORM_LEARNED, 32)
+            eng.set_hint_net(net)
         stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
         ptrs, kinds = [], []
         for f in range(nf):
@@ -1163,7 +1169,8 @@ def run_profile_case(args, local):
             e1.synchronize()
             eng.sync()
             times.append(e0.elapsed_time(e1))
-        print(json.dumps({"profile_case": f"1080p High QP26, 8 streams x {nf} pictures (IDR, then P), one pipelined launch",
+        print(json.dumps({"profile_case": f"1080p High QP26, 8 streams x {nf} pictures (IDR, then P), one pipelined "
+                                          f"launch, {args.profile_form} form",
                           "launch_ms": [round(t, 3) for t in times]}), flush=True)
         eng.close()
         return
@@ -1207,6 +1214,8 @@ def main():
     ap.add_argument("--profile-case", nargs="?", const="wavefront", default=None,
                     choices=["wavefront", "pipelined", "cnn", "learned"],
                     help="a small slice of the workload (the ncu capture case)")
+    ap.add_argument("--profile-form", default="plain", choices=["plain", "learned"],
+                    help="analysis form of --profile-case pipelined")
     ap.add_argument("--profile-frames", type=int, default=3, choices=range(1, 9),
                     help="pictures per stream of the pipelined profile case")
     ap.add_argument("--grid", type=int, default=0,
