@@ -69,7 +69,6 @@ struct InferMisc {
   float bias[3][C];
   float head[kParams - kWp];   // Wp bp Wm bm Wi bi
   float pool[kStripMbs][17][C];  // per macroblock: the 18 x 18 mean, then the 16 block means
-  float logit[kStripMbs][kLogits];
   uint64_t mbar;
   uint32_t tmem;
   int strip;
@@ -150,23 +149,15 @@ struct InferParams {
 
 // The candidates of n logits as a bit mask: the best, then the next ones in logit order (the lower
 // index on ties) up to k in all, each only while its logit is at least the best's minus `margin`.
-template <int N>
-__device__ __forceinline__ uint32_t topk_mask(const float (&l)[N], int k, float margin) {
+__device__ __forceinline__ uint32_t topk_mask(const float* l, int n, int k, float margin) {
   uint32_t m = 0;
   float top = 0.0f;
-#pragma unroll
-  for (int r = 0; r < N; r++) {
-    if (r >= k) break;
+  for (int r = 0; r < k; r++) {
     int best = -1;
-    float bv = 0.0f;
-#pragma unroll
-    for (int i = 0; i < N; i++)
-      if (!((m >> i) & 1) && (best < 0 || l[i] > bv)) {
-        best = i;
-        bv = l[i];
-      }
-    if (r == 0) top = bv;
-    else if (bv < top - margin) break;
+    for (int i = 0; i < n; i++)
+      if (!((m >> i) & 1) && (best < 0 || l[i] > l[best])) best = i;
+    if (r == 0) top = l[best];
+    else if (l[best] < top - margin) break;
     m |= 1u << best;
   }
   return m;
@@ -357,54 +348,53 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) cnn_infer_kernel(InferPa
         for (int k = 0; k < 8; k++) ms.pool[j][0][8 * q + k] = tot[k] * (1.0f / 324.0f);
     }
     __syncthreads();
-    // heads: every thread one logit (a 32-term dot product) of the strip's kStripMbs x 150 --
-    // partition (4), offset (2), then the 9 intra 4x4 modes of each 4x4 block in raster order
-    for (int i = tid; i < kStripMbs * kLogits; i += kThreads) {
-      const int j = i / kLogits, o = i - j * kLogits;
-      const float* H = ms.head;
-      const float* w;
-      const float* f;
-      float acc;
-      if (o < 4) { w = H + o * C; f = ms.pool[j][0]; acc = H[kBp - kWp + o]; }
-      else if (o < 6) { w = H + kWm - kWp + (o - 4) * C; f = ms.pool[j][0]; acc = H[kBm - kWp + o - 4]; }
-      else {
-        const int b = (o - 6) / 9, mode = (o - 6) - 9 * b;
-        w = H + kWi - kWp + mode * C;
-        f = ms.pool[j][1 + b];
-        acc = H[kBi - kWp + mode];
-      }
-#pragma unroll
-      for (int c = 0; c < C; c++) acc = fmaf(w[c], f[c], acc);
-      ms.logit[j][o] = acc;
-      if (jb.logits && mbx0 + j < ip.mb_w) jb.logits[(size_t)(mby * ip.mb_w + mbx0 + j) * kLogits + o] = acc;
-    }
-    __syncthreads();
-    // hints: threads 0 .. 16 kStripMbs - 1 the intra 4x4 blocks (macroblock tid / 16, block tid % 16),
-    // the next kStripMbs threads the partition types and offsets of their macroblock
-    if (tid < 17 * kStripMbs) {
+    // heads and hints: threads 0 .. 16 kStripMbs - 1 the intra 4x4 heads of (macroblock tid / 16,
+    // block tid % 16), the next kStripMbs threads the partition and offset heads of their macroblock
+    if (tid < 16 * kStripMbs + kStripMbs) {
       const bool blockhead = tid < 16 * kStripMbs;
       const int j = blockhead ? tid / 16 : tid - 16 * kStripMbs, mbx = mbx0 + j;
       if (mbx < ip.mb_w) {
-        rg_mb_hint& hh = jb.hints[mby * ip.mb_w + mbx];
+        const float* H = ms.head;
+        const int m = mby * ip.mb_w + mbx;
+        float* lg = jb.logits ? jb.logits + (size_t)m * kLogits : nullptr;
         if (blockhead) {
           const int b = tid % 16;
+          const float* f = ms.pool[j][1 + b];
           float li[9];
-#pragma unroll
-          for (int o = 0; o < 9; o++) li[o] = ms.logit[j][6 + 9 * b + o];
+          for (int o = 0; o < 9; o++) {
+            float s = H[kBi - kWp + o];
+            for (int c = 0; c < C; c++) s += H[kWi - kWp + o * C + c] * f[c];
+            li[o] = s;
+          }
           // 4x4 block b in raster order; the hint holds decoding order
           const int bx = b & 3, by = b >> 2;
           const int dec = ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1);
-          hh.i4_mask[dec] = (uint16_t)topk_mask(li, ip.i4_k, ip.i4_margin);
+          jb.hints[m].i4_mask[dec] = (uint16_t)topk_mask(li, 9, ip.i4_k, ip.i4_margin);
+          if (lg)
+            for (int o = 0; o < 9; o++) lg[6 + b * 9 + o] = li[o];
         } else {
-          float lp[4];
-#pragma unroll
-          for (int o = 0; o < 4; o++) lp[o] = ms.logit[j][o];
-          hh.part_mask = (uint8_t)topk_mask(lp, ip.part_k, ip.part_margin);
+          const float* g = ms.pool[j][0];
+          float lp[4], lm[2];
+          for (int o = 0; o < 4; o++) {
+            float s = H[kBp - kWp + o];
+            for (int c = 0; c < C; c++) s += H[o * C + c] * g[c];
+            lp[o] = s;
+          }
+          for (int o = 0; o < 2; o++) {
+            float s = H[kBm - kWp + o];
+            for (int c = 0; c < C; c++) s += H[kWm - kWp + o * C + c] * g[c];
+            lm[o] = s;
+          }
+          rg_mb_hint& hh = jb.hints[m];
+          hh.part_mask = (uint8_t)topk_mask(lp, 4, ip.part_k, ip.part_margin);
           hh.flags = 0;  // the coarse motion pass, when on, follows
           hh.mv_coarse[0] = hh.mv_coarse[1] = 0;
-#pragma unroll
-          for (int o = 0; o < 2; o++)
-            hh.mv_off[o] = (int8_t)max(-127, min(127, __float2int_rn(16.0f * ms.logit[j][4 + o])));
+          for (int o = 0; o < 2; o++) hh.mv_off[o] = (int8_t)max(-127, min(127, __float2int_rn(16.0f * lm[o])));
+          if (lg) {
+            for (int o = 0; o < 4; o++) lg[o] = lp[o];
+            lg[4] = lm[0];
+            lg[5] = lm[1];
+          }
         }
       }
     }
@@ -416,17 +406,17 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) cnn_infer_kernel(InferPa
 }
 
 // ---------------------------------------------------------------------------------------------
-// Coarse motion (rg_net_set_coarse_range): a block per eight macroblocks of a row, a warp per
-// macroblock, the decimated window of all eight staged once. The decimated picture's sample (x, y)
-// is the rounded mean of the four samples (2x + i, 2y + j), coordinates clamped to the picture; the
-// macroblock's 8 x 8 decimated block is compared with the decimated previous picture at every
-// displacement of +-r (SAD), the least (SAD, |dx| + |dy|, raster index) wins.
+// Coarse motion (rg_net_set_coarse_range): a warp per macroblock, 8 per block. The decimated
+// picture's sample (x, y) is the rounded mean of the four samples (2x + i, 2y + j), coordinates
+// clamped to the picture; the macroblock's 8 x 8 decimated block is compared with the decimated
+// previous picture at every displacement of +-r (SAD), the least (SAD, |dx| + |dy|, raster index)
+// wins.
 constexpr int kCoarseMaxR = 32;
+constexpr int kCoarseRow = (8 + 2 * kCoarseMaxR + 3) / 4 * 4 + 4;  // window row stride (bytes)
 constexpr int kCoarseWarps = 8;
-constexpr int kCoarseRow = 8 * kCoarseWarps + 2 * kCoarseMaxR + 4;  // window row stride (bytes)
 struct CoarseParams {
   const InferJob* jobs;
-  int n_jobs, width, height, stride, mb_w, mb_h, r, groups;  // groups: blocks per macroblock row
+  int n_jobs, width, height, stride, mb_w, mb_h, r;
 };
 __device__ __forceinline__ uint32_t dec_sample(const uint8_t* p, int stride, int w, int h, int x, int y) {
   const int x0 = min(max(2 * x, 0), w - 1), x1 = min(max(2 * x + 1, 0), w - 1);
@@ -441,30 +431,29 @@ __device__ __forceinline__ uint32_t lds4_unaligned(const uint8_t* p) {
   return __funnelshift_r(b[0], b[1], (uint32_t)(a & 3) * 8u);
 }
 __global__ void __launch_bounds__(32 * kCoarseWarps) coarse_motion_kernel(CoarseParams cp) {
-  __shared__ __align__(16) uint8_t win[(8 + 2 * kCoarseMaxR) * kCoarseRow];
+  __shared__ __align__(16) uint8_t win[kCoarseWarps][(8 + 2 * kCoarseMaxR) * kCoarseRow];
   __shared__ __align__(16) uint8_t blk[kCoarseWarps][64];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int per_pic = cp.mb_h * cp.groups;
-  const int job = blockIdx.x / per_pic, rem = blockIdx.x % per_pic;
-  const int mby = rem / cp.groups, mbx0 = (rem % cp.groups) * kCoarseWarps;
+  const int per_pic = cp.mb_w * cp.mb_h;
+  const long task = (long)blockIdx.x * kCoarseWarps + warp;
+  if (task >= (long)cp.n_jobs * per_pic) return;
+  const int job = (int)(task / per_pic), m = (int)(task % per_pic);
   const InferJob jb = cp.jobs[job];
-  if (jb.cur == jb.prev) return;  // an IDR picture (uniform over the block): no previous picture
-  const int R = cp.r, rows = 8 + 2 * R, cols = 8 * kCoarseWarps + 2 * R;
-  const int bx0 = 8 * mbx0, by = 8 * mby;  // decimated origin of the block's first macroblock
-  for (int i = threadIdx.x; i < rows * cols; i += 32 * kCoarseWarps) {
-    const int y = i / cols, x = i - y * cols;
-    win[y * kCoarseRow + x] = (uint8_t)dec_sample(jb.prev, cp.stride, cp.width, cp.height, bx0 - R + x, by - R + y);
+  if (jb.cur == jb.prev) return;  // an IDR picture: no previous picture
+  const int mbx = m % cp.mb_w, mby = m / cp.mb_w, R = cp.r, side = 8 + 2 * R;
+  const int bx = 8 * mbx, by = 8 * mby;  // the block's decimated origin
+  uint8_t* w = win[warp];
+  for (int i = lane; i < side * side; i += 32) {
+    const int y = i / side, x = i - y * side;
+    w[y * kCoarseRow + x] = (uint8_t)dec_sample(jb.prev, cp.stride, cp.width, cp.height, bx - R + x, by - R + y);
   }
-  const int mbx = mbx0 + warp;
   for (int i = lane; i < 64; i += 32)
-    blk[warp][i] = (uint8_t)dec_sample(jb.cur, cp.stride, cp.width, cp.height, 8 * mbx + (i & 7), by + (i >> 3));
-  __syncthreads();
-  if (mbx >= cp.mb_w) return;
+    blk[warp][i] = (uint8_t)dec_sample(jb.cur, cp.stride, cp.width, cp.height, bx + (i & 7), by + (i >> 3));
+  __syncwarp();
   uint32_t b[16];
 #pragma unroll
   for (int k = 0; k < 16; k++) b[k] = ((const uint32_t*)blk[warp])[k];
   const int n = (2 * R + 1) * (2 * R + 1);
-  const uint8_t* w = win + 8 * warp;
   uint64_t best = ~0ull;
   for (int p = lane; p < n; p += 32) {
     const int dyi = p / (2 * R + 1), dxi = p - dyi * (2 * R + 1);
@@ -481,7 +470,7 @@ __global__ void __launch_bounds__(32 * kCoarseWarps) coarse_motion_kernel(Coarse
   for (int o = 16; o > 0; o >>= 1) best = min(best, (uint64_t)__shfl_xor_sync(0xffffffffu, (unsigned long long)best, o));
   if (lane == 0) {
     const int p = (int)(best & 0xffffu), dyi = p / (2 * R + 1), dxi = p - dyi * (2 * R + 1);
-    rg_mb_hint& h = jb.hints[mby * cp.mb_w + mbx];
+    rg_mb_hint& h = jb.hints[m];
     h.mv_coarse[0] = (int16_t)(8 * (dxi - R));
     h.mv_coarse[1] = (int16_t)(8 * (dyi - R));
     h.flags |= 1;
@@ -1052,9 +1041,9 @@ int rg_net_predict_hints(rg_net* net, const uint8_t* const* dev_cur, const uint8
   cnn_infer_kernel<<<ctas, kThreads, kSmemInfer, st>>>(ip);
   NCK(cudaGetLastError());
   if (net->coarse_range > 0) {
-    const int groups = (ip.mb_w + kCoarseWarps - 1) / kCoarseWarps;
-    CoarseParams cp{net->jobs, n_pictures, width, height, (int)stride, ip.mb_w, ip.mb_h, net->coarse_range / 2, groups};
-    coarse_motion_kernel<<<(unsigned)(n_pictures * ip.mb_h * groups), 32 * kCoarseWarps, 0, st>>>(cp);
+    CoarseParams cp{net->jobs, n_pictures, width, height, (int)stride, ip.mb_w, ip.mb_h, net->coarse_range / 2};
+    const long tasks = (long)n_pictures * ip.mb_w * ip.mb_h;
+    coarse_motion_kernel<<<(unsigned)((tasks + kCoarseWarps - 1) / kCoarseWarps), 32 * kCoarseWarps, 0, st>>>(cp);
     NCK(cudaGetLastError());
   }
   return RG_OK;

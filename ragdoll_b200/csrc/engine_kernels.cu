@@ -42,17 +42,6 @@ __constant__ uint8_t c_beta[52];
 __constant__ uint8_t c_tc0[52][3];
 
 // ---------------------------------------------------------------------------------------------
-// Geometry of a half-sample window with kE more integer positions on every side: kE = 0 serves one
-// integer vector (its 16x16 block at quarter-sample offsets -3..3), kE = 2 every vector of a +-2
-// integer window around the vector it is built for.
-template <int kE>
-struct WinGeom {
-  static constexpr int kRows = 23 + 2 * kE;    // integer rows staged (from -2)
-  static constexpr int kStride = 24 + 2 * kE;  // their stride (bytes, a multiple of 4)
-  static constexpr int kWords = kStride / 4;
-  static constexpr int kP = 18 + 2 * kE;       // half-sample planes: kP x kP
-  static constexpr int kPs = 20 + 2 * kE;      // their row stride
-};
 // Shared memory of one macroblock warp.
 struct __align__(16) Smem {
   uint8_t src_y[256];
@@ -62,16 +51,15 @@ struct __align__(16) Smem {
   uint8_t pred_u[64];
   uint8_t pred_v[64];
   uint8_t tmp_y[256];       // plane prediction / I4x4 reconstruction
-  // integer samples of a half-sample window (rows -2.., cols -2..), sized for the widest geometry
-  uint8_t win[WinGeom<2>::kRows * WinGeom<2>::kStride];
+  uint8_t win[23 * 24];     // integer samples of a half-sample window (rows -2.., cols -2..)
   // The half-sample planes live until the sub-pel search ends; the 8x8 transform's intermediates
   // are needed only after it (the residual), so they share the space.
   union {
     struct {
-      uint8_t hph[WinGeom<2>::kP * WinGeom<2>::kPs];  // b samples (horizontal half)
-      uint8_t hpv[WinGeom<2>::kP * WinGeom<2>::kPs];  // h samples (vertical half)
-      uint8_t hpj[WinGeom<2>::kP * WinGeom<2>::kPs];  // j samples (centre)
-      int16_t hr[WinGeom<2>::kRows * WinGeom<2>::kP];  // unrounded horizontal 6-tap sums
+      uint8_t hph[18 * 20];  // b samples (horizontal half)
+      uint8_t hpv[18 * 20];  // h samples (vertical half)
+      uint8_t hpj[18 * 20];  // j samples (centre)
+      int16_t hr[23 * 18];   // unrounded horizontal 6-tap sums
     };
     int32_t t8[256];         // 8x8 transform intermediates
   };
@@ -254,17 +242,14 @@ __device__ __forceinline__ int inv4_pass(int v, int step, int i) {
 // ---------------------------------------------------------------------------------------------
 // Half-sample window (h264_enc.rs:747 hpel_window, :803 hpel_window_centre): integer origin
 // (ox, oy); plane coordinate (r, c) is the sample at (ox + c, oy + r).
-template <int kE = 0>
 __device__ __noinline__ void stage_window(const uint8_t* ref, int stride, int ox, int oy, Smem& sm) {
-  using G = WinGeom<kE>;
-  constexpr int kItems = G::kRows * G::kWords, kPer = (kItems + 31) / 32;
   int lane = lane_id();
-  // kRows rows x kWords words, all of this lane's loads issued before the first use
-  uint32_t lo[kPer], hi[kPer], sh[kPer];
+  // 23 rows x 6 words: five words per lane, all loads issued before the first use
+  uint32_t lo[5], hi[5], sh[5];
 #pragma unroll
-  for (int r = 0; r < kPer; r++) {
-    int q = min(lane + 32 * r, kItems - 1);
-    int k = q / G::kWords, w = q - G::kWords * k;
+  for (int r = 0; r < 5; r++) {
+    int q = min(lane + 32 * r, 23 * 6 - 1);
+    int k = q / 6, w = q - 6 * (q / 6);
     uintptr_t a = (uintptr_t)(ref + (long)(oy - 2 + k) * stride + (ox - 2) + 4 * w);
     const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
     sh[r] = (uint32_t)(a & 3) * 8u;
@@ -272,41 +257,38 @@ __device__ __noinline__ void stage_window(const uint8_t* ref, int stride, int ox
     hi[r] = b[1];
   }
 #pragma unroll
-  for (int r = 0; r < kPer; r++) {
+  for (int r = 0; r < 5; r++) {
     int q = lane + 32 * r;
-    if (q < kItems) {
-      int k = q / G::kWords, w = q - G::kWords * k;
-      *(uint32_t*)&sm.win[k * G::kStride + 4 * w] = __funnelshift_r(lo[r], hi[r], sh[r]);
+    if (q < 23 * 6) {
+      int k = q / 6, w = q - 6 * (q / 6);
+      *(uint32_t*)&sm.win[k * 24 + 4 * w] = __funnelshift_r(lo[r], hi[r], sh[r]);
     }
   }
   __syncwarp();
 }
 // need: bit 0 b plane (h), bit 1 h plane (v), bit 2 j plane (c)
-template <int kE = 0>
 __device__ __noinline__ void build_hpel(Smem& sm, int need) {
-  using G = WinGeom<kE>;
-  constexpr int S = G::kStride, P = G::kP;
   int lane = lane_id();
   if (need & 5) {
-    for (int i = lane; i < G::kRows * P; i += 32) {
-      int k = i / P, c = i - k * P;
-      const uint8_t* w = &sm.win[k * S + c];
+    for (int i = lane; i < 23 * 18; i += 32) {
+      int k = i / 18, c = i - k * 18;
+      const uint8_t* w = &sm.win[k * 24 + c];
       sm.hr[i] = (int16_t)(w[0] - 5 * w[1] + 20 * w[2] + 20 * w[3] - 5 * w[4] + w[5]);
     }
   }
   __syncwarp();
-  for (int i = lane; i < P * P; i += 32) {
-    int r = i / P, c = i - r * P;
-    if (need & 1) sm.hph[r * G::kPs + c] = (uint8_t)clip255((sm.hr[(r + 2) * P + c] + 16) >> 5);
+  for (int i = lane; i < 18 * 18; i += 32) {
+    int r = i / 18, c = i - r * 18;
+    if (need & 1) sm.hph[r * 20 + c] = (uint8_t)clip255((sm.hr[(r + 2) * 18 + c] + 16) >> 5);
     if (need & 2) {
-      const uint8_t* w = &sm.win[r * S + c + 2];
-      int v = w[0] - 5 * w[S] + 20 * w[2 * S] + 20 * w[3 * S] - 5 * w[4 * S] + w[5 * S];
-      sm.hpv[r * G::kPs + c] = (uint8_t)clip255((v + 16) >> 5);
+      const uint8_t* w = &sm.win[r * 24 + c + 2];
+      int v = w[0] - 5 * w[24] + 20 * w[48] + 20 * w[72] - 5 * w[96] + w[120];
+      sm.hpv[r * 20 + c] = (uint8_t)clip255((v + 16) >> 5);
     }
     if (need & 4) {
-      const int16_t* t = &sm.hr[r * P + c];
-      int j = t[0] - 5 * t[P] + 20 * t[2 * P] + 20 * t[3 * P] - 5 * t[4 * P] + t[5 * P];
-      sm.hpj[r * G::kPs + c] = (uint8_t)clip255((j + 512) >> 10);
+      const int16_t* t = &sm.hr[r * 18 + c];
+      int j = t[0] - 5 * t[18] + 20 * t[36] + 20 * t[54] - 5 * t[72] + t[90];
+      sm.hpj[r * 20 + c] = (uint8_t)clip255((j + 512) >> 10);
     }
   }
   __syncwarp();
@@ -329,30 +311,28 @@ struct QSrc {
   const uint8_t* b;
   int sa, sb, avg;
 };
-template <int kE = 0>
 __device__ __noinline__ QSrc qpel_src(const Smem& sm, int wx, int wy, int fx, int fy) {
-  constexpr int S = WinGeom<kE>::kStride, Q = WinGeom<kE>::kPs;
-  const uint8_t* G = &sm.win[(wy + 2) * S + wx + 2];
-  const uint8_t* B = &sm.hph[wy * Q + wx];
-  const uint8_t* V = &sm.hpv[wy * Q + wx];
-  const uint8_t* J = &sm.hpj[wy * Q + wx];
+  const uint8_t* G = &sm.win[(wy + 2) * 24 + wx + 2];
+  const uint8_t* B = &sm.hph[wy * 20 + wx];
+  const uint8_t* V = &sm.hpv[wy * 20 + wx];
+  const uint8_t* J = &sm.hpj[wy * 20 + wx];
   switch (fx | (fy << 2)) {
-    case 0: return {G, G, S, S, 0};
-    case 1: return {G, B, S, Q, 1};
-    case 2: return {B, B, Q, Q, 0};
-    case 3: return {B, G + 1, Q, S, 1};
-    case 4: return {G, V, S, Q, 1};
-    case 5: return {B, V, Q, Q, 1};
-    case 6: return {B, J, Q, Q, 1};
-    case 7: return {B, V + 1, Q, Q, 1};
-    case 8: return {V, V, Q, Q, 0};
-    case 9: return {V, J, Q, Q, 1};
-    case 10: return {J, J, Q, Q, 0};
-    case 11: return {J, V + 1, Q, Q, 1};
-    case 12: return {V, G + S, Q, S, 1};
-    case 13: return {V, B + Q, Q, Q, 1};
-    case 14: return {J, B + Q, Q, Q, 1};
-    default: return {V + 1, B + Q, Q, Q, 1};
+    case 0: return {G, G, 24, 24, 0};
+    case 1: return {G, B, 24, 20, 1};
+    case 2: return {B, B, 20, 20, 0};
+    case 3: return {B, G + 1, 20, 24, 1};
+    case 4: return {G, V, 24, 20, 1};
+    case 5: return {B, V, 20, 20, 1};
+    case 6: return {B, J, 20, 20, 1};
+    case 7: return {B, V + 1, 20, 20, 1};
+    case 8: return {V, V, 20, 20, 0};
+    case 9: return {V, J, 20, 20, 1};
+    case 10: return {J, J, 20, 20, 0};
+    case 11: return {J, V + 1, 20, 20, 1};
+    case 12: return {V, G + 24, 20, 24, 1};
+    case 13: return {V, B + 20, 20, 20, 1};
+    case 14: return {J, B + 20, 20, 20, 1};
+    default: return {V + 1, B + 20, 20, 20, 1};
   }
 }
 // 8 bytes of shared memory at any alignment (rows of the window planes are 4-byte aligned).

@@ -307,42 +307,16 @@ __device__ __constant__ int8_t c_hstep[8][2] = {{0, -2}, {-2, 0}, {2, 0}, {0, 2}
 // The half-sample planes in shared memory serve every part whose integer vector they were built
 // around: a macroblock-level window (origin one sample above-left of the macroblock displaced by the
 // vector) covers every 4x4 block of the macroblock at quarter-sample offsets -3..3.
-// The learned form can instead hold one wide window (WinGeom<2>) that serves every integer vector
-// of a +-2 window.
 struct WinState {
-  int bx, by;  // integer vector of the one-vector planes held, or kNoWin
-  int wide;    // 1: the wide window is held, serving vectors (ox..ox + 4, oy..oy + 4)
-  int ox, oy;
+  int bx, by;  // integer vector of the planes held, or kNoWin
 };
 constexpr int kNoWin = 1 << 20;
 __device__ __forceinline__ void ensure_window(const Ctx& c, Smem& sm, WinState& ws, int bx, int by) {
-  if (!ws.wide && ws.bx == bx && ws.by == by) return;
+  if (ws.bx == bx && ws.by == by) return;
   stage_window(c.sd->ref_y, c.fp->stride_y, c.mbx * 16 + bx - 1, c.mby * 16 + by - 1, sm);
   build_hpel(sm, 7);
   ws.bx = bx;
   ws.by = by;
-  ws.wide = 0;
-}
-__device__ __forceinline__ void build_wide_window(const Ctx& c, Smem& sm, WinState& ws, int ox, int oy) {
-  stage_window<2>(c.sd->ref_y, c.fp->stride_y, c.mbx * 16 + ox - 1, c.mby * 16 + oy - 1, sm);
-  build_hpel<2>(sm, 7);
-  ws.wide = 1;
-  ws.ox = ox;
-  ws.oy = oy;
-  ws.bx = ws.by = kNoWin;
-}
-// The window serving integer vector (bx, by): the wide window when it covers the vector (true),
-// else the vector's own window, built when not held; (ox, oy) the window's origin vector.
-__device__ __forceinline__ bool window_for(const Ctx& c, Smem& sm, WinState& ws, int bx, int by, int& ox, int& oy) {
-  if (ws.wide && bx >= ws.ox && bx <= ws.ox + 4 && by >= ws.oy && by <= ws.oy + 4) {
-    ox = ws.ox;
-    oy = ws.oy;
-    return true;
-  }
-  ensure_window(c, sm, ws, bx, by);
-  ox = bx;
-  oy = by;
-  return false;
 }
 
 __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
@@ -404,10 +378,9 @@ __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& w
 // same at distance 1, up to two steps, each from the step's start), cost SAD + lambda * vector bits
 // against the part's predictor, the first strict minimum in that order; lanes take the part's
 // 4-sample words, one candidate at a time.
-template <int kE>
-__device__ __noinline__ uint32_t part_sad(const Smem& sm, int px, int py, int pw, int ph, int ox, int oy, int vx, int vy) {
+__device__ __noinline__ uint32_t part_sad(const Smem& sm, int px, int py, int pw, int ph, int bx, int by, int vx, int vy) {
   const int lane = lane_id();
-  const QSrc q = qpel_src<kE>(sm, (vx >> 2) - ox + 1 + px, (vy >> 2) - oy + 1 + py, vx & 3, vy & 3);
+  const QSrc q = qpel_src(sm, (vx >> 2) - bx + 1 + px, (vy >> 2) - by + 1 + py, vx & 3, vy & 3);
   const int wpr = pw >> 2, nw = wpr * ph;
   uint32_t s = 0;
   for (int w = lane; w < nw; w += 32) {
@@ -421,20 +394,16 @@ __device__ __noinline__ uint32_t part_sad(const Smem& sm, int px, int py, int pw
 __device__ __noinline__ uint32_t refine_part_sad(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph,
                                                  int bx, int by, const int* mvp, uint32_t lambda, const Bounds& bd,
                                                  int* mv) {
-  int ox, oy;
-  const bool wide = window_for(c, sm, ws, bx, by, ox, oy);
-  auto sad_at = [&](int vx, int vy) {
-    return wide ? part_sad<2>(sm, px, py, pw, ph, ox, oy, vx, vy) : part_sad<0>(sm, px, py, pw, ph, ox, oy, vx, vy);
-  };
+  ensure_window(c, sm, ws, bx, by);
   int cx = 4 * bx, cy = 4 * by;
-  uint32_t best = sad_at(cx, cy) + vec_cost(cx - mvp[0], cy - mvp[1], lambda);
+  uint32_t best = part_sad(sm, px, py, pw, ph, bx, by, cx, cy) + vec_cost(cx - mvp[0], cy - mvp[1], lambda);
   for (int st = 2; st >= 1; st--) {
     for (int it = 0; it < (st == 2 ? 1 : 2); it++) {
       const int fx = cx, fy = cy;
       for (int k = 0; k < 4; k++) {
         const int vx = fx + (k == 1 ? -st : (k == 2 ? st : 0)), vy = fy + (k == 0 ? -st : (k == 3 ? st : 0));
         if (abs(vx - 4 * bx) > 3 || abs(vy - 4 * by) > 3 || !in_bounds(bd, vx, vy)) continue;  // uniform
-        const uint32_t cost = sad_at(vx, vy) + vec_cost(vx - mvp[0], vy - mvp[1], lambda);
+        const uint32_t cost = part_sad(sm, px, py, pw, ph, bx, by, vx, vy) + vec_cost(vx - mvp[0], vy - mvp[1], lambda);
         if (cost < best) { best = cost; cx = vx; cy = vy; }
       }
       if (cx == fx && cy == fy) break;
@@ -450,10 +419,8 @@ __device__ __noinline__ uint32_t refine_part_sad(const Ctx& c, Smem& sm, WinStat
 __device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
                                           int by, const int* mv) {
   const int lane = lane_id();
-  int ox, oy;
-  const bool wide = window_for(c, sm, ws, bx, by, ox, oy);
-  const int wx = (mv[0] >> 2) - ox + 1 + px, wy = (mv[1] >> 2) - oy + 1 + py;
-  QSrc q = wide ? qpel_src<2>(sm, wx, wy, mv[0] & 3, mv[1] & 3) : qpel_src<0>(sm, wx, wy, mv[0] & 3, mv[1] & 3);
+  ensure_window(c, sm, ws, bx, by);
+  QSrc q = qpel_src(sm, (mv[0] >> 2) - bx + 1 + px, (mv[1] >> 2) - by + 1 + py, mv[0] & 3, mv[1] & 3);
   for (int i = lane; i < pw * ph; i += 32) {
     const int r = i / pw, x = i - r * pw;
     int v = q.a[r * q.sa + x];
@@ -682,7 +649,6 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
     yhi = min(lcy + kLearnedRange, imax1);
   }
   IntBest ib;
-  bool fell_back = false;
   int_search(c, sm, ss, xlo, xhi, ylo, yhi, mvp16[0], mvp16[1], lambda, ib);
   if (hint) {
     bool edge = (ib.x[0] == xlo && xlo > imin0) || (ib.x[0] == xhi && xhi < imax0) ||
@@ -698,7 +664,6 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
       edge = (ib.x[0] == xlo && xlo > imin0) || (ib.x[0] == xhi && xhi < imax0) ||
              (ib.y[0] == ylo && ylo > imin1) || (ib.y[0] == yhi && yhi < imax1);
     }
-    fell_back = edge;
     if (edge) {  // the walk did not reach the minimum: full search
       xlo = max(fcx - R, imin0); xhi = min(fcx + R, imax0);
       ylo = max(fcy - R, imin1); yhi = min(fcy + R, imax1);
@@ -710,22 +675,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   int best_t = -1;
   uint32_t best_j = UMAX;
   int bmv[4][2], bmvd[4][2];  // per part (coding order) of the best type
-  WinState ws{kNoWin, kNoWin, 0, 0, 0};  // the skip probe's window is not a refinement window
-  if (hint && !fell_back) {
-    // the parts of the tried types start from two or more integer vectors (all in the last +-2
-    // window): one wide window serves them all
-    bool many = false;
-    int fx = kNoWin, fy = kNoWin;
-    for (int t = 0; t < 4; t++) {
-      if (!((part_mask >> t) & 1)) continue;
-      for (int k = 0; k < c_type_parts[t]; k++) {
-        const int i = c_parts[c_type_first[t] + k][8];
-        if (fx == kNoWin) { fx = ib.x[i]; fy = ib.y[i]; }
-        many |= ib.x[i] != fx || ib.y[i] != fy;
-      }
-    }
-    if (many) build_wide_window(c, sm, ws, xlo, ylo);
-  }
+  WinState ws{kNoWin, kNoWin};  // the skip probe's window is not a refinement window
   for (int t = 0; t < 4; t++) {
     if (!((part_mask >> t) & 1)) continue;
     int own[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
