@@ -294,6 +294,7 @@ def run_batched(args, rank, world, local):
     pictures = len(BATCH_SIZES) * BATCH_STREAMS * BATCH_FRAMES
     wall = statistics.median(walls)
     lat = np.concatenate(lats)
+    one = batched_one_launch(args, local, jobs)
     line = {
         "metric": "batched streams: aggregate encode frames/s (64 streams of mixed size, one GPU)",
         "value": round(pictures / wall, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1),
@@ -308,12 +309,85 @@ def run_batched(args, rank, world, local):
                        "max": round(float(lat.max()), 2), "definition": "a wave's submit to the picture's access unit written"},
         "per_size": {k: {"frames_per_s": round(BATCH_STREAMS * BATCH_FRAMES / statistics.median(t for t, _ in v), 1),
                          "bitstream_bytes": int(statistics.median(nb for _, nb in v))} for k, v in per.items()},
+        "one_launch": one,
         "clocks": clk,
         "gpu_launches": args.steps * len(jobs) * (BATCH_FRAMES // BATCH_WAVE) * 2,
     }
     print(json.dumps(line), flush=True)
     for j in jobs:
         j["enc"].close()
+
+
+def batched_one_launch(args, local, jobs):
+    """The batched configuration's analysis with the sources resident on the device: all 64 streams'
+    30 pictures in ONE persistent launch (rg_analyse_gops_group over one context per size, the
+    sizes' work lists merged), against the four contexts' own launches queued together on their four
+    CUDA streams. Device time with CUDA events; analysis, reconstruction and deblocking only (no
+    copies, no bitstream)."""
+    import torch
+
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_MAIN, Engine
+    engs, planes, kinds, sy, suv, keep = [], [], [], [], [], []
+    for j, (w, h) in zip(jobs, BATCH_SIZES):
+        cw, ch = (w + 1) // 2, (h + 1) // 2
+        dev = j["host"].to(f"cuda:{local}")
+        keep.append(dev)
+        e = Engine(w, h, 26, profile=RG_PROFILE_MAIN, num_streams=BATCH_STREAMS, device=local, max_frames=BATCH_FRAMES)
+        for s, q in enumerate(j["qps"]):
+            e.set_stream_qp(s, q)
+        if j["tuning"]:
+            e.set_pipeline_tuning(**j["tuning"])
+        p, k = [], []
+        for f in range(BATCH_FRAMES):
+            for s in range(BATCH_STREAMS):
+                b = dev[s, f].data_ptr()
+                p += [b, b + w * h, b + w * h + cw * ch]
+                k.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+        engs.append(e)
+        planes.append(p)
+        kinds.append(k)
+        sy.append(w)
+        suv.append(cw)
+    st = torch.cuda.ExternalStream(engs[0].cuda_stream, device=f"cuda:{local}")
+
+    def group():
+        Engine.analyse_gops_group(engs, planes, sy, suv, kinds, BATCH_FRAMES)
+
+    def separate():
+        for e, p, k, a, b in zip(engs, planes, kinds, sy, suv):
+            e.analyse_gops_device(p, a, b, k, BATCH_FRAMES)
+
+    out = {}
+    steps = max(1, min(args.steps, 4))
+    for name, fn in (("one_launch", group), ("launch_per_size", separate)):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        for e in engs:
+            e.sync()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(steps):
+            fn()
+        if name == "launch_per_size":   # the last of the four streams to finish ends the step
+            for e in engs[1:]:
+                ev = torch.cuda.Event()
+                ev.record(torch.cuda.ExternalStream(e.cuda_stream, device=f"cuda:{local}"))
+                st.wait_event(ev)
+        b.record(st)
+        b.synchronize()
+        for e in engs:
+            e.sync()
+        ms = a.elapsed_time(b) / steps
+        out[name] = {"frames_per_s": round(len(jobs) * BATCH_STREAMS * BATCH_FRAMES / (ms / 1000), 1),
+                     "ms_per_step": round(ms, 3), "wall_ms_per_step": round((time.perf_counter() - t0) * 1000 / steps, 3)}
+    out["steps"] = steps
+    out["what"] = ("device step of all 1920 pictures (64 streams x 30) with sources resident: one "
+                   "rg_analyse_gops_group launch vs the four contexts' launches on four streams")
+    for e in engs:
+        e.close()
+    return out
 
 
 def run_reference(args, rank, world):

@@ -185,6 +185,22 @@ int rg_analyse_batch_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_
 int rg_analyse_gops_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t stride_y,
                            size_t stride_uv, const int32_t* kinds, int32_t frames);
 
+/*
+ * rg_analyse_gops_device for n contexts of different picture sizes (1..8 contexts on one device,
+ * all in the plain form or all in the full-search form) in ONE persistent launch: the work lists
+ * of the contexts (each with its own lag; the segment length and SM roles of ctxs[0]) merged in
+ * key order, so macroblocks of every size share the SMs. dev_planes[i], stride_y[i], stride_uv[i],
+ * kinds[i]: context i's arguments as rg_analyse_gops_device takes them; `frames` pictures of every
+ * stream of every context. Queued on ctxs[0]'s stream; each context's later calls wait for it,
+ * and each context resolves its part as its own pending call (a wait that gave up re-runs that
+ * context's pictures on the per-diagonal path). The batched transcode of many independent
+ * streams of several sizes (the pipeline's parallel_gop_map over encoders,
+ * crates/ragdoll-pipeline/src/lib.rs:110-157) as one launch; no single counterpart in the reference.
+ */
+int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
+                          const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                          int32_t frames);
+
 /* Host-buffer form of rg_analyse_gops_device; out receives frames * num_streams * mb_w * mb_h
  * records (or NULL). */
 int rg_analyse_gops(rg_ctx* ctx, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,

@@ -62,7 +62,9 @@ struct StreamDev {
   int32_t qp, qpc;        // the stream's QP and chroma QP
   // SkipBounds (enc.rs:2104) of the stream's QP
   uint32_t sb_luma, sb_luma_ssd, sb_chroma, sb_chroma_ssd, sb_probe;
-  int32_t pad_;
+  // pipelined launches: the descriptor's size group (its FrameParams), the offset of its rows in the
+  // launch's row counters, and the descriptor of the previous picture of its stream (-1: none)
+  int32_t group, rows_base, prev_ps;
   // search forms only (null / 0 in the plain form)
   MbMv4* mv4;              // this picture's quadrant vectors
   const rg_mb_hint* hint;  // learned form: this picture's hints (null: full search)
@@ -73,7 +75,8 @@ struct StreamDev {
 };
 
 // Frame-constant parameters of one wavefront (all streams share the size; qp / qpc / sb_* are the
-// context's default QP -- the kernels read each stream's own from its StreamDev).
+// context's default QP -- the kernels read each stream's own from its StreamDev). A pipelined launch
+// takes up to kMaxGroups of them, one per picture size among its streams.
 struct FrameParams {
   int32_t width, height;      // display size
   int32_t mb_w, mb_h;
@@ -101,6 +104,11 @@ int wavefront_steps(const FrameParams& fp);
 // reach, in macroblock rows and columns beyond zero motion, of the launch's waits for a reference
 // picture (0: no such wait); the work order never waits for an untaken segment when
 // lag >= max(seg, 2) * (4 + rows) + seg + columns + 3.
+constexpr int kMaxGroups = 8;
+struct FrameGroups {
+  FrameParams g[kMaxGroups];
+  int32_t n;
+};
 int pipeline_grid(int device, int form = 0);
 int pipeline_sms(int device);
 size_t pipeline_counter_ints(const FrameParams& fp, int frames);
@@ -109,12 +117,19 @@ size_t pipeline_counter_ints(const FrameParams& fp, int frames);
 size_t pipeline_task_count(const FrameParams& fp, int frames, int seg);
 // Queues: 0 analysis, 1 deblocking (split), 2 analysis of IDR pictures (kinds != null; [f][s]).
 constexpr int kPipeQueues = 3;
+// keys (or null): each task's key, ascending within each queue.
 size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, const int32_t* kinds,
-                          int2* tasks, int qbeg[3], int qend[3]);
-void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
-                     size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
-                     int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
-                     int* host_reach, cudaStream_t st, int form = 0);
+                          int2* tasks, int qbeg[3], int qend[3], uint32_t* keys = nullptr);
+// One launch over n_desc descriptors of up to kMaxGroups picture sizes (descriptor d: group
+// d.group, rows d.rows_base .. + its mb_h in the row counters, total_rows in all). host_err null:
+// no error hand-off kernel (launch_error_to_host queues one per caller instead).
+void launch_pipeline(const FrameGroups& fg, const StreamDev* d_streams, int n_desc, int total_rows, int* counters,
+                     const int2* d_tasks, size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms,
+                     int intra_sms, int sms, int seg, int grid, unsigned long long timeout_ns, int* ready, int seq,
+                     int* host_err, int* host_reach, cudaStream_t st, int form = 0);
+void launch_error_to_host(const int* counters, int n_desc, int total_rows, int* host_err, int* host_reach,
+                          cudaStream_t st);
+size_t pipeline_counter_ints(int total_rows, int n_desc);
 void upload_tables();
 
 }  // namespace rg

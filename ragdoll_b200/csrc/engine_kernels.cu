@@ -2130,10 +2130,10 @@ __device__ __noinline__ void extend_mb(const FrameParams& fp, const StreamDev& s
 struct PipeParams {
   int* ticket;
   int* error;
-  int* ana;    // [F][S][mb_h] analysed macroblocks per row
-  int* db;     // [F][S][mb_h] deblocked macroblocks per row; a macroblock's deblocking also
+  int* ana;    // analysed macroblocks per row, descriptor d's rows from ana + d.rows_base
+  int* db;     // deblocked macroblocks per row (the same layout); a macroblock's deblocking also
                // extends the padding of the macroblocks it makes final
-  const int2* tasks;  // {picture * S + stream, row << 16 | first macroblock << 1 | deblock}
+  const int2* tasks;  // {descriptor, row << 16 | first macroblock << 1 | deblock}
   int n_tasks;
   int qbeg[3], qend[3];  // queue q = tasks[qbeg[q], qend[q]): 0 analysis, 1 deblocking, 2 IDR analysis
   int deblock_sms;    // SMs whose warps take queue 1 first
@@ -2141,8 +2141,8 @@ struct PipeParams {
   int role_by_sm;     // 0: by block index instead (a grid too small to reach every SM)
   int seg;
   unsigned long long timeout_ns;
-  int* rows_done;     // [F][S] rows of a picture fully analysed
-  int* ready;         // [F][S] in mapped host memory (or null): seq once a picture's records are final
+  int* rows_done;     // [descriptor] rows of a picture fully analysed
+  int* ready;         // [descriptor] in mapped host memory (or null): seq once a picture's records are final
   int seq;
   int* host_err;      // mapped host memory: the error word as the launch ends (no copy to wait for)
   int* reach;         // [2] 1 + the largest reach of a reference wait beyond zero motion (rows, columns)
@@ -2168,11 +2168,10 @@ __device__ __noinline__ void picture_row_done(int* rows_done, int* ready, int se
 // At least 16 warps per SM: up to 128 registers a thread, so nothing spills (4.5 % faster than 20,
 // which held it to 96 registers with spills).
 template <int kForm>
-__global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const StreamDev* __restrict__ sds, PipeParams pp) {
+__global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameGroups fg, const StreamDev* __restrict__ sds, PipeParams pp) {
   __shared__ Smem sm;
   __shared__ FormSmem<kForm> ss;
   const int lane = lane_id();
-  const int S = fp.n_streams, H = fp.mb_h, Wm = fp.mb_w;
   // Warps on the first deblock_sms SMs take deblocking segments first, on the next intra_sms SMs
   // segments of IDR pictures (the critical path of a GOP), and the others the remaining analysis
   // (each SM then runs a smaller code footprint); a warp whose queue is empty takes from the next.
@@ -2200,19 +2199,22 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameParams fp, const 
     if (t < 0) break;
     if (__shfl_sync(FULL, lane == 0 ? ld_relaxed(pp.error) : 0, 0)) break;
     int2 task = __ldg(pp.tasks + t);
-    int ps = task.x, f = ps / S;
+    int ps = task.x;
+    const StreamDev& sd = sds[ps];
+    const FrameParams& fp = fg.g[sd.group];  // the descriptor's picture size
+    const int H = fp.mb_h, Wm = fp.mb_w;
     int y = task.y >> 16, x0 = (task.y >> 1) & 0x7fff, x1 = min(x0 + pp.seg, Wm);
     bool ana = (task.y & 1) == 0;
-    const StreamDev& sd = sds[ps];
-    int* ana_rows = pp.ana + ps * H;
-    int* db_rows = pp.db + ps * H;
+    int* ana_rows = pp.ana + sd.rows_base;
+    int* db_rows = pp.db + sd.rows_base;
     bool failed = false;
     if (ana) {
       PipeWait pw;
-      bool has_prev = f > 0 && sd.kind == RG_FRAME_P;
+      bool has_prev = sd.prev_ps >= 0 && sd.kind == RG_FRAME_P;
       if (has_prev) {
-        pw.ana_prev = pp.ana + (ps - S) * H;
-        pw.db_prev = pp.db + (ps - S) * H;
+        const int pb = sds[sd.prev_ps].rows_base;
+        pw.ana_prev = pp.ana + pb;
+        pw.db_prev = pp.db + pb;
       }
       pw.error = pp.error;
       pw.timeout_ns = pp.timeout_ns;
@@ -2400,7 +2402,7 @@ size_t pipeline_task_count(const FrameParams& fp, int frames, int seg) {
 }
 
 size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, bool split, const int32_t* kinds,
-                          int2* tasks, int qbeg[3], int qend[3]) {
+                          int2* tasks, int qbeg[3], int qend[3], uint32_t* keys) {
   int S = fp.n_streams, H = fp.mb_h, W = fp.mb_w;
   int segs = (W + seg - 1) / seg, a = seg > 2 ? seg : 2;
   if (lag <= 0) lag = a * 8 + seg + 7;
@@ -2434,20 +2436,20 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
           for (int k = 0; k < segs; k++) {
             size_t at = start[slot(f, s, role, y, k)]++;
             tasks[at] = make_int2(f * S + s, (y << 16) | ((k * seg) << 1) | role);
+            if (keys) keys[at] = (uint32_t)key(f, role, y, k);
           }
   return pipeline_task_count(fp, frames, seg);
 }
 
-void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int frames, int* counters, const int2* d_tasks,
-                     size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms, int intra_sms, int sms,
-                     int seg, int grid, unsigned long long timeout_ns, int* ready, int seq, int* host_err,
-                     int* host_reach, cudaStream_t st, int form) {
-  int S = fp.n_streams, H = fp.mb_h;
+void launch_pipeline(const FrameGroups& fg, const StreamDev* d_streams, int n_desc, int total_rows, int* counters,
+                     const int2* d_tasks, size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms,
+                     int intra_sms, int sms, int seg, int grid, unsigned long long timeout_ns, int* ready, int seq,
+                     int* host_err, int* host_reach, cudaStream_t st, int form) {
   PipeParams pp;
   pp.ticket = counters;
   pp.error = counters + 1;
   pp.ana = counters + 4;
-  pp.db = pp.ana + frames * S * H;
+  pp.db = pp.ana + total_rows;
   pp.tasks = d_tasks;
   pp.n_tasks = (int)n_tasks;
   for (int q = 0; q < 3; q++) {
@@ -2459,19 +2461,27 @@ void launch_pipeline(const FrameParams& fp, const StreamDev* d_streams, int fram
   pp.role_by_sm = grid >= sms;
   pp.seg = seg;
   pp.timeout_ns = timeout_ns;
-  pp.rows_done = pp.db + frames * S * H;
+  pp.rows_done = pp.db + total_rows;
   pp.ready = ready;
   pp.seq = seq;
   pp.host_err = host_err;
-  pp.reach = pp.rows_done + frames * S;
+  pp.reach = pp.rows_done + n_desc;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;
-  if (form) pipeline_kernel<1><<<g, 32, 0, st>>>(fp, d_streams, pp);
-  else pipeline_kernel<0><<<g, 32, 0, st>>>(fp, d_streams, pp);
-  error_to_host_kernel<<<1, 1, 0, st>>>(pp.error, pp.reach, host_err, host_reach);
+  if (form) pipeline_kernel<1><<<g, 32, 0, st>>>(fg, d_streams, pp);
+  else pipeline_kernel<0><<<g, 32, 0, st>>>(fg, d_streams, pp);
+  if (host_err) error_to_host_kernel<<<1, 1, 0, st>>>(pp.error, pp.reach, host_err, host_reach);
 }
 
+void launch_error_to_host(const int* counters, int n_desc, int total_rows, int* host_err, int* host_reach,
+                          cudaStream_t st) {
+  const int* reach = counters + 4 + 2 * (size_t)total_rows + n_desc;
+  error_to_host_kernel<<<1, 1, 0, st>>>(counters + 1, reach, host_err, host_reach);
+}
+
+size_t pipeline_counter_ints(int total_rows, int n_desc) { return 4 + 2 * (size_t)total_rows + n_desc + 2; }
+
 size_t pipeline_counter_ints(const FrameParams& fp, int frames) {
-  return 4 + 2 * (size_t)frames * fp.n_streams * fp.mb_h + (size_t)frames * fp.n_streams + 2;
+  return pipeline_counter_ints(frames * fp.n_streams * fp.mb_h, frames * fp.n_streams);
 }
 
 void launch_extend_borders(const FrameParams& fp, const StreamDev* d_streams, cudaStream_t st) {

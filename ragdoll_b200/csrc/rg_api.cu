@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "engine.h"
@@ -193,6 +194,19 @@ struct rg_ctx {
   cudaEvent_t a_in_done[2] = {nullptr, nullptr}, a_kern_done[2] = {nullptr, nullptr};
   cudaEvent_t a_out_done[2] = {nullptr, nullptr};
   rg_mb_out* a_out_ptr[2] = {nullptr, nullptr};  // host buffer each slot's call copies into
+  // rg_analyse_gops_group: as the leader, the launch's descriptors, counters and merged work list;
+  // as any member, an event that orders the leader's launch after this context's earlier work
+  StreamDev* g_dstreams = nullptr;
+  StreamDev* g_hstreams = nullptr;  // pinned
+  size_t g_streams_cap = 0;
+  int* g_counters = nullptr;
+  size_t g_counters_cap = 0;
+  int2* g_dtasks = nullptr;
+  size_t g_tasks_cap = 0, g_ntasks = 0;
+  std::vector<int2> g_htasks;
+  std::vector<int64_t> g_shape;
+  int g_qbeg[3] = {0, 0, 0}, g_qend[3] = {0, 0, 0};
+  cudaEvent_t g_done = nullptr, g_order = nullptr;
   int* h_ready[2] = {nullptr, nullptr};  // mapped host memory: per picture, the launch seq once final
   int* d_ready[2] = {nullptr, nullptr};  // the same, as the device sees it
   int a_seq[2] = {0, 0}, a_frames[2] = {0, 0};
@@ -364,6 +378,12 @@ void rg_destroy(rg_ctx* c) {
   cudaFree(c->m_src);
   cudaFree(c->counters);
   cudaFree(c->d_tasks);
+  cudaFree(c->g_dstreams);
+  cudaFree(c->g_counters);
+  cudaFree(c->g_dtasks);
+  if (c->g_hstreams) cudaFreeHost(c->g_hstreams);
+  if (c->g_done) cudaEventDestroy(c->g_done);
+  if (c->g_order) cudaEventDestroy(c->g_order);
   if (c->a_in) cudaStreamSynchronize(c->a_in);
   if (c->a_out) cudaStreamSynchronize(c->a_out);
   for (int i = 0; i < 2; i++) {
@@ -491,7 +511,9 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
     }
     d.kind = kinds[i];
     apply_qp(d, c->qps[s]);
-    d.pad_ = 0;
+    d.group = 0;
+    d.rows_base = 0;
+    d.prev_ps = -1;
     d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + par) * c->n_mb : nullptr;
     d.hint = hints ? hints[i] : nullptr;
     d.search_range = c->search_range;
@@ -518,6 +540,39 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
 // the previous launch without waiting measured slower end to end: the host's writing of the
 // previous wave then runs during that wave's own launch and slows it.) ready / seq: per-picture
 // flags in mapped host memory (rg_analyse_gops_stream), or null.
+// Descriptor of picture f of stream s of a pipelined call (records at rec_base, [f][s]); in a launch
+// of several contexts, this context's descriptors start at desc_base, its row counters at
+// rows_base, and its picture size is group `group`.
+static void gop_desc(const rg_ctx* c, StreamDev& d, int f, int s, const uint8_t* const* dev_planes,
+                     const int32_t* kinds, rg_mb_out* rec_base, const rg_mb_hint* hint, int group, int desc_base,
+                     int rows_base) {
+  const int S = c->S, g = c->frames[s] + f;
+  const int cur = g % c->nslots, prv = (g + c->nslots - 1) % c->nslots;
+  d.src_y = dev_planes[(f * S + s) * 3];
+  d.src_u = dev_planes[(f * S + s) * 3 + 1];
+  d.src_v = dev_planes[(f * S + s) * 3 + 2];
+  d.cur_y = c->pic_plane(s, cur, 0);
+  d.cur_u = c->pic_plane(s, cur, 1);
+  d.cur_v = c->pic_plane(s, cur, 2);
+  d.ref_y = c->pic_plane(s, prv, 0);
+  d.ref_u = c->pic_plane(s, prv, 1);
+  d.ref_v = c->pic_plane(s, prv, 2);
+  d.info = c->infos + ((size_t)s * c->nslots + cur) * c->n_mb;
+  d.prev_info = c->infos + ((size_t)s * c->nslots + prv) * c->n_mb;
+  d.rec = rec_base + ((size_t)f * S + s) * c->n_mb;
+  d.unf_y = d.unf_u = d.unf_v = nullptr;
+  d.kind = kinds[f * S + s];
+  apply_qp(d, c->qps[s]);
+  d.group = group;
+  d.rows_base = rows_base + (f * S + s) * c->fp.mb_h;
+  d.prev_ps = f > 0 ? desc_base + (f - 1) * S + s : -1;
+  d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + cur) * c->n_mb : nullptr;
+  d.hint = hint;
+  d.search_range = c->search_range;
+  d.walk = c->walk;
+  for (int k = 0; k < 4; k++) { d.type_bits[k] = c->type_bits[k]; d.pad3_[k] = 0; }
+}
+
 static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                         const int32_t* kinds, int32_t frames, rg_mb_out* rec_base, int* ready = nullptr, int seq = 0,
                         bool resolved = false) {
@@ -571,32 +626,8 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   CK(cudaEventSynchronize(c->slot_done[slot]));
   StreamDev* h = c->h_streams[slot];
   for (int f = 0; f < frames; f++)
-    for (int s = 0; s < S; s++) {
-      int g = c->frames[s] + f;
-      int cur = g % c->nslots, prv = (g + c->nslots - 1) % c->nslots;
-      StreamDev& d = h[f * S + s];
-      d.src_y = dev_planes[(f * S + s) * 3];
-      d.src_u = dev_planes[(f * S + s) * 3 + 1];
-      d.src_v = dev_planes[(f * S + s) * 3 + 2];
-      d.cur_y = c->pic_plane(s, cur, 0);
-      d.cur_u = c->pic_plane(s, cur, 1);
-      d.cur_v = c->pic_plane(s, cur, 2);
-      d.ref_y = c->pic_plane(s, prv, 0);
-      d.ref_u = c->pic_plane(s, prv, 1);
-      d.ref_v = c->pic_plane(s, prv, 2);
-      d.info = c->infos + ((size_t)s * c->nslots + cur) * c->n_mb;
-      d.prev_info = c->infos + ((size_t)s * c->nslots + prv) * c->n_mb;
-      d.rec = rec_base + ((size_t)f * S + s) * c->n_mb;
-      d.unf_y = d.unf_u = d.unf_v = nullptr;
-      d.kind = kinds[f * S + s];
-      apply_qp(d, c->qps[s]);
-      d.pad_ = 0;
-      d.mv4 = c->mv4s ? c->mv4s + ((size_t)s * c->nslots + cur) * c->n_mb : nullptr;
-      d.hint = hv.empty() ? nullptr : hv[f * S + s];
-      d.search_range = c->search_range;
-      d.walk = c->walk;
-      for (int k = 0; k < 4; k++) { d.type_bits[k] = c->type_bits[k]; d.pad3_[k] = 0; }
-    }
+    for (int s = 0; s < S; s++)
+      gop_desc(c, h[f * S + s], f, s, dev_planes, kinds, rec_base, hv.empty() ? nullptr : hv[f * S + s], 0, 0, 0);
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
   fp.src_stride_uv = (int)stride_uv;
@@ -628,9 +659,12 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   int pslot = (c->pend_head + c->pend_count) & 1;
   rg_ctx::Pending& p = c->pend[pslot];
   *(volatile int*)p.h_err = 0;  // the launch that used this word before was resolved
-  launch_pipeline(fp, c->d_streams[slot], frames, c->counters, c->d_tasks, c->n_tasks, c->qbeg, c->qend, c->deblock_sms,
-                  c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq, c->d_err + pslot,
-                  c->d_err + 2 + 2 * pslot, c->stream, c->form != RG_FORM_PLAIN);
+  FrameGroups fg{};
+  fg.g[0] = fp;
+  fg.n = 1;
+  launch_pipeline(fg, c->d_streams[slot], frames * S, frames * S * fp.mb_h, c->counters, c->d_tasks, c->n_tasks, c->qbeg,
+                  c->qend, c->deblock_sms, c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq,
+                  c->d_err + pslot, c->d_err + 2 + 2 * pslot, c->stream, c->form != RG_FORM_PLAIN);
   CK(cudaGetLastError());
   CK(cudaEventRecord(p.done, c->stream));
   p.planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
@@ -652,6 +686,198 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
                            const int32_t* kinds, int32_t frames) {
   if (!c) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null context");
   return enqueue_gops(c, dev_planes, stride_y, stride_uv, kinds, frames, c->recs);
+}
+
+// ---- several contexts, one persistent launch ----------------------------------------------------
+// The leader (ctxs[0]) keeps the launch's descriptors, counters and merged work list.
+int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
+                          const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                          int32_t frames) {
+  const char* who = "rg_analyse_gops_group";
+  if (!ctxs || !dev_planes || !stride_y || !stride_uv || !kinds || n < 1 || n > kMaxGroups)
+    return fail(RG_ERR_INVALID, "%s: null argument or %d contexts (1..%d)", who, n, kMaxGroups);
+  rg_ctx* L = ctxs[0];
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    if (!c || !dev_planes[i] || !kinds[i]) return fail(RG_ERR_INVALID, "%s: null context or argument %d", who, i);
+    for (int j = 0; j < i; j++)
+      if (ctxs[j] == c) return fail(RG_ERR_INVALID, "%s: context %d given twice", who, i);
+    if (c->cfg.device != L->cfg.device) return fail(RG_ERR_INVALID, "%s: contexts on different devices", who);
+    if ((c->form != RG_FORM_PLAIN) != (L->form != RG_FORM_PLAIN) || c->form == RG_FORM_LEARNED)
+      return fail(RG_ERR_UNSUPPORTED, "%s: the contexts must all be plain or all full search", who);
+    if (frames < 1 || frames > c->max_frames)
+      return fail(RG_ERR_INVALID, "%s: frames %d outside 1..%d of context %d", who, frames, c->max_frames, i);
+    if (stride_y[i] < (size_t)c->cfg.width || stride_uv[i] < (size_t)(c->cfg.width + 1) / 2)
+      return fail(RG_ERR_INVALID, "%s: stride too small (context %d)", who, i);
+  }
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    int r = resolve_pending(c, false);
+    if (r) return r;
+    for (int f = 0; f < frames; f++)
+      for (int s = 0; s < c->S; s++) {
+        const int k = kinds[i][f * c->S + s];
+        if (k != RG_FRAME_IDR && k != RG_FRAME_P)
+          return fail(RG_ERR_INVALID, "%s: context %d picture %d stream %d kind %d", who, i, f, s, k);
+        if (k == RG_FRAME_P && f == 0 && c->frames[s] == 0)
+          return fail(RG_ERR_STATE, "%s: context %d stream %d starts with a P picture", who, i, s);
+        for (int p = 0; p < 3; p++)
+          if (!dev_planes[i][(f * c->S + s) * 3 + p])
+            return fail(RG_ERR_INVALID, "%s: context %d picture %d stream %d null plane", who, i, f, s);
+      }
+    c->hints.clear();
+  }
+  CK(cudaSetDevice(L->cfg.device));
+  // descriptors and rows of every context, one after the other
+  std::vector<int> desc_base(n + 1, 0), rows_base(n + 1, 0);
+  for (int i = 0; i < n; i++) {
+    desc_base[i + 1] = desc_base[i] + frames * ctxs[i]->S;
+    rows_base[i + 1] = rows_base[i] + frames * ctxs[i]->S * ctxs[i]->fp.mb_h;
+  }
+  const int n_desc = desc_base[n], total_rows = rows_base[n];
+  if ((size_t)n_desc > L->g_streams_cap) {
+    if (L->g_done) CK(cudaEventSynchronize(L->g_done));
+    cudaFree(L->g_dstreams);
+    if (L->g_hstreams) cudaFreeHost(L->g_hstreams);
+    L->g_dstreams = nullptr;
+    L->g_hstreams = nullptr;
+    L->g_streams_cap = 0;
+    if (cudaMalloc((void**)&L->g_dstreams, sizeof(StreamDev) * n_desc) != cudaSuccess ||
+        cudaHostAlloc((void**)&L->g_hstreams, sizeof(StreamDev) * n_desc, cudaHostAllocDefault) != cudaSuccess)
+      return fail(RG_ERR_OOM, "%s: %d descriptors", who, n_desc);
+    L->g_streams_cap = n_desc;
+  }
+  const size_t n_counters = pipeline_counter_ints(total_rows, n_desc);
+  if (n_counters > L->g_counters_cap) {
+    if (L->g_done) CK(cudaEventSynchronize(L->g_done));
+    cudaFree(L->g_counters);
+    L->g_counters = nullptr;
+    if (cudaMalloc((void**)&L->g_counters, sizeof(int) * n_counters) != cudaSuccess)
+      return fail(RG_ERR_OOM, "%s: %zu counters", who, n_counters);
+    L->g_counters_cap = n_counters;
+  }
+  if (!L->g_done) CK(cudaEventCreateWithFlags(&L->g_done, cudaEventDisableTiming));
+  CK(cudaEventSynchronize(L->g_done));  // the pinned descriptors of the last group call were copied
+  FrameGroups fg{};
+  fg.n = n;
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    fg.g[i] = c->fp;
+    fg.g[i].src_stride_y = (int)stride_y[i];
+    fg.g[i].src_stride_uv = (int)stride_uv[i];
+    for (int f = 0; f < frames; f++)
+      for (int s = 0; s < c->S; s++)
+        gop_desc(c, L->g_hstreams[desc_base[i] + f * c->S + s], f, s, dev_planes[i], kinds[i], c->recs, nullptr, i,
+                 desc_base[i], rows_base[i]);
+  }
+  // work list: each context's own (the leader's segment length, each context's lag), merged by key
+  // queue by queue; rebuilt only when the shape, the lags or the picture kinds change
+  const int seg = L->seg, a = seg > 2 ? seg : 2;
+  const int split = L->deblock_sms > 0 && L->grid >= 2 ? 1 : 0;
+  const bool intra_q = L->intra_sms > 0 && L->grid >= 3;
+  std::vector<int64_t> shape = {frames, seg, split, intra_q ? 1 : 0, n};
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    const int lag = c->lag > 0 ? c->lag : a * (4 + c->reach_y) + seg + c->reach_x + 3;
+    shape.insert(shape.end(), {c->cfg.width, c->cfg.height, c->S, lag});
+    if (intra_q) shape.insert(shape.end(), kinds[i], kinds[i] + (size_t)frames * c->S);
+  }
+  if (shape != L->g_shape) {
+    std::vector<std::vector<int2>> lists(n);
+    std::vector<std::vector<uint32_t>> keys(n);
+    std::vector<std::array<int, 3>> qb(n), qe(n);
+    size_t total = 0;
+    for (int i = 0; i < n; i++) {
+      rg_ctx* c = ctxs[i];
+      const int lag = c->lag > 0 ? c->lag : a * (4 + c->reach_y) + seg + c->reach_x + 3;
+      FrameParams fp = c->fp;
+      lists[i].resize(pipeline_task_count(fp, frames, seg));
+      keys[i].resize(lists[i].size());
+      std::vector<int32_t> kk;
+      if (intra_q) kk.assign(kinds[i], kinds[i] + (size_t)frames * c->S);
+      pipeline_task_list(fp, frames, lag, seg, split != 0, intra_q ? kk.data() : nullptr, lists[i].data(), qb[i].data(),
+                         qe[i].data(), keys[i].data());
+      total += lists[i].size();
+    }
+    L->g_htasks.resize(total);
+    size_t at = 0;
+    for (int q = 0; q < kPipeQueues; q++) {
+      L->g_qbeg[q] = (int)at;
+      std::vector<int> pos(n);
+      for (int i = 0; i < n; i++) pos[i] = qb[i][q];
+      while (true) {  // the least key first, the lower context on ties
+        int best = -1;
+        for (int i = 0; i < n; i++)
+          if (pos[i] < qe[i][q] && (best < 0 || keys[i][pos[i]] < keys[best][pos[best]])) best = i;
+        if (best < 0) break;
+        int2 t = lists[best][pos[best]++];
+        t.x += desc_base[best];
+        L->g_htasks[at++] = t;
+      }
+      L->g_qend[q] = (int)at;
+    }
+    if (total > L->g_tasks_cap) {
+      CK(cudaStreamSynchronize(L->stream));
+      cudaFree(L->g_dtasks);
+      L->g_dtasks = nullptr;
+      L->g_tasks_cap = 0;
+      if (cudaMalloc((void**)&L->g_dtasks, sizeof(int2) * total) != cudaSuccess)
+        return fail(RG_ERR_OOM, "%s: %zu tasks", who, total);
+      L->g_tasks_cap = total;
+    }
+    CK(cudaMemcpyAsync(L->g_dtasks, L->g_htasks.data(), sizeof(int2) * total, cudaMemcpyHostToDevice, L->stream));
+    L->g_ntasks = total;
+    L->g_shape = shape;
+  }
+  // the launch runs on the leader's stream after every context's earlier work
+  for (int i = 1; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    if (!c->g_order) CK(cudaEventCreateWithFlags(&c->g_order, cudaEventDisableTiming));
+    CK(cudaEventRecord(c->g_order, c->stream));
+    CK(cudaStreamWaitEvent(L->stream, c->g_order, 0));
+  }
+  CK(cudaMemcpyAsync(L->g_dstreams, L->g_hstreams, sizeof(StreamDev) * n_desc, cudaMemcpyHostToDevice, L->stream));
+  CK(cudaEventRecord(L->g_done, L->stream));
+  CK(cudaMemsetAsync(L->g_counters, 0, sizeof(int) * n_counters, L->stream));
+  std::vector<int> pslot(n);
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    pslot[i] = (c->pend_head + c->pend_count) & 1;
+    *(volatile int*)c->pend[pslot[i]].h_err = 0;
+  }
+  launch_pipeline(fg, L->g_dstreams, n_desc, total_rows, L->g_counters, L->g_dtasks, L->g_ntasks, L->g_qbeg, L->g_qend,
+                  L->deblock_sms, L->intra_sms, L->sms, seg, L->grid, L->timeout_ns, nullptr, 0, nullptr, nullptr,
+                  L->stream, L->form != RG_FORM_PLAIN);
+  CK(cudaGetLastError());
+  // every context gets the launch's error word and reach as its own pending call, resolved (and if
+  // a wait gave up, re-run picture by picture) by the context itself
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    launch_error_to_host(L->g_counters, n_desc, total_rows, c->d_err + pslot[i], c->d_err + 2 + 2 * pslot[i],
+                         L->stream);
+  }
+  CK(cudaGetLastError());
+  if (!L->g_order) CK(cudaEventCreateWithFlags(&L->g_order, cudaEventDisableTiming));
+  CK(cudaEventRecord(L->g_order, L->stream));
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    if (i) CK(cudaStreamWaitEvent(c->stream, L->g_order, 0));
+    rg_ctx::Pending& p = c->pend[pslot[i]];
+    CK(cudaEventRecord(p.done, c->stream));
+    p.planes.assign(dev_planes[i], dev_planes[i] + (size_t)frames * c->S * 3);
+    p.kinds.assign(kinds[i], kinds[i] + (size_t)frames * c->S);
+    p.start = c->frames;
+    p.frames = frames;
+    p.sy = stride_y[i];
+    p.suv = stride_uv[i];
+    p.rec = c->recs;
+    p.out = nullptr;
+    p.out_bytes = 0;
+    p.hints.clear();
+    c->pend_count++;
+    for (int s = 0; s < c->S; s++) c->frames[s] += frames;
+  }
+  return RG_OK;
 }
 
 int rg_copy_records_gops(rg_ctx* c, int32_t frames, rg_mb_out* out) {

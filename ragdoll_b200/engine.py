@@ -57,7 +57,7 @@ EXPORTS = [
     "rg_net_param_count", "rg_net_create", "rg_net_destroy", "rg_net_set_params", "rg_net_get_params",
     "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
     "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device", "rg_set_search_tuning",
-    "rg_net_set_hint_policy", "rg_net_set_coarse_range",
+    "rg_net_set_hint_policy", "rg_net_set_coarse_range", "rg_analyse_gops_group",
 ]
 
 
@@ -130,6 +130,7 @@ def lib() -> ctypes.CDLL:
                                 ctypes.POINTER(ctypes.c_double)]
     L.rg_analyse_gops.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_analyse_gops_device.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32]
+    L.rg_analyse_gops_group.argtypes = [P, ctypes.c_int32, P, P, P, P, ctypes.c_int32]
     L.rg_copy_records_gops.argtypes = [P, ctypes.c_int32, P]
     L.rg_analyse_gops_async.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_pipeline_work_list.restype = ctypes.c_int64
@@ -327,6 +328,23 @@ class Engine:
         planes = (ctypes.c_void_p * len(dev_planes))(*dev_planes)
         k = (ctypes.c_int32 * len(kinds))(*kinds)
         _check(lib().rg_analyse_gops_device(self.h, planes, stride_y, stride_uv, k, frames))
+
+    @staticmethod
+    def analyse_gops_group(engines, dev_planes, stride_y, stride_uv, kinds, frames: int) -> None:
+        """rg_analyse_gops_group: ``frames`` pictures of every stream of every engine (each its own
+        picture size) in one persistent launch on the first engine's stream. dev_planes[i] /
+        kinds[i]: engine i's arguments as analyse_gops_device takes them; stride_y / stride_uv: one
+        per engine."""
+        n = len(engines)
+        P = ctypes.c_void_p
+        ctxs = (P * n)(*[e.h for e in engines])
+        plane_arrays = [(P * len(p))(*p) for p in dev_planes]
+        kind_arrays = [(ctypes.c_int32 * len(k))(*k) for k in kinds]
+        planes = (P * n)(*[ctypes.cast(a, P) for a in plane_arrays])
+        ks = (P * n)(*[ctypes.cast(a, P) for a in kind_arrays])
+        sy = (ctypes.c_size_t * n)(*stride_y)
+        suv = (ctypes.c_size_t * n)(*stride_uv)
+        _check(lib().rg_analyse_gops_group(ctxs, n, planes, sy, suv, ks, frames))
 
     def set_analysis_form(self, form: int, search_range: int = 32) -> None:
         """Plain (byte-identical Balanced), full-search or learned analysis of the next calls

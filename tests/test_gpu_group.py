@@ -1,0 +1,99 @@
+"""One persistent launch over several contexts of different picture sizes (rg_analyse_gops_group)
+against each context analysed alone (rg_analyse_gops_device), GPU tests.
+
+The batched configuration transcodes many independent streams of several sizes; the group call
+analyses all of them in one launch whose work list interleaves the sizes' segments by key. It must
+not change a single decision: every record and every reconstruction of every context equals the one
+the same context gives alone, over two calls in a row (the second continuing each GOP from the
+reference the first left), in the plain form (with a QP per stream) and in the full-search form.
+"""
+import numpy as np
+import pytest
+
+from ragdoll_b200.synth import grating_clip
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(160, 96, 3), (96, 64, 2), (208, 80, 1)]   # width, height, streams
+F = 3                                               # pictures per call
+
+
+def _clips():
+    return [[grating_clip(w, h, 2 * F, seed=700 + 10 * i + s, motion=6.0, rects=2) for s in range(S)]
+            for i, (w, h, S) in enumerate(SIZES)]
+
+
+def _engines(form, qps):
+    from ragdoll_b200.engine import RG_PROFILE_MAIN, Engine
+    engs = []
+    for i, (w, h, S) in enumerate(SIZES):
+        e = Engine(w, h, 28, profile=RG_PROFILE_MAIN, num_streams=S, max_frames=F)
+        if form:
+            e.set_analysis_form(form, 16)
+        for s in range(S):
+            e.set_stream_qp(s, qps[i][s])
+        engs.append(e)
+    return engs
+
+
+def _call_args(clips, call):
+    """Device planes ([f][s][y,u,v]) and kinds of every context for call `call` (0: IDR + P, 1: P)."""
+    import torch
+    from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P
+    keep, planes, kinds, sy, suv = [], [], [], [], []
+    for i, (w, h, S) in enumerate(SIZES):
+        cw = (w + 1) // 2
+        p, k = [], []
+        for f in range(F):
+            for s in range(S):
+                for plane in clips[i][s][call * F + f]:
+                    t = torch.from_numpy(np.ascontiguousarray(plane)).cuda()
+                    keep.append(t)
+                    p.append(t.data_ptr())
+                k.append(RG_FRAME_IDR if call == 0 and f == 0 else RG_FRAME_P)
+        planes.append(p)
+        kinds.append(k)
+        sy.append(w)
+        suv.append(cw)
+    return keep, planes, kinds, sy, suv
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_group_launch_equals_each_context_alone(form):
+    import torch
+
+    from ragdoll_b200.engine import Engine
+    rng = np.random.default_rng(form)
+    qps = [rng.integers(20, 37, S).tolist() for _, _, S in SIZES]
+    clips = _clips()
+    group = _engines(form, qps)
+    alone = _engines(form, qps)
+    for call in range(2):
+        keep, planes, kinds, sy, suv = _call_args(clips, call)
+        Engine.analyse_gops_group(group, planes, sy, suv, kinds, F)
+        for i, e in enumerate(alone):
+            e.analyse_gops_device(planes[i], sy[i], suv[i], kinds[i], F)
+        torch.cuda.synchronize()
+        for i, (w, h, S) in enumerate(SIZES):
+            got = group[i].records_gops(F)
+            want = alone[i].records_gops(F)
+            assert got.tobytes() == want.tobytes(), f"call {call}, size {w}x{h}: records differ"
+            for s in range(S):
+                for a, b in zip(group[i].recon(s), alone[i].recon(s)):
+                    assert np.array_equal(a, b), f"call {call}, size {w}x{h}, stream {s}: reconstruction differs"
+        del keep
+    for e in group + alone:
+        e.close()
+
+
+def test_group_launch_rejects_mixed_forms_and_duplicates():
+    from ragdoll_b200.engine import RG_FORM_FULLSEARCH, RG_PROFILE_MAIN, Engine, RgError
+    a = Engine(96, 64, 28, profile=RG_PROFILE_MAIN, max_frames=1)
+    b = Engine(64, 48, 28, profile=RG_PROFILE_MAIN, max_frames=1)
+    b.set_analysis_form(RG_FORM_FULLSEARCH, 8)
+    with pytest.raises(RgError):
+        Engine.analyse_gops_group([a, b], [[0] * 3, [0] * 3], [96, 64], [48, 32], [[0], [0]], 1)
+    with pytest.raises(RgError):
+        Engine.analyse_gops_group([a, a], [[0] * 3, [0] * 3], [96, 96], [48, 48], [[0], [0]], 1)
+    a.close()
+    b.close()
