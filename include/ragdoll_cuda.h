@@ -188,8 +188,9 @@ int rg_analyse_gops_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t
 /*
  * rg_analyse_gops_device for n contexts of different picture sizes (1..8 contexts on one device,
  * all in the plain form or all in the full-search form) in ONE persistent launch: the work lists
- * of the contexts (each with its own lag; the segment length and SM roles of ctxs[0]) merged in
- * key order, so macroblocks of every size share the SMs. dev_planes[i], stride_y[i], stride_uv[i],
+ * of the contexts (each with its own lag) merged in key order, so macroblocks of every size share
+ * the SMs; the segment length, SM roles and wait limit of the context with the most macroblocks
+ * (rg_set_pipeline_tuning), the largest grid of any. dev_planes[i], stride_y[i], stride_uv[i],
  * kinds[i]: context i's arguments as rg_analyse_gops_device takes them; `frames` pictures of every
  * stream of every context. Queued on ctxs[0]'s stream; each context's later calls wait for it,
  * and each context resolves its part as its own pending call (a wait that gave up re-runs that

@@ -770,12 +770,21 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
         gop_desc(c, L->g_hstreams[desc_base[i] + f * c->S + s], f, s, dev_planes[i], kinds[i], c->recs, nullptr, i,
                  desc_base[i], rows_base[i]);
   }
-  // work list: each context's own (the leader's segment length, each context's lag), merged by key
-  // queue by queue; rebuilt only when the shape, the lags or the picture kinds change
-  const int seg = L->seg, a = seg > 2 ? seg : 2;
-  const int split = L->deblock_sms > 0 && L->grid >= 2 ? 1 : 0;
-  const bool intra_q = L->intra_sms > 0 && L->grid >= 3;
-  std::vector<int64_t> shape = {frames, seg, split, intra_q ? 1 : 0, n};
+  // launch shape: the segment length and SM roles of the context with the most macroblocks (its
+  // tuning suits the bulk of the work), the largest grid of any
+  const rg_ctx* T = L;
+  int grid = 0;
+  for (int i = 0; i < n; i++) {
+    const rg_ctx* c = ctxs[i];
+    if ((long)c->n_mb * c->S > (long)T->n_mb * T->S) T = c;
+    grid = std::max(grid, c->grid);
+  }
+  // work list: each context's own (that segment length, each context's lag), merged by key queue
+  // by queue; rebuilt only when the shape, the lags or the picture kinds change
+  const int seg = T->seg, a = seg > 2 ? seg : 2;
+  const int split = T->deblock_sms > 0 && grid >= 2 ? 1 : 0;
+  const bool intra_q = T->intra_sms > 0 && grid >= 3;
+  std::vector<int64_t> shape = {frames, seg, split, intra_q ? 1 : 0, n, grid};
   for (int i = 0; i < n; i++) {
     rg_ctx* c = ctxs[i];
     const int lag = c->lag > 0 ? c->lag : a * (4 + c->reach_y) + seg + c->reach_x + 3;
@@ -846,7 +855,7 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     *(volatile int*)c->pend[pslot[i]].h_err = 0;
   }
   launch_pipeline(fg, L->g_dstreams, n_desc, total_rows, L->g_counters, L->g_dtasks, L->g_ntasks, L->g_qbeg, L->g_qend,
-                  L->deblock_sms, L->intra_sms, L->sms, seg, L->grid, L->timeout_ns, nullptr, 0, nullptr, nullptr,
+                  T->deblock_sms, T->intra_sms, L->sms, seg, grid, T->timeout_ns, nullptr, 0, nullptr, nullptr,
                   L->stream, L->form != RG_FORM_PLAIN);
   CK(cudaGetLastError());
   // every context gets the launch's error word and reach as its own pending call, resolved (and if
