@@ -809,14 +809,21 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
       total += lists[i].size();
     }
     L->g_htasks.resize(total);
+    // on equal keys the context with more macroblocks first: its pictures are the longest chains
+    // (64 streams of four sizes, 30 pictures each: 263 ms against 364 ms with the smallest first)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+      return (long)ctxs[x]->n_mb * ctxs[x]->S > (long)ctxs[y]->n_mb * ctxs[y]->S;
+    });
     size_t at = 0;
     for (int q = 0; q < kPipeQueues; q++) {
       L->g_qbeg[q] = (int)at;
       std::vector<int> pos(n);
       for (int i = 0; i < n; i++) pos[i] = qb[i][q];
-      while (true) {  // the least key first, the lower context on ties
+      while (true) {  // the least key first
         int best = -1;
-        for (int i = 0; i < n; i++)
+        for (int i : order)
           if (pos[i] < qe[i][q] && (best < 0 || keys[i][pos[i]] < keys[best][pos[best]])) best = i;
         if (best < 0) break;
         int2 t = lists[best][pos[best]++];
