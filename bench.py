@@ -488,8 +488,22 @@ def run_learned(args, rank, world, local):
         for field in ("part_mask", "mv_off", "i4_mask"):
             h[field] = fixed[field]
         prior_of[i] = torch.from_numpy(h.view(np.uint8)).to(f"cuda:{local}")
+    # one partition type per macroblock: the network's best against 16x16 always
+    net.set_hint_policy(1)
+    hints1, _ = hints_for(net, [base + i * fbytes for i in idx], [base + i * fbytes for i in prev], W, H, W)
+    net.set_hint_policy()
+    hint1_of = {i: hints1[k] for k, i in enumerate(idx)}
+    fixed1 = prior_hints(n_mb, part_order=(0,))
+    prior1_of = {}
+    torch.cuda.synchronize()
+    for i in idx:
+        h = hint1_of[i].cpu().numpy().view(HINT_DTYPE).copy()
+        for field in ("part_mask", "mv_off", "i4_mask"):
+            h[field] = fixed1[field]
+        prior1_of[i] = torch.from_numpy(h.view(np.uint8)).to(f"cuda:{local}")
     forms = {"plain": RG_FORM_PLAIN, "fullsearch": RG_FORM_FULLSEARCH, "learned": RG_FORM_LEARNED,
-             "no_net": RG_FORM_LEARNED}
+             "no_net": RG_FORM_LEARNED, "learned_top1": RG_FORM_LEARNED, "no_net_top1": RG_FORM_LEARNED}
+    hints_by_form = {"learned": hint_of, "no_net": prior_of, "learned_top1": hint1_of, "no_net_top1": prior1_of}
     torch.cuda.synchronize()
 
     # network inference alone: the 120 pictures' hints
@@ -511,12 +525,13 @@ def run_learned(args, rank, world, local):
     # 1. speed at QP 26: persistent launches, sources resident
     speed = {}
     for name, form in forms.items():
-        if name == "no_net":
+        if name.startswith("no_net"):
             continue
         eng = Engine(W, H, QP, profile=RG_PROFILE_HIGH, num_streams=gops, device=local, max_frames=GOP)
         if form != RG_FORM_PLAIN:
             eng.set_analysis_form(form, 32)
         if form == RG_FORM_LEARNED:
+            net.set_hint_policy(1 if name == "learned_top1" else 3)
             eng.set_hint_net(net)   # each launch first runs the network on its own sources
         stream = torch.cuda.ExternalStream(eng.cuda_stream, device=f"cuda:{local}")
         ptrs, kinds = [], []
@@ -539,6 +554,8 @@ def run_learned(args, rank, world, local):
         speed[name] = {"frames_per_s": round(FRAMES / (ms / 1000), 2), "ms_per_step": round(ms, 3), "steps": steps}
         eng.close()
 
+    net.set_hint_policy()
+
     # 2. rate and distortion at four QPs (per-picture calls; every access unit written)
     rd = {name: {} for name in forms}
     for qp in QPS:
@@ -553,10 +570,8 @@ def run_learned(args, rank, world, local):
                 ptrs = []
                 for g in range(gops):
                     ptrs += planes(g * GOP + f)
-                if name == "learned":
-                    eng.set_hints_device([hint_of[g * GOP + f].data_ptr() for g in range(gops)])
-                elif name == "no_net":
-                    eng.set_hints_device([prior_of[g * GOP + f].data_ptr() for g in range(gops)])
+                if name in hints_by_form:
+                    eng.set_hints_device([hints_by_form[name][g * GOP + f].data_ptr() for g in range(gops)])
                 eng.analyse_device(ptrs, W, cw, [kind] * gops)
                 recs = eng.records()
                 for g in range(gops):
@@ -572,7 +587,7 @@ def run_learned(args, rank, world, local):
 
     bd = {}
     for a, b in (("plain", "learned"), ("fullsearch", "learned"), ("plain", "fullsearch"), ("fullsearch", "no_net"),
-                 ("no_net", "learned")):
+                 ("no_net", "learned"), ("no_net_top1", "learned_top1"), ("plain", "learned_top1")):
         ra, pa = curve(a)
         rb, pb = curve(b)
         bd[f"{b}_vs_{a}"] = round(bd_rate(ra, pa, rb, pb), 3)

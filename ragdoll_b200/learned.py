@@ -20,6 +20,10 @@ from .engine import (HINT_DTYPE, RG_FORM_FULLSEARCH, RG_FRAME_IDR, RG_FRAME_P, R
                      lib)
 
 WEIGHTS = Path(__file__).resolve().parent / "weights" / "candidate_net.f32"
+# the offset head's weights and biases in the parameter vector (rg_net_params order)
+_C = 32
+OFFSET_HEAD = slice(_C * 2 * 9 + _C + 2 * (_C * _C * 9 + _C) + 4 * _C + 4,
+                    _C * 2 * 9 + _C + 2 * (_C * _C * 9 + _C) + 4 * _C + 4 + 2 * _C + 2)
 N_LOGITS = 150
 # decoding-order 4x4 block -> raster index
 DEC_TO_RASTER = np.array([((b >> 1) & 1) * 4 + (b & 1) + ((b >> 3) & 1) * 8 + ((b >> 2) & 1) * 2 for b in range(16)])
@@ -126,17 +130,31 @@ def labels_from_records(recs: np.ndarray, idr: bool):
 
 
 def generate_training_set(n_clips: int, width: int, height: int, frames: int, search_range: int = 32,
-                          qps=(22, 26, 30, 34), device: int = 0, seed0: int = 50000, streams: int = 8):
-    """Runs the full-search form on seeded clips (each a GOP: IDR + P pictures, `streams` clips per
+                          qps=(22, 26, 30, 34), device: int = 0, seed0: int = 50000, streams: int = 8,
+                          labels: str = "fullsearch"):
+    """Runs a labelling form on seeded clips (each a GOP: IDR + P pictures, `streams` clips per
     pipelined launch, QPs cycling through `qps`) and returns device tensors: crops [N][2][24][24] u8,
-    part [N], i4 [N][16], mv [N][2], mvv [N]."""
+    part [N], i4 [N][16], mv [N][2], mvv [N]. labels "fullsearch": the full-search form's decisions;
+    "learned": the learned form's own search with every candidate open (all four partition types,
+    all nine intra 4x4 modes, the coarse motion vector, no network offset) -- the choices the
+    restricted search is to reproduce."""
     import torch
 
-    from .engine import RG_PROFILE_HIGH, Engine
+    from .engine import RG_FORM_LEARNED, RG_PROFILE_HIGH, Engine
     from .synth import grating_clip
 
+    if labels not in ("fullsearch", "learned"):
+        raise ValueError(f"labels {labels!r}")
     dev = torch.device("cuda", device)
     net = CandidateNet(device)
+    opener = None
+    if labels == "learned":
+        # a network whose hints keep every candidate and offer no offset: only its coarse pass matters
+        opener = CandidateNet(device, seed=1)
+        p = opener.params()
+        p[OFFSET_HEAD] = 0.0
+        opener.set_params(p)
+        opener.set_hint_policy(4, float("inf"), 9, float("inf"))
     crops, parts, i4s, mvs, mvvs = [], [], [], [], []
     cw, ch = (width + 1) // 2, (height + 1) // 2
     for c0 in range(0, n_clips, streams):
@@ -144,7 +162,11 @@ def generate_training_set(n_clips: int, width: int, height: int, frames: int, se
         qp = qps[(c0 // streams) % len(qps)]
         clips = [grating_clip(width, height, frames, seed=seed0 + c0 + s, motion=24.0, rects=12) for s in range(S)]
         eng = Engine(width, height, qp, profile=RG_PROFILE_HIGH, num_streams=S, max_frames=frames, device=device)
-        eng.set_analysis_form(RG_FORM_FULLSEARCH, search_range)
+        if opener is None:
+            eng.set_analysis_form(RG_FORM_FULLSEARCH, search_range)
+        else:
+            eng.set_analysis_form(RG_FORM_LEARNED, search_range)
+            eng.set_hint_net(opener)
         kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(frames)]
         recs = eng.analyse_gops([[clips[s][f] for s in range(S)] for f in range(frames)], kinds)
         eng.close()
@@ -162,6 +184,8 @@ def generate_training_set(n_clips: int, width: int, height: int, frames: int, se
                 parts.append(p); i4s.append(i); mvs.append(m); mvvs.append(v)
         del luma
     net.close()
+    if opener is not None:
+        opener.close()
     t = lambda a: torch.from_numpy(np.concatenate(a)).to(dev)  # noqa: E731
     return torch.cat(crops), t(parts), t(i4s), t(mvs), t(mvvs)
 

@@ -2,9 +2,9 @@
 
     python -m ragdoll_b200.train_net --clips 200 --width 1280 --height 720 --frames 3 --out weights.f32
 
-Training set: the full-search form's decisions (search range --range) on `clips` seeded synthetic
-clips (gratings, +-24 px global motion, 12 moving rectangles; one GOP each: an IDR picture and P
-pictures), QPs cycling through 22 / 26 / 30 / 34 -- every macroblock a sample (its two 24 x 24 luma
+Training set: the full-search form's decisions (search range --range; --labels learned: the
+learned form's own search with every candidate open) on `clips` seeded synthetic clips (gratings,
++-24 px global motion, 12 moving rectangles; one GOP each: an IDR picture and P pictures), QPs cycling through 22 / 26 / 30 / 34 -- every macroblock a sample (its two 24 x 24 luma
 windows and its labels). Then `epochs` of Adam over shuffled batches. Prints one JSON line: sample
 and label counts, loss per epoch and the time of each phase.
 """
@@ -28,6 +28,9 @@ def main(argv=None) -> None:
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--labels", default="fullsearch", choices=["fullsearch", "learned"],
+                    help="decisions trained on: the full search's, or the learned form's search with every "
+                         "candidate open")
     ap.add_argument("--out", required=True)
     args = ap.parse_args(argv)
     sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
@@ -36,7 +39,8 @@ def main(argv=None) -> None:
     from ragdoll_b200.learned import CandidateNet, generate_training_set, train
 
     t0 = time.perf_counter()
-    data = generate_training_set(args.clips, args.width, args.height, args.frames, search_range=args.range)
+    data = generate_training_set(args.clips, args.width, args.height, args.frames, search_range=args.range,
+                                 labels=args.labels)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     net = CandidateNet(0, seed=args.seed)
@@ -49,7 +53,8 @@ def main(argv=None) -> None:
     counts = {"samples": int(data[0].shape[0]), "partition_labels": int((part >= 0).sum()),
               "partition_histogram": [int((part == k).sum()) for k in range(4)],
               "intra4x4_block_labels": int((data[2] >= 0).sum()), "offset_labels": int(data[4].sum())}
-    print(json.dumps({"train": {"clips": args.clips, "size": f"{args.width}x{args.height}", "frames": args.frames,
+    print(json.dumps({"train": {"labels": args.labels, "clips": args.clips, "size": f"{args.width}x{args.height}",
+                                "frames": args.frames,
                                 "search_range": args.range, "epochs": args.epochs, "batch": args.batch, **counts,
                                 "loss_per_epoch": [round(x, 5) for x in losses],
                                 "label_generation_s": round(t1 - t0, 1), "training_s": round(t2 - t1, 1)}}), flush=True)
