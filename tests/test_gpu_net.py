@@ -9,6 +9,8 @@
   (fewer candidates, logit margins) the kept candidates are those of the same rule on the host.
 * The coarse motion pass that follows the network (2:1 decimated exhaustive SAD search) gives the
   vectors of a numpy restatement; IDR pictures get none.
+* What the trained network gains: one intra 4x4 mode per block chosen by it codes IDR pictures in
+  far fewer bits, at a higher PSNR, than any fixed mode or an untrained network's choice.
 * Training on full-search labels lowers the loss.
 * End to end: hints from the network drive the learned form; its records equal the oracle's with
   the same hints, and its CABAC stream decodes (FFmpeg) to the engine's reconstruction.
@@ -200,6 +202,63 @@ def test_coarse_motion_matches_host_restatement(search_range):
     hints, _ = hints_for(net, [tc.data_ptr()], [tp.data_ptr()], w, h, w)
     torch.cuda.synchronize()
     assert (hints[0].cpu().numpy().view(HINT_DTYPE)["flags"] == 0).all()
+
+
+def _idr_bits_psnr(frames, w, h, qp, hints):
+    """Bits (CABAC access units) and luma PSNR of IDR pictures analysed by the learned form with
+    the given device hints (one array per picture)."""
+    from ragdoll_b200.engine import RG_FORM_LEARNED, RG_FRAME_IDR, RG_PROFILE_HIGH, BitstreamWriter, Engine
+    n = len(frames)
+    eng = Engine(w, h, qp, profile=RG_PROFILE_HIGH, num_streams=n)
+    eng.set_analysis_form(RG_FORM_LEARNED, 16)
+    eng.set_hints_device([x.data_ptr() for x in hints])
+    eng.analyse(list(frames), [RG_FRAME_IDR] * n)
+    recs = eng.records()
+    bits, sse = 0, 0.0
+    for s in range(n):
+        bits += 8 * len(BitstreamWriter(w, h, qp, profile=RG_PROFILE_HIGH).picture(recs[s], RG_FRAME_IDR))
+        sse += float(((eng.recon(s)[0].astype(np.int64) - frames[s][0].astype(np.int64)) ** 2).sum())
+    eng.close()
+    return bits, 10 * np.log10(65025.0 * w * h * n / max(sse, 1.0))
+
+
+def test_trained_network_gains_over_fixed_intra_modes():
+    """What the trained network gains: with ONE intra 4x4 mode tried per block, the trained network's
+    mode codes the IDR pictures in far fewer bits at a higher PSNR than any fixed mode (DC, V or H
+    everywhere) and than an untrained network's mode -- and within a few per cent of trying all
+    nine modes. (Measured at 320x192: 0.82x the bits of the best fixed mode, +0.8 dB.)"""
+    import torch
+
+    from ragdoll_b200.engine import HINT_DTYPE
+    from ragdoll_b200.learned import WEIGHTS, CandidateNet, hints_for
+    if not WEIGHTS.exists():
+        pytest.skip("no trained weights")
+    w, h, qp = 320, 192, 26
+    frames = [grating_clip(w, h, 1, seed=9100 + s, motion=0.0, rects=6)[0] for s in range(2)]
+    luma = [torch.from_numpy(np.ascontiguousarray(f[0])).cuda() for f in frames]
+    n_mb = ((w + 15) // 16) * ((h + 15) // 16)
+
+    def network(net):
+        net.set_hint_policy(3, float("inf"), 1, float("inf"))
+        hs, _ = hints_for(net, [l.data_ptr() for l in luma], [l.data_ptr() for l in luma], w, h, w)
+        net.check()
+        torch.cuda.synchronize()
+        return hs
+
+    def fixed(mask):
+        a = np.zeros(n_mb, HINT_DTYPE)
+        a["part_mask"] = 15
+        a["i4_mask"] = mask
+        t = torch.from_numpy(a.view(np.uint8)).cuda()
+        return [t] * len(frames)
+
+    trained = _idr_bits_psnr(frames, w, h, qp, network(CandidateNet.trained(0)))
+    untrained = _idr_bits_psnr(frames, w, h, qp, network(CandidateNet(0, params=_params(11))))
+    every = _idr_bits_psnr(frames, w, h, qp, fixed(0x1FF))
+    for name, other in [("untrained", untrained)] + [(m, _idr_bits_psnr(frames, w, h, qp, fixed(1 << k)))
+                                                     for m, k in (("V", 0), ("H", 1), ("DC", 2))]:
+        assert trained[0] < 0.92 * other[0] and trained[1] > other[1], (name, trained, other)
+    assert trained[0] < 1.05 * every[0] and trained[1] > every[1] - 0.5, (trained, every)
 
 
 def test_training_on_full_search_labels_lowers_the_loss():
