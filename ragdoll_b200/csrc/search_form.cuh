@@ -32,9 +32,6 @@ constexpr int kBandBytes = (kBandRows + 15) * (2 * kMaxSearchRange + 28);
 constexpr int kLearnedRange = 2;           // learned form: integer window around the seed
 constexpr int kCentreCands = 7;            // learned form: candidates of the window's centre
 
-struct SearchSmem {
-  uint8_t band[kBandBytes];
-};
 
 // A neighbouring 4x4 block for motion prediction: ref -2 not available, -1 intra, 0 inter.
 struct NbMv {
@@ -47,6 +44,16 @@ struct MbNb {
   int b[2][2];   // top macroblock: quadrants 2 (columns 0-1) and 3 (columns 2-3)
   int cc[2];     // top-right macroblock: quadrant 2
   int d[2];      // top-left macroblock: quadrant 3
+};
+struct IntBest {
+  int x[9], y[9];
+  uint32_t c[9];
+};
+struct SearchSmem {
+  uint8_t band[kBandBytes];
+  IntBest ib;
+  MbNb nb;
+  int bmv[4][2], bmvd[4][2], own[4][2], pm[4][2], pd[4][2], qmv[4][2];
 };
 __device__ __forceinline__ void ld_q(const MbMv4* m, int q, int* v) {
   uint32_t w = ((const uint32_t*)m)[q];
@@ -129,10 +136,6 @@ __device__ __forceinline__ uint32_t vec_cost(int dx, int dy, uint32_t lambda) {
 // rows of 8 vector rows (band) are staged in shared memory, and each lane slides its column's
 // 16 x 16 comparison down the band, a reference row at a time against the source rows it pairs
 // with. best_x / best_y / best_c: the nine parts' results (identical in every lane).
-struct IntBest {
-  int x[9], y[9];
-  uint32_t c[9];
-};
 __device__ __forceinline__ uint32_t lds4u(const uint8_t* p) {
   uintptr_t a = (uintptr_t)p;
   const uint32_t* b = (const uint32_t*)(a & ~(uintptr_t)3);
@@ -586,7 +589,12 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   bd.max0 = 4 * (cw - 16 - x0 + 28);
   bd.max1 = min(4 * (chh - 16 - y0 + 28), 2044);
   const int imin0 = (bd.min0 + 3) >> 2, imin1 = (bd.min1 + 3) >> 2, imax0 = bd.max0 >> 2, imax1 = bd.max1 >> 2;
-  const MbNb nb = load_nb(c);
+  // Warp-uniform state (every lane computes the same values) is held once per warp in shared memory
+  // (SearchSmem) instead of once per lane on the stack; every lane writes the same value, and a
+  // __syncwarp before each rewrite keeps a lane from overwriting what a slower lane still reads.
+  MbNb& nb = ss.nb;
+  __syncwarp();
+  nb = load_nb(c);
   int none[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   int mvp16[2];
   mv_pred(nb, 0, 0, 4, 0, none, 0, mvp16);
@@ -648,7 +656,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
     ylo = max(lcy - kLearnedRange, imin1);
     yhi = min(lcy + kLearnedRange, imax1);
   }
-  IntBest ib;
+  IntBest& ib = ss.ib;  // warp-uniform: once per warp in shared memory
   int_search(c, sm, ss, xlo, xhi, ylo, yhi, mvp16[0], mvp16[1], lambda, ib);
   if (hint) {
     bool edge = (ib.x[0] == xlo && xlo > imin0) || (ib.x[0] == xhi && xhi < imax0) ||
@@ -674,14 +682,18 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   // 3-4. refinement of every tried type, the least total cost wins
   int best_t = -1;
   uint32_t best_j = UMAX;
-  int bmv[4][2], bmvd[4][2];  // per part (coding order) of the best type
+  int (&bmv)[4][2] = ss.bmv;  // per part (coding order) of the best type (warp-uniform, shared)
+  int (&bmvd)[4][2] = ss.bmvd;
   WinState ws{kNoWin, kNoWin};  // the skip probe's window is not a refinement window
   for (int t = 0; t < 4; t++) {
     if (!((part_mask >> t) & 1)) continue;
-    int own[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    int (&own)[4][2] = ss.own;
+    __syncwarp();
+    for (int q = 0; q < 4; q++) own[q][0] = own[q][1] = 0;
     int done = 0;
     uint32_t J = lambda * (uint32_t)sd.type_bits[t];
-    int pm[4][2], pd[4][2];
+    int (&pm)[4][2] = ss.pm;
+    int (&pd)[4][2] = ss.pd;
     const int first = c_type_first[t], np = c_type_parts[t];
     for (int k = 0; k < np; k++) {
       const int8_t* g = c_parts[first + k];
@@ -707,7 +719,8 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
     }
   }
   // quadrant vectors of the chosen type and its prediction
-  int qmv[4][2];
+  int (&qmv)[4][2] = ss.qmv;
+  __syncwarp();
   {
     const int first = c_type_first[best_t], np = c_type_parts[best_t];
     for (int k = 0; k < np; k++) {
