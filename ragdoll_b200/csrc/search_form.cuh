@@ -54,6 +54,8 @@ struct SearchSmem {
   IntBest ib;
   MbNb nb;
   int bmv[4][2], bmvd[4][2], own[4][2], pm[4][2], pd[4][2], qmv[4][2];
+  int ccx[8], ccy[8];  // the learned form's centre candidates (ok: cok)
+  bool cok[8];
 };
 __device__ __forceinline__ void ld_q(const MbMv4* m, int q, int* v) {
   uint32_t w = ((const uint32_t*)m)[q];
@@ -102,24 +104,26 @@ __device__ __forceinline__ NbMv nb4(const MbNb& n, int bx, int by, const int (*o
 }
 // Motion vector predictor of the partition whose top-left 4x4 block is (bx, by) and width pw (4x4
 // units), H.264 8.4.1.3; dir 1 16x8 top, 2 16x8 bottom, 3 8x16 left, 4 8x16 right, 0 median only.
-__device__ __noinline__ void mv_pred(const MbNb& n, int bx, int by, int pw, int dir, const int (*own)[2], int done,
-                                     int* mvp) {
+__device__ __noinline__ int2 mv_pred(const MbNb& n, int bx, int by, int pw, int dir, const int (*own)[2], int done) {
   NbMv A = nb4(n, bx - 1, by, own, done), B = nb4(n, bx, by - 1, own, done), C = nb4(n, bx + pw, by - 1, own, done);
   if (C.ref == -2) C = nb4(n, bx - 1, by - 1, own, done);
-  if (dir == 1 && B.ref == 0) { mvp[0] = B.x; mvp[1] = B.y; return; }
-  if ((dir == 2 || dir == 3) && A.ref == 0) { mvp[0] = A.x; mvp[1] = A.y; return; }
-  if (dir == 4 && C.ref == 0) { mvp[0] = C.x; mvp[1] = C.y; return; }
-  if (B.ref == -2 && C.ref == -2 && A.ref != -2) { mvp[0] = A.x; mvp[1] = A.y; return; }
+  if (dir == 1 && B.ref == 0) return make_int2(B.x, B.y);
+  if ((dir == 2 || dir == 3) && A.ref == 0) return make_int2(A.x, A.y);
+  if (dir == 4 && C.ref == 0) return make_int2(C.x, C.y);
+  if (B.ref == -2 && C.ref == -2 && A.ref != -2) return make_int2(A.x, A.y);
   int m = (A.ref == 0) + (B.ref == 0) + (C.ref == 0);
   if (m == 1) {
     const NbMv& o = A.ref == 0 ? A : (B.ref == 0 ? B : C);
-    mvp[0] = o.x; mvp[1] = o.y;
-    return;
+    return make_int2(o.x, o.y);
   }
   auto med = [](int x, int y, int z) { return min(max(x, y), max(min(x, y), z)); };
-  mvp[0] = med(A.x, B.x, C.x);
-  mvp[1] = med(A.y, B.y, C.y);
+  return make_int2(med(A.x, B.x, C.x), med(A.y, B.y, C.y));
 }
+// A refined part: its cost and quarter-sample vector.
+struct PartFit {
+  uint32_t cost;
+  int x, y;
+};
 
 struct Bounds {
   int min0, min1, max0, max1;  // quarter samples (MvBounds, enc.rs:1105)
@@ -322,8 +326,8 @@ __device__ __forceinline__ void ensure_window(const Ctx& c, Smem& sm, WinState& 
   ws.by = by;
 }
 
-__device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
-                                             int by, const int* mvp, uint32_t lambda, const Bounds& bd, int* mv) {
+__device__ __noinline__ PartFit refine_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
+                                            int by, int2 mvp, uint32_t lambda, Bounds bd) {
   const int lane = lane_id();
   ensure_window(c, sm, ws, bx, by);
   const int bw4 = pw >> 2, nblk = bw4 * (ph >> 2);
@@ -356,7 +360,7 @@ __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& w
       for (int o = 1; o < nblk; o <<= 1) s += __shfl_xor_sync(FULL, s, o);
       uint32_t k = UMAX;
       if (ok && blk == 0) {
-        uint32_t cost = (s >> 1) + vec_cost(vx - mvp[0], vy - mvp[1], lambda);
+        uint32_t cost = (s >> 1) + vec_cost(vx - mvp.x, vy - mvp.y, lambda);
         k = (cost << 4) | (uint32_t)(step == 0 ? cand : cand + 1);
       }
       key = min(key, __reduce_min_sync(FULL, k));
@@ -371,9 +375,7 @@ __device__ __noinline__ uint32_t refine_part(const Ctx& c, Smem& sm, WinState& w
     }
     best_key = (key & ~15u);
   }
-  mv[0] = cx;
-  mv[1] = cy;
-  return best_key >> 4;
+  return PartFit{best_key >> 4, cx, cy};
 }
 
 // Learned form: refinement of one part from its integer best (bx, by) by SAD -- the half-sample
@@ -394,36 +396,33 @@ __device__ __noinline__ uint32_t part_sad(const Smem& sm, int px, int py, int pw
   }
   return wsum(s);
 }
-__device__ __noinline__ uint32_t refine_part_sad(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph,
-                                                 int bx, int by, const int* mvp, uint32_t lambda, const Bounds& bd,
-                                                 int* mv) {
+__device__ __noinline__ PartFit refine_part_sad(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph,
+                                                int bx, int by, int2 mvp, uint32_t lambda, Bounds bd) {
   ensure_window(c, sm, ws, bx, by);
   int cx = 4 * bx, cy = 4 * by;
-  uint32_t best = part_sad(sm, px, py, pw, ph, bx, by, cx, cy) + vec_cost(cx - mvp[0], cy - mvp[1], lambda);
+  uint32_t best = part_sad(sm, px, py, pw, ph, bx, by, cx, cy) + vec_cost(cx - mvp.x, cy - mvp.y, lambda);
   for (int st = 2; st >= 1; st--) {
     for (int it = 0; it < (st == 2 ? 1 : 2); it++) {
       const int fx = cx, fy = cy;
       for (int k = 0; k < 4; k++) {
         const int vx = fx + (k == 1 ? -st : (k == 2 ? st : 0)), vy = fy + (k == 0 ? -st : (k == 3 ? st : 0));
         if (abs(vx - 4 * bx) > 3 || abs(vy - 4 * by) > 3 || !in_bounds(bd, vx, vy)) continue;  // uniform
-        const uint32_t cost = part_sad(sm, px, py, pw, ph, bx, by, vx, vy) + vec_cost(vx - mvp[0], vy - mvp[1], lambda);
+        const uint32_t cost = part_sad(sm, px, py, pw, ph, bx, by, vx, vy) + vec_cost(vx - mvp.x, vy - mvp.y, lambda);
         if (cost < best) { best = cost; cx = vx; cy = vy; }
       }
       if (cx == fx && cy == fy) break;
     }
   }
-  mv[0] = cx;
-  mv[1] = cy;
-  return best;
+  return PartFit{best, cx, cy};
 }
 
 // The luma prediction of a part at quarter-sample vector mv (within 3 quarter samples of 4 (bx, by),
 // the integer vector its refinement started from) into pred_y.
 __device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
-                                          int by, const int* mv) {
+                                          int by, int mvx, int mvy) {
   const int lane = lane_id();
   ensure_window(c, sm, ws, bx, by);
-  QSrc q = qpel_src(sm, (mv[0] >> 2) - bx + 1 + px, (mv[1] >> 2) - by + 1 + py, mv[0] & 3, mv[1] & 3);
+  QSrc q = qpel_src(sm, (mvx >> 2) - bx + 1 + px, (mvy >> 2) - by + 1 + py, mvx & 3, mvy & 3);
   for (int i = lane; i < pw * ph; i += 32) {
     const int r = i / pw, x = i - r * pw;
     int v = q.a[r * q.sa + x];
@@ -596,8 +595,8 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   __syncwarp();
   nb = load_nb(c);
   int none[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  int mvp16[2];
-  mv_pred(nb, 0, 0, 4, 0, none, 0, mvp16);
+  const int2 p16 = mv_pred(nb, 0, 0, 4, 0, none, 0);
+  const int mvp16[2] = {p16.x, p16.y};
   int ps0 = mvp16[0], ps1 = mvp16[1];
   {
     NbMv A = nb4(nb, -1, 0, none, 0), B = nb4(nb, 0, -1, none, 0);
@@ -614,8 +613,9 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
   int xlo = max(fcx - R, imin0), xhi = min(fcx + R, imax0), ylo = max(fcy - R, imin1), yhi = min(fcy + R, imax1);
   int part_mask = 15;
   // learned: the candidates of the first window's centre (integer, clamped to the bounds)
-  int ccx[kCentreCands], ccy[kCentreCands];
-  bool cok[kCentreCands];
+  int* ccx = ss.ccx;  // warp-uniform, in shared memory
+  int* ccy = ss.ccy;
+  bool* cok = ss.cok;
   if (hint) {
     NbMv A = nb4(nb, -1, 0, none, 0), B = nb4(nb, 0, -1, none, 0), C = nb4(nb, 4, -1, none, 0);
     if (C.ref == -2) C = nb4(nb, -1, -1, none, 0);
@@ -697,13 +697,13 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
     const int first = c_type_first[t], np = c_type_parts[t];
     for (int k = 0; k < np; k++) {
       const int8_t* g = c_parts[first + k];
-      int mvp[2], mv[2];
-      mv_pred(nb, g[4], g[5], g[6], g[7], own, done, mvp);
-      uint32_t cost = hint ? refine_part_sad(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv)
-                           : refine_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd, mv);
-      J += cost;
+      const int2 mvp = mv_pred(nb, g[4], g[5], g[6], g[7], own, done);
+      const PartFit fit = hint ? refine_part_sad(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd)
+                               : refine_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], mvp, lambda, bd);
+      const int mv[2] = {fit.x, fit.y};
+      J += fit.cost;
       pm[k][0] = mv[0]; pm[k][1] = mv[1];
-      pd[k][0] = mv[0] - mvp[0]; pd[k][1] = mv[1] - mvp[1];
+      pd[k][0] = mv[0] - mvp.x; pd[k][1] = mv[1] - mvp.y;
       const int qm = c_part_quads[first + k];
       for (int q = 0; q < 4; q++)
         if ((qm >> q) & 1) { own[q][0] = mv[0]; own[q][1] = mv[1]; }
@@ -728,7 +728,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
       for (int q = 0; q < 4; q++)
         if ((qm >> q) & 1) { qmv[q][0] = bmv[k][0]; qmv[q][1] = bmv[k][1]; }
       const int8_t* g = c_parts[first + k];
-      predict_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], bmv[k]);
+      predict_part(c, sm, ws, g[0], g[1], g[2], g[3], ib.x[g[8]], ib.y[g[8]], bmv[k][0], bmv[k][1]);
     }
   }
   // 5. intra 16x16 when the inter prediction is poor (the plain form's rule, enc.rs:3121-3156)
