@@ -149,15 +149,23 @@ struct InferParams {
 
 // The candidates of n logits as a bit mask: the best, then the next ones in logit order (the lower
 // index on ties) up to k in all, each only while its logit is at least the best's minus `margin`.
-__device__ __forceinline__ uint32_t topk_mask(const float* l, int n, int k, float margin) {
+template <int N>
+__device__ __forceinline__ uint32_t topk_mask(const float (&l)[N], int k, float margin) {
   uint32_t m = 0;
   float top = 0.0f;
-  for (int r = 0; r < k; r++) {
+#pragma unroll
+  for (int r = 0; r < N; r++) {
+    if (r >= k) break;
     int best = -1;
-    for (int i = 0; i < n; i++)
-      if (!((m >> i) & 1) && (best < 0 || l[i] > l[best])) best = i;
-    if (r == 0) top = l[best];
-    else if (l[best] < top - margin) break;
+    float bv = 0.0f;
+#pragma unroll
+    for (int i = 0; i < N; i++)  // constant indices: the logits stay in registers
+      if (!((m >> i) & 1) && (best < 0 || l[i] > bv)) {
+        best = i;
+        bv = l[i];
+      }
+    if (r == 0) top = bv;
+    else if (bv < top - margin) break;
     m |= 1u << best;
   }
   return m;
@@ -361,6 +369,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) cnn_infer_kernel(InferPa
           const int b = tid % 16;
           const float* f = ms.pool[j][1 + b];
           float li[9];
+#pragma unroll
           for (int o = 0; o < 9; o++) {
             float s = H[kBi - kWp + o];
             for (int c = 0; c < C; c++) s += H[kWi - kWp + o * C + c] * f[c];
@@ -369,12 +378,13 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) cnn_infer_kernel(InferPa
           // 4x4 block b in raster order; the hint holds decoding order
           const int bx = b & 3, by = b >> 2;
           const int dec = ((by >> 1) << 3) | ((bx >> 1) << 2) | ((by & 1) << 1) | (bx & 1);
-          jb.hints[m].i4_mask[dec] = (uint16_t)topk_mask(li, 9, ip.i4_k, ip.i4_margin);
+          jb.hints[m].i4_mask[dec] = (uint16_t)topk_mask(li, ip.i4_k, ip.i4_margin);
           if (lg)
             for (int o = 0; o < 9; o++) lg[6 + b * 9 + o] = li[o];
         } else {
           const float* g = ms.pool[j][0];
           float lp[4], lm[2];
+#pragma unroll
           for (int o = 0; o < 4; o++) {
             float s = H[kBp - kWp + o];
             for (int c = 0; c < C; c++) s += H[o * C + c] * g[c];
@@ -386,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) cnn_infer_kernel(InferPa
             lm[o] = s;
           }
           rg_mb_hint& hh = jb.hints[m];
-          hh.part_mask = (uint8_t)topk_mask(lp, 4, ip.part_k, ip.part_margin);
+          hh.part_mask = (uint8_t)topk_mask(lp, ip.part_k, ip.part_margin);
           hh.flags = 0;  // the coarse motion pass, when on, follows
           hh.mv_coarse[0] = hh.mv_coarse[1] = 0;
           for (int o = 0; o < 2; o++) hh.mv_off[o] = (int8_t)max(-127, min(127, __float2int_rn(16.0f * lm[o])));
