@@ -204,6 +204,14 @@ BATCH_STREAMS, BATCH_FRAMES, BATCH_WAVE = 16, 30, 10
 
 
 def run_batched(args, rank, world, local):
+    """--workload batched: measure_batched's line."""
+    if rank != 0:
+        return
+    line = measure_batched(args, local)
+    print(json.dumps(line), flush=True)
+
+
+def measure_batched(args, local):
     """The batched-streams configuration: 64 concurrent streams, 16 each at 320x240, 640x360,
     1280x720 and 1920x1080, 30 frames each (one GOP: IDR + 29 P) from independent seeds, Main
     profile (CABAC), a QP drawn uniformly from 20..36 per stream, Balanced analysis. One encoder
@@ -220,8 +228,6 @@ def run_batched(args, rank, world, local):
     from ragdoll_b200.engine import RG_FRAME_IDR, RG_FRAME_P, RG_PROFILE_MAIN
     from ragdoll_b200.synth import grating_clip
 
-    if rank != 0:
-        return
     torch.cuda.set_device(local)
     rng = np.random.default_rng(4)
     cores = os.cpu_count() or 1
@@ -313,9 +319,9 @@ def run_batched(args, rank, world, local):
         "clocks": clk,
         "gpu_launches": args.steps * len(jobs) * (BATCH_FRAMES // BATCH_WAVE) * 2,
     }
-    print(json.dumps(line), flush=True)
     for j in jobs:
         j["enc"].close()
+    return line
 
 
 def batched_one_launch(args, local, jobs):
@@ -360,7 +366,7 @@ def batched_one_launch(args, local, jobs):
     out = {}
     steps = max(1, min(args.steps, 4))
     for name, fn in (("one_launch", group), ("launch_per_size", separate)):
-        for _ in range(max(args.warmup, 1)):
+        for _ in range(max(args.warmup, 3)):   # the work order settles (observed reach) and the graphs are captured
             fn()
         for e in engs:
             e.sync()
@@ -383,8 +389,14 @@ def batched_one_launch(args, local, jobs):
         out[name] = {"frames_per_s": round(len(jobs) * BATCH_STREAMS * BATCH_FRAMES / (ms / 1000), 1),
                      "ms_per_step": round(ms, 3), "wall_ms_per_step": round((time.perf_counter() - t0) * 1000 / steps, 3)}
     out["steps"] = steps
+    import ctypes
+    from ragdoll_b200.engine import lib
+    cap, lau = ctypes.c_int64(), ctypes.c_int64()
+    lib().rg_group_graph_counts(engs[0].h, ctypes.byref(cap), ctypes.byref(lau))
+    out["one_launch"]["cuda_graph"] = {"captures": cap.value, "graph_launches": lau.value}
     out["what"] = ("device step of all 1920 pictures (64 streams x 30) with sources resident: one "
-                   "rg_analyse_gops_group launch vs the four contexts' launches on four streams")
+                   "rg_analyse_gops_group launch (a CUDA graph replayed per call) vs the four contexts' "
+                   "launches on four streams")
     for e in engs:
         e.close()
     return out
@@ -831,8 +843,9 @@ def measure_learned(args, local, dist, base, fbytes, planes, gops, frames_host, 
             out_bytes += sum(len(au) for row in enc.collect() for au in row)
     out_bytes += sum(len(au) for row in enc.collect() for au in row)
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / steps, dist, f"cuda:{local}")
+    rec_bytes = enc.record_bytes()
     enc.close()
-    out = {"step_ms": step_ms, "cnn_ms": cnn_ms, "network_ms": net_ms, "analysis_ms": ana_ms, "e2e_ms": e2e_ms, "steps": steps,
+    out = {"record_bytes_per_step": rec_bytes, "step_ms": step_ms, "cnn_ms": cnn_ms, "network_ms": net_ms, "analysis_ms": ana_ms, "e2e_ms": e2e_ms, "steps": steps,
            "top1_ms": top1_ms, "fullsearch_ms": fs_ms,
            "clocks": clk, "bitstream_bytes_per_step": round(out_bytes / steps), "weights": WEIGHTS.name}
     # 5. rate and distortion (rank 0, outside the timed regions)
@@ -1008,6 +1021,25 @@ def run_engine(args, rank, world, local):
     out_bytes += sum(len(au) for row in last_aus for au in row)
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps, dist, f"cuda:{local}")
     enc_threads = enc.threads
+    rec_bytes = enc.record_bytes()
+    # the same with compact records written by the launch into mapped host memory (opt-in), for
+    # comparison
+    enc.set_record_compaction(96)
+    for _ in range(2):
+        enc.new_gops()
+        enc.submit(frames_host)
+    enc.collect()
+    enc.collect()
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        enc.new_gops()
+        enc.submit(frames_host)
+        if k:
+            enc.collect()
+    enc.collect()
+    e2e_compact_ms = max_over_ranks((time.perf_counter() - t0) * 1000 / args.steps, dist, f"cuda:{local}")
+    compact_bytes = enc.record_bytes()
     enc.close()
 
     # the learned form on the same workload (the headline of the line)
@@ -1079,9 +1111,15 @@ def run_engine(args, rank, world, local):
         tpeak = peaks.get("bf16_tflops", 1590.0)
         plain = {
             "value": round(value, 2), "ms_per_step": round(dev_ms, 3), "steps": args.steps,
-            "e2e": {"value": round(e2e, 2), "unit": UNIT, "bitstream_bytes_per_step": round(out_bytes / args.steps),
+            "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
+                    "d2h_bytes_per_step": rec_bytes, "bitstream_bytes_per_step": round(out_bytes / args.steps),
                     "host_threads": enc_threads,
-                    "path": "rg_encoder_submit/collect: copy in, persistent launch, records out, CABAC on the host"},
+                    "path": "rg_encoder_submit/collect: copy in, persistent launch, each picture's records "
+                            "copied out as the launch finishes it, CABAC on the host"},
+            "e2e_compact_records": {"value": round(frames_total / (e2e_compact_ms / 1000), 2), "unit": UNIT,
+                                    "d2h_bytes_per_step": compact_bytes,
+                                    "path": "the same with rg_set_record_compaction(96): compact records written "
+                                            "by the launch into mapped host memory"},
             "e2e_analysis": {"value": round(frames_total / (ana_ms / 1000), 2), "unit": UNIT,
                              "path": "rg_analyse_gops_async: copy in, persistent launch, records out"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
@@ -1100,7 +1138,7 @@ def run_engine(args, rank, world, local):
             "form": {"headline": "learned: network hints, coarse motion, +-2 windows, full search +-32 fallback",
                      "network_weights": learned["weights"], "compared_with": "plain (ragdoll's Balanced decisions)"},
             "e2e": {"value": round(l_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": FRAMES * fbytes,
-                    "d2h_bytes_per_step": GOP * gops * eng.n_mb * RECORD_DTYPE.itemsize,
+                    "d2h_bytes_per_step": learned["record_bytes_per_step"],
                     "bitstream_bytes_per_step": learned["bitstream_bytes_per_step"], "host_threads": enc_threads,
                     "path": "rg_encoder_set_form(learned) + submit/collect: copy in, network and coarse-motion "
                             "launches, persistent analysis launch, records out, CABAC on the host"},
@@ -1137,6 +1175,14 @@ def run_engine(args, rank, world, local):
             # the persistent analysis launch and the one-thread error hand-off
             "gpu_launches": 4 * learned["steps"],
         }
+        if world == 1 and args.batched:
+            # the batched-streams configuration (64 streams of four sizes), two timed steps, beside
+            # the 1080p numbers: its own untimed region, after the 1080p work is done
+            b_args = argparse.Namespace(**vars(args))
+            b_args.steps, b_args.warmup = 2, 1
+            bl = measure_batched(b_args, local)
+            line["batched"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step", "steps", "latency_ms",
+                                                  "one_launch", "per_size", "config", "clocks", "gpu_launches")}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:
@@ -1294,6 +1340,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="leave the batched-streams measurement out of the 1080p line")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched workload: keep the library's default launch shape for every size")
     ap.add_argument("--workload", default="1080p", choices=["1080p", "batched", "learned", "4k"],

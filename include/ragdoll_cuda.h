@@ -197,10 +197,15 @@ int rg_analyse_gops_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t
  * context's pictures on the per-diagonal path). The batched transcode of many independent
  * streams of several sizes (the pipeline's parallel_gop_map over encoders,
  * crates/ragdoll-pipeline/src/lib.rs:110-157) as one launch; no single counterpart in the reference.
+ * The launch's stream work (descriptor copy, counter reset, the persistent launch, the error
+ * hand-offs) is a CUDA graph captured once per launch shape and replayed by later calls of that
+ * shape.
  */
 int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
                           const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
                           int32_t frames);
+/* Group calls led by ctx (ctxs[0]) so far: graphs captured and graph launches. */
+int rg_group_graph_counts(const rg_ctx* ctx, int64_t* captures, int64_t* launches);
 
 /* Host-buffer form of rg_analyse_gops_device; out receives frames * num_streams * mb_w * mb_h
  * records (or NULL). */
@@ -243,6 +248,35 @@ int rg_analyse_gops_stream(rg_ctx* ctx, const uint8_t* const* planes, size_t str
  * finishing it (call rg_analyse_gops_wait); negative RG_ERR_*. Safe to call from several host threads
  * at once (for different pictures) while the context's own thread is not in another call. */
 int rg_analyse_gops_fetch(rg_ctx* ctx, rg_mb_out* out, int32_t picture);
+
+/*
+ * Compact records. A picture's records in compact form are, per macroblock in raster order,
+ * RG_COMPACT_MASK_WORDS 32-bit mask words -- bit j of mask word i set when the record's 32-bit
+ * word 32 i + j (of the sizeof(rg_mb_out) / 4 = 222) is nonzero -- followed by those nonzero words
+ * in increasing order; zero-filling the rest rebuilds the record exactly. Most of a record is zero
+ * levels, so the form is ~10x smaller than the records.
+ *
+ * rg_set_record_compaction(ctx, words_per_mb > 0) makes the launches of rg_analyse_gops_stream
+ * also write each picture's compact records, row by row as its analysis completes, straight into
+ * mapped host memory of the context (each macroblock row into its own slot of words_per_mb words
+ * per macroblock, packed together by the first fetch; a picture with a row that does not fit is
+ * handed out as full records instead). 0 turns it off (the default). Not while calls are in
+ * flight. No counterpart in the reference (its records never leave the CPU).
+ */
+#define RG_COMPACT_MASK_WORDS 7
+int rg_set_record_compaction(rg_ctx* ctx, int32_t words_per_mb);
+/*
+ * rg_analyse_gops_fetch of a call made with compaction on: 1 with *data / *bytes the picture's
+ * compact records in the context's mapped memory (valid until the call two calls later is
+ * queued), or, when a row did not fit its slot, *data NULL and the full records copied into
+ * out + picture * mb_w * mb_h; 0, 2 and errors as rg_analyse_gops_fetch.
+ */
+int rg_analyse_gops_fetch_compact(rg_ctx* ctx, rg_mb_out* out, int32_t picture, const void** data, size_t* bytes);
+/* Host helpers of the compact form: n records into out (returns the bytes written, or
+ * RG_ERR_INVALID when cap is too small), and back (RG_ERR_INVALID for a stream that is not n
+ * compact records exactly). */
+int64_t rg_records_compact(const rg_mb_out* records, int32_t n, void* out, size_t cap);
+int rg_records_expand(const void* compact, size_t bytes, int32_t n, rg_mb_out* out);
 
 /* Tuning of the pipelined mode (rg_set_pipeline_tuning); 0 in any field selects the default. */
 typedef struct rg_pipeline_tuning {
@@ -537,6 +571,9 @@ size_t rg_writer_bound(const rg_writer* writer);
 /* Writes the access unit of one picture (records: mb_w * mb_h, raster order; kind RG_FRAME_*)
  * into out; returns its size in bytes, or a negative RG_ERR_* (the buffer too small included). */
 int64_t rg_writer_picture(rg_writer* writer, const rg_mb_out* records, int32_t kind, uint8_t* out, size_t cap);
+/* rg_writer_picture from the picture's compact records (rg_analyse_gops_fetch_compact). */
+int64_t rg_writer_picture_compact(rg_writer* writer, const void* compact, size_t bytes, int32_t kind, uint8_t* out,
+                                  size_t cap);
 
 /* ---- Encoder (host + GPU) ---------------------------------------------------------------- */
 /*
@@ -592,6 +629,11 @@ int rg_encoder_set_form(rg_encoder* enc, int32_t form, int32_t search_range, rg_
  * in the reference.
  */
 int32_t rg_encoder_latencies(const rg_encoder* enc, double* ms, int32_t n);
+/* Bytes of records the wave collected last brought to the host: full records, or with
+ * rg_set_record_compaction on rg_encoder_context (off by default: on a PCIe host whose copy engine
+ * hides the full records' copy behind the launch, the launch's compaction costs more than it
+ * saves) compact records plus the full records of pictures handed out without them. */
+int64_t rg_encoder_record_bytes(const rg_encoder* enc);
 
 /* ---- Containers (host) ------------------------------------------------------------------ */
 /*

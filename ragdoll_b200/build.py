@@ -18,7 +18,7 @@ LIB = PKG / "libragdoll_cuda.so"
 BUILD = PKG / "_build"
 
 SOURCES = ["engine_kernels.cu", "ssim_kernels.cu", "rg_api.cu", "ssim_noalloc.cu", "candidate_net.cu", "cavlc_writer.cpp",
-           "cabac_writer.cpp", "containers.cpp", "host_encoder.cpp"]
+           "cabac_writer.cpp", "containers.cpp", "host_encoder.cpp", "records.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "-Xcompiler", "-march=x86-64-v3", "--expt-relaxed-constexpr"]

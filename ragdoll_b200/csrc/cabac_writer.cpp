@@ -183,12 +183,14 @@ class SliceCoder {
     }
   }
 
-  int code(const rg_mb_out* recs) {
+  int code(RecordReader& recs) {
     for (int y = 0; y < mb_h_; y++) {
       left_ = MbSummary();
       std::fill(left_modes_, left_modes_ + 4, 2);
       for (int x = 0; x < mb_w_; x++) {
-        const rg_mb_out& r = recs[y * mb_w_ + x];
+        const rg_mb_out* rp = recs.next();
+        if (!rp) return -1;
+        const rg_mb_out& r = *rp;
         const MbSummary& top = above_[x];
         MbSummary cur;
         int rc = macroblock(r, x, y, top, cur);
@@ -500,7 +502,7 @@ class SliceCoder {
 // Appends the CABAC slice data of one picture (after the byte-aligned slice header) to out;
 // ends with the flushed coder and the alignment to a byte. Returns 0, or -1 for a record that
 // no Balanced slice holds.
-int cabac_slice_data(int mb_w, int mb_h, int qp, bool idr, bool transform_8x8, const rg_mb_out* recs,
+int cabac_slice_data(int mb_w, int mb_h, int qp, bool idr, bool transform_8x8, RecordReader& recs,
                      std::vector<uint8_t>& out) {
   SliceCoder coder(mb_w, mb_h, qp, idr, transform_8x8, out);
   return coder.code(recs);

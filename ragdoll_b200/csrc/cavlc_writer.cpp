@@ -355,8 +355,8 @@ namespace rg {
 // The access unit of one picture (SPS and PPS first for an IDR) with explicit frame_num / POC
 // (pictures since the IDR), idr_pic_id and QP; uses the writer's configuration and scratch only, so
 // writers of the same configuration can write pictures of one stream on several threads.
-int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_t since_idr, uint32_t idr_id,
-                       int qp, std::vector<uint8_t>& au) {
+int writer_access_unit(rg_writer* w, RecordReader& records, bool idr, uint32_t since_idr, uint32_t idr_id, int qp,
+                       std::vector<uint8_t>& au) {
   int n4 = w->mb_w * w->mb_h * 16;
   w->nnz.assign(n4, 0);
   w->cnnz[0].assign(w->mb_w * w->mb_h * 4, 0);
@@ -396,12 +396,15 @@ int writer_access_unit(rg_writer* w, const rg_mb_out* records, bool idr, uint32_
     uint32_t skip_run = 0;
     for (int mby = 0; mby < w->mb_h; mby++)
       for (int mbx = 0; mbx < w->mb_w; mbx++) {
-        int r = w->mb_layer(s, mbx, mby, records[mby * w->mb_w + mbx], idr, skip_run);
+        const rg_mb_out* rec = records.next();
+        if (!rec) return wfail(RG_ERR_INVALID, "rg_writer_picture: compact records end before mb (%d,%d)", mbx, mby);
+        int r = w->mb_layer(s, mbx, mby, *rec, idr, skip_run);
         if (r) return r;
       }
     if (!idr && skip_run) s.ue(skip_run);
     rbsp = &s.close();
   }
+  if (!records.done()) return wfail(RG_ERR_INVALID, "rg_writer_picture: compact records longer than the picture");
   au.clear();
   if (idr) {
     emit_nal(au, 3, 7, w->sps());
@@ -452,8 +455,7 @@ size_t rg_writer_bound(const rg_writer* w) {
   return ((size_t)w->mb_w * w->mb_h * per_mb + 512) * 3 / 2;
 }
 
-int64_t rg_writer_picture(rg_writer* w, const rg_mb_out* records, int32_t kind, uint8_t* out, size_t cap) {
-  if (!w || !records || !out) return wfail(RG_ERR_INVALID, "rg_writer_picture: null argument");
+static int64_t writer_picture(rg_writer* w, rg::RecordReader& records, int32_t kind, uint8_t* out, size_t cap) {
   if (kind != RG_FRAME_IDR && kind != RG_FRAME_P) return wfail(RG_ERR_INVALID, "rg_writer_picture: kind %d", kind);
   if (kind == RG_FRAME_P && !w->have_idr) return wfail(RG_ERR_STATE, "rg_writer_picture: P picture before an IDR");
   bool idr = kind == RG_FRAME_IDR;
@@ -470,6 +472,20 @@ int64_t rg_writer_picture(rg_writer* w, const rg_mb_out* records, int32_t kind, 
   }
   w->since_idr++;
   return (int64_t)au.size();
+}
+
+int64_t rg_writer_picture(rg_writer* w, const rg_mb_out* records, int32_t kind, uint8_t* out, size_t cap) {
+  if (!w || !records || !out) return wfail(RG_ERR_INVALID, "rg_writer_picture: null argument");
+  rg::RecordReader rd(records);
+  return writer_picture(w, rd, kind, out, cap);
+}
+
+int64_t rg_writer_picture_compact(rg_writer* w, const void* compact, size_t bytes, int32_t kind, uint8_t* out,
+                                  size_t cap) {
+  if (!w || !compact || !out) return wfail(RG_ERR_INVALID, "rg_writer_picture_compact: null argument");
+  if (bytes % 4) return wfail(RG_ERR_INVALID, "rg_writer_picture_compact: %zu bytes, not whole words", bytes);
+  rg::RecordReader rd(compact, bytes);
+  return writer_picture(w, rd, kind, out, cap);
 }
 
 }  // extern "C"

@@ -123,10 +123,22 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 // One launch over n_desc descriptors of up to kMaxGroups picture sizes (descriptor d: group
 // d.group, rows d.rows_base .. + its mb_h in the row counters, total_rows in all). host_err null:
 // no error hand-off kernel (launch_error_to_host queues one per caller instead).
+// Compact records (co != null): the warp deblocking a row's last segment also writes that row's
+// records, word-sparse (kCompactMaskWords mask words per record, then its nonzero words in order),
+// into the row's slot (row r of the launch, counted as the row counters are: row_words words at
+// words + r * row_words) and the row's size in bytes, or -1 when it did not fit, into
+// row_bytes[r] -- both before the picture's ready flag.
+constexpr int kRecordWords = 222;      // sizeof(rg_mb_out) / 4
+constexpr int kCompactMaskWords = 7;   // ceil(kRecordWords / 32)
+struct CompactOut {
+  uint32_t* words;   // device address of mapped host memory
+  int row_words;     // words per row slot
+  int* row_bytes;    // device address of mapped host memory: [row]
+};
 void launch_pipeline(const FrameGroups& fg, const StreamDev* d_streams, int n_desc, int total_rows, int* counters,
                      const int2* d_tasks, size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms,
                      int intra_sms, int sms, int seg, int grid, unsigned long long timeout_ns, int* ready, int seq,
-                     int* host_err, int* host_reach, cudaStream_t st, int form = 0);
+                     int* host_err, int* host_reach, cudaStream_t st, int form = 0, const CompactOut* co = nullptr);
 void launch_error_to_host(const int* counters, int n_desc, int total_rows, int* host_err, int* host_reach,
                           cudaStream_t st);
 size_t pipeline_counter_ints(int total_rows, int n_desc);

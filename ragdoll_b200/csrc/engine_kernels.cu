@@ -2146,6 +2146,11 @@ struct PipeParams {
   int seq;
   int* host_err;      // mapped host memory: the error word as the launch ends (no copy to wait for)
   int* reach;         // [2] 1 + the largest reach of a reference wait beyond zero motion (rows, columns)
+  // compact records (cwords null: none): row r of the launch (rows like ana) has a slot of crow
+  // words at cwords + r * crow in mapped host memory and its size in bytes (or -1) at cbytes[r]
+  uint32_t* cwords;
+  int crow;
+  int* cbytes;
 };
 __device__ __forceinline__ unsigned sm_id() {
   unsigned r;
@@ -2162,6 +2167,88 @@ __device__ __noinline__ void picture_row_done(int* rows_done, int* ready, int se
     int before = atom_add_acq_rel(rows_done, 1);
     if (before == H - 1) st_release_sys(ready, seq);
   }
+  __syncwarp();
+}
+
+static_assert(sizeof(rg_mb_out) == 4 * kRecordWords, "a record is kRecordWords words");
+// Staging of compact records in the warp's shared memory (its Smem, which no task reads before
+// writing it): kStageWords words, flushed to host memory in 16-byte stores.
+constexpr int kStageWords = 512;
+static_assert(sizeof(Smem) >= 4 * kStageWords, "the staging buffer fits the warp's shared memory");
+static_assert(kStageWords >= 2 * (kCompactMaskWords + kRecordWords), "a flush leaves room for a whole record");
+
+// Writes the first n (a multiple of 4) staged words to dst + at (16-byte aligned) while they fit
+// the slot of cap words (a multiple of 4), then moves the rest (< 4 words) to the front.
+__device__ __noinline__ void flush_stage(uint32_t* stage, int n, int rest, uint32_t* dst, long long at, int cap) {
+  const int lane = lane_id();
+  __syncwarp();
+  const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+  uint4* d4 = reinterpret_cast<uint4*>(dst + at);
+  for (int c = lane; c < n / 4; c += 32)
+    if (at + 4 * c + 4 <= cap) d4[c] = s4[c];
+  __syncwarp();
+  uint32_t v = lane < rest ? stage[n + lane] : 0u;
+  __syncwarp();
+  if (lane < rest) stage[lane] = v;
+  __syncwarp();
+}
+
+// Compact records of row y, written by the warp that deblocked the row's last segment (after it
+// published its progress) into the row's own slot (no row waits for another). A record's compact form is kCompactMaskWords mask words (bit j of
+// mask word i: record word 32 i + j is nonzero), then its nonzero words in increasing order:
+// zero-filling rebuilds the record exactly. The row's records are final: the deblocking warp
+// acquired the row's analysis progress up to its end; they are read through L2. The
+// words are gathered in shared memory and leave in whole 16-byte stores (word-sized stores to
+// host memory made the row ~10x slower). Words past the slot are not written, and the row's size
+// is then -1 (the host copies the picture's full records instead). The size is written before the
+// row is counted towards the picture's flag. (Scalar arguments: a reference to the kernel's
+// parameters would copy them to local memory.)
+__device__ __noinline__ void compact_row(const rg_mb_out* rec, uint32_t* dst, int cap, int* bytes, int Wm,
+                                         uint32_t* stage) {
+  const int lane = lane_id();
+  long long done = 0;  // words flushed (a multiple of 4)
+  int sp = 0;          // words staged
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(rec);
+  const unsigned below = (1u << lane) - 1u;
+  for (int m0 = 0; m0 < Wm; m0 += 4) {
+    // four records in flight, then their words into the stage
+    uint32_t w[4][kCompactMaskWords];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int i = 0; i < kCompactMaskWords; i++) {
+        const int j = lane + 32 * i;
+        w[k][i] = (m0 + k < Wm && j < kRecordWords) ? __ldcg(src + (size_t)(m0 + k) * kRecordWords + j) : 0u;
+      }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (m0 + k >= Wm) break;
+      if (sp + kCompactMaskWords + kRecordWords > kStageWords) {
+        const int n = sp & ~3;
+        flush_stage(stage, n, sp - n, dst, done, cap);
+        done += n;
+        sp -= n;
+      }
+      uint32_t mask = 0;
+      int at = sp + kCompactMaskWords;
+#pragma unroll
+      for (int i = 0; i < kCompactMaskWords; i++) {
+        const unsigned b = __ballot_sync(FULL, w[k][i] != 0u);
+        if (lane == i) mask = b;
+        if (w[k][i] != 0u) stage[at + __popc(b & below)] = w[k][i];
+        at += __popc(b);
+      }
+      if (lane < kCompactMaskWords) stage[sp + lane] = mask;
+      sp = at;
+    }
+  }
+  // the tail, padded to whole 16-byte stores (the padding stays inside the slot: cap is a
+  // multiple of 4 and the row's words, when they fit, are at most cap)
+  const long long total = done + sp;
+  flush_stage(stage, (sp + 3) & ~3, 0, dst, done, cap);
+  if (lane == 0) *bytes = total <= cap ? (int)(total * 4) : -1;
+  // the row's words and size reach host memory before the row is counted towards the flag
+  __threadfence_system();
   __syncwarp();
 }
 
@@ -2244,7 +2331,9 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameGroups fg, const 
         }
         publish(ana_rows + y, x + 1);
       }
-      if (!failed && x1 == Wm && pp.ready) picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
+      // (with compact records, the row is counted once its deblocking warp has compacted it)
+      if (!failed && x1 == Wm && pp.ready && !pp.cwords)
+        picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
       reach_y = pw.reach_y;
       reach_x = pw.reach_x;
     } else {
@@ -2267,6 +2356,17 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameGroups fg, const 
           if (x == Wm - 1) extend_mb(fp, sd, x, y);
         }
         publish(db_rows + y, x + 1);
+      }
+      // Compact records of the row, by the warp that deblocked its last segment: on the deblocking
+      // SMs and after the row's deblocking progress was published, so neither the analysis
+      // wavefront nor the deblocking chain waits for it (done at the end of the row's analysis it
+      // slowed the launch ~5 %). Its wait for the analysis of the row up to its end ordered every
+      // record of the row before it.
+      if (!failed && x1 == Wm && pp.cwords) {
+        const long long r = (long long)sd.rows_base + y;
+        compact_row(sd.rec + (size_t)y * Wm, pp.cwords + r * pp.crow, pp.crow, pp.cbytes + r, Wm,
+                    reinterpret_cast<uint32_t*>(&sm));
+        if (pp.ready) picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
       }
     }
     if (failed) break;
@@ -2444,7 +2544,7 @@ size_t pipeline_task_list(const FrameParams& fp, int frames, int lag, int seg, b
 void launch_pipeline(const FrameGroups& fg, const StreamDev* d_streams, int n_desc, int total_rows, int* counters,
                      const int2* d_tasks, size_t n_tasks, const int qbeg[3], const int qend[3], int deblock_sms,
                      int intra_sms, int sms, int seg, int grid, unsigned long long timeout_ns, int* ready, int seq,
-                     int* host_err, int* host_reach, cudaStream_t st, int form) {
+                     int* host_err, int* host_reach, cudaStream_t st, int form, const CompactOut* co) {
   PipeParams pp;
   pp.ticket = counters;
   pp.error = counters + 1;
@@ -2466,6 +2566,9 @@ void launch_pipeline(const FrameGroups& fg, const StreamDev* d_streams, int n_de
   pp.seq = seq;
   pp.host_err = host_err;
   pp.reach = pp.rows_done + n_desc;
+  pp.cwords = co ? co->words : nullptr;
+  pp.crow = co ? co->row_words : 0;
+  pp.cbytes = co ? co->row_bytes : nullptr;
   int g = grid < pp.n_tasks ? grid : pp.n_tasks;
   if (form) pipeline_kernel<1><<<g, 32, 0, st>>>(fg, d_streams, pp);
   else pipeline_kernel<0><<<g, 32, 0, st>>>(fg, d_streams, pp);

@@ -107,7 +107,9 @@ struct Wave {
   std::vector<uint32_t> since, idr_id;
   std::chrono::steady_clock::time_point submitted;
   std::vector<double> latency_ms;  // per picture: submit -> access unit written
+  std::atomic<int64_t> record_bytes{0};  // records brought to the host (compact or full)
 };
+
 
 }  // namespace
 
@@ -127,6 +129,7 @@ struct rg_encoder {
   std::vector<std::vector<uint8_t>> aus;         // access units of the wave being written
   std::vector<rg_mb_out> one;                    // records of rg_encode_frame
   std::vector<double> last_latency_ms;           // of the wave collected last
+  int64_t last_record_bytes = 0;                 // of the wave collected last
 
   // Counters of the next picture of stream s, then advances them.
   void next_picture(int s, uint8_t& idr, uint32_t& since_idr, uint32_t& idr_id) {
@@ -280,16 +283,28 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
     w.latency_ms.assign(n, 0.0);
     std::vector<uint8_t> later(n, 0);
     std::atomic<int> err{0};
-    auto write = [&](int i, int worker) {
-      int rc = rg::writer_access_unit(e->writers[worker], w.recs + (size_t)i * e->n_mb, w.idr[i], w.since[i],
-                                      w.idr_id[i], w.qp[i % S], e->aus[i]);
+    w.record_bytes = 0;
+    // data null: the picture's full records in w.recs
+    auto write = [&](int i, int worker, const void* data, size_t bytes) {
+      int rc;
+      if (data) {
+        rg::RecordReader rd(data, bytes);
+        rc = rg::writer_access_unit(e->writers[worker], rd, w.idr[i], w.since[i], w.idr_id[i], w.qp[i % S], e->aus[i]);
+      } else {
+        rc = rg::writer_access_unit(e->writers[worker], w.recs + (size_t)i * e->n_mb, w.idr[i], w.since[i],
+                                    w.idr_id[i], w.qp[i % S], e->aus[i]);
+        bytes = sizeof(rg_mb_out) * e->n_mb;
+      }
+      w.record_bytes += (int64_t)bytes;
       if (rc) err.store(rc);
       w.latency_ms[i] =
           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w.submitted).count();
     };
     e->pool->run(n, [&](int i, int worker) {
+      const void* data = nullptr;
+      size_t bytes = 0;
       for (int spins = 0;; spins++) {
-        int st = rg_analyse_gops_fetch(e->ctx, w.recs, i);
+        int st = rg_analyse_gops_fetch_compact(e->ctx, w.recs, i, &data, &bytes);
         if (st == 1) break;
         if (st != 0) {
           later[i] = 1;
@@ -297,14 +312,14 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
         }
         std::this_thread::sleep_for(std::chrono::microseconds(spins < 64 ? 20 : 200));
       }
-      write(i, worker);
+      write(i, worker, data, bytes);
     });
     int r = rg_analyse_gops_wait(e->ctx, w.recs);  // the launch's end; a re-run if a wait gave up
     if (r) return r;
     std::vector<int> rest;
     for (int i = 0; i < n; i++)
       if (later[i]) rest.push_back(i);
-    if (!rest.empty()) e->pool->run((int)rest.size(), [&](int k, int worker) { write(rest[k], worker); });
+    if (!rest.empty()) e->pool->run((int)rest.size(), [&](int k, int worker) { write(rest[k], worker, nullptr, 0); });
     if (err.load()) return err.load();
     w.written = true;
   }
@@ -322,6 +337,7 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
   }
   w.written = false;
   e->last_latency_ms = w.latency_ms;
+  e->last_record_bytes = w.record_bytes.load();
   e->head ^= 1;
   e->pending--;
   return (int64_t)total;
@@ -341,6 +357,11 @@ int rg_encoder_new_gops(rg_encoder* e) {
   std::fill(e->idrs.begin(), e->idrs.end(), 0u);
   std::fill(e->since.begin(), e->since.end(), 0u);
   return RG_OK;
+}
+
+int64_t rg_encoder_record_bytes(const rg_encoder* e) {
+  if (!e) return efail(RG_ERR_INVALID, "rg_encoder_record_bytes: null encoder");
+  return e->last_record_bytes;
 }
 
 int32_t rg_encoder_latencies(const rg_encoder* e, double* ms, int32_t n) {

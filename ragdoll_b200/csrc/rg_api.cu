@@ -9,6 +9,7 @@
 #include <cstring>
 #include <string>
 #include <array>
+#include <atomic>
 #include <vector>
 
 #include "engine.h"
@@ -207,9 +208,29 @@ struct rg_ctx {
   std::vector<int64_t> g_shape;
   int g_qbeg[3] = {0, 0, 0}, g_qend[3] = {0, 0, 0};
   cudaEvent_t g_done = nullptr, g_order = nullptr;
+  // the launch's stream work as CUDA graphs, one per launch shape (two kept: calls alternate
+  // between two error words), replayed while the shape holds
+  struct GroupGraph {
+    std::vector<int64_t> key;
+    cudaGraphExec_t exec = nullptr;
+  };
+  GroupGraph g_graphs[2];
+  int g_graph_next = 0;
+  int64_t g_graph_captures = 0, g_graph_launches = 0;
   int* h_ready[2] = {nullptr, nullptr};  // mapped host memory: per picture, the launch seq once final
   int* d_ready[2] = {nullptr, nullptr};  // the same, as the device sees it
   int a_seq[2] = {0, 0}, a_frames[2] = {0, 0};
+  // compact records of rg_analyse_gops_stream (rg_set_record_compaction): per slot, mapped host
+  // memory of c_row words per macroblock row, each row's compact size, and per picture the bytes
+  // of its compact records once the host packed its rows together (-1 not yet, -2 did not fit)
+  int compact_words = 0;           // words per macroblock of a slot; 0: off
+  uint32_t* h_cwords[2] = {nullptr, nullptr};
+  uint32_t* d_cwords[2] = {nullptr, nullptr};
+  int* h_cbytes[2] = {nullptr, nullptr};
+  int* d_cbytes[2] = {nullptr, nullptr};
+  int c_row[2] = {0, 0};           // words per row slot of each slot's buffers
+  std::vector<int64_t> c_packed[2];
+  bool a_compact[2] = {false, false};  // the slot's call writes compact records
   int launch_seq = 0;
   int a_slot = 0;
   int form = RG_FORM_PLAIN;        // analysis form (rg_set_analysis_form)
@@ -383,6 +404,8 @@ void rg_destroy(rg_ctx* c) {
   cudaFree(c->g_dtasks);
   if (c->g_hstreams) cudaFreeHost(c->g_hstreams);
   if (c->g_done) cudaEventDestroy(c->g_done);
+  for (auto& g : c->g_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   if (c->g_order) cudaEventDestroy(c->g_order);
   if (c->a_in) cudaStreamSynchronize(c->a_in);
   if (c->a_out) cudaStreamSynchronize(c->a_out);
@@ -390,6 +413,8 @@ void rg_destroy(rg_ctx* c) {
     cudaFree(c->a_srcs[i]);
     cudaFree(c->a_recs[i]);
     if (c->h_ready[i]) cudaFreeHost(c->h_ready[i]);
+    if (c->h_cwords[i]) cudaFreeHost(c->h_cwords[i]);
+    if (c->h_cbytes[i]) cudaFreeHost(c->h_cbytes[i]);
     for (cudaEvent_t e : {c->a_in_done[i], c->a_kern_done[i], c->a_out_done[i]})
       if (e) cudaEventDestroy(e);
   }
@@ -575,7 +600,7 @@ static void gop_desc(const rg_ctx* c, StreamDev& d, int f, int s, const uint8_t*
 
 static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
                         const int32_t* kinds, int32_t frames, rg_mb_out* rec_base, int* ready = nullptr, int seq = 0,
-                        bool resolved = false) {
+                        bool resolved = false, const CompactOut* co = nullptr) {
   if (!c || !dev_planes || !kinds) return fail(RG_ERR_INVALID, "rg_analyse_gops_device: null argument");
   if (frames < 1 || frames > c->max_frames)
     return fail(RG_ERR_INVALID, "rg_analyse_gops_device: frames %d outside 1..%d (rg_config.max_frames)", frames,
@@ -664,7 +689,7 @@ static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stri
   fg.n = 1;
   launch_pipeline(fg, c->d_streams[slot], frames * S, frames * S * fp.mb_h, c->counters, c->d_tasks, c->n_tasks, c->qbeg,
                   c->qend, c->deblock_sms, c->intra_sms, c->sms, c->seg, c->grid, c->timeout_ns, ready, seq,
-                  c->d_err + pslot, c->d_err + 2 + 2 * pslot, c->stream, c->form != RG_FORM_PLAIN);
+                  c->d_err + pslot, c->d_err + 2 + 2 * pslot, c->stream, c->form != RG_FORM_PLAIN, co);
   CK(cudaGetLastError());
   CK(cudaEventRecord(p.done, c->stream));
   p.planes.assign(dev_planes, dev_planes + (size_t)frames * S * 3);
@@ -728,13 +753,22 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     c->hints.clear();
   }
   CK(cudaSetDevice(L->cfg.device));
-  // descriptors and rows of every context, one after the other
-  std::vector<int> desc_base(n + 1, 0), rows_base(n + 1, 0);
-  for (int i = 0; i < n; i++) {
-    desc_base[i + 1] = desc_base[i] + frames * ctxs[i]->S;
-    rows_base[i + 1] = rows_base[i] + frames * ctxs[i]->S * ctxs[i]->fp.mb_h;
+  // descriptors and rows of every context, one after the other, the contexts with more macroblocks
+  // first whatever the argument order (64 streams of four sizes: 263 ms against 364 ms with the
+  // smallest size's descriptors first)
+  std::vector<int> lay(n);
+  for (int i = 0; i < n; i++) lay[i] = i;
+  std::stable_sort(lay.begin(), lay.end(), [&](int x, int y) {
+    return (long)ctxs[x]->n_mb * ctxs[x]->S > (long)ctxs[y]->n_mb * ctxs[y]->S;
+  });
+  std::vector<int> desc_base(n, 0), rows_base(n, 0);
+  int n_desc = 0, total_rows = 0;
+  for (int i : lay) {
+    desc_base[i] = n_desc;
+    rows_base[i] = total_rows;
+    n_desc += frames * ctxs[i]->S;
+    total_rows += frames * ctxs[i]->S * ctxs[i]->fp.mb_h;
   }
-  const int n_desc = desc_base[n], total_rows = rows_base[n];
   if ((size_t)n_desc > L->g_streams_cap) {
     if (L->g_done) CK(cudaEventSynchronize(L->g_done));
     cudaFree(L->g_dstreams);
@@ -852,27 +886,64 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     CK(cudaEventRecord(c->g_order, c->stream));
     CK(cudaStreamWaitEvent(L->stream, c->g_order, 0));
   }
-  CK(cudaMemcpyAsync(L->g_dstreams, L->g_hstreams, sizeof(StreamDev) * n_desc, cudaMemcpyHostToDevice, L->stream));
-  CK(cudaEventRecord(L->g_done, L->stream));
-  CK(cudaMemsetAsync(L->g_counters, 0, sizeof(int) * n_counters, L->stream));
   std::vector<int> pslot(n);
   for (int i = 0; i < n; i++) {
     rg_ctx* c = ctxs[i];
     pslot[i] = (c->pend_head + c->pend_count) & 1;
     *(volatile int*)c->pend[pslot[i]].h_err = 0;
   }
-  launch_pipeline(fg, L->g_dstreams, n_desc, total_rows, L->g_counters, L->g_dtasks, L->g_ntasks, L->g_qbeg, L->g_qend,
-                  T->deblock_sms, T->intra_sms, L->sms, seg, grid, T->timeout_ns, nullptr, 0, nullptr, nullptr,
-                  L->stream, L->form != RG_FORM_PLAIN);
-  CK(cudaGetLastError());
-  // every context gets the launch's error word and reach as its own pending call, resolved (and if
-  // a wait gave up, re-run picture by picture) by the context itself
-  for (int i = 0; i < n; i++) {
-    rg_ctx* c = ctxs[i];
-    launch_error_to_host(L->g_counters, n_desc, total_rows, c->d_err + pslot[i], c->d_err + 2 + 2 * pslot[i],
-                         L->stream);
+  // The stream work of the launch -- the descriptors' copy, the counters' reset, the persistent
+  // launch and, per context, the hand-off of the launch's error word and reach (every context
+  // holds the launch as its own pending call, resolved and if a wait gave up re-run picture by
+  // picture by the context itself) -- as a CUDA graph, captured for each launch shape and replayed
+  // while it holds (the descriptors' contents change per call; the copy reads them as it runs).
+  std::vector<int64_t> key = L->g_shape;
+  key.insert(key.end(), {n_desc, total_rows, (int64_t)n_counters, (int64_t)L->g_ntasks, T->deblock_sms,
+                         T->intra_sms, L->sms, (int64_t)T->timeout_ns, (int64_t)(uintptr_t)L->g_dstreams,
+                         (int64_t)(uintptr_t)L->g_hstreams, (int64_t)(uintptr_t)L->g_counters,
+                         (int64_t)(uintptr_t)L->g_dtasks, L->form});
+  for (int i = 0; i < n; i++)
+    key.insert(key.end(), {(int64_t)stride_y[i], (int64_t)stride_uv[i], (int64_t)(uintptr_t)(ctxs[i]->d_err + pslot[i])});
+  rg_ctx::GroupGraph* gg = nullptr;
+  for (auto& g : L->g_graphs)
+    if (g.exec && g.key == key) gg = &g;
+  if (!gg) {
+    gg = &L->g_graphs[L->g_graph_next];
+    L->g_graph_next ^= 1;
+    if (gg->exec) CK(cudaGraphExecDestroy(gg->exec));
+    gg->exec = nullptr;
+    gg->key.clear();
+    CK(cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemcpyAsync(L->g_dstreams, L->g_hstreams, sizeof(StreamDev) * n_desc, cudaMemcpyHostToDevice,
+                                    L->stream);
+    // an external event node: the event is recorded each time the graph runs (a plain record in a
+    // capture only orders the capture's own streams)
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(L->g_done, L->stream, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L->g_counters, 0, sizeof(int) * n_counters, L->stream);
+    if (e == cudaSuccess) {
+      launch_pipeline(fg, L->g_dstreams, n_desc, total_rows, L->g_counters, L->g_dtasks, L->g_ntasks, L->g_qbeg,
+                      L->g_qend, T->deblock_sms, T->intra_sms, L->sms, seg, grid, T->timeout_ns, nullptr, 0, nullptr,
+                      nullptr, L->stream, L->form != RG_FORM_PLAIN);
+      for (int i = 0; i < n; i++)
+        launch_error_to_host(L->g_counters, n_desc, total_rows, ctxs[i]->d_err + pslot[i],
+                             ctxs[i]->d_err + 2 + 2 * pslot[i], L->stream);
+      e = cudaGetLastError();
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(L->stream, &graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gg->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      gg->exec = nullptr;
+      cudaGetLastError();
+      return fail(RG_ERR_CUDA, "%s: capturing the launch: %s", who, cudaGetErrorString(e));
+    }
+    gg->key = key;
+    L->g_graph_captures++;
   }
-  CK(cudaGetLastError());
+  CK(cudaGraphLaunch(gg->exec, L->stream));
+  L->g_graph_launches++;
   if (!L->g_order) CK(cudaEventCreateWithFlags(&L->g_order, cudaEventDisableTiming));
   CK(cudaEventRecord(L->g_order, L->stream));
   for (int i = 0; i < n; i++) {
@@ -893,6 +964,13 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     c->pend_count++;
     for (int s = 0; s < c->S; s++) c->frames[s] += frames;
   }
+  return RG_OK;
+}
+
+int rg_group_graph_counts(const rg_ctx* c, int64_t* captures, int64_t* launches) {
+  if (!c || !captures || !launches) return fail(RG_ERR_INVALID, "rg_group_graph_counts: null argument");
+  *captures = c->g_graph_captures;
+  *launches = c->g_graph_launches;
   return RG_OK;
 }
 
@@ -1197,7 +1275,37 @@ static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, 
   CK(cudaStreamWaitEvent(c->stream, c->a_in_done[slot], 0));
   CK(cudaStreamWaitEvent(c->stream, c->a_out_done[slot], 0));
   int seq = ++c->launch_seq;
-  r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot], bulk ? nullptr : c->d_ready[slot], seq, true);
+  // compact records: this slot's mapped buffers (re)allocated to the current slot size; the slot's
+  // previous call was resolved above, and its pictures were fetched before this call (the
+  // two-calls rule), so nothing reads them any more
+  CompactOut co{};
+  c->a_compact[slot] = false;
+  if (!bulk && c->compact_words > 0) {
+    const int row = (c->fp.mb_w * c->compact_words + 3) & ~3;  // whole 16-byte stores
+    const size_t rows = (size_t)S * c->max_frames * c->fp.mb_h;
+    if (!c->h_cwords[slot] || c->c_row[slot] != row) {
+      if (c->h_cwords[slot]) cudaFreeHost(c->h_cwords[slot]);
+      if (c->h_cbytes[slot]) cudaFreeHost(c->h_cbytes[slot]);
+      c->h_cwords[slot] = nullptr;
+      c->h_cbytes[slot] = nullptr;
+      if (cudaHostAlloc((void**)&c->h_cwords[slot], sizeof(uint32_t) * row * rows, cudaHostAllocMapped) != cudaSuccess ||
+          cudaHostAlloc((void**)&c->h_cbytes[slot], sizeof(int) * rows, cudaHostAllocMapped) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RG_ERR_OOM, "rg_analyse_gops_stream: %zu bytes of mapped host memory for compact records",
+                    sizeof(uint32_t) * row * rows);
+      }
+      CK(cudaHostGetDevicePointer((void**)&c->d_cwords[slot], c->h_cwords[slot], 0));
+      CK(cudaHostGetDevicePointer((void**)&c->d_cbytes[slot], c->h_cbytes[slot], 0));
+      c->c_row[slot] = row;
+    }
+    c->c_packed[slot].assign((size_t)S * frames, -1);
+    co.words = c->d_cwords[slot];
+    co.row_words = row;
+    co.row_bytes = c->d_cbytes[slot];
+    c->a_compact[slot] = true;
+  }
+  r = enqueue_gops(c, dev.data(), w, cw, kinds, frames, c->a_recs[slot], bulk ? nullptr : c->d_ready[slot], seq, true,
+                   c->a_compact[slot] ? &co : nullptr);
   if (r) return r;
   c->a_seq[slot] = seq;
   c->a_frames[slot] = frames;
@@ -1223,12 +1331,13 @@ int rg_analyse_gops_stream(rg_ctx* c, const uint8_t* const* planes, size_t strid
   return async_gops(c, planes, stride_y, stride_uv, kinds, frames, out, false);
 }
 
-int rg_analyse_gops_fetch(rg_ctx* c, rg_mb_out* out, int32_t picture) {
-  if (!c || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_fetch: null argument");
-  int slot = c->a_out_ptr[0] == out ? 0 : (c->a_out_ptr[1] == out ? 1 : -1);
-  if (slot < 0 || !c->h_ready[slot]) return fail(RG_ERR_STATE, "rg_analyse_gops_fetch: no call in flight writes into out");
+// Whether picture `picture` of the stream call writing into out is final: 1 yes (slot set), 0 not
+// yet, 2 the launch ended without it, or a negative RG_ERR_*.
+static int fetch_state(rg_ctx* c, const rg_mb_out* out, int32_t picture, const char* who, int& slot) {
+  slot = c->a_out_ptr[0] == out ? 0 : (c->a_out_ptr[1] == out ? 1 : -1);
+  if (slot < 0 || !c->h_ready[slot]) return fail(RG_ERR_STATE, "%s: no call in flight writes into out", who);
   if (picture < 0 || picture >= c->a_frames[slot] * c->S)
-    return fail(RG_ERR_INVALID, "rg_analyse_gops_fetch: picture %d of %d", picture, c->a_frames[slot] * c->S);
+    return fail(RG_ERR_INVALID, "%s: picture %d of %d", who, picture, c->a_frames[slot] * c->S);
   volatile int* flag = c->h_ready[slot] + picture;
   if (*flag != c->a_seq[slot]) {
     // the launch flags a picture before it ends: after the end, an unflagged picture means a wait
@@ -1236,6 +1345,12 @@ int rg_analyse_gops_fetch(rg_ctx* c, rg_mb_out* out, int32_t picture) {
     if (cudaEventQuery(c->a_kern_done[slot]) != cudaSuccess) return 0;
     if (*flag != c->a_seq[slot]) return 2;
   }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return 1;
+}
+
+// The picture's full records from the slot's device records into out.
+static int fetch_dense(rg_ctx* c, rg_mb_out* out, int slot, int32_t picture) {
   CK(cudaSetDevice(c->cfg.device));
   thread_local cudaStream_t streams[16] = {};
   int dev = c->cfg.device & 15;
@@ -1245,6 +1360,58 @@ int rg_analyse_gops_fetch(rg_ctx* c, rg_mb_out* out, int32_t picture) {
                      cudaMemcpyDeviceToHost, streams[dev]));
   CK(cudaStreamSynchronize(streams[dev]));
   return 1;
+}
+
+int rg_analyse_gops_fetch(rg_ctx* c, rg_mb_out* out, int32_t picture) {
+  if (!c || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_fetch: null argument");
+  int slot = -1;
+  int st = fetch_state(c, out, picture, "rg_analyse_gops_fetch", slot);
+  if (st != 1) return st;
+  return fetch_dense(c, out, slot, picture);
+}
+
+int rg_analyse_gops_fetch_compact(rg_ctx* c, rg_mb_out* out, int32_t picture, const void** data, size_t* bytes) {
+  if (!c || !out || !data || !bytes) return fail(RG_ERR_INVALID, "rg_analyse_gops_fetch_compact: null argument");
+  *data = nullptr;
+  *bytes = 0;
+  int slot = -1;
+  int st = fetch_state(c, out, picture, "rg_analyse_gops_fetch_compact", slot);
+  if (st != 1) return st;
+  if (c->a_compact[slot]) {
+    // the picture's rows, each in its own slot, packed together in place on the first fetch
+    int64_t& packed = c->c_packed[slot][picture];
+    const int H = c->fp.mb_h, row = c->c_row[slot];
+    uint32_t* base = c->h_cwords[slot] + (size_t)picture * H * row;
+    if (packed == -1) {
+      const volatile int* rb = c->h_cbytes[slot] + (size_t)picture * H;
+      int64_t words = 0;
+      for (int y = 0; y < H && packed == -1; y++)
+        if (rb[y] < 0) packed = -2;  // a row did not fit its slot
+      for (int y = 0; y < H && packed == -1; y++) {
+        const int n = rb[y] / 4;
+        if (y) memmove(base + words, base + (size_t)y * row, sizeof(uint32_t) * n);
+        words += n;
+      }
+      if (packed == -1) packed = words * 4;
+    }
+    if (packed >= 0) {
+      *data = base;
+      *bytes = (size_t)packed;
+      return 1;
+    }
+  }
+  return fetch_dense(c, out, slot, picture);
+}
+
+int rg_set_record_compaction(rg_ctx* c, int32_t words_per_mb) {
+  if (!c) return fail(RG_ERR_INVALID, "rg_set_record_compaction: null context");
+  if (words_per_mb < 0 || (words_per_mb > 0 && words_per_mb < RG_COMPACT_MASK_WORDS) ||
+      words_per_mb > RG_COMPACT_MASK_WORDS + (int)(sizeof(rg_mb_out) / 4))
+    return fail(RG_ERR_INVALID, "rg_set_record_compaction: %d words per macroblock (0, or %d..%d)", words_per_mb,
+                RG_COMPACT_MASK_WORDS, RG_COMPACT_MASK_WORDS + (int)(sizeof(rg_mb_out) / 4));
+  if (c->pend_count) return fail(RG_ERR_STATE, "rg_set_record_compaction: calls in flight");
+  c->compact_words = words_per_mb;
+  return RG_OK;
 }
 
 int rg_analyse_gops_wait(rg_ctx* c, const rg_mb_out* out) {

@@ -56,6 +56,15 @@ class H264Encoder:
         if rc:
             raise RgError(rc, lib().rg_last_error().decode())
 
+    def set_record_compaction(self, words_per_mb: int) -> None:
+        """Compact records of the encoder's waves (rg_set_record_compaction on its context, e.g.
+        96 words per macroblock; 0, the default, turns them off); not while waves are in flight."""
+        if self._inflight:
+            raise RgError(-6, "set_record_compaction: waves in flight")
+        rc = lib().rg_set_record_compaction(lib().rg_encoder_context(self.h), int(words_per_mb))
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+
     def encode_frame(self, frame: Frame, stream: int = 0) -> bytes:
         y, u, v = (np.ascontiguousarray(p, np.uint8) for p in frame)
         n = lib().rg_encode_frame(self.h, stream, _u8(y), _u8(u), _u8(v), y.strides[0], u.strides[0],
@@ -130,6 +139,14 @@ class H264Encoder:
         out = np.zeros(n, np.float64)
         lib().rg_encoder_latencies(self.h, out.ctypes.data, n)
         return out.reshape(-1, self.streams) if n else out
+
+    def record_bytes(self) -> int:
+        """Bytes of records the wave collected last brought to the host (rg_encoder_record_bytes):
+        compact records, plus the full records of pictures handed out without them."""
+        n = lib().rg_encoder_record_bytes(self.h)
+        if n < 0:
+            raise RgError(n, lib().rg_last_error().decode())
+        return n
 
     def close(self) -> None:
         if getattr(self, "h", None):

@@ -58,6 +58,8 @@ EXPORTS = [
     "rg_net_predict_hints", "rg_net_check", "rg_net_crops", "rg_net_forward_backward", "rg_net_adam_step",
     "rg_set_hint_net", "rg_encoder_set_form", "rg_ssim_batch_device", "rg_set_search_tuning",
     "rg_net_set_hint_policy", "rg_net_set_coarse_range", "rg_analyse_gops_group",
+    "rg_set_record_compaction", "rg_analyse_gops_fetch_compact", "rg_records_compact", "rg_records_expand",
+    "rg_writer_picture_compact", "rg_encoder_record_bytes", "rg_group_graph_counts",
 ]
 
 
@@ -151,6 +153,17 @@ def lib() -> ctypes.CDLL:
     L.rg_set_stream_qp.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_analyse_gops_stream.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, ctypes.c_int32, P]
     L.rg_analyse_gops_fetch.argtypes = [P, P, ctypes.c_int32]
+    L.rg_set_record_compaction.argtypes = [P, ctypes.c_int32]
+    L.rg_analyse_gops_fetch_compact.argtypes = [P, P, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+                                                ctypes.POINTER(ctypes.c_size_t)]
+    L.rg_records_compact.restype = ctypes.c_int64
+    L.rg_records_compact.argtypes = [P, ctypes.c_int32, P, ctypes.c_size_t]
+    L.rg_records_expand.argtypes = [P, ctypes.c_size_t, ctypes.c_int32, P]
+    L.rg_writer_picture_compact.restype = ctypes.c_int64
+    L.rg_writer_picture_compact.argtypes = [P, P, ctypes.c_size_t, ctypes.c_int32, P, ctypes.c_size_t]
+    L.rg_encoder_record_bytes.restype = ctypes.c_int64
+    L.rg_encoder_record_bytes.argtypes = [P]
+    L.rg_group_graph_counts.argtypes = [P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     L.rg_set_analysis_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_set_hints.argtypes = [P, P, ctypes.c_int32]
     L.rg_encoder_new_gops.argtypes = [P]
@@ -212,6 +225,29 @@ def lib() -> ctypes.CDLL:
 def _check(rc: int) -> None:
     if rc != 0:
         raise RgError(rc, lib().rg_last_error().decode())
+
+
+COMPACT_MASK_WORDS = 7  # RG_COMPACT_MASK_WORDS
+
+
+def compact_records(records: np.ndarray) -> bytes:
+    """The compact form of records (rg_records_compact): per record, COMPACT_MASK_WORDS mask words
+    of its nonzero 32-bit words, then those words in order."""
+    recs = np.ascontiguousarray(records)
+    cap = recs.size * (RECORD_DTYPE.itemsize + 4 * COMPACT_MASK_WORDS)
+    out = np.zeros(max(cap, 4), np.uint8)
+    n = lib().rg_records_compact(recs.ctypes.data, recs.size, out.ctypes.data, out.size)
+    if n < 0:
+        raise RgError(n, lib().rg_last_error().decode())
+    return out[:n].tobytes()
+
+
+def expand_records(data: bytes, n: int) -> np.ndarray:
+    """Records back from their compact form (rg_records_expand)."""
+    buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(4, np.uint8)
+    out = np.zeros(n, RECORD_DTYPE)
+    _check(lib().rg_records_expand(buf.ctypes.data, len(data), n, out.ctypes.data))
+    return out
 
 
 def _u8(a: np.ndarray):
@@ -502,6 +538,15 @@ class BitstreamWriter:
     def picture(self, records: np.ndarray, kind: int) -> bytes:
         records = np.ascontiguousarray(records, dtype=RECORD_DTYPE)
         n = lib().rg_writer_picture(self.h, records.ctypes.data, kind, self.buf.ctypes.data, self.buf.size)
+        if n < 0:
+            raise RgError(n, lib().rg_last_error().decode())
+        return self.buf[:n].tobytes()
+
+    def picture_compact(self, data: bytes, kind: int) -> bytes:
+        """The access unit from the picture's compact records (rg_writer_picture_compact)."""
+        buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(4, np.uint8)
+        n = lib().rg_writer_picture_compact(self.h, buf.ctypes.data, len(data), kind, self.buf.ctypes.data,
+                                            self.buf.size)
         if n < 0:
             raise RgError(n, lib().rg_last_error().decode())
         return self.buf[:n].tobytes()

@@ -4,8 +4,10 @@ against each context analysed alone (rg_analyse_gops_device), GPU tests.
 The batched configuration transcodes many independent streams of several sizes; the group call
 analyses all of them in one launch whose work list interleaves the sizes' segments by key. It must
 not change a single decision: every record and every reconstruction of every context equals the one
-the same context gives alone, over two calls in a row (the second continuing each GOP from the
-reference the first left), in the plain form (with a QP per stream) and in the full-search form.
+the same context gives alone, over three calls in a row (the second continuing each GOP from the
+reference the first left, the third starting new GOPs), in the plain form (with a QP per stream)
+and in the full-search form. The launch is a CUDA graph captured per launch shape: the third call,
+of the first one's shape, replays the first one's graph.
 """
 import numpy as np
 import pytest
@@ -68,8 +70,12 @@ def test_group_launch_equals_each_context_alone(form):
     clips = _clips()
     group = _engines(form, qps)
     alone = _engines(form, qps)
-    for call in range(2):
-        keep, planes, kinds, sy, suv = _call_args(clips, call)
+    for e in group:   # a fixed lag: the launch shape does not follow the reach the calls observe
+        e.set_pipeline_tuning(lag=64)
+    for call in range(3):
+        # call 2 repeats call 0's pictures and kinds (an IDR picture starts each stream's next GOP):
+        # the same launch shape, so its graph is replayed
+        keep, planes, kinds, sy, suv = _call_args(clips, call % 2)
         Engine.analyse_gops_group(group, planes, sy, suv, kinds, F)
         for i, e in enumerate(alone):
             e.analyse_gops_device(planes[i], sy[i], suv[i], kinds[i], F)
@@ -82,6 +88,11 @@ def test_group_launch_equals_each_context_alone(form):
                 for a, b in zip(group[i].recon(s), alone[i].recon(s)):
                     assert np.array_equal(a, b), f"call {call}, size {w}x{h}, stream {s}: reconstruction differs"
         del keep
+    import ctypes
+    from ragdoll_b200.engine import lib
+    captures, launches = ctypes.c_int64(), ctypes.c_int64()
+    assert lib().rg_group_graph_counts(group[0].h, ctypes.byref(captures), ctypes.byref(launches)) == 0
+    assert (captures.value, launches.value) == (2, 3)
     for e in group + alone:
         e.close()
 

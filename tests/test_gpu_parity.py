@@ -318,3 +318,73 @@ def test_derived_lag_follows_the_reach_of_the_searches():
     assert fixed.pipeline_lag() == 24
     for s in range(S):
         assert all(np.array_equal(x, y) for x, y in zip(auto.recon_coded(s), fixed.recon_coded(s)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,words,give_up", [("plain", 48, False), ("plain", 7, False), ("plain", 48, True),
+                                                ("fullsearch", 96, False)])
+def test_compact_records_written_by_the_launch(form, words, give_up):
+    """rg_set_record_compaction: the launch writes each picture's compact records into mapped host
+    memory as its rows complete; rg_analyse_gops_fetch_compact hands them out, and they are exactly
+    rg_records_compact of the bulk call's records. A picture with a macroblock row whose compact
+    records exceed the row's slot (words per macroblock x its macroblocks; here rows of the IDR
+    pictures at 48, every row at 7, the mask words alone) comes as full records instead. give_up: a wait runs out (one warp, lag one
+    macroblock-time); the unfinished pictures come from the re-run as full records."""
+    import ctypes
+    from ragdoll_b200.engine import (RECORD_DTYPE, RG_FORM_FULLSEARCH, RG_FRAME_IDR, RG_FRAME_P, Engine,
+                                     compact_records, lib)
+    w, h, qp, S, F = 320, 180, 24, 3, 5
+    clips = [grating_clip(w, h, F, seed=900 + s, motion=6.0, rects=2) for s in range(S)]
+    pics = [[clips[s][f] for s in range(S)] for f in range(F)]
+    kinds = [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)]
+
+    def engine():
+        e = Engine(w, h, qp, profile=2, num_streams=S, max_frames=F)
+        if form == "fullsearch":
+            e.set_analysis_form(RG_FORM_FULLSEARCH, 16)
+        return e
+    bulk = engine().analyse_gops(pics, kinds)
+    eng = engine()
+    L = lib()
+    assert L.rg_set_record_compaction(eng.h, 3) < 0                       # fewer than the mask words
+    assert L.rg_set_record_compaction(eng.h, words) == 0
+    if give_up:
+        eng.set_pipeline_tuning(lag=1, grid=1, timeout_ms=300)
+    out = np.zeros((F, S, eng.n_mb), RECORD_DTYPE)
+    planes = [np.ascontiguousarray(p) for f in range(F) for s in range(S) for p in pics[f][s]]
+    ptrs = (ctypes.c_void_p * len(planes))(*[p.ctypes.data for p in planes])
+    k = (ctypes.c_int32 * (F * S))(*[kinds[f][s] for f in range(F) for s in range(S)])
+    assert L.rg_analyse_gops_stream(eng.h, ptrs, w, (w + 1) // 2, k, F, out.ctypes.data) == 0
+    assert L.rg_set_record_compaction(eng.h, 0) < 0                       # a call in flight
+    data, nbytes = ctypes.c_void_p(), ctypes.c_size_t()
+    compact, dense, unfinished = {}, set(), set()
+    while len(compact) + len(dense) + len(unfinished) < F * S:
+        for i in range(F * S):
+            if i in compact or i in dense or i in unfinished:
+                continue
+            st = L.rg_analyse_gops_fetch_compact(eng.h, out.ctypes.data, i, ctypes.byref(data), ctypes.byref(nbytes))
+            assert st in (0, 1, 2), st
+            if st == 1 and data.value:
+                compact[i] = ctypes.string_at(data.value, nbytes.value)
+            elif st == 1:
+                dense.add(i)
+            elif st == 2:
+                unfinished.add(i)
+    assert L.rg_analyse_gops_wait(eng.h, out.ctypes.data) == 0
+    flat = bulk.reshape(F * S, -1)
+    for i, c in compact.items():
+        assert c == compact_records(flat[i]), f"picture {i}"
+    got = out.reshape(F * S, -1)
+    for i in dense | unfinished:
+        assert got[i].tobytes() == flat[i].tobytes(), f"picture {i}"
+    mb_w = (w + 15) // 16
+    fits = {i for i in range(F * S)
+            if all(len(compact_records(row)) <= 4 * words * mb_w for row in flat[i].reshape(-1, mb_w))}
+    assert set(compact) == fits - unfinished
+    assert dense == set(range(F * S)) - fits - unfinished
+    assert bool(unfinished) == give_up
+    if words == 7:
+        assert not compact
+    elif not give_up:   # (a wait that gives up early may leave no picture finished)
+        assert compact and (words == 96 or dense)
+    assert L.rg_set_record_compaction(eng.h, 0) == 0
