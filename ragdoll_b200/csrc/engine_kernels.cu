@@ -2056,7 +2056,7 @@ template <int kForm>
 using FormSmem = typename std::conditional<kForm != 0, SearchSmem, NoSearchSmem>::type;
 
 template <int kForm>
-__global__ void __launch_bounds__(32) wavefront_step_kernel(FrameParams fp, const StreamDev* __restrict__ streams, int step) {
+__global__ void __launch_bounds__(32) wavefront_step_kernel(const __grid_constant__ FrameParams fp, const StreamDev* __restrict__ streams, int step) {
   __shared__ Smem sm;
   __shared__ FormSmem<kForm> ss;
   const StreamDev& sd = streams[blockIdx.y];
@@ -2255,7 +2255,7 @@ __device__ __noinline__ void compact_row(const rg_mb_out* rec, uint32_t* dst, in
 // At least 16 warps per SM: up to 128 registers a thread, so nothing spills (4.5 % faster than 20,
 // which held it to 96 registers with spills).
 template <int kForm>
-__global__ void __launch_bounds__(32, 16) pipeline_kernel(FrameGroups fg, const StreamDev* __restrict__ sds, PipeParams pp) {
+__global__ void __launch_bounds__(32, 16) pipeline_kernel(const __grid_constant__ FrameGroups fg, const StreamDev* __restrict__ sds, PipeParams pp) {
   __shared__ Smem sm;
   __shared__ FormSmem<kForm> ss;
   const int lane = lane_id();
