@@ -958,7 +958,7 @@ struct Ctx {
 
 // Loads the source macroblock, replicating the last row / column past the picture edges
 // (enc.rs:400 MbSrc::load, h264.rs:3660 extract_mb_planes).
-__device__ __noinline__ void load_source(const Ctx& c, Smem& sm) {
+__device__ __noinline__ void load_source(const Ctx c, Smem& sm) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int W = fp.width, H = fp.height, cw = (W + 1) >> 1, ch = (H + 1) >> 1;
@@ -976,7 +976,7 @@ __device__ __noinline__ void load_source(const Ctx& c, Smem& sm) {
   __syncwarp();
 }
 // Intra edges from the unfiltered reconstruction of this picture (enc.rs:1459-1521).
-__device__ __noinline__ void load_edges(const Ctx& c, Smem& sm, bool want_topright, int& tl, int* ctl) {
+__device__ __noinline__ void load_edges(const Ctx c, Smem& sm, bool want_topright, int& tl, int* ctl) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   const uint8_t* Y = c.sd->cur_y;
@@ -1001,7 +1001,7 @@ __device__ __noinline__ void load_edges(const Ctx& c, Smem& sm, bool want_toprig
 }
 
 // Stores the reconstruction of pred_y/u/v (or tmp_y for luma) into the current picture.
-__device__ __noinline__ void store_recon(const Ctx& c, const uint8_t* ly, Smem& sm) {
+__device__ __noinline__ void store_recon(const Ctx c, const uint8_t* ly, Smem& sm) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
   int y = lane >> 1, x = (lane & 1) * 8;
@@ -1075,7 +1075,7 @@ __device__ __noinline__ void record_header(rg_mb_out* rec, int type, int i16_mod
   rec->nz_mask = nz;
   rec->reserved1 = 0;
 }
-__device__ __noinline__ void write_info(const Ctx& c, int flags, int cbpl, int mvx, int mvy, int ref, uint16_t nz, const uint8_t* i4m) {
+__device__ __noinline__ void write_info(const Ctx c, int flags, int cbpl, int mvx, int mvy, int ref, uint16_t nz, const uint8_t* i4m) {
   MbInfo inf;
   inf.mv[0] = (int16_t)mvx;
   inf.mv[1] = (int16_t)mvy;
@@ -1098,7 +1098,7 @@ __device__ __noinline__ void write_info(const Ctx& c, int flags, int cbpl, int m
 }
 
 // I16x16 coding and reconstruction (enc.rs:3587 code_i16) with prediction mode `mode`.
-__device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
+__device__ __noinline__ void code_i16(const Ctx c, Smem& sm, int mode, bool ht, bool hl, int tl, const int* ctl) {
   int lane = lane_id();
   int qp = c.sd->qp, qpc = c.sd->qpc;
   pred16_into(mode, sm, sm.pred_y, ht, hl, tl);
@@ -1227,7 +1227,7 @@ __device__ __noinline__ void code_i16(const Ctx& c, Smem& sm, int mode, bool ht,
 // kMask: only the modes of masks[b] (bit m: Intra4x4PredMode m) that are available at block b are
 // tried -- DC alone when none is (the learned form); the plain form tries every available mode.
 template <bool kMask>
-__device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out,
+__device__ __noinline__ bool analyse_i4(const Ctx c, Smem& sm, uint32_t budget, bool ht_mb, bool hl_mb, int tl_mb, int* cbpl_out,
                                         const uint16_t* masks) {
   const FrameParams& fp = *c.fp;
   int lane = lane_id();
@@ -1356,7 +1356,7 @@ __device__ __noinline__ bool analyse_i4(const Ctx& c, Smem& sm, uint32_t budget,
   return true;
 }
 
-__device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
+__device__ __noinline__ void code_i4(const Ctx c, Smem& sm, int cbpl, bool ht, bool hl, const int* ctl) {
   int lane = lane_id();
   int qpc = c.sd->qpc;
   int cmode = analyse_chroma(sm, ht, hl, ctl);
@@ -1377,7 +1377,7 @@ __device__ __noinline__ void code_i4(const Ctx& c, Smem& sm, int cbpl, bool ht, 
 }
 
 // One macroblock of an I slice (enc.rs:3311 code_intra).
-__device__ __noinline__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
+__device__ __noinline__ void analyse_intra_mb(const Ctx c, Smem& sm) {
   int tl, ctl[2];
   load_edges(c, sm, true, tl, ctl);
   bool ht = c.mby > 0, hl = c.mbx > 0;
@@ -1395,7 +1395,7 @@ __device__ __noinline__ void analyse_intra_mb(const Ctx& c, Smem& sm) {
 }
 
 // Codes P_Skip with vector mv; prediction already in pred_y / pred_u / pred_v.
-__device__ __noinline__ void code_skip(const Ctx& c, Smem& sm, int mvx, int mvy) {
+__device__ __noinline__ void code_skip(const Ctx c, Smem& sm, int mvx, int mvy) {
   int lane = lane_id();
   rg_mb_out* rec = c.sd->rec + c.mb;
   if (lane < 16) {
@@ -1517,7 +1517,7 @@ struct PipeWait {
 // One macroblock of a P slice (enc.rs:3011 code_p_mb). In the pipelined mode (pw != null) it
 // first waits for the reference frame to be final over every sample its search can read; when
 // a wait gives up it returns with pw->failed set and writes nothing.
-__device__ __noinline__ void analyse_p_mb(const Ctx& c, Smem& sm, PipeWait* pw) {
+__device__ __noinline__ void analyse_p_mb(const Ctx c, Smem& sm, PipeWait* pw) {
   const FrameParams& fp = *c.fp;
   const StreamDev& sd = *c.sd;
   int lane = lane_id();

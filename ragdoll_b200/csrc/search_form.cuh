@@ -62,7 +62,7 @@ __device__ __forceinline__ void ld_q(const MbMv4* m, int q, int* v) {
   v[0] = (int16_t)(w & 0xffffu);
   v[1] = (int16_t)(w >> 16);
 }
-__device__ __noinline__ MbNb load_nb(const Ctx& c) {
+__device__ __noinline__ MbNb load_nb(const Ctx c) {
   const StreamDev& sd = *c.sd;
   const int mb_w = c.fp->mb_w, mb = c.mb;
   MbNb n;
@@ -147,7 +147,7 @@ __device__ __forceinline__ uint32_t lds4u(const uint8_t* p) {
 }
 // A window of at most 32 vectors (the learned form's): lane v takes vector v in raster order and
 // sums its four quadrant SADs over the staged band; the same costs and ties as the wide search.
-__device__ __noinline__ void int_search_small(const Ctx& c, const Smem& sm, SearchSmem& ss, int xlo, int xhi, int ylo,
+__device__ __noinline__ void int_search_small(const Ctx c, const Smem& sm, SearchSmem& ss, int xlo, int xhi, int ylo,
                                               int yhi, int mvp0, int mvp1, uint32_t lambda, IntBest& ib) {
   const int lane = lane_id();
   const int x0 = c.mbx * 16, y0 = c.mby * 16, stride = c.fp->stride_y;
@@ -188,7 +188,7 @@ __device__ __noinline__ void int_search_small(const Ctx& c, const Smem& sm, Sear
   }
 }
 
-__device__ __noinline__ void int_search(const Ctx& c, const Smem& sm, SearchSmem& ss, int xlo, int xhi, int ylo, int yhi,
+__device__ __noinline__ void int_search(const Ctx c, const Smem& sm, SearchSmem& ss, int xlo, int xhi, int ylo, int yhi,
                                         int mvp0, int mvp1, uint32_t lambda, IntBest& ib) {
   if ((xhi - xlo + 1) * (yhi - ylo + 1) <= 32) {
     int_search_small(c, sm, ss, xlo, xhi, ylo, yhi, mvp0, mvp1, lambda, ib);
@@ -318,7 +318,7 @@ struct WinState {
   int bx, by;  // integer vector of the planes held, or kNoWin
 };
 constexpr int kNoWin = 1 << 20;
-__device__ __forceinline__ void ensure_window(const Ctx& c, Smem& sm, WinState& ws, int bx, int by) {
+__device__ __forceinline__ void ensure_window(const Ctx c, Smem& sm, WinState& ws, int bx, int by) {
   if (ws.bx == bx && ws.by == by) return;
   stage_window(c.sd->ref_y, c.fp->stride_y, c.mbx * 16 + bx - 1, c.mby * 16 + by - 1, sm);
   build_hpel(sm, 7);
@@ -326,7 +326,7 @@ __device__ __forceinline__ void ensure_window(const Ctx& c, Smem& sm, WinState& 
   ws.by = by;
 }
 
-__device__ __noinline__ PartFit refine_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
+__device__ __noinline__ PartFit refine_part(const Ctx c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
                                             int by, int2 mvp, uint32_t lambda, Bounds bd) {
   const int lane = lane_id();
   ensure_window(c, sm, ws, bx, by);
@@ -396,7 +396,7 @@ __device__ __noinline__ uint32_t part_sad(const Smem& sm, int px, int py, int pw
   }
   return wsum(s);
 }
-__device__ __noinline__ PartFit refine_part_sad(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph,
+__device__ __noinline__ PartFit refine_part_sad(const Ctx c, Smem& sm, WinState& ws, int px, int py, int pw, int ph,
                                                 int bx, int by, int2 mvp, uint32_t lambda, Bounds bd) {
   ensure_window(c, sm, ws, bx, by);
   int cx = 4 * bx, cy = 4 * by;
@@ -418,7 +418,7 @@ __device__ __noinline__ PartFit refine_part_sad(const Ctx& c, Smem& sm, WinState
 
 // The luma prediction of a part at quarter-sample vector mv (within 3 quarter samples of 4 (bx, by),
 // the integer vector its refinement started from) into pred_y.
-__device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
+__device__ __noinline__ void predict_part(const Ctx c, Smem& sm, WinState& ws, int px, int py, int pw, int ph, int bx,
                                           int by, int mvx, int mvy) {
   const int lane = lane_id();
   ensure_window(c, sm, ws, bx, by);
@@ -433,7 +433,7 @@ __device__ __noinline__ void predict_part(const Ctx& c, Smem& sm, WinState& ws, 
 }
 // Chroma prediction of both planes with each 8x8 luma quadrant's own vector (4x4 chroma blocks;
 // the bilinear 1/8-sample filter of chroma_mc_8x8_x2, h264_enc.rs:1279, per sample).
-__device__ __noinline__ void mc_chroma_q(const Ctx& c, Smem& sm, const int (*qmv)[2]) {
+__device__ __noinline__ void mc_chroma_q(const Ctx c, Smem& sm, const int (*qmv)[2]) {
   const FrameParams& fp = *c.fp;
   const StreamDev& sd = *c.sd;
   const int lane = lane_id();
@@ -454,7 +454,7 @@ __device__ __noinline__ void mc_chroma_q(const Ctx& c, Smem& sm, const int (*qmv
 
 // Search-form side state of a coded macroblock: the record's partition fields and the quadrant
 // vectors later macroblocks and the deblocking filter read (lane 0 writes).
-__device__ __noinline__ void search_tail(const Ctx& c, int ptype, const int (*qmv)[2], const int (*pmvd)[2]) {
+__device__ __noinline__ void search_tail(const Ctx c, int ptype, const int (*qmv)[2], const int (*pmvd)[2]) {
   if (lane_id() != 0) return;
   rg_mb_out* rec = c.sd->rec + c.mb;
   MbMv4 m;
@@ -475,7 +475,7 @@ __device__ __noinline__ void search_tail(const Ctx& c, int ptype, const int (*qm
 // sample the integer search (band staging), the refinement windows and the final prediction can
 // read lies above row (y0 + yhi + 28) and left of column (x0 + xhi + 36); everything above and
 // to the left of the macroblock holding that sample is final once it is.
-__device__ __noinline__ bool wait_window(const Ctx& c, PipeWait* pw, int xhi, int yhi) {
+__device__ __noinline__ bool wait_window(const Ctx c, PipeWait* pw, int xhi, int yhi) {
   const FrameParams& fp = *c.fp;
   if (!pw) return true;
   const int x0 = c.mbx * 16, y0 = c.mby * 16;
@@ -497,7 +497,7 @@ __device__ __noinline__ bool wait_window(const Ctx& c, PipeWait* pw, int xhi, in
 
 // P_Skip probe of the plain form (enc.rs:2906 try_p_skip) at skip vector (ps0, ps1): true when the
 // macroblock is coded as P_Skip (prediction left in pred_y / pred_u / pred_v).
-__device__ __noinline__ bool skip_probe(const Ctx& c, Smem& sm, int ps0, int ps1, const Bounds& bd) {
+__device__ __noinline__ bool skip_probe(const Ctx c, Smem& sm, int ps0, int ps1, const Bounds& bd) {
   const FrameParams& fp = *c.fp;
   const StreamDev& sd = *c.sd;
   const int lane = lane_id();
@@ -539,7 +539,7 @@ __device__ __noinline__ bool skip_probe(const Ctx& c, Smem& sm, int ps0, int ps1
 
 // Learned form: the centre of the first +-2 window among n integer candidates (cx, cy; ok false:
 // absent) -- the first of least 16x16 SAD + lambda * vector bits against the 16x16 predictor.
-__device__ __noinline__ void learned_centre(const Ctx& c, const Smem& sm, const int* cx, const int* cy, const bool* ok,
+__device__ __noinline__ void learned_centre(const Ctx c, const Smem& sm, const int* cx, const int* cy, const bool* ok,
                                             int n, int mvp0, int mvp1, uint32_t lambda, int& bx, int& by) {
   const int lane = lane_id();
   const int stride = c.fp->stride_y;
@@ -573,7 +573,7 @@ __device__ __constant__ int8_t c_type_parts[4] = {1, 2, 2, 4};
 __device__ __constant__ uint8_t c_part_quads[9] = {15, 3, 12, 5, 10, 1, 2, 4, 8};
 
 // One macroblock of a P slice in the search forms (see the head of this file).
-__device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchSmem& ss, PipeWait* pw) {
+__device__ __noinline__ void analyse_p_mb_search(const Ctx c, Smem& sm, SearchSmem& ss, PipeWait* pw) {
   const FrameParams& fp = *c.fp;
   const StreamDev& sd = *c.sd;
   const int lane = lane_id();
@@ -817,7 +817,7 @@ __device__ __noinline__ void analyse_p_mb_search(const Ctx& c, Smem& sm, SearchS
 
 // One macroblock of an I slice in the search forms: the plain analysis (enc.rs:3311 code_intra),
 // intra 4x4 blocks restricted to the hinted modes in the learned form.
-__device__ __noinline__ void analyse_intra_mb_search(const Ctx& c, Smem& sm) {
+__device__ __noinline__ void analyse_intra_mb_search(const Ctx c, Smem& sm) {
   int tl, ctl[2];
   load_edges(c, sm, true, tl, ctl);
   bool ht = c.mby > 0, hl = c.mbx > 0;
