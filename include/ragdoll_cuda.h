@@ -204,6 +204,23 @@ int rg_analyse_gops_device(rg_ctx* ctx, const uint8_t* const* dev_planes, size_t
 int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
                           const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
                           int32_t frames);
+/*
+ * rg_analyse_gops_async for n contexts in one group launch (as rg_analyse_gops_group): each
+ * context's host sources (planes[i], strides of its own size) are copied into its staging, the one
+ * launch analyses every context's pictures, and each context's records are copied into outs[i]
+ * (frames * its num_streams * its macroblocks, picture-major). rg_analyse_gops_wait(ctxs[i],
+ * outs[i]) waits for context i's records (re-running its pictures if a wait of the launch gave up).
+ * The batched transcode's waves of many streams of several sizes, one launch per wave.
+ */
+int rg_analyse_gops_group_async(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* planes,
+                                const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                                int32_t frames, rg_mb_out* const* outs);
+/* rg_analyse_gops_group_async without the copy of all records at the end, as
+ * rg_analyse_gops_stream: rg_analyse_gops_fetch(ctxs[i], outs[i], picture) copies each of context
+ * i's pictures as the launch flags it final, and rg_analyse_gops_wait(ctxs[i], outs[i]) ends it. */
+int rg_analyse_gops_group_stream(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* planes,
+                                 const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                                 int32_t frames, rg_mb_out* const* outs);
 /* Group calls led by ctx (ctxs[0]) so far: graphs captured and graph launches. */
 int rg_group_graph_counts(const rg_ctx* ctx, int64_t* captures, int64_t* launches);
 
@@ -605,6 +622,16 @@ int64_t rg_encode_frame(rg_encoder* enc, int32_t stream, const uint8_t* y, const
  * may be reused after the wave is collected; pinned sources copy fastest.
  */
 int rg_encoder_submit(rg_encoder* enc, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, int32_t frames);
+/*
+ * rg_encoder_submit for n encoders of different picture sizes at once (1..8 encoders on one
+ * device, all in the plain form or all in the full-search form): every stream of every encoder is
+ * analysed by ONE persistent launch (rg_analyse_gops_group_async; a CUDA graph per launch shape),
+ * and each encoder's wave is then collected on its own (rg_encoder_collect, from any thread),
+ * its pictures written as the launch finishes them. planes[i], stride_y[i], stride_uv[i]: encoder i's
+ * arguments as rg_encoder_submit takes them. The batched transcode of many streams of mixed size.
+ */
+int rg_encoder_submit_group(rg_encoder* const* encs, int32_t n, const uint8_t* const* const* planes,
+                            const size_t* stride_y, const size_t* stride_uv, int32_t frames);
 /*
  * The access units of the oldest wave, written on the pool's threads: concatenated picture-major
  * ([f][s]) into out, sizes[f * num_streams + s] their sizes; returns the total. With out NULL only

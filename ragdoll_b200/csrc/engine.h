@@ -72,6 +72,9 @@ struct StreamDev {
   int32_t walk;            // learned form: re-centrings of the seed's window before the full search
   uint16_t type_bits[4];   // search forms: bits charged per partition type (x lambda)
   uint16_t pad3_[4];
+  // pipelined launches: this picture's ready flag in mapped host memory (null: the launch's
+  // ready array at the descriptor's index, if any)
+  int32_t* ready;
 };
 
 // Frame-constant parameters of one wavefront (all streams share the size; qp / qpc / sb_* are the

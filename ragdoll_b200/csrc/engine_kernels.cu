@@ -2332,8 +2332,8 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(const __grid_constant_
         publish(ana_rows + y, x + 1);
       }
       // (with compact records, the row is counted once its deblocking warp has compacted it)
-      if (!failed && x1 == Wm && pp.ready && !pp.cwords)
-        picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
+      int* const rdy = sd.ready ? sd.ready : (pp.ready ? pp.ready + ps : nullptr);
+      if (!failed && x1 == Wm && rdy && !pp.cwords) picture_row_done(pp.rows_done + ps, rdy, pp.seq, H);
       reach_y = pw.reach_y;
       reach_x = pw.reach_x;
     } else {
@@ -2366,7 +2366,8 @@ __global__ void __launch_bounds__(32, 16) pipeline_kernel(const __grid_constant_
         const long long r = (long long)sd.rows_base + y;
         compact_row(sd.rec + (size_t)y * Wm, pp.cwords + r * pp.crow, pp.crow, pp.cbytes + r, Wm,
                     reinterpret_cast<uint32_t*>(&sm));
-        if (pp.ready) picture_row_done(pp.rows_done + ps, pp.ready + ps, pp.seq, H);
+        int* const rdy = sd.ready ? sd.ready : (pp.ready ? pp.ready + ps : nullptr);
+        if (rdy) picture_row_done(pp.rows_done + ps, rdy, pp.seq, H);
       }
     }
     if (failed) break;

@@ -229,12 +229,23 @@ int64_t rg_encode_frame(rg_encoder* e, int32_t stream, const uint8_t* y, const u
   return (int64_t)au.size();
 }
 
-int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, int32_t frames) {
-  if (!e || !planes) return efail(RG_ERR_INVALID, "rg_encoder_submit: null argument");
+}  // extern "C"
+
+namespace {
+
+// The next wave of encoder e (frames pictures of every stream): its pinned records, picture
+// counters and kinds; the counters before it in `saved` (restored by rollback when the wave is
+// not queued).
+struct WaveStart {
+  std::vector<int64_t> coded;
+  std::vector<uint32_t> idrs, since;
+  std::vector<int32_t> kinds;
+};
+int start_wave(rg_encoder* e, int32_t frames, const char* who, WaveStart& ws) {
   const int S = (int)e->coded.size();
   if (frames < 1 || frames > std::max(e->cfg.max_frames, 1))
-    return efail(RG_ERR_INVALID, "rg_encoder_submit: %d pictures per stream (max_frames %d)", frames, e->cfg.max_frames);
-  if (e->pending == 2) return efail(RG_ERR_STATE, "rg_encoder_submit: two waves in flight; collect one first");
+    return efail(RG_ERR_INVALID, "%s: %d pictures per stream (max_frames %d)", who, frames, e->cfg.max_frames);
+  if (e->pending == 2) return efail(RG_ERR_STATE, "%s: two waves in flight; collect one first", who);
   Wave& w = e->waves[(e->head + e->pending) & 1];
   if (!w.recs) {  // both waves' pinned records at once: pinning takes a while, and not mid-stream
     size_t bytes = sizeof(rg_mb_out) * e->n_mb * S * std::max(e->cfg.max_frames, 1);
@@ -242,7 +253,7 @@ int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride
       if (!v.recs && cudaHostAlloc((void**)&v.recs, bytes, cudaHostAllocDefault) != cudaSuccess) {
         v.recs = nullptr;
         cudaGetLastError();
-        return efail(RG_ERR_OOM, "rg_encoder_submit: %zu bytes of pinned host memory", bytes);
+        return efail(RG_ERR_OOM, "%s: %zu bytes of pinned host memory", who, bytes);
       }
   }
   w.submitted = std::chrono::steady_clock::now();
@@ -251,23 +262,68 @@ int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride
   w.idr.resize((size_t)frames * S);
   w.since.resize((size_t)frames * S);
   w.idr_id.resize((size_t)frames * S);
-  std::vector<int32_t> kinds((size_t)frames * S);
-  std::vector<int64_t> coded = e->coded;
-  std::vector<uint32_t> idrs = e->idrs, since = e->since;
+  ws.kinds.assign((size_t)frames * S, 0);
+  ws.coded = e->coded;
+  ws.idrs = e->idrs;
+  ws.since = e->since;
   for (int f = 0; f < frames; f++)
     for (int s = 0; s < S; s++) {
       const size_t i = (size_t)f * S + s;
       e->next_picture(s, w.idr[i], w.since[i], w.idr_id[i]);
-      kinds[i] = w.idr[i] ? RG_FRAME_IDR : RG_FRAME_P;
+      ws.kinds[i] = w.idr[i] ? RG_FRAME_IDR : RG_FRAME_P;
     }
-  int r = rg_analyse_gops_stream(e->ctx, planes, stride_y, stride_uv, kinds.data(), frames, w.recs);
+  return RG_OK;
+}
+void rollback_wave(rg_encoder* e, const WaveStart& ws) {
+  e->coded = ws.coded;
+  e->idrs = ws.idrs;
+  e->since = ws.since;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rg_encoder_submit(rg_encoder* e, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, int32_t frames) {
+  if (!e || !planes) return efail(RG_ERR_INVALID, "rg_encoder_submit: null argument");
+  WaveStart ws;
+  int r = start_wave(e, frames, "rg_encoder_submit", ws);
+  if (r) return r;
+  Wave& w = e->waves[(e->head + e->pending) & 1];
+  r = rg_analyse_gops_stream(e->ctx, planes, stride_y, stride_uv, ws.kinds.data(), frames, w.recs);
   if (r) {
-    e->coded = coded;
-    e->idrs = idrs;
-    e->since = since;
+    rollback_wave(e, ws);
     return r;
   }
   e->pending++;
+  return RG_OK;
+}
+
+int rg_encoder_submit_group(rg_encoder* const* encs, int32_t n, const uint8_t* const* const* planes,
+                            const size_t* stride_y, const size_t* stride_uv, int32_t frames) {
+  if (!encs || !planes || !stride_y || !stride_uv || n < 1)
+    return efail(RG_ERR_INVALID, "rg_encoder_submit_group: null argument or %d encoders", n);
+  std::vector<WaveStart> ws(n);
+  std::vector<rg_ctx*> ctxs(n);
+  std::vector<const int32_t*> kinds(n);
+  std::vector<rg_mb_out*> outs(n);
+  for (int i = 0; i < n; i++) {
+    rg_encoder* e = encs[i];
+    int r = e ? start_wave(e, frames, "rg_encoder_submit_group", ws[i]) : efail(RG_ERR_INVALID, "rg_encoder_submit_group: null encoder %d", i);
+    if (r) {
+      for (int j = 0; j < i; j++) rollback_wave(encs[j], ws[j]);
+      return r;
+    }
+    ctxs[i] = e->ctx;
+    kinds[i] = ws[i].kinds.data();
+    outs[i] = e->waves[(e->head + e->pending) & 1].recs;
+  }
+  int r = rg_analyse_gops_group_stream(ctxs.data(), n, planes, stride_y, stride_uv, kinds.data(), frames, outs.data());
+  if (r) {
+    for (int i = 0; i < n; i++) rollback_wave(encs[i], ws[i]);
+    return r;
+  }
+  for (int i = 0; i < n; i++) encs[i]->pending++;
   return RG_OK;
 }
 
@@ -300,26 +356,28 @@ int64_t rg_encoder_collect(rg_encoder* e, uint8_t* out, size_t cap, int64_t* siz
       w.latency_ms[i] =
           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w.submitted).count();
     };
-    e->pool->run(n, [&](int i, int worker) {
-      const void* data = nullptr;
-      size_t bytes = 0;
-      for (int spins = 0;; spins++) {
-        int st = rg_analyse_gops_fetch_compact(e->ctx, w.recs, i, &data, &bytes);
-        if (st == 1) break;
-        if (st != 0) {
-          later[i] = 1;
-          return;
+    {  // a wave of rg_encoder_submit or of rg_encoder_submit_group alike
+      e->pool->run(n, [&](int i, int worker) {
+        const void* data = nullptr;
+        size_t bytes = 0;
+        for (int spins = 0;; spins++) {
+          int st = rg_analyse_gops_fetch_compact(e->ctx, w.recs, i, &data, &bytes);
+          if (st == 1) break;
+          if (st != 0) {
+            later[i] = 1;
+            return;
+          }
+          std::this_thread::sleep_for(std::chrono::microseconds(spins < 64 ? 20 : 200));
         }
-        std::this_thread::sleep_for(std::chrono::microseconds(spins < 64 ? 20 : 200));
-      }
-      write(i, worker, data, bytes);
-    });
-    int r = rg_analyse_gops_wait(e->ctx, w.recs);  // the launch's end; a re-run if a wait gave up
-    if (r) return r;
-    std::vector<int> rest;
-    for (int i = 0; i < n; i++)
-      if (later[i]) rest.push_back(i);
-    if (!rest.empty()) e->pool->run((int)rest.size(), [&](int k, int worker) { write(rest[k], worker, nullptr, 0); });
+        write(i, worker, data, bytes);
+      });
+      int r = rg_analyse_gops_wait(e->ctx, w.recs);  // the launch's end; a re-run if a wait gave up
+      if (r) return r;
+      std::vector<int> rest;
+      for (int i = 0; i < n; i++)
+        if (later[i]) rest.push_back(i);
+      if (!rest.empty()) e->pool->run((int)rest.size(), [&](int k, int worker) { write(rest[k], worker, nullptr, 0); });
+    }
     if (err.load()) return err.load();
     w.written = true;
   }

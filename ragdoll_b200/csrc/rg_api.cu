@@ -454,6 +454,8 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
                              const int32_t* kinds, rg_mb_out* rec_base, int only = -1,
                              const rg_mb_hint* const* hints = nullptr);
 static int take_hints(rg_ctx* c, int count, const char* who, std::vector<const rg_mb_hint*>& out);
+static int async_copy_in(rg_ctx* c, int slot, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                         int32_t frames, std::vector<const uint8_t*>& dev, const char* who);
 static int resolve_pending(rg_ctx* c, bool wait_out);
 static int resolve_oldest(rg_ctx* c);
 static int auto_lag(const rg_ctx* c);
@@ -544,6 +546,7 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
     d.search_range = c->search_range;
     d.walk = c->walk;
     for (int k = 0; k < 4; k++) { d.type_bits[k] = c->type_bits[k]; d.pad3_[k] = 0; }
+    d.ready = nullptr;
   }
   FrameParams fp = c->fp;
   fp.src_stride_y = (int)stride_y;
@@ -570,7 +573,7 @@ static int enqueue_wavefront(rg_ctx* c, const uint8_t* const* dev_planes, size_t
 // rows_base, and its picture size is group `group`.
 static void gop_desc(const rg_ctx* c, StreamDev& d, int f, int s, const uint8_t* const* dev_planes,
                      const int32_t* kinds, rg_mb_out* rec_base, const rg_mb_hint* hint, int group, int desc_base,
-                     int rows_base) {
+                     int rows_base, int* ready = nullptr) {
   const int S = c->S, g = c->frames[s] + f;
   const int cur = g % c->nslots, prv = (g + c->nslots - 1) % c->nslots;
   d.src_y = dev_planes[(f * S + s) * 3];
@@ -596,6 +599,7 @@ static void gop_desc(const rg_ctx* c, StreamDev& d, int f, int s, const uint8_t*
   d.search_range = c->search_range;
   d.walk = c->walk;
   for (int k = 0; k < 4; k++) { d.type_bits[k] = c->type_bits[k]; d.pad3_[k] = 0; }
+  d.ready = ready ? ready + f * S + s : nullptr;
 }
 
 static int enqueue_gops(rg_ctx* c, const uint8_t* const* dev_planes, size_t stride_y, size_t stride_uv,
@@ -715,10 +719,14 @@ int rg_analyse_gops_device(rg_ctx* c, const uint8_t* const* dev_planes, size_t s
 
 // ---- several contexts, one persistent launch ----------------------------------------------------
 // The leader (ctxs[0]) keeps the launch's descriptors, counters and merged work list.
-int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
-                          const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
-                          int32_t frames) {
-  const char* who = "rg_analyse_gops_group";
+// The group launch (rg_analyse_gops_group): each context's records at rec_bases[i] (null: its own
+// records buffer); resolved: the caller already resolved every context's earlier calls.
+// readies (or null): per context the device address of its per-picture ready flags, set to seq
+// as each picture's records are final.
+static int group_launch(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
+                        const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds, int32_t frames,
+                        rg_mb_out* const* rec_bases, bool resolved, const char* who, int* const* readies = nullptr,
+                        int seq = 0) {
   if (!ctxs || !dev_planes || !stride_y || !stride_uv || !kinds || n < 1 || n > kMaxGroups)
     return fail(RG_ERR_INVALID, "%s: null argument or %d contexts (1..%d)", who, n, kMaxGroups);
   rg_ctx* L = ctxs[0];
@@ -737,7 +745,7 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
   }
   for (int i = 0; i < n; i++) {
     rg_ctx* c = ctxs[i];
-    int r = resolve_pending(c, false);
+    int r = resolved ? RG_OK : resolve_pending(c, false);
     if (r) return r;
     for (int f = 0; f < frames; f++)
       for (int s = 0; s < c->S; s++) {
@@ -801,8 +809,9 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     fg.g[i].src_stride_uv = (int)stride_uv[i];
     for (int f = 0; f < frames; f++)
       for (int s = 0; s < c->S; s++)
-        gop_desc(c, L->g_hstreams[desc_base[i] + f * c->S + s], f, s, dev_planes[i], kinds[i], c->recs, nullptr, i,
-                 desc_base[i], rows_base[i]);
+        gop_desc(c, L->g_hstreams[desc_base[i] + f * c->S + s], f, s, dev_planes[i], kinds[i],
+                 rec_bases && rec_bases[i] ? rec_bases[i] : c->recs, nullptr, i, desc_base[i], rows_base[i],
+                 readies ? readies[i] : nullptr);
   }
   // launch shape: the segment length and SM roles of the context with the most macroblocks (its
   // tuning suits the bulk of the work), the largest grid of any
@@ -901,7 +910,7 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
   key.insert(key.end(), {n_desc, total_rows, (int64_t)n_counters, (int64_t)L->g_ntasks, T->deblock_sms,
                          T->intra_sms, L->sms, (int64_t)T->timeout_ns, (int64_t)(uintptr_t)L->g_dstreams,
                          (int64_t)(uintptr_t)L->g_hstreams, (int64_t)(uintptr_t)L->g_counters,
-                         (int64_t)(uintptr_t)L->g_dtasks, L->form});
+                         (int64_t)(uintptr_t)L->g_dtasks, L->form, seq});
   for (int i = 0; i < n; i++)
     key.insert(key.end(), {(int64_t)stride_y[i], (int64_t)stride_uv[i], (int64_t)(uintptr_t)(ctxs[i]->d_err + pslot[i])});
   rg_ctx::GroupGraph* gg = nullptr;
@@ -922,7 +931,7 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     if (e == cudaSuccess) e = cudaMemsetAsync(L->g_counters, 0, sizeof(int) * n_counters, L->stream);
     if (e == cudaSuccess) {
       launch_pipeline(fg, L->g_dstreams, n_desc, total_rows, L->g_counters, L->g_dtasks, L->g_ntasks, L->g_qbeg,
-                      L->g_qend, T->deblock_sms, T->intra_sms, L->sms, seg, grid, T->timeout_ns, nullptr, 0, nullptr,
+                      L->g_qend, T->deblock_sms, T->intra_sms, L->sms, seg, grid, T->timeout_ns, nullptr, seq, nullptr,
                       nullptr, L->stream, L->form != RG_FORM_PLAIN);
       for (int i = 0; i < n; i++)
         launch_error_to_host(L->g_counters, n_desc, total_rows, ctxs[i]->d_err + pslot[i],
@@ -957,7 +966,7 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     p.frames = frames;
     p.sy = stride_y[i];
     p.suv = stride_uv[i];
-    p.rec = c->recs;
+    p.rec = rec_bases && rec_bases[i] ? rec_bases[i] : c->recs;
     p.out = nullptr;
     p.out_bytes = 0;
     p.hints.clear();
@@ -965,6 +974,91 @@ int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* 
     for (int s = 0; s < c->S; s++) c->frames[s] += frames;
   }
   return RG_OK;
+}
+
+int rg_analyse_gops_group(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* dev_planes,
+                          const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                          int32_t frames) {
+  return group_launch(ctxs, n, dev_planes, stride_y, stride_uv, kinds, frames, nullptr, false,
+                      "rg_analyse_gops_group");
+}
+
+// rg_analyse_gops_group_async (bulk: each context's records copied out after the launch) and
+// rg_analyse_gops_group_stream (each picture flagged as its records are final, fetched per picture).
+static int group_async(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* planes, const size_t* stride_y,
+                       const size_t* stride_uv, const int32_t* const* kinds, int32_t frames, rg_mb_out* const* outs,
+                       bool bulk, const char* who) {
+  if (!ctxs || !planes || !stride_y || !stride_uv || !kinds || !outs || n < 1 || n > kMaxGroups)
+    return fail(RG_ERR_INVALID, "%s: null argument or %d contexts (1..%d)", who, n, kMaxGroups);
+  for (int i = 0; i < n; i++)
+    if (!ctxs[i] || !planes[i] || !kinds[i] || !outs[i]) return fail(RG_ERR_INVALID, "%s: null argument %d", who, i);
+  // each context's sources into its next staging slot (copy-in streams, overlapping the launches
+  // still running)
+  std::vector<std::vector<const uint8_t*>> dev(n);
+  std::vector<const uint8_t* const*> devp(n);
+  std::vector<int> slot(n);
+  std::vector<rg_mb_out*> recs(n);
+  std::vector<size_t> sy(n), suv(n);
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    slot[i] = c->a_slot;
+    int r = async_copy_in(c, slot[i], planes[i], stride_y[i], stride_uv[i], frames, dev[i], who);
+    if (r) return r;
+    devp[i] = dev[i].data();
+    recs[i] = c->a_recs[slot[i]];
+    sy[i] = c->cfg.width;
+    suv[i] = (c->cfg.width + 1) / 2;
+  }
+  // earlier calls resolved (re-run if a wait gave up) before any launch stream waits for a copy
+  for (int i = 0; i < n; i++) {
+    int r = resolve_pending(ctxs[i], false);
+    if (r) return r;
+  }
+  // streamed: the slot's flags cleared (its last call was resolved and fetched), each picture's set
+  // to 1 by the launch (a constant, so the launch's CUDA graph replays)
+  std::vector<int*> readies(n);
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    CK(cudaStreamWaitEvent(c->stream, c->a_in_done[slot[i]], 0));
+    CK(cudaStreamWaitEvent(c->stream, c->a_out_done[slot[i]], 0));
+    if (!bulk) memset((void*)c->h_ready[slot[i]], 0, sizeof(int) * (size_t)frames * c->S);
+    readies[i] = c->d_ready[slot[i]];
+  }
+  int r = group_launch(ctxs, n, devp.data(), sy.data(), suv.data(), kinds, frames, recs.data(), true, who,
+                       bulk ? nullptr : readies.data(), bulk ? 0 : 1);
+  if (r) return r;
+  // each context's records out on its copy-out stream once the launch is done (its stream waits
+  // for the launch); its pending call copies them again if it has to be re-run
+  for (int i = 0; i < n; i++) {
+    rg_ctx* c = ctxs[i];
+    const int sl = slot[i];
+    c->a_slot = sl ^ 1;
+    c->a_seq[sl] = bulk ? 0 : 1;
+    c->a_frames[sl] = frames;
+    c->a_compact[sl] = false;
+    CK(cudaEventRecord(c->a_kern_done[sl], c->stream));
+    const size_t bytes = sizeof(rg_mb_out) * c->n_mb * c->S * frames;
+    CK(cudaStreamWaitEvent(c->a_out, c->a_kern_done[sl], 0));
+    if (bulk) CK(cudaMemcpyAsync(outs[i], c->a_recs[sl], bytes, cudaMemcpyDeviceToHost, c->a_out));
+    CK(cudaEventRecord(c->a_out_done[sl], c->a_out));
+    c->a_out_ptr[sl] = outs[i];
+    rg_ctx::Pending& p = c->pend[(c->pend_head + c->pend_count - 1) & 1];  // the call just queued
+    p.out = outs[i];
+    p.out_bytes = bytes;
+  }
+  return RG_OK;
+}
+
+int rg_analyse_gops_group_async(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* planes,
+                                const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                                int32_t frames, rg_mb_out* const* outs) {
+  return group_async(ctxs, n, planes, stride_y, stride_uv, kinds, frames, outs, true, "rg_analyse_gops_group_async");
+}
+
+int rg_analyse_gops_group_stream(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* const* planes,
+                                 const size_t* stride_y, const size_t* stride_uv, const int32_t* const* kinds,
+                                 int32_t frames, rg_mb_out* const* outs) {
+  return group_async(ctxs, n, planes, stride_y, stride_uv, kinds, frames, outs, false, "rg_analyse_gops_group_stream");
 }
 
 int rg_group_graph_counts(const rg_ctx* c, int64_t* captures, int64_t* launches) {
@@ -1225,15 +1319,9 @@ int rg_sync(rg_ctx* c) {
 
 // rg_analyse_gops_async (bulk: the records copied out after the launch) and rg_analyse_gops_stream
 // (the host fetches each picture's records once the launch flags them final).
-static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
-                      int32_t frames, rg_mb_out* out, bool bulk) {
-  if (!c || !planes || !kinds || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: null argument");
-  if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: frames %d", frames);
-  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
-  if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: stride too small");
-  int S = c->S;
-  for (int i = 0; i < 3 * S * frames; i++)
-    if (!planes[i]) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: picture %d stream %d null plane", i / 3 / S, (i / 3) % S);
+// The asynchronous calls' two slots of staging, records and events, allocated on first use.
+static int async_setup(rg_ctx* c) {
+  const int S = c->S;
   if (!c->a_in) {
     size_t nsrc = c->src_bytes() * S * c->max_frames, nrec = sizeof(rg_mb_out) * c->n_mb * S * c->max_frames;
     for (int i = 0; i < 2; i++) {
@@ -1251,11 +1339,23 @@ static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, 
     CK(cudaStreamCreateWithFlags(&c->a_out, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->a_in, cudaStreamNonBlocking));
   }
-  int slot = c->a_slot;
-  c->a_slot ^= 1;
-  // sources into this slot's staging once the launch that last read it is done
+  return RG_OK;
+}
+
+// Checks a call's host sources and copies them into slot `slot`'s staging on the copy-in stream, once
+// the launch that last read that staging is done; dev receives the device planes.
+static int async_copy_in(rg_ctx* c, int slot, const uint8_t* const* planes, size_t stride_y, size_t stride_uv,
+                         int32_t frames, std::vector<const uint8_t*>& dev, const char* who) {
+  if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "%s: frames %d", who, frames);
+  int w = c->cfg.width, h = c->cfg.height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  if (stride_y < (size_t)w || stride_uv < (size_t)cw) return fail(RG_ERR_INVALID, "%s: stride too small", who);
+  int S = c->S;
+  for (int i = 0; i < 3 * S * frames; i++)
+    if (!planes[i]) return fail(RG_ERR_INVALID, "%s: picture %d stream %d null plane", who, i / 3 / S, (i / 3) % S);
+  int r = async_setup(c);
+  if (r) return r;
   CK(cudaStreamWaitEvent(c->a_in, c->a_kern_done[slot], 0));
-  std::vector<const uint8_t*> dev(3 * (size_t)S * frames);
+  dev.assign(3 * (size_t)S * frames, nullptr);
   const size_t ny = (size_t)w * h, nc = (size_t)cw * ch;
   for (int i = 0; i < S * frames; i++) {
     const uint8_t* const* pl = planes + 3 * i;
@@ -1266,6 +1366,22 @@ static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, 
     dev[3 * i + 2] = d + ny + nc;
   }
   CK(cudaEventRecord(c->a_in_done[slot], c->a_in));
+  return RG_OK;
+}
+
+static int async_gops(rg_ctx* c, const uint8_t* const* planes, size_t stride_y, size_t stride_uv, const int32_t* kinds,
+                      int32_t frames, rg_mb_out* out, bool bulk) {
+  if (!c || !planes || !kinds || !out) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: null argument");
+  int w = c->cfg.width, cw = (w + 1) / 2;
+  int S = c->S;
+  if (frames < 1 || frames > c->max_frames) return fail(RG_ERR_INVALID, "rg_analyse_gops_async: frames %d", frames);
+  int slot = c->a_slot;
+  std::vector<const uint8_t*> dev;
+  {
+    int r0 = async_copy_in(c, slot, planes, stride_y, stride_uv, frames, dev, "rg_analyse_gops_async");
+    if (r0) return r0;
+  }
+  c->a_slot ^= 1;
   // The previous launch is resolved (waited for, re-run if it failed) before the launch stream is
   // told to wait for this copy: resolving ends with a synchronisation of that stream, which would
   // otherwise wait for the copy too and hold the caller for its whole duration.

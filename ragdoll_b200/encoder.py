@@ -90,6 +90,39 @@ class H264Encoder:
             raise RgError(rc, lib().rg_last_error().decode())
         self._inflight.append((keep, len(frames)))
 
+    def _planes(self, frames):
+        keep, ptrs = [], []
+        for pics in frames:
+            if len(pics) != self.streams:
+                raise RgError(-1, f"submit: {len(pics)} pictures for {self.streams} streams")
+            for y, u, v in pics:
+                planes = [np.ascontiguousarray(p, np.uint8) for p in (y, u, v)]
+                keep.append(planes)
+                ptrs += [p.ctypes.data for p in planes]
+        return keep, ptrs
+
+    @staticmethod
+    def submit_group(encoders: Sequence["H264Encoder"], frames: Sequence[Sequence[Sequence[Frame]]]) -> None:
+        """frames[i][f][s]: the next len(frames[i]) pictures of every stream of encoders[i], all of
+        them analysed by one persistent launch (rg_encoder_submit_group); collect each encoder's
+        wave with its own collect()."""
+        n = len(encoders)
+        keeps, arrs, sy, suv = [], [], [], []
+        for e, fr in zip(encoders, frames):
+            keep, ptrs = e._planes(fr)
+            keeps.append(keep)
+            arrs.append((ctypes.c_void_p * len(ptrs))(*ptrs))
+            sy.append(keep[0][0].strides[0])
+            suv.append(keep[0][1].strides[0])
+        planes = (ctypes.c_void_p * n)(*[ctypes.cast(a, ctypes.c_void_p) for a in arrs])
+        hs = (ctypes.c_void_p * n)(*[e.h for e in encoders])
+        rc = lib().rg_encoder_submit_group(hs, n, planes, (ctypes.c_size_t * n)(*sy), (ctypes.c_size_t * n)(*suv),
+                                           len(frames[0]))
+        if rc:
+            raise RgError(rc, lib().rg_last_error().decode())
+        for e, keep, fr in zip(encoders, keeps, frames):
+            e._inflight.append((keep, len(fr)))
+
     def collect(self) -> List[List[bytes]]:
         """Access units of the oldest submitted wave, [f][s]."""
         if not self._inflight:

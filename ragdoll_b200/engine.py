@@ -60,6 +60,7 @@ EXPORTS = [
     "rg_net_set_hint_policy", "rg_net_set_coarse_range", "rg_analyse_gops_group",
     "rg_set_record_compaction", "rg_analyse_gops_fetch_compact", "rg_records_compact", "rg_records_expand",
     "rg_writer_picture_compact", "rg_encoder_record_bytes", "rg_group_graph_counts",
+    "rg_analyse_gops_group_async", "rg_analyse_gops_group_stream", "rg_encoder_submit_group",
 ]
 
 
@@ -164,6 +165,9 @@ def lib() -> ctypes.CDLL:
     L.rg_encoder_record_bytes.restype = ctypes.c_int64
     L.rg_encoder_record_bytes.argtypes = [P]
     L.rg_group_graph_counts.argtypes = [P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    L.rg_analyse_gops_group_async.argtypes = [P, ctypes.c_int32, P, P, P, P, ctypes.c_int32, P]
+    L.rg_encoder_submit_group.argtypes = [P, ctypes.c_int32, P, P, P, ctypes.c_int32]
+    L.rg_analyse_gops_group_stream.argtypes = [P, ctypes.c_int32, P, P, P, P, ctypes.c_int32, P]
     L.rg_set_analysis_form.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     L.rg_set_hints.argtypes = [P, P, ctypes.c_int32]
     L.rg_encoder_new_gops.argtypes = [P]

@@ -108,3 +108,85 @@ def test_group_launch_rejects_mixed_forms_and_duplicates():
         Engine.analyse_gops_group([a, a], [[0] * 3, [0] * 3], [96, 96], [48, 48], [[0], [0]], 1)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("give_up", [False, True])
+def test_group_encoder_waves_equal_each_encoder_alone(give_up):
+    """rg_encoder_submit_group: the waves of encoders of three sizes (a QP per stream), analysed by
+    one launch per wave and collected per encoder, give exactly the access units of the same
+    encoders submitting alone, over two waves. give_up: one warp and a lag of one macroblock-time
+    make a wait run out; each context re-runs its pictures and the access units are still exact."""
+    from ragdoll_b200.encoder import H264Encoder
+    from ragdoll_b200.engine import RG_PROFILE_MAIN
+    rng = np.random.default_rng(11)
+    qps = [rng.integers(20, 37, S).tolist() for _, _, S in SIZES]
+    clips = _clips()
+
+    def encoders():
+        out = []
+        for i, (w, h, S) in enumerate(SIZES):
+            e = H264Encoder(w, h, 28, profile=RG_PROFILE_MAIN, keyint=2 * F, streams=S, max_frames=F, threads=2)
+            for s in range(S):
+                e.set_stream_qp(s, qps[i][s])
+            out.append(e)
+        return out
+    group, alone = encoders(), encoders()
+    if give_up:   # the launch takes the largest grid of any context: one warp everywhere
+        for e in group:
+            e.set_pipeline_tuning(lag=1, grid=1, timeout_ms=300)
+    waves = [[[[clips[i][s][wv * F + f] for s in range(S)] for f in range(F)] for i, (_, _, S) in enumerate(SIZES)]
+             for wv in range(2)]
+    got, want = [], []
+    for wv in range(2):
+        H264Encoder.submit_group(group, waves[wv])
+        got.append([e.collect() for e in group])
+        for e, fr in zip(alone, waves[wv]):
+            e.submit(fr)
+        want.append([e.collect() for e in alone])
+    for wv in range(2):
+        for i, (w, h, S) in enumerate(SIZES):
+            assert got[wv][i] == want[wv][i], f"wave {wv}, size {w}x{h}: access units differ"
+    for e in group + alone:
+        e.close()
+
+
+def test_group_async_records_equal_each_context_alone():
+    """rg_analyse_gops_group_async: host sources of three sizes in, one launch, each context's
+    records copied into its own host buffer -- the records of each context analysed alone."""
+    import ctypes
+
+    from ragdoll_b200.engine import RECORD_DTYPE, RG_FRAME_IDR, RG_FRAME_P, lib
+    rng = np.random.default_rng(3)
+    qps = [rng.integers(20, 37, S).tolist() for _, _, S in SIZES]
+    clips = _clips()
+    group, alone = _engines(0, qps), _engines(0, qps)
+    L = lib()
+    n = len(SIZES)
+    keep, arrs, outs, kinds = [], [], [], []
+    for i, (w, h, S) in enumerate(SIZES):
+        ptrs, k = [], []
+        for f in range(F):
+            for s in range(S):
+                for p in clips[i][s][f]:
+                    a = np.ascontiguousarray(p)
+                    keep.append(a)
+                    ptrs.append(a.ctypes.data)
+                k.append(RG_FRAME_IDR if f == 0 else RG_FRAME_P)
+        arrs.append((ctypes.c_void_p * len(ptrs))(*ptrs))
+        kinds.append((ctypes.c_int32 * len(k))(*k))
+        outs.append(np.zeros((F, S, group[i].n_mb), RECORD_DTYPE))
+    P = ctypes.c_void_p
+    rc = L.rg_analyse_gops_group_async((P * n)(*[e.h for e in group]), n,
+                                       (P * n)(*[ctypes.cast(a, P) for a in arrs]),
+                                       (ctypes.c_size_t * n)(*[w for w, _, _ in SIZES]),
+                                       (ctypes.c_size_t * n)(*[(w + 1) // 2 for w, _, _ in SIZES]),
+                                       (P * n)(*[ctypes.cast(k, P) for k in kinds]), F,
+                                       (P * n)(*[o.ctypes.data for o in outs]))
+    assert rc == 0
+    for i, (w, h, S) in enumerate(SIZES):
+        assert L.rg_analyse_gops_wait(group[i].h, outs[i].ctypes.data) == 0
+        want = alone[i].analyse_gops([[clips[i][s][f] for s in range(S)] for f in range(F)],
+                                     [[RG_FRAME_IDR if f == 0 else RG_FRAME_P] * S for f in range(F)])
+        assert outs[i].tobytes() == want.tobytes(), f"size {w}x{h}: records differ"
+    for e in group + alone:
+        e.close()
