@@ -1033,7 +1033,7 @@ static int group_async(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* con
     rg_ctx* c = ctxs[i];
     const int sl = slot[i];
     c->a_slot = sl ^ 1;
-    c->a_seq[sl] = bulk ? 0 : 1;
+    c->a_seq[sl] = bulk ? -1 : 1;  // bulk: no flag is ever set; a fetch waits for the launch's end
     c->a_frames[sl] = frames;
     c->a_compact[sl] = false;
     CK(cudaEventRecord(c->a_kern_done[sl], c->stream));
