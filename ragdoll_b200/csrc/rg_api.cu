@@ -1009,11 +1009,15 @@ static int group_async(rg_ctx* const* ctxs, int32_t n, const uint8_t* const* con
     sy[i] = c->cfg.width;
     suv[i] = (c->cfg.width + 1) / 2;
   }
-  // earlier calls resolved (re-run if a wait gave up) before any launch stream waits for a copy
-  for (int i = 0; i < n; i++) {
-    int r = resolve_pending(ctxs[i], false);
-    if (r) return r;
-  }
+  // at most one earlier call left in flight per context (the call two back, which last used this
+  // staging slot, resolved -- re-run if a wait gave up -- and fetched): the launch is queued behind
+  // the running one, whose pictures the caller fetches meanwhile. A wait that gives up in the
+  // running launch re-runs both calls (resolve_oldest re-runs every pending call).
+  for (int i = 0; i < n; i++)
+    while (ctxs[i]->pend_count >= 2) {
+      int r = resolve_oldest(ctxs[i]);
+      if (r) return r;
+    }
   // streamed: the slot's flags cleared (its last call was resolved and fetched), each picture's set
   // to 1 by the launch (a constant, so the launch's CUDA graph replays)
   std::vector<int*> readies(n);
