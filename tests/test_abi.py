@@ -42,3 +42,27 @@ def test_create_rejects_bad_config_without_a_device():
 def test_version_string():
     from ragdoll_b200.engine import lib
     assert b"sm_100a" in lib().rg_version()
+
+
+def test_group_and_compaction_calls_reject_bad_arguments_without_a_device():
+    """The group calls, the compact-record calls and the encoder's group submit check their
+    arguments before touching a device: null pointers, context counts outside 1..8 and null
+    contexts are RG_ERR_INVALID."""
+    from ragdoll_b200.engine import lib
+    L = lib()
+    P = ctypes.c_void_p
+    one = (P * 1)(None)
+    sz = (ctypes.c_size_t * 1)(64)
+    for n in (0, 9, 1):
+        assert L.rg_analyse_gops_group(one, n, one, sz, sz, one, 1) < 0
+        assert L.rg_analyse_gops_group_async(one, n, one, sz, sz, one, 1, one) < 0
+        assert L.rg_analyse_gops_group_stream(one, n, one, sz, sz, one, 1, one) < 0
+        assert L.rg_encoder_submit_group(one, n, one, sz, sz, 1) < 0
+    assert L.rg_analyse_gops_group_async(None, 1, None, None, None, None, 1, None) < 0
+    assert L.rg_set_record_compaction(None, 96) < 0
+    data, nbytes = P(), ctypes.c_size_t()
+    assert L.rg_analyse_gops_fetch_compact(None, None, 0, ctypes.byref(data), ctypes.byref(nbytes)) < 0
+    assert L.rg_encoder_record_bytes(None) < 0
+    cap, lau = ctypes.c_int64(), ctypes.c_int64()
+    assert L.rg_group_graph_counts(None, ctypes.byref(cap), ctypes.byref(lau)) < 0
+    assert L.rg_last_error()
